@@ -1,0 +1,138 @@
+"""Synthetic structured tetrahedral meshes of the unit cube.
+
+The reference solve path consumes an ``fe_em::EMMeshData`` (nodes, TET4_EDGE
+elements with a material id, and a DIRICHLET / VECTOR_EDGE_ONLY boundary
+marker holding edge node pairs; ``include/fe_em/em_mesh_data.hpp:90-230``).
+This module builds the same data as flat numpy arrays for an n^3 hex grid with
+every hex split into 6 tetrahedra (Kuhn split), the layout every test and the
+benchmark use:
+
+* node gid = i + (n+1) * (j + (n+1) * k), coordinates (i, j, k) / n;
+* hexes in k -> j -> i order; hex vertices v0..v7 = (i,j,k), (i+1,j,k),
+  (i+1,j+1,k), (i,j+1,k) and the same at k+1;
+* tets per hex {0,1,2,6}, {0,2,3,6}, {0,3,7,6}, {0,7,4,6}, {0,4,5,6}, {0,5,1,6};
+* Dirichlet edges: every mesh edge lying in a boundary face (n x A = 0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KUHN = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6],
+                 [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]], dtype=np.int64)
+# TET4 local edges, ElementGeometry::get_local_edges(TET4)
+GEO_EDGES = np.array([[0, 1], [1, 2], [0, 2], [0, 3], [1, 3], [2, 3]], dtype=np.int64)
+
+# Source region kinds (same values as the C ABI's EMG_SRC_*).
+SRC_BOX = 1
+SRC_ANNULUS_Z = 2
+
+
+@dataclass
+class Source:
+    """Uniform current density ``j`` inside an open region evaluated at
+    quadrature points: BOX p = (xmin, xmax, ymin, ymax, zmin, zmax);
+    ANNULUS_Z p = (cx, cy, rmin, rmax, zmin, zmax)."""
+    kind: int
+    j: tuple
+    p: tuple
+
+
+@dataclass
+class CubeMesh:
+    n: int
+    xyz: np.ndarray          # (V, 3) float64
+    tets: np.ndarray         # (T, 4) int32
+    material: np.ndarray     # (T,) int32
+    dirichlet: np.ndarray    # (D, 2) int32 node pairs
+    nu: np.ndarray           # per-material reluctivity 1/mu
+    sigma: np.ndarray        # per-material conductivity
+    sources: list = field(default_factory=list)
+    name: str = ""
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.xyz.shape[0])
+
+    @property
+    def n_tets(self) -> int:
+        return int(self.tets.shape[0])
+
+
+def cube_topology(n: int):
+    """Nodes, tets and boundary-face edge pairs of the n^3 Kuhn-split cube."""
+    n1 = n + 1
+    g = np.arange(n1, dtype=np.float64) / n
+    kk, jj, ii = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")
+    xyz = np.stack([g[ii.ravel()], g[jj.ravel()], g[kk.ravel()]], axis=1)
+    hk, hj, hi = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()
+    off = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    verts = np.stack([(hi + a) + n1 * ((hj + b) + n1 * (hk + c)) for a, b, c in off], axis=1)
+    tets = verts[:, KUHN].reshape(-1, 4).astype(np.int32)
+    # boundary-face edges: unique element edges whose two nodes share a
+    # coordinate plane at 0 or n
+    e = tets[:, GEO_EDGES].reshape(-1, 2).astype(np.int64)
+    e.sort(axis=1)
+    e = np.unique(e[:, 0] * (n1 ** 3) + e[:, 1])
+    a, b = e // (n1 ** 3), e % (n1 ** 3)
+    ia, ja, ka = a % n1, (a // n1) % n1, a // (n1 * n1)
+    ib, jb, kb = b % n1, (b // n1) % n1, b // (n1 * n1)
+    on = np.zeros(a.shape, dtype=bool)
+    for ca, cb in ((ia, ib), (ja, jb), (ka, kb)):
+        on |= (ca == cb) & ((ca == 0) | (ca == n))
+    dirichlet = np.stack([a[on], b[on]], axis=1).astype(np.int32)
+    return xyz, tets, dirichlet
+
+
+def centroids(xyz: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    return xyz[tets].mean(axis=1)
+
+
+def plain_small(n: int = 16) -> CubeMesh:
+    """Plain method, small: nu = 1 everywhere, J = (0,0,1) inside the central
+    box [0.375, 0.625]^3 (grid-aligned at n = 16)."""
+    xyz, tets, dirichlet = cube_topology(n)
+    return CubeMesh(n=n, xyz=xyz, tets=tets, material=np.zeros(len(tets), np.int32),
+                    dirichlet=dirichlet, nu=np.array([1.0]), sigma=np.array([0.0]),
+                    sources=[Source(SRC_BOX, (0.0, 0.0, 1.0),
+                                    (0.375, 0.625, 0.375, 0.625, 0.375, 0.625))],
+                    name=f"cube{n}_box")
+
+
+def plain_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
+    """Plain method at scale: iron block [0.25,0.75]^2 x [0.4,0.6] (mu_r =
+    1000, by tet centroid), mu_r = 1 elsewhere; z-directed coil current on the
+    annulus 0.3 < r < 0.45 (axis x = y = 0.5), 0.2 < z < 0.8."""
+    xyz, tets, dirichlet = cube_topology(n)
+    c = centroids(xyz, tets)
+    iron = ((c[:, 0] > 0.25) & (c[:, 0] < 0.75) & (c[:, 1] > 0.25) & (c[:, 1] < 0.75)
+            & (c[:, 2] > 0.4) & (c[:, 2] < 0.6))
+    return CubeMesh(n=n, xyz=xyz, tets=tets, material=iron.astype(np.int32),
+                    dirichlet=dirichlet, nu=np.array([1.0, 1.0 / mu_iron]),
+                    sigma=np.array([0.0, 0.0]),
+                    sources=[Source(SRC_ANNULUS_Z, (0.0, 0.0, 1.0),
+                                    (0.5, 0.5, 0.3, 0.45, 0.2, 0.8))],
+                    name=f"cube{n}_iron_coil")
+
+
+def random_instance(n: int, seed: int) -> CubeMesh:
+    """One many-instance case: a random axis-aligned box with mu_r in
+    [1, 1000] (1 elsewhere) and a uniform J_z in a random sub-box."""
+    rng = np.random.default_rng(seed)
+    xyz, tets, dirichlet = cube_topology(n)
+    lo = rng.uniform(0.05, 0.5, 3)
+    hi = lo + rng.uniform(0.2, 0.45, 3)
+    mu = rng.uniform(1.0, 1000.0)
+    c = centroids(xyz, tets)
+    inside = np.all((c > lo) & (c < np.minimum(hi, 0.95)), axis=1)
+    slo = rng.uniform(0.1, 0.5, 3)
+    shi = slo + rng.uniform(0.15, 0.4, 3)
+    return CubeMesh(n=n, xyz=xyz, tets=tets, material=inside.astype(np.int32),
+                    dirichlet=dirichlet, nu=np.array([1.0, 1.0 / mu]),
+                    sigma=np.array([0.0, 0.0]),
+                    sources=[Source(SRC_BOX, (0.0, 0.0, 1.0),
+                                    (slo[0], min(shi[0], 0.9), slo[1], min(shi[1], 0.9),
+                                     slo[2], min(shi[2], 0.9)))],
+                    name=f"cube{n}_rand{seed}")

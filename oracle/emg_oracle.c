@@ -1,0 +1,757 @@
+/*
+ * emg_oracle.c -- CPU oracle (test infrastructure only) for the TET4 Nedelec
+ * curl-curl solve path of Poofee/emagddm.  See emg_oracle.h for how each part
+ * is pinned.  Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline
+ * and the reference arm) load this file's library.
+ *
+ * Deliberate deviations from the reference's literal element output, each
+ * switchable by a flag for element-level comparison:
+ *   1. edge signs: the reference scatters unsigned element matrices
+ *      (src/numeric/em_assembly.cpp:654-718); a conforming H(curl) assembly
+ *      needs s_k = +-1 per local edge.  Convention: global edge oriented from
+ *      the lower to the higher global node ID.  ORC_FLAG_NO_EDGE_SIGNS turns
+ *      signs off.
+ *   2. covariant map W_phys = J^-T W_ref; the reference text divides by detJ as
+ *      well (src/numeric/magnetic_vector_3d_integrator.cpp:429-430);
+ *      ORC_FLAG_PIOLA_LITERAL restores that.
+ *   3. Hammer 4-point rule with weights summing to 1/6; the reference pops the
+ *      third point (src/numeric/gauss_quadrature.cpp:205-219) and, called with
+ *      TET4_EDGE, returns no points at all (:36-60), so its K_e is zero.
+ *      ORC_FLAG_QUAD3_LITERAL restores the 3-point rule.
+ *   4. F_i = int W_i . J_s is computed; the reference returns zero
+ *      (magnetic_vector_3d_integrator.cpp:343-364, formula at :353).
+ */
+#include "emg_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* TET4 geometry edge table, ElementGeometry::get_local_edges(TET4)
+ * (src/fe_em/element_geometry.cpp:115-126). */
+static const int GEO_EDGE[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+/* Nedelec TET4_EDGE edge table (src/numeric/nedelec_element.cpp:54-60). */
+static const int NED_EDGE[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+/* Constant reference curls, curlTet4Edge (nedelec_element.cpp:461-505). */
+static const double CURL_REF[6][3] = {{0, 0, -2}, {-2, 0, 0}, {0, -2, 0},
+                                      {0, -2, 2}, {2, 0, -2}, {-2, 2, 0}};
+
+/* ---------------------------------------------------------------------------
+ * Stable LSD radix sort of (key, payload) pairs, 11-bit digits.
+ * ------------------------------------------------------------------------- */
+static int radix_sort_u64(int64_t n, uint64_t* key, int64_t* pay, uint64_t max_key) {
+  if (n <= 1) return 0;
+  int bits = 0;
+  while (bits < 64 && (max_key >> bits) != 0) bits++;
+  if (bits == 0) return 0;
+  uint64_t* k2 = (uint64_t*)malloc((size_t)n * sizeof(uint64_t));
+  int64_t* p2 = (int64_t*)malloc((size_t)n * sizeof(int64_t));
+  if (!k2 || !p2) { free(k2); free(p2); return -1; }
+  const int D = 11, B = 1 << D;
+  int64_t cnt[1 << 11];
+  uint64_t *ks = key, *kd = k2;
+  int64_t *ps = pay, *pd = p2;
+  for (int shift = 0; shift < bits; shift += D) {
+    memset(cnt, 0, sizeof(cnt));
+    for (int64_t i = 0; i < n; i++) cnt[(ks[i] >> shift) & (B - 1)]++;
+    int64_t s = 0;
+    for (int b = 0; b < B; b++) { int64_t c = cnt[b]; cnt[b] = s; s += c; }
+    for (int64_t i = 0; i < n; i++) {
+      int64_t d = cnt[(ks[i] >> shift) & (B - 1)]++;
+      kd[d] = ks[i];
+      pd[d] = ps[i];
+    }
+    uint64_t* tk = ks; ks = kd; kd = tk;
+    int64_t* tp = ps; ps = pd; pd = tp;
+  }
+  if (ks != key) {
+    memcpy(key, ks, (size_t)n * sizeof(uint64_t));
+    memcpy(pay, ps, (size_t)n * sizeof(int64_t));
+  }
+  free(k2);
+  free(p2);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Global edge IDs: key = sorted global node pair, ID = order of first
+ * appearance over elements in order and local edges in order
+ * (global_edge_id_generator.cpp:44-97).  Sort-based restatement of the hash
+ * map: a stable sort groups equal keys with the first appearance leading its
+ * group, and IDs are the prefix count of group leaders by position.
+ * ------------------------------------------------------------------------- */
+int orc_edge_ids(int64_t n_tets, const int32_t* tets, int32_t* elem_edge,
+                 int32_t* edge_nodes, int64_t* n_edges) {
+  int64_t m = 6 * n_tets;
+  *n_edges = 0;
+  if (n_tets <= 0) return 0;
+  int32_t maxg = 0;
+  for (int64_t i = 0; i < 4 * n_tets; i++) {
+    if (tets[i] < 0) return ORC_INVALID_INPUT;
+    if (tets[i] > maxg) maxg = tets[i];
+  }
+  uint64_t span = (uint64_t)maxg + 1;
+  uint64_t* key = (uint64_t*)malloc((size_t)m * sizeof(uint64_t));
+  int64_t* pos = (int64_t*)malloc((size_t)m * sizeof(int64_t));
+  int64_t* id_at = (int64_t*)malloc((size_t)m * sizeof(int64_t));
+  if (!key || !pos || !id_at) { free(key); free(pos); free(id_at); return -1; }
+  for (int64_t t = 0; t < n_tets; t++)
+    for (int k = 0; k < 6; k++) {
+      uint64_t a = (uint64_t)tets[4 * t + GEO_EDGE[k][0]];
+      uint64_t b = (uint64_t)tets[4 * t + GEO_EDGE[k][1]];
+      uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+      key[6 * t + k] = lo * span + hi;
+      pos[6 * t + k] = 6 * t + k;
+    }
+  if (radix_sort_u64(m, key, pos, span * span - 1)) { free(key); free(pos); free(id_at); return -1; }
+  /* leader flags by position */
+  for (int64_t i = 0; i < m; i++) id_at[i] = 0;
+  for (int64_t i = 0; i < m; i++)
+    if (i == 0 || key[i] != key[i - 1]) id_at[pos[i]] = 1;
+  int64_t run = 0;
+  for (int64_t i = 0; i < m; i++) {
+    int64_t f = id_at[i];
+    id_at[i] = f ? run : -1;
+    run += f;
+  }
+  *n_edges = run;
+  int64_t lead = 0;
+  for (int64_t i = 0; i < m; i++) {
+    if (i == 0 || key[i] != key[i - 1]) lead = pos[i];
+    int64_t id = id_at[lead];
+    elem_edge[pos[i]] = (int32_t)id;
+    if (edge_nodes) {
+      edge_nodes[2 * id] = (int32_t)(key[i] / span);
+      edge_nodes[2 * id + 1] = (int32_t)(key[i] % span);
+    }
+  }
+  free(key);
+  free(pos);
+  free(id_at);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * DOF numbering and tree gauge.
+ * ------------------------------------------------------------------------- */
+static int64_t find_edge(const uint64_t* skey, const int32_t* sid, int64_t ne, uint64_t k) {
+  int64_t lo = 0, hi = ne;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (skey[mid] < k) lo = mid + 1; else hi = mid;
+  }
+  if (lo < ne && skey[lo] == k) return sid[lo];
+  return -1;
+}
+
+int orc_dof_build(int64_t n_tets, const int32_t* tets, const int32_t* elem_edge,
+                  const int32_t* edge_nodes, int64_t n_edges, int64_t n_dir,
+                  const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge,
+                  int32_t* l2g, int32_t* edge_dof, int64_t* n_free,
+                  int64_t* n_dofs, int32_t* root_node) {
+  int64_t E = n_edges;
+  *n_free = 0; *n_dofs = 0;
+  if (root_node) *root_node = -1;
+  if (n_tets <= 0 || E <= 0) return ORC_INVALID_INPUT;
+  int32_t maxg = 0;
+  for (int64_t i = 0; i < 2 * E; i++) if (edge_nodes[i] > maxg) maxg = edge_nodes[i];
+  for (int64_t i = 0; i < 4 * n_tets; i++) if (tets[i] > maxg) maxg = tets[i];
+  uint64_t span = (uint64_t)maxg + 1;
+
+  /* Edge lookup by sorted node pair (GlobalEdgeIDGenerator::getGlobalEdgeID,
+   * global_edge_id_generator.cpp:124-140). */
+  uint64_t* skey = (uint64_t*)malloc((size_t)E * sizeof(uint64_t));
+  int64_t* spay = (int64_t*)malloc((size_t)E * sizeof(int64_t));
+  int32_t* sid = (int32_t*)malloc((size_t)E * sizeof(int32_t));
+  char* constrained = (char*)calloc((size_t)E, 1);
+  int32_t* free_of = (int32_t*)malloc((size_t)E * sizeof(int32_t));
+  if (!skey || !spay || !sid || !constrained || !free_of) return -1;
+  for (int64_t e = 0; e < E; e++) {
+    skey[e] = (uint64_t)edge_nodes[2 * e] * span + (uint64_t)edge_nodes[2 * e + 1];
+    spay[e] = e;
+  }
+  radix_sort_u64(E, skey, spay, span * span - 1);
+  for (int64_t e = 0; e < E; e++) sid[e] = (int32_t)spay[e];
+  free(spay);
+
+  /* markConstrainedDOFs (em_dof_manager.cpp:152-243): Dirichlet node pairs
+   * -> global edge IDs; pairs that are not mesh edges are skipped. */
+  for (int64_t d = 0; d < n_dir; d++) {
+    int32_t a = dir_pairs[2 * d], b = dir_pairs[2 * d + 1];
+    if (a < 0 || b < 0 || (uint64_t)a >= span || (uint64_t)b >= span) continue;
+    uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    int64_t id = find_edge(skey, sid, E, lo * span + hi);
+    if (id >= 0) constrained[id] = 1;
+  }
+  /* assignPrenumbering + renumberFreeDOFs (em_dof_manager.cpp:91-150,
+   * :245-286): for an all-vector mesh the prenumber of an edge is its global
+   * ID, and the free index is the rank among unconstrained prenumbers. */
+  int64_t nf = 0;
+  for (int64_t e = 0; e < E; e++) free_of[e] = constrained[e] ? -1 : (int32_t)nf++;
+  *n_free = nf;
+
+  if (gauge < 0) {
+    for (int64_t e = 0; e < E; e++) edge_dof[e] = free_of[e];
+    *n_dofs = nf;
+  } else {
+    /* ---- TreeGauge::build (src/fe_em/tree_gauge.cpp:37-212) ---- */
+    /* MeshGraphExtractor (mesh_graph_extractor.cpp:29-176): compact node
+     * index = rank of the global node ID among referenced nodes. */
+    int32_t* cidx = (int32_t*)malloc((size_t)span * sizeof(int32_t));
+    for (uint64_t g = 0; g < span; g++) cidx[g] = -1;
+    for (int64_t i = 0; i < 4 * n_tets; i++) cidx[tets[i]] = 1;
+    int32_t V = 0;
+    for (uint64_t g = 0; g < span; g++) if (cidx[g] == 1) cidx[g] = V++;
+    /* sorted adjacency with the edge of each entry */
+    int64_t* aptr = (int64_t*)calloc((size_t)V + 1, sizeof(int64_t));
+    int32_t* anb = (int32_t*)malloc((size_t)(2 * E) * sizeof(int32_t));
+    int32_t* aed = (int32_t*)malloc((size_t)(2 * E) * sizeof(int32_t));
+    for (int64_t e = 0; e < E; e++) {
+      aptr[cidx[edge_nodes[2 * e]] + 1]++;
+      aptr[cidx[edge_nodes[2 * e + 1]] + 1]++;
+    }
+    for (int32_t v = 0; v < V; v++) aptr[v + 1] += aptr[v];
+    int64_t* fill = (int64_t*)malloc((size_t)V * sizeof(int64_t));
+    for (int32_t v = 0; v < V; v++) fill[v] = aptr[v];
+    for (int64_t e = 0; e < E; e++) {
+      int32_t u = cidx[edge_nodes[2 * e]], w = cidx[edge_nodes[2 * e + 1]];
+      anb[fill[u]] = w; aed[fill[u]++] = (int32_t)e;
+      anb[fill[w]] = u; aed[fill[w]++] = (int32_t)e;
+    }
+    free(fill);
+    for (int32_t v = 0; v < V; v++) { /* insertion sort by neighbour */
+      for (int64_t i = aptr[v] + 1; i < aptr[v + 1]; i++) {
+        int32_t nb = anb[i], ed = aed[i];
+        int64_t j = i - 1;
+        while (j >= aptr[v] && anb[j] > nb) { anb[j + 1] = anb[j]; aed[j + 1] = aed[j]; j--; }
+        anb[j + 1] = nb; aed[j + 1] = ed;
+      }
+    }
+    /* selectRootNode DIRICHLET_BOUNDARY (spanning_tree.cpp:517-540): smaller
+     * compact endpoint of the smallest constrained edge ID, else node 0. */
+    int32_t root = 0;
+    for (int64_t e = 0; e < E; e++)
+      if (constrained[e]) { root = cidx[edge_nodes[2 * e]]; break; }
+    if (root_node) *root_node = root;
+
+    char* tree = (char*)calloc((size_t)E, 1);
+    char* visited = (char*)calloc((size_t)V, 1);
+    int32_t* queue = (int32_t*)malloc((size_t)V * sizeof(int32_t));
+    int32_t* dn = (int32_t*)malloc(64 * sizeof(int32_t));
+    int32_t* de = (int32_t*)malloc(64 * sizeof(int32_t));
+    int32_t* nn = (int32_t*)malloc(64 * sizeof(int32_t));
+    int32_t* ne_ = (int32_t*)malloc(64 * sizeof(int32_t));
+    int64_t cap = 64;
+    int64_t qh = 0, qt = 0;
+    visited[root] = 1;
+    queue[qt++] = root;
+    if (gauge == ORC_GAUGE_REF) {
+      /* buildBFSTreeWithBoundaryPriority (spanning_tree.cpp:295-416): per
+       * dequeued node, unvisited neighbours over constrained edges are
+       * enqueued first, then the others, each in ascending index order. */
+      while (qh < qt) {
+        int32_t u = queue[qh++];
+        int64_t deg = aptr[u + 1] - aptr[u];
+        if (deg > cap) {
+          cap = deg;
+          dn = (int32_t*)realloc(dn, cap * sizeof(int32_t));
+          de = (int32_t*)realloc(de, cap * sizeof(int32_t));
+          nn = (int32_t*)realloc(nn, cap * sizeof(int32_t));
+          ne_ = (int32_t*)realloc(ne_, cap * sizeof(int32_t));
+        }
+        int64_t nd = 0, nnn = 0;
+        for (int64_t i = aptr[u]; i < aptr[u + 1]; i++) {
+          int32_t v = anb[i];
+          if (visited[v]) continue;
+          if (constrained[aed[i]]) { dn[nd] = v; de[nd++] = aed[i]; }
+          else { nn[nnn] = v; ne_[nnn++] = aed[i]; }
+        }
+        for (int64_t i = 0; i < nd; i++)
+          if (!visited[dn[i]]) { visited[dn[i]] = 1; tree[de[i]] = 1; queue[qt++] = dn[i]; }
+        for (int64_t i = 0; i < nnn; i++)
+          if (!visited[nn[i]]) { visited[nn[i]] = 1; tree[ne_[i]] = 1; queue[qt++] = nn[i]; }
+      }
+    } else {
+      /* boundary_first (this build's corrected gauge): phase 1 spans the
+       * constrained-edge subgraph by BFS from the root; phase 2 continues a
+       * plain BFS over all edges from every node reached so far, in visit
+       * order.  Each unconstrained node then owns exactly one tree edge. */
+      while (qh < qt) {
+        int32_t u = queue[qh++];
+        for (int64_t i = aptr[u]; i < aptr[u + 1]; i++) {
+          int32_t v = anb[i];
+          if (!visited[v] && constrained[aed[i]]) { visited[v] = 1; tree[aed[i]] = 1; queue[qt++] = v; }
+        }
+      }
+      /* constrained subgraph components not reached from the root */
+      for (int64_t e = 0; e < E; e++) {
+        if (!constrained[e]) continue;
+        int32_t s0 = cidx[edge_nodes[2 * e]];
+        if (visited[s0]) continue;
+        visited[s0] = 1; queue[qt++] = s0;
+        while (qh < qt) {
+          int32_t u = queue[qh++];
+          for (int64_t i = aptr[u]; i < aptr[u + 1]; i++) {
+            int32_t v = anb[i];
+            if (!visited[v] && constrained[aed[i]]) { visited[v] = 1; tree[aed[i]] = 1; queue[qt++] = v; }
+          }
+        }
+      }
+      qh = 0;
+      while (qh < qt) {
+        int32_t u = queue[qh++];
+        for (int64_t i = aptr[u]; i < aptr[u + 1]; i++) {
+          int32_t v = anb[i];
+          if (!visited[v]) { visited[v] = 1; tree[aed[i]] = 1; queue[qt++] = v; }
+        }
+      }
+    }
+    /* remaining components: plain BFS from the lowest unvisited index
+     * (spanning_tree.cpp:418-445) */
+    for (int32_t s = 0; s < V; s++) {
+      if (visited[s]) continue;
+      visited[s] = 1;
+      qh = qt = 0;
+      queue[qt++] = s;
+      while (qh < qt) {
+        int32_t u = queue[qh++];
+        for (int64_t i = aptr[u]; i < aptr[u + 1]; i++) {
+          int32_t v = anb[i];
+          if (!visited[v]) { visited[v] = 1; tree[aed[i]] = 1; queue[qt++] = v; }
+        }
+      }
+    }
+    /* MultiConnectedDomainDetector::selectCirculationDOFs
+     * (multi_connected_domain.cpp:190-232): evenly spaced picks from the
+     * ascending cotree list (before constrained edges are promoted). */
+    char* circ = (char*)calloc((size_t)E, 1);
+    int64_t n_cot = 0;
+    for (int64_t e = 0; e < E; e++) if (!tree[e]) n_cot++;
+    if (n_hole_markers > 0 && n_cot > 0) {
+      int64_t pick = n_hole_markers < n_cot ? n_hole_markers : n_cot;
+      int32_t* cot = (int32_t*)malloc((size_t)n_cot * sizeof(int32_t));
+      int64_t c = 0;
+      for (int64_t e = 0; e < E; e++) if (!tree[e]) cot[c++] = (int32_t)e;
+      for (int64_t i = 0; i < pick; i++) {
+        int64_t idx = (i * n_cot) / pick;
+        if (idx > n_cot - 1) idx = n_cot - 1;
+        circ[cot[idx]] = 1;
+      }
+      free(cot);
+    }
+    /* classifyEdges + buildReducedMapping (tree_gauge.cpp:159-212): final
+     * cotree = cotree minus constrained minus circulation; reduced index =
+     * ascending edge ID rank, then circulation edges not yet numbered. */
+    int32_t* red = (int32_t*)malloc((size_t)E * sizeof(int32_t));
+    int64_t nr = 0;
+    for (int64_t e = 0; e < E; e++) {
+      red[e] = -1;
+      if (!tree[e] && !constrained[e] && !circ[e]) red[e] = (int32_t)nr++;
+    }
+    for (int64_t e = 0; e < E; e++)
+      if (circ[e] && red[e] < 0) red[e] = (int32_t)nr++;
+    /* renumberVectorDOFsWithTreeGauge (em_dof_manager.cpp:501-626): only
+     * free entries are rewritten; cotree or circulation edges take their
+     * reduced index, the rest become -1. */
+    for (int64_t e = 0; e < E; e++) {
+      if (free_of[e] < 0) { edge_dof[e] = -1; continue; }
+      int cot_or_circ = (!tree[e] && !constrained[e] && !circ[e]) || circ[e];
+      edge_dof[e] = cot_or_circ ? red[e] : -1;
+    }
+    *n_dofs = nr;
+    free(red); free(circ); free(tree); free(visited); free(queue);
+    free(dn); free(de); free(nn); free(ne_);
+    free(aptr); free(anb); free(aed); free(cidx);
+  }
+  /* buildVectorElementMapping (em_dof_manager.cpp:353-393) */
+  for (int64_t i = 0; i < 6 * n_tets; i++) l2g[i] = edge_dof[elem_edge[i]];
+  free(skey); free(sid); free(constrained); free(free_of);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Element integration (MagneticVector3DIntegrator, intended formulas).
+ * ------------------------------------------------------------------------- */
+static void ref_basis(int k, const double* xi, double* w) {
+  /* evalTet4Edge (nedelec_element.cpp:411-459) */
+  double l1 = xi[0], l2 = xi[1], l3 = xi[2], l4 = 1.0 - xi[0] - xi[1] - xi[2];
+  switch (k) {
+    case 0: w[0] = l2; w[1] = -l1; w[2] = 0.0; break;
+    case 1: w[0] = 0.0; w[1] = l3; w[2] = -l2; break;
+    case 2: w[0] = -l3; w[1] = 0.0; w[2] = l1; break;
+    case 3: w[0] = l4 + l1; w[1] = l1; w[2] = l1; break;
+    case 4: w[0] = l2; w[1] = l4 + l2; w[2] = l2; break;
+    default: w[0] = l3; w[1] = l3; w[2] = l4 + l3; break;
+  }
+}
+
+static void source_at(const orc_source* src, int32_t n_src, const double* x, double* js) {
+  js[0] = js[1] = js[2] = 0.0;
+  for (int32_t s = 0; s < n_src; s++) {
+    const double* p = src[s].p;
+    int in = 0;
+    if (src[s].kind == ORC_SRC_BOX) {
+      in = x[0] > p[0] && x[0] < p[1] && x[1] > p[2] && x[1] < p[3] && x[2] > p[4] && x[2] < p[5];
+    } else if (src[s].kind == ORC_SRC_ANNULUS_Z) {
+      double dx = x[0] - p[0], dy = x[1] - p[1];
+      double r = sqrt(dx * dx + dy * dy);
+      in = r > p[2] && r < p[3] && x[2] > p[4] && x[2] < p[5];
+    }
+    if (in) { js[0] += src[s].j[0]; js[1] += src[s].j[1]; js[2] += src[s].j[2]; }
+  }
+}
+
+void orc_element(const double* X, double nu, double sigma, const orc_source* src,
+                 int32_t n_src, int32_t flags, double* Ke, double* Me, double* Fe) {
+  /* GaussQuadrature::getTet4Points(4) intended points (gauss_quadrature.cpp:
+   * 198-219), weight 1/24 each. */
+  const double a = (5.0 - sqrt(5.0)) / 20.0, b = (5.0 + 3.0 * sqrt(5.0)) / 20.0;
+  double qp[4][3] = {{a, a, b}, {a, b, a}, {b, a, a}, {a, a, a}};
+  int nq = 4;
+  if (flags & ORC_FLAG_QUAD3_LITERAL) { qp[2][0] = a; qp[2][1] = a; qp[2][2] = a; nq = 3; }
+  const double w = 1.0 / 24.0;
+  for (int i = 0; i < 36; i++) { Ke[i] = 0.0; if (Me) Me[i] = 0.0; }
+  for (int i = 0; i < 6; i++) if (Fe) Fe[i] = 0.0;
+  /* calcJacobian with the TET4 Lagrange gradients (shape_function_base.hpp:
+   * 335-364, lagrange_element.cpp:658-683): columns x0-x3, x1-x3, x2-x3. */
+  double J[3][3];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) J[r][c] = X[3 * c + r] - X[9 + r];
+  double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+               J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+               J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double adet = fabs(det);
+  if (adet < 1e-15) return; /* magnetic_vector_3d_integrator.cpp:169 */
+  double inv[3][3]; /* J^-1 */
+  inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+  inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+  inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  /* physical curls: J curl_ref / detJ (nedelec_element.cpp:246-247) */
+  double c[6][3];
+  for (int k = 0; k < 6; k++)
+    for (int r = 0; r < 3; r++)
+      c[k][r] = (J[r][0] * CURL_REF[k][0] + J[r][1] * CURL_REF[k][1] + J[r][2] * CURL_REF[k][2]) / det;
+  for (int q = 0; q < nq; q++) {
+    /* computeStiffnessMatrix (magnetic_vector_3d_integrator.cpp:139-229) */
+    double wf = w * adet * nu;
+    for (int i = 0; i < 6; i++)
+      for (int j = i; j < 6; j++) {
+        double d = c[i][0] * c[j][0] + c[i][1] * c[j][1] + c[i][2] * c[j][2];
+        Ke[6 * i + j] += wf * d;
+        if (j != i) Ke[6 * j + i] = Ke[6 * i + j];
+      }
+    /* basis values for M and F: covariant map J^-T W_ref */
+    double W[6][3];
+    for (int k = 0; k < 6; k++) {
+      double wr[3];
+      ref_basis(k, qp[q], wr);
+      for (int r = 0; r < 3; r++) {
+        W[k][r] = inv[0][r] * wr[0] + inv[1][r] * wr[1] + inv[2][r] * wr[2];
+        if (flags & ORC_FLAG_PIOLA_LITERAL) W[k][r] /= det;
+      }
+    }
+    if (Me && (flags & ORC_FLAG_MASS) && sigma > 0.0) {
+      /* computeMassMatrix (:233-323) */
+      double wm = w * adet * sigma;
+      for (int i = 0; i < 6; i++)
+        for (int j = i; j < 6; j++) {
+          double d = W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2];
+          Me[6 * i + j] += wm * d;
+          if (j != i) Me[6 * j + i] = Me[6 * i + j];
+        }
+    }
+    if (Fe && n_src > 0) {
+      /* F_i = int W_i . J_s (theory formula at :353), physical position by
+       * the TET4 map N0=xi, N1=eta, N2=zeta, N3=1-xi-eta-zeta (:437-483). */
+      double N[4] = {qp[q][0], qp[q][1], qp[q][2], 1.0 - qp[q][0] - qp[q][1] - qp[q][2]};
+      double x[3];
+      for (int r = 0; r < 3; r++) x[r] = N[0] * X[r] + N[1] * X[3 + r] + N[2] * X[6 + r] + N[3] * X[9 + r];
+      double js[3];
+      source_at(src, n_src, x, js);
+      double wfj = w * adet;
+      for (int i = 0; i < 6; i++) Fe[i] += wfj * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
+    }
+  }
+}
+
+void orc_edge_signs(const int32_t* tet, int32_t* s) {
+  for (int k = 0; k < 6; k++) {
+    int32_t ga = tet[NED_EDGE[k][0]], gb = tet[NED_EDGE[k][1]];
+    s[k] = gb < ga ? 1 : -1;
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * CSR pattern and numeric assembly (EMAssembly::assemble,
+ * src/numeric/em_assembly.cpp:144-420, scatter :654-765; duplicates summed
+ * as SparseConverter::to_eigen does, sparse_converter.cpp:19-80).
+ * ------------------------------------------------------------------------- */
+static int build_incidence(int64_t n_tets, const int32_t* l2g, int64_t n, int64_t** iptr_o, int64_t** ilist_o) {
+  int64_t* iptr = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+  if (!iptr) return -1;
+  for (int64_t i = 0; i < 6 * n_tets; i++) {
+    int32_t r = l2g[i];
+    if (r >= n) { free(iptr); return ORC_INVALID_INPUT; }
+    if (r >= 0) iptr[r + 1]++;
+  }
+  for (int64_t r = 0; r < n; r++) iptr[r + 1] += iptr[r];
+  int64_t* ilist = (int64_t*)malloc((size_t)(iptr[n] > 0 ? iptr[n] : 1) * sizeof(int64_t));
+  int64_t* fill = (int64_t*)malloc((size_t)(n > 0 ? n : 1) * sizeof(int64_t));
+  for (int64_t r = 0; r < n; r++) fill[r] = iptr[r];
+  for (int64_t i = 0; i < 6 * n_tets; i++)
+    if (l2g[i] >= 0) ilist[fill[l2g[i]]++] = i;
+  free(fill);
+  *iptr_o = iptr;
+  *ilist_o = ilist;
+  return 0;
+}
+
+int orc_pattern(int64_t n_tets, const int32_t* l2g, int64_t n, int64_t* row_ptr,
+                int32_t* col, int64_t* nnz) {
+  int64_t *iptr, *ilist;
+  int rc = build_incidence(n_tets, l2g, n, &iptr, &ilist);
+  if (rc) return rc;
+  row_ptr[0] = 0;
+  int64_t total = 0;
+  int32_t buf[1024];
+  for (int64_t r = 0; r < n; r++) {
+    int m = 0;
+    for (int64_t q = iptr[r]; q < iptr[r + 1]; q++) {
+      int64_t t = ilist[q] / 6;
+      for (int k = 0; k < 6; k++) {
+        int32_t c = l2g[6 * t + k];
+        if (c < 0) continue;
+        int found = 0;
+        for (int z = 0; z < m; z++) if (buf[z] == c) { found = 1; break; }
+        if (!found && m < 1024) buf[m++] = c;
+      }
+    }
+    for (int i = 1; i < m; i++) { /* sort the row */
+      int32_t v = buf[i];
+      int j = i - 1;
+      while (j >= 0 && buf[j] > v) { buf[j + 1] = buf[j]; j--; }
+      buf[j + 1] = v;
+    }
+    if (col) memcpy(col + total, buf, (size_t)m * sizeof(int32_t));
+    total += m;
+    row_ptr[r + 1] = total;
+  }
+  *nnz = total;
+  free(iptr);
+  free(ilist);
+  return 0;
+}
+
+static int64_t slot_of(const int64_t* row_ptr, const int32_t* col, int32_t r, int32_t c) {
+  int64_t lo = row_ptr[r], hi = row_ptr[r + 1];
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    if (col[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  return (lo < row_ptr[r + 1] && col[lo] == c) ? lo : -1;
+}
+
+int orc_assemble(int64_t n_nodes, const double* xyz, int64_t n_tets,
+                 const int32_t* tets, const int32_t* material, const int32_t* l2g,
+                 const double* nu_mat, const double* sigma_mat, int32_t n_mat,
+                 const orc_source* src, int32_t n_src, int32_t flags, int64_t n,
+                 const int64_t* row_ptr, const int32_t* col, double* kval,
+                 double* mval, double* rhs) {
+  int64_t nnz = row_ptr[n];
+  for (int64_t i = 0; i < nnz; i++) { kval[i] = 0.0; if (mval) mval[i] = 0.0; }
+  if (rhs) for (int64_t i = 0; i < n; i++) rhs[i] = 0.0;
+  for (int64_t t = 0; t < n_tets; t++) {
+    int32_t mid = material ? material[t] : 0;
+    if (mid < 0 || mid >= n_mat) continue; /* em_assembly.cpp:270-276 */
+    double X[12];
+    for (int a = 0; a < 4; a++) {
+      int32_t g = tets[4 * t + a];
+      if (g < 0 || g >= n_nodes) return ORC_INVALID_INPUT;
+      X[3 * a] = xyz[3 * g]; X[3 * a + 1] = xyz[3 * g + 1]; X[3 * a + 2] = xyz[3 * g + 2];
+    }
+    double Ke[36], Me[36], Fe[6];
+    orc_element(X, nu_mat[mid], sigma_mat ? sigma_mat[mid] : 0.0, src, n_src, flags, Ke, Me, Fe);
+    int32_t s[6];
+    orc_edge_signs(tets + 4 * t, s);
+    if (flags & ORC_FLAG_NO_EDGE_SIGNS) for (int k = 0; k < 6; k++) s[k] = 1;
+    const int32_t* L = l2g + 6 * t;
+    for (int i = 0; i < 6; i++) {
+      if (L[i] < 0) continue;
+      if (rhs) rhs[L[i]] += s[i] * Fe[i];
+      for (int j = 0; j < 6; j++) {
+        if (L[j] < 0) continue;
+        int64_t p = slot_of(row_ptr, col, L[i], L[j]);
+        if (p < 0) return ORC_INVALID_INPUT;
+        kval[p] += (double)(s[i] * s[j]) * Ke[6 * i + j];
+        if (mval && (flags & ORC_FLAG_MASS)) mval[p] += (double)(s[i] * s[j]) * Me[6 * i + j];
+      }
+    }
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Krylov solvers.
+ * ------------------------------------------------------------------------- */
+void orc_spmv(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
+              const double* x, double* y) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    double s = 0.0;
+    for (int64_t k = rp[i]; k < rp[i + 1]; k++) s += val[k] * x[col[k]];
+    y[i] = s;
+  }
+}
+
+static double vdot(int64_t n, const double* a, const double* b) {
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (int64_t i = 0; i < n; i++) s += a[i] * b[i];
+  return s;
+}
+
+static void jacobi_inverse(int64_t n, const int64_t* rp, const int32_t* col,
+                           const double* val, double* dinv) {
+  /* CGSolver::setup_preconditioner (iterative_solvers.cpp:261-292) */
+  for (int64_t i = 0; i < n; i++) {
+    double d = 0.0;
+    for (int64_t k = rp[i]; k < rp[i + 1]; k++) if (col[k] == i) d += val[k];
+    dinv[i] = fabs(d) > 1e-15 ? 1.0 / d : 1.0;
+  }
+}
+
+int orc_pcg(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
+            const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
+            int32_t* iterations, double* residual_norm) {
+  *iterations = 0;
+  *residual_norm = 0.0;
+  if (n <= 0) return ORC_INVALID_INPUT;
+  double* r = (double*)malloc((size_t)n * sizeof(double));
+  double* z = (double*)malloc((size_t)n * sizeof(double));
+  double* p = (double*)malloc((size_t)n * sizeof(double));
+  double* q = (double*)malloc((size_t)n * sizeof(double));
+  double* dinv = (double*)malloc((size_t)n * sizeof(double));
+  if (!r || !z || !p || !q || !dinv) return -1;
+  if (precond) jacobi_inverse(n, rp, col, val, dinv);
+  else for (int64_t i = 0; i < n; i++) dinv[i] = 1.0;
+  for (int64_t i = 0; i < n; i++) { x[i] = 0.0; r[i] = b[i]; z[i] = dinv[i] * r[i]; p[i] = z[i]; }
+  double rz = vdot(n, r, z);
+  double bnorm = sqrt(vdot(n, b, b));
+  int status = ORC_MAX_ITER_REACHED;
+  if (bnorm < 1e-15) { /* :361-367 / :440-446 */
+    free(r); free(z); free(p); free(q); free(dinv);
+    return ORC_SUCCESS;
+  }
+  double res = sqrt(vdot(n, r, r)) / bnorm, prev = res;
+  int32_t it;
+  for (it = 1; it <= max_iter; it++) {
+    orc_spmv(n, rp, col, val, p, q);
+    double pq = vdot(n, p, q);
+    if (fabs(pq) < 1e-30) { status = ORC_NUMERICAL_ERROR; break; }
+    double alpha = rz / pq;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+      z[i] = dinv[i] * r[i];
+    }
+    double rz_new = vdot(n, r, z);
+    res = sqrt(vdot(n, r, r)) / bnorm;
+    if (res < tol) { status = ORC_SUCCESS; break; }
+    if (it > 10 && res > prev * 1000.0) { status = ORC_DIVERGED; break; }
+    double beta = rz_new / rz;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    rz = rz_new;
+    prev = res;
+  }
+  *iterations = it <= max_iter ? it : max_iter;
+  *residual_norm = res;
+  free(r); free(z); free(p); free(q); free(dinv);
+  return status;
+}
+
+int orc_bicgstab(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
+                 const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
+                 int32_t* iterations, double* residual_norm) {
+  *iterations = 0;
+  *residual_norm = 0.0;
+  if (n <= 0) return ORC_INVALID_INPUT;
+  size_t sz = (size_t)n * sizeof(double);
+  double *r = malloc(sz), *rh = malloc(sz), *p = malloc(sz), *v = malloc(sz);
+  double *s = malloc(sz), *z = malloc(sz), *t = malloc(sz), *dinv = malloc(sz);
+  if (!r || !rh || !p || !v || !s || !z || !t || !dinv) return -1;
+  if (precond) jacobi_inverse(n, rp, col, val, dinv);
+  else for (int64_t i = 0; i < n; i++) dinv[i] = 1.0;
+  for (int64_t i = 0; i < n; i++) { x[i] = 0.0; r[i] = b[i]; rh[i] = b[i]; p[i] = b[i]; v[i] = 0.0; }
+  double rho = vdot(n, r, rh), alpha = 1.0, omega = 1.0;
+  double bnorm = sqrt(vdot(n, b, b));
+  int status = ORC_MAX_ITER_REACHED;
+  if (bnorm < 1e-15) { free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv); return ORC_SUCCESS; }
+  double res = sqrt(vdot(n, r, r)) / bnorm, prev = res;
+  int dcount = 0;
+  int32_t it;
+  for (it = 1; it <= max_iter; it++) {
+    double rho_old = rho;
+    rho = vdot(n, r, rh);
+    if (fabs(rho) < 1e-30) { status = ORC_NUMERICAL_ERROR; break; }
+    double beta = (rho / rho_old) * (alpha / omega);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+    orc_spmv(n, rp, col, val, p, v);
+    double rv = vdot(n, rh, v);
+    if (fabs(rv) < 1e-30) { status = ORC_NUMERICAL_ERROR; break; }
+    alpha = rho / rv;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) s[i] = r[i] - alpha * v[i];
+    res = sqrt(vdot(n, s, s)) / bnorm;
+    if (res < tol) { /* early exit on ||s|| (:1050-1058) */
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; i++) x[i] += alpha * p[i];
+      *iterations = it;
+      *residual_norm = res;
+      free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv);
+      return ORC_SUCCESS;
+    }
+    /* precondition s only (:1061) */
+    for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * s[i];
+    orc_spmv(n, rp, col, val, z, t);
+    double tt = vdot(n, t, t);
+    omega = fabs(tt) < 1e-30 ? 0.0 : vdot(n, z, t) / tt;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+      x[i] += alpha * p[i] + omega * z[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    res = sqrt(vdot(n, r, r)) / bnorm;
+    if (res < tol) { status = ORC_SUCCESS; break; }
+    if (res > prev * 1.5 && it > 20) {
+      if (++dcount >= 3) { status = ORC_DIVERGED; break; }
+    } else {
+      dcount = 0;
+    }
+    if (it > 10 && res > prev * 1000.0) { status = ORC_DIVERGED; break; }
+    prev = res;
+  }
+  *iterations = it <= max_iter ? it : max_iter;
+  *residual_norm = res;
+  free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv);
+  return status;
+}

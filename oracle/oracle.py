@@ -1,0 +1,182 @@
+"""ctypes wrapper of the CPU oracle (emg_oracle.c) -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline / reference
+arm) import this module; the product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+I64P = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+STATUS = {0: "SUCCESS", 1: "NUMERICAL_ERROR", 2: "DIVERGED", 3: "MAX_ITER_REACHED", 4: "INVALID_INPUT"}
+FLAG_MASS, FLAG_NO_EDGE_SIGNS, FLAG_PIOLA_LITERAL, FLAG_QUAD3_LITERAL = 1, 2, 4, 8
+GAUGE_NONE, GAUGE_REF, GAUGE_BOUNDARY_FIRST = -1, 0, 1
+
+
+class OrcSource(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("j", C.c_double * 3), ("p", C.c_double * 6)]
+
+
+def build() -> str:
+    path = os.path.join(_HERE, "libemg_oracle.so")
+    src = os.path.join(_HERE, "emg_oracle.c")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "libemg_oracle.so"])
+    return path
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(build())
+        L = _LIB
+        L.orc_edge_ids.argtypes = [C.c_int64, I32P, I32P, I32P, C.POINTER(C.c_int64)]
+        L.orc_dof_build.argtypes = [C.c_int64, I32P, I32P, I32P, C.c_int64, C.c_int64, I32P,
+                                    C.c_int32, C.c_int32, I32P, I32P, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        L.orc_element.argtypes = [F64P, C.c_double, C.c_double, C.c_void_p, C.c_int32, C.c_int32,
+                                  F64P, F64P, F64P]
+        L.orc_element.restype = None
+        L.orc_edge_signs.argtypes = [I32P, I32P]
+        L.orc_edge_signs.restype = None
+        L.orc_pattern.argtypes = [C.c_int64, I32P, C.c_int64, I64P, C.c_void_p, C.POINTER(C.c_int64)]
+        L.orc_assemble.argtypes = [C.c_int64, F64P, C.c_int64, I32P, I32P, I32P, F64P, F64P,
+                                   C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int64, I64P,
+                                   I32P, F64P, C.c_void_p, C.c_void_p]
+        L.orc_spmv.argtypes = [C.c_int64, I64P, I32P, F64P, F64P, F64P]
+        L.orc_spmv.restype = None
+        for f in (L.orc_pcg, L.orc_bicgstab):
+            f.argtypes = [C.c_int64, I64P, I32P, F64P, F64P, F64P, C.c_double, C.c_int32,
+                          C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.orc_num_threads.restype = C.c_int
+    return _LIB
+
+
+def sources_array(sources):
+    if not sources:
+        return None, 0
+    arr = (OrcSource * len(sources))()
+    for k, s in enumerate(sources):
+        arr[k].kind = int(s.kind)
+        for i in range(3):
+            arr[k].j[i] = float(s.j[i])
+        for i in range(6):
+            arr[k].p[i] = float(s.p[i])
+    return arr, len(sources)
+
+
+def edge_ids(tets):
+    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    T = tets.shape[0]
+    elem_edge = np.empty(6 * T, np.int32)
+    edge_nodes = np.empty(12 * T, np.int32)
+    ne = C.c_int64()
+    rc = lib().orc_edge_ids(T, tets.ravel(), elem_edge, edge_nodes, C.byref(ne))
+    assert rc == 0, rc
+    return elem_edge.reshape(T, 6), edge_nodes[: 2 * ne.value].reshape(-1, 2)
+
+
+def dof_build(tets, dirichlet, gauge=GAUGE_REF, n_holes=0, elem_edge=None, edge_nodes=None):
+    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    if elem_edge is None:
+        elem_edge, edge_nodes = edge_ids(tets)
+    T, E = tets.shape[0], edge_nodes.shape[0]
+    d = np.ascontiguousarray(dirichlet, dtype=np.int32).reshape(-1)
+    l2g = np.empty(6 * T, np.int32)
+    edge_dof = np.empty(E, np.int32)
+    nf, nd, root = C.c_int64(), C.c_int64(), C.c_int32()
+    rc = lib().orc_dof_build(T, tets.ravel(), np.ascontiguousarray(elem_edge, np.int32).ravel(),
+                             np.ascontiguousarray(edge_nodes, np.int32).ravel(), E, d.size // 2,
+                             d if d.size else np.zeros(2, np.int32), n_holes, gauge, l2g, edge_dof,
+                             C.byref(nf), C.byref(nd), C.byref(root))
+    assert rc == 0, rc
+    return dict(elem_edge=elem_edge, edge_nodes=edge_nodes, l2g=l2g.reshape(T, 6),
+                edge_dof=edge_dof, n_edges=E, n_free=nf.value, n_dofs=nd.value, root=root.value)
+
+
+def element(X, nu=1.0, sigma=0.0, sources=(), flags=0):
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(12)
+    K, M, F = np.empty(36), np.empty(36), np.empty(6)
+    arr, ns = sources_array(list(sources))
+    lib().orc_element(X, nu, sigma, C.cast(arr, C.c_void_p) if arr is not None else None, ns,
+                      flags, K, M, F)
+    return K.reshape(6, 6), M.reshape(6, 6), F
+
+
+def edge_signs(tet):
+    s = np.empty(6, np.int32)
+    lib().orc_edge_signs(np.ascontiguousarray(tet, np.int32), s)
+    return s
+
+
+def pattern(l2g, n):
+    l2g = np.ascontiguousarray(l2g, dtype=np.int32).ravel()
+    T = l2g.size // 6
+    rp = np.empty(n + 1, np.int64)
+    nnz = C.c_int64()
+    rc = lib().orc_pattern(T, l2g, n, rp, None, C.byref(nnz))
+    assert rc == 0, rc
+    col = np.empty(max(nnz.value, 1), np.int32)
+    rc = lib().orc_pattern(T, l2g, n, rp, col.ctypes.data_as(C.c_void_p), C.byref(nnz))
+    assert rc == 0, rc
+    return rp, col[: nnz.value]
+
+
+def assemble(mesh, l2g, n, flags=0, rp=None, col=None):
+    """Merged CSR (int64 row_ptr, int32 col), K values, M values, rhs."""
+    if rp is None:
+        rp, col = pattern(l2g, n)
+    nnz = int(rp[-1])
+    kval = np.empty(nnz)
+    mval = np.empty(nnz) if flags & FLAG_MASS else None
+    rhs = np.empty(n)
+    arr, ns = sources_array(mesh.sources)
+    rc = lib().orc_assemble(mesh.n_nodes, np.ascontiguousarray(mesh.xyz).ravel(), mesh.n_tets,
+                            np.ascontiguousarray(mesh.tets, np.int32).ravel(),
+                            np.ascontiguousarray(mesh.material, np.int32),
+                            np.ascontiguousarray(l2g, np.int32).ravel(),
+                            np.ascontiguousarray(mesh.nu, np.float64),
+                            np.ascontiguousarray(mesh.sigma, np.float64), len(mesh.nu),
+                            C.cast(arr, C.c_void_p) if arr is not None else None, ns, flags, n,
+                            rp, col, kval,
+                            mval.ctypes.data_as(C.c_void_p) if mval is not None else None,
+                            rhs.ctypes.data_as(C.c_void_p))
+    assert rc == 0, rc
+    return rp, col, kval, mval, rhs
+
+
+def spmv(rp, col, val, x):
+    y = np.empty(rp.size - 1)
+    lib().orc_spmv(rp.size - 1, rp, col, val, np.ascontiguousarray(x, np.float64), y)
+    return y
+
+
+def _krylov(fn, rp, col, val, b, tol, max_iter, precond):
+    n = rp.size - 1
+    x = np.empty(n)
+    it, res = C.c_int32(), C.c_double()
+    st = fn(n, rp, col, val, np.ascontiguousarray(b, np.float64), x, tol, max_iter, precond,
+            C.byref(it), C.byref(res))
+    return x, st, it.value, res.value
+
+
+def pcg(rp, col, val, b, tol=1e-8, max_iter=1000, precond=1):
+    return _krylov(lib().orc_pcg, rp, col, val, b, tol, max_iter, precond)
+
+
+def bicgstab(rp, col, val, b, tol=1e-8, max_iter=1000, precond=1):
+    return _krylov(lib().orc_bicgstab, rp, col, val, b, tol, max_iter, precond)
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())

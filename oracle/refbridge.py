@@ -1,0 +1,114 @@
+"""ctypes wrapper of oracle/_ref/libemg_ref.so -- TEST INFRASTRUCTURE.
+
+The library is the reference's own C++ sources compiled in place by
+oracle/Makefile.ref plus ref_bridge.cpp.  It is built here (where the
+reference sources exist) and travels with the repository snapshot; when it is
+absent, callers skip the reference comparisons.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(_HERE, "_ref", "libemg_ref.so")
+_LIB = None
+
+I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+I64P = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def available() -> bool:
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(PATH)
+        L = _LIB
+        L.refb_quiet.argtypes = [C.c_int]
+        L.refb_quiet.restype = None
+        L.refb_dof_build.argtypes = [C.c_int64, C.c_int64, I32P, C.c_int64, I32P, C.c_int32,
+                                     C.c_int32, I32P, I32P, C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.refb_pattern.argtypes = [C.c_int64, F64P, C.c_int64, I32P, I32P, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64)]
+        L.refb_krylov.argtypes = [C.c_int32, C.c_int64, I64P, I32P, F64P, F64P, F64P, C.c_double,
+                                  C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]
+        L.refb_nedelec_tet4.argtypes = [C.c_double, C.c_double, C.c_double, F64P, F64P]
+        L.refb_nedelec_tet4.restype = None
+        L.refb_quadrature.argtypes = [C.c_int32, C.c_int32, F64P]
+        L.refb_integrator_k.argtypes = [F64P, C.c_double, F64P]
+        L.refb_quiet(1)
+    return _LIB
+
+
+def dof_build(n_nodes, tets, dirichlet, gauge=True, n_holes=0):
+    tets = np.ascontiguousarray(tets, np.int32)
+    T = tets.shape[0]
+    d = np.ascontiguousarray(dirichlet, np.int32).reshape(-1)
+    ee = np.empty(6 * T, np.int32)
+    l2g = np.empty(6 * T, np.int32)
+    ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+    rc = lib().refb_dof_build(n_nodes, T, tets.ravel(), d.size // 2,
+                              d if d.size else np.zeros(2, np.int32), n_holes, int(gauge), ee,
+                              l2g, C.byref(ne), C.byref(nf), C.byref(nd))
+    assert rc == 0, rc
+    return dict(elem_edge=ee.reshape(T, 6), l2g=l2g.reshape(T, 6), n_edges=ne.value,
+                n_free=nf.value, n_dofs=nd.value)
+
+
+def pattern(xyz, tets, l2g):
+    tets = np.ascontiguousarray(tets, np.int32)
+    l2g = np.ascontiguousarray(l2g, np.int32).ravel()
+    xyz = np.ascontiguousarray(xyz, np.float64).ravel()
+    nnz, raw, nr = C.c_int64(), C.c_int64(), C.c_int64()
+    rc = lib().refb_pattern(xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g, None, None,
+                            C.byref(nnz), C.byref(raw), C.byref(nr))
+    assert rc == 0, rc
+    rp = np.empty(nr.value + 1, np.int64)
+    col = np.empty(nnz.value, np.int32)
+    rc = lib().refb_pattern(xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g,
+                            rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                            C.byref(nnz), C.byref(raw), C.byref(nr))
+    assert rc == 0, rc
+    return rp, col, raw.value
+
+
+def krylov(kind, rp, col, val, b, tol=1e-8, max_iter=1000, precond=1):
+    """kind 0 = CGSolver, 1 = BiCGSTABSolver.  Returns x, status, iterations,
+    relative residual, set_matrix ms, solve ms."""
+    n = rp.size - 1
+    x = np.zeros(n)
+    it, res, s_ms, t_ms = C.c_int32(), C.c_double(), C.c_double(), C.c_double()
+    st = lib().refb_krylov(kind, n, np.ascontiguousarray(rp, np.int64),
+                           np.ascontiguousarray(col, np.int32), np.ascontiguousarray(val, np.float64),
+                           np.ascontiguousarray(b, np.float64), x, tol, max_iter, precond,
+                           C.byref(it), C.byref(res), C.byref(s_ms), C.byref(t_ms))
+    return x, st, it.value, res.value, s_ms.value, t_ms.value
+
+
+def nedelec_tet4(xi, eta, zeta):
+    w, c = np.empty(18), np.empty(18)
+    lib().refb_nedelec_tet4(xi, eta, zeta, w, c)
+    return w.reshape(6, 3), c.reshape(6, 3)
+
+
+def quadrature(edge_type, order):
+    p = np.zeros(16)
+    n = lib().refb_quadrature(edge_type, order, p)
+    return p.reshape(4, 4)[:n]
+
+
+def integrator_k(X, mu=1.0):
+    K = np.empty(36)
+    rc = lib().refb_integrator_k(np.ascontiguousarray(X, np.float64).ravel(), mu, K)
+    assert rc == 0, rc
+    return K.reshape(6, 6)
