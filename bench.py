@@ -1,0 +1,370 @@
+"""Benchmark of the B200 solve path on the 'plain method at scale' workload.
+
+Workload (one step = one pass of the hot path): the 64^3 hex grid of the unit
+cube split into 6 tets per hex (1,572,864 TET4_EDGE elements), iron block
+mu_r = 1000 in [0.25,0.75]^2 x [0.4,0.6], z-directed coil current on the
+annulus 0.3 < r < 0.45, 0.2 < z < 0.8, n x A = 0 on all faces, reference tree
+gauge (bit-exact numbering), FP64 assembly on the GPU (CSR pattern + K + F),
+then Jacobi-PCG to a relative residual of 1e-8.  The edge numbering / gauge is
+host integer setup done once per mesh (reported as setup_dof_ms).
+
+`value` times the step with inputs resident in HBM (emg_system_create_device
++ emg_system_assemble + emg_system_solve); `e2e` times the same C-ABI calls
+with host buffers (geometry and DOF map copied in, solution copied out).
+Both in solves/s; ms_per_step is the time to a 1e-8 residual.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-8 residual, learned+batched vs plain PCG/FETI-DP; SpMV GB/s vs HBM"
+TOL = 1e-8
+MAX_ITER = 50000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="hex grid size (64 = the quoted workload)")
+    ap.add_argument("--cpu-iters", type=int, default=20, help="iterations in the CPU sample")
+    return ap.parse_args()
+
+
+def workload(n):
+    from emagddm_b200 import mesh
+    return mesh.plain_scale(n)
+
+
+def workload_config(n, n_dofs=None, nnz=None):
+    cfg = {"workload": f"cube{n}_iron_coil: {n}^3 hex x 6 TET4_EDGE ({6 * n ** 3} tets), mu_r 1000 "
+                       f"block, annulus coil J_z, ref tree gauge, FP64 GPU assembly + Jacobi-PCG "
+                       f"to 1e-8",
+           "n": n, "tets": 6 * n ** 3, "gauge": "ref", "tol": TOL, "precond": "jacobi",
+           "l2": "inputs larger than L2 (CSR values+indices > 126 MB), no flush"}
+    if n_dofs is not None:
+        cfg["dofs"] = int(n_dofs)
+    if nnz is not None:
+        cfg["nnz"] = int(nnz)
+        cfg["csr_bytes"] = int(12 * nnz + 4 * (n_dofs + 1))
+    return cfg
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons through NVML while running."""
+
+    def __init__(self, dev_index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._t = None
+        self.dev_index = dev_index
+
+    def __enter__(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.dev_index)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            names = {getattr(N, k): k for k in dir(N) if k.startswith("nvmlClocksEventReason")
+                     and isinstance(getattr(N, k), int)}
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                        r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for bit, name in names.items():
+                            if bit and (r & bit) == bit and name not in ("nvmlClocksEventReasonAll",):
+                                self.reasons.add(name.replace("nvmlClocksEventReason", ""))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.1)
+            self._t = threading.Thread(target=run, daemon=True)
+            self._t.start()
+        except Exception as e:  # NVML unavailable: report it
+            self.reasons.add(f"nvml_unavailable:{type(e).__name__}")
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "samples": len(self.samples),
+                "reasons": sorted(self.reasons)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the SpMV kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "cg_spmv_dot_cube64.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch_full:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------- ours
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from emagddm_b200 import _abi, api
+    L = _abi.lib()
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    m = workload(args.n)
+    md = api.EMMeshData.from_cube(m)
+    t0 = time.perf_counter()
+    dm = api.EMDOFManager(md)
+    dm.build()
+    dm.applyTreeGauge(api.GaugeMode.REF)
+    setup_dof_ms = (time.perf_counter() - t0) * 1e3
+    l2g = np.ascontiguousarray(dm.getElemLocalToGlobal(), np.int32)
+    n_dofs = int(l2g.max()) + 1
+    xyz = np.ascontiguousarray(m.xyz, np.float64)
+    tets = np.ascontiguousarray(m.tets, np.int32)
+    mat = np.ascontiguousarray(m.material, np.int32)
+    d_xyz, d_tets = torch.from_numpy(xyz).to(dev), torch.from_numpy(tets).to(dev)
+    d_mat, d_l2g = torch.from_numpy(mat).to(dev), torch.from_numpy(l2g).to(dev)
+    d_x = torch.empty(n_dofs, dtype=torch.float64, device=dev)
+    h_x = np.empty(n_dofs)
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    src, nsrc = _abi.sources_array(m.sources)
+    srcp = C.cast(src, C.c_void_p)
+    nu = np.ascontiguousarray(m.nu)
+    sigma = np.ascontiguousarray(m.sigma)
+    cfg = _abi.KrylovConfig(TOL, MAX_ITER, _abi.PRECOND_JACOBI)
+    info = {}
+
+    def step(resident: bool):
+        h = C.c_void_p()
+        if resident:
+            rc = L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                            C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                            C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h))
+        else:
+            rc = L.emg_system_create(xyz.shape[0], _abi.ptr(xyz), tets.shape[0], _abi.ptr(tets),
+                                     _abi.ptr(mat), _abi.ptr(l2g), n_dofs, sp, C.byref(h))
+        _abi.check(rc, "emg_system_create")
+        _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
+                   "emg_system_assemble")
+        out = _abi.Result()
+        if resident:
+            rc = L.emg_system_solve(h, 0, C.byref(cfg), C.c_void_p(d_x.data_ptr()), 1, sp, C.byref(out))
+        else:
+            rc = L.emg_system_solve(h, 0, C.byref(cfg), _abi.ptr(h_x), 0, sp, C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"solve status {rc}: {L.emg_last_error().decode()}")
+        if "nnz" not in info:
+            n_, nnz_ = C.c_int64(), C.c_int64()
+            L.emg_system_info(h, C.byref(n_), C.byref(nnz_))
+            info["nnz"] = nnz_.value
+        info["iters"] = out.iterations
+        info["res"] = out.residual_norm
+        info["solve_ms"] = out.solve_time_ms
+        L.emg_system_destroy(h)
+
+    def timed(resident, k, w):
+        for _ in range(w):
+            step(resident)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            step(resident)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        return max_over_ranks(ms)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with Clocks(local_rank) as clk:
+        total_ms = timed(True, args.steps, args.warmup)
+    iters = info["iters"]
+    total_e2e = timed(False, args.steps, 1)
+    e2e_iters = info["iters"]
+
+    # roofline of the dominant kernel (SpMV + p.q of CG), live CUDA-event times
+    h = C.c_void_p()
+    _abi.check(L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                          C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                          C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h)), "create")
+    _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp), "asm")
+    kt = (C.c_double * 3)()
+    _abi.check(L.emg_cg_kernel_times(L.emg_system_matrix(h, 0), 50, sp, kt), "kernel times")
+    L.emg_system_destroy(h)
+    nnz = info["nnz"]
+    spmv_bytes = 12 * nnz + 4 * (n_dofs + 1) + 8 * n_dofs + 8 * n_dofs
+    peak, peak_kind = measured_peak()
+    achieved = spmv_bytes / (kt[0] * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    it_ms = sum(kt[:3])
+
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms * 1e-3)
+    e2e_value = world * args.steps / (total_e2e * 1e-3)
+    chunks = -(-iters // 16)
+    launches_per_step = 11 + 1 + 2 + chunks * 16 * 3
+    h2d = xyz.nbytes + tets.nbytes + mat.nbytes + l2g.nbytes
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seedless structured cube mesh; iron block + annulus coil)",
+        "config": {**workload_config(args.n, n_dofs, nnz), "parallelism": f"replicas{world}",
+                   "pcg_iterations": iters, "final_residual": info["res"],
+                   "setup_dof_ms": setup_dof_ms,
+                   "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]},
+                   "cg_iteration_ms_kernels": it_ms,
+                   "solve_ms": info["solve_ms"]},
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(h_x.nbytes), "ms_per_step": total_e2e / args.steps,
+                "pcg_iterations": e2e_iters},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "roofline": {"kernel": "k_cg_spmv_dot (CSR SpMV + p.q)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": spmv_bytes},
+    }
+    if rank == 0:
+        line["cpu_baseline"] = cpu_baseline(args, m, l2g, n_dofs, iters)
+    return line
+
+
+# ----------------------------------------------------------------- CPU side
+def cpu_system(m, l2g, n_dofs):
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    rp, col = O.pattern(l2g, n_dofs)
+    rp, col, kv, _, rhs = O.assemble(m, l2g, n_dofs, rp=rp, col=col)
+    return rp, col, kv, rhs, (time.perf_counter() - t0) * 1e3
+
+
+def cpu_sample(m, l2g, n_dofs, iters_needed, sample_iters):
+    """Reference CGSolver (oracle/_ref) when built, else the oracle port:
+    a bounded sample of iterations, projected to the full solve."""
+    from oracle import oracle as O
+    from oracle import refbridge as R
+    rp, col, kv, rhs, asm_ms = cpu_system(m, l2g, n_dofs)
+    if R.available():
+        _, st, it, res, setup_ms, solve_ms = R.krylov(0, rp, col, kv, rhs, tol=TOL,
+                                                      max_iter=sample_iters, precond=1)
+        kind, cores = "reference", 1
+        what = (f"reference CGSolver+Jacobi (Eigen, 1 thread) set_matrix + {it} iterations on the same "
+                f"system, projected to {iters_needed} iterations; assembly by the restated oracle "
+                f"(1 thread; the reference's TET4_EDGE integrator returns zeros)")
+    else:
+        t0 = time.perf_counter()
+        _, st, it, res = O.pcg(rp, col, kv, rhs, tol=TOL, max_iter=sample_iters, precond=1)
+        solve_ms, setup_ms = (time.perf_counter() - t0) * 1e3, 0.0
+        kind, cores = "port", O.num_threads()
+        what = f"oracle port Jacobi-PCG, {it} iterations, projected to {iters_needed}"
+    per_iter = solve_ms / max(it, 1)
+    total_ms = asm_ms + setup_ms + per_iter * iters_needed
+    return total_ms, {"kind": kind, "cores": cores, "sample": what,
+                      "assembly_ms": asm_ms, "set_matrix_ms": setup_ms, "ms_per_iteration": per_iter,
+                      "projected_ms_per_solve": total_ms}
+
+
+def cpu_baseline(args, m, l2g, n_dofs, iters):
+    total_ms, d = cpu_sample(m, l2g, n_dofs, iters, args.cpu_iters)
+    return {"value": 1e3 / total_ms, "unit": "solves/s", **d}
+
+
+def run_reference(args):
+    from oracle import oracle as O
+    m = workload(args.n)
+    dof = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+    l2g = dof["l2g"]
+    n_dofs = int(l2g.max()) + 1
+    rp, col, kv, rhs, _ = cpu_system(m, l2g, n_dofs)
+    # iterations to 1e-8 of this system, from the oracle port on all host threads
+    _, st, iters_needed, _ = O.pcg(rp, col, kv, rhs, tol=TOL, max_iter=MAX_ITER, precond=1)
+    vals = []
+    d = None
+    for k in range(args.warmup + args.steps):
+        total_ms, d = cpu_sample(m, l2g, n_dofs, iters_needed, args.cpu_iters)
+        if k >= args.warmup:
+            vals.append(total_ms)
+    ms = statistics.mean(vals)
+    v = 1e3 / ms
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {**workload_config(args.n, n_dofs, int(rp[-1])), "pcg_iterations": iters_needed},
+            "cpu_baseline": {"value": v, **d},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        line = run_ours(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

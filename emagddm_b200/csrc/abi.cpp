@@ -1,0 +1,455 @@
+// abi.cpp -- the extern "C" entry points declared in include/emagddm_b200.h.
+// Handles wrap host C++ objects (numbering) and device objects (assembly,
+// CSR, Krylov workspaces).  No exception crosses the ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "device.h"
+#include "internal.h"
+
+struct emg_mesh_t {
+  emg::Mesh m;
+};
+struct emg_dofmap_t {
+  emg::DofMap d;
+};
+struct emg_csr_t {
+  emg::DevCsr* csr = nullptr;
+  bool owned = true;
+};
+struct emg_system_t {
+  emg::System s;
+  emg_csr_t k_handle, m_handle;
+};
+
+namespace emg {
+namespace {
+thread_local std::string g_error;
+}
+void set_error(const std::string& msg) { g_error = msg; }
+}  // namespace emg
+
+namespace {
+
+using emg::set_error;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return EMG_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return EMG_ERR_INTERNAL;
+  } catch (...) {
+    set_error("unknown exception");
+    return EMG_ERR_INTERNAL;
+  }
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+template <class T>
+int upload(T** dst, const T* src, int64_t count, bool src_on_device, cudaStream_t st) {
+  size_t bytes = sizeof(T) * static_cast<size_t>(count > 0 ? count : 1);
+  EMG_CK(cudaMallocAsync(reinterpret_cast<void**>(dst), bytes, st));
+  if (count > 0 && src)
+    EMG_CK(cudaMemcpyAsync(*dst, src, sizeof(T) * count,
+                           src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  return EMG_SUCCESS;
+}
+
+int system_create_impl(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
+                       const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
+                       emg_system* out, bool on_device) {
+  if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
+  *out = nullptr;
+  if (n_nodes <= 0 || n_tets <= 0 || !xyz || !tets || !l2g) {
+    set_error("mesh is empty");  // em_assembly.cpp:154-166
+    return EMG_INVALID_INPUT;
+  }
+  if (n_dofs <= 0) {
+    // matrix dimension = largest equation index + 1 (em_assembly.cpp:190-215)
+    std::vector<int32_t> h;
+    const int32_t* src = l2g;
+    if (on_device) {
+      h.resize(6 * n_tets);
+      EMG_CK(cudaMemcpy(h.data(), l2g, sizeof(int32_t) * 6 * n_tets, cudaMemcpyDeviceToHost));
+      src = h.data();
+    }
+    int64_t mx = -1;
+    for (int64_t i = 0; i < 6 * n_tets; ++i) mx = std::max<int64_t>(mx, src[i]);
+    n_dofs = mx + 1;
+    if (n_dofs <= 0) { set_error("no free DOF (all constrained)"); return EMG_INVALID_INPUT; }
+  }
+  emg::keep_pool_memory();
+  auto* h = new emg_system_t();
+  emg::System& s = h->s;
+  cudaStream_t st = as_stream(stream);
+  s.n_nodes = n_nodes;
+  s.n_tets = n_tets;
+  s.n = n_dofs;
+  int rc = EMG_SUCCESS;
+  if (!rc) rc = upload(&s.xyz, xyz, 3 * n_nodes, on_device, st);
+  if (!rc) rc = upload(&s.tets, tets, 4 * n_tets, on_device, st);
+  if (!rc) rc = upload(&s.l2g, l2g, 6 * n_tets, on_device, st);
+  if (!rc) {
+    rc = upload(&s.material, material, n_tets, on_device, st);
+    if (!rc && !material) {
+      cudaError_t e = cudaMemsetAsync(s.material, 0, sizeof(int32_t) * n_tets, st);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
+    }
+  }
+  if (!rc) {
+    cudaError_t e = cudaMallocAsync(&s.err, sizeof(int32_t), st);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
+  }
+  if (!rc) rc = emg::system_build(s, st);
+  if (rc) { delete h; return rc; }
+  h->k_handle.csr = &s.K;
+  h->k_handle.owned = false;
+  h->m_handle.csr = &s.M;
+  h->m_handle.owned = false;
+  *out = h;
+  return EMG_SUCCESS;
+}
+
+int csr_from_device(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* col,
+                    const double* val, bool src_dev, cudaStream_t st, emg_csr* out) {
+  auto* h = new emg_csr_t();
+  h->csr = new emg::DevCsr();
+  emg::DevCsr& A = *h->csr;
+  A.n = n;
+  A.nnz = nnz;
+  emg::keep_pool_memory();
+  int rc = upload(&A.row_ptr, rp, n + 1, src_dev, st);
+  if (!rc) rc = upload(&A.col, col, nnz, src_dev, st);
+  if (!rc) rc = upload(&A.val, val, nnz, src_dev, st);
+  if (!rc && src_dev) rc = emg::check_csr(n, A.row_ptr, A.col, nnz, st);
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
+  }
+  if (rc) { delete h->csr; delete h; return rc; }
+  *out = h;
+  return EMG_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t emg_abi_version(void) { return EMG_ABI_VERSION; }
+
+const char* emg_last_error(void) { return emg::g_error.c_str(); }
+
+int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
+                    const int32_t* material_id, int64_t n_dirichlet,
+                    const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out) {
+  return guarded([&]() -> int {
+    if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    if (n_nodes <= 0 || n_tets <= 0 || !tets) { set_error("mesh is empty"); return EMG_INVALID_INPUT; }
+    if (n_dirichlet < 0 || (n_dirichlet > 0 && !dirichlet_pairs)) {
+      set_error("bad Dirichlet pair list");
+      return EMG_INVALID_INPUT;
+    }
+    for (int64_t i = 0; i < 4 * n_tets; ++i)
+      if (tets[i] < 0 || tets[i] >= n_nodes) {
+        set_error("element node index out of range");  // em_assembly.cpp:603-608
+        return EMG_INVALID_INPUT;
+      }
+    auto* h = new emg_mesh_t();
+    emg::Mesh& m = h->m;
+    m.n_nodes = n_nodes;
+    m.n_tets = n_tets;
+    if (xyz) m.xyz.assign(xyz, xyz + 3 * n_nodes);
+    m.tets.assign(tets, tets + 4 * n_tets);
+    if (material_id) m.material.assign(material_id, material_id + n_tets);
+    else m.material.assign(n_tets, 0);
+    if (n_dirichlet > 0) m.dirichlet.assign(dirichlet_pairs, dirichlet_pairs + 2 * n_dirichlet);
+    m.n_hole_markers = n_hole_markers > 0 ? n_hole_markers : 0;
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+void emg_mesh_destroy(emg_mesh mesh) { delete mesh; }
+
+int emg_edge_ids(emg_mesh mesh, int32_t* elem_edge, int32_t* edge_nodes, int64_t* n_edges) {
+  return guarded([&]() -> int {
+    if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
+    int rc = emg::build_edge_ids(mesh->m);
+    if (rc) return rc;
+    if (n_edges) *n_edges = mesh->m.n_edges;
+    if (elem_edge) std::memcpy(elem_edge, mesh->m.elem_edge.data(), sizeof(int32_t) * mesh->m.elem_edge.size());
+    if (edge_nodes) std::memcpy(edge_nodes, mesh->m.edge_nodes.data(), sizeof(int32_t) * mesh->m.edge_nodes.size());
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_dof_build(emg_mesh mesh, int32_t gauge_mode, emg_dofmap* out) {
+  return guarded([&]() -> int {
+    if (!mesh || !out) { set_error("null handle"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    auto* h = new emg_dofmap_t();
+    int rc = emg::build_dofmap(mesh->m, gauge_mode, h->d);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_dofmap_info(emg_dofmap map, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs) {
+  if (!map) { set_error("null dofmap"); return EMG_INVALID_INPUT; }
+  if (n_edges) *n_edges = map->d.n_edges;
+  if (n_free) *n_free = map->d.n_free;
+  if (n_dofs) *n_dofs = map->d.n_dofs;
+  return EMG_SUCCESS;
+}
+
+int emg_dofmap_export(emg_dofmap map, int32_t* l2g, int32_t* edge_dof) {
+  if (!map) { set_error("null dofmap"); return EMG_INVALID_INPUT; }
+  if (l2g) std::memcpy(l2g, map->d.l2g.data(), sizeof(int32_t) * map->d.l2g.size());
+  if (edge_dof) std::memcpy(edge_dof, map->d.edge_dof.data(), sizeof(int32_t) * map->d.edge_dof.size());
+  return EMG_SUCCESS;
+}
+
+int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full) {
+  if (!map || !reduced || !full) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  for (int64_t e = 0; e < map->d.n_edges; ++e) {
+    int32_t k = map->d.edge_dof[e];
+    full[e] = k >= 0 ? reduced[k] : 0.0;
+  }
+  return EMG_SUCCESS;
+}
+
+void emg_dofmap_destroy(emg_dofmap map) { delete map; }
+
+int emg_system_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
+                      const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
+                      emg_system* out) {
+  return guarded([&]() -> int {
+    return system_create_impl(n_nodes, xyz, n_tets, tets, material, l2g, n_dofs, stream, out, false);
+  });
+}
+
+int emg_system_create_device(int64_t n_nodes, const double* xyz_d, int64_t n_tets,
+                             const int32_t* tets_d, const int32_t* material_d,
+                             const int32_t* l2g_d, int64_t n_dofs, void* stream, emg_system* out) {
+  return guarded([&]() -> int {
+    return system_create_impl(n_nodes, xyz_d, n_tets, tets_d, material_d, l2g_d, n_dofs, stream, out, true);
+  });
+}
+
+int emg_system_assemble(emg_system sys, const double* nu, const double* sigma, int32_t n_materials,
+                        const emg_source* sources, int32_t n_sources, int32_t flags, void* stream) {
+  return guarded([&]() -> int {
+    if (!sys) { set_error("null system"); return EMG_INVALID_INPUT; }
+    return emg::system_assemble(sys->s, nu, sigma, n_materials, sources, n_sources, flags, as_stream(stream));
+  });
+}
+
+int emg_system_info(emg_system sys, int64_t* n_rows, int64_t* nnz) {
+  if (!sys) { set_error("null system"); return EMG_INVALID_INPUT; }
+  if (n_rows) *n_rows = sys->s.n;
+  if (nnz) *nnz = sys->s.K.nnz;
+  return EMG_SUCCESS;
+}
+
+int emg_system_export(emg_system sys, int32_t* row_ptr, int32_t* col, double* kval, double* mval,
+                      double* rhs) {
+  return guarded([&]() -> int {
+    if (!sys) { set_error("null system"); return EMG_INVALID_INPUT; }
+    const emg::System& s = sys->s;
+    if (row_ptr) EMG_CK(cudaMemcpy(row_ptr, s.K.row_ptr, sizeof(int32_t) * (s.n + 1), cudaMemcpyDeviceToHost));
+    if (col) EMG_CK(cudaMemcpy(col, s.K.col, sizeof(int32_t) * s.K.nnz, cudaMemcpyDeviceToHost));
+    if (kval) EMG_CK(cudaMemcpy(kval, s.K.val, sizeof(double) * s.K.nnz, cudaMemcpyDeviceToHost));
+    if (mval) {
+      if (!s.M.val) { set_error("mass matrix was not assembled"); return EMG_INVALID_INPUT; }
+      EMG_CK(cudaMemcpy(mval, s.M.val, sizeof(double) * s.K.nnz, cudaMemcpyDeviceToHost));
+    }
+    if (rhs) EMG_CK(cudaMemcpy(rhs, s.rhs, sizeof(double) * s.n, cudaMemcpyDeviceToHost));
+    return EMG_SUCCESS;
+  });
+}
+
+emg_csr emg_system_matrix(emg_system sys, int32_t which) {
+  if (!sys) return nullptr;
+  if (which == 1) return sys->s.M.val ? &sys->m_handle : nullptr;
+  return &sys->k_handle;
+}
+
+const double* emg_system_rhs_device(emg_system sys) { return sys ? sys->s.rhs : nullptr; }
+
+void emg_system_destroy(emg_system sys) {
+  if (!sys) return;
+  cudaDeviceSynchronize();
+  delete sys;
+}
+
+int emg_csr_create(int64_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                   void* stream, emg_csr* out) {
+  return guarded([&]() -> int {
+    if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    if (n <= 0 || !row_ptr || !col || !val) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
+    if (row_ptr[0] != 0) { set_error("row_ptr[0] != 0"); return EMG_INVALID_INPUT; }
+    for (int64_t i = 0; i < n; ++i)
+      if (row_ptr[i + 1] < row_ptr[i]) { set_error("row_ptr not monotone"); return EMG_INVALID_INPUT; }
+    // Merge duplicates and sort columns per row, as SparseConverter::to_eigen
+    // (setFromTriplets) does before the reference solvers see the matrix.
+    std::vector<int32_t> rp(n + 1, 0), cc;
+    std::vector<double> vv;
+    cc.reserve(row_ptr[n]);
+    vv.reserve(row_ptr[n]);
+    std::vector<std::pair<int32_t, double>> row;
+    for (int64_t i = 0; i < n; ++i) {
+      row.clear();
+      for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+        if (col[k] < 0 || col[k] >= n) { set_error("column index out of range"); return EMG_INVALID_INPUT; }
+        row.emplace_back(col[k], val[k]);
+      }
+      std::stable_sort(row.begin(), row.end(),
+                       [](const auto& a, const auto& b) { return a.first < b.first; });
+      for (size_t k = 0; k < row.size(); ++k) {
+        if (k > 0 && row[k].first == row[k - 1].first) vv.back() += row[k].second;
+        else { cc.push_back(row[k].first); vv.push_back(row[k].second); }
+      }
+      rp[i + 1] = static_cast<int32_t>(cc.size());
+    }
+    return csr_from_device(n, static_cast<int64_t>(cc.size()), rp.data(), cc.data(), vv.data(), false,
+                           as_stream(stream), out);
+  });
+}
+
+int emg_csr_create_device(int64_t n, int64_t nnz, const int32_t* row_ptr_d, const int32_t* col_d,
+                          const double* val_d, void* stream, emg_csr* out) {
+  return guarded([&]() -> int {
+    if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    if (n <= 0 || nnz < 0 || !row_ptr_d || !col_d || !val_d) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
+    return csr_from_device(n, nnz, row_ptr_d, col_d, val_d, true, as_stream(stream), out);
+  });
+}
+
+int emg_csr_info(emg_csr A, int64_t* n, int64_t* nnz) {
+  if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
+  if (n) *n = A->csr->n;
+  if (nnz) *nnz = A->csr->nnz;
+  return EMG_SUCCESS;
+}
+
+void emg_csr_destroy(emg_csr A) {
+  if (!A || !A->owned) return;  // borrowed handles belong to their system
+  cudaDeviceSynchronize();
+  delete A->csr;
+  delete A;
+}
+
+int emg_spmv(emg_csr A, const double* x_d, double* y_d, void* stream) {
+  return guarded([&]() -> int {
+    if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
+    return emg::csr_spmv(*A->csr, x_d, y_d, as_stream(stream));
+  });
+}
+
+namespace {
+int solve_host(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg, emg_result* out,
+               bool bicg) {
+  return guarded([&]() -> int {
+    emg_result dummy;
+    if (!out) out = &dummy;
+    std::memset(out, 0, sizeof(*out));
+    out->status = EMG_INVALID_INPUT;
+    if (!A || !A->csr || !cfg || !b || !x) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    const int64_t n = A->csr->n;
+    double *bd = nullptr, *xd = nullptr;
+    EMG_CK(cudaMalloc(&bd, sizeof(double) * n));
+    EMG_CK(cudaMalloc(&xd, sizeof(double) * n));
+    EMG_CK(cudaMemcpy(bd, b, sizeof(double) * n, cudaMemcpyHostToDevice));
+    int rc = bicg ? emg::bicgstab_solve(*A->csr, bd, xd, *cfg, nullptr, out)
+                  : emg::cg_solve(*A->csr, bd, xd, *cfg, nullptr, out);
+    if (rc == EMG_SUCCESS || rc == EMG_NUMERICAL_ERROR || rc == EMG_DIVERGED || rc == EMG_MAX_ITER_REACHED)
+      EMG_CK(cudaMemcpy(x, xd, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    cudaFree(bd);
+    cudaFree(xd);
+    return rc;
+  });
+}
+int solve_device(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg, void* stream,
+                 emg_result* out, bool bicg) {
+  return guarded([&]() -> int {
+    emg_result dummy;
+    if (!out) out = &dummy;
+    std::memset(out, 0, sizeof(*out));
+    out->status = EMG_INVALID_INPUT;
+    if (!A || !A->csr || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    return bicg ? emg::bicgstab_solve(*A->csr, b, x, *cfg, as_stream(stream), out)
+                : emg::cg_solve(*A->csr, b, x, *cfg, as_stream(stream), out);
+  });
+}
+}  // namespace
+
+int emg_cg_solve(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg, emg_result* out) {
+  return solve_host(A, b, x, cfg, out, false);
+}
+int emg_cg_solve_device(emg_csr A, const double* b_d, double* x_d, const emg_krylov_config* cfg,
+                        void* stream, emg_result* out) {
+  return solve_device(A, b_d, x_d, cfg, stream, out, false);
+}
+int emg_bicgstab_solve(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg,
+                       emg_result* out) {
+  return solve_host(A, b, x, cfg, out, true);
+}
+int emg_bicgstab_solve_device(emg_csr A, const double* b_d, double* x_d, const emg_krylov_config* cfg,
+                              void* stream, emg_result* out) {
+  return solve_device(A, b_d, x_d, cfg, stream, out, true);
+}
+
+int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg, double* x,
+                     int32_t x_on_device, void* stream, emg_result* out) {
+  return guarded([&]() -> int {
+    emg_result dummy;
+    if (!out) out = &dummy;
+    std::memset(out, 0, sizeof(*out));
+    out->status = EMG_INVALID_INPUT;
+    if (!sys || !cfg || !x) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    emg::System& s = sys->s;
+    cudaStream_t st = as_stream(stream);
+    double* xd = x;
+    if (!x_on_device) EMG_CK(cudaMallocAsync(&xd, sizeof(double) * s.n, st));
+    int rc = kind == 1 ? emg::bicgstab_solve(s.K, s.rhs, xd, *cfg, st, out)
+                       : emg::cg_solve(s.K, s.rhs, xd, *cfg, st, out);
+    if (!x_on_device) {
+      if (rc <= EMG_MAX_ITER_REACHED)
+        EMG_CK(cudaMemcpyAsync(x, xd, sizeof(double) * s.n, cudaMemcpyDeviceToHost, st));
+      EMG_CK(cudaFreeAsync(xd, st));
+      EMG_CK(cudaStreamSynchronize(st));
+    }
+    return rc;
+  });
+}
+
+int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms) {
+  return guarded([&]() -> int {
+    if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
+    return emg::cg_kernel_times(*A->csr, iterations, as_stream(stream), ms);
+  });
+}
+
+int emg_last_history(emg_csr A, double* residuals, int32_t cap) {
+  if (!A || !A->csr || !residuals || cap <= 0) return 0;
+  int n = emg::csr_history(*A->csr, residuals, cap);
+  return n < 0 ? 0 : n;
+}
+
+}  // extern "C"

@@ -1,0 +1,602 @@
+// assembly.cu -- EMAssembly::assemble on the GPU for TET4_EDGE elements
+// (reference: src/numeric/em_assembly.cpp:144-420 with the intended
+// MagneticVector3DIntegrator formulas, magnetic_vector_3d_integrator.cpp:139-364).
+//
+// Symbolic phase (once per mesh + DOF map):
+//   k_count_rows / scan / k_fill_incidence / k_sort_incidence build, for every
+//   equation row r, the sorted list of (tet, local edge) slots that map to r;
+//   k_row_pattern (count, scan, write) turns those lists into the merged CSR
+//   pattern with ascending columns -- the pattern SparseConverter::to_eigen
+//   produces from the reference's unmerged CSR (sparse_converter.cpp:19-80).
+// Numeric phase:
+//   k_assemble_rows gathers, for each row, the contributions of its incident
+//   tets in ascending tet order and writes the row's values once: no atomics,
+//   deterministic, and every sum is formed in the same order as an element
+//   loop would form it.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "common.cuh"
+#include "device.h"
+
+namespace emg {
+
+namespace {
+
+constexpr int kMaxSources = 16;
+constexpr int kPatternCap = 256;  // candidate columns per row (warp-shared)
+
+__constant__ emg_source c_src[kMaxSources];
+
+enum : int32_t {
+  kErrIndex = 1,     // l2g entry >= n
+  kErrRowCap = 2,    // more candidate columns than kPatternCap
+  kErrSlot = 4,      // column missing from the pattern (internal)
+  kErrNode = 8,      // node index out of range
+};
+
+// ---------------------------------------------------------------- scan ----
+constexpr int kScanTile = 2048;  // elements per block (256 threads x 8)
+
+__global__ void k_scan_tile_sums(const int32_t* __restrict__ in, int64_t n,
+                                 int64_t* __restrict__ tile_sums) {
+  __shared__ double red[8];
+  int64_t base = static_cast<int64_t>(blockIdx.x) * kScanTile;
+  int64_t s = 0;
+  for (int i = threadIdx.x; i < kScanTile; i += blockDim.x) {
+    int64_t g = base + i;
+    if (g < n) s += in[g];
+  }
+  double t = block_sum(static_cast<double>(s), red);  // exact below 2^53
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = static_cast<int64_t>(t);
+}
+
+__global__ void k_scan_tiles(int64_t* __restrict__ tile_sums, int64_t n_tiles,
+                             int64_t* __restrict__ total) {
+  // single block, sequential chunks of blockDim.x
+  __shared__ int64_t buf[1024];
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < n_tiles; base += blockDim.x) {
+    int64_t g = base + threadIdx.x;
+    int64_t v = g < n_tiles ? tile_sums[g] : 0;
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {  // Hillis-Steele inclusive
+      int64_t a = threadIdx.x >= o ? buf[threadIdx.x - o] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += a;
+      __syncthreads();
+    }
+    if (g < n_tiles) tile_sums[g] = carry + buf[threadIdx.x] - v;  // exclusive
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n,
+                             const int64_t* __restrict__ tile_off, int32_t* __restrict__ out) {
+  // 256 threads x 8 consecutive elements
+  __shared__ int64_t part[256];
+  int64_t base = static_cast<int64_t>(blockIdx.x) * kScanTile + threadIdx.x * 8;
+  int64_t loc[8];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int64_t g = base + i;
+    loc[i] = s;
+    s += g < n ? in[g] : 0;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 256; o <<= 1) {
+    int64_t a = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += a;
+    __syncthreads();
+  }
+  int64_t off = tile_off[blockIdx.x] + part[threadIdx.x] - s;
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = static_cast<int32_t>(tile_off[gridDim.x]);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int64_t g = base + i;
+    if (g < n) out[g] = static_cast<int32_t>(off + loc[i]);
+  }
+}
+
+// ----------------------------------------------------------- incidence ----
+__global__ void k_count_rows(const int32_t* __restrict__ l2g, int64_t m, int64_t n,
+                             int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+  for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < m;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int32_t r = l2g[p];
+    if (r >= n || r < -1) { atomicOr(err, kErrIndex); continue; }
+    if (r >= 0) atomicAdd(&cnt[r], 1);
+  }
+}
+
+__global__ void k_fill_incidence(const int32_t* __restrict__ l2g, int64_t m,
+                                 const int32_t* __restrict__ inc_ptr, int32_t* __restrict__ cursor,
+                                 int32_t* __restrict__ inc) {
+  for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < m;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int32_t r = l2g[p];
+    if (r < 0) continue;
+    int32_t s = inc_ptr[r] + atomicAdd(&cursor[r], 1);
+    inc[s] = static_cast<int32_t>(p);
+  }
+}
+
+__global__ void k_sort_incidence(const int32_t* __restrict__ inc_ptr, int32_t* __restrict__ inc,
+                                 int64_t n) {
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int32_t a = inc_ptr[r], b = inc_ptr[r + 1];
+    for (int32_t i = a + 1; i < b; ++i) {
+      int32_t v = inc[i];
+      int32_t j = i - 1;
+      while (j >= a && inc[j] > v) { inc[j + 1] = inc[j]; --j; }
+      inc[j + 1] = v;
+    }
+  }
+}
+
+// Warp per row: candidate columns of all incident tets -> distinct, ranked.
+// write == false: counts[r] = number of distinct columns.
+// write == true : col[row_ptr[r] + rank] = column.
+template <bool kWrite>
+__global__ void __launch_bounds__(128) k_row_pattern(int64_t n, const int32_t* __restrict__ inc_ptr,
+                                                     const int32_t* __restrict__ inc,
+                                                     const int32_t* __restrict__ l2g,
+                                                     int32_t* __restrict__ counts,
+                                                     const int32_t* __restrict__ row_ptr,
+                                                     int32_t* __restrict__ col,
+                                                     int32_t* __restrict__ err) {
+  __shared__ int32_t cand_all[4][kPatternCap];
+  __shared__ uint8_t first_all[4][kPatternCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int32_t* cand = cand_all[wib];
+  uint8_t* first = first_all[wib];
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + wib; r < n; r += warps) {
+    const int32_t a = inc_ptr[r], b = inc_ptr[r + 1];
+    const int m = 6 * (b - a);
+    if (m > kPatternCap) {
+      if (lane == 0) {
+        atomicOr(err, kErrRowCap);
+        if (!kWrite) counts[r] = 0;
+      }
+      continue;
+    }
+    for (int idx = lane; idx < m; idx += 32) {
+      const int32_t slot = inc[a + idx / 6];
+      cand[idx] = l2g[6 * (slot / 6) + (idx % 6)];
+    }
+    __syncwarp();
+    for (int idx = lane; idx < m; idx += 32) {  // first occurrence of each valid column
+      const int32_t c = cand[idx];
+      bool f = c >= 0;
+      for (int j = 0; j < idx && f; ++j) f = cand[j] != c;
+      first[idx] = f ? 1 : 0;
+    }
+    __syncwarp();
+    int kept = 0;
+    for (int base = 0; base < m; base += 32) {
+      const int idx = base + lane;
+      const bool keep = idx < m && first[idx];
+      kept += __popc(__ballot_sync(0xffffffffu, keep));
+      if (kWrite && keep) {
+        const int32_t c = cand[idx];
+        int rank = 0;  // distinct columns smaller than c
+        for (int j = 0; j < m; ++j) rank += (first[j] && cand[j] < c) ? 1 : 0;
+        col[row_ptr[r] + rank] = c;
+      }
+    }
+    if (!kWrite && lane == 0) counts[r] = kept;
+    __syncwarp();
+  }
+}
+
+// --------------------------------------------------------------- numeric ----
+// Nedelec TET4_EDGE edge table (nedelec_element.cpp:54-60): basis k is
+// lambda_b grad(lambda_a) - lambda_a grad(lambda_b) for (a, b) = kNed[k].
+__constant__ int kNedA[6] = {0, 1, 2, 0, 1, 2};
+__constant__ int kNedB[6] = {1, 2, 0, 3, 3, 3};
+
+struct Tet {
+  double d[3][3];  // d[c] = x_c - x_3 (Jacobian columns)
+  double det;
+  double g[4][3];  // physical gradients of the barycentric coordinates
+  double c[6][3];  // physical curls (J curl_ref / det)
+  double x3[3];
+  int32_t node[4];
+};
+
+__device__ __forceinline__ void cross(const double* a, const double* b, double* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ bool load_tet(const int32_t* __restrict__ tets,
+                                         const double* __restrict__ xyz, int64_t n_nodes,
+                                         int64_t t, Tet& T) {
+  int4 nd = reinterpret_cast<const int4*>(tets)[t];
+  T.node[0] = nd.x; T.node[1] = nd.y; T.node[2] = nd.z; T.node[3] = nd.w;
+  double x[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    int32_t g = T.node[a];
+    if (g < 0 || g >= n_nodes) return false;
+    x[a][0] = xyz[3 * g]; x[a][1] = xyz[3 * g + 1]; x[a][2] = xyz[3 * g + 2];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) T.d[c][r] = x[c][r] - x[3][r];
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) T.x3[r] = x[3][r];
+  double c12[3], c20[3], c01[3];
+  cross(T.d[1], T.d[2], c12);
+  cross(T.d[2], T.d[0], c20);
+  cross(T.d[0], T.d[1], c01);
+  T.det = T.d[0][0] * c12[0] + T.d[0][1] * c12[1] + T.d[0][2] * c12[2];
+  const double inv = 1.0 / T.det;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    T.g[0][r] = c12[r] * inv;  // rows of J^-1 = physical gradients
+    T.g[1][r] = c20[r] * inv;
+    T.g[2][r] = c01[r] * inv;
+    T.g[3][r] = -(T.g[0][r] + T.g[1][r] + T.g[2][r]);
+  }
+  // J * curl_ref / det with curl_ref from curlTet4Edge (nedelec_element.cpp:461-505)
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const double a0 = T.d[0][r] * inv, a1 = T.d[1][r] * inv, a2 = T.d[2][r] * inv;
+    T.c[0][r] = -2.0 * a2;
+    T.c[1][r] = -2.0 * a0;
+    T.c[2][r] = -2.0 * a1;
+    T.c[3][r] = -2.0 * a1 + 2.0 * a2;
+    T.c[4][r] = 2.0 * a0 - 2.0 * a2;
+    T.c[5][r] = -2.0 * a0 + 2.0 * a1;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void source_at(const double* x, int n_src, double* js) {
+  js[0] = js[1] = js[2] = 0.0;
+  for (int s = 0; s < n_src; ++s) {
+    const double* p = c_src[s].p;
+    bool in = false;
+    if (c_src[s].kind == EMG_SRC_BOX) {
+      in = x[0] > p[0] && x[0] < p[1] && x[1] > p[2] && x[1] < p[3] && x[2] > p[4] && x[2] < p[5];
+    } else if (c_src[s].kind == EMG_SRC_ANNULUS_Z) {
+      const double dx = x[0] - p[0], dy = x[1] - p[1];
+      const double rr = sqrt(dx * dx + dy * dy);
+      in = rr > p[2] && rr < p[3] && x[2] > p[4] && x[2] < p[5];
+    }
+    if (in) { js[0] += c_src[s].j[0]; js[1] += c_src[s].j[1]; js[2] += c_src[s].j[2]; }
+  }
+}
+
+__device__ __forceinline__ int find_slot(const int32_t* __restrict__ col, int32_t lo, int32_t hi,
+                                         int32_t c) {
+  while (lo < hi) {
+    int32_t mid = (lo + hi) >> 1;
+    if (col[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+struct AsmArgs {
+  int64_t n, n_nodes;
+  const int32_t* row_ptr;
+  const int32_t* col;
+  const int32_t* inc_ptr;
+  const int32_t* inc;
+  const int32_t* tets;
+  const double* xyz;
+  const int32_t* material;
+  const int32_t* l2g;
+  const double* nu;
+  const double* sigma;
+  int32_t n_mat, n_src, flags;
+  double* kval;
+  double* mval;
+  double* rhs;
+  int32_t* err;
+};
+
+// Thread per row: K(r, c) = sum over incident tets of
+//   nu |det| wsum s_i s_j curl_i . curl_j
+// where curl_k = J curl_ref_k / det is constant per tet, so the quadrature
+// sum collapses to the weight sum (1/6 for the Hammer rule, 1/8 for the
+// reference's 3-point rule).  M and F are integrated at the quadrature points.
+__global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
+  const double qa = 0.13819660112501051517954131656343619;   // (5 - sqrt 5) / 20
+  const double qb = 0.58541019662496845446137605030969143;   // (5 + 3 sqrt 5) / 20
+  const bool quad3 = (A.flags & EMG_FLAG_QUAD3_LITERAL) != 0;
+  const int nq = quad3 ? 3 : 4;
+  const double w = 1.0 / 24.0;
+  const bool want_mass = (A.flags & EMG_FLAG_MASS) != 0 && A.mval != nullptr;
+  const bool signs = (A.flags & EMG_FLAG_NO_EDGE_SIGNS) == 0;
+  const bool literal = (A.flags & EMG_FLAG_PIOLA_LITERAL) != 0;
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < A.n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s0 = A.row_ptr[r], s1 = A.row_ptr[r + 1];
+    for (int32_t k = s0; k < s1; ++k) {
+      A.kval[k] = 0.0;
+      if (want_mass) A.mval[k] = 0.0;
+    }
+    double f = 0.0;
+    for (int32_t q = A.inc_ptr[r]; q < A.inc_ptr[r + 1]; ++q) {
+      const int32_t slot = A.inc[q];
+      const int64_t t = slot / 6;
+      const int i = slot - 6 * static_cast<int>(t);
+      const int32_t mid = A.material ? A.material[t] : 0;
+      if (mid < 0 || mid >= A.n_mat) continue;  // em_assembly.cpp:270-276 skips the element
+      Tet T;
+      if (!load_tet(A.tets, A.xyz, A.n_nodes, t, T)) { atomicOr(A.err, kErrNode); continue; }
+      const double adet = fabs(T.det);
+      if (adet < 1e-15) continue;  // every quadrature point skipped (:169)
+      int sg[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        sg[k] = signs ? (T.node[kNedB[k]] < T.node[kNedA[k]] ? 1 : -1) : 1;
+      const double kf = nq * w * adet * A.nu[mid];
+      const double sig = A.sigma ? A.sigma[mid] : 0.0;
+      const bool do_mass = want_mass && sig > 0.0;
+      const bool do_src = A.n_src > 0;
+      int32_t cj[6];
+      int32_t pos[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        cj[j] = A.l2g[6 * t + j];
+        pos[j] = cj[j] >= 0 ? find_slot(A.col, s0, s1, cj[j]) : -1;
+        if (cj[j] >= 0 && (pos[j] >= s1 || A.col[pos[j]] != cj[j])) {
+          atomicOr(A.err, kErrSlot);
+          pos[j] = -1;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        if (pos[j] < 0) continue;
+        const double d = T.c[i][0] * T.c[j][0] + T.c[i][1] * T.c[j][1] + T.c[i][2] * T.c[j][2];
+        A.kval[pos[j]] += static_cast<double>(sg[i] * sg[j]) * (kf * d);
+      }
+      if (do_mass || do_src) {
+        double mrow[6] = {0, 0, 0, 0, 0, 0};
+        double fi = 0.0;
+        for (int qq = 0; qq < nq; ++qq) {
+          double lam[4];
+          if (qq == 0) { lam[0] = qa; lam[1] = qa; lam[2] = qb; }
+          else if (qq == 1) { lam[0] = qa; lam[1] = qb; lam[2] = qa; }
+          else if (qq == 2 && !quad3) { lam[0] = qb; lam[1] = qa; lam[2] = qa; }
+          else { lam[0] = qa; lam[1] = qa; lam[2] = qa; }
+          lam[3] = 1.0 - lam[0] - lam[1] - lam[2];
+          double W[6][3];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const int a = kNedA[k], b = kNedB[k];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              W[k][c] = lam[b] * T.g[a][c] - lam[a] * T.g[b][c];
+              if (literal) W[k][c] /= T.det;
+            }
+          }
+          if (do_mass) {
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+              mrow[j] += w * adet * sig * (W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2]);
+          }
+          if (do_src) {
+            double x[3], js[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              x[c] = T.x3[c] + lam[0] * T.d[0][c] + lam[1] * T.d[1][c] + lam[2] * T.d[2][c];
+            source_at(x, A.n_src, js);
+            fi += w * adet * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
+          }
+        }
+        if (do_mass) {
+#pragma unroll
+          for (int j = 0; j < 6; ++j)
+            if (pos[j] >= 0) A.mval[pos[j]] += static_cast<double>(sg[i] * sg[j]) * mrow[j];
+        }
+        f += sg[i] * fi;
+      }
+    }
+    A.rhs[r] = f;
+  }
+}
+
+int grid_for(int64_t work, int threads, int max_blocks = 148 * 16) {
+  int64_t b = (work + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return static_cast<int>(b);
+}
+
+std::string err_text(int32_t e) {
+  std::string s;
+  if (e & kErrIndex) s += " l2g index outside [-1, n_dofs);";
+  if (e & kErrRowCap) s += " a row has more than 256 candidate columns;";
+  if (e & kErrSlot) s += " pattern lookup failed;";
+  if (e & kErrNode) s += " node index outside [0, n_nodes);";
+  return s;
+}
+
+}  // namespace
+
+int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, cudaStream_t st) {
+  int64_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles < 1) tiles = 1;
+  int64_t* tile = nullptr;
+  EMG_CK(cudaMallocAsync(&tile, sizeof(int64_t) * (tiles + 1), st));
+  k_scan_tile_sums<<<static_cast<unsigned>(tiles), 256, 0, st>>>(counts, n, tile);
+  k_scan_tiles<<<1, 1024, 0, st>>>(tile, tiles, tile + tiles);
+  k_scan_apply<<<static_cast<unsigned>(tiles), 256, 0, st>>>(counts, n, tile, out);
+  int64_t tot = 0;
+  EMG_CK(cudaMemcpyAsync(&tot, tile + tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  EMG_CK(cudaFreeAsync(tile, st));
+  EMG_CK(cudaGetLastError());
+  *total = tot;
+  return EMG_SUCCESS;
+}
+
+int system_build(System& s, cudaStream_t st) {
+  const int64_t m = 6 * s.n_tets, n = s.n;
+  int32_t* cnt = nullptr;
+  EMG_CK(cudaMallocAsync(&cnt, sizeof(int32_t) * (n + 1), st));
+  EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
+  EMG_CK(cudaMemsetAsync(s.err, 0, sizeof(int32_t), st));
+  k_count_rows<<<grid_for(m, 256), 256, 0, st>>>(s.l2g, m, n, cnt, s.err);
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaMallocAsync(&s.inc_ptr, sizeof(int32_t) * (n + 1), st));
+  int64_t inc_total = 0;
+  int rc = scan_counts(cnt, s.inc_ptr, n, &inc_total, st);
+  if (rc) return rc;
+  int32_t herr = 0;
+  EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  if (herr) { set_error("system build:" + err_text(herr)); return EMG_INVALID_INPUT; }
+  EMG_CK(cudaMallocAsync(&s.inc, sizeof(int32_t) * (inc_total > 0 ? inc_total : 1), st));
+  EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
+  k_fill_incidence<<<grid_for(m, 256), 256, 0, st>>>(s.l2g, m, s.inc_ptr, cnt, s.inc);
+  k_sort_incidence<<<grid_for(n, 128), 128, 0, st>>>(s.inc_ptr, s.inc, n);
+  k_row_pattern<false><<<grid_for(n * 32, 128), 128, 0, st>>>(n, s.inc_ptr, s.inc, s.l2g, cnt,
+                                                             nullptr, nullptr, s.err);
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaMallocAsync(&s.K.row_ptr, sizeof(int32_t) * (n + 1), st));
+  int64_t nnz = 0;
+  rc = scan_counts(cnt, s.K.row_ptr, n, &nnz, st);
+  if (rc) return rc;
+  EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  if (herr) { set_error("system build:" + err_text(herr)); return EMG_INVALID_INPUT; }
+  if (nnz >= (int64_t(1) << 31)) { set_error("nnz exceeds int32 range"); return EMG_INVALID_INPUT; }
+  s.K.n = n;
+  s.K.nnz = nnz;
+  EMG_CK(cudaMallocAsync(&s.K.col, sizeof(int32_t) * (nnz > 0 ? nnz : 1), st));
+  EMG_CK(cudaMallocAsync(&s.K.val, sizeof(double) * (nnz > 0 ? nnz : 1), st));
+  k_row_pattern<true><<<grid_for(n * 32, 128), 128, 0, st>>>(n, s.inc_ptr, s.inc, s.l2g, nullptr,
+                                                            s.K.row_ptr, s.K.col, s.err);
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaMallocAsync(&s.rhs, sizeof(double) * (n > 0 ? n : 1), st));
+  EMG_CK(cudaMemsetAsync(s.rhs, 0, sizeof(double) * (n > 0 ? n : 1), st));
+  EMG_CK(cudaMemsetAsync(s.K.val, 0, sizeof(double) * (nnz > 0 ? nnz : 1), st));
+  EMG_CK(cudaFreeAsync(cnt, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  // M shares the pattern of K
+  s.M.n = n;
+  s.M.nnz = nnz;
+  s.M.row_ptr = s.K.row_ptr;
+  s.M.col = s.K.col;
+  s.M.owns_pattern = false;
+  return EMG_SUCCESS;
+}
+
+int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_mat,
+                    const emg_source* src, int32_t n_src, int32_t flags, cudaStream_t st) {
+  if (n_mat <= 0 || !nu) { set_error("materials list is empty"); return EMG_INVALID_INPUT; }
+  if (n_src < 0 || n_src > kMaxSources || (n_src > 0 && !src)) {
+    set_error("between 0 and 16 source regions are supported");
+    return EMG_INVALID_INPUT;
+  }
+  for (int32_t k = 0; k < n_mat; ++k)
+    if (!(nu[k] > 0.0) || (sigma && sigma[k] < 0.0)) {
+      // MaterialProperties rejects mu <= 0 and sigma < 0
+      set_error("material " + std::to_string(k) + ": nu must be > 0 and sigma >= 0");
+      return EMG_INVALID_INPUT;
+    }
+  const bool mass = (flags & EMG_FLAG_MASS) != 0;
+  if (mass && !s.M.val) EMG_CK(cudaMallocAsync(&s.M.val, sizeof(double) * (s.K.nnz > 0 ? s.K.nnz : 1), st));
+  s.has_mass = s.has_mass || mass;
+  double* mat = nullptr;
+  EMG_CK(cudaMallocAsync(&mat, sizeof(double) * 2 * n_mat, st));
+  std::vector<double> h(2 * n_mat, 0.0);
+  for (int32_t k = 0; k < n_mat; ++k) { h[k] = nu[k]; h[n_mat + k] = sigma ? sigma[k] : 0.0; }
+  EMG_CK(cudaMemcpyAsync(mat, h.data(), sizeof(double) * 2 * n_mat, cudaMemcpyHostToDevice, st));
+  if (n_src > 0)
+    EMG_CK(cudaMemcpyToSymbolAsync(c_src, src, sizeof(emg_source) * n_src, 0,
+                                   cudaMemcpyHostToDevice, st));
+  EMG_CK(cudaMemsetAsync(s.err, 0, sizeof(int32_t), st));
+  AsmArgs a;
+  a.n = s.n; a.n_nodes = s.n_nodes;
+  a.row_ptr = s.K.row_ptr; a.col = s.K.col; a.inc_ptr = s.inc_ptr; a.inc = s.inc;
+  a.tets = s.tets; a.xyz = s.xyz; a.material = s.material; a.l2g = s.l2g;
+  a.nu = mat; a.sigma = mat + n_mat; a.n_mat = n_mat; a.n_src = n_src; a.flags = flags;
+  a.kval = s.K.val; a.mval = mass ? s.M.val : nullptr; a.rhs = s.rhs; a.err = s.err;
+  k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
+  EMG_CK(cudaGetLastError());
+  int32_t herr = 0;
+  EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaFreeAsync(mat, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  if (herr) { set_error("assembly:" + err_text(herr)); return EMG_INVALID_INPUT; }
+  return EMG_SUCCESS;
+}
+
+// Buffers of a System come from the stream-ordered pool (cudaMallocAsync);
+// the owner synchronizes the device before destruction.
+System::~System() {
+  for (void* p : {static_cast<void*>(xyz), static_cast<void*>(tets), static_cast<void*>(material),
+                  static_cast<void*>(l2g), static_cast<void*>(inc_ptr), static_cast<void*>(inc),
+                  static_cast<void*>(err), static_cast<void*>(rhs)})
+    if (p) cudaFreeAsync(p, 0);
+}
+
+namespace {
+__global__ void k_check_csr(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                            int64_t nnz, int32_t* __restrict__ bad) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t a = rp[i], b = rp[i + 1];
+    if (a < 0 || b < a || b > nnz || (i == 0 && a != 0) || (i == n - 1 && b != nnz)) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    for (int32_t k = a; k < b; ++k) {
+      const int32_t c = col[k];
+      if (c < 0 || c >= n || (k > a && col[k - 1] >= c)) { atomicOr(bad, 2); break; }
+    }
+  }
+}
+}  // namespace
+
+int check_csr(int64_t n, const int32_t* rp, const int32_t* col, int64_t nnz, cudaStream_t st) {
+  int32_t* bad = nullptr;
+  EMG_CK(cudaMallocAsync(&bad, sizeof(int32_t), st));
+  EMG_CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
+  k_check_csr<<<grid_for(n, 256), 256, 0, st>>>(n, rp, col, nnz, bad);
+  int32_t h = 0;
+  EMG_CK(cudaMemcpyAsync(&h, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  EMG_CK(cudaFreeAsync(bad, st));
+  if (h & 1) { set_error("row_ptr is not a valid offset array"); return EMG_INVALID_INPUT; }
+  if (h & 2) { set_error("columns out of range or not strictly ascending in a row"); return EMG_INVALID_INPUT; }
+  return EMG_SUCCESS;
+}
+
+void keep_pool_memory() {
+  // Keep freed stream-ordered memory in the pool instead of returning it to
+  // the driver at every synchronization (per-process setting).
+  static int done_for = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev == done_for) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done_for = dev;
+}
+
+}  // namespace emg

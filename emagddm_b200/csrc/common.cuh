@@ -1,0 +1,55 @@
+// common.cuh -- device helpers shared by the assembly and Krylov kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace emg {
+
+constexpr int kWarp = 32;
+
+// Deterministic warp sum (fixed butterfly).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum of one value per thread; result valid in every
+// thread.  `scratch` holds blockDim.x / 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) scratch[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < nw; ++w) t += scratch[w];
+  return t;
+}
+
+// Streaming loads for matrix entries: read once per SpMV, so they carry an
+// L2 evict-first policy and skip L1, leaving L2 to the vectors (x, p, r, ...)
+// that are re-read every iteration.
+__device__ __forceinline__ uint64_t evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
+               : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int ld_stream(const int* p, uint64_t pol) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+               : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+// Coherent-at-L2 load for values written by other blocks of the same kernel.
+__device__ __forceinline__ double ld_l2(const double* p) { return __ldcg(p); }
+
+}  // namespace emg

@@ -1,0 +1,78 @@
+// device.h -- host-side interface of the CUDA parts of libemagddm_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "emagddm_b200.h"
+
+namespace emg {
+
+void set_error(const std::string& msg);
+
+#define EMG_CK(call)                                                              \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      ::emg::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));       \
+      return EMG_ERR_CUDA;                                                        \
+    }                                                                             \
+  } while (0)
+
+struct KrylovWorkspace;
+
+// Device CSR matrix (int32 row_ptr / col, fp64 values, rows sorted, merged).
+struct DevCsr {
+  int64_t n = 0;
+  int64_t nnz = 0;
+  int32_t* row_ptr = nullptr;
+  int32_t* col = nullptr;
+  double* val = nullptr;
+  bool owns_pattern = true;
+  bool owns_values = true;
+  KrylovWorkspace* ws = nullptr;
+  ~DevCsr();
+};
+
+// Assembled system on the device (EMAssembly state).
+struct System {
+  int64_t n_nodes = 0, n_tets = 0, n = 0;
+  double* xyz = nullptr;       // 3 * n_nodes
+  int32_t* tets = nullptr;     // 4 * n_tets
+  int32_t* material = nullptr; // n_tets
+  int32_t* l2g = nullptr;      // 6 * n_tets
+  int32_t* inc_ptr = nullptr;  // n + 1: incidence of every row (tet-edge slots)
+  int32_t* inc = nullptr;      // sorted slots 6 * t + k per row
+  int32_t* err = nullptr;      // device error word
+  double* rhs = nullptr;       // n
+  DevCsr K, M;                 // M shares K's pattern
+  bool has_mass = false;
+  ~System();
+};
+
+// Symbolic phase: incidence lists and the merged CSR pattern, all on the device.
+int system_build(System& s, cudaStream_t st);
+// Numeric phase: K (and M), F.
+int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_mat,
+                    const emg_source* src, int32_t n_src, int32_t flags, cudaStream_t st);
+
+// Exclusive scan of n int32 counts into out[0..n]; returns the total.
+int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, cudaStream_t st);
+
+// Validates a device CSR (offsets, column range, ascending columns).
+int check_csr(int64_t n, const int32_t* rp, const int32_t* col, int64_t nnz, cudaStream_t st);
+// Keeps the default memory pool's freed blocks cached (once per device).
+void keep_pool_memory();
+
+int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st);
+int cg_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
+             cudaStream_t st, emg_result* res);
+int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
+                   cudaStream_t st, emg_result* res);
+int csr_history(DevCsr& A, double* out, int32_t cap);
+int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
+void free_workspace(KrylovWorkspace* ws);
+
+}  // namespace emg

@@ -1,0 +1,698 @@
+// krylov.cu -- FP64 CSR SpMV and the Jacobi-preconditioned CG / BiCGSTAB
+// solvers of the reference (src/numeric/iterative_solvers.cpp:343-503 and
+// :869-1118), with the same iteration, stopping and failure rules.
+//
+// Structure of one iteration (CG):
+//   k_cg_spmv_dot   q = A p and p.q        (last block: alpha / breakdown)
+//   k_cg_update     x += a p, r -= a q, z = D^-1 r, r.z and r.r
+//                   (last block: residual, convergence, divergence, beta)
+//   k_cg_direction  p = z + b p
+// Reductions are deterministic: a fixed grid, one partial per block, and the
+// last block to finish (atomic ticket) sums the partials in a fixed order and
+// updates the solver state on the device.  The host never reads a scalar
+// inside the loop: iterations run as CUDA-graph chunks and every kernel of a
+// finished solve returns at once; the host polls the state between chunks.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "device.h"
+
+namespace emg {
+
+struct SolverState {
+  double tol;
+  double bnorm;
+  double rz;      // CG: r.z of the current iteration
+  double rho;     // BiCGSTAB: rho of the current iteration
+  double alpha, beta, omega;
+  double res;     // last relative residual
+  double prev;    // previous relative residual
+  int32_t max_iter;
+  int32_t iter;   // current iteration (1-based)
+  int32_t status;
+  int32_t done;
+  int32_t early;  // BiCGSTAB early exit on ||s|| pending
+  int32_t dcount; // BiCGSTAB growth counter
+  uint32_t ticket;
+  int32_t pad;
+};
+
+struct KrylovWorkspace {
+  int64_t n = 0;
+  int grid = 0;
+  double *dinv = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+  double *rh = nullptr, *v = nullptr, *s = nullptr, *t = nullptr;
+  double* partial = nullptr;
+  double* hist = nullptr;
+  int32_t hist_cap = 0;
+  int32_t hist_len = 0;
+  SolverState* state = nullptr;
+  SolverState* state_h = nullptr;  // pinned
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  cudaGraphExec_t bi_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kLanes = 8;      // lanes per CSR row in the SpMV
+constexpr int kChunk = 16;     // iterations per graph launch
+
+__device__ __forceinline__ int64_t gtid() {
+  return static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+}
+__device__ __forceinline__ int64_t gstride() {
+  return static_cast<int64_t>(gridDim.x) * blockDim.x;
+}
+
+// Rows handled by this thread's lane group; y = A x for those rows.  Returns
+// this thread's share of sum_i w[i] * y[i] (only the group leader
+// contributes), w may be null.
+template <int L>
+__device__ __forceinline__ double spmv_rows(int64_t n, const int32_t* __restrict__ rp,
+                                            const int32_t* __restrict__ col,
+                                            const double* __restrict__ val,
+                                            const double* __restrict__ x, double* __restrict__ y,
+                                            const double* __restrict__ w) {
+  constexpr int G = kWarp / L;  // rows per warp step
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & (L - 1);
+  const int64_t warp = gtid() >> 5;
+  const int64_t nwarps = gstride() >> 5;
+  const uint64_t pol = evict_first_policy();
+  double dot = 0.0;
+  for (int64_t base = warp * G; base < n; base += nwarps * G) {
+    const int64_t row = base + lane / L;
+    double sum = 0.0;
+    if (row < n) {
+      const int32_t e = rp[row + 1];
+      for (int32_t k = rp[row] + sub; k < e; k += L) sum += ld_stream(val + k, pol) * x[ld_stream(col + k, pol)];
+    }
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (row < n && sub == 0) {
+      y[row] = sum;
+      if (w) dot += w[row] * sum;
+    }
+  }
+  return dot;
+}
+
+// One partial per block; true in the block that finished last (all partials
+// visible).  `vals` has kVals entries per thread.
+template <int kVals>
+__device__ __forceinline__ bool reduce_partials(const double (&vals)[kVals], double* partial,
+                                                SolverState* st, double (&tot)[kVals]) {
+  __shared__ double red[kThreads / 32];
+  __shared__ bool last;
+  for (int k = 0; k < kVals; ++k) {
+    double b = block_sum(vals[k], red);
+    if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = b;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  for (int k = 0; k < kVals; ++k) {
+    double a = 0.0;
+    for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += blockDim.x)
+      a += ld_l2(partial + k * gridDim.x + i);
+    tot[k] = block_sum(a, red);
+  }
+  if (threadIdx.x == 0) st->ticket = 0;
+  return true;
+}
+
+// ------------------------------------------------------------- Jacobi ----
+// CGSolver::setup_preconditioner (iterative_solvers.cpp:261-292):
+// 1/A(i,i), or 1 where |A(i,i)| <= 1e-15.  precond == 0 gives D^-1 = I.
+__global__ void k_jacobi(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                         const double* __restrict__ val, int precond, double* __restrict__ dinv) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    double d = 1.0;
+    if (precond) {
+      int32_t lo = rp[i], hi = rp[i + 1];
+      while (lo < hi) {
+        int32_t mid = (lo + hi) >> 1;
+        if (col[mid] < i) lo = mid + 1; else hi = mid;
+      }
+      double a = (lo < rp[i + 1] && col[lo] == i) ? val[lo] : 0.0;
+      d = fabs(a) > 1e-15 ? 1.0 / a : 1.0;
+    }
+    dinv[i] = d;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ col,
+                                                   const double* __restrict__ val,
+                                                   const double* __restrict__ x,
+                                                   double* __restrict__ y) {
+  spmv_rows<kLanes>(n, rp, col, val, x, y, nullptr);
+}
+
+// ----------------------------------------------------------------- CG ----
+__global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* __restrict__ b,
+                                                      const double* __restrict__ dinv,
+                                                      double* __restrict__ x, double* __restrict__ r,
+                                                      double* __restrict__ z, double* __restrict__ p,
+                                                      double* partial, SolverState* st) {
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double bi = b[i], zi = dinv[i] * bi;
+    x[i] = 0.0; r[i] = bi; z[i] = zi; p[i] = zi;
+    acc[0] += bi * bi;
+    acc[1] += bi * zi;
+  }
+  double tot[2];
+  if (!reduce_partials<2>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const double bn = sqrt(tot[0]);
+    st->bnorm = bn;
+    st->rz = tot[1];
+    st->iter = 1;
+    st->done = 0;
+    st->status = EMG_MAX_ITER_REACHED;
+    if (bn < 1e-15) {  // iterative_solvers.cpp:440-446
+      st->status = EMG_SUCCESS; st->iter = 0; st->res = 0.0; st->done = 1;
+      return;
+    }
+    st->res = sqrt(tot[0]) / bn;
+    st->prev = st->res;
+    if (st->max_iter < 1) { st->iter = st->max_iter; st->done = 1; }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(int64_t n, const int32_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ col,
+                                                          const double* __restrict__ val,
+                                                          const double* __restrict__ p,
+                                                          double* __restrict__ q, double* partial,
+                                                          SolverState* st) {
+  if (st->done) return;
+  double acc[1] = {spmv_rows<kLanes>(n, rp, col, val, p, q, p)};
+  double tot[1];
+  if (!reduce_partials<1>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const double pq = tot[0];
+    if (fabs(pq) < 1e-30) {  // :453-457
+      st->status = EMG_NUMERICAL_ERROR;
+      st->done = 1;
+    } else {
+      st->alpha = st->rz / pq;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, double* __restrict__ x,
+                                                        double* __restrict__ r,
+                                                        double* __restrict__ z,
+                                                        const double* __restrict__ p,
+                                                        const double* __restrict__ q,
+                                                        const double* __restrict__ dinv,
+                                                        double* partial, SolverState* st,
+                                                        double* hist, int32_t hist_cap) {
+  if (st->done) return;
+  const double a = st->alpha;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    const double zi = dinv[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    acc[0] += ri * zi;
+    acc[1] += ri * ri;
+  }
+  double tot[2];
+  if (!reduce_partials<2>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const int it = st->iter;
+    const double res = sqrt(tot[1]) / st->bnorm;
+    st->res = res;
+    if (it - 1 < hist_cap) hist[it - 1] = res;
+    if (res < st->tol) {
+      st->status = EMG_SUCCESS; st->done = 1;
+    } else if (it > 10 && res > st->prev * 1000.0) {  // :477-483
+      st->status = EMG_DIVERGED; st->done = 1;
+    } else {
+      st->beta = tot[0] / st->rz;
+      st->rz = tot[0];
+      st->prev = res;
+      if (it >= st->max_iter) { st->status = EMG_MAX_ITER_REACHED; st->done = 1; }
+      else st->iter = it + 1;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_direction(int64_t n, double* __restrict__ p,
+                                                           const double* __restrict__ z,
+                                                           const SolverState* st) {
+  if (st->done) return;
+  const double b = st->beta;
+  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + b * p[i];
+}
+
+// ----------------------------------------------------------- BiCGSTAB ----
+// Decide the start of iteration `next` (= it + 1) from rho_n = r.r_hat:
+// max-iteration stop, rho breakdown, else beta and rho.
+__device__ void bi_next_iteration(SolverState* st, int next, double rho_n) {
+  if (next > st->max_iter) {
+    st->status = EMG_MAX_ITER_REACHED; st->iter = st->max_iter; st->done = 1;
+  } else if (fabs(rho_n) < 1e-30) {  // :1031-1035
+    st->status = EMG_NUMERICAL_ERROR; st->iter = next; st->done = 1;
+  } else {
+    st->beta = (rho_n / st->rho) * (st->alpha / st->omega);
+    st->rho = rho_n;
+    st->iter = next;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_bi_init(int64_t n, const double* __restrict__ b,
+                                                      double* __restrict__ x, double* __restrict__ r,
+                                                      double* __restrict__ rh, double* __restrict__ p,
+                                                      double* __restrict__ v, double* partial,
+                                                      SolverState* st) {
+  double acc[1] = {0.0};
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double bi = b[i];
+    x[i] = 0.0; r[i] = bi; rh[i] = bi; p[i] = bi; v[i] = 0.0;
+    acc[0] += bi * bi;
+  }
+  double tot[1];
+  if (!reduce_partials<1>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const double bn = sqrt(tot[0]);
+    st->bnorm = bn;
+    st->rho = tot[0];
+    st->alpha = 1.0; st->omega = 1.0;
+    st->done = 0; st->early = 0; st->dcount = 0;
+    st->status = EMG_MAX_ITER_REACHED;
+    if (bn < 1e-15) {
+      st->status = EMG_SUCCESS; st->iter = 0; st->res = 0.0; st->done = 1;
+      return;
+    }
+    st->res = sqrt(tot[0]) / bn;
+    st->prev = st->res;
+    bi_next_iteration(st, 1, tot[0]);  // rho of iteration 1 = r.r_hat = b.b
+  }
+}
+
+// p = r + beta (p - omega v)
+__global__ void __launch_bounds__(kThreads) k_bi_p(int64_t n, double* __restrict__ p,
+                                                   const double* __restrict__ r,
+                                                   const double* __restrict__ v,
+                                                   const SolverState* st) {
+  if (st->done) return;
+  const double b = st->beta, w = st->omega;
+  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = r[i] + b * (p[i] - w * v[i]);
+}
+
+// v = A p, r_hat . v -> alpha
+__global__ void __launch_bounds__(kThreads) k_bi_v(int64_t n, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ col,
+                                                   const double* __restrict__ val,
+                                                   const double* __restrict__ p,
+                                                   double* __restrict__ v,
+                                                   const double* __restrict__ rh, double* partial,
+                                                   SolverState* st) {
+  if (st->done) return;
+  double acc[1] = {spmv_rows<kLanes>(n, rp, col, val, p, v, rh)};
+  double tot[1];
+  if (!reduce_partials<1>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    if (fabs(tot[0]) < 1e-30) {  // :1043-1047
+      st->status = EMG_NUMERICAL_ERROR; st->done = 1;
+    } else {
+      st->alpha = st->rho / tot[0];
+    }
+  }
+}
+
+// s = r - alpha v, z = D^-1 s, ||s|| -> early exit
+__global__ void __launch_bounds__(kThreads) k_bi_s(int64_t n, const double* __restrict__ r,
+                                                   const double* __restrict__ v,
+                                                   const double* __restrict__ dinv,
+                                                   double* __restrict__ s, double* __restrict__ z,
+                                                   double* partial, SolverState* st) {
+  if (st->done) return;
+  const double a = st->alpha;
+  double acc[1] = {0.0};
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double si = r[i] - a * v[i];
+    s[i] = si;
+    z[i] = dinv[i] * si;
+    acc[0] += si * si;
+  }
+  double tot[1];
+  if (!reduce_partials<1>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const double rs = sqrt(tot[0]) / st->bnorm;
+    if (rs < st->tol) {  // :1050-1058
+      st->res = rs;
+      st->early = 1;
+    }
+  }
+}
+
+// t = A z, t.t and z.t -> omega
+__global__ void __launch_bounds__(kThreads) k_bi_t(int64_t n, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ col,
+                                                   const double* __restrict__ val,
+                                                   const double* __restrict__ z,
+                                                   double* __restrict__ t, double* partial,
+                                                   SolverState* st) {
+  if (st->done || st->early) return;
+  const int lane = threadIdx.x & 31;
+  (void)lane;
+  double tt = 0.0, zt = 0.0;
+  {
+    constexpr int L = kLanes, G = kWarp / L;
+    const int sub = threadIdx.x & (L - 1);
+    const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+    const uint64_t pol = evict_first_policy();
+    for (int64_t base = warp * G; base < n; base += nwarps * G) {
+      const int64_t row = base + (threadIdx.x & 31) / L;
+      double sum = 0.0;
+      if (row < n) {
+        const int32_t e = rp[row + 1];
+        for (int32_t k = rp[row] + sub; k < e; k += L) sum += ld_stream(val + k, pol) * z[ld_stream(col + k, pol)];
+      }
+#pragma unroll
+      for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (row < n && sub == 0) {
+        t[row] = sum;
+        tt += sum * sum;
+        zt += z[row] * sum;
+      }
+    }
+  }
+  double acc[2] = {tt, zt};
+  double tot[2];
+  if (!reduce_partials<2>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) st->omega = fabs(tot[0]) < 1e-30 ? 0.0 : tot[1] / tot[0];
+}
+
+// x += alpha p + omega z, r = s - omega t; residual checks; next rho
+__global__ void __launch_bounds__(kThreads) k_bi_x(int64_t n, double* __restrict__ x,
+                                                   double* __restrict__ r,
+                                                   const double* __restrict__ p,
+                                                   const double* __restrict__ z,
+                                                   const double* __restrict__ s,
+                                                   const double* __restrict__ t,
+                                                   const double* __restrict__ rh, double* partial,
+                                                   SolverState* st, double* hist,
+                                                   int32_t hist_cap) {
+  if (st->done) return;
+  const double a = st->alpha;
+  if (st->early) {
+    for (int64_t i = gtid(); i < n; i += gstride()) x[i] += a * p[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->status = EMG_SUCCESS;
+      const int it = st->iter;
+      if (it - 1 < hist_cap) hist[it - 1] = st->res;
+    }
+    // `done` is raised by the host-visible ticket below so that every block
+    // has read `early` before it changes.
+    double acc0[1] = {0.0}, tot0[1];
+    if (reduce_partials<1>(acc0, partial, st, tot0) && threadIdx.x == 0) st->done = 1;
+    return;
+  }
+  const double w = st->omega;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    x[i] += a * p[i] + w * z[i];
+    const double ri = s[i] - w * t[i];
+    r[i] = ri;
+    acc[0] += ri * ri;
+    acc[1] += ri * rh[i];
+  }
+  double tot[2];
+  if (!reduce_partials<2>(acc, partial, st, tot)) return;
+  if (threadIdx.x == 0) {
+    const int it = st->iter;
+    const double res = sqrt(tot[0]) / st->bnorm;
+    st->res = res;
+    if (it - 1 < hist_cap) hist[it - 1] = res;
+    if (res < st->tol) { st->status = EMG_SUCCESS; st->done = 1; return; }
+    if (res > st->prev * 1.5 && it > 20) {  // :1083-1093
+      if (++st->dcount >= 3) { st->status = EMG_DIVERGED; st->done = 1; return; }
+    } else {
+      st->dcount = 0;
+    }
+    if (it > 10 && res > st->prev * 1000.0) { st->status = EMG_DIVERGED; st->done = 1; return; }
+    st->prev = res;
+    bi_next_iteration(st, it + 1, tot[1]);
+  }
+}
+
+int grid_size() {
+  static int g = 0;
+  if (!g) {
+    int dev = 0, sms = 148, per = 4;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g = sms * per;
+  }
+  return g;
+}
+
+int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter) {
+  if (!A.ws) {
+    A.ws = new KrylovWorkspace();
+    KrylovWorkspace& w = *A.ws;
+    w.n = A.n;
+    w.grid = grid_size();
+    const size_t vb = sizeof(double) * (A.n > 0 ? A.n : 1);
+    EMG_CK(cudaMalloc(&w.dinv, vb));
+    EMG_CK(cudaMalloc(&w.x, vb));
+    EMG_CK(cudaMalloc(&w.r, vb));
+    EMG_CK(cudaMalloc(&w.z, vb));
+    EMG_CK(cudaMalloc(&w.p, vb));
+    EMG_CK(cudaMalloc(&w.q, vb));
+    EMG_CK(cudaMalloc(&w.partial, sizeof(double) * 4 * w.grid));
+    EMG_CK(cudaMalloc(&w.state, sizeof(SolverState)));
+    EMG_CK(cudaMemset(w.state, 0, sizeof(SolverState)));
+    EMG_CK(cudaMallocHost(&w.state_h, sizeof(SolverState)));
+    EMG_CK(cudaStreamCreate(&w.cap));
+    EMG_CK(cudaEventCreate(&w.ev0));
+    EMG_CK(cudaEventCreate(&w.ev1));
+  }
+  KrylovWorkspace& w = *A.ws;
+  if (bicg && !w.rh) {
+    const size_t vb = sizeof(double) * (A.n > 0 ? A.n : 1);
+    EMG_CK(cudaMalloc(&w.rh, vb));
+    EMG_CK(cudaMalloc(&w.v, vb));
+    EMG_CK(cudaMalloc(&w.s, vb));
+    EMG_CK(cudaMalloc(&w.t, vb));
+  }
+  if (max_iter > w.hist_cap) {
+    if (w.hist) EMG_CK(cudaFree(w.hist));
+    w.hist_cap = max_iter;
+    EMG_CK(cudaMalloc(&w.hist, sizeof(double) * w.hist_cap));
+    // the chunk graphs hold the old pointer
+    if (w.cg_exec) { cudaGraphExecDestroy(w.cg_exec); w.cg_exec = nullptr; }
+    if (w.bi_exec) { cudaGraphExecDestroy(w.bi_exec); w.bi_exec = nullptr; }
+  }
+  return EMG_SUCCESS;
+}
+
+int capture_chunk(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
+  KrylovWorkspace& w = *A.ws;
+  const int g = w.grid;
+  cudaGraph_t graph = nullptr;
+  EMG_CK(cudaStreamBeginCapture(w.cap, cudaStreamCaptureModeThreadLocal));
+  for (int c = 0; c < kChunk; ++c) {
+    if (!bicg) {
+      k_cg_spmv_dot<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.q, w.partial, w.state);
+      k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
+                                             w.hist, w.hist_cap);
+      k_cg_direction<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
+    } else {
+      k_bi_p<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
+      k_bi_v<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.v, w.rh, w.partial, w.state);
+      k_bi_s<<<g, kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
+      k_bi_t<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.z, w.t, w.partial, w.state);
+      k_bi_x<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
+                                        w.hist, w.hist_cap);
+    }
+  }
+  cudaError_t e = cudaStreamEndCapture(w.cap, &graph);
+  if (e != cudaSuccess) { set_error(std::string("graph capture: ") + cudaGetErrorString(e)); return EMG_ERR_CUDA; }
+  e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { set_error(std::string("graph instantiate: ") + cudaGetErrorString(e)); return EMG_ERR_CUDA; }
+  return EMG_SUCCESS;
+}
+
+int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
+               cudaStream_t user, emg_result* res, bool bicg) {
+  std::memset(res, 0, sizeof(*res));
+  res->status = EMG_INVALID_INPUT;
+  if (!b || !x) { set_error("null vector"); return EMG_INVALID_INPUT; }
+  if (A.n <= 0) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
+  const int32_t max_iter = cfg.max_iterations;
+  int rc = ensure_ws(A, bicg, max_iter > 0 ? max_iter : 1);
+  if (rc) { res->status = rc; return rc; }
+  KrylovWorkspace& w = *A.ws;
+  cudaStream_t st = user ? user : w.cap;
+  cudaGraphExec_t* exec = bicg ? &w.bi_exec : &w.cg_exec;
+  if (!*exec) {
+    rc = capture_chunk(A, bicg, exec);
+    if (rc) { res->status = rc; return rc; }
+  }
+  SolverState init;
+  std::memset(&init, 0, sizeof(init));
+  init.tol = cfg.tolerance;
+  init.max_iter = max_iter;
+  *w.state_h = init;
+  EMG_CK(cudaEventRecord(w.ev0, st));
+  EMG_CK(cudaMemcpyAsync(w.state, w.state_h, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+  const int g = w.grid;
+  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, cfg.preconditioner, w.dinv);
+  if (!bicg)
+    k_cg_init<<<g, kThreads, 0, st>>>(A.n, b, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
+  else
+    k_bi_init<<<g, kThreads, 0, st>>>(A.n, b, w.x, w.r, w.rh, w.p, w.v, w.partial, w.state);
+  EMG_CK(cudaGetLastError());
+  // Graph chunks until the device state says done; bounded by max_iter.
+  const int64_t max_chunks = (static_cast<int64_t>(max_iter > 0 ? max_iter : 0) + kChunk - 1) / kChunk + 1;
+  bool done = false;
+  for (int64_t c = 0; c <= max_chunks; ++c) {
+    EMG_CK(cudaMemcpyAsync(w.state_h, w.state, sizeof(SolverState), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    if (w.state_h->done) { done = true; break; }
+    EMG_CK(cudaGraphLaunch(*exec, st));
+  }
+  EMG_CK(cudaEventRecord(w.ev1, st));
+  EMG_CK(cudaMemcpyAsync(x, w.x, sizeof(double) * A.n, cudaMemcpyDeviceToDevice, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  float ms = 0.0f;
+  EMG_CK(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
+  if (!done) {
+    set_error("solver state did not finish within the iteration bound");
+    res->status = EMG_ERR_INTERNAL;
+    return EMG_ERR_INTERNAL;
+  }
+  const SolverState& s = *w.state_h;
+  res->status = s.status;
+  res->iterations = s.iter;
+  res->residual_norm = s.res;
+  res->solve_time_ms = ms;
+  w.hist_len = s.iter < w.hist_cap ? s.iter : w.hist_cap;
+  if (w.hist_len < 0) w.hist_len = 0;
+  return s.status;
+}
+
+}  // namespace
+
+int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
+  if (!x || !y) { set_error("null vector"); return EMG_INVALID_INPUT; }
+  k_spmv<<<grid_size(), kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, x, y);
+  EMG_CK(cudaGetLastError());
+  return EMG_SUCCESS;
+}
+
+int cg_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg, cudaStream_t st,
+             emg_result* res) {
+  return run_solver(A, b, x, cfg, st, res, false);
+}
+
+int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
+                   cudaStream_t st, emg_result* res) {
+  return run_solver(A, b, x, cfg, st, res, true);
+}
+
+int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms) {
+  if (iterations <= 0 || !ms) { set_error("bad arguments"); return EMG_INVALID_INPUT; }
+  int rc = ensure_ws(A, false, 1);
+  if (rc) return rc;
+  KrylovWorkspace& w = *A.ws;
+  cudaStream_t st = user ? user : w.cap;
+  const int g = w.grid;
+  double* ones = nullptr;
+  EMG_CK(cudaMallocAsync(&ones, sizeof(double) * A.n, st));
+  std::vector<double> h(A.n, 1.0);
+  EMG_CK(cudaMemcpyAsync(ones, h.data(), sizeof(double) * A.n, cudaMemcpyHostToDevice, st));
+  SolverState init;
+  std::memset(&init, 0, sizeof(init));
+  init.tol = 0.0;
+  init.max_iter = 1 << 30;
+  *w.state_h = init;
+  EMG_CK(cudaMemcpyAsync(w.state, w.state_h, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, 1, w.dinv);
+  k_cg_init<<<g, kThreads, 0, st>>>(A.n, ones, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
+  std::vector<cudaEvent_t> ev(4 * iterations);
+  for (auto& e : ev) EMG_CK(cudaEventCreate(&e));
+  for (int i = 0; i < iterations; ++i) {
+    EMG_CK(cudaEventRecord(ev[4 * i], st));
+    k_cg_spmv_dot<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.q, w.partial, w.state);
+    EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
+    k_cg_update<<<g, kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
+                                        w.hist, w.hist_cap);
+    EMG_CK(cudaEventRecord(ev[4 * i + 2], st));
+    k_cg_direction<<<g, kThreads, 0, st>>>(A.n, w.p, w.z, w.state);
+    EMG_CK(cudaEventRecord(ev[4 * i + 3], st));
+  }
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaStreamSynchronize(st));
+  EMG_CK(cudaMemcpy(w.state_h, w.state, sizeof(SolverState), cudaMemcpyDeviceToHost));
+  double acc[3] = {0, 0, 0};
+  for (int i = 0; i < iterations; ++i)
+    for (int k = 0; k < 3; ++k) {
+      float t = 0.0f;
+      EMG_CK(cudaEventElapsedTime(&t, ev[4 * i + k], ev[4 * i + k + 1]));
+      acc[k] += t;
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  EMG_CK(cudaFreeAsync(ones, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  if (w.state_h->done) {
+    set_error("solver state finished during kernel timing (breakdown)");
+    return EMG_NUMERICAL_ERROR;
+  }
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iterations;
+  return EMG_SUCCESS;
+}
+
+int csr_history(DevCsr& A, double* out, int32_t cap) {
+  if (!A.ws || !A.ws->hist || A.ws->hist_len <= 0) return 0;
+  int32_t n = A.ws->hist_len < cap ? A.ws->hist_len : cap;
+  if (n <= 0) return 0;
+  EMG_CK(cudaMemcpy(out, A.ws->hist, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return n;
+}
+
+void free_workspace(KrylovWorkspace* w) {
+  if (!w) return;
+  if (w->cg_exec) cudaGraphExecDestroy(w->cg_exec);
+  if (w->bi_exec) cudaGraphExecDestroy(w->bi_exec);
+  cudaFree(w->dinv); cudaFree(w->x); cudaFree(w->r); cudaFree(w->z); cudaFree(w->p); cudaFree(w->q);
+  cudaFree(w->rh); cudaFree(w->v); cudaFree(w->s); cudaFree(w->t);
+  cudaFree(w->partial); cudaFree(w->hist); cudaFree(w->state);
+  if (w->state_h) cudaFreeHost(w->state_h);
+  if (w->cap) cudaStreamDestroy(w->cap);
+  if (w->ev0) cudaEventDestroy(w->ev0);
+  if (w->ev1) cudaEventDestroy(w->ev1);
+  delete w;
+}
+
+// Pattern and values come from the stream-ordered pool (cudaMallocAsync).
+DevCsr::~DevCsr() {
+  free_workspace(ws);
+  if (owns_pattern) {
+    if (row_ptr) cudaFreeAsync(row_ptr, 0);
+    if (col) cudaFreeAsync(col, 0);
+  }
+  if (owns_values && val) cudaFreeAsync(val, 0);
+}
+
+}  // namespace emg

@@ -1,0 +1,317 @@
+// numbering.cpp -- host integer work of the solve path: global edge IDs, the
+// free-DOF numbering and the tree-cotree gauge.  The results are bit-exact to
+// the reference classes
+//   GlobalEdgeIDGenerator  (src/fe_em/global_edge_id_generator.cpp:30-110)
+//   EMDOFManager           (src/fe_em/em_dof_manager.cpp:29-393, :448-626)
+//   MeshGraphExtractor     (src/fe_em/mesh_graph_extractor.cpp:29-176)
+//   SpanningTreeBuilder    (src/fe_em/spanning_tree.cpp:295-598)
+//   MultiConnectedDomainDetector (src/fe_em/multi_connected_domain.cpp:21-250)
+//   TreeGauge              (src/fe_em/tree_gauge.cpp:37-290)
+// but run in O(E) / O(E log d) with flat arrays instead of hash maps and
+// std::set, and without the O(N^2) renumbering scan of em_dof_manager.cpp:245-286.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "internal.h"
+
+namespace emg {
+namespace {
+
+// TET4 local edges, ElementGeometry::get_local_edges(TET4) (element_geometry.cpp:115-126).
+constexpr int kGeoEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+
+// Compressed adjacency: for every bucket a contiguous run of entries.
+struct Buckets {
+  std::vector<int64_t> ptr;
+  std::vector<int32_t> a;  // first payload
+  std::vector<int32_t> b;  // second payload
+};
+
+}  // namespace
+
+// Edge IDs by first appearance.  Each element edge (lo, hi, position) is
+// bucketed by its lower node; buckets are filled in position order, so the
+// leader of a (lo, hi) key is the first entry of the bucket with that hi.  The
+// leaders in position order receive consecutive IDs -- exactly the order in
+// which the reference's hash map assigns new IDs.
+int build_edge_ids(Mesh& m) {
+  if (m.edges_built) return EMG_SUCCESS;
+  const int64_t T = m.n_tets, V = m.n_nodes, M = 6 * T;
+  Buckets bk;
+  bk.ptr.assign(V + 1, 0);
+  for (int64_t t = 0; t < T; ++t)
+    for (int k = 0; k < 6; ++k) {
+      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+      bk.ptr[std::min(u, w) + 1]++;
+    }
+  for (int64_t v = 0; v < V; ++v) bk.ptr[v + 1] += bk.ptr[v];
+  bk.a.resize(M);  // hi node
+  bk.b.resize(M);  // position
+  std::vector<int64_t> cur(bk.ptr.begin(), bk.ptr.end() - 1);
+  for (int64_t t = 0; t < T; ++t)
+    for (int k = 0; k < 6; ++k) {
+      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+      int64_t s = cur[std::min(u, w)]++;
+      bk.a[s] = std::max(u, w);
+      bk.b[s] = static_cast<int32_t>(6 * t + k);
+    }
+  // leader position of every entry
+  std::vector<int32_t> leader(M);
+  std::vector<uint8_t> is_leader(M, 0);
+  for (int64_t v = 0; v < V; ++v) {
+    for (int64_t s = bk.ptr[v]; s < bk.ptr[v + 1]; ++s) {
+      int64_t f = bk.ptr[v];
+      while (bk.a[f] != bk.a[s]) ++f;  // first entry with the same hi
+      leader[bk.b[s]] = bk.b[f];
+      if (f == s) is_leader[bk.b[s]] = 1;
+    }
+  }
+  std::vector<int32_t> id_at(M, -1);
+  int64_t next = 0;
+  for (int64_t p = 0; p < M; ++p)
+    if (is_leader[p]) id_at[p] = static_cast<int32_t>(next++);
+  m.n_edges = next;
+  m.elem_edge.resize(M);
+  m.edge_nodes.resize(2 * next);
+  for (int64_t p = 0; p < M; ++p) {
+    int32_t id = id_at[leader[p]];
+    m.elem_edge[p] = id;
+    if (is_leader[p]) {
+      int64_t t = p / 6;
+      int k = static_cast<int>(p % 6);
+      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+      m.edge_nodes[2 * id] = std::min(u, w);
+      m.edge_nodes[2 * id + 1] = std::max(u, w);
+    }
+  }
+  m.edges_built = true;
+  return EMG_SUCCESS;
+}
+
+namespace {
+
+// Graph of the mesh edges over compact node indices (rank of the global node
+// ID among referenced nodes), neighbours ascending -- MeshGraphExtractor.
+struct EdgeGraph {
+  int32_t n_nodes = 0;
+  std::vector<int32_t> compact;  // global node -> compact index or -1
+  std::vector<int64_t> ptr;
+  std::vector<int32_t> nb;       // neighbour compact index
+  std::vector<int32_t> edge;     // global edge ID of the entry
+};
+
+EdgeGraph make_graph(const Mesh& m) {
+  EdgeGraph g;
+  g.compact.assign(m.n_nodes, -1);
+  for (int32_t v : m.tets) g.compact[v] = 0;
+  int32_t c = 0;
+  for (int64_t v = 0; v < m.n_nodes; ++v)
+    if (g.compact[v] == 0) g.compact[v] = c++;
+  g.n_nodes = c;
+  g.ptr.assign(static_cast<size_t>(c) + 1, 0);
+  const int64_t E = m.n_edges;
+  for (int64_t e = 0; e < E; ++e) {
+    g.ptr[g.compact[m.edge_nodes[2 * e]] + 1]++;
+    g.ptr[g.compact[m.edge_nodes[2 * e + 1]] + 1]++;
+  }
+  for (int32_t v = 0; v < c; ++v) g.ptr[v + 1] += g.ptr[v];
+  g.nb.resize(2 * E);
+  g.edge.resize(2 * E);
+  std::vector<int64_t> cur(g.ptr.begin(), g.ptr.end() - 1);
+  for (int64_t e = 0; e < E; ++e) {
+    int32_t u = g.compact[m.edge_nodes[2 * e]], w = g.compact[m.edge_nodes[2 * e + 1]];
+    g.nb[cur[u]] = w; g.edge[cur[u]++] = static_cast<int32_t>(e);
+    g.nb[cur[w]] = u; g.edge[cur[w]++] = static_cast<int32_t>(e);
+  }
+  std::vector<std::pair<int32_t, int32_t>> tmp;
+  for (int32_t v = 0; v < c; ++v) {
+    tmp.clear();
+    for (int64_t s = g.ptr[v]; s < g.ptr[v + 1]; ++s) tmp.emplace_back(g.nb[s], g.edge[s]);
+    std::sort(tmp.begin(), tmp.end());
+    for (size_t i = 0; i < tmp.size(); ++i) {
+      g.nb[g.ptr[v] + i] = tmp[i].first;
+      g.edge[g.ptr[v] + i] = tmp[i].second;
+    }
+  }
+  return g;
+}
+
+// Plain BFS over all edges from the nodes already queued (queue[head..tail)).
+void bfs_all(const EdgeGraph& g, std::vector<int32_t>& queue, size_t head,
+             std::vector<uint8_t>& seen, std::vector<uint8_t>& tree) {
+  for (size_t h = head; h < queue.size(); ++h) {
+    int32_t u = queue[h];
+    for (int64_t s = g.ptr[u]; s < g.ptr[u + 1]; ++s) {
+      int32_t v = g.nb[s];
+      if (seen[v]) continue;
+      seen[v] = 1;
+      tree[g.edge[s]] = 1;
+      queue.push_back(v);
+    }
+  }
+}
+
+// Spanning tree; tree[e] = 1 for tree edges.  Returns the root.
+int32_t spanning_tree(const Mesh& m, const EdgeGraph& g, const std::vector<uint8_t>& constrained,
+                      int32_t gauge_mode, std::vector<uint8_t>& tree) {
+  const int64_t E = m.n_edges;
+  tree.assign(E, 0);
+  std::vector<uint8_t> seen(g.n_nodes, 0);
+  std::vector<int32_t> queue;
+  queue.reserve(g.n_nodes);
+  // Root: smaller compact endpoint of the lowest constrained edge ID, else 0
+  // (SpanningTreeBuilder::selectRootNode, DIRICHLET_BOUNDARY, spanning_tree.cpp:517-540).
+  int32_t root = 0;
+  for (int64_t e = 0; e < E; ++e)
+    if (constrained[e]) { root = g.compact[m.edge_nodes[2 * e]]; break; }
+  if (g.n_nodes == 0) return -1;
+  seen[root] = 1;
+  queue.push_back(root);
+  if (gauge_mode == EMG_GAUGE_REF) {
+    // buildBFSTreeWithBoundaryPriority (spanning_tree.cpp:353-416): for each
+    // dequeued node, its unseen neighbours across constrained edges join the
+    // tree first, then the others; both groups in ascending neighbour order.
+    std::vector<int64_t> later;
+    for (size_t h = 0; h < queue.size(); ++h) {
+      int32_t u = queue[h];
+      later.clear();
+      for (int64_t s = g.ptr[u]; s < g.ptr[u + 1]; ++s) {
+        int32_t v = g.nb[s];
+        if (seen[v]) continue;
+        if (constrained[g.edge[s]]) {
+          seen[v] = 1;
+          tree[g.edge[s]] = 1;
+          queue.push_back(v);
+        } else {
+          later.push_back(s);
+        }
+      }
+      for (int64_t s : later) {
+        int32_t v = g.nb[s];
+        if (seen[v]) continue;
+        seen[v] = 1;
+        tree[g.edge[s]] = 1;
+        queue.push_back(v);
+      }
+    }
+  } else {
+    // Boundary-first: span the constrained-edge subgraph before anything else
+    // (every constrained component, lowest edge first), then grow the tree
+    // into the interior by plain BFS in visit order.  Every node off the
+    // constrained subgraph then owns exactly one tree edge, so the kept
+    // unknowns are E_free - V_interior (a complete, not over-constrained,
+    // gauge for a connected Dirichlet boundary).
+    auto span_constrained = [&](size_t head) {
+      for (size_t h = head; h < queue.size(); ++h) {
+        int32_t u = queue[h];
+        for (int64_t s = g.ptr[u]; s < g.ptr[u + 1]; ++s) {
+          int32_t v = g.nb[s];
+          if (seen[v] || !constrained[g.edge[s]]) continue;
+          seen[v] = 1;
+          tree[g.edge[s]] = 1;
+          queue.push_back(v);
+        }
+      }
+    };
+    span_constrained(0);
+    for (int64_t e = 0; e < E; ++e) {
+      if (!constrained[e]) continue;
+      int32_t s0 = g.compact[m.edge_nodes[2 * e]];
+      if (seen[s0]) continue;
+      seen[s0] = 1;
+      size_t head = queue.size();
+      queue.push_back(s0);
+      span_constrained(head);
+    }
+    bfs_all(g, queue, 0, seen, tree);
+  }
+  // Remaining components, lowest unseen index first (spanning_tree.cpp:418-445).
+  for (int32_t s = 0; s < g.n_nodes; ++s) {
+    if (seen[s]) continue;
+    seen[s] = 1;
+    size_t head = queue.size();
+    queue.push_back(s);
+    bfs_all(g, queue, head, seen, tree);
+  }
+  return root;
+}
+
+}  // namespace
+
+int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
+  int rc = build_edge_ids(m);
+  if (rc) return rc;
+  const int64_t E = m.n_edges, T = m.n_tets;
+  out = DofMap{};
+  out.n_tets = T;
+  out.n_edges = E;
+  // Edge lookup by node pair: edges bucketed by lower node.
+  std::vector<int64_t> lptr(m.n_nodes + 1, 0);
+  for (int64_t e = 0; e < E; ++e) lptr[m.edge_nodes[2 * e] + 1]++;
+  for (int64_t v = 0; v < m.n_nodes; ++v) lptr[v + 1] += lptr[v];
+  std::vector<int32_t> lid(E);
+  {
+    std::vector<int64_t> cur(lptr.begin(), lptr.end() - 1);
+    for (int64_t e = 0; e < E; ++e) lid[cur[m.edge_nodes[2 * e]]++] = static_cast<int32_t>(e);
+  }
+  // markConstrainedDOFs (em_dof_manager.cpp:152-243): node pairs that are not
+  // mesh edges are skipped.
+  std::vector<uint8_t> constrained(E, 0);
+  const int64_t D = static_cast<int64_t>(m.dirichlet.size() / 2);
+  for (int64_t d = 0; d < D; ++d) {
+    int32_t a = m.dirichlet[2 * d], b = m.dirichlet[2 * d + 1];
+    if (a < 0 || b < 0 || a >= m.n_nodes || b >= m.n_nodes) continue;
+    int32_t lo = std::min(a, b), hi = std::max(a, b);
+    for (int64_t s = lptr[lo]; s < lptr[lo + 1]; ++s)
+      if (m.edge_nodes[2 * lid[s] + 1] == hi) { constrained[lid[s]] = 1; break; }
+  }
+  // Prenumber of an edge in an all-vector mesh = its global ID
+  // (assignPrenumbering, :91-150); free index = rank among the unconstrained
+  // (renumberFreeDOFs, :245-286).
+  std::vector<int32_t> free_of(E);
+  int64_t nf = 0;
+  for (int64_t e = 0; e < E; ++e) free_of[e] = constrained[e] ? -1 : static_cast<int32_t>(nf++);
+  out.n_free = nf;
+  out.edge_dof.assign(E, -1);
+  if (gauge_mode == EMG_GAUGE_NONE) {
+    out.edge_dof = free_of;
+    out.n_dofs = nf;
+  } else if (gauge_mode == EMG_GAUGE_REF || gauge_mode == EMG_GAUGE_BOUNDARY_FIRST) {
+    EdgeGraph g = make_graph(m);
+    std::vector<uint8_t> tree;
+    out.root = spanning_tree(m, g, constrained, gauge_mode, tree);
+    // Circulation DOFs (selectCirculationDOFs, multi_connected_domain.cpp:190-232):
+    // one evenly spaced pick per hole marker from the ascending cotree list,
+    // taken before constrained edges are promoted to the tree.
+    std::vector<uint8_t> circ(E, 0);
+    std::vector<int32_t> cot;
+    for (int64_t e = 0; e < E; ++e) if (!tree[e]) cot.push_back(static_cast<int32_t>(e));
+    if (m.n_hole_markers > 0 && !cot.empty()) {
+      int64_t pick = std::min<int64_t>(m.n_hole_markers, static_cast<int64_t>(cot.size()));
+      for (int64_t i = 0; i < pick; ++i) {
+        int64_t idx = std::min<int64_t>((i * static_cast<int64_t>(cot.size())) / pick,
+                                        static_cast<int64_t>(cot.size()) - 1);
+        circ[cot[idx]] = 1;
+      }
+    }
+    // classifyEdges / buildReducedMapping (tree_gauge.cpp:159-212) and
+    // renumberVectorDOFsWithTreeGauge (em_dof_manager.cpp:501-626).
+    std::vector<int32_t> reduced(E, -1);
+    int64_t nr = 0;
+    for (int64_t e = 0; e < E; ++e)
+      if (!tree[e] && !constrained[e] && !circ[e]) reduced[e] = static_cast<int32_t>(nr++);
+    for (int64_t e = 0; e < E; ++e)
+      if (circ[e] && reduced[e] < 0) reduced[e] = static_cast<int32_t>(nr++);
+    for (int64_t e = 0; e < E; ++e) out.edge_dof[e] = free_of[e] < 0 ? -1 : reduced[e];
+    out.n_dofs = nr;
+  } else {
+    set_error("unknown gauge mode");
+    return EMG_INVALID_INPUT;
+  }
+  out.l2g.resize(6 * T);
+  for (int64_t p = 0; p < 6 * T; ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  return EMG_SUCCESS;
+}
+
+}  // namespace emg

@@ -1,0 +1,201 @@
+/*
+ * emagddm_b200.h -- C ABI of the B200-native TET4 Nedelec curl-curl solve path.
+ *
+ * The entry points replace the CPU chain of Poofee/emagddm
+ *   GlobalEdgeIDGenerator -> EMDOFManager (+ TreeGauge) -> EMAssembly
+ *   -> CsrMatrix -> CGSolver / BiCGSTABSolver
+ * with host C++ integer numbering and hand-written sm_100a CUDA kernels.  Each
+ * declaration cites the reference interface it replaces (paths inside the
+ * reference project).
+ *
+ * Conventions
+ *   - Every function returns an int status; 0 (EMG_SUCCESS) means the call
+ *     ran.  Solver entry points return the solver outcome (the values of
+ *     numeric::SolverStatus, include/numeric/em_linear_solver.h:26-32) and
+ *     also store it in emg_result.status.  Nothing throws across the ABI.
+ *   - emg_last_error() returns a message for the last failing call of the
+ *     calling thread.
+ *   - Pointers are host pointers unless the name ends in _d (device).
+ *   - Handles own their device memory; arrays passed in are copied; arrays
+ *     passed out are caller-allocated.  One handle per thread / stream.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *   - Indices are 0-based int32 (the reference uses int throughout).
+ */
+#ifndef EMAGDDM_B200_H
+#define EMAGDDM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMG_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+  EMG_SUCCESS = 0,          /* SolverStatus::SUCCESS           */
+  EMG_NUMERICAL_ERROR = 1,  /* SolverStatus::NUMERICAL_ERROR   */
+  EMG_DIVERGED = 2,         /* SolverStatus::DIVERGED          */
+  EMG_MAX_ITER_REACHED = 3, /* SolverStatus::MAX_ITER_REACHED  */
+  EMG_INVALID_INPUT = 4,    /* SolverStatus::INVALID_INPUT     */
+  EMG_ERR_CUDA = 5,         /* a CUDA runtime call failed      */
+  EMG_ERR_TIMEOUT = 6,      /* a bounded device wait ran out   */
+  EMG_ERR_NOMEM = 7,        /* host or device allocation failed */
+  EMG_ERR_INTERNAL = 8      /* device-side consistency check failed */
+};
+
+/* ---- gauge modes (EMDOFManager::applyTreeGauge) -------------------------- */
+enum {
+  EMG_GAUGE_NONE = -1,          /* EMDOFManager::build only                   */
+  EMG_GAUGE_REF = 0,            /* reference tree gauge, bit-exact numbering  */
+  EMG_GAUGE_BOUNDARY_FIRST = 1  /* tree spans the Dirichlet boundary first    */
+};
+
+/* ---- assembly flags ------------------------------------------------------ */
+enum {
+  EMG_FLAG_MASS = 1,           /* also assemble M_ij = int sigma W_i . W_j      */
+  EMG_FLAG_NO_EDGE_SIGNS = 2,  /* scatter unsigned element matrices            */
+  EMG_FLAG_PIOLA_LITERAL = 4,  /* W_phys = J^-T W_ref / detJ (reference text)   */
+  EMG_FLAG_QUAD3_LITERAL = 8   /* the reference's 3-point TET4 rule             */
+};
+
+/* ---- source regions: J evaluated at quadrature points ------------------- */
+enum { EMG_SRC_BOX = 1, EMG_SRC_ANNULUS_Z = 2 };
+typedef struct {
+  int32_t kind;   /* EMG_SRC_*                                                  */
+  double j[3];    /* current density inside the region                          */
+  double p[6];    /* BOX: xmin,xmax,ymin,ymax,zmin,zmax (open intervals)        */
+                  /* ANNULUS_Z: cx,cy,rmin,rmax,zmin,zmax (r from (cx,cy), open) */
+} emg_source;
+
+/* ---- solver configuration and result ------------------------------------ */
+enum { EMG_PRECOND_NONE = 0, EMG_PRECOND_JACOBI = 1 };
+typedef struct {
+  double tolerance;          /* ||r||/||b|| stop threshold (IterativeSolverConfig, default 1e-8) */
+  int32_t max_iterations;    /* default 1000                                          */
+  int32_t preconditioner;    /* EMG_PRECOND_*                                          */
+} emg_krylov_config;
+
+typedef struct {
+  int32_t status;            /* SolverStatus value                           */
+  int32_t iterations;        /* iterations performed                         */
+  double residual_norm;      /* relative residual ||r||/||b||                */
+  double solve_time_ms;      /* device time of the solve (CUDA events)       */
+} emg_result;                /* numeric::SolverResult, em_linear_solver.h:53-61 */
+
+typedef struct emg_mesh_t* emg_mesh;
+typedef struct emg_dofmap_t* emg_dofmap;
+typedef struct emg_system_t* emg_system;
+typedef struct emg_csr_t* emg_csr;
+
+/* ---- library ------------------------------------------------------------ */
+int32_t emg_abi_version(void);
+const char* emg_last_error(void);
+
+/* ---- mesh: fe_em::EMMeshData (include/fe_em/em_mesh_data.hpp:90-230) ----
+ * xyz: 3*n_nodes; tets: 4*n_tets (TET4_EDGE, VECTOR_EDGE_ONLY); material_id:
+ * n_tets or NULL; dirichlet_pairs: 2*n_dirichlet node pairs of the
+ * DIRICHLET / VECTOR_EDGE_ONLY marker; n_hole_markers: number of boundary
+ * markers the reference's name heuristic counts as holes
+ * (src/fe_em/multi_connected_domain.cpp:126-188). */
+int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
+                    const int32_t* material_id, int64_t n_dirichlet,
+                    const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out);
+void emg_mesh_destroy(emg_mesh mesh);
+
+/* ---- GlobalEdgeIDGenerator::generate (src/fe_em/global_edge_id_generator.cpp:30-110)
+ * elem_edge: 6*n_tets output or NULL; edge_nodes: 2*n_edges sorted node pair
+ * per edge or NULL (size the buffer with a first call passing NULL). */
+int emg_edge_ids(emg_mesh mesh, int32_t* elem_edge, int32_t* edge_nodes, int64_t* n_edges);
+
+/* ---- EMDOFManager::build (src/fe_em/em_dof_manager.cpp:29-65) and, for
+ * gauge_mode >= 0, EMDOFManager::applyTreeGauge (:448-495) with TreeGauge::build
+ * (src/fe_em/tree_gauge.cpp:37-212). */
+int emg_dof_build(emg_mesh mesh, int32_t gauge_mode, emg_dofmap* out);
+int emg_dofmap_info(emg_dofmap map, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs);
+/* l2g: 6*n_tets Local2Global::indices (-1 = constrained or tree edge);
+ * edge_dof: n_edges (equation index of each global edge or -1). */
+int emg_dofmap_export(emg_dofmap map, int32_t* l2g, int32_t* edge_dof);
+/* TreeGauge::mapReducedSolutionToFull (src/fe_em/tree_gauge.cpp:261-290):
+ * full[e] = reduced[edge_dof[e]] or 0. */
+int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full);
+void emg_dofmap_destroy(emg_dofmap map);
+
+/* ---- EMAssembly::assemble on the GPU (src/numeric/em_assembly.cpp:144-420)
+ * A system owns the device copy of the geometry and DOF map, the CSR pattern
+ * (merged, rows sorted: what SparseConverter::to_eigen yields), the stiffness
+ * values K, optional mass values M and the source vector F.
+ * Geometry arrays: xyz 3*n_nodes, tets 4*n_tets, material n_tets (NULL = 0),
+ * l2g 6*n_tets; n_dofs <= 0 means max index + 1 (em_assembly.cpp:190-215).
+ * emg_system_create reads host arrays; emg_system_create_device reads device
+ * arrays (resident inputs) and copies nothing back.  Both build the pattern
+ * on the device. */
+int emg_system_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
+                      const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
+                      emg_system* out);
+int emg_system_create_device(int64_t n_nodes, const double* xyz_d, int64_t n_tets,
+                             const int32_t* tets_d, const int32_t* material_d,
+                             const int32_t* l2g_d, int64_t n_dofs, void* stream, emg_system* out);
+/* Numeric assembly: nu (1/mu) and sigma per material; sources; EMG_FLAG_*. */
+int emg_system_assemble(emg_system sys, const double* nu_per_material,
+                        const double* sigma_per_material, int32_t n_materials,
+                        const emg_source* sources, int32_t n_sources, int32_t flags, void* stream);
+int emg_system_info(emg_system sys, int64_t* n_rows, int64_t* nnz);
+/* Copies to host; any pointer may be NULL.  row_ptr n+1, col/kval/mval nnz, rhs n. */
+int emg_system_export(emg_system sys, int32_t* row_ptr, int32_t* col, double* kval,
+                      double* mval, double* rhs);
+/* Borrowed handles / pointers, valid while the system lives. which: 0 K, 1 M. */
+emg_csr emg_system_matrix(emg_system sys, int32_t which);
+const double* emg_system_rhs_device(emg_system sys);
+void emg_system_destroy(emg_system sys);
+
+/* ---- CsrMatrix<double> + CGSolver::set_matrix (include/numeric/csr_matrix.hpp:31-259,
+ * src/numeric/iterative_solvers.cpp:83-97).  Host CSR, duplicates allowed and
+ * summed, columns in any order (CsrMatrix::build_from_coo keeps duplicates,
+ * SparseConverter::to_eigen sums them).  The device variant expects a merged
+ * CSR with sorted rows. */
+int emg_csr_create(int64_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                   void* stream, emg_csr* out);
+int emg_csr_create_device(int64_t n, int64_t nnz, const int32_t* row_ptr_d,
+                          const int32_t* col_d, const double* val_d, void* stream,
+                          emg_csr* out);
+int emg_csr_info(emg_csr A, int64_t* n, int64_t* nnz);
+void emg_csr_destroy(emg_csr A);
+
+/* ---- CsrMatrix::mat_vec (include/numeric/csr_matrix_impl.hpp:131-147): y_d = A x_d */
+int emg_spmv(emg_csr A, const double* x_d, double* y_d, void* stream);
+
+/* ---- CGSolver::solve (src/numeric/iterative_solvers.cpp:294-503) and
+ * BiCGSTABSolver::solve (:820-1118), same iteration, stopping and failure
+ * rules.  Host b/x or device b_d/x_d; x starts at zero. */
+int emg_cg_solve(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg,
+                 emg_result* out);
+int emg_cg_solve_device(emg_csr A, const double* b_d, double* x_d,
+                        const emg_krylov_config* cfg, void* stream, emg_result* out);
+int emg_bicgstab_solve(emg_csr A, const double* b, double* x, const emg_krylov_config* cfg,
+                       emg_result* out);
+int emg_bicgstab_solve_device(emg_csr A, const double* b_d, double* x_d,
+                              const emg_krylov_config* cfg, void* stream, emg_result* out);
+
+/* Assemble-and-solve convenience for a system: K x = F with the system's own
+ * source vector (CGSolver / BiCGSTABSolver after EMAssembly::assemble).
+ * kind: 0 CG, 1 BiCGSTAB.  x is a host array, or a device array when
+ * x_on_device != 0. */
+int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg, double* x,
+                     int32_t x_on_device, void* stream, emg_result* out);
+
+/* Profiling hook: device time of each CG kernel (SpMV + p.q, update, direction;
+ * ms[0..2]) averaged over `iterations` plain launches from a fresh start with
+ * b = ones, each launch bracketed by CUDA events on `stream`. */
+int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms);
+
+/* Residual monitor of the last solve on A (ConvergenceHistory,
+ * iterative_solvers.cpp:24-60): relative residual after every iteration, up
+ * to cap entries; returns the number written. */
+int emg_last_history(emg_csr A, double* residuals, int32_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMAGDDM_B200_H */

@@ -1,0 +1,156 @@
+"""GPU CG / BiCGSTAB against the oracle and the reference's golden solves.
+
+Tolerances: solutions of converged solves agree with the oracle / reference
+to 1e-8 relative (the solve path's bar); iteration counts agree within a few
+iterations (reduction order differs); failure statuses match exactly."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from emagddm_b200 import _abi, mesh
+from oracle import oracle as O
+from tests.helpers import HostCsr, System, lib, oracle_system, solve
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+FIX = np.load(os.path.join(GOLD, "reference_fixtures.npz"))
+COUNTS = json.load(open(os.path.join(GOLD, "reference_counts.json")))
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("kind,name", [("cg", "cg"), ("bicgstab", "bicgstab")])
+@pytest.mark.parametrize("pc", [0, 1])
+def test_golden_reference_solves(kind, name, pc):
+    A = HostCsr(FIX["solve_n4_row_ptr"].astype(np.int32), FIX["solve_n4_col"], FIX["solve_n4_val"])
+    x, out = solve(A.h, FIX["solve_n4_rhs"], kind, tol=1e-10, max_iter=1000, precond=pc)
+    ref = COUNTS[f"solve_n4_{name}_p{pc}"]
+    assert out.status == ref["status"]
+    if ref["status"] == 0:
+        assert abs(out.iterations - ref["iterations"]) <= max(3, 0.15 * ref["iterations"])
+        assert rel(x, FIX[f"solve_n4_{name}_p{pc}_x"]) <= 1e-8
+    else:  # the reference's half-preconditioned BiCGSTAB stalls; so does this one
+        assert out.iterations == ref["iterations"]
+        assert out.residual_norm == pytest.approx(ref["residual"], rel=1e-6)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+@pytest.mark.parametrize("case", [("small", 8, 1e-10), ("scale", 12, 1e-8), ("scale", 16, 1e-8)])
+def test_assembled_solve_matches_oracle(kind, case):
+    name, n, tol = case
+    m = mesh.plain_small(n) if name == "small" else mesh.plain_scale(n)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    s = System(m, l2g)
+    rp, col, kv, _, rhs = oracle_system(m, l2g)
+    pc = 1 if kind == "cg" else 0
+    x, out = solve(s.matrix(0), rhs, kind, tol=tol, max_iter=20000, precond=pc)
+    fn = O.pcg if kind == "cg" else O.bicgstab
+    xo, st, it, res = fn(rp, col, kv, rhs, tol=tol, max_iter=20000, precond=pc)
+    assert out.status == st == 0
+    assert abs(out.iterations - it) <= max(3, 0.15 * it)
+    # true residual of the GPU solution, computed on the CPU
+    r = rhs - O.spmv(rp, col, kv, x)
+    assert np.linalg.norm(r) / np.linalg.norm(rhs) <= 2 * tol
+    # both solutions approximate the same x*: agree to the solve path's bar
+    xt, _, _, _ = O.pcg(rp, col, kv, rhs, tol=1e-13, max_iter=50000, precond=1)
+    assert rel(x, xt) <= 1e-8 if tol <= 1e-10 else rel(x, xt) <= 1e-6
+
+
+def test_cg_tight_solution_within_1e8_of_oracle():
+    m = mesh.plain_scale(12)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    rp, col, kv, _, rhs = oracle_system(m, l2g)
+    s = System(m, l2g)
+    x, out = solve(s.matrix(0), rhs, "cg", tol=1e-12, max_iter=50000, precond=1)
+    xo, st, it, res = O.pcg(rp, col, kv, rhs, tol=1e-12, max_iter=50000, precond=1)
+    assert out.status == 0 and st == 0
+    assert rel(x, xo) <= 1e-8
+
+
+def test_zero_rhs_and_iteration_limits():
+    m = mesh.plain_small(4)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    s = System(m, l2g)
+    n = int(l2g.max()) + 1
+    x, out = solve(s.matrix(0), np.zeros(n), "cg")
+    assert out.status == 0 and out.iterations == 0 and out.residual_norm == 0.0 and np.all(x == 0)
+    x, out = solve(s.matrix(0), np.zeros(n), "bicgstab")
+    assert out.status == 0 and out.iterations == 0
+    _, _, _, _, rhs = oracle_system(m, l2g)
+    for kind in ("cg", "bicgstab"):
+        x, out = solve(s.matrix(0), rhs, kind, tol=1e-14, max_iter=5)
+        assert out.status == _abi.EMG_MAX_ITER_REACHED and out.iterations == 5
+        x, out = solve(s.matrix(0), rhs, kind, tol=1e-14, max_iter=0)
+        assert out.status == _abi.EMG_MAX_ITER_REACHED and out.iterations == 0
+
+
+def test_breakdown_reports_numerical_error():
+    # a zero matrix: p^T A p = 0 at the first iteration (iterative_solvers.cpp:453-457)
+    n = 50
+    rp = np.arange(n + 1, dtype=np.int32)
+    col = np.arange(n, dtype=np.int32)
+    A = HostCsr(rp, col, np.zeros(n))
+    b = np.ones(n)
+    x, out = solve(A.h, b, "cg")
+    xo, st, it, res = O.pcg(rp.astype(np.int64), col, np.zeros(n), b)
+    assert out.status == st == _abi.EMG_NUMERICAL_ERROR
+    assert out.iterations == it == 1
+    x, out = solve(A.h, b, "bicgstab")
+    xo, st, it, res = O.bicgstab(rp.astype(np.int64), col, np.zeros(n), b)
+    assert out.status == st == _abi.EMG_NUMERICAL_ERROR and out.iterations == it
+
+
+def test_unmerged_host_csr_is_summed():
+    # the reference's CsrMatrix keeps duplicate (row, col) entries; the
+    # solver sees them summed (SparseConverter::to_eigen)
+    m = mesh.plain_small(4)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    rp, col, kv, _, rhs = oracle_system(m, l2g)
+    n = rp.size - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    rows2 = np.concatenate([rows, rows])
+    cols2 = np.concatenate([col, col])
+    vals2 = np.concatenate([0.25 * kv, 0.75 * kv])
+    order = np.lexsort((cols2[::-1], rows2))  # unsorted columns inside rows
+    rows2, cols2, vals2 = rows2[order], cols2[order], vals2[order]
+    rp2 = np.concatenate([[0], np.cumsum(np.bincount(rows2, minlength=n))]).astype(np.int32)
+    A = HostCsr(rp2, cols2, vals2)
+    B = HostCsr(rp.astype(np.int32), col, kv)
+    xa, oa = solve(A.h, rhs, "cg", tol=1e-10)
+    xb, ob = solve(B.h, rhs, "cg", tol=1e-10)
+    assert oa.status == ob.status == 0
+    assert rel(xa, xb) <= 1e-12
+
+
+def test_spmv_matches_oracle():
+    import torch
+    m = mesh.plain_scale(10)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    rp, col, kv, _, _ = oracle_system(m, l2g)
+    A = HostCsr(rp.astype(np.int32), col, kv)
+    x = np.random.default_rng(0).normal(size=rp.size - 1)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    import ctypes as C
+    _abi.check(lib().emg_spmv(A.h, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), None), "spmv")
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy()
+    yo = O.spmv(rp, col, kv, x)
+    assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
+
+
+def test_history_records_every_iteration():
+    import ctypes as C
+    m = mesh.plain_small(6)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    s = System(m, l2g)
+    _, _, _, _, rhs = oracle_system(m, l2g)
+    x, out = solve(s.matrix(0), rhs, "cg", tol=1e-9)
+    h = np.empty(out.iterations)
+    k = lib().emg_last_history(s.matrix(0), _abi.ptr(h), out.iterations)
+    assert k == out.iterations
+    assert h[-1] == out.residual_norm and h[-1] < 1e-9 <= h[-2]
