@@ -233,8 +233,34 @@ def run_ours(args, rank, world, local_rank):
                                           C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h)), "create")
     _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp), "asm")
     kt = (C.c_double * 3)()
-    _abi.check(L.emg_cg_kernel_times(L.emg_system_matrix(h, 0), 50, sp, kt), "kernel times")
+    Kh = L.emg_system_matrix(h, 0)
+    _abi.check(L.emg_cg_kernel_times(Kh, 50, sp, kt), "kernel times")
+    slots, slices = C.c_int64(), C.c_int64()
+    L.emg_csr_solver_format(Kh, C.byref(slots), C.byref(slices))
     L.emg_system_destroy(h)
+    # one instrumented step: host wall time of each phase (synchronized)
+    phases = {}
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    h = C.c_void_p()
+    L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                               C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                               C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h))
+    torch.cuda.synchronize(dev)
+    phases["create_symbolic"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp)
+    torch.cuda.synchronize(dev)
+    phases["assemble"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    out = _abi.Result()
+    L.emg_system_solve(h, 0, C.byref(cfg), C.c_void_p(d_x.data_ptr()), 1, sp, C.byref(out))
+    torch.cuda.synchronize(dev)
+    phases["solve"] = (time.perf_counter() - t) * 1e3
+    phases["solve_device"] = out.solve_time_ms
+    t = time.perf_counter()
+    L.emg_system_destroy(h)
+    phases["destroy"] = (time.perf_counter() - t) * 1e3
     nnz = info["nnz"]
     spmv_bytes = 12 * nnz + 4 * (n_dofs + 1) + 8 * n_dofs + 8 * n_dofs
     peak, peak_kind = measured_peak()
@@ -258,7 +284,9 @@ def run_ours(args, rank, world, local_rank):
                    "setup_dof_ms": setup_dof_ms,
                    "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]},
                    "cg_iteration_ms_kernels": it_ms,
-                   "solve_ms": info["solve_ms"]},
+                   "solve_ms": info["solve_ms"], "phase_ms": phases,
+                   "solver_format": {"kind": "SELL-32-sigma4096", "slots": slots.value,
+                                     "padding": slots.value / nnz - 1.0}},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h_x.nbytes), "ms_per_step": total_e2e / args.steps,

@@ -446,6 +446,13 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
   });
 }
 
+int emg_csr_solver_format(emg_csr A, int64_t* slots, int64_t* slices) {
+  if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
+  if (slots) *slots = emg::sell_slots(*A->csr);
+  if (slices) *slices = emg::sell_slices(*A->csr);
+  return EMG_SUCCESS;
+}
+
 int emg_last_history(emg_csr A, double* residuals, int32_t cap) {
   if (!A || !A->csr || !residuals || cap <= 0) return 0;
   int n = emg::csr_history(*A->csr, residuals, cap);

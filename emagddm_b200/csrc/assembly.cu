@@ -536,6 +536,8 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
   a.kval = s.K.val; a.mval = mass ? s.M.val : nullptr; a.rhs = s.rhs; a.err = s.err;
   k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
   EMG_CK(cudaGetLastError());
+  ++s.K.version;
+  if (mass) ++s.M.version;
   int32_t herr = 0;
   EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   EMG_CK(cudaFreeAsync(mat, st));

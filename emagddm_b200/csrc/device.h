@@ -22,8 +22,11 @@ void set_error(const std::string& msg);
   } while (0)
 
 struct KrylovWorkspace;
+struct Sell;
 
 // Device CSR matrix (int32 row_ptr / col, fp64 values, rows sorted, merged).
+// `version` changes whenever the values change (re-assembly), so derived
+// solver formats know when to refresh.
 struct DevCsr {
   int64_t n = 0;
   int64_t nnz = 0;
@@ -32,7 +35,9 @@ struct DevCsr {
   double* val = nullptr;
   bool owns_pattern = true;
   bool owns_values = true;
+  uint64_t version = 0;
   KrylovWorkspace* ws = nullptr;
+  Sell* sell = nullptr;
   ~DevCsr();
 };
 
@@ -74,5 +79,7 @@ int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_confi
 int csr_history(DevCsr& A, double* out, int32_t cap);
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
 void free_workspace(KrylovWorkspace* ws);
+int64_t sell_slots(DevCsr& A);
+int64_t sell_slices(DevCsr& A);
 
 }  // namespace emg

@@ -1,8 +1,16 @@
-// krylov.cu -- FP64 CSR SpMV and the Jacobi-preconditioned CG / BiCGSTAB
-// solvers of the reference (src/numeric/iterative_solvers.cpp:343-503 and
-// :869-1118), with the same iteration, stopping and failure rules.
+// krylov.cu -- FP64 sparse matrix-vector product and the Jacobi-preconditioned
+// CG / BiCGSTAB solvers of the reference (src/numeric/iterative_solvers.cpp:
+// 343-503 and :869-1118), with the same iteration, stopping and failure rules.
 //
-// Structure of one iteration (CG):
+// Matrix format inside the solvers: SELL-32-sigma.  Rows are sorted by length
+// (descending) inside windows of 4096 rows, cut into slices of 32 rows, and
+// each slice is stored column-major and padded to its longest row, so one warp
+// reads a slice with 256-byte coalesced loads and every lane has a whole row
+// (no shuffles, many independent loads in flight).  The solvers run in the
+// permuted numbering (P A P^T, P b): all vector kernels stay contiguous; b is
+// permuted on entry and x on exit.  The CSR handed in stays the exported form.
+//
+// One CG iteration:
 //   k_cg_spmv_dot   q = A p and p.q        (last block: alpha / breakdown)
 //   k_cg_update     x += a p, r -= a q, z = D^-1 r, r.z and r.r
 //                   (last block: residual, convergence, divergence, beta)
@@ -14,6 +22,7 @@
 // finished solve returns at once; the host polls the state between chunks.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -41,6 +50,17 @@ struct SolverState {
   int32_t pad;
 };
 
+// SELL-32-sigma copy of a DevCsr in the permuted numbering.
+struct Sell {
+  int64_t n = 0, nslices = 0, slots = 0;
+  int32_t* perm = nullptr;       // new row -> old row
+  int64_t* slice_ptr = nullptr;  // nslices + 1 slot offsets (multiples of 32)
+  int32_t* col = nullptr;        // permuted column of every slot
+  int32_t* src = nullptr;        // CSR index of every slot, -1 = padding
+  double* val = nullptr;
+  uint64_t version = ~uint64_t(0);
+};
+
 struct KrylovWorkspace {
   int64_t n = 0;
   int grid = 0;
@@ -61,8 +81,9 @@ struct KrylovWorkspace {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kLanes = 8;      // lanes per CSR row in the SpMV
-constexpr int kChunk = 16;     // iterations per graph launch
+constexpr int kChunk = 16;      // iterations per graph launch
+constexpr int kSliceRows = 32;  // SELL slice height = warp width
+constexpr int kWindow = 4096;   // sigma: rows sorted by length inside a window
 
 __device__ __forceinline__ int64_t gtid() {
   return static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -71,37 +92,42 @@ __device__ __forceinline__ int64_t gstride() {
   return static_cast<int64_t>(gridDim.x) * blockDim.x;
 }
 
-// Rows handled by this thread's lane group; y = A x for those rows.  Returns
-// this thread's share of sum_i w[i] * y[i] (only the group leader
-// contributes), w may be null.
-template <int L>
-__device__ __forceinline__ double spmv_rows(int64_t n, const int32_t* __restrict__ rp,
-                                            const int32_t* __restrict__ col,
-                                            const double* __restrict__ val,
-                                            const double* __restrict__ x, double* __restrict__ y,
-                                            const double* __restrict__ w) {
-  constexpr int G = kWarp / L;  // rows per warp step
+// Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
+// out(row, y_row) for every real row.  Entries of a row are summed in CSR
+// order, four loads in flight per lane at a time.
+template <class Out>
+__device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
   const int lane = threadIdx.x & 31;
-  const int sub = lane & (L - 1);
-  const int64_t warp = gtid() >> 5;
-  const int64_t nwarps = gstride() >> 5;
+  const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   const uint64_t pol = evict_first_policy();
-  double dot = 0.0;
-  for (int64_t base = warp * G; base < n; base += nwarps * G) {
-    const int64_t row = base + lane / L;
+  const int64_t* __restrict__ sp = A.slice_ptr;
+  const int32_t* __restrict__ col = A.col;
+  const double* __restrict__ val = A.val;
+  for (int64_t s = warp; s < A.nslices; s += nwarps) {
+    const int64_t b0 = sp[s], b1 = sp[s + 1];
+    const int len = static_cast<int>((b1 - b0) >> 5);
+    const int64_t base = b0 + lane;
     double sum = 0.0;
-    if (row < n) {
-      const int32_t e = rp[row + 1];
-      for (int32_t k = rp[row] + sub; k < e; k += L) sum += ld_stream(val + k, pol) * x[ld_stream(col + k, pol)];
+    int j = 0;
+    for (; j + 4 <= len; j += 4) {
+      const int64_t k = base + 32 * j;
+      const int c0 = ld_stream(col + k, pol), c1 = ld_stream(col + k + 32, pol);
+      const int c2 = ld_stream(col + k + 64, pol), c3 = ld_stream(col + k + 96, pol);
+      const double v0 = ld_stream(val + k, pol), v1 = ld_stream(val + k + 32, pol);
+      const double v2 = ld_stream(val + k + 64, pol), v3 = ld_stream(val + k + 96, pol);
+      const double x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
+      sum += v0 * x0;
+      sum += v1 * x1;
+      sum += v2 * x2;
+      sum += v3 * x3;
     }
-#pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (row < n && sub == 0) {
-      y[row] = sum;
-      if (w) dot += w[row] * sum;
+    for (; j < len; ++j) {
+      const int64_t k = base + 32 * j;
+      sum += ld_stream(val + k, pol) * x[ld_stream(col + k, pol)];
     }
+    const int64_t row = s * kSliceRows + lane;
+    if (row < A.n) out(row, sum);
   }
-  return dot;
 }
 
 // One partial per block; true in the block that finished last (all partials
@@ -131,43 +157,98 @@ __device__ __forceinline__ bool reduce_partials(const double (&vals)[kVals], dou
   return true;
 }
 
+// ------------------------------------------------------------ SELL build ----
+// Warp per slice: column index (permuted) and CSR source of every slot.
+__global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restrict__ sp,
+                            const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
+                            const int32_t* __restrict__ rp, const int32_t* __restrict__ ccol,
+                            int32_t* __restrict__ col, int32_t* __restrict__ src) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+  for (int64_t s = warp; s < nslices; s += nwarps) {
+    const int64_t b0 = sp[s];
+    const int len = static_cast<int>((sp[s + 1] - b0) >> 5);
+    const int64_t row = s * kSliceRows + lane;
+    int32_t a = 0, rl = 0;
+    const int32_t self = static_cast<int32_t>(row < n ? row : n - 1);
+    if (row < n) {
+      const int32_t old = perm[row];
+      a = rp[old];
+      rl = rp[old + 1] - a;
+    }
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = b0 + 32 * j + lane;
+      if (j < rl) {
+        col[k] = iperm[ccol[a + j]];
+        src[k] = a + j;
+      } else {
+        col[k] = self;  // padding reads a valid entry and multiplies it by 0
+        src[k] = -1;
+      }
+    }
+  }
+}
+
+__global__ void k_sell_values(int64_t slots, const int32_t* __restrict__ src,
+                              const double* __restrict__ cval, double* __restrict__ val) {
+  for (int64_t i = gtid(); i < slots; i += gstride()) {
+    const int32_t s = src[i];
+    val[i] = s >= 0 ? cval[s] : 0.0;
+  }
+}
+
+__global__ void k_invert_perm(int64_t n, const int32_t* __restrict__ perm, int32_t* __restrict__ iperm) {
+  for (int64_t i = gtid(); i < n; i += gstride()) iperm[perm[i]] = static_cast<int32_t>(i);
+}
+
 // ------------------------------------------------------------- Jacobi ----
 // CGSolver::setup_preconditioner (iterative_solvers.cpp:261-292):
 // 1/A(i,i), or 1 where |A(i,i)| <= 1e-15.  precond == 0 gives D^-1 = I.
+// Written in the permuted numbering.
 __global__ void k_jacobi(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                         const double* __restrict__ val, int precond, double* __restrict__ dinv) {
+                         const double* __restrict__ val, const int32_t* __restrict__ perm,
+                         int precond, double* __restrict__ dinv) {
   for (int64_t i = gtid(); i < n; i += gstride()) {
     double d = 1.0;
     if (precond) {
-      int32_t lo = rp[i], hi = rp[i + 1];
+      const int32_t o = perm[i];
+      int32_t lo = rp[o], hi = rp[o + 1];
       while (lo < hi) {
         int32_t mid = (lo + hi) >> 1;
-        if (col[mid] < i) lo = mid + 1; else hi = mid;
+        if (col[mid] < o) lo = mid + 1; else hi = mid;
       }
-      double a = (lo < rp[i + 1] && col[lo] == i) ? val[lo] : 0.0;
+      const double a = (lo < rp[o + 1] && col[lo] == o) ? val[lo] : 0.0;
       d = fabs(a) > 1e-15 ? 1.0 / a : 1.0;
     }
     dinv[i] = d;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int32_t* __restrict__ rp,
-                                                   const int32_t* __restrict__ col,
-                                                   const double* __restrict__ val,
-                                                   const double* __restrict__ x,
+__global__ void k_gather(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ in,
+                         double* __restrict__ out) {
+  for (int64_t i = gtid(); i < n; i += gstride()) out[i] = in[perm[i]];
+}
+
+__global__ void k_scatter(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ in,
+                          double* __restrict__ out) {
+  for (int64_t i = gtid(); i < n; i += gstride()) out[perm[i]] = in[i];
+}
+
+__global__ void __launch_bounds__(kThreads) k_spmv(Sell A, const double* __restrict__ x,
                                                    double* __restrict__ y) {
-  spmv_rows<kLanes>(n, rp, col, val, x, y, nullptr);
+  sell_rows(A, x, [&](int64_t row, double s) { y[row] = s; });
 }
 
 // ----------------------------------------------------------------- CG ----
 __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* __restrict__ b,
+                                                      const int32_t* __restrict__ perm,
                                                       const double* __restrict__ dinv,
                                                       double* __restrict__ x, double* __restrict__ r,
                                                       double* __restrict__ z, double* __restrict__ p,
                                                       double* partial, SolverState* st) {
   double acc[2] = {0.0, 0.0};
   for (int64_t i = gtid(); i < n; i += gstride()) {
-    const double bi = b[i], zi = dinv[i] * bi;
+    const double bi = b[perm[i]], zi = dinv[i] * bi;
     x[i] = 0.0; r[i] = bi; z[i] = zi; p[i] = zi;
     acc[0] += bi * bi;
     acc[1] += bi * zi;
@@ -191,14 +272,16 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* _
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(int64_t n, const int32_t* __restrict__ rp,
-                                                          const int32_t* __restrict__ col,
-                                                          const double* __restrict__ val,
-                                                          const double* __restrict__ p,
+__global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(Sell A, const double* __restrict__ p,
                                                           double* __restrict__ q, double* partial,
                                                           SolverState* st) {
   if (st->done) return;
-  double acc[1] = {spmv_rows<kLanes>(n, rp, col, val, p, q, p)};
+  double dot = 0.0;
+  sell_rows(A, p, [&](int64_t row, double s) {
+    q[row] = s;
+    dot += p[row] * s;
+  });
+  double acc[1] = {dot};
   double tot[1];
   if (!reduce_partials<1>(acc, partial, st, tot)) return;
   if (threadIdx.x == 0) {
@@ -262,8 +345,8 @@ __global__ void __launch_bounds__(kThreads) k_cg_direction(int64_t n, double* __
 }
 
 // ----------------------------------------------------------- BiCGSTAB ----
-// Decide the start of iteration `next` (= it + 1) from rho_n = r.r_hat:
-// max-iteration stop, rho breakdown, else beta and rho.
+// Start of iteration `next` (= it + 1) from rho_n = r.r_hat: max-iteration
+// stop, rho breakdown, else beta and rho.
 __device__ void bi_next_iteration(SolverState* st, int next, double rho_n) {
   if (next > st->max_iter) {
     st->status = EMG_MAX_ITER_REACHED; st->iter = st->max_iter; st->done = 1;
@@ -277,13 +360,14 @@ __device__ void bi_next_iteration(SolverState* st, int next, double rho_n) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_bi_init(int64_t n, const double* __restrict__ b,
+                                                      const int32_t* __restrict__ perm,
                                                       double* __restrict__ x, double* __restrict__ r,
                                                       double* __restrict__ rh, double* __restrict__ p,
                                                       double* __restrict__ v, double* partial,
                                                       SolverState* st) {
   double acc[1] = {0.0};
   for (int64_t i = gtid(); i < n; i += gstride()) {
-    const double bi = b[i];
+    const double bi = b[perm[i]];
     x[i] = 0.0; r[i] = bi; rh[i] = bi; p[i] = bi; v[i] = 0.0;
     acc[0] += bi * bi;
   }
@@ -317,15 +401,17 @@ __global__ void __launch_bounds__(kThreads) k_bi_p(int64_t n, double* __restrict
 }
 
 // v = A p, r_hat . v -> alpha
-__global__ void __launch_bounds__(kThreads) k_bi_v(int64_t n, const int32_t* __restrict__ rp,
-                                                   const int32_t* __restrict__ col,
-                                                   const double* __restrict__ val,
-                                                   const double* __restrict__ p,
+__global__ void __launch_bounds__(kThreads) k_bi_v(Sell A, const double* __restrict__ p,
                                                    double* __restrict__ v,
                                                    const double* __restrict__ rh, double* partial,
                                                    SolverState* st) {
   if (st->done) return;
-  double acc[1] = {spmv_rows<kLanes>(n, rp, col, val, p, v, rh)};
+  double dot = 0.0;
+  sell_rows(A, p, [&](int64_t row, double s) {
+    v[row] = s;
+    dot += rh[row] * s;
+  });
+  double acc[1] = {dot};
   double tot[1];
   if (!reduce_partials<1>(acc, partial, st, tot)) return;
   if (threadIdx.x == 0) {
@@ -364,37 +450,16 @@ __global__ void __launch_bounds__(kThreads) k_bi_s(int64_t n, const double* __re
 }
 
 // t = A z, t.t and z.t -> omega
-__global__ void __launch_bounds__(kThreads) k_bi_t(int64_t n, const int32_t* __restrict__ rp,
-                                                   const int32_t* __restrict__ col,
-                                                   const double* __restrict__ val,
-                                                   const double* __restrict__ z,
+__global__ void __launch_bounds__(kThreads) k_bi_t(Sell A, const double* __restrict__ z,
                                                    double* __restrict__ t, double* partial,
                                                    SolverState* st) {
   if (st->done || st->early) return;
-  const int lane = threadIdx.x & 31;
-  (void)lane;
   double tt = 0.0, zt = 0.0;
-  {
-    constexpr int L = kLanes, G = kWarp / L;
-    const int sub = threadIdx.x & (L - 1);
-    const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
-    const uint64_t pol = evict_first_policy();
-    for (int64_t base = warp * G; base < n; base += nwarps * G) {
-      const int64_t row = base + (threadIdx.x & 31) / L;
-      double sum = 0.0;
-      if (row < n) {
-        const int32_t e = rp[row + 1];
-        for (int32_t k = rp[row] + sub; k < e; k += L) sum += ld_stream(val + k, pol) * z[ld_stream(col + k, pol)];
-      }
-#pragma unroll
-      for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-      if (row < n && sub == 0) {
-        t[row] = sum;
-        tt += sum * sum;
-        zt += z[row] * sum;
-      }
-    }
-  }
+  sell_rows(A, z, [&](int64_t row, double s) {
+    t[row] = s;
+    tt += s * s;
+    zt += z[row] * s;
+  });
   double acc[2] = {tt, zt};
   double tot[2];
   if (!reduce_partials<2>(acc, partial, st, tot)) return;
@@ -420,8 +485,8 @@ __global__ void __launch_bounds__(kThreads) k_bi_x(int64_t n, double* __restrict
       const int it = st->iter;
       if (it - 1 < hist_cap) hist[it - 1] = st->res;
     }
-    // `done` is raised by the host-visible ticket below so that every block
-    // has read `early` before it changes.
+    // `done` is raised by the last block so that every block has read
+    // `early` before it changes.
     double acc0[1] = {0.0}, tot0[1];
     if (reduce_partials<1>(acc0, partial, st, tot0) && threadIdx.x == 0) st->done = 1;
     return;
@@ -457,12 +522,82 @@ __global__ void __launch_bounds__(kThreads) k_bi_x(int64_t n, double* __restrict
 int grid_size() {
   static int g = 0;
   if (!g) {
-    int dev = 0, sms = 148, per = 4;
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    g = sms * per;
+    g = sms * 8;  // 8 blocks of 256 threads per SM: 64 resident warps
   }
   return g;
+}
+
+// Host: permutation sorting rows by length inside windows (stable), slice
+// offsets; device: slots.
+int build_sell(DevCsr& A, cudaStream_t st) {
+  if (!A.sell) A.sell = new Sell();
+  Sell& S = *A.sell;
+  const int64_t n = A.n;
+  S.n = n;
+  std::vector<int32_t> rp(n + 1);
+  EMG_CK(cudaMemcpyAsync(rp.data(), A.row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  std::vector<int32_t> perm(n);
+  int32_t maxlen = 0;
+  for (int64_t i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
+  std::vector<int64_t> cnt(static_cast<size_t>(maxlen) + 2);
+  for (int64_t w0 = 0; w0 < n; w0 += kWindow) {
+    const int64_t w1 = std::min<int64_t>(n, w0 + kWindow);
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (int64_t i = w0; i < w1; ++i) cnt[maxlen - (rp[i + 1] - rp[i]) + 1]++;  // descending
+    for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
+    for (int64_t i = w0; i < w1; ++i) perm[w0 + cnt[maxlen - (rp[i + 1] - rp[i])]++] = static_cast<int32_t>(i);
+  }
+  S.nslices = (n + kSliceRows - 1) / kSliceRows;
+  std::vector<int64_t> sp(S.nslices + 1, 0);
+  for (int64_t s = 0; s < S.nslices; ++s) {
+    int32_t len = 0;
+    for (int64_t r = s * kSliceRows; r < std::min<int64_t>(n, (s + 1) * kSliceRows); ++r)
+      len = std::max(len, rp[perm[r] + 1] - rp[perm[r]]);
+    sp[s + 1] = sp[s] + static_cast<int64_t>(kSliceRows) * len;
+  }
+  S.slots = sp[S.nslices];
+  if (S.slots >= (int64_t(1) << 31)) { set_error("matrix too large for the solver format"); return EMG_INVALID_INPUT; }
+  int32_t* iperm = nullptr;
+  EMG_CK(cudaMalloc(&S.perm, sizeof(int32_t) * n));
+  EMG_CK(cudaMalloc(&iperm, sizeof(int32_t) * n));
+  EMG_CK(cudaMalloc(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1)));
+  EMG_CK(cudaMalloc(&S.col, sizeof(int32_t) * std::max<int64_t>(S.slots, 1)));
+  EMG_CK(cudaMalloc(&S.src, sizeof(int32_t) * std::max<int64_t>(S.slots, 1)));
+  EMG_CK(cudaMalloc(&S.val, sizeof(double) * std::max<int64_t>(S.slots, 1)));
+  EMG_CK(cudaMemcpyAsync(S.perm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  EMG_CK(cudaMemcpyAsync(S.slice_ptr, sp.data(), sizeof(int64_t) * (S.nslices + 1), cudaMemcpyHostToDevice, st));
+  const int g = grid_size();
+  k_invert_perm<<<g, kThreads, 0, st>>>(n, S.perm, iperm);
+  k_sell_fill<<<g, kThreads, 0, st>>>(n, S.nslices, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col, S.src);
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaStreamSynchronize(st));
+  cudaFree(iperm);
+  S.version = ~uint64_t(0);
+  return EMG_SUCCESS;
+}
+
+int ensure_sell(DevCsr& A, cudaStream_t st) {
+  if (!A.sell) {
+    int rc = build_sell(A, st);
+    if (rc) return rc;
+  }
+  Sell& S = *A.sell;
+  if (S.version != A.version) {
+    k_sell_values<<<grid_size(), kThreads, 0, st>>>(S.slots, S.src, A.val, S.val);
+    EMG_CK(cudaGetLastError());
+    S.version = A.version;
+  }
+  return EMG_SUCCESS;
+}
+
+void free_sell(Sell* s) {
+  if (!s) return;
+  cudaFree(s->perm); cudaFree(s->slice_ptr); cudaFree(s->col); cudaFree(s->src); cudaFree(s->val);
+  delete s;
 }
 
 int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter) {
@@ -507,20 +642,21 @@ int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter) {
 
 int capture_chunk(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
   KrylovWorkspace& w = *A.ws;
+  const Sell S = *A.sell;
   const int g = w.grid;
   cudaGraph_t graph = nullptr;
   EMG_CK(cudaStreamBeginCapture(w.cap, cudaStreamCaptureModeThreadLocal));
   for (int c = 0; c < kChunk; ++c) {
     if (!bicg) {
-      k_cg_spmv_dot<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.q, w.partial, w.state);
+      k_cg_spmv_dot<<<g, kThreads, 0, w.cap>>>(S, w.p, w.q, w.partial, w.state);
       k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                              w.hist, w.hist_cap);
       k_cg_direction<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
     } else {
       k_bi_p<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
-      k_bi_v<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.v, w.rh, w.partial, w.state);
+      k_bi_v<<<g, kThreads, 0, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
       k_bi_s<<<g, kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
-      k_bi_t<<<g, kThreads, 0, w.cap>>>(A.n, A.row_ptr, A.col, A.val, w.z, w.t, w.partial, w.state);
+      k_bi_t<<<g, kThreads, 0, w.cap>>>(S, w.z, w.t, w.partial, w.state);
       k_bi_x<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
                                         w.hist, w.hist_cap);
     }
@@ -544,11 +680,14 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   if (rc) { res->status = rc; return rc; }
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
+  rc = ensure_sell(A, st);
+  if (rc) { res->status = rc; return rc; }
   cudaGraphExec_t* exec = bicg ? &w.bi_exec : &w.cg_exec;
   if (!*exec) {
     rc = capture_chunk(A, bicg, exec);
     if (rc) { res->status = rc; return rc; }
   }
+  const Sell& S = *A.sell;
   SolverState init;
   std::memset(&init, 0, sizeof(init));
   init.tol = cfg.tolerance;
@@ -557,11 +696,11 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   EMG_CK(cudaEventRecord(w.ev0, st));
   EMG_CK(cudaMemcpyAsync(w.state, w.state_h, sizeof(SolverState), cudaMemcpyHostToDevice, st));
   const int g = w.grid;
-  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, cfg.preconditioner, w.dinv);
+  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, S.perm, cfg.preconditioner, w.dinv);
   if (!bicg)
-    k_cg_init<<<g, kThreads, 0, st>>>(A.n, b, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
+    k_cg_init<<<g, kThreads, 0, st>>>(A.n, b, S.perm, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
   else
-    k_bi_init<<<g, kThreads, 0, st>>>(A.n, b, w.x, w.r, w.rh, w.p, w.v, w.partial, w.state);
+    k_bi_init<<<g, kThreads, 0, st>>>(A.n, b, S.perm, w.x, w.r, w.rh, w.p, w.v, w.partial, w.state);
   EMG_CK(cudaGetLastError());
   // Graph chunks until the device state says done; bounded by max_iter.
   const int64_t max_chunks = (static_cast<int64_t>(max_iter > 0 ? max_iter : 0) + kChunk - 1) / kChunk + 1;
@@ -572,8 +711,8 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
     if (w.state_h->done) { done = true; break; }
     EMG_CK(cudaGraphLaunch(*exec, st));
   }
+  k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, w.x, x);
   EMG_CK(cudaEventRecord(w.ev1, st));
-  EMG_CK(cudaMemcpyAsync(x, w.x, sizeof(double) * A.n, cudaMemcpyDeviceToDevice, st));
   EMG_CK(cudaStreamSynchronize(st));
   float ms = 0.0f;
   EMG_CK(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
@@ -596,7 +735,16 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
 
 int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
   if (!x || !y) { set_error("null vector"); return EMG_INVALID_INPUT; }
-  k_spmv<<<grid_size(), kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, x, y);
+  int rc = ensure_ws(A, false, 1);
+  if (rc) return rc;
+  rc = ensure_sell(A, st);
+  if (rc) return rc;
+  const int g = grid_size();
+  const Sell& S = *A.sell;
+  // the workspace vectors hold the permuted operands
+  k_gather<<<g, kThreads, 0, st>>>(A.n, S.perm, x, A.ws->p);
+  k_spmv<<<g, kThreads, 0, st>>>(S, A.ws->p, A.ws->q);
+  k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, A.ws->q, y);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
 }
@@ -617,6 +765,9 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
   if (rc) return rc;
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
+  rc = ensure_sell(A, st);
+  if (rc) return rc;
+  const Sell S = *A.sell;
   const int g = w.grid;
   double* ones = nullptr;
   EMG_CK(cudaMallocAsync(&ones, sizeof(double) * A.n, st));
@@ -628,13 +779,13 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
   init.max_iter = 1 << 30;
   *w.state_h = init;
   EMG_CK(cudaMemcpyAsync(w.state, w.state_h, sizeof(SolverState), cudaMemcpyHostToDevice, st));
-  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, 1, w.dinv);
-  k_cg_init<<<g, kThreads, 0, st>>>(A.n, ones, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
+  k_jacobi<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, S.perm, 1, w.dinv);
+  k_cg_init<<<g, kThreads, 0, st>>>(A.n, ones, S.perm, w.dinv, w.x, w.r, w.z, w.p, w.partial, w.state);
   std::vector<cudaEvent_t> ev(4 * iterations);
   for (auto& e : ev) EMG_CK(cudaEventCreate(&e));
   for (int i = 0; i < iterations; ++i) {
     EMG_CK(cudaEventRecord(ev[4 * i], st));
-    k_cg_spmv_dot<<<g, kThreads, 0, st>>>(A.n, A.row_ptr, A.col, A.val, w.p, w.q, w.partial, w.state);
+    k_cg_spmv_dot<<<g, kThreads, 0, st>>>(S, w.p, w.q, w.partial, w.state);
     EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
     k_cg_update<<<g, kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                         w.hist, w.hist_cap);
@@ -671,6 +822,9 @@ int csr_history(DevCsr& A, double* out, int32_t cap) {
   return n;
 }
 
+int64_t sell_slots(DevCsr& A) { return A.sell ? A.sell->slots : -1; }
+int64_t sell_slices(DevCsr& A) { return A.sell ? A.sell->nslices : -1; }
+
 void free_workspace(KrylovWorkspace* w) {
   if (!w) return;
   if (w->cg_exec) cudaGraphExecDestroy(w->cg_exec);
@@ -688,6 +842,7 @@ void free_workspace(KrylovWorkspace* w) {
 // Pattern and values come from the stream-ordered pool (cudaMallocAsync).
 DevCsr::~DevCsr() {
   free_workspace(ws);
+  free_sell(sell);
   if (owns_pattern) {
     if (row_ptr) cudaFreeAsync(row_ptr, 0);
     if (col) cudaFreeAsync(col, 0);

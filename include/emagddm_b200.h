@@ -190,6 +190,11 @@ int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg,
  * b = ones, each launch bracketed by CUDA events on `stream`. */
 int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms);
 
+/* Solver storage of A (SELL-32-sigma copy built at the first solve or SpMV):
+ * stored slots including padding and number of 32-row slices; -1 before the
+ * first solve. */
+int emg_csr_solver_format(emg_csr A, int64_t* slots, int64_t* slices);
+
 /* Residual monitor of the last solve on A (ConvergenceHistory,
  * iterative_solvers.cpp:24-60): relative residual after every iteration, up
  * to cap entries; returns the number written. */
