@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="hex grid size (64 = the quoted workload)")
     ap.add_argument("--cpu-iters", type=int, default=20, help="iterations in the CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline (profiling runs)")
     return ap.parse_args()
 
 
@@ -297,7 +299,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": spmv_bytes},
     }
-    if rank == 0:
+    if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, m, l2g, n_dofs, iters)
     return line
 

@@ -47,6 +47,8 @@ struct SolverState {
   int32_t early;  // BiCGSTAB early exit on ||s|| pending
   int32_t dcount; // BiCGSTAB growth counter
   uint32_t ticket;
+  int32_t loops;       // device-loop bodies executed in this solve
+  int32_t loop_limit;  // hard bound on loop bodies (stops the loop without `done`)
   int32_t pad;
 };
 
@@ -73,15 +75,19 @@ struct KrylovWorkspace {
   SolverState* state = nullptr;
   SolverState* state_h = nullptr;  // pinned
   cudaStream_t cap = nullptr;
-  cudaGraphExec_t cg_exec = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;  // chunk of kChunk iterations (host-polled)
   cudaGraphExec_t bi_exec = nullptr;
+  cudaGraphExec_t cg_loop = nullptr;  // whole solve as a device while-loop
+  cudaGraphExec_t bi_loop = nullptr;
+  bool loop_unavailable = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kChunk = 16;      // iterations per graph launch
+constexpr int kChunk = 16;      // iterations per host-polled graph launch
+constexpr int kBody = 4;        // iterations per body of the device while-loop
 constexpr int kSliceRows = 32;  // SELL slice height = warp width
 constexpr int kWindow = 4096;   // sigma: rows sorted by length inside a window
 
@@ -519,6 +525,17 @@ __global__ void __launch_bounds__(kThreads) k_bi_x(int64_t n, double* __restrict
   }
 }
 
+// Last node of every while-loop body: keep looping while the solve is not
+// done and the body count is below its bound.  The bound is independent of
+// the solver state, so the loop ends even if that state were wrong.
+__global__ void k_loop_control(SolverState* st, cudaGraphConditionalHandle handle) {
+  if (threadIdx.x != 0) return;
+  const int loops = st->loops + 1;
+  st->loops = loops;
+  const bool go = !st->done && loops < st->loop_limit;
+  cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
 int grid_size() {
   static int g = 0;
   if (!g) {
@@ -562,12 +579,13 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   S.slots = sp[S.nslices];
   if (S.slots >= (int64_t(1) << 31)) { set_error("matrix too large for the solver format"); return EMG_INVALID_INPUT; }
   int32_t* iperm = nullptr;
-  EMG_CK(cudaMalloc(&S.perm, sizeof(int32_t) * n));
-  EMG_CK(cudaMalloc(&iperm, sizeof(int32_t) * n));
-  EMG_CK(cudaMalloc(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1)));
-  EMG_CK(cudaMalloc(&S.col, sizeof(int32_t) * std::max<int64_t>(S.slots, 1)));
-  EMG_CK(cudaMalloc(&S.src, sizeof(int32_t) * std::max<int64_t>(S.slots, 1)));
-  EMG_CK(cudaMalloc(&S.val, sizeof(double) * std::max<int64_t>(S.slots, 1)));
+  const size_t ns = static_cast<size_t>(std::max<int64_t>(S.slots, 1));
+  EMG_CK(cudaMallocAsync(&S.perm, sizeof(int32_t) * n, st));
+  EMG_CK(cudaMallocAsync(&iperm, sizeof(int32_t) * n, st));
+  EMG_CK(cudaMallocAsync(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), st));
+  EMG_CK(cudaMallocAsync(&S.col, sizeof(int32_t) * ns, st));
+  EMG_CK(cudaMallocAsync(&S.src, sizeof(int32_t) * ns, st));
+  EMG_CK(cudaMallocAsync(&S.val, sizeof(double) * ns, st));
   EMG_CK(cudaMemcpyAsync(S.perm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
   EMG_CK(cudaMemcpyAsync(S.slice_ptr, sp.data(), sizeof(int64_t) * (S.nslices + 1), cudaMemcpyHostToDevice, st));
   const int g = grid_size();
@@ -575,7 +593,7 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   k_sell_fill<<<g, kThreads, 0, st>>>(n, S.nslices, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col, S.src);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaStreamSynchronize(st));
-  cudaFree(iperm);
+  EMG_CK(cudaFreeAsync(iperm, st));
   S.version = ~uint64_t(0);
   return EMG_SUCCESS;
 }
@@ -596,25 +614,26 @@ int ensure_sell(DevCsr& A, cudaStream_t st) {
 
 void free_sell(Sell* s) {
   if (!s) return;
-  cudaFree(s->perm); cudaFree(s->slice_ptr); cudaFree(s->col); cudaFree(s->src); cudaFree(s->val);
+  for (void* p : {static_cast<void*>(s->perm), static_cast<void*>(s->slice_ptr),
+                  static_cast<void*>(s->col), static_cast<void*>(s->src), static_cast<void*>(s->val)})
+    if (p) cudaFreeAsync(p, 0);
   delete s;
 }
 
-int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter) {
+// Workspace vectors come from the stream-ordered pool (allocated on `st`,
+// returned with cudaFreeAsync once the device is idle).
+int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
   if (!A.ws) {
     A.ws = new KrylovWorkspace();
     KrylovWorkspace& w = *A.ws;
     w.n = A.n;
     w.grid = grid_size();
     const size_t vb = sizeof(double) * (A.n > 0 ? A.n : 1);
-    EMG_CK(cudaMalloc(&w.dinv, vb));
-    EMG_CK(cudaMalloc(&w.x, vb));
-    EMG_CK(cudaMalloc(&w.r, vb));
-    EMG_CK(cudaMalloc(&w.z, vb));
-    EMG_CK(cudaMalloc(&w.p, vb));
-    EMG_CK(cudaMalloc(&w.q, vb));
-    EMG_CK(cudaMalloc(&w.partial, sizeof(double) * 4 * w.grid));
-    EMG_CK(cudaMalloc(&w.state, sizeof(SolverState)));
+    for (double** v : {&w.dinv, &w.x, &w.r, &w.z, &w.p, &w.q})
+      EMG_CK(cudaMallocAsync(v, vb, st));
+    EMG_CK(cudaMallocAsync(&w.partial, sizeof(double) * 4 * w.grid, st));
+    EMG_CK(cudaMallocAsync(&w.state, sizeof(SolverState), st));
+    EMG_CK(cudaStreamSynchronize(st));
     EMG_CK(cudaMemset(w.state, 0, sizeof(SolverState)));
     EMG_CK(cudaMallocHost(&w.state_h, sizeof(SolverState)));
     EMG_CK(cudaStreamCreate(&w.cap));
@@ -624,29 +643,66 @@ int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter) {
   KrylovWorkspace& w = *A.ws;
   if (bicg && !w.rh) {
     const size_t vb = sizeof(double) * (A.n > 0 ? A.n : 1);
-    EMG_CK(cudaMalloc(&w.rh, vb));
-    EMG_CK(cudaMalloc(&w.v, vb));
-    EMG_CK(cudaMalloc(&w.s, vb));
-    EMG_CK(cudaMalloc(&w.t, vb));
+    for (double** v : {&w.rh, &w.v, &w.s, &w.t}) EMG_CK(cudaMallocAsync(v, vb, st));
+    EMG_CK(cudaStreamSynchronize(st));
   }
   if (max_iter > w.hist_cap) {
-    if (w.hist) EMG_CK(cudaFree(w.hist));
+    if (w.hist) EMG_CK(cudaFreeAsync(w.hist, st));
     w.hist_cap = max_iter;
-    EMG_CK(cudaMalloc(&w.hist, sizeof(double) * w.hist_cap));
+    EMG_CK(cudaMallocAsync(&w.hist, sizeof(double) * w.hist_cap, st));
+    EMG_CK(cudaStreamSynchronize(st));
     // the chunk graphs hold the old pointer
-    if (w.cg_exec) { cudaGraphExecDestroy(w.cg_exec); w.cg_exec = nullptr; }
-    if (w.bi_exec) { cudaGraphExecDestroy(w.bi_exec); w.bi_exec = nullptr; }
+    for (cudaGraphExec_t* g : {&w.cg_exec, &w.bi_exec, &w.cg_loop, &w.bi_loop})
+      if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
   }
   return EMG_SUCCESS;
 }
 
-int capture_chunk(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
+void launch_iterations(DevCsr& A, bool bicg, int count);
+
+// The whole solve as one graph: a conditional while-node whose body runs
+// kBody iterations and then k_loop_control.
+int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
+  KrylovWorkspace& w = *A.ws;
+  cudaGraph_t graph = nullptr;
+  EMG_CK(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    cudaGetLastError();
+    set_error(std::string("conditional graph node: ") + cudaGetErrorString(e));
+    return EMG_ERR_CUDA;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(w.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    launch_iterations(A, bicg, kBody);
+    k_loop_control<<<1, 32, 0, w.cap>>>(w.state, handle);
+    e = cudaStreamEndCapture(w.cap, &body);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("while-loop graph: ") + cudaGetErrorString(e));
+    return EMG_ERR_CUDA;
+  }
+  return EMG_SUCCESS;
+}
+
+void launch_iterations(DevCsr& A, bool bicg, int count) {
   KrylovWorkspace& w = *A.ws;
   const Sell S = *A.sell;
   const int g = w.grid;
-  cudaGraph_t graph = nullptr;
-  EMG_CK(cudaStreamBeginCapture(w.cap, cudaStreamCaptureModeThreadLocal));
-  for (int c = 0; c < kChunk; ++c) {
+  for (int c = 0; c < count; ++c) {
     if (!bicg) {
       k_cg_spmv_dot<<<g, kThreads, 0, w.cap>>>(S, w.p, w.q, w.partial, w.state);
       k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
@@ -661,6 +717,13 @@ int capture_chunk(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
                                         w.hist, w.hist_cap);
     }
   }
+}
+
+int capture_chunk(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
+  KrylovWorkspace& w = *A.ws;
+  cudaGraph_t graph = nullptr;
+  EMG_CK(cudaStreamBeginCapture(w.cap, cudaStreamCaptureModeThreadLocal));
+  launch_iterations(A, bicg, kChunk);
   cudaError_t e = cudaStreamEndCapture(w.cap, &graph);
   if (e != cudaSuccess) { set_error(std::string("graph capture: ") + cudaGetErrorString(e)); return EMG_ERR_CUDA; }
   e = cudaGraphInstantiate(out, graph, 0);
@@ -676,14 +739,21 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   if (!b || !x) { set_error("null vector"); return EMG_INVALID_INPUT; }
   if (A.n <= 0) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
   const int32_t max_iter = cfg.max_iterations;
-  int rc = ensure_ws(A, bicg, max_iter > 0 ? max_iter : 1);
+  int rc = ensure_ws(A, bicg, max_iter > 0 ? max_iter : 1, user);
   if (rc) { res->status = rc; return rc; }
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
   rc = ensure_sell(A, st);
   if (rc) { res->status = rc; return rc; }
+  // Preferred: the whole solve as one graph with a device while-loop; else
+  // host-polled chunks of kChunk iterations.
+  cudaGraphExec_t* loop = bicg ? &w.bi_loop : &w.cg_loop;
+  if (!*loop && !w.loop_unavailable && capture_loop(A, bicg, loop) != EMG_SUCCESS) {
+    w.loop_unavailable = true;
+    *loop = nullptr;
+  }
   cudaGraphExec_t* exec = bicg ? &w.bi_exec : &w.cg_exec;
-  if (!*exec) {
+  if (!*loop && !*exec) {
     rc = capture_chunk(A, bicg, exec);
     if (rc) { res->status = rc; return rc; }
   }
@@ -692,6 +762,7 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   std::memset(&init, 0, sizeof(init));
   init.tol = cfg.tolerance;
   init.max_iter = max_iter;
+  init.loop_limit = (max_iter > 0 ? max_iter : 0) / kBody + 2;
   *w.state_h = init;
   EMG_CK(cudaEventRecord(w.ev0, st));
   EMG_CK(cudaMemcpyAsync(w.state, w.state_h, sizeof(SolverState), cudaMemcpyHostToDevice, st));
@@ -705,15 +776,24 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   // Graph chunks until the device state says done; bounded by max_iter.
   const int64_t max_chunks = (static_cast<int64_t>(max_iter > 0 ? max_iter : 0) + kChunk - 1) / kChunk + 1;
   bool done = false;
-  for (int64_t c = 0; c <= max_chunks; ++c) {
+  if (*loop) {
+    EMG_CK(cudaGraphLaunch(*loop, st));
+    k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, w.x, x);
+    EMG_CK(cudaEventRecord(w.ev1, st));
     EMG_CK(cudaMemcpyAsync(w.state_h, w.state, sizeof(SolverState), cudaMemcpyDeviceToHost, st));
     EMG_CK(cudaStreamSynchronize(st));
-    if (w.state_h->done) { done = true; break; }
-    EMG_CK(cudaGraphLaunch(*exec, st));
+    done = w.state_h->done != 0;
+  } else {
+    for (int64_t c = 0; c <= max_chunks; ++c) {
+      EMG_CK(cudaMemcpyAsync(w.state_h, w.state, sizeof(SolverState), cudaMemcpyDeviceToHost, st));
+      EMG_CK(cudaStreamSynchronize(st));
+      if (w.state_h->done) { done = true; break; }
+      EMG_CK(cudaGraphLaunch(*exec, st));
+    }
+    k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, w.x, x);
+    EMG_CK(cudaEventRecord(w.ev1, st));
+    EMG_CK(cudaStreamSynchronize(st));
   }
-  k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, w.x, x);
-  EMG_CK(cudaEventRecord(w.ev1, st));
-  EMG_CK(cudaStreamSynchronize(st));
   float ms = 0.0f;
   EMG_CK(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
   if (!done) {
@@ -735,7 +815,7 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
 
 int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
   if (!x || !y) { set_error("null vector"); return EMG_INVALID_INPUT; }
-  int rc = ensure_ws(A, false, 1);
+  int rc = ensure_ws(A, false, 1, st);
   if (rc) return rc;
   rc = ensure_sell(A, st);
   if (rc) return rc;
@@ -761,7 +841,7 @@ int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_confi
 
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms) {
   if (iterations <= 0 || !ms) { set_error("bad arguments"); return EMG_INVALID_INPUT; }
-  int rc = ensure_ws(A, false, 1);
+  int rc = ensure_ws(A, false, 1, user);
   if (rc) return rc;
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
@@ -827,11 +907,11 @@ int64_t sell_slices(DevCsr& A) { return A.sell ? A.sell->nslices : -1; }
 
 void free_workspace(KrylovWorkspace* w) {
   if (!w) return;
-  if (w->cg_exec) cudaGraphExecDestroy(w->cg_exec);
-  if (w->bi_exec) cudaGraphExecDestroy(w->bi_exec);
-  cudaFree(w->dinv); cudaFree(w->x); cudaFree(w->r); cudaFree(w->z); cudaFree(w->p); cudaFree(w->q);
-  cudaFree(w->rh); cudaFree(w->v); cudaFree(w->s); cudaFree(w->t);
-  cudaFree(w->partial); cudaFree(w->hist); cudaFree(w->state);
+  for (cudaGraphExec_t g : {w->cg_exec, w->bi_exec, w->cg_loop, w->bi_loop})
+    if (g) cudaGraphExecDestroy(g);
+  for (double* p : {w->dinv, w->x, w->r, w->z, w->p, w->q, w->rh, w->v, w->s, w->t, w->partial, w->hist})
+    if (p) cudaFreeAsync(p, 0);
+  if (w->state) cudaFreeAsync(w->state, 0);
   if (w->state_h) cudaFreeHost(w->state_h);
   if (w->cap) cudaStreamDestroy(w->cap);
   if (w->ev0) cudaEventDestroy(w->ev0);

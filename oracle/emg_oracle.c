@@ -620,10 +620,20 @@ void orc_spmv(int64_t n, const int64_t* rp, const int32_t* col, const double* va
   }
 }
 
+/* Deterministic dot product: fixed 64 chunks summed in order, independent of
+ * the thread count. */
 static double vdot(int64_t n, const double* a, const double* b) {
+  enum { NCH = 64 };
+  double part[NCH];
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < NCH; c++) {
+    int64_t lo = n * c / NCH, hi = n * (c + 1) / NCH;
+    double s = 0.0;
+    for (int64_t i = lo; i < hi; i++) s += a[i] * b[i];
+    part[c] = s;
+  }
   double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-  for (int64_t i = 0; i < n; i++) s += a[i] * b[i];
+  for (int c = 0; c < NCH; c++) s += part[c];
   return s;
 }
 
