@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="iterations in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--kernels-only", type=int, default=0, metavar="ITERS",
+                    help="profiling mode: assemble once, then launch ITERS plain CG iterations "
+                         "(no graphs) and print their per-kernel CUDA-event times")
     return ap.parse_args()
 
 
@@ -166,6 +169,19 @@ def run_ours(args, rank, world, local_rank):
     sigma = np.ascontiguousarray(m.sigma)
     cfg = _abi.KrylovConfig(TOL, MAX_ITER, _abi.PRECOND_JACOBI)
     info = {}
+
+    if args.kernels_only:
+        h = C.c_void_p()
+        _abi.check(L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                              C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                              C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h)), "create")
+        _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
+                   "assemble")
+        kt = (C.c_double * 3)()
+        _abi.check(L.emg_cg_kernel_times(L.emg_system_matrix(h, 0), args.kernels_only, sp, kt), "times")
+        L.emg_system_destroy(h)
+        return {"mode": "kernels-only", "iterations": args.kernels_only,
+                "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]}}
 
     def step(resident: bool):
         h = C.c_void_p()
