@@ -12,6 +12,7 @@
 
 #include "device.h"
 #include "internal.h"
+#include "trace.h"
 
 struct emg_mesh_t {
   emg::Mesh m;
@@ -112,7 +113,10 @@ int system_create_impl(int64_t n_nodes, const double* xyz, int64_t n_tets, const
     cudaError_t e = cudaMallocAsync(&s.err, sizeof(int32_t), st);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
   }
-  if (!rc) rc = emg::system_build(s, st);
+  if (!rc) {
+    emg::TraceScope t("system_create.build");
+    rc = emg::system_build(s, st);
+  }
   if (rc) { delete h; return rc; }
   h->k_handle.csr = &s.K;
   h->k_handle.owned = false;
@@ -292,7 +296,11 @@ const double* emg_system_rhs_device(emg_system sys) { return sys ? sys->s.rhs : 
 
 void emg_system_destroy(emg_system sys) {
   if (!sys) return;
-  cudaDeviceSynchronize();
+  emg::TraceScope t("emg_system_destroy");
+  {
+    emg::TraceScope t2("emg_system_destroy.sync");
+    cudaDeviceSynchronize();
+  }
   delete sys;
 }
 

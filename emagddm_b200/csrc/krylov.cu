@@ -29,6 +29,8 @@
 
 #include "common.cuh"
 #include "device.h"
+#include "sell_tma.cuh"
+#include "trace.h"
 
 namespace emg {
 
@@ -49,12 +51,14 @@ struct SolverState {
   uint32_t ticket;
   int32_t loops;       // device-loop bodies executed in this solve
   int32_t loop_limit;  // hard bound on loop bodies (stops the loop without `done`)
-  int32_t pad;
+  int32_t copy_err;    // a bounded wait on a bulk copy ran out
 };
 
 // SELL-32-sigma copy of a DevCsr in the permuted numbering.
 struct Sell {
   int64_t n = 0, nslices = 0, slots = 0;
+  int64_t max_tile_slots = 0;    // largest 8-slice tile (bulk-copy stage size)
+  bool tma = false;              // stages of the bulk-copy kernels fit in shared memory
   int32_t* perm = nullptr;       // new row -> old row
   int64_t* slice_ptr = nullptr;  // nslices + 1 slot offsets (multiples of 32)
   int32_t* col = nullptr;        // permuted column of every slot
@@ -98,6 +102,10 @@ __device__ __forceinline__ int64_t gstride() {
   return static_cast<int64_t>(gridDim.x) * blockDim.x;
 }
 
+#ifndef EMG_SELL_TMA
+#define EMG_SELL_TMA 1  // stream SpMV slices through shared memory by bulk copies
+#endif
+
 // Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
 // out(row, y_row) for every real row.  Entries of a row are summed in CSR
 // order, four loads in flight per lane at a time.
@@ -134,6 +142,111 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     const int64_t row = s * kSliceRows + lane;
     if (row < A.n) out(row, sum);
   }
+}
+
+// Same product with the slices streamed through shared memory by bulk
+// asynchronous copies (see sell_tma.cuh).  Launch: persistent grid, 256
+// threads, tma::smem_bytes() of dynamic shared memory.  A bounded wait that
+// runs out raises *err and the block drains its copies and stops.
+template <class Out>
+__device__ __forceinline__ void sell_rows_tma(const Sell& A, const double* __restrict__ x, Out out,
+                                              int32_t* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const tma::Layout Ly = tma::layout_for(static_cast<uint32_t>(A.max_tile_slots));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + tma::kStages * Ly.stage_bytes);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t* __restrict__ sp = A.slice_ptr;
+  const int64_t ns = A.nslices;
+  const int64_t ntiles = (ns + tma::kWarps - 1) / tma::kWarps;
+  const int64_t stride = gridDim.x;
+  const uint64_t pol = evict_first_policy();
+  auto tile_range = [&](int64_t t, int64_t& a, int64_t& b) {
+    const int64_t s0 = t * tma::kWarps;
+    const int64_t s1 = s0 + tma::kWarps < ns ? s0 + tma::kWarps : ns;
+    a = sp[s0];
+    b = sp[s1];
+  };
+  auto issue = [&](int64_t t, int stage) {
+    int64_t a, b;
+    tile_range(t, a, b);
+    const uint32_t slots = static_cast<uint32_t>(b - a);
+    unsigned char* base = smem + stage * Ly.stage_bytes;
+    tma::mbar_expect_tx(&bars[stage], slots * 12u);  // 0 bytes: the arrival alone completes it
+    if (slots > 0) {
+      tma::bulk_g2s(base, A.val + a, slots * 8u, &bars[stage], pol);
+      tma::bulk_g2s(base + slots * 8u, A.col + a, slots * 4u, &bars[stage], pol);
+    }
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < tma::kStages; ++s) tma::mbar_init(&bars[s], 1);
+    tma::fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < tma::kStages; ++k) {
+      const int64_t t = blockIdx.x + k * stride;
+      if (t < ntiles) issue(t, k);
+    }
+  bool ok = true;
+  int k = 0;
+  int64_t t = blockIdx.x;
+  for (; t < ntiles; t += stride, ++k) {
+    const int stage = k % tma::kStages;
+    const uint32_t parity = static_cast<uint32_t>(k / tma::kStages) & 1u;
+    ok = __syncthreads_and(tma::mbar_wait(&bars[stage], parity) ? 1 : 0) != 0;
+    if (!ok) break;
+    const int64_t s = t * tma::kWarps + warp;
+    if (s < ns) {
+      int64_t a, b;
+      tile_range(t, a, b);
+      const int64_t b0 = sp[s];
+      const int len = static_cast<int>((sp[s + 1] - b0) >> 5);
+      const unsigned char* base = smem + stage * Ly.stage_bytes;
+      const double* sv = reinterpret_cast<const double*>(base) + (b0 - a) + lane;
+      const int32_t* sc =
+          reinterpret_cast<const int32_t*>(base + static_cast<uint32_t>(b - a) * 8u) + (b0 - a) + lane;
+      double sum = 0.0;
+      int j = 0;
+      for (; j + 4 <= len; j += 4) {
+        const int c0 = sc[32 * j], c1 = sc[32 * j + 32], c2 = sc[32 * j + 64], c3 = sc[32 * j + 96];
+        const double x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
+        sum += sv[32 * j] * x0;
+        sum += sv[32 * j + 32] * x1;
+        sum += sv[32 * j + 64] * x2;
+        sum += sv[32 * j + 96] * x3;
+      }
+      for (; j < len; ++j) sum += sv[32 * j] * x[sc[32 * j]];
+      const int64_t row = s * kSliceRows + lane;
+      if (row < A.n) out(row, sum);
+    }
+    __syncthreads();  // every warp is done with this stage
+    if (threadIdx.x == 0) {
+      const int64_t tn = t + tma::kStages * stride;
+      if (tn < ntiles) {
+        tma::fence_proxy_async();
+        issue(tn, stage);
+      }
+    }
+  }
+  if (!ok) {
+    // drain the copies this block still has in flight (bounded), then stop
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1);
+      for (int q = 0; q < tma::kStages; ++q, ++k, t += stride) {
+        if (t >= ntiles) break;
+        tma::mbar_wait(&bars[k % tma::kStages], static_cast<uint32_t>(k / tma::kStages) & 1u);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Row kernels run either the plain SELL loop or the bulk-copy pipeline.
+template <bool kTma, class Out>
+__device__ __forceinline__ void spmv_rows(const Sell& A, const double* __restrict__ x, Out out,
+                                          int32_t* err) {
+  if constexpr (kTma) sell_rows_tma(A, x, out, err);
+  else sell_rows(A, x, out);
 }
 
 // One partial per block; true in the block that finished last (all partials
@@ -240,9 +353,10 @@ __global__ void k_scatter(int64_t n, const int32_t* __restrict__ perm, const dou
   for (int64_t i = gtid(); i < n; i += gstride()) out[perm[i]] = in[i];
 }
 
+template <bool kTma>
 __global__ void __launch_bounds__(kThreads) k_spmv(Sell A, const double* __restrict__ x,
-                                                   double* __restrict__ y) {
-  sell_rows(A, x, [&](int64_t row, double s) { y[row] = s; });
+                                                   double* __restrict__ y, int32_t* err) {
+  spmv_rows<kTma>(A, x, [&](int64_t row, double s) { y[row] = s; }, err);
 }
 
 // ----------------------------------------------------------------- CG ----
@@ -278,21 +392,25 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* _
   }
 }
 
+template <bool kTma>
 __global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(Sell A, const double* __restrict__ p,
                                                           double* __restrict__ q, double* partial,
                                                           SolverState* st) {
   if (st->done) return;
   double dot = 0.0;
-  sell_rows(A, p, [&](int64_t row, double s) {
+  spmv_rows<kTma>(A, p, [&](int64_t row, double s) {
     q[row] = s;
     dot += p[row] * s;
-  });
+  }, &st->copy_err);
   double acc[1] = {dot};
   double tot[1];
   if (!reduce_partials<1>(acc, partial, st, tot)) return;
   if (threadIdx.x == 0) {
     const double pq = tot[0];
-    if (fabs(pq) < 1e-30) {  // :453-457
+    if (st->copy_err) {
+      st->status = EMG_ERR_TIMEOUT;
+      st->done = 1;
+    } else if (fabs(pq) < 1e-30) {  // :453-457
       st->status = EMG_NUMERICAL_ERROR;
       st->done = 1;
     } else {
@@ -407,21 +525,24 @@ __global__ void __launch_bounds__(kThreads) k_bi_p(int64_t n, double* __restrict
 }
 
 // v = A p, r_hat . v -> alpha
+template <bool kTma>
 __global__ void __launch_bounds__(kThreads) k_bi_v(Sell A, const double* __restrict__ p,
                                                    double* __restrict__ v,
                                                    const double* __restrict__ rh, double* partial,
                                                    SolverState* st) {
   if (st->done) return;
   double dot = 0.0;
-  sell_rows(A, p, [&](int64_t row, double s) {
+  spmv_rows<kTma>(A, p, [&](int64_t row, double s) {
     v[row] = s;
     dot += rh[row] * s;
-  });
+  }, &st->copy_err);
   double acc[1] = {dot};
   double tot[1];
   if (!reduce_partials<1>(acc, partial, st, tot)) return;
   if (threadIdx.x == 0) {
-    if (fabs(tot[0]) < 1e-30) {  // :1043-1047
+    if (st->copy_err) {
+      st->status = EMG_ERR_TIMEOUT; st->done = 1;
+    } else if (fabs(tot[0]) < 1e-30) {  // :1043-1047
       st->status = EMG_NUMERICAL_ERROR; st->done = 1;
     } else {
       st->alpha = st->rho / tot[0];
@@ -456,20 +577,24 @@ __global__ void __launch_bounds__(kThreads) k_bi_s(int64_t n, const double* __re
 }
 
 // t = A z, t.t and z.t -> omega
+template <bool kTma>
 __global__ void __launch_bounds__(kThreads) k_bi_t(Sell A, const double* __restrict__ z,
                                                    double* __restrict__ t, double* partial,
                                                    SolverState* st) {
   if (st->done || st->early) return;
   double tt = 0.0, zt = 0.0;
-  sell_rows(A, z, [&](int64_t row, double s) {
+  spmv_rows<kTma>(A, z, [&](int64_t row, double s) {
     t[row] = s;
     tt += s * s;
     zt += z[row] * s;
-  });
+  }, &st->copy_err);
   double acc[2] = {tt, zt};
   double tot[2];
   if (!reduce_partials<2>(acc, partial, st, tot)) return;
-  if (threadIdx.x == 0) st->omega = fabs(tot[0]) < 1e-30 ? 0.0 : tot[1] / tot[0];
+  if (threadIdx.x == 0) {
+    st->omega = fabs(tot[0]) < 1e-30 ? 0.0 : tot[1] / tot[0];
+    if (st->copy_err) { st->status = EMG_ERR_TIMEOUT; st->done = 1; }
+  }
 }
 
 // x += alpha p + omega z, r = s - omega t; residual checks; next rho
@@ -536,6 +661,29 @@ __global__ void k_loop_control(SolverState* st, cudaGraphConditionalHandle handl
   cudaGraphSetConditional(handle, go ? 1u : 0u);
 }
 
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// Launch shape of the SpMV kernels: the bulk-copy pipeline runs one
+// persistent block per SM with its stages in dynamic shared memory.
+struct SpmvShape {
+  int grid;
+  size_t smem;
+};
+SpmvShape spmv_shape(const Sell& S, int plain_grid) {
+  if (S.tma)
+    return {num_sms(), tma::smem_bytes(tma::layout_for(static_cast<uint32_t>(S.max_tile_slots)))};
+  return {plain_grid, 0};
+}
+
 int grid_size() {
   static int g = 0;
   if (!g) {
@@ -595,6 +743,29 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   EMG_CK(cudaStreamSynchronize(st));
   EMG_CK(cudaFreeAsync(iperm, st));
   S.version = ~uint64_t(0);
+  // bulk-copy pipeline: tiles of 8 slices, kStages stages in shared memory
+  S.max_tile_slots = 0;
+  for (int64_t s0 = 0; s0 < S.nslices; s0 += tma::kWarps) {
+    const int64_t s1 = std::min<int64_t>(S.nslices, s0 + tma::kWarps);
+    S.max_tile_slots = std::max<int64_t>(S.max_tile_slots, sp[s1] - sp[s0]);
+  }
+  S.tma = false;
+#if EMG_SELL_TMA
+  {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t need = tma::smem_bytes(tma::layout_for(static_cast<uint32_t>(S.max_tile_slots)));
+    if (S.max_tile_slots > 0 && need <= static_cast<size_t>(optin)) {
+      const int b = static_cast<int>(need);
+      EMG_CK(cudaFuncSetAttribute(k_cg_spmv_dot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_v<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      S.tma = true;
+    }
+  }
+#endif
   return EMG_SUCCESS;
 }
 
@@ -702,17 +873,27 @@ void launch_iterations(DevCsr& A, bool bicg, int count) {
   KrylovWorkspace& w = *A.ws;
   const Sell S = *A.sell;
   const int g = w.grid;
+  const SpmvShape sh = spmv_shape(S, g);
   for (int c = 0; c < count; ++c) {
     if (!bicg) {
-      k_cg_spmv_dot<<<g, kThreads, 0, w.cap>>>(S, w.p, w.q, w.partial, w.state);
+      if (S.tma)
+        k_cg_spmv_dot<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.p, w.q, w.partial, w.state);
+      else
+        k_cg_spmv_dot<false><<<g, kThreads, 0, w.cap>>>(S, w.p, w.q, w.partial, w.state);
       k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                              w.hist, w.hist_cap);
       k_cg_direction<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
     } else {
       k_bi_p<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
-      k_bi_v<<<g, kThreads, 0, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
+      if (S.tma)
+        k_bi_v<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
+      else
+        k_bi_v<false><<<g, kThreads, 0, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
       k_bi_s<<<g, kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
-      k_bi_t<<<g, kThreads, 0, w.cap>>>(S, w.z, w.t, w.partial, w.state);
+      if (S.tma)
+        k_bi_t<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.z, w.t, w.partial, w.state);
+      else
+        k_bi_t<false><<<g, kThreads, 0, w.cap>>>(S, w.z, w.t, w.partial, w.state);
       k_bi_x<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
                                         w.hist, w.hist_cap);
     }
@@ -739,18 +920,28 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   if (!b || !x) { set_error("null vector"); return EMG_INVALID_INPUT; }
   if (A.n <= 0) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
   const int32_t max_iter = cfg.max_iterations;
-  int rc = ensure_ws(A, bicg, max_iter > 0 ? max_iter : 1, user);
+  int rc;
+  {
+    TraceScope t("solve.workspace");
+    rc = ensure_ws(A, bicg, max_iter > 0 ? max_iter : 1, user);
+  }
   if (rc) { res->status = rc; return rc; }
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
-  rc = ensure_sell(A, st);
+  {
+    TraceScope t("solve.sell");
+    rc = ensure_sell(A, st);
+  }
   if (rc) { res->status = rc; return rc; }
   // Preferred: the whole solve as one graph with a device while-loop; else
   // host-polled chunks of kChunk iterations.
   cudaGraphExec_t* loop = bicg ? &w.bi_loop : &w.cg_loop;
-  if (!*loop && !w.loop_unavailable && capture_loop(A, bicg, loop) != EMG_SUCCESS) {
-    w.loop_unavailable = true;
-    *loop = nullptr;
+  if (!*loop && !w.loop_unavailable) {
+    TraceScope t("solve.capture_loop");
+    if (capture_loop(A, bicg, loop) != EMG_SUCCESS) {
+      w.loop_unavailable = true;
+      *loop = nullptr;
+    }
   }
   cudaGraphExec_t* exec = bicg ? &w.bi_exec : &w.cg_exec;
   if (!*loop && !*exec) {
@@ -823,7 +1014,13 @@ int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
   const Sell& S = *A.sell;
   // the workspace vectors hold the permuted operands
   k_gather<<<g, kThreads, 0, st>>>(A.n, S.perm, x, A.ws->p);
-  k_spmv<<<g, kThreads, 0, st>>>(S, A.ws->p, A.ws->q);
+  const SpmvShape sh = spmv_shape(S, g);
+  int32_t* err = &A.ws->state->copy_err;
+  EMG_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+  if (S.tma)
+    k_spmv<true><<<sh.grid, kThreads, sh.smem, st>>>(S, A.ws->p, A.ws->q, err);
+  else
+    k_spmv<false><<<g, kThreads, 0, st>>>(S, A.ws->p, A.ws->q, err);
   k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, A.ws->q, y);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -865,7 +1062,12 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
   for (auto& e : ev) EMG_CK(cudaEventCreate(&e));
   for (int i = 0; i < iterations; ++i) {
     EMG_CK(cudaEventRecord(ev[4 * i], st));
-    k_cg_spmv_dot<<<g, kThreads, 0, st>>>(S, w.p, w.q, w.partial, w.state);
+    if (S.tma) {
+      const SpmvShape sh = spmv_shape(S, g);
+      k_cg_spmv_dot<true><<<sh.grid, kThreads, sh.smem, st>>>(S, w.p, w.q, w.partial, w.state);
+    } else {
+      k_cg_spmv_dot<false><<<g, kThreads, 0, st>>>(S, w.p, w.q, w.partial, w.state);
+    }
     EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
     k_cg_update<<<g, kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                         w.hist, w.hist_cap);
@@ -907,15 +1109,27 @@ int64_t sell_slices(DevCsr& A) { return A.sell ? A.sell->nslices : -1; }
 
 void free_workspace(KrylovWorkspace* w) {
   if (!w) return;
-  for (cudaGraphExec_t g : {w->cg_exec, w->bi_exec, w->cg_loop, w->bi_loop})
-    if (g) cudaGraphExecDestroy(g);
-  for (double* p : {w->dinv, w->x, w->r, w->z, w->p, w->q, w->rh, w->v, w->s, w->t, w->partial, w->hist})
-    if (p) cudaFreeAsync(p, 0);
-  if (w->state) cudaFreeAsync(w->state, 0);
-  if (w->state_h) cudaFreeHost(w->state_h);
-  if (w->cap) cudaStreamDestroy(w->cap);
-  if (w->ev0) cudaEventDestroy(w->ev0);
-  if (w->ev1) cudaEventDestroy(w->ev1);
+  {
+    TraceScope t("free_workspace.graphs");
+    for (cudaGraphExec_t g : {w->cg_exec, w->bi_exec, w->cg_loop, w->bi_loop})
+      if (g) cudaGraphExecDestroy(g);
+  }
+  {
+    TraceScope t("free_workspace.vectors");
+    for (double* p : {w->dinv, w->x, w->r, w->z, w->p, w->q, w->rh, w->v, w->s, w->t, w->partial, w->hist})
+      if (p) cudaFreeAsync(p, 0);
+    if (w->state) cudaFreeAsync(w->state, 0);
+  }
+  {
+    TraceScope t("free_workspace.host_state");
+    if (w->state_h) cudaFreeHost(w->state_h);
+  }
+  {
+    TraceScope t("free_workspace.stream_events");
+    if (w->cap) cudaStreamDestroy(w->cap);
+    if (w->ev0) cudaEventDestroy(w->ev0);
+    if (w->ev1) cudaEventDestroy(w->ev1);
+  }
   delete w;
 }
 
