@@ -105,6 +105,9 @@ __device__ __forceinline__ int64_t gstride() {
 #ifndef EMG_SELL_TMA
 #define EMG_SELL_TMA 1  // stream SpMV slices through shared memory by bulk copies
 #endif
+#ifndef EMG_SELL_UNROLL
+#define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
+#endif
 
 // Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
 // out(row, y_row) for every real row.  Entries of a row are summed in CSR
@@ -123,17 +126,19 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     const int64_t base = b0 + lane;
     double sum = 0.0;
     int j = 0;
-    for (; j + 4 <= len; j += 4) {
+    for (; j + EMG_SELL_UNROLL <= len; j += EMG_SELL_UNROLL) {
       const int64_t k = base + 32 * j;
-      const int c0 = ld_stream(col + k, pol), c1 = ld_stream(col + k + 32, pol);
-      const int c2 = ld_stream(col + k + 64, pol), c3 = ld_stream(col + k + 96, pol);
-      const double v0 = ld_stream(val + k, pol), v1 = ld_stream(val + k + 32, pol);
-      const double v2 = ld_stream(val + k + 64, pol), v3 = ld_stream(val + k + 96, pol);
-      const double x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
-      sum += v0 * x0;
-      sum += v1 * x1;
-      sum += v2 * x2;
-      sum += v3 * x3;
+      int c[EMG_SELL_UNROLL];
+      double v[EMG_SELL_UNROLL], xv[EMG_SELL_UNROLL];
+#pragma unroll
+      for (int u = 0; u < EMG_SELL_UNROLL; ++u) {
+        c[u] = ld_stream(col + k + 32 * u, pol);
+        v[u] = ld_stream(val + k + 32 * u, pol);
+      }
+#pragma unroll
+      for (int u = 0; u < EMG_SELL_UNROLL; ++u) xv[u] = x[c[u]];
+#pragma unroll
+      for (int u = 0; u < EMG_SELL_UNROLL; ++u) sum += v[u] * xv[u];
     }
     for (; j < len; ++j) {
       const int64_t k = base + 32 * j;
@@ -205,17 +210,16 @@ __device__ __forceinline__ void sell_rows_tma(const Sell& A, const double* __res
       const double* sv = reinterpret_cast<const double*>(base) + (b0 - a) + lane;
       const int32_t* sc =
           reinterpret_cast<const int32_t*>(base + static_cast<uint32_t>(b - a) * 8u) + (b0 - a) + lane;
+      // up to 16 gathers of x in flight per lane; summed in row order
       double sum = 0.0;
-      int j = 0;
-      for (; j + 4 <= len; j += 4) {
-        const int c0 = sc[32 * j], c1 = sc[32 * j + 32], c2 = sc[32 * j + 64], c3 = sc[32 * j + 96];
-        const double x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
-        sum += sv[32 * j] * x0;
-        sum += sv[32 * j + 32] * x1;
-        sum += sv[32 * j + 64] * x2;
-        sum += sv[32 * j + 96] * x3;
+      for (int j0 = 0; j0 < len; j0 += 16) {
+        double xv[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) xv[u] = j0 + u < len ? x[sc[32 * (j0 + u)]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+          if (j0 + u < len) sum += sv[32 * (j0 + u)] * xv[u];
       }
-      for (; j < len; ++j) sum += sv[32 * j] * x[sc[32 * j]];
       const int64_t row = s * kSliceRows + lane;
       if (row < A.n) out(row, sum);
     }
@@ -680,7 +684,8 @@ struct SpmvShape {
 };
 SpmvShape spmv_shape(const Sell& S, int plain_grid) {
   if (S.tma)
-    return {num_sms(), tma::smem_bytes(tma::layout_for(static_cast<uint32_t>(S.max_tile_slots)))};
+    return {tma::kBlocksPerSm * num_sms(),
+            tma::smem_bytes(tma::layout_for(static_cast<uint32_t>(S.max_tile_slots)))};
   return {plain_grid, 0};
 }
 

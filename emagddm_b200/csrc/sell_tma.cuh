@@ -19,7 +19,8 @@ namespace emg {
 namespace tma {
 
 constexpr int kWarps = 8;               // warps per block = slices per tile
-constexpr int kStages = 4;
+constexpr int kStages = 2;              // double buffering; two blocks per SM
+constexpr int kBlocksPerSm = 2;
 constexpr uint32_t kSpinLimit = 1u << 22;  // try_wait polls before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
