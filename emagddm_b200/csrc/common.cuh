@@ -49,6 +49,13 @@ __device__ __forceinline__ int ld_stream(const int* p, uint64_t pol) {
                : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
+// 16-bit signed load, sign-extended to int.
+__device__ __forceinline__ int ld_stream(const int16_t* p, uint64_t pol) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s16 %0, [%1], %2;"
+      : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
 // Coherent-at-L2 load for values written by other blocks of the same kernel.
 __device__ __forceinline__ double ld_l2(const double* p) { return __ldcg(p); }
 

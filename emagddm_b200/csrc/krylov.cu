@@ -61,6 +61,8 @@ struct Sell {
   bool tma = false;              // stages of the bulk-copy kernels fit in shared memory
   int32_t* perm = nullptr;       // new row -> old row
   int64_t* slice_ptr = nullptr;  // nslices + 1 slot offsets (multiples of 32)
+  int16_t* dcol = nullptr;       // column - row of every slot, when all fit in 16 bits
+  bool narrow = false;           // dcol in use (col freed): 10 bytes per slot instead of 12
   int32_t* col = nullptr;        // permuted column of every slot
   int32_t* src = nullptr;        // CSR index of every slot, -1 = padding
   double* val = nullptr;
@@ -93,7 +95,10 @@ constexpr int kThreads = 256;
 constexpr int kChunk = 16;      // iterations per host-polled graph launch
 constexpr int kBody = 4;        // iterations per body of the device while-loop
 constexpr int kSliceRows = 32;  // SELL slice height = warp width
-constexpr int kWindow = 4096;   // sigma: rows sorted by length inside a window
+#ifndef EMG_SELL_WINDOW
+#define EMG_SELL_WINDOW 4096
+#endif
+constexpr int kWindow = EMG_SELL_WINDOW;  // sigma: rows sorted by length inside a window
 
 __device__ __forceinline__ int64_t gtid() {
   return static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -102,8 +107,14 @@ __device__ __forceinline__ int64_t gstride() {
   return static_cast<int64_t>(gridDim.x) * blockDim.x;
 }
 
+// Bulk-copy (TMA) pipeline for the SpMV: built and tested, but on the 64^3
+// curl-curl matrix it measured slower than the plain SELL loop, so it is a
+// build-time option (-DEMG_SELL_TMA=1) rather than the default.
 #ifndef EMG_SELL_TMA
-#define EMG_SELL_TMA 1  // stream SpMV slices through shared memory by bulk copies
+#define EMG_SELL_TMA 0
+#endif
+#ifndef EMG_SELL_NARROW
+#define EMG_SELL_NARROW 1  // 16-bit column offsets when the matrix bandwidth allows
 #endif
 #ifndef EMG_SELL_UNROLL
 #define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
@@ -112,18 +123,25 @@ __device__ __forceinline__ int64_t gstride() {
 // Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
 // out(row, y_row) for every real row.  Entries of a row are summed in CSR
 // order, four loads in flight per lane at a time.
-template <class Out>
+// kNarrow: columns are stored as 16-bit offsets from the row (A.dcol).
+template <bool kNarrow, class Out>
 __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   const uint64_t pol = evict_first_policy();
   const int64_t* __restrict__ sp = A.slice_ptr;
   const int32_t* __restrict__ col = A.col;
+  const int16_t* __restrict__ dcol = A.dcol;
   const double* __restrict__ val = A.val;
+  auto column = [&](int64_t k, int row) -> int {
+    if constexpr (kNarrow) return row + ld_stream(dcol + k, pol);
+    else return ld_stream(col + k, pol);
+  };
   for (int64_t s = warp; s < A.nslices; s += nwarps) {
     const int64_t b0 = sp[s], b1 = sp[s + 1];
     const int len = static_cast<int>((b1 - b0) >> 5);
     const int64_t base = b0 + lane;
+    const int row32 = static_cast<int>(s * kSliceRows + lane);
     double sum = 0.0;
     int j = 0;
     for (; j + EMG_SELL_UNROLL <= len; j += EMG_SELL_UNROLL) {
@@ -132,7 +150,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
       double v[EMG_SELL_UNROLL], xv[EMG_SELL_UNROLL];
 #pragma unroll
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) {
-        c[u] = ld_stream(col + k + 32 * u, pol);
+        c[u] = column(k + 32 * u, row32);
         v[u] = ld_stream(val + k + 32 * u, pol);
       }
 #pragma unroll
@@ -142,7 +160,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     }
     for (; j < len; ++j) {
       const int64_t k = base + 32 * j;
-      sum += ld_stream(val + k, pol) * x[ld_stream(col + k, pol)];
+      sum += ld_stream(val + k, pol) * x[column(k, row32)];
     }
     const int64_t row = s * kSliceRows + lane;
     if (row < A.n) out(row, sum);
@@ -245,12 +263,13 @@ __device__ __forceinline__ void sell_rows_tma(const Sell& A, const double* __res
   }
 }
 
-// Row kernels run either the plain SELL loop or the bulk-copy pipeline.
-template <bool kTma, class Out>
+// Row kernels: kMode 0 = SELL with 32-bit columns, 1 = SELL with 16-bit
+// column offsets, 2 = bulk-copy pipeline (32-bit columns).
+template <int kMode, class Out>
 __device__ __forceinline__ void spmv_rows(const Sell& A, const double* __restrict__ x, Out out,
                                           int32_t* err) {
-  if constexpr (kTma) sell_rows_tma(A, x, out, err);
-  else sell_rows(A, x, out);
+  if constexpr (kMode == 2) sell_rows_tma(A, x, out, err);
+  else sell_rows<kMode == 1>(A, x, out);
 }
 
 // One partial per block; true in the block that finished last (all partials
@@ -312,6 +331,27 @@ __global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restric
   }
 }
 
+// Warp per slice: dcol = col - row; *overflow = 1 if any offset leaves int16.
+__global__ void k_sell_narrow(int64_t nslices, const int64_t* __restrict__ sp,
+                              const int32_t* __restrict__ col, int16_t* __restrict__ dcol,
+                              int32_t* __restrict__ overflow) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+  for (int64_t s = warp; s < nslices; s += nwarps) {
+    const int64_t b0 = sp[s];
+    const int len = static_cast<int>((sp[s + 1] - b0) >> 5);
+    const int64_t row = s * kSliceRows + lane;
+    bool bad = false;
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = b0 + 32 * j + lane;
+      const int64_t d = static_cast<int64_t>(col[k]) - row;
+      bad |= d < -32768 || d > 32767;
+      dcol[k] = static_cast<int16_t>(d);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(overflow, 1);
+  }
+}
+
 __global__ void k_sell_values(int64_t slots, const int32_t* __restrict__ src,
                               const double* __restrict__ cval, double* __restrict__ val) {
   for (int64_t i = gtid(); i < slots; i += gstride()) {
@@ -357,10 +397,10 @@ __global__ void k_scatter(int64_t n, const int32_t* __restrict__ perm, const dou
   for (int64_t i = gtid(); i < n; i += gstride()) out[perm[i]] = in[i];
 }
 
-template <bool kTma>
+template <int kMode>
 __global__ void __launch_bounds__(kThreads) k_spmv(Sell A, const double* __restrict__ x,
                                                    double* __restrict__ y, int32_t* err) {
-  spmv_rows<kTma>(A, x, [&](int64_t row, double s) { y[row] = s; }, err);
+  spmv_rows<kMode>(A, x, [&](int64_t row, double s) { y[row] = s; }, err);
 }
 
 // ----------------------------------------------------------------- CG ----
@@ -396,13 +436,13 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* _
   }
 }
 
-template <bool kTma>
+template <int kMode>
 __global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(Sell A, const double* __restrict__ p,
                                                           double* __restrict__ q, double* partial,
                                                           SolverState* st) {
   if (st->done) return;
   double dot = 0.0;
-  spmv_rows<kTma>(A, p, [&](int64_t row, double s) {
+  spmv_rows<kMode>(A, p, [&](int64_t row, double s) {
     q[row] = s;
     dot += p[row] * s;
   }, &st->copy_err);
@@ -529,14 +569,14 @@ __global__ void __launch_bounds__(kThreads) k_bi_p(int64_t n, double* __restrict
 }
 
 // v = A p, r_hat . v -> alpha
-template <bool kTma>
+template <int kMode>
 __global__ void __launch_bounds__(kThreads) k_bi_v(Sell A, const double* __restrict__ p,
                                                    double* __restrict__ v,
                                                    const double* __restrict__ rh, double* partial,
                                                    SolverState* st) {
   if (st->done) return;
   double dot = 0.0;
-  spmv_rows<kTma>(A, p, [&](int64_t row, double s) {
+  spmv_rows<kMode>(A, p, [&](int64_t row, double s) {
     v[row] = s;
     dot += rh[row] * s;
   }, &st->copy_err);
@@ -581,13 +621,13 @@ __global__ void __launch_bounds__(kThreads) k_bi_s(int64_t n, const double* __re
 }
 
 // t = A z, t.t and z.t -> omega
-template <bool kTma>
+template <int kMode>
 __global__ void __launch_bounds__(kThreads) k_bi_t(Sell A, const double* __restrict__ z,
                                                    double* __restrict__ t, double* partial,
                                                    SolverState* st) {
   if (st->done || st->early) return;
   double tt = 0.0, zt = 0.0;
-  spmv_rows<kTma>(A, z, [&](int64_t row, double s) {
+  spmv_rows<kMode>(A, z, [&](int64_t row, double s) {
     t[row] = s;
     tt += s * s;
     zt += z[row] * s;
@@ -763,14 +803,36 @@ int build_sell(DevCsr& A, cudaStream_t st) {
     const size_t need = tma::smem_bytes(tma::layout_for(static_cast<uint32_t>(S.max_tile_slots)));
     if (S.max_tile_slots > 0 && need <= static_cast<size_t>(optin)) {
       const int b = static_cast<int>(need);
-      EMG_CK(cudaFuncSetAttribute(k_cg_spmv_dot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-      EMG_CK(cudaFuncSetAttribute(k_bi_v<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-      EMG_CK(cudaFuncSetAttribute(k_bi_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-      EMG_CK(cudaFuncSetAttribute(k_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_cg_spmv_dot<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_v<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_spmv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
       S.tma = true;
     }
   }
 #endif
+  // 16-bit column offsets when every |column - row| fits (banded numberings,
+  // e.g. first-appearance edge IDs of structured meshes): 10 bytes per slot.
+  S.narrow = false;
+  if (EMG_SELL_NARROW && !S.tma && S.slots > 0) {
+    int32_t* overflow = nullptr;
+    EMG_CK(cudaMallocAsync(&S.dcol, sizeof(int16_t) * S.slots, st));
+    EMG_CK(cudaMallocAsync(&overflow, sizeof(int32_t), st));
+    EMG_CK(cudaMemsetAsync(overflow, 0, sizeof(int32_t), st));
+    k_sell_narrow<<<g, kThreads, 0, st>>>(S.nslices, S.slice_ptr, S.col, S.dcol, overflow);
+    int32_t h_over = 0;
+    EMG_CK(cudaMemcpyAsync(&h_over, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    EMG_CK(cudaFreeAsync(overflow, st));
+    if (h_over) {
+      EMG_CK(cudaFreeAsync(S.dcol, st));
+      S.dcol = nullptr;
+    } else {
+      EMG_CK(cudaFreeAsync(S.col, st));
+      S.col = nullptr;
+      S.narrow = true;
+    }
+  }
   return EMG_SUCCESS;
 }
 
@@ -791,7 +853,8 @@ int ensure_sell(DevCsr& A, cudaStream_t st) {
 void free_sell(Sell* s) {
   if (!s) return;
   for (void* p : {static_cast<void*>(s->perm), static_cast<void*>(s->slice_ptr),
-                  static_cast<void*>(s->col), static_cast<void*>(s->src), static_cast<void*>(s->val)})
+                  static_cast<void*>(s->col), static_cast<void*>(s->dcol), static_cast<void*>(s->src),
+                  static_cast<void*>(s->val)})
     if (p) cudaFreeAsync(p, 0);
   delete s;
 }
@@ -874,31 +937,36 @@ int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
   return EMG_SUCCESS;
 }
 
+// Launches KERNEL<mode> for the storage format of S: the bulk-copy pipeline
+// (mode 2, persistent grid + dynamic shared memory), 16-bit column offsets
+// (mode 1) or 32-bit columns (mode 0).
+#define EMG_LAUNCH_SPMV(KERNEL, S, g, st, ...)                            \
+  do {                                                                    \
+    if ((S).tma) {                                                        \
+      const SpmvShape sh_ = spmv_shape(S, g);                             \
+      KERNEL<2><<<sh_.grid, kThreads, sh_.smem, st>>>(__VA_ARGS__);       \
+    } else if ((S).narrow) {                                              \
+      KERNEL<1><<<g, kThreads, 0, st>>>(__VA_ARGS__);                     \
+    } else {                                                              \
+      KERNEL<0><<<g, kThreads, 0, st>>>(__VA_ARGS__);                     \
+    }                                                                     \
+  } while (0)
+
 void launch_iterations(DevCsr& A, bool bicg, int count) {
   KrylovWorkspace& w = *A.ws;
   const Sell S = *A.sell;
   const int g = w.grid;
-  const SpmvShape sh = spmv_shape(S, g);
   for (int c = 0; c < count; ++c) {
     if (!bicg) {
-      if (S.tma)
-        k_cg_spmv_dot<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.p, w.q, w.partial, w.state);
-      else
-        k_cg_spmv_dot<false><<<g, kThreads, 0, w.cap>>>(S, w.p, w.q, w.partial, w.state);
+      EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, w.cap, S, w.p, w.q, w.partial, w.state);
       k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                              w.hist, w.hist_cap);
       k_cg_direction<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
     } else {
       k_bi_p<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
-      if (S.tma)
-        k_bi_v<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
-      else
-        k_bi_v<false><<<g, kThreads, 0, w.cap>>>(S, w.p, w.v, w.rh, w.partial, w.state);
+      EMG_LAUNCH_SPMV(k_bi_v, S, g, w.cap, S, w.p, w.v, w.rh, w.partial, w.state);
       k_bi_s<<<g, kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
-      if (S.tma)
-        k_bi_t<true><<<sh.grid, kThreads, sh.smem, w.cap>>>(S, w.z, w.t, w.partial, w.state);
-      else
-        k_bi_t<false><<<g, kThreads, 0, w.cap>>>(S, w.z, w.t, w.partial, w.state);
+      EMG_LAUNCH_SPMV(k_bi_t, S, g, w.cap, S, w.z, w.t, w.partial, w.state);
       k_bi_x<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
                                         w.hist, w.hist_cap);
     }
@@ -1019,13 +1087,9 @@ int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
   const Sell& S = *A.sell;
   // the workspace vectors hold the permuted operands
   k_gather<<<g, kThreads, 0, st>>>(A.n, S.perm, x, A.ws->p);
-  const SpmvShape sh = spmv_shape(S, g);
   int32_t* err = &A.ws->state->copy_err;
   EMG_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
-  if (S.tma)
-    k_spmv<true><<<sh.grid, kThreads, sh.smem, st>>>(S, A.ws->p, A.ws->q, err);
-  else
-    k_spmv<false><<<g, kThreads, 0, st>>>(S, A.ws->p, A.ws->q, err);
+  EMG_LAUNCH_SPMV(k_spmv, S, g, st, S, A.ws->p, A.ws->q, err);
   k_scatter<<<g, kThreads, 0, st>>>(A.n, S.perm, A.ws->q, y);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -1067,12 +1131,7 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
   for (auto& e : ev) EMG_CK(cudaEventCreate(&e));
   for (int i = 0; i < iterations; ++i) {
     EMG_CK(cudaEventRecord(ev[4 * i], st));
-    if (S.tma) {
-      const SpmvShape sh = spmv_shape(S, g);
-      k_cg_spmv_dot<true><<<sh.grid, kThreads, sh.smem, st>>>(S, w.p, w.q, w.partial, w.state);
-    } else {
-      k_cg_spmv_dot<false><<<g, kThreads, 0, st>>>(S, w.p, w.q, w.partial, w.state);
-    }
+    EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, st, S, w.p, w.q, w.partial, w.state);
     EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
     k_cg_update<<<g, kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                         w.hist, w.hist_cap);
