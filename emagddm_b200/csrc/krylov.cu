@@ -113,8 +113,11 @@ __device__ __forceinline__ int64_t gstride() {
 #ifndef EMG_SELL_TMA
 #define EMG_SELL_TMA 0
 #endif
+// 16-bit column offsets (10 instead of 12 bytes per slot) when the matrix
+// bandwidth allows: fewer bytes, but measured slower than 32-bit columns on
+// B200 for the 64^3 curl-curl matrix, so off by default.
 #ifndef EMG_SELL_NARROW
-#define EMG_SELL_NARROW 1  // 16-bit column offsets when the matrix bandwidth allows
+#define EMG_SELL_NARROW 0
 #endif
 #ifndef EMG_SELL_UNROLL
 #define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
