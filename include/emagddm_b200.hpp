@@ -1,0 +1,247 @@
+// emagddm_b200.hpp -- header-only C++ adapters over the C ABI that mirror the
+// reference's classes on the TET4_EDGE solve path, so a C++ caller of
+//   fe_em::GlobalEdgeIDGenerator / fe_em::EMDOFManager   (src/fe_em/)
+//   numeric::EMAssembly                                  (src/numeric/em_assembly.cpp)
+//   numeric::CGSolver / numeric::BiCGSTABSolver          (src/numeric/iterative_solvers.cpp)
+// switches by type.  Same method names and argument meaning; errors follow
+// the reference: numbering misuse throws std::invalid_argument /
+// std::runtime_error, assemble() returns false with a message, solve()
+// never throws and reports through SolverResult::status.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "emagddm_b200.h"
+
+namespace emg {
+
+enum class SolverStatus : int {
+  SUCCESS = EMG_SUCCESS,
+  NUMERICAL_ERROR = EMG_NUMERICAL_ERROR,
+  DIVERGED = EMG_DIVERGED,
+  MAX_ITER_REACHED = EMG_MAX_ITER_REACHED,
+  INVALID_INPUT = EMG_INVALID_INPUT
+};
+
+// numeric::SolverResult (include/numeric/em_linear_solver.h:53-61)
+struct SolverResult {
+  std::vector<double> x;
+  SolverStatus status = SolverStatus::INVALID_INPUT;
+  int iterations = 0;
+  double residual_norm = 0.0;
+  double solve_time_ms = 0.0;
+  std::string error_msg;
+};
+
+inline std::string last_error() { return emg_last_error(); }
+
+// fe_em::EMMeshData restricted to the edge path: nodes (id = index), TET4_EDGE
+// elements with material ids, Dirichlet edge node pairs, hole-marker count.
+class Mesh {
+ public:
+  Mesh(std::vector<double> xyz, std::vector<int32_t> tets, std::vector<int32_t> material,
+       std::vector<int32_t> dirichlet_pairs, int32_t n_hole_markers = 0)
+      : xyz_(std::move(xyz)), tets_(std::move(tets)), material_(std::move(material)) {
+    const int rc = emg_mesh_create(static_cast<int64_t>(xyz_.size() / 3), xyz_.data(),
+                                   static_cast<int64_t>(tets_.size() / 4), tets_.data(),
+                                   material_.empty() ? nullptr : material_.data(),
+                                   static_cast<int64_t>(dirichlet_pairs.size() / 2),
+                                   dirichlet_pairs.empty() ? nullptr : dirichlet_pairs.data(),
+                                   n_hole_markers, &h_);
+    if (rc != EMG_SUCCESS) throw std::invalid_argument("emg_mesh_create: " + last_error());
+  }
+  ~Mesh() { emg_mesh_destroy(h_); }
+  Mesh(const Mesh&) = delete;
+  Mesh& operator=(const Mesh&) = delete;
+  emg_mesh handle() const { return h_; }
+  int64_t getNodeCount() const { return static_cast<int64_t>(xyz_.size() / 3); }
+  int64_t getElementCount() const { return static_cast<int64_t>(tets_.size() / 4); }
+  const std::vector<double>& xyz() const { return xyz_; }
+  const std::vector<int32_t>& tets() const { return tets_; }
+  const std::vector<int32_t>& material() const { return material_; }
+
+ private:
+  std::vector<double> xyz_;
+  std::vector<int32_t> tets_, material_;
+  emg_mesh h_ = nullptr;
+};
+
+// fe_em::GlobalEdgeIDGenerator (src/fe_em/global_edge_id_generator.cpp:30-140)
+class GlobalEdgeIDGenerator {
+ public:
+  explicit GlobalEdgeIDGenerator(const Mesh& mesh) : mesh_(mesh) {}
+  void generate() {
+    int64_t n = 0;
+    if (emg_edge_ids(mesh_.handle(), nullptr, nullptr, &n) != EMG_SUCCESS)
+      throw std::invalid_argument("GlobalEdgeIDGenerator::generate: " + last_error());
+    elem_edge_.resize(6 * mesh_.getElementCount());
+    edge_nodes_.resize(2 * n);
+    emg_edge_ids(mesh_.handle(), elem_edge_.data(), edge_nodes_.data(), &n);
+  }
+  int getNumGlobalEdges() const { return static_cast<int>(edge_nodes_.size() / 2); }
+  // element-major, 6 local edges per element (ElementGeometry TET4 order)
+  const std::vector<int32_t>& getElemLocalToGlobalEdge() const { return elem_edge_; }
+  const std::vector<int32_t>& getEdgeNodes() const { return edge_nodes_; }
+
+ private:
+  const Mesh& mesh_;
+  std::vector<int32_t> elem_edge_, edge_nodes_;
+};
+
+// fe_em::EMDOFManager (src/fe_em/em_dof_manager.cpp:29-626)
+class EMDOFManager {
+ public:
+  explicit EMDOFManager(const Mesh& mesh) : mesh_(mesh) {}
+  ~EMDOFManager() { emg_dofmap_destroy(map_); }
+  EMDOFManager(const EMDOFManager&) = delete;
+  EMDOFManager& operator=(const EMDOFManager&) = delete;
+  void build() { run(EMG_GAUGE_NONE); gauged_ = false; }
+  void applyTreeGauge(int32_t mode = EMG_GAUGE_REF) {
+    if (!map_) throw std::runtime_error("build() must be called before applyTreeGauge()");
+    if (gauged_) return;  // repeated calls are ignored, as in the reference
+    run(mode);
+    gauged_ = true;
+  }
+  int getNumFreeDOFs() const { return static_cast<int>(n_dofs_); }
+  const std::vector<int32_t>& getElemLocalToGlobal() const { return l2g_; }
+  const std::vector<int32_t>& getEdgeToDOF() const { return edge_dof_; }
+  std::vector<double> mapReducedSolutionToFull(const std::vector<double>& reduced) const {
+    std::vector<double> full(edge_dof_.size());
+    if (emg_dofmap_expand(map_, reduced.data(), full.data()) != EMG_SUCCESS)
+      throw std::invalid_argument("mapReducedSolutionToFull: " + last_error());
+    return full;
+  }
+
+ private:
+  void run(int32_t mode) {
+    emg_dofmap m = nullptr;
+    if (emg_dof_build(mesh_.handle(), mode, &m) != EMG_SUCCESS)
+      throw std::invalid_argument("EMDOFManager: " + last_error());
+    if (map_) emg_dofmap_destroy(map_);
+    map_ = m;
+    int64_t ne = 0, nf = 0;
+    emg_dofmap_info(map_, &ne, &nf, &n_dofs_);
+    l2g_.resize(6 * mesh_.getElementCount());
+    edge_dof_.resize(ne);
+    emg_dofmap_export(map_, l2g_.data(), edge_dof_.data());
+  }
+  const Mesh& mesh_;
+  emg_dofmap map_ = nullptr;
+  int64_t n_dofs_ = 0;
+  bool gauged_ = false;
+  std::vector<int32_t> l2g_, edge_dof_;
+};
+
+// numeric::EMAssembly for TET4_EDGE on the GPU (src/numeric/em_assembly.cpp:144-420).
+// Materials are reluctivity nu = 1/mu and conductivity sigma per material id.
+class GpuEMAssembly {
+ public:
+  ~GpuEMAssembly() { clear(); }
+  bool assemble(const Mesh& mesh, const std::vector<int32_t>& elem_local_to_global,
+                const std::vector<double>& nu, const std::vector<double>& sigma,
+                const std::vector<emg_source>& sources = {}, bool is_transient = false,
+                int32_t flags = 0) {
+    clear();
+    int rc = emg_system_create(mesh.getNodeCount(), mesh.xyz().data(), mesh.getElementCount(),
+                               mesh.tets().data(), mesh.material().empty() ? nullptr : mesh.material().data(),
+                               elem_local_to_global.data(), 0, nullptr, &sys_);
+    if (rc == EMG_SUCCESS)
+      rc = emg_system_assemble(sys_, nu.data(), sigma.empty() ? nullptr : sigma.data(),
+                               static_cast<int32_t>(nu.size()), sources.empty() ? nullptr : sources.data(),
+                               static_cast<int32_t>(sources.size()),
+                               flags | (is_transient ? EMG_FLAG_MASS : 0), nullptr);
+    if (rc != EMG_SUCCESS) {
+      error_ = last_error();
+      return false;
+    }
+    return true;
+  }
+  // Borrowed device matrix handles (valid while this object lives).
+  emg_csr getStiffnessMatrix() const { return emg_system_matrix(sys_, 0); }
+  emg_csr getMassMatrix() const { return emg_system_matrix(sys_, 1); }
+  std::vector<double> getSourceVector() const {
+    int64_t n = 0, nnz = 0;
+    emg_system_info(sys_, &n, &nnz);
+    std::vector<double> f(n);
+    emg_system_export(sys_, nullptr, nullptr, nullptr, nullptr, f.data());
+    return f;
+  }
+  int64_t rows() const {
+    int64_t n = 0, nnz = 0;
+    emg_system_info(sys_, &n, &nnz);
+    return n;
+  }
+  emg_system handle() const { return sys_; }
+  const std::string& error_message() const { return error_; }
+  void clear() {
+    emg_system_destroy(sys_);
+    sys_ = nullptr;
+  }
+
+ private:
+  emg_system sys_ = nullptr;
+  std::string error_;
+};
+
+// numeric::CGSolver / numeric::BiCGSTABSolver (iterative_solvers.cpp:64-503, :820-1118)
+template <bool kBiCG>
+class GpuKrylovSolver {
+ public:
+  explicit GpuKrylovSolver(double tolerance = 1e-8, int32_t max_iterations = 1000,
+                           bool jacobi = false)
+      : cfg_{tolerance, max_iterations, jacobi ? EMG_PRECOND_JACOBI : EMG_PRECOND_NONE} {}
+  ~GpuKrylovSolver() { clear(); }
+  // CsrMatrix<double> from host arrays (duplicates summed, as to_eigen does).
+  void set_matrix(int64_t n, const std::vector<int32_t>& row_ptr, const std::vector<int32_t>& col,
+                  const std::vector<double>& val) {
+    clear();
+    if (emg_csr_create(n, row_ptr.data(), col.data(), val.data(), nullptr, &owned_) != EMG_SUCCESS)
+      throw std::invalid_argument("set_matrix: " + last_error());
+    A_ = owned_;
+  }
+  // Device matrix of a GpuEMAssembly (borrowed).
+  void set_matrix(emg_csr device_matrix) {
+    clear();
+    A_ = device_matrix;
+  }
+  SolverResult solve(const std::vector<double>& b) {
+    SolverResult r;
+    if (!A_) {
+      r.error_msg = "matrix not set";
+      return r;
+    }
+    r.x.resize(b.size());
+    emg_result out{};
+    const int rc = kBiCG ? emg_bicgstab_solve(A_, b.data(), r.x.data(), &cfg_, &out)
+                         : emg_cg_solve(A_, b.data(), r.x.data(), &cfg_, &out);
+    r.status = static_cast<SolverStatus>(out.status <= EMG_INVALID_INPUT ? out.status : EMG_NUMERICAL_ERROR);
+    r.iterations = out.iterations;
+    r.residual_norm = out.residual_norm;
+    r.solve_time_ms = out.solve_time_ms;
+    if (rc > EMG_INVALID_INPUT) r.error_msg = last_error();
+    return r;
+  }
+  std::string get_solver_name() const {
+    return std::string(kBiCG ? "BiCGSTABSolver" : "CGSolver") +
+           (cfg_.preconditioner == EMG_PRECOND_JACOBI ? "_Jacobi" : "_None");
+  }
+  void clear() {
+    if (owned_) emg_csr_destroy(owned_);
+    owned_ = nullptr;
+    A_ = nullptr;
+  }
+
+ private:
+  emg_krylov_config cfg_;
+  emg_csr A_ = nullptr;
+  emg_csr owned_ = nullptr;
+};
+
+using GpuCGSolver = GpuKrylovSolver<false>;
+using GpuBiCGSTABSolver = GpuKrylovSolver<true>;
+
+}  // namespace emg

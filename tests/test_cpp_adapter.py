@@ -1,0 +1,49 @@
+"""The C++ adapters (include/emagddm_b200.hpp) driven by a C++ program that
+calls them the way a reference caller would (tests/cpp/solve_cube.cpp)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from emagddm_b200 import mesh
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "tests", "cpp", "solve_cube")
+
+
+def run(*args):
+    if not os.path.exists(EXE):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "emagddm_b200", "csrc"), "demo"])
+    out = subprocess.run([EXE, *map(str, args)], capture_output=True, text=True, timeout=600)
+    kv = dict(t.split("=", 1) for t in out.stdout.split() if "=" in t)
+    return out.returncode, kv
+
+
+@pytest.mark.parametrize("n", [2, 4, 7])
+def test_cpp_numbering_matches_oracle(n):
+    rc, kv = run(n, "--numbering-only")
+    assert rc == 0
+    m = mesh.plain_small(n)
+    o = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+    assert int(kv["edges"]) == o["n_edges"]
+    assert int(kv["free"]) == o["n_free"]
+    assert int(kv["dofs"]) == o["n_dofs"]
+    assert int(kv["l2g_sum"]) == int(o["l2g"].astype(np.int64).sum())
+
+
+@pytest.mark.gpu
+def test_cpp_chain_solution_matches_oracle(tmp_path):
+    n = 6
+    xfile = tmp_path / "x.bin"
+    rc, kv = run(n, "--x", xfile)
+    assert rc == 0, kv
+    assert kv["status"] == "0" and kv["solver"] == "CGSolver_Jacobi"
+    m = mesh.plain_small(n)
+    o = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+    rp, col, kv_, _, rhs = O.assemble(m, o["l2g"], o["n_dofs"])
+    xo, st, it, res = O.pcg(rp, col, kv_, rhs, tol=1e-10, max_iter=10000, precond=1)
+    x = np.fromfile(xfile, dtype=np.float64)
+    assert abs(int(kv["iterations"]) - it) <= max(3, 0.15 * it)
+    assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
