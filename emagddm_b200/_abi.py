@@ -74,6 +74,8 @@ SIGNATURES = {
     "emg_system_solve": ([H, C.c_int32, C.POINTER(KrylovConfig), VP, C.c_int32, VP,
                           C.POINTER(Result)], C.c_int),
     "emg_cg_kernel_times": ([H, C.c_int32, VP, VP], C.c_int),
+    "emg_cg_solve_noalloc": ([C.c_int64, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(KrylovConfig), VP,
+                              C.POINTER(Result)], C.c_int),
     "emg_csr_solver_format": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "emg_last_history": ([H, VP, C.c_int32], C.c_int),
 }

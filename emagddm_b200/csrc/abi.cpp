@@ -454,6 +454,19 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
   });
 }
 
+int emg_cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* row_ptr_d, const int32_t* col_d,
+                         const double* val_d, const double* b_d, double* x_d,
+                         const emg_krylov_config* cfg, void* stream, emg_result* out) {
+  return guarded([&]() -> int {
+    emg_result dummy;
+    if (!out) out = &dummy;
+    std::memset(out, 0, sizeof(*out));
+    out->status = EMG_INVALID_INPUT;
+    if (!cfg) { set_error("emg_cg_solve_noalloc: null config"); return EMG_INVALID_INPUT; }
+    return emg::cg_solve_noalloc(n, nnz, row_ptr_d, col_d, val_d, b_d, x_d, *cfg, as_stream(stream), out);
+  });
+}
+
 int emg_csr_solver_format(emg_csr A, int64_t* slots, int64_t* slices) {
   if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
   if (slots) *slots = emg::sell_slots(*A->csr);

@@ -79,6 +79,10 @@ int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_confi
 int csr_history(DevCsr& A, double* out, int32_t cap);
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
 void free_workspace(KrylovWorkspace* ws);
+// Allocation-free CG on a caller-owned device CSR (noalloc.cu).
+int cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* col, const double* val,
+                     const double* b, double* x, const emg_krylov_config& cfg, cudaStream_t st,
+                     emg_result* res);
 int64_t sell_slots(DevCsr& A);
 int64_t sell_slices(DevCsr& A);
 

@@ -195,6 +195,23 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
  * first solve. */
 int emg_csr_solver_format(emg_csr A, int64_t* slots, int64_t* slices);
 
+/* ---- Allocation-free CG (no counterpart in the reference) --------------
+ * For callers that must not let a library allocate GPU memory: applications
+ * that budget all device memory themselves, and loops that may not call the
+ * CUDA allocator after start-up (cudaMalloc/cudaFree synchronize the device
+ * and take unbounded time).  Same iteration, stopping and failure rules as
+ * emg_cg_solve_device, on a caller-owned merged CSR in device memory
+ * (row_ptr_d n+1, col_d/val_d nnz; b_d, x_d n).  Allocates nothing: the work
+ * vectors live in a fixed scratch array inside the library (about 10 MiB,
+ * held by every GPU that loads the library until exit), so n is limited to
+ * 262,144 rows; larger n returns EMG_INVALID_INPUT.  The first call on a
+ * device looks up the scratch address and should come before any stream
+ * capture.  Calls share the scratch: calls that overlap on the GPU (other
+ * streams or threads) race.  solve_time_ms is host wall time. */
+int emg_cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* row_ptr_d, const int32_t* col_d,
+                         const double* val_d, const double* b_d, double* x_d,
+                         const emg_krylov_config* cfg, void* stream, emg_result* out);
+
 /* Residual monitor of the last solve on A (ConvergenceHistory,
  * iterative_solvers.cpp:24-60): relative residual after every iteration, up
  * to cap entries; returns the number written. */
