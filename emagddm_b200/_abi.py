@@ -57,6 +57,7 @@ SIGNATURES = {
     "emg_system_create_device": ([C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, VP,
                                   C.POINTER(H)], C.c_int),
     "emg_system_assemble": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32, VP], C.c_int),
+    "emg_system_set_source_map": ([H, VP], C.c_int),
     "emg_system_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "emg_system_export": ([H, VP, VP, VP, VP, VP], C.c_int),
     "emg_system_matrix": ([H, C.c_int32], H),
@@ -74,6 +75,7 @@ SIGNATURES = {
     "emg_system_solve": ([H, C.c_int32, C.POINTER(KrylovConfig), VP, C.c_int32, VP,
                           C.POINTER(Result)], C.c_int),
     "emg_cg_kernel_times": ([H, C.c_int32, VP, VP], C.c_int),
+    "emg_batch_cg_solve_device": ([H, C.c_int32, VP, VP, VP, C.POINTER(KrylovConfig), VP, VP], C.c_int),
     "emg_cg_solve_noalloc": ([C.c_int64, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(KrylovConfig), VP,
                               C.POINTER(Result)], C.c_int),
     "emg_csr_solver_format": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),

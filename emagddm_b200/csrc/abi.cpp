@@ -262,6 +262,19 @@ int emg_system_assemble(emg_system sys, const double* nu, const double* sigma, i
   });
 }
 
+int emg_system_set_source_map(emg_system sys, const int32_t* tet_source) {
+  return guarded([&]() -> int {
+    if (!sys) { set_error("null system"); return EMG_INVALID_INPUT; }
+    emg::System& s = sys->s;
+    if (s.src_map) { EMG_CK(cudaFreeAsync(s.src_map, 0)); s.src_map = nullptr; }
+    if (!tet_source) return EMG_SUCCESS;
+    EMG_CK(cudaMallocAsync(&s.src_map, sizeof(int32_t) * s.n_tets, 0));
+    EMG_CK(cudaMemcpyAsync(s.src_map, tet_source, sizeof(int32_t) * s.n_tets, cudaMemcpyHostToDevice, 0));
+    EMG_CK(cudaStreamSynchronize(0));
+    return EMG_SUCCESS;
+  });
+}
+
 int emg_system_info(emg_system sys, int64_t* n_rows, int64_t* nnz) {
   if (!sys) { set_error("null system"); return EMG_INVALID_INPUT; }
   if (n_rows) *n_rows = sys->s.n;
@@ -451,6 +464,16 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
   return guarded([&]() -> int {
     if (!A || !A->csr) { set_error("null matrix"); return EMG_INVALID_INPUT; }
     return emg::cg_kernel_times(*A->csr, iterations, as_stream(stream), ms);
+  });
+}
+
+int emg_batch_cg_solve_device(emg_csr A, int32_t n_blocks, const int64_t* block_row_ptr,
+                              const double* b_d, double* x_d, const emg_krylov_config* cfg,
+                              void* stream, emg_result* results) {
+  return guarded([&]() -> int {
+    if (!A || !A->csr || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    return emg::batch_cg_solve(*A->csr, n_blocks, block_row_ptr, b_d, x_d, *cfg, as_stream(stream),
+                               results);
   });
 }
 

@@ -269,19 +269,22 @@ __device__ __forceinline__ bool load_tet(const int32_t* __restrict__ tets,
   return true;
 }
 
-__device__ __forceinline__ void source_at(const double* x, int n_src, double* js) {
+// Sum of the current densities of the regions tab[first .. first+count) that
+// contain x (open regions).
+__device__ __forceinline__ void source_at(const double* x, const emg_source* tab, int first, int count,
+                                          double* js) {
   js[0] = js[1] = js[2] = 0.0;
-  for (int s = 0; s < n_src; ++s) {
-    const double* p = c_src[s].p;
+  for (int s = first; s < first + count; ++s) {
+    const double* p = tab[s].p;
     bool in = false;
-    if (c_src[s].kind == EMG_SRC_BOX) {
+    if (tab[s].kind == EMG_SRC_BOX) {
       in = x[0] > p[0] && x[0] < p[1] && x[1] > p[2] && x[1] < p[3] && x[2] > p[4] && x[2] < p[5];
-    } else if (c_src[s].kind == EMG_SRC_ANNULUS_Z) {
+    } else if (tab[s].kind == EMG_SRC_ANNULUS_Z) {
       const double dx = x[0] - p[0], dy = x[1] - p[1];
       const double rr = sqrt(dx * dx + dy * dy);
       in = rr > p[2] && rr < p[3] && x[2] > p[4] && x[2] < p[5];
     }
-    if (in) { js[0] += c_src[s].j[0]; js[1] += c_src[s].j[1]; js[2] += c_src[s].j[2]; }
+    if (in) { js[0] += tab[s].j[0]; js[1] += tab[s].j[1]; js[2] += tab[s].j[2]; }
   }
 }
 
@@ -307,6 +310,8 @@ struct AsmArgs {
   const double* nu;
   const double* sigma;
   int32_t n_mat, n_src, flags;
+  const emg_source* src_tab;  // global source table when src_map is set
+  const int32_t* src_map;     // per-tet source index (-1 = none) or null
   double* kval;
   double* mval;
   double* rhs;
@@ -352,7 +357,15 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
       const double kf = nq * w * adet * A.nu[mid];
       const double sig = A.sigma ? A.sigma[mid] : 0.0;
       const bool do_mass = want_mass && sig > 0.0;
-      const bool do_src = A.n_src > 0;
+      const emg_source* tab = c_src;
+      int src_first = 0, src_count = A.n_src;
+      if (A.src_map) {
+        tab = A.src_tab;
+        const int32_t sid = A.src_map[t];
+        src_first = sid;
+        src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
+      }
+      const bool do_src = src_count > 0;
       int32_t cj[6];
       int32_t pos[6];
 #pragma unroll
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
               x[c] = T.x3[c] + lam[0] * T.d[0][c] + lam[1] * T.d[1][c] + lam[2] * T.d[2][c];
-            source_at(x, A.n_src, js);
+            source_at(x, tab, src_first, src_count, js);
             fi += w * adet * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
           }
         }
@@ -506,8 +519,8 @@ int system_build(System& s, cudaStream_t st) {
 int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_mat,
                     const emg_source* src, int32_t n_src, int32_t flags, cudaStream_t st) {
   if (n_mat <= 0 || !nu) { set_error("materials list is empty"); return EMG_INVALID_INPUT; }
-  if (n_src < 0 || n_src > kMaxSources || (n_src > 0 && !src)) {
-    set_error("between 0 and 16 source regions are supported");
+  if (n_src < 0 || (n_src > 0 && !src) || (!s.src_map && n_src > kMaxSources)) {
+    set_error("between 0 and 16 source regions are supported without a per-tet source map");
     return EMG_INVALID_INPUT;
   }
   for (int32_t k = 0; k < n_mat; ++k)
@@ -524,15 +537,21 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
   std::vector<double> h(2 * n_mat, 0.0);
   for (int32_t k = 0; k < n_mat; ++k) { h[k] = nu[k]; h[n_mat + k] = sigma ? sigma[k] : 0.0; }
   EMG_CK(cudaMemcpyAsync(mat, h.data(), sizeof(double) * 2 * n_mat, cudaMemcpyHostToDevice, st));
-  if (n_src > 0)
+  emg_source* src_tab = nullptr;
+  if (n_src > 0 && !s.src_map)
     EMG_CK(cudaMemcpyToSymbolAsync(c_src, src, sizeof(emg_source) * n_src, 0,
                                    cudaMemcpyHostToDevice, st));
+  if (n_src > 0 && s.src_map) {
+    EMG_CK(cudaMallocAsync(&src_tab, sizeof(emg_source) * n_src, st));
+    EMG_CK(cudaMemcpyAsync(src_tab, src, sizeof(emg_source) * n_src, cudaMemcpyHostToDevice, st));
+  }
   EMG_CK(cudaMemsetAsync(s.err, 0, sizeof(int32_t), st));
   AsmArgs a;
   a.n = s.n; a.n_nodes = s.n_nodes;
   a.row_ptr = s.K.row_ptr; a.col = s.K.col; a.inc_ptr = s.inc_ptr; a.inc = s.inc;
   a.tets = s.tets; a.xyz = s.xyz; a.material = s.material; a.l2g = s.l2g;
   a.nu = mat; a.sigma = mat + n_mat; a.n_mat = n_mat; a.n_src = n_src; a.flags = flags;
+  a.src_tab = src_tab; a.src_map = s.src_map;
   a.kval = s.K.val; a.mval = mass ? s.M.val : nullptr; a.rhs = s.rhs; a.err = s.err;
   k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
   EMG_CK(cudaGetLastError());
@@ -541,6 +560,7 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
   int32_t herr = 0;
   EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   EMG_CK(cudaFreeAsync(mat, st));
+  if (src_tab) EMG_CK(cudaFreeAsync(src_tab, st));
   EMG_CK(cudaStreamSynchronize(st));
   if (herr) { set_error("assembly:" + err_text(herr)); return EMG_INVALID_INPUT; }
   return EMG_SUCCESS;
@@ -551,7 +571,7 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
 System::~System() {
   for (void* p : {static_cast<void*>(xyz), static_cast<void*>(tets), static_cast<void*>(material),
                   static_cast<void*>(l2g), static_cast<void*>(inc_ptr), static_cast<void*>(inc),
-                  static_cast<void*>(err), static_cast<void*>(rhs)})
+                  static_cast<void*>(err), static_cast<void*>(rhs), static_cast<void*>(src_map)})
     if (p) cudaFreeAsync(p, 0);
 }
 

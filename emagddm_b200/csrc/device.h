@@ -23,6 +23,7 @@ void set_error(const std::string& msg);
 
 struct KrylovWorkspace;
 struct Sell;
+struct BatchPlan;
 
 // Device CSR matrix (int32 row_ptr / col, fp64 values, rows sorted, merged).
 // `version` changes whenever the values change (re-assembly), so derived
@@ -38,6 +39,7 @@ struct DevCsr {
   uint64_t version = 0;
   KrylovWorkspace* ws = nullptr;
   Sell* sell = nullptr;
+  BatchPlan* batch = nullptr;  // lockstep batch layout (batch.cu)
   ~DevCsr();
 };
 
@@ -52,6 +54,7 @@ struct System {
   int32_t* inc = nullptr;      // sorted slots 6 * t + k per row
   int32_t* err = nullptr;      // device error word
   double* rhs = nullptr;       // n
+  int32_t* src_map = nullptr;  // optional per-tet source index (n_tets)
   DevCsr K, M;                 // M shares K's pattern
   bool has_mass = false;
   ~System();
@@ -79,6 +82,10 @@ int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_confi
 int csr_history(DevCsr& A, double* out, int32_t cap);
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
 void free_workspace(KrylovWorkspace* ws);
+void free_batch(BatchPlan* p);
+// Lockstep CG over the diagonal blocks [blocks[k], blocks[k+1]) of A (batch.cu).
+int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks, const double* b, double* x,
+                   const emg_krylov_config& cfg, cudaStream_t st, emg_result* results);
 // Allocation-free CG on a caller-owned device CSR (noalloc.cu).
 int cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* col, const double* val,
                      const double* b, double* x, const emg_krylov_config& cfg, cudaStream_t st,

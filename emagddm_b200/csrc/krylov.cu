@@ -1204,6 +1204,7 @@ void free_workspace(KrylovWorkspace* w) {
 DevCsr::~DevCsr() {
   free_workspace(ws);
   free_sell(sell);
+  free_batch(batch);
   if (owns_pattern) {
     if (row_ptr) cudaFreeAsync(row_ptr, 0);
     if (col) cudaFreeAsync(col, 0);

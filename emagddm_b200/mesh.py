@@ -17,6 +17,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
+from functools import lru_cache
+
 import numpy as np
 
 KUHN = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6],
@@ -61,7 +63,14 @@ class CubeMesh:
 
 
 def cube_topology(n: int):
-    """Nodes, tets and boundary-face edge pairs of the n^3 Kuhn-split cube."""
+    """Nodes, tets and boundary-face edge pairs of the n^3 Kuhn-split cube
+    (fresh copies of a cached topology)."""
+    xyz, tets, dirichlet = _cube_topology(n)
+    return xyz.copy(), tets.copy(), dirichlet.copy()
+
+
+@lru_cache(maxsize=64)
+def _cube_topology(n: int):
     n1 = n + 1
     g = np.arange(n1, dtype=np.float64) / n
     kk, jj, ii = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")

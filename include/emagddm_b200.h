@@ -141,6 +141,11 @@ int emg_system_create_device(int64_t n_nodes, const double* xyz_d, int64_t n_tet
 int emg_system_assemble(emg_system sys, const double* nu_per_material,
                         const double* sigma_per_material, int32_t n_materials,
                         const emg_source* sources, int32_t n_sources, int32_t flags, void* stream);
+/* Per-tet source selection (host array of n_tets; NULL clears): with a map
+ * set, tet t evaluates only sources[tet_source[t]] (none when < 0) and the
+ * source table passed to emg_system_assemble may have any length.  Used to
+ * give every instance of a batched (block-diagonal) system its own source. */
+int emg_system_set_source_map(emg_system sys, const int32_t* tet_source);
 int emg_system_info(emg_system sys, int64_t* n_rows, int64_t* nnz);
 /* Copies to host; any pointer may be NULL.  row_ptr n+1, col/kval/mval nnz, rhs n. */
 int emg_system_export(emg_system sys, int32_t* row_ptr, int32_t* col, double* kval,
@@ -194,6 +199,20 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
  * stored slots including padding and number of 32-row slices; -1 before the
  * first solve. */
 int emg_csr_solver_format(emg_csr A, int64_t* slots, int64_t* slices);
+
+/* ---- Batched solves: many independent systems in one device loop ---------
+ * A is block diagonal: rows [block_row_ptr[k], block_row_ptr[k+1]) form
+ * system k and couple to no other block (checked; the union of disjoint
+ * meshes assembled as one system has exactly this form).  Every block runs
+ * CGSolver's Jacobi/plain CG (iterative_solvers.cpp:424-503) with its own
+ * scalars, statuses and iteration counts, in lockstep, as one CUDA graph.
+ * block_row_ptr is a host array of n_blocks+1; b_d/x_d are device vectors of
+ * A's size; results[k] (host, n_blocks) receives each block's outcome, with
+ * solve_time_ms = device time of the whole batch.  Returns EMG_SUCCESS when
+ * every block converged, else the first non-success block status. */
+int emg_batch_cg_solve_device(emg_csr A, int32_t n_blocks, const int64_t* block_row_ptr,
+                              const double* b_d, double* x_d, const emg_krylov_config* cfg,
+                              void* stream, emg_result* results);
 
 /* ---- Allocation-free CG (no counterpart in the reference) --------------
  * For callers that must not let a library allocate GPU memory: applications

@@ -1,0 +1,80 @@
+"""Batched many-instance solves: the union of disjoint instance meshes is one
+block-diagonal system solved in lockstep (emg_batch_cg_solve_device).
+Each block must match the oracle's solve of that instance alone:
+solutions to 1e-8 relative, matrices to 1e-12 of their scale."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from emagddm_b200 import _abi, batch, mesh
+from oracle import oracle as O
+
+CASES = [(3, 1), (5, 2), (4, 3), (6, 4), (2, 5), (7, 6), (3, 7)]
+
+
+def instances():
+    return [mesh.random_instance(n, s) for n, s in CASES]
+
+
+def test_batch_layout_cpu():
+    b = batch.build_batch(instances(), threads=2)
+    assert b.block_row_ptr[0] == 0 and len(b.block_row_ptr) == len(CASES) + 1
+    for k, (m, l) in enumerate(zip(b.instances, b.l2g_each)):
+        o = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+        np.testing.assert_array_equal(l, o["l2g"])
+        assert b.block_row_ptr[k + 1] - b.block_row_ptr[k] == int(o["l2g"].max()) + 1
+    assert b.l2g.max() + 1 == b.n_rows
+    assert len(b.sources) == len(CASES) and b.tet_source.max() == len(CASES) - 1
+    assert b.material.max() == len(b.nu) - 1
+    sizes = batch.instance_sizes(512)
+    assert min(sizes) >= 8 and max(sizes) <= 32 and len(set(sizes)) > 10
+
+
+@pytest.mark.gpu
+def test_batch_blocks_match_oracle():
+    import torch
+    b = batch.build_batch(instances(), threads=2)
+    S = batch.BatchSystem(b)
+    rp, col, kv, rhs = S.export()
+    x = torch.zeros(b.n_rows, dtype=torch.float64, device="cuda")
+    rc, res = S.solve(x.data_ptr(), tol=1e-12, max_iter=20000)
+    torch.cuda.synchronize()
+    assert rc == _abi.EMG_SUCCESS, (rc, res, _abi.lib().emg_last_error())
+    xs = x.cpu().numpy()
+    for k, m in enumerate(b.instances):
+        r0, r1 = b.block_row_ptr[k], b.block_row_ptr[k + 1]
+        l2g = b.l2g_each[k]
+        orp, ocol, okv, _, orhs = O.assemble(m, l2g, r1 - r0)
+        # the block of the batched matrix equals the instance's own matrix
+        blk = slice(rp[r0], rp[r1])
+        np.testing.assert_array_equal(rp[r0:r1 + 1] - rp[r0], orp)
+        np.testing.assert_array_equal(col[blk] - r0, ocol)
+        assert np.abs(kv[blk] - okv).max() <= 1e-12 * np.abs(okv).max()
+        assert np.abs(rhs[r0:r1] - orhs).max() <= 1e-12 * max(np.abs(orhs).max(), 1e-300)
+        xo, st, it, _ = O.pcg(orp, ocol, okv, orhs, tol=1e-12, max_iter=20000, precond=1)
+        assert res[k]["status"] == st == 0
+        assert abs(res[k]["iterations"] - it) <= max(3, 0.15 * it)
+        assert np.linalg.norm(xs[r0:r1] - xo) <= 1e-8 * max(np.linalg.norm(xo), 1e-300)
+
+
+@pytest.mark.gpu
+def test_batch_statuses_and_coupling_check():
+    import torch
+    b = batch.build_batch(instances()[:3], threads=2)
+    S = batch.BatchSystem(b)
+    x = torch.zeros(b.n_rows, dtype=torch.float64, device="cuda")
+    rc, res = S.solve(x.data_ptr(), tol=1e-14, max_iter=4)
+    assert rc == _abi.EMG_MAX_ITER_REACHED
+    assert all(r["status"] == _abi.EMG_MAX_ITER_REACHED and r["iterations"] == 4 for r in res)
+    # a partition that cuts through a block couples two "systems": rejected
+    L = _abi.lib()
+    bad = b.block_row_ptr.copy()
+    bad[1] += 1
+    out = (_abi.Result * 3)()
+    cfg = _abi.KrylovConfig(1e-8, 100, 1)
+    rc = L.emg_batch_cg_solve_device(L.emg_system_matrix(S.h, 0), 3, _abi.ptr(bad),
+                                     C.c_void_p(L.emg_system_rhs_device(S.h)), C.c_void_p(x.data_ptr()),
+                                     C.byref(cfg), None, out)
+    assert rc == _abi.EMG_INVALID_INPUT
+    assert b"couples" in L.emg_last_error()
