@@ -299,6 +299,22 @@ int emg_system_export(emg_system sys, int32_t* row_ptr, int32_t* col, double* kv
   });
 }
 
+int emg_system_combine(emg_system sys, double alpha, double beta, emg_csr* out) {
+  return guarded([&]() -> int {
+    if (!sys || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    const emg::System& s = sys->s;
+    if (!s.M.val) { set_error("mass matrix was not assembled (EMG_FLAG_MASS)"); return EMG_INVALID_INPUT; }
+    emg_csr h = nullptr;
+    int rc = csr_from_device(s.n, s.K.nnz, s.K.row_ptr, s.K.col, s.K.val, true, nullptr, &h);
+    if (rc) return rc;
+    rc = emg::axpby_values(h->csr->val, alpha, s.K.val, beta, s.M.val, s.K.nnz, nullptr);
+    if (rc) { emg_csr_destroy(h); return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
 emg_csr emg_system_matrix(emg_system sys, int32_t which) {
   if (!sys) return nullptr;
   if (which == 1) return sys->s.M.val ? &sys->m_handle : nullptr;

@@ -71,6 +71,9 @@ int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, 
 
 // Validates a device CSR (offsets, column range, ascending columns).
 int check_csr(int64_t n, const int32_t* rp, const int32_t* col, int64_t nnz, cudaStream_t st);
+// out = a x + b y (n values; ops.cu).
+int axpby_values(double* out, double a, const double* x, double b, const double* y, int64_t n,
+                 cudaStream_t st);
 // Keeps the default memory pool's freed blocks cached (once per device).
 void keep_pool_memory();
 

@@ -150,6 +150,11 @@ int emg_system_info(emg_system sys, int64_t* n_rows, int64_t* nnz);
 /* Copies to host; any pointer may be NULL.  row_ptr n+1, col/kval/mval nnz, rhs n. */
 int emg_system_export(emg_system sys, int32_t* row_ptr, int32_t* col, double* kval,
                       double* mval, double* rhs);
+/* Transient / eddy-current operator alpha*K + beta*M (e.g. K + M/dt for the
+ * sigma dA/dt term, magnetic_vector_3d_integrator.cpp:233-339) as a new,
+ * caller-owned device matrix on K's pattern (destroy with emg_csr_destroy).
+ * Needs a system assembled with EMG_FLAG_MASS. */
+int emg_system_combine(emg_system sys, double alpha, double beta, emg_csr* out);
 /* Borrowed handles / pointers, valid while the system lives. which: 0 K, 1 M. */
 emg_csr emg_system_matrix(emg_system sys, int32_t which);
 const double* emg_system_rhs_device(emg_system sys);

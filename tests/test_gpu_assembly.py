@@ -102,3 +102,40 @@ def test_invalid_material_rejected():
     s.nu = np.array([-1.0])
     with pytest.raises(_abi.EmgError):
         s.assemble()
+
+
+def test_transient_operator_and_bicgstab():
+    """K + M/dt (eddy-current time step) on K's pattern, solved with BiCGSTAB
+    and CG, against the oracle's assembly and solvers."""
+    import ctypes as C
+
+    from tests.helpers import lib, solve
+    m = mesh.plain_scale(6)
+    sigma = np.array([1.0, 5.0])
+    l2g = maps(m)
+    s = System(m, l2g, flags=_abi.FLAG_MASS, sigma=sigma)
+    dt = 0.05
+    h = C.c_void_p()
+    _abi.check(lib().emg_system_combine(s.h, 1.0, 1.0 / dt, C.byref(h)), "combine")
+    try:
+        orp, ocol, okv, omv, orhs = oracle_system(m, l2g, flags=_abi.FLAG_MASS, sigma=sigma)
+        A = okv + omv / dt
+        import torch
+        x = np.random.default_rng(3).normal(size=orhs.size)
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.empty_like(xd)
+        _abi.check(lib().emg_spmv(h, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), None), "spmv")
+        yo = O.spmv(orp, ocol, A, x)
+        assert np.abs(yd.cpu().numpy() - yo).max() <= 1e-12 * np.abs(yo).max()
+        for kind, pc in (("bicgstab", 0), ("cg", 1)):
+            x, out = solve(h, orhs, kind, tol=1e-11, max_iter=5000, precond=pc)
+            fn = O.bicgstab if kind == "bicgstab" else O.pcg
+            xo, st, it, _ = fn(orp, ocol, A, orhs, tol=1e-11, max_iter=5000, precond=pc)
+            assert out.status == st == 0
+            assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+    finally:
+        lib().emg_csr_destroy(h)
+    # without a mass matrix the combination is refused
+    s2 = System(m, l2g)
+    h2 = C.c_void_p()
+    assert lib().emg_system_combine(s2.h, 1.0, 1.0, C.byref(h2)) == _abi.EMG_INVALID_INPUT
