@@ -53,6 +53,9 @@ SIGNATURES = {
     "emg_dofmap_export": ([H, VP, VP], C.c_int),
     "emg_dofmap_expand": ([H, VP, VP], C.c_int),
     "emg_dofmap_destroy": ([H], None),
+    "emg_dof_build_partitioned": ([H, VP, C.c_int32, C.POINTER(H)], C.c_int),
+    "emg_dofmap_partition_info": ([H, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64), VP],
+                                  C.c_int),
     "emg_system_create": ([C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, VP, C.POINTER(H)], C.c_int),
     "emg_system_create_device": ([C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, VP,
                                   C.POINTER(H)], C.c_int),
@@ -81,6 +84,13 @@ SIGNATURES = {
                               C.POINTER(Result)], C.c_int),
     "emg_csr_solver_format": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "emg_last_history": ([H, VP, C.c_int32], C.c_int),
+    "emg_fetidp_plan_info": ([H, H, VP, C.c_int32], C.c_int),
+    "emg_fetidp_create": ([H, H, VP, C.POINTER(H)], C.c_int),
+    "emg_fetidp_factor": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32], C.c_int),
+    "emg_fetidp_solve": ([H, C.POINTER(KrylovConfig), VP, C.c_int32, C.POINTER(Result)], C.c_int),
+    "emg_fetidp_info": ([H, VP, C.c_int32], C.c_int),
+    "emg_fetidp_stats": ([H, VP, C.c_int32], C.c_int),
+    "emg_fetidp_destroy": ([H], None),
 }
 
 _LIB = None

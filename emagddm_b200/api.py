@@ -130,7 +130,7 @@ class _Mesh:
                                 ptr(self.material), d.shape[0], ptr(d) if d.size else None,
                                 mesh.hole_marker_count(), C.byref(self.h)), "emg_mesh_create")
 
-    def __del__(self):
+    def __del__(self, _abi=_abi):
         if getattr(self, "h", None) and _abi._LIB is not None:
             _abi._LIB.emg_mesh_destroy(self.h)
             self.h = None
@@ -228,7 +228,7 @@ class EMDOFManager:
         check(lib().emg_dofmap_expand(self._map, ptr(reduced), ptr(full)), "emg_dofmap_expand")
         return full
 
-    def __del__(self):
+    def __del__(self, _abi=_abi):
         if getattr(self, "_map", None) is not None and _abi._LIB is not None:
             _abi._LIB.emg_dofmap_destroy(self._map)
             self._map = None
@@ -307,7 +307,7 @@ class CsrMatrix:
                              C.c_void_p(torch.cuda.current_stream().cuda_stream)), "emg_spmv")
         return yd.cpu().numpy()
 
-    def __del__(self):
+    def __del__(self, _abi=_abi):
         if getattr(self, "_owned", False) and _abi._LIB is not None and self.h:
             _abi._LIB.emg_csr_destroy(self.h)
             self.h = None
@@ -406,7 +406,7 @@ class EMAssembly:
         self._sys = None
         self._host = None
 
-    def __del__(self):
+    def __del__(self, _abi=_abi):
         self.clear()
 
 

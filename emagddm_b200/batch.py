@@ -136,7 +136,7 @@ class BatchSystem:
                    "emg_system_export")
         return rp, col, kv, rhs
 
-    def __del__(self):
+    def __del__(self, _abi=_abi):
         if getattr(self, "h", None) and _abi._LIB is not None:
             _abi._LIB.emg_system_destroy(self.h)
             self.h = None

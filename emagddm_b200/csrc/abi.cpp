@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "device.h"
+#include "fetidp_dev.h"
 #include "internal.h"
 #include "trace.h"
 
@@ -23,6 +24,9 @@ struct emg_dofmap_t {
 struct emg_csr_t {
   emg::DevCsr* csr = nullptr;
   bool owned = true;
+};
+struct emg_fetidp_t {
+  emg::FetiDP fd;
 };
 struct emg_system_t {
   emg::System s;
@@ -147,6 +151,30 @@ int csr_from_device(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* co
   return EMG_SUCCESS;
 }
 
+void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
+  int64_t v[17] = {0};
+  v[0] = p.n_parts;
+  v[1] = p.n_dofs;
+  v[2] = p.n_union;
+  v[3] = p.n_lambda;
+  v[4] = p.n_coarse;
+  v[5] = static_cast<int64_t>(p.fronts.size());
+  v[6] = static_cast<int64_t>(p.level_ptr.size()) - 1;
+  v[7] = p.max_front;
+  v[8] = p.max_npiv;
+  v[9] = p.fac_size;
+  v[10] = p.upd_pool;
+  v[11] = p.root_off.empty() ? 0 : p.root_off.back();
+  for (int32_t s = 0; s < p.n_parts; ++s) {
+    v[12] += p.nI[s];
+    v[13] += p.nD[s];
+    v[14] += p.nP[s];
+    v[15] = std::max<int64_t>(v[15], p.nD[s]);
+  }
+  v[16] = p.max_children;
+  for (int32_t i = 0; i < n && i < 17; ++i) info[i] = v[i];
+}
+
 }  // namespace
 
 extern "C" {
@@ -237,6 +265,34 @@ int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full) {
 }
 
 void emg_dofmap_destroy(emg_dofmap map) { delete map; }
+
+int emg_dof_build_partitioned(emg_mesh mesh, const int32_t* tet_part, int32_t n_parts,
+                              emg_dofmap* out) {
+  return guarded([&]() -> int {
+    if (!mesh || !out) { set_error("null handle"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    auto* h = new emg_dofmap_t();
+    int rc = emg::build_dofmap_partitioned(mesh->m, tet_part, n_parts, h->d);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_dofmap_partition_info(emg_dofmap map, int32_t* n_parts, int64_t* n_primal,
+                              int64_t* n_primal_fix, int32_t* primal) {
+  if (!map) { set_error("null dofmap"); return EMG_INVALID_INPUT; }
+  const emg::DofMap& d = map->d;
+  if (d.n_parts < 1) { set_error("dofmap has no partition"); return EMG_INVALID_INPUT; }
+  if (n_parts) *n_parts = d.n_parts;
+  int64_t np = 0;
+  for (uint8_t f : d.dof_primal) np += f;
+  if (n_primal) *n_primal = np;
+  if (n_primal_fix) *n_primal_fix = d.n_primal_fix;
+  if (primal)
+    for (int64_t k = 0; k < d.n_dofs; ++k) primal[k] = d.dof_primal[k];
+  return EMG_SUCCESS;
+}
 
 int emg_system_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
                       const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
@@ -518,5 +574,74 @@ int emg_last_history(emg_csr A, double* residuals, int32_t cap) {
   int n = emg::csr_history(*A->csr, residuals, cap);
   return n < 0 ? 0 : n;
 }
+
+int emg_fetidp_plan_info(emg_mesh mesh, emg_dofmap map, int64_t* info, int32_t n_info) {
+  return guarded([&]() -> int {
+    if (!mesh || !map || (!info && n_info > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    emg::FetiPlan p;
+    int rc = emg::build_feti_plan(mesh->m, map->d, p);
+    if (rc) return rc;
+    feti_info(p, info, n_info);
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* out) {
+  return guarded([&]() -> int {
+    if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    emg::keep_pool_memory();
+    auto* h = new emg_fetidp_t();
+    int rc = h->fd.create(mesh->m, map->d, as_stream(stream));
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_fetidp_factor(emg_fetidp fd, const double* nu, const double* sigma, int32_t n_materials,
+                      const emg_source* sources, int32_t n_sources, int32_t flags) {
+  return guarded([&]() -> int {
+    if (!fd) { set_error("null FETI-DP handle"); return EMG_INVALID_INPUT; }
+    return fd->fd.factor(nu, sigma, n_materials, sources, n_sources, flags);
+  });
+}
+
+int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int32_t x_on_device,
+                     emg_result* out) {
+  return guarded([&]() -> int {
+    if (!fd || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    if (cfg->max_iterations < 0 || !(cfg->tolerance > 0.0)) {
+      set_error("bad tolerance or iteration limit");
+      return EMG_INVALID_INPUT;
+    }
+    emg_result r{};
+    int rc = fd->fd.solve(*cfg, x_on_device ? x : nullptr, &r);
+    if (rc == EMG_SUCCESS || rc == EMG_MAX_ITER_REACHED || rc == EMG_NUMERICAL_ERROR) {
+      if (x && !x_on_device) {
+        cudaError_t e = cudaMemcpy(x, fd->fd.xg_d, sizeof(double) * fd->fd.plan.n_dofs, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return EMG_ERR_CUDA; }
+      }
+      if (out) *out = r;
+    }
+    return rc;
+  });
+}
+
+int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info) {
+  if (!fd || (!info && n_info > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  feti_info(fd->fd.plan, info, n_info);
+  return EMG_SUCCESS;
+}
+
+int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats) {
+  if (!fd || (!stats && n_stats > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  const emg::FetiStats& s = fd->fd.stats;
+  const double v[5] = {s.factor_ms, s.solve_ms, static_cast<double>(s.iterations), s.lambda_residual, s.residual};
+  for (int32_t i = 0; i < n_stats && i < 5; ++i) stats[i] = v[i];
+  return EMG_SUCCESS;
+}
+
+void emg_fetidp_destroy(emg_fetidp fd) { delete fd; }
 
 }  // extern "C"

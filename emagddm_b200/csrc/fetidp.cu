@@ -1,0 +1,1227 @@
+// fetidp.cu -- FETI-DP on one GPU: numeric factorization of every subdomain's
+// K_rr (multifrontal, batched over all subdomains level by level), the dense
+// Dirichlet Schur complements S_DD and their inverse Cholesky factors, the
+// primal coarse problem, the lambda-PCG and the recovery of the primal
+// solution.  No reference counterpart exists: the reference's FETI-DP layer
+// (include/fetidp/fetidp_context.hpp:20-66) declares the context only.
+//
+// Formulation (per subdomain s; B_s = +-1 on its dual DOFs, R_s = coarse
+// restriction, Phi_s = K_rr^-1 K_rP):
+//   S_cc = sum_s R_s^T (K_PP - K_Pr Phi_s) R_s          (coarse matrix)
+//   G    = sum_s B_s Phi_s R_s,  F_rr = sum_s B_s K_rr^-1 B_s^T
+//   (F_rr + G S_cc^-1 G^T) lambda = d - G S_cc^-1 g_c,
+//   d = sum_s B_s K_rr^-1 f_r,  g_c = sum_s R_s^T (f_P - K_Pr K_rr^-1 f_r)
+// and, because B_s touches only the dual rows and the duals are eliminated
+// last, (K_rr^-1)_DD = S_DD^-1 = L^-T L^-1 with L the root front's Cholesky
+// factor: every lambda iteration is batched dense triangular mat-vecs with
+// L^-1 plus the Dirichlet preconditioner sum_s B_Ds S_DD B_Ds^T (stiffness
+// scaled), all HBM-bound.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "common.cuh"
+#include "device.h"
+#include "fetidp.h"
+#include "fetidp_dev.h"
+#include "trace.h"
+
+namespace emg {
+namespace {
+
+constexpr int kNB = 32;       // panel width of the partial Cholesky
+constexpr int kTile = 64;     // output tile of the rank-k updates
+constexpr int kKC = 32;       // k-chunk of the rank-k updates
+constexpr int kTrsmRows = 128;
+
+enum : int32_t { kErrPivot = 1, kErrAsm = 2 };
+
+// ---------------------------------------------------------------- assembly
+
+__global__ void k_front_zero(FrontsDev F, int32_t f0, double* __restrict__ fac, double* __restrict__ upd) {
+  const int32_t k = f0 + blockIdx.y;
+  const int64_t n1 = static_cast<int64_t>(F.f[k]) * F.npiv[k];
+  const int64_t nu = F.f[k] - F.npiv[k];
+  const int64_t n2 = nu * nu;
+  double* a = fac + F.fac[k];
+  double* b = n2 > 0 ? upd + F.upd[k] : nullptr;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n1 + n2;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (i < n1) a[i] = 0.0;
+    else b[i - n1] = 0.0;
+  }
+}
+
+__device__ __forceinline__ int32_t find_row(const int32_t* __restrict__ r, int32_t n, int32_t v) {
+  int32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (r[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return (lo < n && r[lo] == v) ? lo : -1;
+}
+
+// Pivot rows of a front take the union-CSR entries (j >= i, j in r) of their
+// subdomain row: F[pos(j), i - p0] = K(i, j).  One warp per pivot row.
+__global__ void k_front_scatter(FrontsDev F, int32_t f0, const int64_t* __restrict__ loc_off,
+                                const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
+                                const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                const double* __restrict__ val, double* __restrict__ fac,
+                                int32_t* __restrict__ err) {
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t lane = threadIdx.x & 31;
+  const int32_t a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int32_t np = F.npiv[k];
+  if (a >= np) return;
+  const int32_t s = F.sub[k], p0 = F.p0[k], fs = F.f[k];
+  const int64_t base = loc_off[s];
+  const int32_t nr = nI[s] + nD[s];
+  const int32_t i = p0 + a;
+  const int64_t u = base + i;
+  const int32_t* rows = F.rows_v + F.rows[k];
+  double* col_a = fac + F.fac[k] + static_cast<int64_t>(a) * fs;
+  for (int32_t q = rp[u] + lane; q < rp[u + 1]; q += 32) {
+    const int32_t j = static_cast<int32_t>(col[q] - base);
+    if (j < i || j >= nr) continue;
+    const int32_t pj = j < p0 + np ? j - p0 : find_row(rows, fs, j);
+    if (pj < 0) { atomicOr(err, kErrAsm); continue; }
+    col_a[pj] = val[q];
+  }
+}
+
+// Extend-add of every level front's `slot`-th child update block (lower part)
+// into the front: columns left of npiv go to the factor block, the rest to the
+// front's own update block.  One child per front per launch, so no two
+// threads add into the same entry.
+__global__ void k_extend_add(FrontsDev F, int32_t f0, int32_t slot, double* __restrict__ fac,
+                             double* __restrict__ upd) {
+  const int32_t k = f0 + blockIdx.y;
+  if (slot >= F.nchild[k]) return;
+  const int32_t c = F.child_v[F.child0[k] + slot];
+  const int32_t nc = F.f[c] - F.npiv[c];
+  const int32_t fp = F.f[k], np = F.npiv[k], nup = fp - np;
+  const double* U = upd + F.upd[c];
+  const int32_t* cp = F.cpos_v + F.cpos[c];
+  double* A = fac + F.fac[k];
+  double* B = nup > 0 ? upd + F.upd[k] : nullptr;
+  const int64_t tot = static_cast<int64_t>(nc) * nc;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t j = static_cast<int32_t>(e / nc), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * nc);
+    if (i < j) continue;
+    const int32_t ri = cp[i], rj = cp[j];
+    const double v = U[e];
+    if (rj < np) A[ri + static_cast<int64_t>(rj) * fp] += v;
+    else B[(ri - np) + static_cast<int64_t>(rj - np) * nup] += v;
+  }
+}
+
+// Root fronts: keep the assembled S_DD (symmetrised, full) before factoring.
+__global__ void k_copy_roots(FrontsDev F, int32_t f0, const int64_t* __restrict__ root_off,
+                             const double* __restrict__ fac, double* __restrict__ S) {
+  const int32_t k = f0 + blockIdx.y;
+  if (!F.is_root[k]) return;
+  const int32_t n = F.npiv[k];
+  const double* A = fac + F.fac[k];
+  double* out = S + root_off[F.sub[k]];
+  const int64_t tot = static_cast<int64_t>(n) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t j = static_cast<int32_t>(e / n), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * n);
+    out[e] = i >= j ? A[e] : A[j + static_cast<int64_t>(i) * n];
+  }
+}
+
+// ----------------------------------------------------- partial Cholesky
+
+// Diagonal block [k0, k0+nb) of every front in the range with npiv > k0.
+__global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
+                                                    int32_t* __restrict__ err) {
+  __shared__ double D[kNB][kNB + 1];
+  __shared__ double piv;
+  const int32_t k = f0 + blockIdx.x;
+  const int32_t np = F.npiv[k];
+  if (k0 >= np) return;
+  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
+  double* A = fac + F.fac[k] + k0 + static_cast<int64_t>(k0) * fs;
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int c = e / nb, r = e - c * nb;
+    D[r][c] = r >= c ? A[r + static_cast<int64_t>(c) * fs] : 0.0;
+  }
+  __syncthreads();
+  for (int c = 0; c < nb; ++c) {
+    if (threadIdx.x == 0) {
+      double d = D[c][c];
+      if (!(d > 0.0)) { atomicOr(err, kErrPivot); d = 1.0; }
+      piv = sqrt(d);
+      D[c][c] = piv;
+    }
+    __syncthreads();
+    for (int r = c + 1 + threadIdx.x; r < nb; r += blockDim.x) D[r][c] /= piv;
+    __syncthreads();
+    const int m = nb - c - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int q = c + 1 + e / m, r = c + 1 + e % m;
+      if (r >= q) D[r][q] -= D[r][c] * D[q][c];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int c = e / nb, r = e - c * nb;
+    if (r >= c) A[r + static_cast<int64_t>(c) * fs] = D[r][c];
+  }
+}
+
+// Panel rows below the diagonal block: X L_kk^T = F[i, k0:k0+nb].
+__global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(FrontsDev F, int32_t f0, int32_t k0,
+                                                          double* __restrict__ fac) {
+  __shared__ double D[kNB][kNB + 1];
+  __shared__ double X[kNB][kTrsmRows];
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k];
+  if (k0 >= np) return;
+  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
+  const int32_t r0 = k0 + nb + blockIdx.x * kTrsmRows;
+  if (r0 >= fs) return;
+  double* A = fac + F.fac[k];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int c = e / nb, r = e - c * nb;
+    D[r][c] = A[(k0 + r) + static_cast<int64_t>(k0 + c) * fs];
+  }
+  const int32_t i = r0 + threadIdx.x;
+  const bool live = i < fs;
+  for (int c = 0; c < nb; ++c) X[c][threadIdx.x] = live ? A[i + static_cast<int64_t>(k0 + c) * fs] : 0.0;
+  __syncthreads();
+  for (int c = 0; c < nb; ++c) {
+    double v = X[c][threadIdx.x];
+    for (int q = 0; q < c; ++q) v -= X[q][threadIdx.x] * D[c][q];
+    X[c][threadIdx.x] = v / D[c][c];
+  }
+  if (live)
+    for (int c = 0; c < nb; ++c) A[i + static_cast<int64_t>(k0 + c) * fs] = X[c][threadIdx.x];
+}
+
+// C[0:mr, 0:mc] -= A[0:mr, 0:K] * B[0:mc, 0:K]^T for one 64x64 tile; A, B, C
+// column-major.  Thread (tx, ty) owns rows 4*tx .. +3 and columns 4*ty .. +3.
+__device__ __forceinline__ void tile_update(double* __restrict__ C, int64_t ldc, int mr, int mc,
+                                            const double* __restrict__ A, int64_t lda,
+                                            const double* __restrict__ B, int64_t ldb, int K,
+                                            double (*As)[kTile + 1], double (*Bs)[kTile + 1]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < K; kc += kKC) {
+    const int kw = min(kKC, K - kc);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kKC * kTile; e += blockDim.x) {
+      const int c = e / kTile, r = e - c * kTile;
+      const bool ok = c < kw;
+      As[c][r] = (ok && r < mr) ? A[r + static_cast<int64_t>(kc + c) * lda] : 0.0;
+      Bs[c][r] = (ok && r < mc) ? B[r + static_cast<int64_t>(kc + c) * ldb] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int c = 0; c < kKC; ++c) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) { a[q] = As[c][4 * tx + q]; b[q] = Bs[c][4 * ty + q]; }
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+    }
+  }
+#pragma unroll
+  for (int y = 0; y < 4; ++y) {
+    const int cc = 4 * ty + y;
+    if (cc >= mc) continue;
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      const int rr = 4 * tx + x;
+      if (rr < mr) C[rr + static_cast<int64_t>(cc) * ldc] -= acc[x][y];
+    }
+  }
+}
+
+// Right-looking update of the remaining pivot columns [k0+nb, npiv), rows >= column.
+__global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0, int32_t k0,
+                                                        double* __restrict__ fac) {
+  __shared__ double As[kKC][kTile + 1];
+  __shared__ double Bs[kKC][kTile + 1];
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k];
+  if (k0 >= np) return;
+  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
+  const int32_t c0 = k0 + nb;
+  if (c0 >= np) return;
+  const int32_t nct = (np - c0 + kTile - 1) / kTile, nrt = (fs - c0 + kTile - 1) / kTile;
+  const int32_t t = blockIdx.x;
+  if (t >= nct * nrt) return;
+  const int32_t tc = t % nct, tr = t / nct;
+  const int32_t cs = c0 + tc * kTile, rs = c0 + tr * kTile;
+  if (rs + kTile <= cs) return;  // strictly above the diagonal
+  const int mc = min(kTile, np - cs), mr = min(kTile, fs - rs);
+  double* A = fac + F.fac[k];
+  tile_update(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
+              A + cs + static_cast<int64_t>(k0) * fs, fs, nb, As, Bs);
+}
+
+// Update block: U -= L21 L21^T (lower tiles), K = npiv.
+__global__ void __launch_bounds__(256) k_syrk_update(FrontsDev F, int32_t f0, const double* __restrict__ fac,
+                                                     double* __restrict__ upd) {
+  __shared__ double As[kKC][kTile + 1];
+  __shared__ double Bs[kKC][kTile + 1];
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np;
+  if (nu <= 0) return;
+  const int32_t nt = (nu + kTile - 1) / kTile;
+  const int32_t t = blockIdx.x;
+  if (t >= nt * (nt + 1) / 2) return;
+  // t -> lower tile (tr >= tc), t = tr (tr + 1) / 2 + tc
+  int32_t tr = static_cast<int32_t>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((tr + 1) * (tr + 2) / 2 <= t) ++tr;
+  while (tr * (tr + 1) / 2 > t) --tr;
+  const int32_t tc = t - tr * (tr + 1) / 2;
+  const int32_t rs = tr * kTile, cs = tc * kTile;
+  const int mr = min(kTile, nu - rs), mc = min(kTile, nu - cs);
+  const double* L = fac + F.fac[k];
+  double* U = upd + F.upd[k];
+  tile_update(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, As, Bs);
+}
+
+// --------------------------------------------------- triangular inverse
+
+// X = L^-1 for a list of lower-triangular matrices (column-major, ld n).
+// One warp per column c: forward substitution of L x = e_c in place in X.
+__global__ void __launch_bounds__(512) k_trtri(int32_t n_mat, const int32_t* __restrict__ dim,
+                                               const int64_t* __restrict__ l_off, const int64_t* __restrict__ x_off,
+                                               const double* __restrict__ Lbase, double* __restrict__ Xbase) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m];
+  const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= n) return;
+  const int lane = threadIdx.x & 31;
+  const double* L = Lbase + l_off[m];
+  double* x = Xbase + x_off[m] + static_cast<int64_t>(c) * n;
+  for (int32_t i = lane; i < n; i += 32) x[i] = i == c ? 1.0 : 0.0;
+  __syncwarp();
+  for (int32_t j = c; j < n; ++j) {
+    const double* Lj = L + static_cast<int64_t>(j) * n;
+    const double xj = x[j] / Lj[j];
+    __syncwarp();
+    if (lane == 0) x[j] = xj;
+    for (int32_t i = j + 1 + lane; i < n; i += 32) x[i] -= Lj[i] * xj;
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------ multifrontal solve
+
+// Forward sweep, one warp per (front, right-hand-side column): add the
+// children's update vectors, eliminate the pivots, leave this front's update
+// vector for the parent.
+__global__ void k_front_fwd(FrontsDev F, int32_t f0, RhsDev R, const int32_t* __restrict__ nI,
+                            const int32_t* __restrict__ nD, const double* __restrict__ fac) {
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t s = F.sub[k];
+  const int32_t col = blockIdx.x;
+  if (col >= R.ncol[s]) return;
+  const int lane = threadIdx.x;
+  const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
+  const int32_t ld = nI[s] + nD[s];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
+  for (int32_t i = lane; i < nu; i += 32) V[i] = 0.0;
+  __syncwarp();
+  for (int32_t ci = 0; ci < F.nchild[k]; ++ci) {
+    const int32_t c = F.child_v[F.child0[k] + ci];
+    const int32_t ncu = F.f[c] - F.npiv[c];
+    const double* Vc = R.v + R.voff[c] + static_cast<int64_t>(col) * ncu;
+    const int32_t* cp = F.cpos_v + F.cpos[c];
+    for (int32_t a = lane; a < ncu; a += 32) {
+      const int32_t r = cp[a];
+      if (r < np) x[p0 + r] += Vc[a];
+      else V[r - np] += Vc[a];
+    }
+    __syncwarp();
+  }
+  const double* L = fac + F.fac[k];
+  for (int32_t j = 0; j < np; ++j) {
+    const double* Lj = L + static_cast<int64_t>(j) * fs;
+    const double yj = x[p0 + j] / Lj[j];
+    __syncwarp();
+    if (lane == 0) x[p0 + j] = yj;
+    for (int32_t i = j + 1 + lane; i < fs; i += 32) {
+      const double t = Lj[i] * yj;
+      if (i < np) x[p0 + i] -= t;
+      else V[i - np] -= t;
+    }
+    __syncwarp();
+  }
+}
+
+// Backward sweep: x_piv = L11^-T (y_piv - L21^T x_border), border values final.
+__global__ void k_front_bwd(FrontsDev F, int32_t f0, RhsDev R, const int32_t* __restrict__ nI,
+                            const int32_t* __restrict__ nD, const double* __restrict__ fac) {
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t s = F.sub[k];
+  const int32_t col = blockIdx.x;
+  if (col >= R.ncol[s]) return;
+  const int lane = threadIdx.x;
+  const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
+  const int32_t ld = nI[s] + nD[s];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  const int32_t* rows = F.rows_v + F.rows[k];
+  const double* L = fac + F.fac[k];
+  for (int32_t j = np - 1; j >= 0; --j) {
+    const double* Lj = L + static_cast<int64_t>(j) * fs;
+    double acc = 0.0;
+    for (int32_t i = j + 1 + lane; i < fs; i += 32) acc += Lj[i] * x[i < np ? p0 + i : rows[i]];
+    acc = warp_sum(acc);
+    if (lane == 0) x[p0 + j] = (x[p0 + j] - acc) / Lj[j];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------- right-hand sides, coarse
+
+// Setup right-hand sides of subdomain s: columns 0..nP-1 = K_rP, column nP = f_r.
+__global__ void k_setup_rhs(const int64_t* __restrict__ loc_off, const int32_t* __restrict__ nI,
+                            const int32_t* __restrict__ nD, const int32_t* __restrict__ nP,
+                            const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                            const double* __restrict__ val, const double* __restrict__ frhs, RhsDev R) {
+  const int32_t s = blockIdx.y;
+  const int32_t nr = nI[s] + nD[s];
+  const int64_t base = loc_off[s];
+  double* x = R.x + R.off[s];
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x) {
+    const int64_t u = base + i;
+    for (int32_t q = rp[u]; q < rp[u + 1]; ++q) {
+      const int32_t j = static_cast<int32_t>(col[q] - base);
+      if (j >= nr) x[i + static_cast<int64_t>(j - nr) * nr] = val[q];
+    }
+    x[i + static_cast<int64_t>(nP[s]) * nr] = frhs[u];
+  }
+}
+
+// Coarse block C_s[p, q] = K_PP(p, q) - K_Pr Phi[:, q] and h_s[p] = f_P(p) - K_Pr z.
+// One warp per (p, q); q == nP means the h entry.
+__global__ void k_coarse_blocks(const int64_t* __restrict__ loc_off, const int32_t* __restrict__ nI,
+                                const int32_t* __restrict__ nD, const int32_t* __restrict__ nP,
+                                const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                const double* __restrict__ val, const double* __restrict__ frhs, RhsDev R,
+                                const int64_t* __restrict__ cblk_off, const int64_t* __restrict__ pri_off,
+                                double* __restrict__ cblk, double* __restrict__ h) {
+  const int32_t s = blockIdx.y;
+  const int32_t np = nP[s];
+  const int32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= np * (np + 1)) return;
+  const int32_t p = w % np, q = w / np;
+  const int lane = threadIdx.x & 31;
+  const int32_t nr = nI[s] + nD[s];
+  const int64_t base = loc_off[s];
+  const int64_t u = base + nr + p;
+  const double* phi = R.x + R.off[s] + static_cast<int64_t>(q) * nr;
+  double acc = 0.0;
+  for (int32_t e = rp[u] + lane; e < rp[u + 1]; e += 32) {
+    const int32_t j = static_cast<int32_t>(col[e] - base);
+    if (j < nr) acc -= val[e] * phi[j];
+    else if (q < np && j - nr == q) acc += val[e];
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) {
+    if (q < np) cblk[cblk_off[s] + p + static_cast<int64_t>(q) * np] = acc;
+    else h[pri_off[s] + p] = frhs[u] + acc;
+  }
+}
+
+template <class I>
+__global__ void k_gather_sum(int64_t n, const int64_t* __restrict__ ptr, const I* __restrict__ list,
+                             const double* __restrict__ src, double* __restrict__ out) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t q = ptr[t]; q < ptr[t + 1]; ++q) acc += src[list[q]];
+    out[t] = acc;
+  }
+}
+
+// Stiffness-scaling weight of every dual entry: rho_other / (rho_self + rho_other),
+// rho = the subdomain matrix's diagonal at the dual DOF.
+__global__ void k_dual_weights(const int64_t* __restrict__ loc_off, const int32_t* __restrict__ nI,
+                               const int64_t* __restrict__ dual_off, const int32_t* __restrict__ dual_lam,
+                               const int32_t* __restrict__ dual_sign, const int32_t* __restrict__ lam_entry,
+                               const int32_t* __restrict__ dual_sub, const int32_t* __restrict__ rp,
+                               const int32_t* __restrict__ col, const double* __restrict__ val,
+                               int64_t n_entries, double* __restrict__ rho, double* __restrict__ wt, int pass) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n_entries;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (pass == 0) {
+      const int32_t s = dual_sub[e];
+      const int64_t u = loc_off[s] + nI[s] + (e - dual_off[s]);
+      double d = 0.0;
+      for (int32_t q = rp[u]; q < rp[u + 1]; ++q)
+        if (col[q] == u) d = val[q];
+      rho[e] = fabs(d);
+    } else {
+      const int64_t l = dual_lam[e];
+      const int32_t o = lam_entry[2 * l + (dual_sign[e] > 0 ? 1 : 0)];
+      const double a = rho[e], b = rho[o];
+      wt[e] = (a + b) > 0.0 ? b / (a + b) : 0.5;
+    }
+  }
+}
+
+// ------------------------------------------------------ lambda operators
+
+// w[e] = sign * scale[e] * lam[dual_lam[e]]  (scale may be null)
+__global__ void k_dual_gather(int64_t ne, const int32_t* __restrict__ dual_lam, const int32_t* __restrict__ sign,
+                              const double* __restrict__ scale, const double* __restrict__ lam,
+                              double* __restrict__ w) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < ne;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double v = sign[e] * lam[dual_lam[e]];
+    if (scale) v *= scale[e];
+    w[e] = v;
+  }
+}
+
+// out[l] = sum over the two sides of sign * scale * y  (B_s y_s assembled),
+// plus the per-block partial of dot(out, a) when part != null.
+__global__ void __launch_bounds__(256) k_lambda_scatter(int64_t nl, const int32_t* __restrict__ lam_entry,
+                                                        const double* __restrict__ scale,
+                                                        const double* __restrict__ y, double* __restrict__ out,
+                                                        const double* __restrict__ a, double* __restrict__ part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (int64_t l = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; l < nl;
+       l += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t ep = lam_entry[2 * l], em = lam_entry[2 * l + 1];
+    const double v = scale ? scale[ep] * y[ep] - scale[em] * y[em] : y[ep] - y[em];
+    out[l] = v;
+    if (a) acc += v * a[l];
+  }
+  if (part) {
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  }
+}
+
+// Row-parallel mat-vec of dense per-subdomain blocks: y_m = M_m w_m with M_m
+// column-major n x n; lower != 0 uses only j <= i (y = tril(M) w).
+__global__ void __launch_bounds__(128) k_block_gemv(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                    const int64_t* __restrict__ m_off, const double* __restrict__ M,
+                                                    const int64_t* __restrict__ v_off, const double* __restrict__ w,
+                                                    double* __restrict__ y, int lower) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m];
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* wm = w + v_off[m];
+  const double* Mi = M + m_off[m] + i;
+  const int32_t jend = lower ? i + 1 : n;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int32_t j = 0;
+  for (; j + 4 <= jend; j += 4) {
+    a0 = fma(Mi[static_cast<int64_t>(j) * n], __ldg(wm + j), a0);
+    a1 = fma(Mi[static_cast<int64_t>(j + 1) * n], __ldg(wm + j + 1), a1);
+    a2 = fma(Mi[static_cast<int64_t>(j + 2) * n], __ldg(wm + j + 2), a2);
+    a3 = fma(Mi[static_cast<int64_t>(j + 3) * n], __ldg(wm + j + 3), a3);
+  }
+  for (; j < jend; ++j) a0 = fma(Mi[static_cast<int64_t>(j) * n], __ldg(wm + j), a0);
+  y[v_off[m] + i] = (a0 + a1) + (a2 + a3);
+}
+
+// Column-parallel transposed mat-vec over the lower triangle: y_j = sum_{i>=j} M[i, j] w_i.
+__global__ void __launch_bounds__(256) k_block_gemv_lt(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                       const int64_t* __restrict__ m_off,
+                                                       const double* __restrict__ M,
+                                                       const int64_t* __restrict__ v_off,
+                                                       const double* __restrict__ w, double* __restrict__ y) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m];
+  const int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const int lane = threadIdx.x & 31;
+  const double* Mj = M + m_off[m] + static_cast<int64_t>(j) * n;
+  const double* wm = w + v_off[m];
+  double acc = 0.0;
+  for (int32_t i = j + lane; i < n; i += 32) acc = fma(Mj[i], wm[i], acc);
+  acc = warp_sum(acc);
+  if (lane == 0) y[v_off[m] + j] = acc;
+}
+
+// t[P] = add[P] + sum over the primal entries (s, p) of coarse DOF P of Phi_D[:, p] . w_s
+__global__ void k_coarse_apply_t(int32_t nc, const int64_t* __restrict__ coarse_ptr,
+                                 const int32_t* __restrict__ coarse_list, const int32_t* __restrict__ pri_sub,
+                                 const int64_t* __restrict__ pri_off, const int32_t* __restrict__ nI,
+                                 const int32_t* __restrict__ nD, const int64_t* __restrict__ dual_off, RhsDev R,
+                                 const double* __restrict__ w, const double* __restrict__ add,
+                                 double* __restrict__ t) {
+  const int32_t P = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (P >= nc) return;
+  const int lane = threadIdx.x & 31;
+  double tot = 0.0;
+  for (int64_t q = coarse_ptr[P]; q < coarse_ptr[P + 1]; ++q) {
+    const int32_t e = coarse_list[q];
+    const int32_t s = pri_sub[e];
+    const int32_t p = static_cast<int32_t>(e - pri_off[s]);
+    const int32_t nr = nI[s] + nD[s];
+    const double* phi = R.x + R.off[s] + static_cast<int64_t>(p) * nr + nI[s];
+    const double* ws = w + dual_off[s];
+    double acc = 0.0;
+    for (int32_t i = lane; i < nD[s]; i += 32) acc = fma(phi[i], ws[i], acc);
+    tot += warp_sum(acc);
+  }
+  if (lane == 0) t[P] = (add ? add[P] : 0.0) + tot;
+}
+
+// y[e] = base + scale * sum_p Phi_D[i, p] u[coarse(s, p)] for every dual entry
+// e = (s, i); base = base_v[e], or the dual row of the setup solve's last
+// column (z = K_rr^-1 f_r) when base_v is null.  u may be null (no coarse term).
+__global__ void k_dual_add_phi(int64_t ne, const int32_t* __restrict__ dual_sub, const int64_t* __restrict__ dual_off,
+                               const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
+                               const int32_t* __restrict__ nP, const int64_t* __restrict__ pri_off,
+                               const int32_t* __restrict__ pri_coarse, RhsDev R, const double* __restrict__ u,
+                               const double* base_v, double scale, double* y) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < ne;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s = dual_sub[e];
+    const int32_t i = static_cast<int32_t>(e - dual_off[s]);
+    const int32_t nr = nI[s] + nD[s];
+    const double* phi = R.x + R.off[s] + nI[s] + i;
+    double acc = 0.0;
+    if (u)
+      for (int32_t p = 0; p < nP[s]; ++p)
+        acc = fma(phi[static_cast<int64_t>(p) * nr], u[pri_coarse[pri_off[s] + p]], acc);
+    const double b = base_v ? base_v[e] : phi[static_cast<int64_t>(nP[s]) * nr];
+    y[e] = b + scale * acc;
+  }
+}
+
+// ------------------------------------------------------------- PCG pieces
+
+struct LamState {
+  double rz, rz_old, pq, rr, rr0, alpha, beta;
+};
+
+__global__ void __launch_bounds__(256) k_dot_part(int64_t n, const double* __restrict__ a,
+                                                  const double* __restrict__ b, double* __restrict__ part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    acc = fma(a[i], b[i], acc);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// which: 0 pq -> alpha, 1 rz -> beta, 2 rr, 3 rz (first), 4 rr0
+__global__ void k_reduce_state(const double* __restrict__ part, int32_t np, LamState* st, int which) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) {
+    if (which == 0) { st->pq = acc; st->alpha = acc != 0.0 ? st->rz / acc : 0.0; }
+    else if (which == 1) { st->rz_old = st->rz; st->rz = acc; st->beta = st->rz_old != 0.0 ? acc / st->rz_old : 0.0; }
+    else if (which == 2) st->rr = acc;
+    else if (which == 3) st->rz = acc;
+    else { st->rr0 = acc; st->rr = acc; }
+  }
+}
+
+__global__ void k_lam_update(int64_t n, const LamState* __restrict__ st, double* __restrict__ x,
+                             double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ q) {
+  const double a = st->alpha;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    x[i] = fma(a, p[i], x[i]);
+    r[i] = fma(-a, q[i], r[i]);
+  }
+}
+
+__global__ void k_lam_direction(int64_t n, const LamState* __restrict__ st, double* __restrict__ p,
+                                const double* __restrict__ z, int first) {
+  const double b = first ? 0.0 : st->beta;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    p[i] = first ? z[i] : fma(b, p[i], z[i]);
+}
+
+// ---------------------------------------------------------------- recovery
+
+// Local right-hand side f_r - K_rP u_c - B^T lambda (one column, union layout).
+__global__ void k_recover_rhs(const int64_t* __restrict__ loc_off, const int32_t* __restrict__ nI,
+                              const int32_t* __restrict__ nD, const int64_t* __restrict__ pri_off,
+                              const int32_t* __restrict__ pri_coarse, const int64_t* __restrict__ dual_off,
+                              const int32_t* __restrict__ dual_lam, const int32_t* __restrict__ dual_sign,
+                              const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                              const double* __restrict__ val, const double* __restrict__ frhs,
+                              const double* __restrict__ uc, const double* __restrict__ lam, int has_lam,
+                              double* __restrict__ x) {
+  const int32_t s = blockIdx.y;
+  const int32_t nr = nI[s] + nD[s];
+  const int64_t base = loc_off[s];
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x) {
+    const int64_t u = base + i;
+    double v = frhs[u];
+    for (int32_t q = rp[u]; q < rp[u + 1]; ++q) {
+      const int32_t j = static_cast<int32_t>(col[q] - base);
+      if (j >= nr) v -= val[q] * uc[pri_coarse[pri_off[s] + (j - nr)]];
+    }
+    if (has_lam && i >= nI[s]) {
+      const int64_t e = dual_off[s] + (i - nI[s]);
+      v -= dual_sign[e] * lam[dual_lam[e]];
+    }
+    x[u] = v;
+  }
+}
+
+// Global solution: average of the subdomain copies (primal copies = u_c).
+__global__ void k_global_average(int64_t n, const int64_t* __restrict__ gptr, const int32_t* __restrict__ glist,
+                                 const double* __restrict__ xu, double* __restrict__ x) {
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < n;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t q = gptr[g]; q < gptr[g + 1]; ++q) acc += xu[glist[q]];
+    x[g] = acc / static_cast<double>(gptr[g + 1] - gptr[g]);
+  }
+}
+
+__global__ void k_set_primal(const int64_t* __restrict__ loc_off, const int32_t* __restrict__ nI,
+                             const int32_t* __restrict__ nD, const int32_t* __restrict__ nP,
+                             const int64_t* __restrict__ pri_off, const int32_t* __restrict__ pri_coarse,
+                             const double* __restrict__ uc, double* __restrict__ xu) {
+  const int32_t s = blockIdx.y;
+  for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < nP[s]; p += gridDim.x * blockDim.x)
+    xu[loc_off[s] + nI[s] + nD[s] + p] = uc[pri_coarse[pri_off[s] + p]];
+}
+
+__global__ void k_scatter_global(int64_t nu, const int32_t* __restrict__ ugdof, const double* __restrict__ x,
+                                 double* __restrict__ xu) {
+  for (int64_t u = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; u < nu;
+       u += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    xu[u] = x[ugdof[u]];
+}
+
+__global__ void k_axmy(int64_t n, const double* __restrict__ a, double* __restrict__ y) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = a[i] - y[i];
+}
+
+unsigned blocks_for(int64_t work, int threads, int cap = 148 * 8) {
+  int64_t b = (work + threads - 1) / threads;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(b, cap)));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+
+FetiDP::~FetiDP() { release(); }
+
+void FetiDP::release() {
+  if (!dev.empty()) cudaStreamSynchronize(st);
+  for (void* p : dev) cudaFree(p);
+  dev.clear();
+}
+
+template <class T>
+int FetiDP::up(T** dst, const std::vector<T>& src) {
+  *dst = nullptr;
+  const size_t n = std::max<size_t>(src.size(), 1);
+  void* p = nullptr;
+  EMG_CK(cudaMalloc(&p, sizeof(T) * n));
+  dev.push_back(p);
+  if (!src.empty()) EMG_CK(cudaMemcpyAsync(p, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st));
+  else EMG_CK(cudaMemsetAsync(p, 0, sizeof(T), st));
+  *dst = static_cast<T*>(p);
+  return EMG_SUCCESS;
+}
+
+int FetiDP::zalloc(double** dst, int64_t n) {
+  *dst = nullptr;
+  n = std::max<int64_t>(n, 1);
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, sizeof(double) * n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("FETI-DP: device allocation of " + std::to_string((n * 8) >> 20) + " MiB failed: " +
+              cudaGetErrorString(e));
+    return EMG_ERR_NOMEM;
+  }
+  dev.push_back(p);
+  EMG_CK(cudaMemsetAsync(p, 0, sizeof(double) * n, st));
+  *dst = static_cast<double*>(p);
+  return EMG_SUCCESS;
+}
+
+int FetiDP::create(const Mesh& m, const DofMap& d, cudaStream_t stream) {
+  st = stream;
+  {
+    TraceScope t("fetidp.plan");
+    int rc = build_feti_plan(m, d, plan);
+    if (rc) return rc;
+  }
+  // union system: every tet once, its DOFs in its own subdomain's block
+  un.n_nodes = m.n_nodes;
+  un.n_tets = m.n_tets;
+  un.n = plan.n_union;
+  std::vector<int32_t> mat = m.material;
+  if (mat.empty()) mat.assign(m.n_tets, 0);
+  int rc = EMG_SUCCESS;
+  auto upload = [&](auto** dst, const auto& v) -> int {
+    using T = typename std::remove_reference<decltype(v)>::type::value_type;
+    EMG_CK(cudaMallocAsync(reinterpret_cast<void**>(dst), sizeof(T) * v.size(), st));
+    EMG_CK(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+    return EMG_SUCCESS;
+  };
+  if ((rc = upload(&un.xyz, m.xyz)) || (rc = upload(&un.tets, m.tets)) || (rc = upload(&un.material, mat)) ||
+      (rc = upload(&un.l2g, plan.l2g_union)))
+    return rc;
+  EMG_CK(cudaMallocAsync(&un.err, sizeof(int32_t), st));
+  {
+    TraceScope t("fetidp.union_build");
+    rc = system_build(un, st);
+    if (rc) return rc;
+  }
+  TraceScope t("fetidp.setup_device");
+  return setup_device();
+}
+
+int FetiDP::setup_device() {
+  const FetiPlan& P = plan;
+  const int32_t F = static_cast<int32_t>(P.fronts.size());
+  const int32_t S = P.n_parts;
+  std::vector<int32_t> sub(F + 1), p0(F + 1), npiv(F + 1), f(F + 1), nch(F + 1), ch0(F + 1), isr(F + 1);
+  std::vector<int64_t> rows(F + 1), fac(F + 1), upd(F + 1), cpos(F + 1), vec(F + 1);
+  for (int32_t k = 0; k < F; ++k) {
+    const FetiFront& x = P.fronts[k];
+    sub[k] = x.sub; p0[k] = x.p0; npiv[k] = x.npiv; f[k] = x.f; nch[k] = x.nchild; ch0[k] = x.child0;
+    isr[k] = x.is_root; rows[k] = x.rows; fac[k] = x.fac; upd[k] = x.upd; cpos[k] = x.cpos; vec[k] = x.vec;
+  }
+  // front F is the coarse matrix, factored by the same kernels
+  coarse_fac = P.fac_size;
+  sub[F] = 0; p0[F] = 0; npiv[F] = P.n_coarse; f[F] = P.n_coarse; nch[F] = 0; ch0[F] = 0; isr[F] = 0;
+  rows[F] = 0; fac[F] = coarse_fac; upd[F] = -1; cpos[F] = 0; vec[F] = 0;
+  int rc = EMG_SUCCESS;
+  int32_t *d_sub, *d_p0, *d_npiv, *d_f, *d_nch, *d_ch0, *d_isr, *d_rows_v, *d_child_v, *d_cpos_v;
+  int64_t *d_rows, *d_fac, *d_upd, *d_cpos, *d_vec;
+  if ((rc = up(&d_sub, sub)) || (rc = up(&d_p0, p0)) || (rc = up(&d_npiv, npiv)) || (rc = up(&d_f, f)) ||
+      (rc = up(&d_nch, nch)) || (rc = up(&d_ch0, ch0)) || (rc = up(&d_isr, isr)) || (rc = up(&d_rows, rows)) ||
+      (rc = up(&d_fac, fac)) || (rc = up(&d_upd, upd)) || (rc = up(&d_cpos, cpos)) || (rc = up(&d_vec, vec)) ||
+      (rc = up(&d_rows_v, P.rows)) || (rc = up(&d_child_v, P.child_list)) || (rc = up(&d_cpos_v, P.cpos)))
+    return rc;
+  fd = FrontsDev{d_sub, d_p0, d_npiv, d_f, d_nch, d_ch0, d_isr, d_rows, d_fac, d_upd, d_cpos, d_vec,
+                 d_rows_v, d_child_v, d_cpos_v};
+  std::vector<int32_t> dual_sub(P.dual_off[S]), pri_sub(P.pri_off[S]);
+  for (int32_t s = 0; s < S; ++s) {
+    for (int64_t e = P.dual_off[s]; e < P.dual_off[s + 1]; ++e) dual_sub[e] = s;
+    for (int64_t e = P.pri_off[s]; e < P.pri_off[s + 1]; ++e) pri_sub[e] = s;
+  }
+  if ((rc = up(&d_loc_off, P.loc_off)) || (rc = up(&d_nI, P.nI)) || (rc = up(&d_nD, P.nD)) ||
+      (rc = up(&d_nP, P.nP)) || (rc = up(&d_dual_off, P.dual_off)) || (rc = up(&d_dual_lam, P.dual_lam)) ||
+      (rc = up(&d_dual_sign, P.dual_sign)) || (rc = up(&d_lam_entry, P.lam_entry)) ||
+      (rc = up(&d_dual_sub, dual_sub)) || (rc = up(&d_pri_off, P.pri_off)) ||
+      (rc = up(&d_pri_coarse, P.pri_coarse)) || (rc = up(&d_pri_sub, pri_sub)) ||
+      (rc = up(&d_coarse_ptr, P.coarse_ptr)) || (rc = up(&d_coarse_list, P.coarse_list)) ||
+      (rc = up(&d_cblk_off, P.cblk_off)) || (rc = up(&d_sc_ptr, P.sc_ptr)) || (rc = up(&d_sc_list, P.sc_list)) ||
+      (rc = up(&d_gptr, P.gptr)) || (rc = up(&d_glist, P.glist)) || (rc = up(&d_union_gdof, P.union_gdof)) ||
+      (rc = up(&d_root_off, P.root_off)))
+    return rc;
+  std::vector<int32_t> rdim;
+  std::vector<int64_t> rfac, roff, rvoff;
+  max_nD = 0;
+  for (int32_t s = 0; s < S; ++s) {
+    if (P.nD[s] == 0) continue;
+    rdim.push_back(P.nD[s]);
+    rfac.push_back(P.fronts[P.root_front[s]].fac);
+    roff.push_back(P.root_off[s]);
+    rvoff.push_back(P.dual_off[s]);
+    max_nD = std::max(max_nD, P.nD[s]);
+  }
+  n_roots = static_cast<int32_t>(rdim.size());
+  std::vector<int32_t> cdim{P.n_coarse};
+  std::vector<int64_t> cfac{coarse_fac}, czero{0};
+  if ((rc = up(&d_rdim, rdim)) || (rc = up(&d_rfac, rfac)) || (rc = up(&d_roff, roff)) ||
+      (rc = up(&d_rvoff, rvoff)) || (rc = up(&d_cdim, cdim)) || (rc = up(&d_cfac, cfac)) ||
+      (rc = up(&d_czero, czero)))
+    return rc;
+  // setup solves: n_r x (nP + 1) per subdomain; recovery: one column in union layout
+  std::vector<int64_t> roff_s(S), roff1(S);
+  std::vector<int32_t> ncol_s(S), ncol1(S, 1);
+  int64_t tot = 0;
+  max_ncol = 1;
+  for (int32_t s = 0; s < S; ++s) {
+    roff_s[s] = tot;
+    ncol_s[s] = P.nP[s] + 1;
+    max_ncol = std::max(max_ncol, ncol_s[s]);
+    tot += static_cast<int64_t>(P.nI[s] + P.nD[s]) * ncol_s[s];
+    roff1[s] = P.loc_off[s];
+  }
+  std::vector<int64_t> voff_s(F + 1, 0), voff1(F + 1, 0);
+  int64_t vt = 0;
+  for (int32_t k = 0; k < F; ++k) {
+    voff_s[k] = vt;
+    vt += static_cast<int64_t>(P.fronts[k].f - P.fronts[k].npiv) * ncol_s[P.fronts[k].sub];
+    voff1[k] = P.fronts[k].vec;
+  }
+  if ((rc = up(&d_roff_s, roff_s)) || (rc = up(&d_ncol_s, ncol_s)) || (rc = up(&d_roff1, roff1)) ||
+      (rc = up(&d_ncol1, ncol1)) || (rc = up(&d_voff_s, voff_s)) || (rc = up(&d_voff1, voff1)))
+    return rc;
+  phi_size = tot;
+  vs_size = vt;
+  const int64_t nc = P.n_coarse, nd = P.dual_off[S], nl = P.n_lambda;
+  if ((rc = zalloc(&fac_d, P.fac_size + nc * nc)) || (rc = zalloc(&upd_d, P.upd_pool)) ||
+      (rc = zalloc(&S_d, P.root_off[S])) || (rc = zalloc(&Linv_d, P.root_off[S])) ||
+      (rc = zalloc(&Lcc_d, nc * nc)) || (rc = zalloc(&phi_d, phi_size)) || (rc = zalloc(&vs_d, vs_size)) ||
+      (rc = zalloc(&v1_d, P.vec_rows)) || (rc = zalloc(&cblk_d, P.cblk_off[S])) ||
+      (rc = zalloc(&h_d, P.pri_off[S])) || (rc = zalloc(&gc_d, nc)) || (rc = zalloc(&uc_d, nc)) ||
+      (rc = zalloc(&t_d, nc)) || (rc = zalloc(&t2_d, nc)) || (rc = zalloc(&rho_d, nd)) ||
+      (rc = zalloc(&wt_d, nd)) || (rc = zalloc(&w_d, nd)) || (rc = zalloc(&y_d, nd)) || (rc = zalloc(&y2_d, nd)) ||
+      (rc = zalloc(&xu_d, P.n_union)) || (rc = zalloc(&ru_d, P.n_union)) || (rc = zalloc(&xg_d, P.n_dofs)) ||
+      (rc = zalloc(&rg_d, P.n_dofs)) || (rc = zalloc(&bg_d, P.n_dofs)) || (rc = zalloc(&lam_d, nl)) ||
+      (rc = zalloc(&r_d, nl)) || (rc = zalloc(&z_d, nl)) || (rc = zalloc(&p_d, nl)) || (rc = zalloc(&q_d, nl)) ||
+      (rc = zalloc(&rhs_d, nl)) || (rc = zalloc(&part_d, kParts)))
+    return rc;
+  void* ps = nullptr;
+  EMG_CK(cudaMalloc(&ps, sizeof(LamState)));
+  dev.push_back(ps);
+  state_d = ps;
+  void* pe = nullptr;
+  EMG_CK(cudaMalloc(&pe, sizeof(int32_t)));
+  dev.push_back(pe);
+  err_d = static_cast<int32_t*>(pe);
+  EMG_CK(cudaStreamSynchronize(st));
+  return EMG_SUCCESS;
+}
+
+int FetiDP::check_err(const char* where) {
+  int32_t e = 0;
+  EMG_CK(cudaMemcpyAsync(&e, err_d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  EMG_CK(cudaGetLastError());
+  if (e & kErrPivot) {
+    set_error(std::string(where) + ": non-positive pivot (a subdomain matrix is not positive definite)");
+    return EMG_NUMERICAL_ERROR;
+  }
+  if (e) {
+    set_error(std::string(where) + ": front assembly lookup failed");
+    return EMG_ERR_INTERNAL;
+  }
+  return EMG_SUCCESS;
+}
+
+// Partial Cholesky of fronts [f0, f1): panels of kNB columns (diagonal block,
+// panel rows, remaining pivot columns), then the update block in one rank-npiv
+// update.  Front index F (one past the plan's fronts) is the coarse matrix.
+int FetiDP::factor_range(int32_t f0, int32_t f1) {
+  const int32_t F = static_cast<int32_t>(plan.fronts.size());
+  int32_t max_np = 0, max_f = 0, max_nu = 0;
+  for (int32_t k = f0; k < f1; ++k) {
+    const int32_t np = k < F ? plan.fronts[k].npiv : plan.n_coarse;
+    const int32_t fs = k < F ? plan.fronts[k].f : plan.n_coarse;
+    max_np = std::max(max_np, np);
+    max_f = std::max(max_f, fs);
+    max_nu = std::max(max_nu, fs - np);
+  }
+  const unsigned nf = static_cast<unsigned>(f1 - f0);
+  if (nf == 0 || max_np == 0) return EMG_SUCCESS;
+  for (int32_t k0 = 0; k0 < max_np; k0 += kNB) {
+    k_potrf_diag<<<nf, 256, 0, st>>>(fd, f0, k0, fac_d, err_d);
+    const int32_t rows = max_f - k0 - 1;
+    if (rows > 0) {
+      const unsigned rb = static_cast<unsigned>((rows + kTrsmRows - 1) / kTrsmRows);
+      k_trsm_panel<<<dim3(rb, nf), kTrsmRows, 0, st>>>(fd, f0, k0, fac_d);
+    }
+    const int32_t c0 = k0 + kNB;
+    if (c0 < max_np) {
+      const int32_t nct = (max_np - c0 + kTile - 1) / kTile, nrt = (max_f - c0 + kTile - 1) / kTile;
+      k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), nf), 256, 0, st>>>(fd, f0, k0, fac_d);
+    }
+  }
+  if (max_nu > 0) {
+    const int32_t nt = (max_nu + kTile - 1) / kTile;
+    k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
+  }
+  EMG_CK(cudaGetLastError());
+  return EMG_SUCCESS;
+}
+
+int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
+  const int32_t nlev = static_cast<int32_t>(plan.level_ptr.size()) - 1;
+  for (int32_t h = 0; h < nlev; ++h) {
+    const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
+    if (nf > 0)
+      k_front_fwd<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 32, 0, st>>>(fd, f0, R, d_nI,
+                                                                                               d_nD, fac_d);
+  }
+  for (int32_t h = nlev - 1; h >= 0; --h) {
+    const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
+    if (nf > 0)
+      k_front_bwd<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 32, 0, st>>>(fd, f0, R, d_nI,
+                                                                                               d_nD, fac_d);
+  }
+  EMG_CK(cudaGetLastError());
+  return EMG_SUCCESS;
+}
+
+// u = S_cc^-1 t = L^-T (L^-1 t)
+void FetiDP::coarse_solve(const double* t, double* u) {
+  const int32_t nc = plan.n_coarse;
+  if (nc == 0) return;
+  k_block_gemv<<<dim3(static_cast<unsigned>((nc + 127) / 128), 1), 128, 0, st>>>(1, d_cdim, d_czero, Lcc_d,
+                                                                                 d_czero, t, t2_d, 1);
+  k_block_gemv_lt<<<dim3(static_cast<unsigned>((nc + 7) / 8), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d,
+                                                                                d_czero, t2_d, u);
+}
+
+// q = (F_rr + G S_cc^-1 G^T) p, part = per-block partials of p . q
+void FetiDP::apply_F(const double* p, double* q, double* part) {
+  const FetiPlan& P = plan;
+  const int64_t ne = P.dual_off[P.n_parts];
+  RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
+  k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, p, w_d);
+  const unsigned gx = static_cast<unsigned>((max_nD + 127) / 128), gy = static_cast<unsigned>(n_roots);
+  k_block_gemv<<<dim3(gx, gy), 128, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 1);
+  k_block_gemv_lt<<<dim3(static_cast<unsigned>((max_nD + 7) / 8), gy), 256, 0, st>>>(n_roots, d_rdim, d_roff,
+                                                                                     Linv_d, d_rvoff, y2_d, y_d);
+  if (P.n_coarse > 0) {
+    k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
+        P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, nullptr, t_d);
+    coarse_solve(t_d, uc_d);
+    k_dual_add_phi<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_sub, d_dual_off, d_nI, d_nD, d_nP, d_pri_off,
+                                                         d_pri_coarse, R, uc_d, y_d, 1.0, y_d);
+  }
+  k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, y_d, q, p, part);
+}
+
+// z = sum_s B_Ds S_DD,s B_Ds^T r, part = partials of r . z
+void FetiDP::apply_M(const double* r, double* z, double* part) {
+  const FetiPlan& P = plan;
+  const int64_t ne = P.dual_off[P.n_parts];
+  k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, wt_d, r, w_d);
+  const unsigned gx = static_cast<unsigned>((max_nD + 127) / 128), gy = static_cast<unsigned>(n_roots);
+  k_block_gemv<<<dim3(gx, gy), 128, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 0);
+  k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, wt_d, y_d, z, r, part);
+}
+
+int FetiDP::dot(const double* a, const double* b, int64_t n, int which) {
+  k_dot_part<<<kParts, 256, 0, st>>>(n, a, b, part_d);
+  k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, static_cast<LamState*>(state_d), which);
+  EMG_CK(cudaGetLastError());
+  return EMG_SUCCESS;
+}
+
+namespace {
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  EventPair() { cudaEventCreate(&a); cudaEventCreate(&b); }
+  ~EventPair() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  double ms() {
+    float v = 0.f;
+    cudaEventElapsedTime(&v, a, b);
+    return v;
+  }
+};
+}  // namespace
+
+int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const emg_source* src, int32_t n_src,
+                   int32_t flags) {
+  TraceScope tr("fetidp.factor");
+  factored = false;
+  const FetiPlan& P = plan;
+  const int32_t S = P.n_parts;
+  const int32_t F = static_cast<int32_t>(P.fronts.size());
+  EventPair ev;
+  EMG_CK(cudaEventRecord(ev.a, st));
+  int rc = system_assemble(un, nu, sigma, n_mat, src, n_src, flags & ~EMG_FLAG_MASS, st);
+  if (rc) return rc;
+  const int32_t* rp = un.K.row_ptr;
+  const int32_t* cl = un.K.col;
+  const double* vl = un.K.val;
+  EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
+  const int32_t nlev = static_cast<int32_t>(P.level_ptr.size()) - 1;
+  for (int32_t h = 0; h < nlev && !rc; ++h) {
+    const int32_t f0 = P.level_ptr[h], f1 = P.level_ptr[h + 1];
+    const unsigned nf = static_cast<unsigned>(f1 - f0);
+    if (nf == 0) continue;
+    int32_t max_np = 0, max_ch = 0, max_root = 0;
+    int64_t max_el = 0, max_cu = 0;
+    for (int32_t k = f0; k < f1; ++k) {
+      const FetiFront& x = P.fronts[k];
+      const int64_t nu1 = x.f - x.npiv;
+      max_np = std::max(max_np, x.npiv);
+      max_ch = std::max(max_ch, x.nchild);
+      if (x.is_root) max_root = std::max(max_root, x.npiv);
+      max_el = std::max(max_el, static_cast<int64_t>(x.f) * x.npiv + nu1 * nu1);
+      for (int32_t c = 0; c < x.nchild; ++c) {
+        const FetiFront& y = P.fronts[P.child_list[x.child0 + c]];
+        max_cu = std::max(max_cu, static_cast<int64_t>(y.f - y.npiv) * (y.f - y.npiv));
+      }
+    }
+    k_front_zero<<<dim3(blocks_for(max_el, 256, 512), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
+    k_front_scatter<<<dim3(static_cast<unsigned>((max_np + 7) / 8), nf), 256, 0, st>>>(
+        fd, f0, d_loc_off, d_nI, d_nD, rp, cl, vl, fac_d, err_d);
+    for (int32_t slot = 0; slot < max_ch; ++slot)
+      k_extend_add<<<dim3(blocks_for(max_cu, 256, 512), nf), 256, 0, st>>>(fd, f0, slot, fac_d, upd_d);
+    if (max_root > 0)
+      k_copy_roots<<<dim3(blocks_for(static_cast<int64_t>(max_root) * max_root, 256, 512), nf), 256, 0, st>>>(
+          fd, f0, d_root_off, fac_d, S_d);
+    rc = factor_range(f0, f1);
+  }
+  if (!rc) rc = check_err("FETI-DP factorization");
+  if (rc) return rc;
+  if (n_roots > 0)
+    k_trtri<<<dim3(static_cast<unsigned>((max_nD + 15) / 16), static_cast<unsigned>(n_roots)), 512, 0, st>>>(
+        n_roots, d_rdim, d_rfac, d_roff, fac_d, Linv_d);
+  // Phi = K_rr^-1 K_rP (columns 0..nP-1) and z = K_rr^-1 f_r (column nP)
+  EMG_CK(cudaMemsetAsync(phi_d, 0, sizeof(double) * std::max<int64_t>(phi_size, 1), st));
+  RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
+  k_setup_rhs<<<dim3(64, static_cast<unsigned>(S)), 256, 0, st>>>(d_loc_off, d_nI, d_nD, d_nP, rp, cl, vl, un.rhs, R);
+  rc = solve_fronts(R, max_ncol);
+  if (rc) return rc;
+  const int64_t nc = P.n_coarse;
+  if (nc > 0) {
+    int32_t maxw = 0;
+    for (int32_t s = 0; s < S; ++s) maxw = std::max(maxw, P.nP[s] * (P.nP[s] + 1));
+    if (maxw > 0)
+      k_coarse_blocks<<<dim3(static_cast<unsigned>((maxw + 7) / 8), static_cast<unsigned>(S)), 256, 0, st>>>(
+          d_loc_off, d_nI, d_nD, d_nP, rp, cl, vl, un.rhs, R, d_cblk_off, d_pri_off, cblk_d, h_d);
+    k_gather_sum<int64_t><<<blocks_for(nc * nc, 256), 256, 0, st>>>(nc * nc, d_sc_ptr, d_sc_list, cblk_d,
+                                                                     fac_d + coarse_fac);
+    k_gather_sum<int32_t><<<blocks_for(nc, 256), 256, 0, st>>>(nc, d_coarse_ptr, d_coarse_list, h_d, gc_d);
+    EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
+    rc = factor_range(F, F + 1);
+    if (!rc) rc = check_err("FETI-DP coarse factorization");
+    if (rc) return rc;
+    k_trtri<<<dim3(static_cast<unsigned>((nc + 15) / 16), 1), 512, 0, st>>>(1, d_cdim, d_cfac, d_czero, fac_d, Lcc_d);
+  }
+  const int64_t ne = P.dual_off[S];
+  if (ne > 0) {
+    k_dual_weights<<<blocks_for(ne, 256), 256, 0, st>>>(d_loc_off, d_nI, d_dual_off, d_dual_lam, d_dual_sign,
+                                                         d_lam_entry, d_dual_sub, rp, cl, vl, ne, rho_d, wt_d, 0);
+    k_dual_weights<<<blocks_for(ne, 256), 256, 0, st>>>(d_loc_off, d_nI, d_dual_off, d_dual_lam, d_dual_sign,
+                                                         d_lam_entry, d_dual_sub, rp, cl, vl, ne, rho_d, wt_d, 1);
+    // lambda right-hand side d - G S_cc^-1 g_c
+    coarse_solve(gc_d, uc_d);
+    k_dual_add_phi<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_sub, d_dual_off, d_nI, d_nD, d_nP, d_pri_off,
+                                                         d_pri_coarse, R, nc > 0 ? uc_d : nullptr, nullptr, -1.0,
+                                                         y_d);
+    k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, y_d, rhs_d, nullptr, nullptr);
+  }
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaEventRecord(ev.b, st));
+  EMG_CK(cudaEventSynchronize(ev.b));
+  stats.factor_ms = ev.ms();
+  factored = true;
+  return EMG_SUCCESS;
+}
+
+int FetiDP::solve(const emg_krylov_config& cfg, double* x_d, emg_result* res) {
+  TraceScope tr("fetidp.solve");
+  if (!factored) { set_error("FETI-DP: factor() has not succeeded"); return EMG_INVALID_INPUT; }
+  const FetiPlan& P = plan;
+  const int32_t S = P.n_parts;
+  const int64_t nl = P.n_lambda;
+  LamState* sd = static_cast<LamState*>(state_d);
+  LamState hs{};
+  EventPair ev;
+  EMG_CK(cudaEventRecord(ev.a, st));
+  int status = EMG_SUCCESS;
+  int32_t it = 0;
+  double rel = 0.0;
+  if (nl > 0) {
+    EMG_CK(cudaMemsetAsync(lam_d, 0, sizeof(double) * nl, st));
+    EMG_CK(cudaMemcpyAsync(r_d, rhs_d, sizeof(double) * nl, cudaMemcpyDeviceToDevice, st));
+    dot(r_d, r_d, nl, 4);
+    apply_M(r_d, z_d, part_d);
+    k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 3);
+    k_lam_direction<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, p_d, z_d, 1);
+    EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    const double rr0 = hs.rr0;
+    if (rr0 > 0.0) {
+      status = EMG_MAX_ITER_REACHED;
+      for (it = 1; it <= cfg.max_iterations; ++it) {
+        apply_F(p_d, q_d, part_d);
+        k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 0);
+        k_lam_update<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, lam_d, r_d, p_d, q_d);
+        dot(r_d, r_d, nl, 2);
+        apply_M(r_d, z_d, part_d);
+        k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 1);
+        k_lam_direction<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, p_d, z_d, 0);
+        EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
+        EMG_CK(cudaStreamSynchronize(st));
+        rel = std::sqrt(std::max(hs.rr, 0.0) / rr0);
+        if (!(hs.pq > 0.0) || !std::isfinite(hs.rr)) { status = EMG_NUMERICAL_ERROR; break; }
+        if (rel < cfg.tolerance) { status = EMG_SUCCESS; break; }
+      }
+      if (it > cfg.max_iterations) it = cfg.max_iterations;
+    }
+  }
+  // recovery: u_c = S_cc^-1 (g_c + G^T lambda), u_r = K_rr^-1 (f_r - K_rP u_c - B^T lambda)
+  const int64_t ne = P.dual_off[S];
+  RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
+  if (P.n_coarse > 0) {
+    if (ne > 0) k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, lam_d, w_d);
+    k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
+        P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, gc_d, t_d);
+    coarse_solve(t_d, uc_d);
+  }
+  const int32_t* rp = un.K.row_ptr;
+  const int32_t* cl = un.K.col;
+  const double* vl = un.K.val;
+  k_recover_rhs<<<dim3(64, static_cast<unsigned>(S)), 256, 0, st>>>(d_loc_off, d_nI, d_nD, d_pri_off, d_pri_coarse,
+                                                                    d_dual_off, d_dual_lam, d_dual_sign, rp, cl, vl,
+                                                                    un.rhs, uc_d, lam_d, nl > 0 ? 1 : 0, xu_d);
+  RhsDev R1{xu_d, d_roff1, d_ncol1, d_voff1, v1_d};
+  int rc = solve_fronts(R1, 1);
+  if (rc) return rc;
+  k_set_primal<<<dim3(1, static_cast<unsigned>(S)), 256, 0, st>>>(d_loc_off, d_nI, d_nD, d_nP, d_pri_off,
+                                                                  d_pri_coarse, uc_d, xu_d);
+  k_global_average<<<blocks_for(P.n_dofs, 256), 256, 0, st>>>(P.n_dofs, d_gptr, d_glist, xu_d, xg_d);
+  EMG_CK(cudaEventRecord(ev.b, st));
+  // true residual of the global system: r = sum over copies of (f - K_s x)
+  k_scatter_global<<<blocks_for(P.n_union, 256), 256, 0, st>>>(P.n_union, d_union_gdof, xg_d, xu_d);
+  rc = csr_spmv(un.K, xu_d, ru_d, st);
+  if (rc) return rc;
+  k_axmy<<<blocks_for(P.n_union, 256), 256, 0, st>>>(P.n_union, un.rhs, ru_d);
+  k_gather_sum<int32_t><<<blocks_for(P.n_dofs, 256), 256, 0, st>>>(P.n_dofs, d_gptr, d_glist, ru_d, rg_d);
+  k_gather_sum<int32_t><<<blocks_for(P.n_dofs, 256), 256, 0, st>>>(P.n_dofs, d_gptr, d_glist, un.rhs, bg_d);
+  dot(rg_d, rg_d, P.n_dofs, 2);
+  EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  const double rres = hs.rr;
+  dot(bg_d, bg_d, P.n_dofs, 2);
+  EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  const double bb = hs.rr;
+  if (x_d) EMG_CK(cudaMemcpyAsync(x_d, xg_d, sizeof(double) * P.n_dofs, cudaMemcpyDeviceToDevice, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  stats.iterations = it;
+  stats.lambda_residual = rel;
+  stats.residual = bb > 0.0 ? std::sqrt(rres / bb) : 0.0;
+  stats.solve_ms = ev.ms();
+  if (res) {
+    res->status = status;
+    res->iterations = it;
+    res->residual_norm = stats.residual;
+    res->solve_time_ms = stats.solve_ms;
+  }
+  return status;
+}
+
+}  // namespace emg

@@ -1,0 +1,119 @@
+// fetidp_dev.h -- device state of the FETI-DP solver (fetidp.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "device.h"
+#include "fetidp.h"
+
+namespace emg {
+
+// Front table in structure-of-arrays form (front index F = the coarse matrix).
+struct FrontsDev {
+  const int32_t* sub;
+  const int32_t* p0;
+  const int32_t* npiv;
+  const int32_t* f;
+  const int32_t* nchild;
+  const int32_t* child0;
+  const int32_t* is_root;
+  const int64_t* rows;
+  const int64_t* fac;
+  const int64_t* upd;
+  const int64_t* cpos;
+  const int64_t* vec;
+  const int32_t* rows_v;
+  const int32_t* child_v;
+  const int32_t* cpos_v;
+};
+
+// Right-hand-side blocks of the multifrontal solves: subdomain s holds
+// ncol[s] columns of n_r values at x[off[s] + pos + col * n_r].
+struct RhsDev {
+  double* x;
+  const int64_t* off;
+  const int32_t* ncol;
+  const int64_t* voff;  // per front: offset of its nupd x ncol update vectors
+  double* v;
+};
+
+struct FetiStats {
+  int32_t iterations = 0;
+  double lambda_residual = 0.0;   // ||r_lambda|| / ||r_lambda,0||
+  double residual = 0.0;          // true ||b - A x|| / ||b|| of the global system
+  double factor_ms = 0.0, solve_ms = 0.0;
+};
+
+struct FetiDP {
+  FetiPlan plan;
+  System un;  // block-diagonal union of the subdomain matrices
+  cudaStream_t st = nullptr;
+  std::vector<void*> dev;
+  FrontsDev fd{};
+  bool factored = false;
+  FetiStats stats;
+  // plan tables
+  int64_t* d_loc_off = nullptr;
+  int32_t *d_nI = nullptr, *d_nD = nullptr, *d_nP = nullptr;
+  int64_t* d_dual_off = nullptr;
+  int32_t *d_dual_lam = nullptr, *d_dual_sign = nullptr, *d_lam_entry = nullptr, *d_dual_sub = nullptr;
+  int64_t* d_pri_off = nullptr;
+  int32_t *d_pri_coarse = nullptr, *d_pri_sub = nullptr;
+  int64_t* d_coarse_ptr = nullptr;
+  int32_t* d_coarse_list = nullptr;
+  int64_t *d_cblk_off = nullptr, *d_sc_ptr = nullptr, *d_sc_list = nullptr;
+  int64_t* d_gptr = nullptr;
+  int32_t *d_glist = nullptr, *d_union_gdof = nullptr;
+  int64_t* d_root_off = nullptr;
+  // dense blocks
+  int32_t n_roots = 0, max_nD = 0, max_ncol = 1;
+  int32_t* d_rdim = nullptr;
+  int64_t *d_rfac = nullptr, *d_roff = nullptr, *d_rvoff = nullptr;
+  int32_t* d_cdim = nullptr;
+  int64_t *d_cfac = nullptr, *d_czero = nullptr;
+  int64_t coarse_fac = 0;
+  // solve layouts
+  int64_t *d_roff_s = nullptr, *d_roff1 = nullptr, *d_voff_s = nullptr, *d_voff1 = nullptr;
+  int32_t *d_ncol_s = nullptr, *d_ncol1 = nullptr;
+  int64_t phi_size = 0, vs_size = 0;
+  // numeric storage
+  double *fac_d = nullptr, *upd_d = nullptr, *S_d = nullptr, *Linv_d = nullptr, *Lcc_d = nullptr;
+  double *phi_d = nullptr, *vs_d = nullptr, *v1_d = nullptr, *cblk_d = nullptr, *h_d = nullptr;
+  double *gc_d = nullptr, *uc_d = nullptr, *t_d = nullptr, *t2_d = nullptr;
+  double *rho_d = nullptr, *wt_d = nullptr, *w_d = nullptr, *y_d = nullptr, *y2_d = nullptr;
+  double *xu_d = nullptr, *ru_d = nullptr, *xg_d = nullptr, *rg_d = nullptr, *bg_d = nullptr;
+  double *lam_d = nullptr, *r_d = nullptr, *z_d = nullptr, *p_d = nullptr, *q_d = nullptr, *rhs_d = nullptr;
+  double* part_d = nullptr;
+  void* state_d = nullptr;
+  int32_t* err_d = nullptr;
+  static constexpr int kParts = 592;
+
+  ~FetiDP();
+  void release();
+  // Symbolic phase: plan, union system pattern, device tables and storage.
+  int create(const Mesh& m, const DofMap& d, cudaStream_t stream);
+  // Numeric phase for the given materials / sources.
+  int factor(const double* nu, const double* sigma, int32_t n_mat, const emg_source* src, int32_t n_src,
+             int32_t flags);
+  // lambda-PCG to cfg.tolerance (relative lambda residual), then recovery of
+  // the global solution x_d (n_dofs, device) and its true residual.
+  int solve(const emg_krylov_config& cfg, double* x_d, emg_result* res);
+
+ private:
+  template <class T>
+  int up(T** dst, const std::vector<T>& src);
+  int zalloc(double** dst, int64_t n);
+  int setup_device();
+  int check_err(const char* where);
+  int factor_range(int32_t f0, int32_t f1);
+  int solve_fronts(const RhsDev& R, int32_t ncol);
+  void coarse_solve(const double* t, double* u);
+  void apply_F(const double* p, double* q, double* part);
+  void apply_M(const double* r, double* z, double* part);
+  int dot(const double* a, const double* b, int64_t n, int which);
+};
+
+}  // namespace emg

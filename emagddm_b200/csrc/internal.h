@@ -35,10 +35,16 @@ struct DofMap {
   int32_t root = -1;
   std::vector<int32_t> l2g;       // 6 * n_tets
   std::vector<int32_t> edge_dof;  // n_edges
+  // Set by the partitioned gauge only.
+  int32_t n_parts = 0;
+  std::vector<int32_t> tet_part;    // n_tets, subdomain of every tet
+  std::vector<uint8_t> dof_primal;  // n_dofs, 1 = primal (coarse) DOF
+  int64_t n_primal_fix = 0;         // primal DOFs added to connect a subdomain
 };
 
 // Host integer numbering (numbering.cpp).
 int build_edge_ids(Mesh& m);
 int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out);
+int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, DofMap& out);
 
 }  // namespace emg

@@ -237,15 +237,11 @@ int32_t spanning_tree(const Mesh& m, const EdgeGraph& g, const std::vector<uint8
   return root;
 }
 
-}  // namespace
-
-int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
-  int rc = build_edge_ids(m);
-  if (rc) return rc;
-  const int64_t E = m.n_edges, T = m.n_tets;
-  out = DofMap{};
-  out.n_tets = T;
-  out.n_edges = E;
+// markConstrainedDOFs (em_dof_manager.cpp:152-243): constrained[e] = 1 for
+// every mesh edge listed as a Dirichlet node pair; pairs that are not mesh
+// edges are skipped.
+void mark_constrained(const Mesh& m, std::vector<uint8_t>& constrained) {
+  const int64_t E = m.n_edges;
   // Edge lookup by node pair: edges bucketed by lower node.
   std::vector<int64_t> lptr(m.n_nodes + 1, 0);
   for (int64_t e = 0; e < E; ++e) lptr[m.edge_nodes[2 * e] + 1]++;
@@ -255,9 +251,7 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
     std::vector<int64_t> cur(lptr.begin(), lptr.end() - 1);
     for (int64_t e = 0; e < E; ++e) lid[cur[m.edge_nodes[2 * e]]++] = static_cast<int32_t>(e);
   }
-  // markConstrainedDOFs (em_dof_manager.cpp:152-243): node pairs that are not
-  // mesh edges are skipped.
-  std::vector<uint8_t> constrained(E, 0);
+  constrained.assign(E, 0);
   const int64_t D = static_cast<int64_t>(m.dirichlet.size() / 2);
   for (int64_t d = 0; d < D; ++d) {
     int32_t a = m.dirichlet[2 * d], b = m.dirichlet[2 * d + 1];
@@ -266,6 +260,19 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
     for (int64_t s = lptr[lo]; s < lptr[lo + 1]; ++s)
       if (m.edge_nodes[2 * lid[s] + 1] == hi) { constrained[lid[s]] = 1; break; }
   }
+}
+
+}  // namespace
+
+int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
+  int rc = build_edge_ids(m);
+  if (rc) return rc;
+  const int64_t E = m.n_edges, T = m.n_tets;
+  out = DofMap{};
+  out.n_tets = T;
+  out.n_edges = E;
+  std::vector<uint8_t> constrained;
+  mark_constrained(m, constrained);
   // Prenumber of an edge in an all-vector mesh = its global ID
   // (assignPrenumbering, :91-150); free index = rank among the unconstrained
   // (renumberFreeDOFs, :245-286).
@@ -309,6 +316,165 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
     set_error("unknown gauge mode");
     return EMG_INVALID_INPUT;
   }
+  out.l2g.resize(6 * T);
+  for (int64_t p = 0; p < 6 * T; ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  return EMG_SUCCESS;
+}
+
+// Tree-cotree gauge for a non-overlapping partition of the tets (no
+// counterpart in the reference, whose FETI-DP context is a stub:
+// include/fetidp/fetidp_context.hpp:20-66).  Edges are ranked by class:
+//   0 Dirichlet, 1 wire basket (shared by >= 3 subdomains),
+//   2 subdomain face (shared by 2), 3 subdomain interior,
+// and the spanning tree is grown Prim-style, always through the lowest class
+// available (FIFO inside a class).  The Dirichlet surface is spanned first,
+// then the wire basket, then every face from its rim, then every interior
+// from its boundary, so the tree restricted to one subdomain hangs off that
+// subdomain's wire basket.  Primal (coarse) DOFs are the cotree wire-basket
+// edges; with the tree and the Dirichlet edges they keep every wire basket
+// continuous.  A subdomain whose tree + Dirichlet + primal edges still fall
+// apart into several node components gets, in ascending edge-ID order, the
+// cotree edges that join two components as extra primal DOFs
+// (n_primal_fix) -- that is what makes every local K_rr nonsingular: a local
+// gradient field vanishing on a connected edge set is zero.  Reduced DOFs
+// are the unconstrained cotree edges in ascending edge ID.
+int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, DofMap& out) {
+  if (n_parts < 1 || (m.n_tets > 0 && tet_part == nullptr)) {
+    set_error("partitioned gauge: need n_parts >= 1 and a tet_part array");
+    return EMG_INVALID_INPUT;
+  }
+  if (m.n_hole_markers > 0) {
+    set_error("partitioned gauge: hole markers (circulation DOFs) are not supported");
+    return EMG_INVALID_INPUT;
+  }
+  const int64_t T = m.n_tets;
+  for (int64_t t = 0; t < T; ++t)
+    if (tet_part[t] < 0 || tet_part[t] >= n_parts) {
+      set_error("partitioned gauge: tet_part[" + std::to_string(t) + "] outside [0, n_parts)");
+      return EMG_INVALID_INPUT;
+    }
+  int rc = build_edge_ids(m);
+  if (rc) return rc;
+  const int64_t E = m.n_edges;
+  out = DofMap{};
+  out.n_tets = T;
+  out.n_edges = E;
+  out.n_parts = n_parts;
+  out.tet_part.assign(tet_part, tet_part + T);
+  std::vector<uint8_t> constrained;
+  mark_constrained(m, constrained);
+  // subdomain multiplicity of every edge: 1, 2 or "3 or more"
+  std::vector<int32_t> p1(E, -1), p2(E, -1);
+  std::vector<uint8_t> many(E, 0);
+  for (int64_t t = 0; t < T; ++t) {
+    const int32_t p = tet_part[t];
+    for (int k = 0; k < 6; ++k) {
+      const int32_t e = m.elem_edge[6 * t + k];
+      if (p1[e] < 0) p1[e] = p;
+      else if (p1[e] != p) {
+        if (p2[e] < 0) p2[e] = p;
+        else if (p2[e] != p) many[e] = 1;
+      }
+    }
+  }
+  std::vector<uint8_t> cls(E);
+  for (int64_t e = 0; e < E; ++e)
+    cls[e] = constrained[e] ? 0 : many[e] ? 1 : (p2[e] >= 0 ? 2 : 3);
+
+  EdgeGraph g = make_graph(m);
+  std::vector<uint8_t> seen(g.n_nodes, 0), tree(E, 0);
+  std::vector<int64_t> bucket[4];
+  size_t head[4] = {0, 0, 0, 0};
+  auto visit = [&](int32_t v) {
+    seen[v] = 1;
+    for (int64_t s = g.ptr[v]; s < g.ptr[v + 1]; ++s)
+      if (!seen[g.nb[s]]) bucket[cls[g.edge[s]]].push_back(s);
+  };
+  int32_t root = 0;
+  for (int64_t e = 0; e < E; ++e)
+    if (constrained[e]) { root = g.compact[m.edge_nodes[2 * e]]; break; }
+  int32_t cursor = 0;
+  if (g.n_nodes > 0) visit(root);
+  out.root = g.n_nodes > 0 ? root : -1;
+  for (;;) {
+    int c = 0;
+    while (c < 4 && head[c] >= bucket[c].size()) ++c;
+    if (c == 4) {
+      // next component: lowest unseen node
+      while (cursor < g.n_nodes && seen[cursor]) ++cursor;
+      if (cursor >= g.n_nodes) break;
+      visit(cursor);
+      continue;
+    }
+    const int64_t s = bucket[c][head[c]++];
+    const int32_t v = g.nb[s];
+    if (seen[v]) continue;
+    tree[g.edge[s]] = 1;
+    visit(v);
+  }
+
+  std::vector<uint8_t> primal(E, 0);
+  for (int64_t e = 0; e < E; ++e)
+    if (!tree[e] && !constrained[e] && cls[e] == 1) primal[e] = 1;
+
+  // Connect every subdomain: union-find over its nodes through its tree,
+  // Dirichlet and primal edges, then promote joining cotree edges.
+  std::vector<int64_t> tptr(static_cast<size_t>(n_parts) + 1, 0);
+  for (int64_t t = 0; t < T; ++t) tptr[tet_part[t] + 1]++;
+  for (int32_t p = 0; p < n_parts; ++p) tptr[p + 1] += tptr[p];
+  std::vector<int32_t> tlist(T);
+  {
+    std::vector<int64_t> cur(tptr.begin(), tptr.end() - 1);
+    for (int64_t t = 0; t < T; ++t) tlist[cur[tet_part[t]]++] = static_cast<int32_t>(t);
+  }
+  std::vector<int32_t> node_loc(m.n_nodes, -1), uf;
+  std::vector<int32_t> nodes, edges;
+  auto find = [&](int32_t a) {
+    while (uf[a] != a) { uf[a] = uf[uf[a]]; a = uf[a]; }
+    return a;
+  };
+  int64_t fixes = 0;
+  for (int32_t p = 0; p < n_parts; ++p) {
+    nodes.clear();
+    edges.clear();
+    for (int64_t q = tptr[p]; q < tptr[p + 1]; ++q) {
+      const int64_t t = tlist[q];
+      for (int a = 0; a < 4; ++a) {
+        const int32_t v = m.tets[4 * t + a];
+        if (node_loc[v] < 0) { node_loc[v] = static_cast<int32_t>(nodes.size()); nodes.push_back(v); }
+      }
+      for (int k = 0; k < 6; ++k) edges.push_back(m.elem_edge[6 * t + k]);
+    }
+    std::sort(edges.begin(), edges.end());
+    edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+    uf.resize(nodes.size());
+    std::iota(uf.begin(), uf.end(), 0);
+    for (int32_t e : edges) {
+      if (!(tree[e] || constrained[e] || primal[e])) continue;
+      int32_t a = find(node_loc[m.edge_nodes[2 * e]]), b = find(node_loc[m.edge_nodes[2 * e + 1]]);
+      if (a != b) uf[a] = b;
+    }
+    for (int32_t e : edges) {
+      if (tree[e] || constrained[e] || primal[e]) continue;
+      int32_t a = find(node_loc[m.edge_nodes[2 * e]]), b = find(node_loc[m.edge_nodes[2 * e + 1]]);
+      if (a != b) { uf[a] = b; primal[e] = 1; ++fixes; }
+    }
+    for (int32_t v : nodes) node_loc[v] = -1;
+  }
+
+  std::vector<int32_t> free_of(E);
+  int64_t nf = 0;
+  for (int64_t e = 0; e < E; ++e) free_of[e] = constrained[e] ? -1 : static_cast<int32_t>(nf++);
+  out.n_free = nf;
+  out.edge_dof.assign(E, -1);
+  int64_t nr = 0;
+  for (int64_t e = 0; e < E; ++e)
+    if (!tree[e] && !constrained[e]) {
+      out.edge_dof[e] = static_cast<int32_t>(nr++);
+      out.dof_primal.push_back(primal[e]);
+    }
+  out.n_dofs = nr;
+  out.n_primal_fix = fixes;
   out.l2g.resize(6 * T);
   for (int64_t p = 0; p < 6 * T; ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
   return EMG_SUCCESS;

@@ -1,0 +1,137 @@
+"""FETI-DP solve of the gauged TET4_EDGE curl-curl system on one GPU.
+
+The reference declares FETI-DP (``include/fetidp/fetidp_context.hpp:20-66``,
+``src/fetidp/fetidp_context.cpp:15-45``: a subdomain count and zeroed
+``SubdomainData`` records) but has no operators; this module is the host
+mirror of the library's FETI-DP entry points (``emg_dof_build_partitioned``,
+``emg_fetidp_*`` in ``include/emagddm_b200.h``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib, ptr
+
+
+@dataclass
+class PartitionedMap:
+    """Result of the partitioned tree-cotree gauge."""
+    l2g: np.ndarray          # (T, 6) int32, -1 = Dirichlet or tree edge
+    edge_dof: np.ndarray     # (E,) int32
+    n_free: int
+    n_dofs: int
+    n_parts: int
+    primal: np.ndarray       # (n_dofs,) int32 flags
+    n_primal_fix: int
+
+
+class _MeshHandle:
+    def __init__(self, m):
+        self.xyz = np.ascontiguousarray(m.xyz, np.float64)
+        self.tets = np.ascontiguousarray(m.tets, np.int32)
+        self.material = np.ascontiguousarray(m.material, np.int32)
+        d = np.ascontiguousarray(m.dirichlet, np.int32)
+        self.h = C.c_void_p()
+        check(lib().emg_mesh_create(self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0], ptr(self.tets),
+                                    ptr(self.material), d.shape[0], ptr(d) if d.size else None, 0,
+                                    C.byref(self.h)), "emg_mesh_create")
+
+    def __del__(self, _abi=_abi):
+        if getattr(self, "h", None) and _abi._LIB is not None:
+            _abi._LIB.emg_mesh_destroy(self.h)
+            self.h = None
+
+
+class _MapHandle:
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self, _abi=_abi):
+        if getattr(self, "h", None) and _abi._LIB is not None:
+            _abi._LIB.emg_dofmap_destroy(self.h)
+            self.h = None
+
+
+def partitioned_dofmap(m, tet_part, n_parts: int, keep_handles: bool = False):
+    """Gauge the mesh for a partition; with keep_handles also return the
+    (mesh, dofmap) handle owners the FETI-DP solver is created from."""
+    mh = _MeshHandle(m)
+    part = np.ascontiguousarray(tet_part, np.int32)
+    h = C.c_void_p()
+    check(lib().emg_dof_build_partitioned(mh.h, ptr(part), int(n_parts), C.byref(h)),
+          "emg_dof_build_partitioned")
+    ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+    lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
+    l2g = np.empty((m.n_tets, 6), np.int32)
+    ed = np.empty(ne.value, np.int32)
+    lib().emg_dofmap_export(h, ptr(l2g), ptr(ed))
+    npart, npri, nfix = C.c_int32(), C.c_int64(), C.c_int64()
+    pri = np.empty(nd.value, np.int32)
+    check(lib().emg_dofmap_partition_info(h, C.byref(npart), C.byref(npri), C.byref(nfix), ptr(pri)),
+          "emg_dofmap_partition_info")
+    pm = PartitionedMap(l2g, ed, nf.value, nd.value, npart.value, pri, nfix.value)
+    if keep_handles:
+        return pm, mh, _MapHandle(h)
+    lib().emg_dofmap_destroy(h)
+    return pm
+
+
+INFO_KEYS = ("n_parts", "n_dofs", "n_union", "n_lambda", "n_coarse", "n_fronts", "n_levels", "max_front",
+             "max_pivots", "factor_doubles", "update_pool_doubles", "dual_block_doubles", "sum_nI", "sum_nD",
+             "sum_nP", "max_nD", "max_children")
+STATS_KEYS = ("factor_ms", "solve_ms", "iterations", "lambda_residual", "residual")
+
+
+def plan_info(m, tet_part, n_parts: int) -> dict:
+    """Symbolic analysis on the host only (no GPU): sizes of the FETI-DP plan."""
+    pm, mh, maph = partitioned_dofmap(m, tet_part, n_parts, keep_handles=True)
+    info = np.zeros(len(INFO_KEYS), np.int64)
+    check(lib().emg_fetidp_plan_info(mh.h, maph.h, ptr(info), len(INFO_KEYS)), "emg_fetidp_plan_info")
+    return dict(zip(INFO_KEYS, (int(v) for v in info)))
+
+
+class FetiDP:
+    """FETI-DP solver for the partitioned, gauged system of mesh ``m``.
+
+    ``factor()`` runs the numeric phase for the mesh's materials and sources,
+    ``solve()`` returns (x, SolverResult-like dict) with x in the partitioned
+    map's numbering (``self.map.l2g``)."""
+
+    def __init__(self, m, tet_part, n_parts: int, stream=None):
+        self.m = m
+        self.map, self._mesh, self._maph = partitioned_dofmap(m, tet_part, n_parts, keep_handles=True)
+        self.h = C.c_void_p()
+        check(lib().emg_fetidp_create(self._mesh.h, self._maph.h, stream, C.byref(self.h)), "emg_fetidp_create")
+
+    def info(self) -> dict:
+        v = np.zeros(len(INFO_KEYS), np.int64)
+        check(lib().emg_fetidp_info(self.h, ptr(v), len(v)), "emg_fetidp_info")
+        return dict(zip(INFO_KEYS, (int(a) for a in v)))
+
+    def stats(self) -> dict:
+        v = np.zeros(len(STATS_KEYS))
+        check(lib().emg_fetidp_stats(self.h, ptr(v), len(v)), "emg_fetidp_stats")
+        return dict(zip(STATS_KEYS, (float(a) for a in v)))
+
+    def factor(self, flags: int = 0, nu=None, sigma=None) -> int:
+        nu = np.ascontiguousarray(self.m.nu if nu is None else nu, np.float64)
+        sg = np.ascontiguousarray(self.m.sigma if sigma is None else sigma, np.float64)
+        arr, ns = _abi.sources_array(self.m.sources)
+        return lib().emg_fetidp_factor(self.h, ptr(nu), ptr(sg), len(nu),
+                                       C.cast(arr, C.c_void_p) if arr is not None else None, ns, flags)
+
+    def solve(self, tol: float = 1e-10, max_iter: int = 500):
+        x = np.empty(self.map.n_dofs)
+        cfg = _abi.KrylovConfig(tol, max_iter, 0)
+        out = _abi.Result()
+        rc = lib().emg_fetidp_solve(self.h, C.byref(cfg), ptr(x), 0, C.byref(out))
+        return x, rc, out
+
+    def __del__(self, _abi=_abi):
+        if getattr(self, "h", None) and _abi._LIB is not None:
+            _abi._LIB.emg_fetidp_destroy(self.h)
+            self.h = None

@@ -126,6 +126,29 @@ def plain_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
                     name=f"cube{n}_iron_coil")
 
 
+def jittered_cuts(n: int, parts: int = 4, seed: int = 20261203, jitter: int | None = None):
+    """Cut positions (in cells) per axis: ``parts - 1`` planes at multiples of
+    n / parts, each moved by an integer in [-jitter, jitter] (default
+    n / parts / 8, i.e. slab widths 12..20 cells for n = 64, 4 parts), so
+    subdomain volumes vary about 0.4-2x."""
+    if n % parts:
+        raise ValueError("n must be a multiple of parts")
+    w = n // parts
+    j = max(w // 8, 1 if w >= 3 else 0) if jitter is None else jitter
+    rng = np.random.default_rng(seed)
+    return [np.array([k * w + int(rng.integers(-j, j + 1)) for k in range(1, parts)], np.int64)
+            for _ in range(3)]
+
+
+def jittered_partition(m: CubeMesh, parts: int = 4, seed: int = 20261203, jitter: int | None = None):
+    """Tet -> subdomain by centroid for a parts^3 box partition of the cube
+    with jittered cut planes; subdomain id = ix + parts * (iy + parts * iz)."""
+    cuts = jittered_cuts(m.n, parts, seed, jitter)
+    c = centroids(m.xyz, m.tets) * m.n
+    idx = [np.searchsorted(cuts[a], c[:, a], side="right") for a in range(3)]
+    return (idx[0] + parts * (idx[1] + parts * idx[2])).astype(np.int32)
+
+
 def random_instance(n: int, seed: int) -> CubeMesh:
     """One many-instance case: a random axis-aligned box with mu_r in
     [1, 1000] (1 elsewhere) and a uniform J_z in a random sub-box."""

@@ -122,6 +122,59 @@ int emg_dofmap_export(emg_dofmap map, int32_t* l2g, int32_t* edge_dof);
 int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full);
 void emg_dofmap_destroy(emg_dofmap map);
 
+/* ---- Tree-cotree gauge for a non-overlapping partition of the tets, the
+ * numbering the FETI-DP solver below works on.  No reference counterpart:
+ * the reference's FETI-DP layer is a stub (include/fetidp/fetidp_context.hpp:20-66,
+ * src/fetidp/fetidp_context.cpp:15-45).  tet_part[t] in [0, n_parts).  The
+ * tree spans the Dirichlet surface, then the subdomain wire baskets (edges
+ * shared by >= 3 subdomains), then each face, then each interior; reduced DOFs
+ * are the unconstrained cotree edges in ascending edge ID (as in the `ref`
+ * gauge's reduced map).  Primal DOFs: the cotree wire-basket edges, plus any
+ * cotree edge needed to connect a subdomain's tree.  Hole markers are
+ * rejected. */
+int emg_dof_build_partitioned(emg_mesh mesh, const int32_t* tet_part, int32_t n_parts,
+                              emg_dofmap* out);
+/* Partition data of a map from emg_dof_build_partitioned: primal: n_dofs flags
+ * (1 = primal) or NULL; n_parts / n_primal / n_primal_fix may be NULL.
+ * EMG_INVALID_INPUT for a map without a partition. */
+int emg_dofmap_partition_info(emg_dofmap map, int32_t* n_parts, int64_t* n_primal,
+                              int64_t* n_primal_fix, int32_t* primal);
+
+/* ---- FETI-DP (dual-primal domain decomposition) of the gauged curl-curl
+ * system on one GPU.  The reference has only the FETI-DP context
+ * (include/fetidp/fetidp_context.hpp:20-66: subdomain count and zeroed
+ * SubdomainData); the operators it leaves out are built here:
+ *   - local Neumann matrices K^(s) of every subdomain (one block-diagonal
+ *     GPU assembly), K_rr^(s) factored by a batched multifrontal Cholesky
+ *     (nested dissection inside the subdomain, dual DOFs last);
+ *   - the jump operator B (one multiplier per dual DOF, +1 on the lower
+ *     subdomain id) and its transpose;
+ *   - the primal coarse Schur complement S_cc, factored on the GPU;
+ *   - the Dirichlet preconditioner with stiffness scaling.
+ * The interface problem is solved by FP64 PCG; x is the global solution in
+ * the partitioned map's numbering (n_dofs), out->residual_norm the true
+ * ||F - K x|| / ||F|| of the global system and cfg->tolerance the stopping
+ * bound on the relative multiplier residual.  cfg->preconditioner is ignored.
+ * map must come from emg_dof_build_partitioned on the same mesh. */
+typedef struct emg_fetidp_t* emg_fetidp;
+int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* out);
+/* Numeric phase (materials and sources as emg_system_assemble; EMG_FLAG_MASS
+ * is ignored).  EMG_NUMERICAL_ERROR when a subdomain matrix is not positive
+ * definite. */
+int emg_fetidp_factor(emg_fetidp fd, const double* nu, const double* sigma, int32_t n_materials,
+                      const emg_source* sources, int32_t n_sources, int32_t flags);
+int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int32_t x_on_device,
+                     emg_result* out);
+/* info[0..16]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
+ * n_levels, max_front, max_pivots, factor doubles, update-pool doubles,
+ * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children. */
+int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
+/* stats[0..4]: factor ms, solve ms, iterations, multiplier residual, true residual. */
+int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats);
+void emg_fetidp_destroy(emg_fetidp fd);
+/* Host-only symbolic analysis (no GPU needed): the info[] of the plan. */
+int emg_fetidp_plan_info(emg_mesh mesh, emg_dofmap map, int64_t* info, int32_t n_info);
+
 /* ---- EMAssembly::assemble on the GPU (src/numeric/em_assembly.cpp:144-420)
  * A system owns the device copy of the geometry and DOF map, the CSR pattern
  * (merged, rows sorted: what SparseConverter::to_eigen yields), the stiffness
