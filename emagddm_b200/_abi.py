@@ -88,6 +88,7 @@ SIGNATURES = {
     "emg_fetidp_create": ([H, H, VP, C.POINTER(H)], C.c_int),
     "emg_fetidp_factor": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32], C.c_int),
     "emg_fetidp_solve": ([H, C.POINTER(KrylovConfig), VP, C.c_int32, C.POINTER(Result)], C.c_int),
+    "emg_fetidp_solve_rhs": ([H, C.POINTER(KrylovConfig), VP, VP, C.c_int32, C.POINTER(Result)], C.c_int),
     "emg_fetidp_info": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_stats": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_destroy": ([H], None),

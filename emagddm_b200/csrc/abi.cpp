@@ -607,24 +607,48 @@ int emg_fetidp_factor(emg_fetidp fd, const double* nu, const double* sigma, int3
   });
 }
 
+namespace {
+int fetidp_solve_impl(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x, int32_t on_device,
+                      emg_result* out) {
+  if (!fd || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  if (cfg->max_iterations < 0 || !(cfg->tolerance > 0.0)) {
+    set_error("bad tolerance or iteration limit");
+    return EMG_INVALID_INPUT;
+  }
+  emg::FetiDP& F = fd->fd;
+  const int64_t n = F.plan.n_dofs;
+  const double* bd = nullptr;
+  if (b) {
+    if (on_device) bd = b;
+    else {
+      cudaError_t e = cudaMemcpyAsync(F.rglob_d, b, sizeof(double) * n, cudaMemcpyHostToDevice, F.st);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return EMG_ERR_CUDA; }
+      bd = F.rglob_d;  // copied into the solver's own right-hand side before use
+    }
+  }
+  emg_result r{};
+  int rc = F.solve(*cfg, bd, on_device ? x : nullptr, &r);
+  if (rc == EMG_SUCCESS || rc == EMG_MAX_ITER_REACHED || rc == EMG_NUMERICAL_ERROR) {
+    if (x && !on_device) {
+      cudaError_t e = cudaMemcpy(x, F.xacc_d, sizeof(double) * n, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return EMG_ERR_CUDA; }
+    }
+    if (out) *out = r;
+  }
+  return rc;
+}
+}  // namespace
+
 int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int32_t x_on_device,
                      emg_result* out) {
+  return guarded([&]() -> int { return fetidp_solve_impl(fd, cfg, nullptr, x, x_on_device, out); });
+}
+
+int emg_fetidp_solve_rhs(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x,
+                         int32_t on_device, emg_result* out) {
   return guarded([&]() -> int {
-    if (!fd || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
-    if (cfg->max_iterations < 0 || !(cfg->tolerance > 0.0)) {
-      set_error("bad tolerance or iteration limit");
-      return EMG_INVALID_INPUT;
-    }
-    emg_result r{};
-    int rc = fd->fd.solve(*cfg, x_on_device ? x : nullptr, &r);
-    if (rc == EMG_SUCCESS || rc == EMG_MAX_ITER_REACHED || rc == EMG_NUMERICAL_ERROR) {
-      if (x && !x_on_device) {
-        cudaError_t e = cudaMemcpy(x, fd->fd.xg_d, sizeof(double) * fd->fd.plan.n_dofs, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return EMG_ERR_CUDA; }
-      }
-      if (out) *out = r;
-    }
-    return rc;
+    if (!b) { set_error("null right-hand side"); return EMG_INVALID_INPUT; }
+    return fetidp_solve_impl(fd, cfg, b, x, on_device, out);
   });
 }
 
@@ -637,8 +661,9 @@ int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info) {
 int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats) {
   if (!fd || (!stats && n_stats > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
   const emg::FetiStats& s = fd->fd.stats;
-  const double v[5] = {s.factor_ms, s.solve_ms, static_cast<double>(s.iterations), s.lambda_residual, s.residual};
-  for (int32_t i = 0; i < n_stats && i < 5; ++i) stats[i] = v[i];
+  const double v[6] = {s.factor_ms, s.solve_ms, static_cast<double>(s.iterations), s.lambda_residual, s.residual,
+                       static_cast<double>(s.refinements)};
+  for (int32_t i = 0; i < n_stats && i < 6; ++i) stats[i] = v[i];
   return EMG_SUCCESS;
 }
 

@@ -55,6 +55,12 @@ struct FetiPlan {
   std::vector<int64_t> cblk_off;          // n_parts + 1: nP x nP coarse blocks
   std::vector<int64_t> sc_ptr;            // n_coarse^2 + 1 (column-major targets)
   std::vector<int64_t> sc_list;           // coarse-block entries per target
+  // faces (deluxe scaling): the multipliers grouped by their subdomain pair
+  int32_t n_faces = 0;
+  std::vector<int32_t> face_a, face_b;    // subdomains, face_a < face_b
+  std::vector<int64_t> face_ptr;          // n_faces + 1 into face_lam
+  std::vector<int32_t> face_lam;          // multipliers of each face, ascending
+  std::vector<int64_t> face_off;          // n_faces + 1: f x f dense blocks (padded)
   // fronts (level order: by height, then subdomain, then postorder)
   std::vector<FetiFront> fronts;
   std::vector<int32_t> level_ptr;         // n_levels + 1

@@ -40,8 +40,21 @@ struct RhsDev {
   double* v;
 };
 
+// Faces of the deluxe scaling (multipliers grouped by subdomain pair).
+struct FacesDev {
+  int32_t n;
+  const int32_t* a;
+  const int32_t* b;
+  const int32_t* dim;
+  const int64_t* ptr;
+  const int32_t* lam;
+  const int64_t* off;  // f x f block offset of every face
+  const int64_t* fac;  // offset of the face's Sa + Sb factor block in fac
+};
+
 struct FetiStats {
-  int32_t iterations = 0;
+  int32_t iterations = 0;         // multiplier iterations over all correction passes
+  int32_t refinements = 0;        // FETI-DP passes (1 + defect corrections)
   double lambda_residual = 0.0;   // ||r_lambda|| / ||r_lambda,0||
   double residual = 0.0;          // true ||b - A x|| / ||b|| of the global system
   double factor_ms = 0.0, solve_ms = 0.0;
@@ -53,7 +66,9 @@ struct FetiDP {
   cudaStream_t st = nullptr;
   std::vector<void*> dev;
   FrontsDev fd{};
+  FacesDev fc{};
   bool factored = false;
+  int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 Dirichlet deluxe-scaled
   FetiStats stats;
   // plan tables
   int64_t* d_loc_off = nullptr;
@@ -75,6 +90,9 @@ struct FetiDP {
   int32_t* d_cdim = nullptr;
   int64_t *d_cfac = nullptr, *d_czero = nullptr;
   int64_t coarse_fac = 0;
+  // extra fronts after the plan's: [0] the coarse matrix, [1 + f] face f's S_a + S_b
+  std::vector<int32_t> xnp;
+  int32_t max_fdim = 0;
   // solve layouts
   int64_t *d_roff_s = nullptr, *d_roff1 = nullptr, *d_voff_s = nullptr, *d_voff1 = nullptr;
   int32_t *d_ncol_s = nullptr, *d_ncol1 = nullptr;
@@ -87,6 +105,9 @@ struct FetiDP {
   double *xu_d = nullptr, *ru_d = nullptr, *xg_d = nullptr, *rg_d = nullptr, *bg_d = nullptr;
   double *lam_d = nullptr, *r_d = nullptr, *z_d = nullptr, *p_d = nullptr, *q_d = nullptr, *rhs_d = nullptr;
   double* part_d = nullptr;
+  double *fSa_d = nullptr, *fSb_d = nullptr, *fX_d = nullptr, *fXt_d = nullptr, *fZ_d = nullptr;
+  double *fDa_d = nullptr, *fDb_d = nullptr, *c_d = nullptr;
+  double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr;
   void* state_d = nullptr;
   int32_t* err_d = nullptr;
   static constexpr int kParts = 592;
@@ -98,9 +119,10 @@ struct FetiDP {
   // Numeric phase for the given materials / sources.
   int factor(const double* nu, const double* sigma, int32_t n_mat, const emg_source* src, int32_t n_src,
              int32_t flags);
-  // lambda-PCG to cfg.tolerance (relative lambda residual), then recovery of
-  // the global solution x_d (n_dofs, device) and its true residual.
-  int solve(const emg_krylov_config& cfg, double* x_d, emg_result* res);
+  // K x = b for the global right-hand side b_d (device, n_dofs; null = the
+  // assembled F) to the true relative residual cfg.tolerance: FETI-DP passes
+  // (lambda-PCG, recovery) with defect correction on the true residual.
+  int solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, emg_result* res);
 
  private:
   template <class T>
@@ -114,6 +136,11 @@ struct FetiDP {
   void apply_F(const double* p, double* q, double* part);
   void apply_M(const double* r, double* z, double* part);
   int dot(const double* a, const double* b, int64_t n, int which);
+  int setup_deluxe();
+  int prepare_rhs(const double* fu);
+  int lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel);
+  int recover(const double* fu);
+  int global_residual(const double* b, const double* x, double* rr);
 };
 
 }  // namespace emg

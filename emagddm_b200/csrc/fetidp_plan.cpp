@@ -389,6 +389,37 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
       p.dual_sign[e] = plus ? 1 : -1;
       p.lam_entry[2 * static_cast<int64_t>(lam) + (plus ? 0 : 1)] = static_cast<int32_t>(e);
     }
+  // faces: multipliers grouped by (plus-side subdomain, minus-side subdomain)
+  {
+    std::vector<int32_t> dsub(p.dual_off[S]);
+    for (int32_t s = 0; s < S; ++s)
+      for (int64_t e = p.dual_off[s]; e < p.dual_off[s + 1]; ++e) dsub[e] = s;
+    std::vector<std::pair<int64_t, int32_t>> key(p.n_lambda);
+    for (int64_t l = 0; l < p.n_lambda; ++l)
+      key[l] = {static_cast<int64_t>(dsub[p.lam_entry[2 * l]]) * S + dsub[p.lam_entry[2 * l + 1]],
+                static_cast<int32_t>(l)};
+    std::sort(key.begin(), key.end());
+    p.face_ptr.push_back(0);
+    p.face_off.push_back(0);
+    for (int64_t i = 0; i < p.n_lambda; ++i) {
+      if (i == 0 || key[i].first != key[i - 1].first) {
+        if (i > 0) {
+          p.face_ptr.push_back(i);
+          const int64_t f = i - p.face_ptr[p.face_ptr.size() - 2];
+          p.face_off.push_back(p.face_off.back() + pad(f * f));
+        }
+        p.face_a.push_back(static_cast<int32_t>(key[i].first / S));
+        p.face_b.push_back(static_cast<int32_t>(key[i].first % S));
+      }
+      p.face_lam.push_back(key[i].second);
+    }
+    if (p.n_lambda > 0) {
+      p.face_ptr.push_back(p.n_lambda);
+      const int64_t f = p.n_lambda - p.face_ptr[p.face_ptr.size() - 2];
+      p.face_off.push_back(p.face_off.back() + pad(f * f));
+    }
+    p.n_faces = static_cast<int32_t>(p.face_a.size());
+  }
   // primal entries and coarse gather lists
   p.pri_coarse.resize(p.pri_off[S]);
   p.coarse_ptr.assign(static_cast<size_t>(p.n_coarse) + 1, 0);
@@ -539,6 +570,23 @@ int validate_feti_plan(const FetiPlan& p) {
   }
   for (int32_t c : p.pri_coarse)
     if (c < 0 || c >= p.n_coarse) return fail("coarse index");
+  if (static_cast<int64_t>(p.face_ptr.size()) != p.n_faces + 1 ||
+      static_cast<int64_t>(p.face_off.size()) != p.n_faces + 1 ||
+      static_cast<int64_t>(p.face_lam.size()) != p.n_lambda || p.face_ptr.back() != p.n_lambda)
+    return fail("face tables");
+  for (int32_t f = 0; f < p.n_faces; ++f) {
+    const int64_t n = p.face_ptr[f + 1] - p.face_ptr[f];
+    if (n < 1 || p.face_off[f + 1] - p.face_off[f] < n * n) return fail("face block");
+    if (p.face_a[f] < 0 || p.face_a[f] >= p.face_b[f] || p.face_b[f] >= S) return fail("face sides");
+    for (int64_t i = p.face_ptr[f]; i < p.face_ptr[f + 1]; ++i) {
+      const int32_t l = p.face_lam[i];
+      if (l < 0 || l >= p.n_lambda || (i > p.face_ptr[f] && l <= p.face_lam[i - 1])) return fail("face multipliers");
+      const int32_t ea = p.lam_entry[2 * l], eb = p.lam_entry[2 * l + 1];
+      if (ea < p.dual_off[p.face_a[f]] || ea >= p.dual_off[p.face_a[f] + 1] || eb < p.dual_off[p.face_b[f]] ||
+          eb >= p.dual_off[p.face_b[f] + 1])
+        return fail("face entries");
+    }
+  }
   for (int64_t e : p.sc_list)
     if (e < 0 || e >= p.cblk_off[S]) return fail("coarse block entry");
   const int32_t F = static_cast<int32_t>(p.fronts.size());

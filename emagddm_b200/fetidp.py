@@ -83,7 +83,7 @@ def partitioned_dofmap(m, tet_part, n_parts: int, keep_handles: bool = False):
 INFO_KEYS = ("n_parts", "n_dofs", "n_union", "n_lambda", "n_coarse", "n_fronts", "n_levels", "max_front",
              "max_pivots", "factor_doubles", "update_pool_doubles", "dual_block_doubles", "sum_nI", "sum_nD",
              "sum_nP", "max_nD", "max_children")
-STATS_KEYS = ("factor_ms", "solve_ms", "iterations", "lambda_residual", "residual")
+STATS_KEYS = ("factor_ms", "solve_ms", "iterations", "lambda_residual", "residual", "passes")
 
 
 def plan_info(m, tet_part, n_parts: int) -> dict:
@@ -124,11 +124,21 @@ class FetiDP:
         return lib().emg_fetidp_factor(self.h, ptr(nu), ptr(sg), len(nu),
                                        C.cast(arr, C.c_void_p) if arr is not None else None, ns, flags)
 
-    def solve(self, tol: float = 1e-10, max_iter: int = 500):
+    def solve(self, tol: float = 1e-10, max_iter: int = 500, precond: int = 2):
+        """precond: 0 none, 1 Dirichlet with stiffness scaling, 2 Dirichlet with deluxe scaling."""
         x = np.empty(self.map.n_dofs)
-        cfg = _abi.KrylovConfig(tol, max_iter, 0)
+        cfg = _abi.KrylovConfig(tol, max_iter, precond)
         out = _abi.Result()
         rc = lib().emg_fetidp_solve(self.h, C.byref(cfg), ptr(x), 0, C.byref(out))
+        return x, rc, out
+
+    def solve_rhs(self, b, tol: float = 1e-10, max_iter: int = 500, precond: int = 2):
+        """Solve with a caller's right-hand side (n_dofs, this map's numbering)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.empty(self.map.n_dofs)
+        cfg = _abi.KrylovConfig(tol, max_iter, precond)
+        out = _abi.Result()
+        rc = lib().emg_fetidp_solve_rhs(self.h, C.byref(cfg), ptr(b), ptr(x), 0, C.byref(out))
         return x, rc, out
 
     def __del__(self, _abi=_abi):

@@ -150,12 +150,20 @@ int emg_dofmap_partition_info(emg_dofmap map, int32_t* n_parts, int64_t* n_prima
  *   - the jump operator B (one multiplier per dual DOF, +1 on the lower
  *     subdomain id) and its transpose;
  *   - the primal coarse Schur complement S_cc, factored on the GPU;
- *   - the Dirichlet preconditioner with stiffness scaling.
+ *   - the Dirichlet preconditioner, scaled per face by "deluxe" weights
+ *     (S_a,F + S_b,F)^-1 S_b,F built from the two sides' Schur complements,
+ *     which keeps the iteration count flat across coefficient jumps that cut
+ *     through subdomains, or by diagonal stiffness weights.
  * The interface problem is solved by FP64 PCG; x is the global solution in
  * the partitioned map's numbering (n_dofs), out->residual_norm the true
- * ||F - K x|| / ||F|| of the global system and cfg->tolerance the stopping
- * bound on the relative multiplier residual.  cfg->preconditioner is ignored.
- * map must come from emg_dof_build_partitioned on the same mesh. */
+ * ||F - K x|| / ||F|| of the global system and cfg->tolerance the bound on
+ * it: a multiplier PCG pass (inner relative tolerance 1e-10) is followed by
+ * defect-correction passes on the true residual until it holds, the residual
+ * stops shrinking, or cfg->max_iterations multiplier iterations are spent in
+ * total.  cfg->preconditioner:
+ * EMG_FETI_PRECOND_NONE, _STIFFNESS or _DELUXE.  map must come from
+ * emg_dof_build_partitioned on the same mesh. */
+enum { EMG_FETI_PRECOND_NONE = 0, EMG_FETI_PRECOND_STIFFNESS = 1, EMG_FETI_PRECOND_DELUXE = 2 };
 typedef struct emg_fetidp_t* emg_fetidp;
 int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* out);
 /* Numeric phase (materials and sources as emg_system_assemble; EMG_FLAG_MASS
@@ -165,11 +173,18 @@ int emg_fetidp_factor(emg_fetidp fd, const double* nu, const double* sigma, int3
                       const emg_source* sources, int32_t n_sources, int32_t flags);
 int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int32_t x_on_device,
                      emg_result* out);
+/* Same for a caller's global right-hand side b (n_dofs, the partitioned map's
+ * numbering) instead of the assembled F; b and x are both host or both device
+ * arrays.  The factorization is reused, so many right-hand sides cost one
+ * emg_fetidp_factor. */
+int emg_fetidp_solve_rhs(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x,
+                         int32_t on_device, emg_result* out);
 /* info[0..16]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
  * n_levels, max_front, max_pivots, factor doubles, update-pool doubles,
  * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children. */
 int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
-/* stats[0..4]: factor ms, solve ms, iterations, multiplier residual, true residual. */
+/* stats[0..5]: factor ms, solve ms, iterations, multiplier residual, true
+ * residual, FETI-DP passes. */
 int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats);
 void emg_fetidp_destroy(emg_fetidp fd);
 /* Host-only symbolic analysis (no GPU needed): the info[] of the plan. */
