@@ -335,70 +335,201 @@ __global__ void __launch_bounds__(512) k_trtri(int32_t n_mat, const int32_t* __r
 
 // ------------------------------------------------------ multifrontal solve
 
-// Forward sweep, one warp per (front, right-hand-side column): add the
-// children's update vectors, eliminate the pivots, leave this front's update
-// vector for the parent.
-__global__ void k_front_fwd(FrontsDev F, int32_t f0, RhsDev R, const int32_t* __restrict__ nI,
-                            const int32_t* __restrict__ nD, const double* __restrict__ fac) {
+// Blocked variants, one CTA (256 threads) per (front, column), root fronts
+// skipped (they are solved with L^-1).  Forward: per block of 32 pivots one
+// warp solves the diagonal block, then all warps update the rows below it.
+constexpr int kSB = 32;
+
+__global__ void __launch_bounds__(256) k_front_fwd_blk(FrontsDev F, int32_t f0, RhsDev R,
+                                                       const int32_t* __restrict__ nI,
+                                                       const int32_t* __restrict__ nD,
+                                                       const double* __restrict__ fac) {
   const int32_t k = f0 + blockIdx.y;
+  if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
   const int32_t col = blockIdx.x;
   if (col >= R.ncol[s]) return;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
   const int32_t ld = nI[s] + nD[s];
   double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
   double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
-  for (int32_t i = lane; i < nu; i += 32) V[i] = 0.0;
-  __syncwarp();
+  for (int32_t i = tid; i < nu; i += blockDim.x) V[i] = 0.0;
+  __syncthreads();
   for (int32_t ci = 0; ci < F.nchild[k]; ++ci) {
     const int32_t c = F.child_v[F.child0[k] + ci];
     const int32_t ncu = F.f[c] - F.npiv[c];
     const double* Vc = R.v + R.voff[c] + static_cast<int64_t>(col) * ncu;
     const int32_t* cp = F.cpos_v + F.cpos[c];
-    for (int32_t a = lane; a < ncu; a += 32) {
+    for (int32_t a = tid; a < ncu; a += blockDim.x) {
       const int32_t r = cp[a];
       if (r < np) x[p0 + r] += Vc[a];
       else V[r - np] += Vc[a];
     }
-    __syncwarp();
+    __syncthreads();
   }
   const double* L = fac + F.fac[k];
-  for (int32_t j = 0; j < np; ++j) {
-    const double* Lj = L + static_cast<int64_t>(j) * fs;
-    const double yj = x[p0 + j] / Lj[j];
-    __syncwarp();
-    if (lane == 0) x[p0 + j] = yj;
-    for (int32_t i = j + 1 + lane; i < fs; i += 32) {
-      const double t = Lj[i] * yj;
-      if (i < np) x[p0 + i] -= t;
-      else V[i - np] -= t;
+  __shared__ double yb[kSB];
+  for (int32_t jb = 0; jb < np; jb += kSB) {
+    const int32_t nb = min(kSB, np - jb);
+    if (wid == 0) {
+      double v = lane < nb ? x[p0 + jb + lane] : 0.0;
+      for (int32_t j = 0; j < nb; ++j) {
+        const double* Lj = L + static_cast<int64_t>(jb + j) * fs + jb;
+        const double yj = __shfl_sync(0xffffffffu, v, j) / Lj[j];
+        if (lane == j) v = yj;
+        if (lane > j && lane < nb) v -= Lj[lane] * yj;
+      }
+      if (lane < nb) { x[p0 + jb + lane] = v; yb[lane] = v; }
     }
-    __syncwarp();
+    __syncthreads();
+    for (int32_t i = jb + nb + tid; i < fs; i += blockDim.x) {
+      double acc = 0.0;
+      for (int32_t j = 0; j < nb; ++j) acc = fma(L[i + static_cast<int64_t>(jb + j) * fs], yb[j], acc);
+      if (i < np) x[p0 + i] -= acc;
+      else V[i - np] -= acc;
+    }
+    __syncthreads();
   }
 }
 
-// Backward sweep: x_piv = L11^-T (y_piv - L21^T x_border), border values final.
-__global__ void k_front_bwd(FrontsDev F, int32_t f0, RhsDev R, const int32_t* __restrict__ nI,
-                            const int32_t* __restrict__ nD, const double* __restrict__ fac) {
+// Backward: per block (last first) the warps form the dot products with the
+// rows below the block, then one warp solves the diagonal block.
+__global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, RhsDev R,
+                                                       const int32_t* __restrict__ nI,
+                                                       const int32_t* __restrict__ nD,
+                                                       const double* __restrict__ fac) {
   const int32_t k = f0 + blockIdx.y;
+  if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
   const int32_t col = blockIdx.x;
   if (col >= R.ncol[s]) return;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
   const int32_t ld = nI[s] + nD[s];
   double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
   const int32_t* rows = F.rows_v + F.rows[k];
   const double* L = fac + F.fac[k];
-  for (int32_t j = np - 1; j >= 0; --j) {
-    const double* Lj = L + static_cast<int64_t>(j) * fs;
-    double acc = 0.0;
-    for (int32_t i = j + 1 + lane; i < fs; i += 32) acc += Lj[i] * x[i < np ? p0 + i : rows[i]];
-    acc = warp_sum(acc);
-    if (lane == 0) x[p0 + j] = (x[p0 + j] - acc) / Lj[j];
-    __syncwarp();
+  __shared__ double tb[kSB];
+  for (int32_t jb = ((np - 1) / kSB) * kSB; jb >= 0; jb -= kSB) {
+    const int32_t nb = min(kSB, np - jb);
+    for (int32_t j = wid; j < nb; j += nw) {
+      const double* Lj = L + static_cast<int64_t>(jb + j) * fs;
+      double acc = 0.0;
+      for (int32_t i = jb + nb + lane; i < fs; i += 32) acc = fma(Lj[i], x[i < np ? p0 + i : rows[i]], acc);
+      acc = warp_sum(acc);
+      if (lane == 0) tb[j] = acc;
+    }
+    __syncthreads();
+    if (wid == 0) {
+      double v = lane < nb ? x[p0 + jb + lane] - tb[lane] : 0.0;
+      for (int32_t j = nb - 1; j >= 0; --j) {
+        const double* Lj = L + static_cast<int64_t>(jb + j) * fs + jb;
+        // x_j = (v_j - sum_{i > j in block} L[i, j] x_i) / L[j, j]
+        double part = (lane > j && lane < nb) ? Lj[lane] * v : 0.0;
+        part = warp_sum(part);
+        const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / Lj[j];
+        if (lane == j) v = xj;
+      }
+      if (lane < nb) x[p0 + jb + lane] = v;
+    }
+    __syncthreads();
   }
+}
+
+// Root fronts, forward part: add the children's update vectors into x_D.
+__global__ void k_root_gather(FrontsDev F, const int32_t* __restrict__ root_k, RhsDev R,
+                              const int32_t* __restrict__ nI, const int32_t* __restrict__ nD) {
+  const int32_t k = root_k[blockIdx.y];
+  const int32_t s = F.sub[k];
+  const int32_t col = blockIdx.x;
+  if (col >= R.ncol[s]) return;
+  const int32_t ld = nI[s] + nD[s], p0 = F.p0[k];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  for (int32_t ci = 0; ci < F.nchild[k]; ++ci) {
+    const int32_t c = F.child_v[F.child0[k] + ci];
+    const int32_t ncu = F.f[c] - F.npiv[c];
+    const double* Vc = R.v + R.voff[c] + static_cast<int64_t>(col) * ncu;
+    const int32_t* cp = F.cpos_v + F.cpos[c];
+    for (int32_t a = threadIdx.x; a < ncu; a += blockDim.x) x[p0 + cp[a]] += Vc[a];
+    __syncthreads();
+  }
+}
+
+// Root solve x_D = L^-T (L^-1 x_D) with the mirrored inverse M (M = L^-1 in
+// the lower triangle, its transpose in the upper): pass 0 tmp = L^-1 x_D
+// (column c, rows <= c), pass 1 x_D = L^-T tmp (column c, rows >= c).  One
+// warp per (root, column, row c).
+__global__ void __launch_bounds__(256) k_root_apply(const int32_t* __restrict__ root_sub, RhsDev R,
+                                                    const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
+                                                    const int64_t* __restrict__ root_off, const double* __restrict__ M,
+                                                    const int64_t* __restrict__ rvoff, double* __restrict__ tmp,
+                                                    int32_t max_ncol, int pass) {
+  const int32_t r = blockIdx.y / max_ncol, col = blockIdx.y - r * max_ncol;
+  const int32_t s = root_sub[r];
+  if (col >= R.ncol[s]) return;
+  const int32_t n = nD[s];
+  const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= n) return;
+  const int lane = threadIdx.x & 31;
+  const int32_t ld = nI[s] + n;
+  double* xd = R.x + R.off[s] + static_cast<int64_t>(col) * ld + nI[s];
+  double* t = tmp + rvoff[r] * max_ncol + static_cast<int64_t>(col) * n;
+  const double* Mc = M + root_off[s] + static_cast<int64_t>(c) * n;
+  double acc = 0.0;
+  if (pass == 0) {
+    for (int32_t i = lane; i <= c; i += 32) acc = fma(Mc[i], xd[i], acc);
+  } else {
+    for (int32_t i = c + lane; i < n; i += 32) acc = fma(Mc[i], t[i], acc);
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) {
+    if (pass == 0) t[c] = acc;
+    else xd[c] = acc;
+  }
+}
+
+// Mirror the lower triangle of each n x n block into its upper triangle.
+__global__ void k_mirror_lower(int32_t n_mat, const int32_t* __restrict__ dim, const int64_t* __restrict__ off,
+                               double* __restrict__ M) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m];
+  double* A = M + off[m];
+  const int64_t tot = static_cast<int64_t>(n) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t j = static_cast<int32_t>(e / n), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * n);
+    if (i < j) A[e] = A[j + static_cast<int64_t>(i) * n];
+  }
+}
+
+// Column-dot mat-vec of dense blocks: y_c = sum over rows r in the range of
+// column c of M[r, c] w_r; range 0: r <= c, 1: r >= c, 2: all rows.
+__global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                       const int64_t* __restrict__ m_off,
+                                                       const double* __restrict__ M,
+                                                       const int64_t* __restrict__ v_off,
+                                                       const double* __restrict__ w, double* __restrict__ y,
+                                                       int range) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m];
+  const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= n) return;
+  const int lane = threadIdx.x & 31;
+  const double* Mc = M + m_off[m] + static_cast<int64_t>(c) * n;
+  const double* wm = w + v_off[m];
+  const int32_t lo = range == 1 ? c : 0, hi = range == 0 ? c + 1 : n;
+  double a0 = 0.0, a1 = 0.0;
+  int32_t i = lo + lane;
+  for (; i + 32 < hi; i += 64) {
+    a0 = fma(Mc[i], wm[i], a0);
+    a1 = fma(Mc[i + 32], wm[i + 32], a1);
+  }
+  if (i < hi) a0 = fma(Mc[i], wm[i], a0);
+  const double acc = warp_sum(a0 + a1);
+  if (lane == 0) y[v_off[m] + c] = acc;
 }
 
 // ---------------------------------------------- right-hand sides, coarse
@@ -523,52 +654,6 @@ __global__ void __launch_bounds__(256) k_lambda_scatter(int64_t nl, const int32_
     acc = block_sum(acc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = acc;
   }
-}
-
-// Row-parallel mat-vec of dense per-subdomain blocks: y_m = M_m w_m with M_m
-// column-major n x n; lower != 0 uses only j <= i (y = tril(M) w).
-__global__ void __launch_bounds__(128) k_block_gemv(int32_t n_mat, const int32_t* __restrict__ dim,
-                                                    const int64_t* __restrict__ m_off, const double* __restrict__ M,
-                                                    const int64_t* __restrict__ v_off, const double* __restrict__ w,
-                                                    double* __restrict__ y, int lower) {
-  const int32_t m = blockIdx.y;
-  if (m >= n_mat) return;
-  const int32_t n = dim[m];
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double* wm = w + v_off[m];
-  const double* Mi = M + m_off[m] + i;
-  const int32_t jend = lower ? i + 1 : n;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int32_t j = 0;
-  for (; j + 4 <= jend; j += 4) {
-    a0 = fma(Mi[static_cast<int64_t>(j) * n], __ldg(wm + j), a0);
-    a1 = fma(Mi[static_cast<int64_t>(j + 1) * n], __ldg(wm + j + 1), a1);
-    a2 = fma(Mi[static_cast<int64_t>(j + 2) * n], __ldg(wm + j + 2), a2);
-    a3 = fma(Mi[static_cast<int64_t>(j + 3) * n], __ldg(wm + j + 3), a3);
-  }
-  for (; j < jend; ++j) a0 = fma(Mi[static_cast<int64_t>(j) * n], __ldg(wm + j), a0);
-  y[v_off[m] + i] = (a0 + a1) + (a2 + a3);
-}
-
-// Column-parallel transposed mat-vec over the lower triangle: y_j = sum_{i>=j} M[i, j] w_i.
-__global__ void __launch_bounds__(256) k_block_gemv_lt(int32_t n_mat, const int32_t* __restrict__ dim,
-                                                       const int64_t* __restrict__ m_off,
-                                                       const double* __restrict__ M,
-                                                       const int64_t* __restrict__ v_off,
-                                                       const double* __restrict__ w, double* __restrict__ y) {
-  const int32_t m = blockIdx.y;
-  if (m >= n_mat) return;
-  const int32_t n = dim[m];
-  const int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (j >= n) return;
-  const int lane = threadIdx.x & 31;
-  const double* Mj = M + m_off[m] + static_cast<int64_t>(j) * n;
-  const double* wm = w + v_off[m];
-  double acc = 0.0;
-  for (int32_t i = j + lane; i < n; i += 32) acc = fma(Mj[i], wm[i], acc);
-  acc = warp_sum(acc);
-  if (lane == 0) y[v_off[m] + j] = acc;
 }
 
 // t[P] = add[P] + sum over the primal entries (s, p) of coarse DOF P of Phi_D[:, p] . w_s
@@ -1014,6 +1099,12 @@ int FetiDP::setup_device() {
     max_nD = std::max(max_nD, P.nD[s]);
   }
   n_roots = static_cast<int32_t>(rdim.size());
+  {
+    std::vector<int32_t> rk, rs;
+    for (int32_t s2 = 0; s2 < S; ++s2)
+      if (P.nD[s2] > 0) { rk.push_back(P.root_front[s2]); rs.push_back(s2); }
+    if ((rc = up(&d_root_k, rk)) || (rc = up(&d_root_sub, rs))) return rc;
+  }
   std::vector<int32_t> cdim{P.n_coarse};
   std::vector<int64_t> cfac{coarse_fac}, czero{0};
   if ((rc = up(&d_rdim, rdim)) || (rc = up(&d_rfac, rfac)) || (rc = up(&d_roff, roff)) ||
@@ -1058,7 +1149,8 @@ int FetiDP::setup_device() {
   if ((rc = zalloc(&fSa_d, fsz)) || (rc = zalloc(&fSb_d, fsz)) || (rc = zalloc(&fX_d, fsz)) ||
       (rc = zalloc(&fXt_d, fsz)) || (rc = zalloc(&fZ_d, fsz)) || (rc = zalloc(&fDa_d, fsz)) ||
       (rc = zalloc(&fDb_d, fsz)) || (rc = zalloc(&c_d, nd)) || (rc = zalloc(&fu_d, P.n_union)) ||
-      (rc = zalloc(&xacc_d, P.n_dofs)) || (rc = zalloc(&rglob_d, P.n_dofs)))
+      (rc = zalloc(&xacc_d, P.n_dofs)) || (rc = zalloc(&rglob_d, P.n_dofs)) ||
+      (rc = zalloc(&root_tmp_d, nd * max_ncol)))
     return rc;
   if ((rc = zalloc(&fac_d, P.fac_size + nc2 + fsz)) || (rc = zalloc(&upd_d, P.upd_pool)) ||
       (rc = zalloc(&S_d, P.root_off[S])) || (rc = zalloc(&Linv_d, P.root_off[S])) ||
@@ -1136,19 +1228,32 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   return EMG_SUCCESS;
 }
 
+// Multifrontal forward / backward solve of K_rr x = b for ncol right-hand
+// sides: blocked front kernels level by level, the root (dual) fronts with
+// their explicit inverse factors.
 int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   const int32_t nlev = static_cast<int32_t>(plan.level_ptr.size()) - 1;
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf > 0)
-      k_front_fwd<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 32, 0, st>>>(fd, f0, R, d_nI,
-                                                                                               d_nD, fac_d);
+      k_front_fwd_blk<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 256, 0, st>>>(fd, f0, R, d_nI,
+                                                                                                    d_nD, fac_d);
+  }
+  if (n_roots > 0) {
+    const unsigned rc = static_cast<unsigned>(n_roots * ncol);
+    k_root_gather<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(n_roots)), 256, 0, st>>>(fd, d_root_k, R,
+                                                                                                     d_nI, d_nD);
+    const unsigned gx = static_cast<unsigned>((max_nD + 7) / 8);
+    k_root_apply<<<dim3(gx, rc), 256, 0, st>>>(d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d,
+                                               ncol, 0);
+    k_root_apply<<<dim3(gx, rc), 256, 0, st>>>(d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d,
+                                               ncol, 1);
   }
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf > 0)
-      k_front_bwd<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 32, 0, st>>>(fd, f0, R, d_nI,
-                                                                                               d_nD, fac_d);
+      k_front_bwd_blk<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 256, 0, st>>>(fd, f0, R, d_nI,
+                                                                                                    d_nD, fac_d);
   }
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -1158,10 +1263,9 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
 void FetiDP::coarse_solve(const double* t, double* u) {
   const int32_t nc = plan.n_coarse;
   if (nc == 0) return;
-  k_block_gemv<<<dim3(static_cast<unsigned>((nc + 127) / 128), 1), 128, 0, st>>>(1, d_cdim, d_czero, Lcc_d,
-                                                                                 d_czero, t, t2_d, 1);
-  k_block_gemv_lt<<<dim3(static_cast<unsigned>((nc + 7) / 8), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d,
-                                                                                d_czero, t2_d, u);
+  const dim3 g(static_cast<unsigned>((nc + 7) / 8), 1);
+  k_block_colgemv<<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t, t2_d, 0);
+  k_block_colgemv<<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t2_d, u, 1);
 }
 
 // q = (F_rr + G S_cc^-1 G^T) p, part = per-block partials of p . q
@@ -1170,10 +1274,9 @@ void FetiDP::apply_F(const double* p, double* q, double* part) {
   const int64_t ne = P.dual_off[P.n_parts];
   RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, p, w_d);
-  const unsigned gx = static_cast<unsigned>((max_nD + 127) / 128), gy = static_cast<unsigned>(n_roots);
-  k_block_gemv<<<dim3(gx, gy), 128, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 1);
-  k_block_gemv_lt<<<dim3(static_cast<unsigned>((max_nD + 7) / 8), gy), 256, 0, st>>>(n_roots, d_rdim, d_roff,
-                                                                                     Linv_d, d_rvoff, y2_d, y_d);
+  const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
+  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
+  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
   if (P.n_coarse > 0) {
     k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
         P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, nullptr, t_d);
@@ -1198,19 +1301,19 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     k_dot_part<<<kParts, 256, 0, st>>>(P.n_lambda, r, z, part);
     return;
   }
-  const unsigned gx = static_cast<unsigned>((max_nD + 127) / 128), gy = static_cast<unsigned>(n_roots);
+  const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
   if (precond == 2 && P.n_faces > 0) {
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
     k_face_w<<<dim3(static_cast<unsigned>((max_fdim + 127) / 128), nfs), 128, 0, st>>>(fc, d_lam_entry, fDa_d,
                                                                                      fDb_d, r, w_d);
-    k_block_gemv<<<dim3(gx, gy), 128, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 0);
+    k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
     k_face_c<<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
                                                                                   y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, wt_d, r, w_d);
-  k_block_gemv<<<dim3(gx, gy), 128, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 0);
+  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
   k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, wt_d, y_d, z, r, part);
 }
 
@@ -1306,9 +1409,12 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   }
   if (!rc) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
-  if (n_roots > 0)
+  if (n_roots > 0) {
     k_trtri<<<dim3(static_cast<unsigned>((max_nD + 15) / 16), static_cast<unsigned>(n_roots)), 512, 0, st>>>(
         n_roots, d_rdim, d_rfac, d_roff, fac_d, Linv_d);
+    k_mirror_lower<<<dim3(blocks_for(static_cast<int64_t>(max_nD) * max_nD, 256, 256),
+                          static_cast<unsigned>(n_roots)), 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d);
+  }
   // Phi = K_rr^-1 K_rP (columns 0..nP-1) and z = K_rr^-1 f_r (column nP)
   EMG_CK(cudaMemsetAsync(phi_d, 0, sizeof(double) * std::max<int64_t>(phi_size, 1), st));
   RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
@@ -1330,6 +1436,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     if (!rc) rc = check_err("FETI-DP coarse factorization");
     if (rc) return rc;
     k_trtri<<<dim3(static_cast<unsigned>((nc + 15) / 16), 1), 512, 0, st>>>(1, d_cdim, d_cfac, d_czero, fac_d, Lcc_d);
+    k_mirror_lower<<<dim3(blocks_for(nc * nc, 256, 256), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d);
   }
   const int64_t ne = P.dual_off[S];
   if (ne > 0) {

@@ -86,6 +86,7 @@ struct FetiDP {
   // dense blocks
   int32_t n_roots = 0, max_nD = 0, max_ncol = 1;
   int32_t* d_rdim = nullptr;
+  int32_t *d_root_k = nullptr, *d_root_sub = nullptr;
   int64_t *d_rfac = nullptr, *d_roff = nullptr, *d_rvoff = nullptr;
   int32_t* d_cdim = nullptr;
   int64_t *d_cfac = nullptr, *d_czero = nullptr;
@@ -107,7 +108,7 @@ struct FetiDP {
   double* part_d = nullptr;
   double *fSa_d = nullptr, *fSb_d = nullptr, *fX_d = nullptr, *fXt_d = nullptr, *fZ_d = nullptr;
   double *fDa_d = nullptr, *fDb_d = nullptr, *c_d = nullptr;
-  double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr;
+  double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr, *root_tmp_d = nullptr;
   void* state_d = nullptr;
   int32_t* err_d = nullptr;
   static constexpr int kParts = 592;
