@@ -308,28 +308,90 @@ __global__ void __launch_bounds__(256) k_syrk_update(FrontsDev F, int32_t f0, co
 
 // --------------------------------------------------- triangular inverse
 
-// X = L^-1 for a list of lower-triangular matrices (column-major, ld n).
-// One warp per column c: forward substitution of L x = e_c in place in X.
-__global__ void __launch_bounds__(512) k_trtri(int32_t n_mat, const int32_t* __restrict__ dim,
-                                               const int64_t* __restrict__ l_off, const int64_t* __restrict__ x_off,
-                                               const double* __restrict__ Lbase, double* __restrict__ Xbase) {
+// Blocked X = L^-1: one CTA per 64-column block J of one matrix; row blocks
+// I = J, J+1, ... in order: X_IJ = L_II^-1 (E_IJ - sum_{J<=K<I} L_IK X_KJ),
+// the sum as 64 x 64 tile products staged in shared memory, the small
+// triangular solve in shared memory.  The strict upper part of X is zero.
+constexpr int kTB = 64;
+constexpr size_t kTrtriSmem = sizeof(double) * 2 * kTB * (kTB + 1);
+
+__global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                   const int64_t* __restrict__ l_off,
+                                                   const int64_t* __restrict__ x_off,
+                                                   const double* __restrict__ Lbase, double* __restrict__ Xbase) {
+  extern __shared__ double sm[];
   const int32_t m = blockIdx.y;
   if (m >= n_mat) return;
   const int32_t n = dim[m];
-  const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (c >= n) return;
-  const int lane = threadIdx.x & 31;
+  const int32_t c0 = blockIdx.x * kTB;
+  if (c0 >= n) return;
+  const int32_t w = min(kTB, n - c0);
   const double* L = Lbase + l_off[m];
-  double* x = Xbase + x_off[m] + static_cast<int64_t>(c) * n;
-  for (int32_t i = lane; i < n; i += 32) x[i] = i == c ? 1.0 : 0.0;
-  __syncwarp();
-  for (int32_t j = c; j < n; ++j) {
-    const double* Lj = L + static_cast<int64_t>(j) * n;
-    const double xj = x[j] / Lj[j];
-    __syncwarp();
-    if (lane == 0) x[j] = xj;
-    for (int32_t i = j + 1 + lane; i < n; i += 32) x[i] -= Lj[i] * xj;
-    __syncwarp();
+  double* X = Xbase + x_off[m];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double (*As)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);               // [kKC][kTB+1]
+  double (*Bs)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kKC * (kTB + 1));
+  double (*T)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);                // [kTB][kTB+1]
+  double (*Ls)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kTB * (kTB + 1));
+  for (int64_t e = tid; e < static_cast<int64_t>(c0) * w; e += blockDim.x) {
+    const int32_t c = static_cast<int32_t>(e / c0), r = static_cast<int32_t>(e - static_cast<int64_t>(c) * c0);
+    X[r + static_cast<int64_t>(c0 + c) * n] = 0.0;
+  }
+  const int32_t nb = (n + kTB - 1) / kTB;
+  for (int32_t I = blockIdx.x; I < nb; ++I) {
+    const int32_t r0 = I * kTB, h = min(kTB, n - r0);
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = (r0 == c0 && 4 * tx + a == 4 * ty + b) ? 1.0 : 0.0;
+    for (int32_t k0 = c0; k0 < r0; k0 += kKC) {  // K blocks left of I are full
+      __syncthreads();
+      for (int e = tid; e < kKC * kTB; e += blockDim.x) {
+        const int k = e / kTB, r = e - k * kTB;
+        As[k][r] = r < h ? L[(r0 + r) + static_cast<int64_t>(k0 + k) * n] : 0.0;
+      }
+      for (int e = tid; e < kKC * kTB; e += blockDim.x) {
+        const int c = e / kKC, k = e - c * kKC;
+        Bs[k][c] = c < w ? X[(k0 + k) + static_cast<int64_t>(c0 + c) * n] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int k = 0; k < kKC; ++k) {
+        double a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { a[q] = As[k][4 * tx + q]; b[q] = Bs[k][4 * ty + q]; }
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] = fma(-a[x], b[y], acc[x][y]);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) T[4 * tx + x][4 * ty + y] = acc[x][y];
+    for (int e = tid; e < kTB * kTB; e += blockDim.x) {
+      const int q = e / kTB, r = e - q * kTB;
+      Ls[r][q] = (r < h && q < h && r >= q) ? L[(r0 + r) + static_cast<int64_t>(r0 + q) * n] : 0.0;
+    }
+    __syncthreads();
+    for (int q = 0; q < h; ++q) {
+      if (tid < w) T[q][tid] /= Ls[q][q];
+      __syncthreads();
+      const int rows = h - q - 1;
+      for (int e = tid; e < rows * w; e += blockDim.x) {
+        const int r = q + 1 + e / w, c = e % w;
+        T[r][c] -= Ls[r][q] * T[q][c];
+      }
+      __syncthreads();
+    }
+    for (int e = tid; e < h * w; e += blockDim.x) {
+      const int c = e / h, r = e - c * h;
+      X[(r0 + r) + static_cast<int64_t>(c0 + c) * n] = T[r][c];
+    }
+    __syncthreads();
   }
 }
 
@@ -1228,6 +1290,19 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   return EMG_SUCCESS;
 }
 
+// X = L^-1 for n_mat lower factors stored in fac_d (blocked kernel).
+void FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
+                   double* X) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrtriSmem));
+    attr = true;
+  }
+  if (n_mat == 0 || max_n == 0) return;
+  k_trtri_blk<<<dim3(static_cast<unsigned>((max_n + kTB - 1) / kTB), static_cast<unsigned>(n_mat)), 256, kTrtriSmem,
+                st>>>(n_mat, dim, l_off, x_off, fac_d, X);
+}
+
 // Multifrontal forward / backward solve of K_rr x = b for ncol right-hand
 // sides: blocked front kernels level by level, the root (dual) fronts with
 // their explicit inverse factors.
@@ -1331,8 +1406,7 @@ int FetiDP::setup_deluxe() {
   int rc = factor_range(F + 1, F + 1 + NF);
   if (!rc) rc = check_err("FETI-DP face factorization");
   if (rc) return rc;
-  k_trtri<<<dim3(static_cast<unsigned>((max_fdim + 15) / 16), nf), 512, 0, st>>>(NF, fc.dim, fc.fac, fc.off, fac_d,
-                                                                                fX_d);
+  trtri(NF, max_fdim, fc.dim, fc.fac, fc.off, fX_d);
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);
   const int32_t nt = (max_fdim + kTile - 1) / kTile;
   const dim3 g(static_cast<unsigned>(nt * nt), nf);
@@ -1410,8 +1484,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   if (!rc) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
   if (n_roots > 0) {
-    k_trtri<<<dim3(static_cast<unsigned>((max_nD + 15) / 16), static_cast<unsigned>(n_roots)), 512, 0, st>>>(
-        n_roots, d_rdim, d_rfac, d_roff, fac_d, Linv_d);
+    trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);
     k_mirror_lower<<<dim3(blocks_for(static_cast<int64_t>(max_nD) * max_nD, 256, 256),
                           static_cast<unsigned>(n_roots)), 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d);
   }
@@ -1435,7 +1508,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     rc = factor_range(F, F + 1);
     if (!rc) rc = check_err("FETI-DP coarse factorization");
     if (rc) return rc;
-    k_trtri<<<dim3(static_cast<unsigned>((nc + 15) / 16), 1), 512, 0, st>>>(1, d_cdim, d_cfac, d_czero, fac_d, Lcc_d);
+    trtri(1, static_cast<int32_t>(nc), d_cdim, d_cfac, d_czero, Lcc_d);
     k_mirror_lower<<<dim3(blocks_for(nc * nc, 256, 256), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d);
   }
   const int64_t ne = P.dual_off[S];
