@@ -152,7 +152,7 @@ int csr_from_device(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* co
 }
 
 void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
-  int64_t v[17] = {0};
+  int64_t v[20] = {0};
   v[0] = p.n_parts;
   v[1] = p.n_dofs;
   v[2] = p.n_union;
@@ -172,7 +172,24 @@ void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
     v[15] = std::max<int64_t>(v[15], p.nD[s]);
   }
   v[16] = p.max_children;
-  for (int32_t i = 0; i < n && i < 17; ++i) info[i] = v[i];
+  // flops of the numeric phase: partial Cholesky of the fronts (panel part,
+  // rank-npiv update of the update block), inverse factors of S_DD and the
+  // three deluxe products per face
+  double panel = 0.0, syrk = 0.0, other = 0.0;
+  for (const emg::FetiFront& f : p.fronts) {
+    const double np = f.npiv, nu = f.f - f.npiv;
+    panel += np * np * np / 3.0 + nu * np * np;
+    syrk += nu * nu * np;
+  }
+  for (int32_t s = 0; s < p.n_parts; ++s) other += static_cast<double>(p.nD[s]) * p.nD[s] * p.nD[s] / 3.0;
+  for (int32_t f = 0; f < p.n_faces; ++f) {
+    const double m = static_cast<double>(p.face_ptr[f + 1] - p.face_ptr[f]);
+    other += 6.0 * m * m * m + m * m * m / 3.0 + m * m * m / 3.0;
+  }
+  v[17] = static_cast<int64_t>(panel);
+  v[18] = static_cast<int64_t>(syrk);
+  v[19] = static_cast<int64_t>(other);
+  for (int32_t i = 0; i < n && i < 20; ++i) info[i] = v[i];
 }
 
 }  // namespace

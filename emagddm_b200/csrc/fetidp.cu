@@ -37,6 +37,7 @@ constexpr int kNB = 32;       // panel width of the partial Cholesky
 constexpr int kTile = 64;     // output tile of the rank-k updates
 constexpr int kKC = 32;       // k-chunk of the rank-k updates
 constexpr int kTrsmRows = 128;
+constexpr double kMinInnerTol = 1e-12;  // floor of a pass's multiplier tolerance
 
 enum : int32_t { kErrPivot = 1, kErrAsm = 2 };
 
@@ -819,19 +820,22 @@ __global__ void __launch_bounds__(256) k_face_gemm_nt(FacesDev Fc, const double*
   tile_update<true>(C + o + rs + static_cast<int64_t>(cs) * n, n, mr, mc, A + o + rs, n, B + o + cs, n, n, As, Bs);
 }
 
-// w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1).
-__global__ void __launch_bounds__(128) k_face_w(FacesDev Fc, const int32_t* __restrict__ lam_entry,
-                                                const double* __restrict__ Da, const double* __restrict__ Db,
+// w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
+// as column dots over the stored transposes DT (one warp per i).
+__global__ void __launch_bounds__(256) k_face_w(FacesDev Fc, const int32_t* __restrict__ lam_entry,
+                                                const double* __restrict__ DaT, const double* __restrict__ DbT,
                                                 const double* __restrict__ r, double* __restrict__ w) {
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i >= n) return;
+  const int lane = threadIdx.x & 31;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
-  const double* D = (side ? Db : Da) + Fc.off[f] + i;
+  const double* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
   double acc = 0.0;
-  for (int32_t j = 0; j < n; ++j) acc = fma(D[static_cast<int64_t>(j) * n], __ldg(r + lam[j]), acc);
-  w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
+  for (int32_t j = lane; j < n; j += 32) acc = fma(Dt[j], r[lam[j]], acc);
+  acc = warp_sum(acc);
+  if (lane == 0) w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
 }
 
 // c[e_i] = sum_j D[j, i] y[e_j] (column dot, one warp per i).
@@ -896,10 +900,10 @@ __global__ void k_extract_dual(int64_t ne, const int32_t* __restrict__ dual_sub,
   }
 }
 
-__global__ void k_axpy1(int64_t n, const double* __restrict__ x, double* __restrict__ y) {
+__global__ void k_axpy_s(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    y[i] += x[i];
+    y[i] = fma(a, x[i], y[i]);
 }
 
 // ------------------------------------------------------------- PCG pieces
@@ -1379,8 +1383,8 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
   const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
   if (precond == 2 && P.n_faces > 0) {
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
-    k_face_w<<<dim3(static_cast<unsigned>((max_fdim + 127) / 128), nfs), 128, 0, st>>>(fc, d_lam_entry, fDa_d,
-                                                                                     fDb_d, r, w_d);
+    k_face_w<<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fX_d, fXt_d,
+                                                                                  r, w_d);
     k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
     k_face_c<<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
                                                                                   y_d, c_d);
@@ -1413,6 +1417,9 @@ int FetiDP::setup_deluxe() {
   k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
   k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
   k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
+  // transposes for the row pass, in the buffers of X and X^T (no longer needed)
+  k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
+  k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
 }
@@ -1663,37 +1670,48 @@ int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, 
   EMG_CK(cudaMemcpyAsync(rglob_d, bg_d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
   int status = EMG_SUCCESS;
   int32_t total = 0, refinements = 0;
-  double rel = bb > 0.0 ? 1.0 : 0.0, lam_rel = 0.0, prev = 2.0;
-  // Defect correction: each pass solves K dx = b - K x by FETI-DP to the
-  // inner multiplier tolerance kInnerTol, until the true relative residual
-  // meets cfg.tolerance, stops shrinking or the iteration budget ends.  The
-  // true residual is the multiplier residual amplified by the jump of the
-  // dual copies (10^2..10^4 here), so every pass runs to the full inner
-  // tolerance and then gains about that many orders.
-  constexpr double kInnerTol = 1e-10;
+  double rel = bb > 0.0 ? 1.0 : 0.0, lam_rel = 0.0;
+  // Defect correction: each pass solves K dx = b - K x by FETI-DP until the
+  // true relative residual meets cfg.tolerance, stops shrinking or the
+  // iteration budget ends.  The true residual shrinks less than the
+  // multiplier residual by the amplification `amp` (the jump between the dual
+  // copies, 10^2..10^4 here; the largest seen so far), so each pass's
+  // multiplier tolerance is the reduction still needed divided by amp, with a
+  // safety factor of 10 and a floor of kMinInnerTol.  A pass that does not
+  // halve the true residual is undone and retried 1000x tighter.
   constexpr int kMaxPasses = 6;
+  double amp = 1e4;  // true-residual reduction / multiplier-residual reduction, updated per pass
   while (bb > 0.0 && refinements < kMaxPasses) {
     k_distribute<<<blocks_for(N, 256), 256, 0, st>>>(N, d_gptr, d_glist, rglob_d, fu_d);
     int rc = prepare_rhs(fu_d);
     if (rc) return rc;
     int32_t it = 0;
-    status = lambda_pcg(kInnerTol, cfg.max_iterations - total, &it, &lam_rel);
+    const double want = 0.1 * cfg.tolerance / std::max(rel, 1e-300) / amp;
+    status = lambda_pcg(std::min(1e-2, std::max(kMinInnerTol, want)), cfg.max_iterations - total, &it, &lam_rel);
     total += it;
     ++refinements;
     rc = recover(fu_d);
     if (rc) return rc;
-    k_axpy1<<<blocks_for(N, 256), 256, 0, st>>>(N, xg_d, xacc_d);
+    k_axpy_s<<<blocks_for(N, 256), 256, 0, st>>>(N, 1.0, xg_d, xacc_d);
     double rr = 0.0;
     rc = global_residual(bg_d, xacc_d, &rr);
     if (rc) return rc;
-    EMG_CK(cudaMemcpyAsync(rglob_d, rg_d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-    rel = std::sqrt(rr / bb);
+    const double rel_new = std::sqrt(rr / bb);
     if (status == EMG_NUMERICAL_ERROR) break;
+    if (!(rel_new < 0.5 * rel)) {
+      // the pass did not pay: undo it and retry with a much tighter tolerance
+      k_axpy_s<<<blocks_for(N, 256), 256, 0, st>>>(N, -1.0, xg_d, xacc_d);
+      amp *= 1e3;
+      status = EMG_MAX_ITER_REACHED;
+      if (total >= cfg.max_iterations) break;
+      continue;
+    }
+    EMG_CK(cudaMemcpyAsync(rglob_d, rg_d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    if (lam_rel > 0.0 && rel > 0.0) amp = std::max(amp, (rel_new / rel) / lam_rel);
+    rel = rel_new;
     if (rel < cfg.tolerance) { status = EMG_SUCCESS; break; }
-    if (total >= cfg.max_iterations) { status = EMG_MAX_ITER_REACHED; break; }
-    if (rel > 0.5 * prev) { status = EMG_MAX_ITER_REACHED; break; }  // no longer converging
-    prev = rel;
     status = EMG_MAX_ITER_REACHED;
+    if (total >= cfg.max_iterations) break;
   }
   if (bb > 0.0 && status == EMG_SUCCESS && !(rel < cfg.tolerance)) status = EMG_MAX_ITER_REACHED;
   EMG_CK(cudaEventRecord(ev.b, st));

@@ -179,9 +179,11 @@ int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int
  * emg_fetidp_factor. */
 int emg_fetidp_solve_rhs(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x,
                          int32_t on_device, emg_result* out);
-/* info[0..16]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
+/* info[0..19]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
  * n_levels, max_front, max_pivots, factor doubles, update-pool doubles,
- * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children. */
+ * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children, and the
+ * flops of the numeric phase: front panels, front update blocks, inverse
+ * factors + deluxe weights. */
 int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
 /* stats[0..5]: factor ms, solve ms, iterations, multiplier residual, true
  * residual, FETI-DP passes. */
