@@ -212,13 +212,95 @@ __global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(FrontsDev F, int32_t f
     for (int c = 0; c < nb; ++c) A[i + static_cast<int64_t>(k0 + c) * fs] = X[c][threadIdx.x];
 }
 
-// C[0:mr, 0:mc] -= (or, kOverwrite, =) A[0:mr, 0:K] * B[0:mc, 0:K]^T for one 64x64 tile; A, B, C
-// column-major.  Thread (tx, ty) owns rows 4*tx .. +3 and columns 4*ty .. +3.
+// Asynchronous 8-byte global -> shared copy; `valid` false fills a zero
+// (no bytes are read; `src` must still be a mapped address).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+constexpr int kGK = 16;  // k-chunk of the tile GEMM
+
+struct TileSmem {
+  double a[2][kGK][kTile];
+  double b[2][kGK][kTile];
+};
+
+// C[0:mr, 0:mc] -= (or, kOverwrite, =) A[0:mr, 0:K] * B[0:mc, 0:K]^T for one
+// 64x64 tile with 64 threads; A, B, C column-major.  Thread (tx, ty) owns rows
+// tx + 8a and columns ty + 8b (8 x 8 registers: 16 shared loads per 64 FMAs,
+// conflict-free); k-chunks of 16 double-buffered with cp.async.
 template <bool kOverwrite = false>
 __device__ __forceinline__ void tile_update(double* __restrict__ C, int64_t ldc, int mr, int mc,
                                             const double* __restrict__ A, int64_t lda,
-                                            const double* __restrict__ B, int64_t ldb, int K,
-                                            double (*As)[kTile + 1], double (*Bs)[kTile + 1]) {
+                                            const double* __restrict__ B, int64_t ldb, int K, TileSmem& sm) {
+  const int t = threadIdx.x, tx = t & 7, ty = t >> 3;
+  double acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+  const int nk = (K + kGK - 1) / kGK;
+  auto load = [&](int chunk, int buf) {
+    const int k0 = chunk * kGK;
+#pragma unroll
+    for (int c = 0; c < kGK; ++c) {
+      const bool kin = k0 + c < K;
+      const bool va = kin && t < mr, vb = kin && t < mc;
+      cp_async8(&sm.a[buf][c][t], va ? A + t + static_cast<int64_t>(k0 + c) * lda : A, va);
+      cp_async8(&sm.b[buf][c][t], vb ? B + t + static_cast<int64_t>(k0 + c) * ldb : B, vb);
+    }
+    cp_async_commit();
+  };
+  if (nk > 0) load(0, 0);
+  for (int i = 0; i < nk; ++i) {
+    if (i + 1 < nk) {
+      load(i + 1, (i + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int buf = i & 1;
+#pragma unroll 2
+    for (int c = 0; c < kGK; ++c) {
+      double av[8], bv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) { av[q] = sm.a[buf][c][tx + 8 * q]; bv[q] = sm.b[buf][c][ty + 8 * q]; }
+#pragma unroll
+      for (int x = 0; x < 8; ++x)
+#pragma unroll
+        for (int y = 0; y < 8; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int y = 0; y < 8; ++y) {
+    const int cc = ty + 8 * y;
+    if (cc >= mc) continue;
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const int rr = tx + 8 * x;
+      if (rr < mr) {
+        if (kOverwrite) C[rr + static_cast<int64_t>(cc) * ldc] = acc[x][y];
+        else C[rr + static_cast<int64_t>(cc) * ldc] -= acc[x][y];
+      }
+    }
+  }
+}
+
+// C[0:mr, 0:mc] -= A[0:mr, 0:K] * B[0:mc, 0:K]^T for one 64x64 tile with 256
+// threads (4 x 4 registers each, rows 4*tx.., columns 4*ty..), for small K
+// where the update is bound by the C read-modify-write and wants many
+// threads in flight.
+__device__ __forceinline__ void tile_update_wide(double* __restrict__ C, int64_t ldc, int mr, int mc,
+                                                 const double* __restrict__ A, int64_t lda,
+                                                 const double* __restrict__ B, int64_t ldb, int K,
+                                                 double (*As)[kTile + 1], double (*Bs)[kTile + 1]) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double acc[4][4];
 #pragma unroll
@@ -253,10 +335,7 @@ __device__ __forceinline__ void tile_update(double* __restrict__ C, int64_t ldc,
 #pragma unroll
     for (int x = 0; x < 4; ++x) {
       const int rr = 4 * tx + x;
-      if (rr < mr) {
-        if (kOverwrite) C[rr + static_cast<int64_t>(cc) * ldc] = acc[x][y];
-        else C[rr + static_cast<int64_t>(cc) * ldc] -= acc[x][y];
-      }
+      if (rr < mr) C[rr + static_cast<int64_t>(cc) * ldc] -= acc[x][y];
     }
   }
 }
@@ -280,15 +359,14 @@ __global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0,
   if (rs + kTile <= cs) return;  // strictly above the diagonal
   const int mc = min(kTile, np - cs), mr = min(kTile, fs - rs);
   double* A = fac + F.fac[k];
-  tile_update(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
-              A + cs + static_cast<int64_t>(k0) * fs, fs, nb, As, Bs);
+  tile_update_wide(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
+                   A + cs + static_cast<int64_t>(k0) * fs, fs, nb, As, Bs);
 }
 
 // Update block: U -= L21 L21^T (lower tiles), K = npiv.
-__global__ void __launch_bounds__(256) k_syrk_update(FrontsDev F, int32_t f0, const double* __restrict__ fac,
-                                                     double* __restrict__ upd) {
-  __shared__ double As[kKC][kTile + 1];
-  __shared__ double Bs[kKC][kTile + 1];
+__global__ void __launch_bounds__(64) k_syrk_update(FrontsDev F, int32_t f0, const double* __restrict__ fac,
+                                                    double* __restrict__ upd) {
+  __shared__ TileSmem sm;
   const int32_t k = f0 + blockIdx.y;
   const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np;
   if (nu <= 0) return;
@@ -304,7 +382,7 @@ __global__ void __launch_bounds__(256) k_syrk_update(FrontsDev F, int32_t f0, co
   const int mr = min(kTile, nu - rs), mc = min(kTile, nu - cs);
   const double* L = fac + F.fac[k];
   double* U = upd + F.upd[k];
-  tile_update(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, As, Bs);
+  tile_update(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, sm);
 }
 
 // --------------------------------------------------- triangular inverse
@@ -433,15 +511,20 @@ __global__ void __launch_bounds__(256) k_front_fwd_blk(FrontsDev F, int32_t f0, 
   }
   const double* L = fac + F.fac[k];
   __shared__ double yb[kSB];
+  __shared__ double Db[kSB][kSB + 1];
   for (int32_t jb = 0; jb < np; jb += kSB) {
     const int32_t nb = min(kSB, np - jb);
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+      const int c = e / nb, r = e - c * nb;
+      Db[r][c] = L[(jb + r) + static_cast<int64_t>(jb + c) * fs];
+    }
+    __syncthreads();
     if (wid == 0) {
       double v = lane < nb ? x[p0 + jb + lane] : 0.0;
       for (int32_t j = 0; j < nb; ++j) {
-        const double* Lj = L + static_cast<int64_t>(jb + j) * fs + jb;
-        const double yj = __shfl_sync(0xffffffffu, v, j) / Lj[j];
+        const double yj = __shfl_sync(0xffffffffu, v, j) / Db[j][j];
         if (lane == j) v = yj;
-        if (lane > j && lane < nb) v -= Lj[lane] * yj;
+        if (lane > j && lane < nb) v -= Db[lane][j] * yj;
       }
       if (lane < nb) { x[p0 + jb + lane] = v; yb[lane] = v; }
     }
@@ -474,8 +557,13 @@ __global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, 
   const int32_t* rows = F.rows_v + F.rows[k];
   const double* L = fac + F.fac[k];
   __shared__ double tb[kSB];
+  __shared__ double Db[kSB][kSB + 1];
   for (int32_t jb = ((np - 1) / kSB) * kSB; jb >= 0; jb -= kSB) {
     const int32_t nb = min(kSB, np - jb);
+    for (int e = tid; e < nb * nb; e += blockDim.x) {
+      const int c = e / nb, r = e - c * nb;
+      Db[r][c] = L[(jb + r) + static_cast<int64_t>(jb + c) * fs];
+    }
     for (int32_t j = wid; j < nb; j += nw) {
       const double* Lj = L + static_cast<int64_t>(jb + j) * fs;
       double acc = 0.0;
@@ -487,11 +575,10 @@ __global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, 
     if (wid == 0) {
       double v = lane < nb ? x[p0 + jb + lane] - tb[lane] : 0.0;
       for (int32_t j = nb - 1; j >= 0; --j) {
-        const double* Lj = L + static_cast<int64_t>(jb + j) * fs + jb;
         // x_j = (v_j - sum_{i > j in block} L[i, j] x_i) / L[j, j]
-        double part = (lane > j && lane < nb) ? Lj[lane] * v : 0.0;
+        double part = (lane > j && lane < nb) ? Db[lane][j] * v : 0.0;
         part = warp_sum(part);
-        const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / Lj[j];
+        const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / Db[j][j];
         if (lane == j) v = xj;
       }
       if (lane < nb) x[p0 + jb + lane] = v;
@@ -804,10 +891,9 @@ __global__ void k_face_transpose(FacesDev Fc, const double* __restrict__ X, doub
 }
 
 // C_f = A_f B_f^T for every face (n x n, column-major, same offsets).
-__global__ void __launch_bounds__(256) k_face_gemm_nt(FacesDev Fc, const double* __restrict__ A,
-                                                      const double* __restrict__ B, double* __restrict__ C) {
-  __shared__ double As[kKC][kTile + 1];
-  __shared__ double Bs[kKC][kTile + 1];
+__global__ void __launch_bounds__(64) k_face_gemm_nt(FacesDev Fc, const double* __restrict__ A,
+                                                     const double* __restrict__ B, double* __restrict__ C) {
+  __shared__ TileSmem sm;
   const int32_t f = blockIdx.y;
   const int32_t n = Fc.dim[f];
   const int32_t nt = (n + kTile - 1) / kTile;
@@ -817,7 +903,7 @@ __global__ void __launch_bounds__(256) k_face_gemm_nt(FacesDev Fc, const double*
   const int32_t rs = tr * kTile, cs = tc * kTile;
   const int mr = min(kTile, n - rs), mc = min(kTile, n - cs);
   const int64_t o = Fc.off[f];
-  tile_update<true>(C + o + rs + static_cast<int64_t>(cs) * n, n, mr, mc, A + o + rs, n, B + o + cs, n, n, As, Bs);
+  tile_update<true>(C + o + rs + static_cast<int64_t>(cs) * n, n, mr, mc, A + o + rs, n, B + o + cs, n, n, sm);
 }
 
 // w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
@@ -1288,7 +1374,7 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   }
   if (max_nu > 0) {
     const int32_t nt = (max_nu + kTile - 1) / kTile;
-    k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
+    k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), 64, 0, st>>>(fd, f0, fac_d, upd_d);
   }
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -1414,9 +1500,9 @@ int FetiDP::setup_deluxe() {
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);
   const int32_t nt = (max_fdim + kTile - 1) / kTile;
   const dim3 g(static_cast<unsigned>(nt * nt), nf);
-  k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
-  k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
-  k_face_gemm_nt<<<g, 256, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
+  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
+  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
+  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
   // transposes for the row pass, in the buffers of X and X^T (no longer needed)
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
