@@ -92,6 +92,11 @@ SIGNATURES = {
     "emg_fetidp_info": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_stats": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_destroy": ([H], None),
+    "emg_direct_create": ([H, H, VP, C.POINTER(H)], C.c_int),
+    "emg_direct_factor": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32], C.c_int),
+    "emg_direct_solve": ([H, C.POINTER(KrylovConfig), VP, VP, C.c_int32, C.POINTER(Result)], C.c_int),
+    "emg_direct_info": ([H, VP, C.c_int32], C.c_int),
+    "emg_direct_destroy": ([H], None),
 }
 
 _LIB = None

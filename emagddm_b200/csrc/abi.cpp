@@ -28,6 +28,9 @@ struct emg_csr_t {
 struct emg_fetidp_t {
   emg::FetiDP fd;
 };
+struct emg_direct_t {
+  emg::FetiDP fd;  // one subdomain: nested dissection + multifrontal Cholesky
+};
 struct emg_system_t {
   emg::System s;
   emg_csr_t k_handle, m_handle;
@@ -190,6 +193,16 @@ void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
   v[18] = static_cast<int64_t>(syrk);
   v[19] = static_cast<int64_t>(other);
   for (int32_t i = 0; i < n && i < 20; ++i) info[i] = v[i];
+}
+
+// A DOF map viewed as one subdomain (the direct solver's plan).
+emg::DofMap single_part(const emg::DofMap& d) {
+  emg::DofMap s = d;
+  s.n_parts = 1;
+  s.tet_part.assign(d.n_tets, 0);
+  s.dof_primal.assign(d.n_dofs, 0);
+  s.n_primal_fix = 0;
+  return s;
 }
 
 }  // namespace
@@ -596,7 +609,8 @@ int emg_fetidp_plan_info(emg_mesh mesh, emg_dofmap map, int64_t* info, int32_t n
   return guarded([&]() -> int {
     if (!mesh || !map || (!info && n_info > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
     emg::FetiPlan p;
-    int rc = emg::build_feti_plan(mesh->m, map->d, p);
+    int rc = map->d.n_parts < 1 ? emg::build_feti_plan(mesh->m, single_part(map->d), p)
+                                : emg::build_feti_plan(mesh->m, map->d, p);
     if (rc) return rc;
     feti_info(p, info, n_info);
     return EMG_SUCCESS;
@@ -625,14 +639,14 @@ int emg_fetidp_factor(emg_fetidp fd, const double* nu, const double* sigma, int3
 }
 
 namespace {
-int fetidp_solve_impl(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x, int32_t on_device,
+int fetidp_solve_impl(emg::FetiDP* fp, const emg_krylov_config* cfg, const double* b, double* x, int32_t on_device,
                       emg_result* out) {
-  if (!fd || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  if (!fp || !cfg) { set_error("null argument"); return EMG_INVALID_INPUT; }
   if (cfg->max_iterations < 0 || !(cfg->tolerance > 0.0)) {
     set_error("bad tolerance or iteration limit");
     return EMG_INVALID_INPUT;
   }
-  emg::FetiDP& F = fd->fd;
+  emg::FetiDP& F = *fp;
   const int64_t n = F.plan.n_dofs;
   const double* bd = nullptr;
   if (b) {
@@ -658,14 +672,14 @@ int fetidp_solve_impl(emg_fetidp fd, const emg_krylov_config* cfg, const double*
 
 int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int32_t x_on_device,
                      emg_result* out) {
-  return guarded([&]() -> int { return fetidp_solve_impl(fd, cfg, nullptr, x, x_on_device, out); });
+  return guarded([&]() -> int { return fetidp_solve_impl(fd ? &fd->fd : nullptr, cfg, nullptr, x, x_on_device, out); });
 }
 
 int emg_fetidp_solve_rhs(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x,
                          int32_t on_device, emg_result* out) {
   return guarded([&]() -> int {
     if (!b) { set_error("null right-hand side"); return EMG_INVALID_INPUT; }
-    return fetidp_solve_impl(fd, cfg, b, x, on_device, out);
+    return fetidp_solve_impl(fd ? &fd->fd : nullptr, cfg, b, x, on_device, out);
   });
 }
 
@@ -685,5 +699,46 @@ int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats) {
 }
 
 void emg_fetidp_destroy(emg_fetidp fd) { delete fd; }
+
+int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* out) {
+  return guarded([&]() -> int {
+    if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    if (map->d.n_tets != mesh->m.n_tets || map->d.l2g.size() != static_cast<size_t>(6 * mesh->m.n_tets)) {
+      set_error("DOF map does not belong to this mesh");
+      return EMG_INVALID_INPUT;
+    }
+    emg::keep_pool_memory();
+    auto* h = new emg_direct_t();
+    int rc = h->fd.create(mesh->m, single_part(map->d), as_stream(stream));
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_direct_factor(emg_direct d, const double* nu, const double* sigma, int32_t n_materials,
+                      const emg_source* sources, int32_t n_sources, int32_t flags) {
+  return guarded([&]() -> int {
+    if (!d) { set_error("null direct-solver handle"); return EMG_INVALID_INPUT; }
+    return d->fd.factor(nu, sigma, n_materials, sources, n_sources, flags);
+  });
+}
+
+int emg_direct_solve(emg_direct d, const emg_krylov_config* cfg, const double* b, double* x, int32_t on_device,
+                     emg_result* out) {
+  return guarded([&]() -> int {
+    if (!d) { set_error("null direct-solver handle"); return EMG_INVALID_INPUT; }
+    return fetidp_solve_impl(&d->fd, cfg, b, x, on_device, out);
+  });
+}
+
+int emg_direct_info(emg_direct d, int64_t* info, int32_t n_info) {
+  if (!d || (!info && n_info > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
+  feti_info(d->fd.plan, info, n_info);
+  return EMG_SUCCESS;
+}
+
+void emg_direct_destroy(emg_direct d) { delete d; }
 
 }  // extern "C"

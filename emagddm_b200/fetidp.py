@@ -145,3 +145,59 @@ class FetiDP:
         if getattr(self, "h", None) and _abi._LIB is not None:
             _abi._LIB.emg_fetidp_destroy(self.h)
             self.h = None
+
+
+def gauged_map(m, gauge: int):
+    """DOF map of the mesh under a tree gauge (emg_dof_build); returns the
+    map handle owner, the mesh handle owner and the (T, 6) l2g."""
+    mh = _MeshHandle(m)
+    h = C.c_void_p()
+    check(lib().emg_dof_build(mh.h, int(gauge), C.byref(h)), "emg_dof_build")
+    ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+    lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
+    l2g = np.empty((m.n_tets, 6), np.int32)
+    lib().emg_dofmap_export(h, ptr(l2g), None)
+    return _MapHandle(h), mh, l2g, nd.value
+
+
+class DirectSolver:
+    """GPU sparse direct solver (nested dissection + multifrontal Cholesky,
+    iterative refinement) for the gauged system of mesh ``m`` -- the
+    SolverBackend role of the reference's MUMPS / Eigen LLT backends.  The DOF
+    map comes from ``emg_dof_build(gauge)`` (the reference-exact ``ref`` gauge
+    by default) or from a partitioned map when ``tet_part`` is given."""
+
+    def __init__(self, m, gauge: int = _abi.GAUGE_REF, tet_part=None, n_parts: int = 0, stream=None):
+        self.m = m
+        if tet_part is not None:
+            pm, self._mesh, self._maph = partitioned_dofmap(m, tet_part, n_parts, keep_handles=True)
+            self.l2g, self.n_dofs = pm.l2g, pm.n_dofs
+        else:
+            self._maph, self._mesh, self.l2g, self.n_dofs = gauged_map(m, gauge)
+        self.h = C.c_void_p()
+        check(lib().emg_direct_create(self._mesh.h, self._maph.h, stream, C.byref(self.h)), "emg_direct_create")
+
+    def info(self) -> dict:
+        v = np.zeros(len(INFO_KEYS), np.int64)
+        check(lib().emg_direct_info(self.h, ptr(v), len(v)), "emg_direct_info")
+        return dict(zip(INFO_KEYS, (int(a) for a in v)))
+
+    def factor(self, flags: int = 0, nu=None, sigma=None) -> int:
+        nu = np.ascontiguousarray(self.m.nu if nu is None else nu, np.float64)
+        sg = np.ascontiguousarray(self.m.sigma if sigma is None else sigma, np.float64)
+        arr, ns = _abi.sources_array(self.m.sources)
+        return lib().emg_direct_factor(self.h, ptr(nu), ptr(sg), len(nu),
+                                       C.cast(arr, C.c_void_p) if arr is not None else None, ns, flags)
+
+    def solve(self, b=None, tol: float = 1e-12, passes: int = 6):
+        x = np.empty(self.n_dofs)
+        bb = None if b is None else np.ascontiguousarray(b, np.float64)
+        cfg = _abi.KrylovConfig(tol, passes, 0)
+        out = _abi.Result()
+        rc = lib().emg_direct_solve(self.h, C.byref(cfg), ptr(bb), ptr(x), 0, C.byref(out))
+        return x, rc, out
+
+    def __del__(self, _abi=_abi):
+        if getattr(self, "h", None) and _abi._LIB is not None:
+            _abi._LIB.emg_direct_destroy(self.h)
+            self.h = None

@@ -189,8 +189,32 @@ int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
  * residual, FETI-DP passes. */
 int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats);
 void emg_fetidp_destroy(emg_fetidp fd);
-/* Host-only symbolic analysis (no GPU needed): the info[] of the plan. */
+/* Host-only symbolic analysis (no GPU needed): the info[] of the plan; a map
+ * without a partition is analysed as one subdomain (the direct solver's plan). */
 int emg_fetidp_plan_info(emg_mesh mesh, emg_dofmap map, int64_t* info, int32_t n_info);
+
+/* ---- GPU sparse direct solver for the gauged system: the SolverBackend
+ * role of MUMPSBackend / EigenLLTBackend (include/numeric/solver_backend.h:81-244,
+ * include/numeric/mumps_solver_backend.h:96-140, eigen_solver_backends.h:338-420).
+ * Nested dissection of the edge DOFs (edge midpoints), multifrontal Cholesky
+ * on the GPU (fronts of one height factored together, FP64), then forward /
+ * backward solves with iterative refinement on the true residual until
+ * ||F - K x|| / ||F|| < cfg->tolerance (cfg->max_iterations bounds the
+ * refinement passes; cfg->preconditioner is ignored).  map: any map of the
+ * mesh (emg_dof_build with any gauge, or emg_dof_build_partitioned); the
+ * system must be symmetric positive definite (a gauged curl-curl system is).
+ * EMG_NUMERICAL_ERROR from emg_direct_factor when it is not. */
+typedef struct emg_direct_t* emg_direct;
+int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* out);
+int emg_direct_factor(emg_direct d, const double* nu, const double* sigma, int32_t n_materials,
+                      const emg_source* sources, int32_t n_sources, int32_t flags);
+/* b: right-hand side (n_dofs) or NULL for the assembled F; b and x both host
+ * or both device arrays. */
+int emg_direct_solve(emg_direct d, const emg_krylov_config* cfg, const double* b, double* x,
+                     int32_t on_device, emg_result* out);
+/* info as emg_fetidp_info (one subdomain, no multipliers). */
+int emg_direct_info(emg_direct d, int64_t* info, int32_t n_info);
+void emg_direct_destroy(emg_direct d);
 
 /* ---- EMAssembly::assemble on the GPU (src/numeric/em_assembly.cpp:144-420)
  * A system owns the device copy of the geometry and DOF map, the CSR pattern

@@ -100,6 +100,15 @@ class EMDOFManager {
   EMDOFManager(const EMDOFManager&) = delete;
   EMDOFManager& operator=(const EMDOFManager&) = delete;
   void build() { run(EMG_GAUGE_NONE); gauged_ = false; }
+  // Tree gauge for a partition of the tets (FETI-DP); replaces any gauge.
+  void applyPartitionedGauge(const std::vector<int32_t>& tet_part, int32_t n_parts) {
+    emg_dofmap m = nullptr;
+    if (emg_dof_build_partitioned(mesh_.handle(), tet_part.data(), n_parts, &m) != EMG_SUCCESS)
+      throw std::invalid_argument("EMDOFManager: " + last_error());
+    adopt(m);
+    gauged_ = true;
+  }
+  emg_dofmap handle() const { return map_; }
   void applyTreeGauge(int32_t mode = EMG_GAUGE_REF) {
     if (!map_) throw std::runtime_error("build() must be called before applyTreeGauge()");
     if (gauged_) return;  // repeated calls are ignored, as in the reference
@@ -121,6 +130,9 @@ class EMDOFManager {
     emg_dofmap m = nullptr;
     if (emg_dof_build(mesh_.handle(), mode, &m) != EMG_SUCCESS)
       throw std::invalid_argument("EMDOFManager: " + last_error());
+    adopt(m);
+  }
+  void adopt(emg_dofmap m) {
     if (map_) emg_dofmap_destroy(map_);
     map_ = m;
     int64_t ne = 0, nf = 0;
@@ -243,5 +255,73 @@ class GpuKrylovSolver {
 
 using GpuCGSolver = GpuKrylovSolver<false>;
 using GpuBiCGSTABSolver = GpuKrylovSolver<true>;
+
+// Mesh-level GPU solvers that own their factorization: kind false = the
+// direct backend (SolverBackend / MUMPSBackend role, mumps_solver_backend.h:96-140),
+// kind true = FETI-DP (fetidp_context.hpp:20-66 has no operators).
+template <bool kFeti>
+class GpuMeshSolver {
+ public:
+  GpuMeshSolver(const Mesh& mesh, const EMDOFManager& dofs) {
+    const int rc = kFeti ? emg_fetidp_create(mesh.handle(), dofs.handle(), nullptr,
+                                             reinterpret_cast<emg_fetidp*>(&h_))
+                         : emg_direct_create(mesh.handle(), dofs.handle(), nullptr,
+                                             reinterpret_cast<emg_direct*>(&h_));
+    if (rc != EMG_SUCCESS) throw std::runtime_error(std::string(name()) + ": " + last_error());
+  }
+  ~GpuMeshSolver() {
+    if (kFeti) emg_fetidp_destroy(static_cast<emg_fetidp>(h_));
+    else emg_direct_destroy(static_cast<emg_direct>(h_));
+  }
+  GpuMeshSolver(const GpuMeshSolver&) = delete;
+  GpuMeshSolver& operator=(const GpuMeshSolver&) = delete;
+  // Numeric factorization for the materials (nu = 1/mu per material id) and sources.
+  bool factor(const std::vector<double>& nu, const std::vector<double>& sigma = {},
+              const std::vector<emg_source>& sources = {}) {
+    const int32_t nm = static_cast<int32_t>(nu.size()), ns = static_cast<int32_t>(sources.size());
+    const double* sg = sigma.empty() ? nullptr : sigma.data();
+    const emg_source* src = sources.empty() ? nullptr : sources.data();
+    const int rc = kFeti ? emg_fetidp_factor(static_cast<emg_fetidp>(h_), nu.data(), sg, nm, src, ns, 0)
+                         : emg_direct_factor(static_cast<emg_direct>(h_), nu.data(), sg, nm, src, ns, 0);
+    error_ = rc == EMG_SUCCESS ? "" : last_error();
+    return rc == EMG_SUCCESS;
+  }
+  // K x = b (b empty: the assembled F) to a true relative residual `tolerance`.
+  SolverResult solve(const std::vector<double>& b = {}, double tolerance = 1e-8, int32_t max_iterations = 1000) {
+    SolverResult r;
+    r.x.resize(n_dofs());
+    emg_krylov_config cfg{tolerance, max_iterations, kFeti ? EMG_FETI_PRECOND_DELUXE : 0};
+    emg_result out{};
+    const double* bp = b.empty() ? nullptr : b.data();
+    int rc;
+    if (kFeti)
+      rc = bp ? emg_fetidp_solve_rhs(static_cast<emg_fetidp>(h_), &cfg, bp, r.x.data(), 0, &out)
+              : emg_fetidp_solve(static_cast<emg_fetidp>(h_), &cfg, r.x.data(), 0, &out);
+    else
+      rc = emg_direct_solve(static_cast<emg_direct>(h_), &cfg, bp, r.x.data(), 0, &out);
+    r.status = static_cast<SolverStatus>(out.status <= EMG_INVALID_INPUT ? out.status : EMG_NUMERICAL_ERROR);
+    if (rc > EMG_INVALID_INPUT) r.status = SolverStatus::NUMERICAL_ERROR;
+    r.iterations = out.iterations;
+    r.residual_norm = out.residual_norm;
+    r.solve_time_ms = out.solve_time_ms;
+    if (rc != EMG_SUCCESS) r.error_msg = last_error();
+    return r;
+  }
+  int64_t n_dofs() const {
+    int64_t info[2] = {0, 0};
+    if (kFeti) emg_fetidp_info(static_cast<emg_fetidp>(h_), info, 2);
+    else emg_direct_info(static_cast<emg_direct>(h_), info, 2);
+    return info[1];
+  }
+  static const char* name() { return kFeti ? "GpuFetiDpSolver" : "GpuDirectBackend"; }
+  const std::string& error_message() const { return error_; }
+
+ private:
+  void* h_ = nullptr;
+  std::string error_;
+};
+
+using GpuDirectBackend = GpuMeshSolver<false>;
+using GpuFetiDpSolver = GpuMeshSolver<true>;
 
 }  // namespace emg

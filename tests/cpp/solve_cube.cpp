@@ -2,8 +2,9 @@
 // written against the C++ adapters (include/emagddm_b200.hpp) the way a
 // reference caller would write it:
 //   GlobalEdgeIDGenerator -> EMDOFManager::build/applyTreeGauge
-//   -> GpuEMAssembly::assemble -> GpuCGSolver::set_matrix/solve.
-// Usage: solve_cube <n> [--numbering-only] [--x out.bin]
+//   -> GpuEMAssembly::assemble -> GpuCGSolver::set_matrix/solve,
+// or (--direct) the GPU direct backend on the same gauged system.
+// Usage: solve_cube <n> [--numbering-only] [--direct] [--x out.bin]
 // Prints one line of key=value pairs.
 #include <cmath>
 #include <cstdio>
@@ -15,10 +16,11 @@
 
 int main(int argc, char** argv) {
   const int n = argc > 1 ? std::atoi(argv[1]) : 4;
-  bool numbering_only = false;
+  bool numbering_only = false, direct = false;
   const char* xout = nullptr;
   for (int i = 2; i < argc; ++i) {
     if (!std::strcmp(argv[i], "--numbering-only")) numbering_only = true;
+    if (!std::strcmp(argv[i], "--direct")) direct = true;
     if (!std::strcmp(argv[i], "--x") && i + 1 < argc) xout = argv[++i];
   }
   const int n1 = n + 1;
@@ -77,6 +79,26 @@ int main(int argc, char** argv) {
   box.j[2] = 1.0;
   const double p[6] = {0.375, 0.625, 0.375, 0.625, 0.375, 0.625};
   std::memcpy(box.p, p, sizeof(p));
+  if (direct) {
+    emg::GpuDirectBackend ds(mesh, dofs);
+    if (!ds.factor({1.0}, {0.0}, {box})) {
+      std::printf(" factor_error=\"%s\"\n", ds.error_message().c_str());
+      return 2;
+    }
+    const emg::SolverResult r = ds.solve({}, 1e-12, 6);
+    double norm = 0.0;
+    for (double v : r.x) norm += v * v;
+    std::printf(" solver=%s status=%d residual=%.3e xnorm=%.12e\n", emg::GpuDirectBackend::name(),
+                static_cast<int>(r.status), r.residual_norm, std::sqrt(norm));
+    if (xout) {
+      FILE* f = std::fopen(xout, "wb");
+      if (f) {
+        std::fwrite(r.x.data(), sizeof(double), r.x.size(), f);
+        std::fclose(f);
+      }
+    }
+    return r.status == emg::SolverStatus::SUCCESS ? 0 : 1;
+  }
   emg::GpuEMAssembly as;
   if (!as.assemble(mesh, dofs.getElemLocalToGlobal(), {1.0}, {0.0}, {box})) {
     std::printf(" assemble_error=\"%s\"\n", as.error_message().c_str());

@@ -47,3 +47,19 @@ def test_cpp_chain_solution_matches_oracle(tmp_path):
     x = np.fromfile(xfile, dtype=np.float64)
     assert abs(int(kv["iterations"]) - it) <= max(3, 0.15 * it)
     assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+@pytest.mark.gpu
+def test_cpp_direct_backend_matches_oracle(tmp_path):
+    n = 6
+    xfile = tmp_path / "xd.bin"
+    rc, kv = run(n, "--direct", "--x", xfile)
+    assert rc == 0, kv
+    assert kv["status"] == "0" and kv["solver"] == "GpuDirectBackend"
+    assert float(kv["residual"]) <= 1e-12
+    m = mesh.plain_small(n)
+    o = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+    rp, col, kv_, _, rhs = O.assemble(m, o["l2g"], o["n_dofs"])
+    xo, st, it, res = O.pcg(rp, col, kv_, rhs, tol=1e-12, max_iter=10000, precond=1)
+    x = np.fromfile(xfile, dtype=np.float64)
+    assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)

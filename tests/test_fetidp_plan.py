@@ -87,3 +87,17 @@ def test_bad_partition_rejected():
     part[5] = 7
     with pytest.raises(RuntimeError, match="tet_part"):
         fetidp.partitioned_dofmap(m, part, 2)
+
+
+@pytest.mark.parametrize("gauge", [O.GAUGE_REF, O.GAUGE_BOUNDARY_FIRST])
+def test_direct_solver_plan_on_gauged_maps(gauge):
+    # the direct solver analyses any map as one subdomain
+    m = mesh.plain_scale(10)
+    maph, mh, l2g, n = fetidp.gauged_map(m, gauge)
+    info = np.zeros(len(fetidp.INFO_KEYS), np.int64)
+    from emagddm_b200 import _abi
+    _abi.check(_abi.lib().emg_fetidp_plan_info(mh.h, maph.h, _abi.ptr(info), len(info)), "plan_info")
+    d = dict(zip(fetidp.INFO_KEYS, info))
+    assert d["n_parts"] == 1 and d["n_lambda"] == 0 and d["n_coarse"] == 0
+    assert d["n_dofs"] == n == d["n_union"] == d["sum_nI"]
+    assert n == O.dof_build(m.tets, m.dirichlet, gauge=gauge)["n_dofs"]

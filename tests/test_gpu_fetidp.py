@@ -112,3 +112,23 @@ def test_gauge_only_removes_gradients():
     xfull[free_of_edge[kept]] = x[fd.map.edge_dof[kept]]
     r = Ffree - O.spmv(frp, fcol, fkv, xfull)
     assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(Ffree)
+
+
+@pytest.mark.parametrize("kind,n", [("scale", 6), ("scale", 10), ("rand", 9), ("small", 12)])
+def test_direct_solver_on_reference_gauge(kind, n):
+    """Multifrontal GPU Cholesky of the reference-exact (ref-gauge) system
+    against the oracle's monolithic solve."""
+    m = {"scale": mesh.plain_scale, "small": mesh.plain_small}.get(kind, lambda k: mesh.random_instance(k, 11))(n)
+    ds = fetidp.DirectSolver(m)
+    assert ds.factor() == 0, _abi.lib().emg_last_error()
+    x, rc, out = ds.solve(tol=1e-12)
+    assert rc == 0, _abi.lib().emg_last_error()
+    xo, rhs = monolithic(m, ds.l2g)
+    assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+    assert out.residual_norm <= 1e-12
+    # a second right-hand side on the same factorization
+    b2 = np.random.default_rng(1).normal(size=ds.n_dofs)
+    x2, rc, out2 = ds.solve(b2, tol=1e-12)
+    assert rc == 0 and out2.residual_norm <= 1e-12
+    rp, col, kv, _, _ = oracle_system(m, ds.l2g)
+    assert np.linalg.norm(b2 - O.spmv(rp, col, kv, x2)) <= 1e-11 * np.linalg.norm(b2)
