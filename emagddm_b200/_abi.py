@@ -47,6 +47,11 @@ SIGNATURES = {
     "emg_mesh_create": ([C.c_int64, VP, C.c_int64, VP, VP, C.c_int64, VP, C.c_int32,
                          C.POINTER(H)], C.c_int),
     "emg_mesh_destroy": ([H], None),
+    "emg_mesh_read_gmsh": ([C.c_char_p, VP, C.c_int32, C.POINTER(H)], C.c_int),
+    "emg_mesh_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                       C.POINTER(C.c_int32)], C.c_int),
+    "emg_mesh_export": ([H, VP, VP, VP, VP], C.c_int),
+    "emg_mesh_material_tags": ([H, VP], C.c_int),
     "emg_edge_ids": ([H, VP, VP, C.POINTER(C.c_int64)], C.c_int),
     "emg_dof_build": ([H, C.c_int32, C.POINTER(H)], C.c_int),
     "emg_dofmap_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),

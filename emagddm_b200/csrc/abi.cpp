@@ -17,6 +17,7 @@
 
 struct emg_mesh_t {
   emg::Mesh m;
+  std::vector<int32_t> material_tags;  // physical tag of each material id (Gmsh input)
 };
 struct emg_dofmap_t {
   emg::DofMap d;
@@ -245,6 +246,53 @@ int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const in
 }
 
 void emg_mesh_destroy(emg_mesh mesh) { delete mesh; }
+
+int emg_mesh_read_gmsh(const char* path, const int32_t* dirichlet_tags, int32_t n_tags, emg_mesh* out) {
+  return guarded([&]() -> int {
+    if (!path || !out || n_tags < 0 || (n_tags > 0 && !dirichlet_tags)) {
+      set_error("bad argument");
+      return EMG_INVALID_INPUT;
+    }
+    *out = nullptr;
+    auto* h = new emg_mesh_t();
+    int rc = emg::read_gmsh(path, dirichlet_tags, n_tags, h->m, h->material_tags);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_mesh_info(emg_mesh mesh, int64_t* n_nodes, int64_t* n_tets, int64_t* n_dirichlet, int32_t* n_materials) {
+  if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
+  const emg::Mesh& m = mesh->m;
+  if (n_nodes) *n_nodes = m.n_nodes;
+  if (n_tets) *n_tets = m.n_tets;
+  if (n_dirichlet) *n_dirichlet = static_cast<int64_t>(m.dirichlet.size() / 2);
+  if (n_materials) {
+    int32_t mx = -1;
+    for (int32_t v : m.material) mx = std::max(mx, v);
+    *n_materials = mx + 1;
+  }
+  return EMG_SUCCESS;
+}
+
+int emg_mesh_export(emg_mesh mesh, double* xyz, int32_t* tets, int32_t* material, int32_t* dirichlet_pairs) {
+  if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
+  const emg::Mesh& m = mesh->m;
+  if (xyz && !m.xyz.empty()) std::memcpy(xyz, m.xyz.data(), sizeof(double) * m.xyz.size());
+  if (tets) std::memcpy(tets, m.tets.data(), sizeof(int32_t) * m.tets.size());
+  if (material) std::memcpy(material, m.material.data(), sizeof(int32_t) * m.material.size());
+  if (dirichlet_pairs && !m.dirichlet.empty())
+    std::memcpy(dirichlet_pairs, m.dirichlet.data(), sizeof(int32_t) * m.dirichlet.size());
+  return EMG_SUCCESS;
+}
+
+int emg_mesh_material_tags(emg_mesh mesh, int32_t* tags) {
+  if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
+  if (tags && !mesh->material_tags.empty())
+    std::memcpy(tags, mesh->material_tags.data(), sizeof(int32_t) * mesh->material_tags.size());
+  return EMG_SUCCESS;
+}
 
 int emg_edge_ids(emg_mesh mesh, int32_t* elem_edge, int32_t* edge_nodes, int64_t* n_edges) {
   return guarded([&]() -> int {

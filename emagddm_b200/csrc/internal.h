@@ -46,5 +46,8 @@ struct DofMap {
 int build_edge_ids(Mesh& m);
 int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out);
 int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, DofMap& out);
+// Gmsh ASCII reader (gmsh.cpp); material_tags[i] = physical tag of material i.
+int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_tags, Mesh& m,
+              std::vector<int32_t>& material_tags);
 
 }  // namespace emg

@@ -168,3 +168,96 @@ def random_instance(n: int, seed: int) -> CubeMesh:
                                     (slo[0], min(shi[0], 0.9), slo[1], min(shi[1], 0.9),
                                      slo[2], min(shi[2], 0.9)))],
                     name=f"cube{n}_rand{seed}")
+
+
+def perturbed(m: CubeMesh, amplitude: float = 0.2, seed: int = 0) -> CubeMesh:
+    """The same mesh with every interior node moved by up to `amplitude` cell
+    widths per coordinate (uniform random, seeded): unstructured geometry on
+    the same topology; boundary nodes stay on the faces."""
+    rng = np.random.default_rng(seed)
+    xyz = m.xyz.copy()
+    interior = np.all((xyz > 1e-12) & (xyz < 1.0 - 1e-12), axis=1)
+    h = 1.0 / m.n
+    xyz[interior] += rng.uniform(-amplitude * h, amplitude * h, (int(interior.sum()), 3))
+    return CubeMesh(**{**m.__dict__, "xyz": xyz, "name": m.name + f"_perturbed{seed}"})
+
+
+def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2), boundary_tag: int = 100):
+    """Write the mesh as an ASCII Gmsh file (2.2 or 4.1): node tags 1..V,
+    the tetrahedra with physical tag volume_tags[material], and every
+    boundary face as a triangle with physical tag `boundary_tag`."""
+    tets = np.asarray(m.tets, np.int64)
+    faces = np.sort(tets[:, [[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]]].reshape(-1, 3), axis=1)
+    uf, cnt = np.unique(faces, axis=0, return_counts=True)
+    bfaces = uf[cnt == 1]
+    vt = np.asarray(volume_tags)[np.asarray(m.material)]
+    with open(path, "w") as f:
+        if version.startswith("2"):
+            f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % m.n_nodes)
+            for i, (x, y, z) in enumerate(m.xyz):
+                f.write(f"{i + 1} {float(x)!r} {float(y)!r} {float(z)!r}\n")
+            f.write("$EndNodes\n$Elements\n%d\n" % (len(bfaces) + len(tets)))
+            eid = 1
+            for a, b, c in bfaces:
+                f.write(f"{eid} 2 2 {boundary_tag} 1 {a + 1} {b + 1} {c + 1}\n")
+                eid += 1
+            for t, tag in zip(tets, vt):
+                f.write(f"{eid} 4 2 {int(tag)} {int(tag)} {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
+                eid += 1
+            f.write("$EndElements\n")
+        else:
+            vols = sorted(set(int(v) for v in vt))
+            f.write("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Entities\n0 0 1 %d\n" % len(vols))
+            f.write(f"1 0 0 0 1 1 1 1 {boundary_tag} 0\n")
+            for v in vols:
+                f.write(f"{v} 0 0 0 1 1 1 1 {v} 0\n")
+            f.write("$EndEntities\n$Nodes\n1 %d 1 %d\n3 1 0 %d\n" % (m.n_nodes, m.n_nodes, m.n_nodes))
+            f.write("".join(f"{i + 1}\n" for i in range(m.n_nodes)))
+            f.write("".join(f"{float(x)!r} {float(y)!r} {float(z)!r}\n" for x, y, z in m.xyz))
+            f.write("$EndNodes\n$Elements\n%d %d 1 %d\n" % (1 + len(vols), len(bfaces) + len(tets),
+                                                           len(bfaces) + len(tets)))
+            eid = 1
+            f.write(f"2 1 2 {len(bfaces)}\n")
+            for a, b, c in bfaces:
+                f.write(f"{eid} {a + 1} {b + 1} {c + 1}\n")
+                eid += 1
+            for v in vols:
+                sel = tets[vt == v]
+                f.write(f"3 {v} 4 {len(sel)}\n")
+                for t in sel:
+                    f.write(f"{eid} {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
+                    eid += 1
+            f.write("$EndElements\n")
+
+
+def read_gmsh(path: str, dirichlet_tags=None, nu=None, sigma=None, sources=None) -> CubeMesh:
+    """Read an ASCII Gmsh file through the library (emg_mesh_read_gmsh).
+    Materials: one per physical volume tag (ascending); nu / sigma per
+    material (default 1 / 0)."""
+    import ctypes as C
+
+    from . import _abi
+    L = _abi.lib()
+    tags = None if not dirichlet_tags else np.ascontiguousarray(dirichlet_tags, np.int32)
+    h = C.c_void_p()
+    _abi.check(L.emg_mesh_read_gmsh(path.encode(), _abi.ptr(tags), 0 if tags is None else len(tags),
+                                    C.byref(h)), "emg_mesh_read_gmsh")
+    try:
+        nn, nt, nd, nm = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        L.emg_mesh_info(h, C.byref(nn), C.byref(nt), C.byref(nd), C.byref(nm))
+        xyz = np.empty((nn.value, 3))
+        tets = np.empty((nt.value, 4), np.int32)
+        mat = np.empty(nt.value, np.int32)
+        dp = np.empty((nd.value, 2), np.int32)
+        L.emg_mesh_export(h, _abi.ptr(xyz), _abi.ptr(tets), _abi.ptr(mat), _abi.ptr(dp))
+        mtags = np.empty(max(nm.value, 1), np.int32)
+        L.emg_mesh_material_tags(h, _abi.ptr(mtags))
+    finally:
+        L.emg_mesh_destroy(h)
+    k = nm.value
+    m = CubeMesh(n=0, xyz=xyz, tets=tets, material=mat, dirichlet=dp,
+                 nu=np.ones(k) if nu is None else np.asarray(nu, np.float64),
+                 sigma=np.zeros(k) if sigma is None else np.asarray(sigma, np.float64),
+                 sources=list(sources or []), name=path)
+    m.material_tags = mtags[:k]
+    return m

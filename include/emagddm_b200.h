@@ -103,6 +103,23 @@ int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const in
                     const int32_t* material_id, int64_t n_dirichlet,
                     const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out);
 void emg_mesh_destroy(emg_mesh mesh);
+/* Gmsh ASCII mesh (format 2.2 or 4.1; the reference's planned mesh format,
+ * mesh/README.md) as an EMMeshData (include/fe_em/em_mesh_data.hpp:90-230):
+ * nodes in ascending Gmsh tag order, the 4-node tetrahedra (type 4) in file
+ * order with material id = rank of their physical tag among the tetrahedra's
+ * distinct physical tags, Dirichlet node pairs = edges of the triangles whose
+ * physical tag is in dirichlet_tags, or of every boundary face (a face of one
+ * tetrahedron) when n_tags == 0.  Binary files and higher-order tetrahedra are
+ * rejected with EMG_INVALID_INPUT. */
+int emg_mesh_read_gmsh(const char* path, const int32_t* dirichlet_tags, int32_t n_tags, emg_mesh* out);
+/* Sizes of a mesh handle; any pointer may be NULL. */
+int emg_mesh_info(emg_mesh mesh, int64_t* n_nodes, int64_t* n_tets, int64_t* n_dirichlet_pairs,
+                  int32_t* n_materials);
+/* Copies out 3*n_nodes coordinates, 4*n_tets nodes, n_tets material ids and
+ * 2*n_dirichlet_pairs nodes; any pointer may be NULL. */
+int emg_mesh_export(emg_mesh mesh, double* xyz, int32_t* tets, int32_t* material, int32_t* dirichlet_pairs);
+/* Physical tag of each material id (n_materials values) of a Gmsh mesh. */
+int emg_mesh_material_tags(emg_mesh mesh, int32_t* tags);
 
 /* ---- GlobalEdgeIDGenerator::generate (src/fe_em/global_edge_id_generator.cpp:30-110)
  * elem_edge: 6*n_tets output or NULL; edge_nodes: 2*n_edges sorted node pair
