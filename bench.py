@@ -52,6 +52,8 @@ def parse():
                          "fetidp64: the 64^3 problem split into 64 jittered box subdomains, "
                          "FETI-DP (factor + solve) next to plain PCG on the same gauged system")
     ap.add_argument("--parts", type=int, default=4, help="fetidp64: subdomains per axis")
+    ap.add_argument("--feti-precond", type=int, default=2,
+                    help="fetidp64: 2 deluxe (FP64 blocks), 3 deluxe with FP32 blocks (mixed precision)")
     ap.add_argument("--instances", type=int, default=512, help="batch512: number of instances")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="ITERS",
                     help="profiling mode: assemble once, then launch ITERS plain CG iterations "
@@ -487,7 +489,7 @@ def run_fetidp(args, rank, world, local_rank):
         rc = fd.factor()
         if rc:
             raise RuntimeError(f"factor {rc}: {L.emg_last_error().decode()}")
-        x, rc, res = fd.solve(tol=TOL, max_iter=2000, precond=2)
+        x, rc, res = fd.solve(tol=TOL, max_iter=2000, precond=args.feti_precond)
         if rc:
             raise RuntimeError(f"solve {rc}: {L.emg_last_error().decode()}")
         out["x"], out["res"], out["stats"] = x, res, fd.stats()
@@ -537,6 +539,9 @@ def run_fetidp(args, rank, world, local_rank):
                                f"subdomains, partition tree gauge, FETI-DP (multifrontal K_rr, deluxe-scaled "
                                f"Dirichlet preconditioner, defect correction) to a true residual of 1e-8",
                    "n": args.n, "subdomains": args.parts ** 3, "setup_host_ms": setup_ms,
+                   "preconditioner": {2: "deluxe-scaled Dirichlet, FP64 blocks",
+                                      3: "deluxe-scaled Dirichlet, FP32 blocks (mixed precision)"}.get(
+                                          args.feti_precond, str(args.feti_precond)),
                    "factor_ms": st["factor_ms"], "solve_ms": st["solve_ms"],
                    "lambda_iterations": int(st["iterations"]), "passes": int(st["passes"]),
                    "true_residual": st["residual"], "plan": info,

@@ -656,9 +656,10 @@ __global__ void k_mirror_lower(int32_t n_mat, const int32_t* __restrict__ dim, c
 
 // Column-dot mat-vec of dense blocks: y_c = sum over rows r in the range of
 // column c of M[r, c] w_r; range 0: r <= c, 1: r >= c, 2: all rows.
+template <class T>
 __global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int32_t* __restrict__ dim,
                                                        const int64_t* __restrict__ m_off,
-                                                       const double* __restrict__ M,
+                                                       const T* __restrict__ M,
                                                        const int64_t* __restrict__ v_off,
                                                        const double* __restrict__ w, double* __restrict__ y,
                                                        int range) {
@@ -668,16 +669,16 @@ __global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int3
   const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (c >= n) return;
   const int lane = threadIdx.x & 31;
-  const double* Mc = M + m_off[m] + static_cast<int64_t>(c) * n;
+  const T* Mc = M + m_off[m] + static_cast<int64_t>(c) * n;
   const double* wm = w + v_off[m];
   const int32_t lo = range == 1 ? c : 0, hi = range == 0 ? c + 1 : n;
   double a0 = 0.0, a1 = 0.0;
   int32_t i = lo + lane;
   for (; i + 32 < hi; i += 64) {
-    a0 = fma(Mc[i], wm[i], a0);
-    a1 = fma(Mc[i + 32], wm[i + 32], a1);
+    a0 = fma(static_cast<double>(Mc[i]), wm[i], a0);
+    a1 = fma(static_cast<double>(Mc[i + 32]), wm[i + 32], a1);
   }
-  if (i < hi) a0 = fma(Mc[i], wm[i], a0);
+  if (i < hi) a0 = fma(static_cast<double>(Mc[i]), wm[i], a0);
   const double acc = warp_sum(a0 + a1);
   if (lane == 0) y[v_off[m] + c] = acc;
 }
@@ -908,8 +909,9 @@ __global__ void __launch_bounds__(64) k_face_gemm_nt(FacesDev Fc, const double* 
 
 // w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
 // as column dots over the stored transposes DT (one warp per i).
+template <class T>
 __global__ void __launch_bounds__(256) k_face_w(FacesDev Fc, const int32_t* __restrict__ lam_entry,
-                                                const double* __restrict__ DaT, const double* __restrict__ DbT,
+                                                const T* __restrict__ DaT, const T* __restrict__ DbT,
                                                 const double* __restrict__ r, double* __restrict__ w) {
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
@@ -917,16 +919,17 @@ __global__ void __launch_bounds__(256) k_face_w(FacesDev Fc, const int32_t* __re
   if (i >= n) return;
   const int lane = threadIdx.x & 31;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
-  const double* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
+  const T* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
   double acc = 0.0;
-  for (int32_t j = lane; j < n; j += 32) acc = fma(Dt[j], r[lam[j]], acc);
+  for (int32_t j = lane; j < n; j += 32) acc = fma(static_cast<double>(Dt[j]), r[lam[j]], acc);
   acc = warp_sum(acc);
   if (lane == 0) w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
 }
 
 // c[e_i] = sum_j D[j, i] y[e_j] (column dot, one warp per i).
+template <class T>
 __global__ void __launch_bounds__(256) k_face_c(FacesDev Fc, const int32_t* __restrict__ lam_entry,
-                                                const double* __restrict__ Da, const double* __restrict__ Db,
+                                                const T* __restrict__ Da, const T* __restrict__ Db,
                                                 const double* __restrict__ y, double* __restrict__ c) {
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
@@ -934,9 +937,9 @@ __global__ void __launch_bounds__(256) k_face_c(FacesDev Fc, const int32_t* __re
   if (i >= n) return;
   const int lane = threadIdx.x & 31;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
-  const double* D = (side ? Db : Da) + Fc.off[f] + static_cast<int64_t>(i) * n;
+  const T* D = (side ? Db : Da) + Fc.off[f] + static_cast<int64_t>(i) * n;
   double acc = 0.0;
-  for (int32_t j = lane; j < n; j += 32) acc = fma(D[j], y[lam_entry[2 * lam[j] + side]], acc);
+  for (int32_t j = lane; j < n; j += 32) acc = fma(static_cast<double>(D[j]), y[lam_entry[2 * lam[j] + side]], acc);
   acc = warp_sum(acc);
   if (lane == 0) c[lam_entry[2 * lam[i] + side]] = acc;
 }
@@ -990,6 +993,12 @@ __global__ void k_axpy_s(int64_t n, double a, const double* __restrict__ x, doub
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     y[i] = fma(a, x[i], y[i]);
+}
+
+__global__ void k_to_f32(int64_t n, const double* __restrict__ x, float* __restrict__ y) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = static_cast<float>(x[i]);
 }
 
 // ------------------------------------------------------------- PCG pieces
@@ -1184,6 +1193,23 @@ int FetiDP::create(const Mesh& m, const DofMap& d, cudaStream_t stream) {
   return setup_device();
 }
 
+int FetiDP::zallocf(float** dst, int64_t n) {
+  *dst = nullptr;
+  n = std::max<int64_t>(n, 1);
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, sizeof(float) * n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("FETI-DP: device allocation of " + std::to_string((n * 4) >> 20) + " MiB failed: " +
+              cudaGetErrorString(e));
+    return EMG_ERR_NOMEM;
+  }
+  dev.push_back(p);
+  EMG_CK(cudaMemsetAsync(p, 0, sizeof(float) * n, st));
+  *dst = static_cast<float*>(p);
+  return EMG_SUCCESS;
+}
+
 int FetiDP::setup_device() {
   const FetiPlan& P = plan;
   const int32_t F = static_cast<int32_t>(P.fronts.size());
@@ -1303,6 +1329,9 @@ int FetiDP::setup_device() {
       (rc = zalloc(&fDb_d, fsz)) || (rc = zalloc(&c_d, nd)) || (rc = zalloc(&fu_d, P.n_union)) ||
       (rc = zalloc(&xacc_d, P.n_dofs)) || (rc = zalloc(&rglob_d, P.n_dofs)) ||
       (rc = zalloc(&root_tmp_d, nd * max_ncol)))
+    return rc;
+  if ((rc = zallocf(&S32_d, P.root_off[S])) || (rc = zallocf(&fDa32_d, fsz)) || (rc = zallocf(&fDb32_d, fsz)) ||
+      (rc = zallocf(&fDaT32_d, fsz)) || (rc = zallocf(&fDbT32_d, fsz)))
     return rc;
   if ((rc = zalloc(&fac_d, P.fac_size + nc2 + fsz)) || (rc = zalloc(&upd_d, P.upd_pool)) ||
       (rc = zalloc(&S_d, P.root_off[S])) || (rc = zalloc(&Linv_d, P.root_off[S])) ||
@@ -1429,8 +1458,8 @@ void FetiDP::coarse_solve(const double* t, double* u) {
   const int32_t nc = plan.n_coarse;
   if (nc == 0) return;
   const dim3 g(static_cast<unsigned>((nc + 7) / 8), 1);
-  k_block_colgemv<<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t, t2_d, 0);
-  k_block_colgemv<<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t2_d, u, 1);
+  k_block_colgemv<double><<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t, t2_d, 0);
+  k_block_colgemv<double><<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t2_d, u, 1);
 }
 
 // q = (F_rr + G S_cc^-1 G^T) p, part = per-block partials of p . q
@@ -1440,8 +1469,8 @@ void FetiDP::apply_F(const double* p, double* q, double* part) {
   RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, p, w_d);
   const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
-  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
-  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
+  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
+  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
   if (P.n_coarse > 0) {
     k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
         P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, nullptr, t_d);
@@ -1467,18 +1496,27 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     return;
   }
   const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
-  if (precond == 2 && P.n_faces > 0) {
+  if (precond >= 2 && P.n_faces > 0) {
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
-    k_face_w<<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fX_d, fXt_d,
-                                                                                  r, w_d);
-    k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
-    k_face_c<<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
+    if (precond == 3) {
+      k_face_w<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
+          fc, d_lam_entry, fDaT32_d, fDbT32_d, r, w_d);
+      k_block_colgemv<float><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S32_d, d_rvoff, w_d, y_d, 2);
+      k_face_c<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
+          fc, d_lam_entry, fDa32_d, fDb32_d, y_d, c_d);
+      k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
+      return;
+    }
+    k_face_w<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fX_d,
+                                                                                          fXt_d, r, w_d);
+    k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+    k_face_c<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
                                                                                   y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, wt_d, r, w_d);
-  k_block_colgemv<<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
   k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, wt_d, y_d, z, r, part);
 }
 
@@ -1506,6 +1544,12 @@ int FetiDP::setup_deluxe() {
   // transposes for the row pass, in the buffers of X and X^T (no longer needed)
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
+  // FP32 copies for the mixed-precision preconditioner
+  const int64_t fsz = P.face_off.back();
+  k_to_f32<<<blocks_for(fsz, 256), 256, 0, st>>>(fsz, fDa_d, fDa32_d);
+  k_to_f32<<<blocks_for(fsz, 256), 256, 0, st>>>(fsz, fDb_d, fDb32_d);
+  k_to_f32<<<blocks_for(fsz, 256), 256, 0, st>>>(fsz, fX_d, fDaT32_d);
+  k_to_f32<<<blocks_for(fsz, 256), 256, 0, st>>>(fsz, fXt_d, fDbT32_d);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
 }
@@ -1610,6 +1654,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
                                                          d_lam_entry, d_dual_sub, rp, cl, vl, ne, rho_d, wt_d, 0);
     k_dual_weights<<<blocks_for(ne, 256), 256, 0, st>>>(d_loc_off, d_nI, d_dual_off, d_dual_lam, d_dual_sign,
                                                          d_lam_entry, d_dual_sub, rp, cl, vl, ne, rho_d, wt_d, 1);
+    k_to_f32<<<blocks_for(P.root_off[S], 256), 256, 0, st>>>(P.root_off[S], S_d, S32_d);
     rc = setup_deluxe();
     if (rc) return rc;
   }
@@ -1735,8 +1780,9 @@ int FetiDP::global_residual(const double* b, const double* x, double* rr) {
 int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, emg_result* res) {
   TraceScope tr("fetidp.solve");
   if (!factored) { set_error("FETI-DP: factor() has not succeeded"); return EMG_INVALID_INPUT; }
-  if (cfg.preconditioner < 0 || cfg.preconditioner > 2) {
-    set_error("FETI-DP preconditioner must be 0 (none), 1 (Dirichlet, stiffness scaling) or 2 (Dirichlet, deluxe)");
+  if (cfg.preconditioner < 0 || cfg.preconditioner > 3) {
+    set_error("FETI-DP preconditioner must be 0 (none), 1 (Dirichlet, stiffness scaling), 2 (Dirichlet, deluxe) "
+              "or 3 (Dirichlet, deluxe, FP32 blocks)");
     return EMG_INVALID_INPUT;
   }
   precond = cfg.preconditioner;

@@ -68,7 +68,7 @@ struct FetiDP {
   FrontsDev fd{};
   FacesDev fc{};
   bool factored = false;
-  int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 Dirichlet deluxe-scaled
+  int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks
   FetiStats stats;
   // plan tables
   int64_t* d_loc_off = nullptr;
@@ -109,6 +109,8 @@ struct FetiDP {
   double *fSa_d = nullptr, *fSb_d = nullptr, *fX_d = nullptr, *fXt_d = nullptr, *fZ_d = nullptr;
   double *fDa_d = nullptr, *fDb_d = nullptr, *c_d = nullptr;
   double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr, *root_tmp_d = nullptr;
+  // FP32 copies of the preconditioner blocks (mixed-precision mode)
+  float *S32_d = nullptr, *fDa32_d = nullptr, *fDb32_d = nullptr, *fDaT32_d = nullptr, *fDbT32_d = nullptr;
   void* state_d = nullptr;
   int32_t* err_d = nullptr;
   static constexpr int kParts = 592;
@@ -129,6 +131,7 @@ struct FetiDP {
   template <class T>
   int up(T** dst, const std::vector<T>& src);
   int zalloc(double** dst, int64_t n);
+  int zallocf(float** dst, int64_t n);
   int setup_device();
   int check_err(const char* where);
   int factor_range(int32_t f0, int32_t f1);

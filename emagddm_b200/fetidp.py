@@ -125,7 +125,8 @@ class FetiDP:
                                        C.cast(arr, C.c_void_p) if arr is not None else None, ns, flags)
 
     def solve(self, tol: float = 1e-10, max_iter: int = 500, precond: int = 2):
-        """precond: 0 none, 1 Dirichlet with stiffness scaling, 2 Dirichlet with deluxe scaling."""
+        """precond: 0 none, 1 Dirichlet with stiffness scaling, 2 Dirichlet with deluxe
+        scaling, 3 the same with the S_DD blocks and face weights stored in FP32."""
         x = np.empty(self.map.n_dofs)
         cfg = _abi.KrylovConfig(tol, max_iter, precond)
         out = _abi.Result()

@@ -174,13 +174,18 @@ int emg_dofmap_partition_info(emg_dofmap map, int32_t* n_parts, int64_t* n_prima
  * The interface problem is solved by FP64 PCG; x is the global solution in
  * the partitioned map's numbering (n_dofs), out->residual_norm the true
  * ||F - K x|| / ||F|| of the global system and cfg->tolerance the bound on
- * it: a multiplier PCG pass (inner relative tolerance 1e-10) is followed by
- * defect-correction passes on the true residual until it holds, the residual
- * stops shrinking, or cfg->max_iterations multiplier iterations are spent in
- * total.  cfg->preconditioner:
- * EMG_FETI_PRECOND_NONE, _STIFFNESS or _DELUXE.  map must come from
- * emg_dof_build_partitioned on the same mesh. */
-enum { EMG_FETI_PRECOND_NONE = 0, EMG_FETI_PRECOND_STIFFNESS = 1, EMG_FETI_PRECOND_DELUXE = 2 };
+ * it: multiplier PCG passes with defect correction on the true residual
+ * (each pass's multiplier tolerance from the measured amplification of the
+ * dual jump) until it holds or cfg->max_iterations multiplier iterations are
+ * spent in total.  cfg->preconditioner: EMG_FETI_PRECOND_NONE, _STIFFNESS,
+ * _DELUXE or _DELUXE_FP32.  map must come from emg_dof_build_partitioned on
+ * the same mesh. */
+enum {
+  EMG_FETI_PRECOND_NONE = 0,
+  EMG_FETI_PRECOND_STIFFNESS = 1,
+  EMG_FETI_PRECOND_DELUXE = 2,
+  EMG_FETI_PRECOND_DELUXE_FP32 = 3  /* deluxe, S_DD and face weights stored in FP32 (mixed precision) */
+};
 typedef struct emg_fetidp_t* emg_fetidp;
 int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* out);
 /* Numeric phase (materials and sources as emg_system_assemble; EMG_FLAG_MASS

@@ -47,7 +47,7 @@ def test_fetidp_matches_monolithic_oracle(kind, n, parts):
     assert st["iterations"] == out.iterations and st["residual"] == out.residual_norm
 
 
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3])
 def test_fetidp_preconditioners_agree(precond):
     m, part, k = make("scale", 8, 2)
     fd = fetidp.FetiDP(m, part, k)
@@ -56,7 +56,7 @@ def test_fetidp_preconditioners_agree(precond):
     assert rc == 0, _abi.lib().emg_last_error()
     xo, _ = monolithic(m, fd.map.l2g)
     assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
-    _, rc, _ = fd.solve(precond=3)
+    _, rc, _ = fd.solve(precond=4)
     assert rc == _abi.EMG_INVALID_INPUT
 
 
