@@ -1388,17 +1388,35 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   }
   const unsigned nf = static_cast<unsigned>(f1 - f0);
   if (nf == 0 || max_np == 0) return EMG_SUCCESS;
+  // fronts ordered by pivot count (descending): a panel step launches only
+  // the prefix that still has pivots, sized to the largest of them
+  std::vector<int32_t> npk(nf), fk(nf);
+  bool sorted = true;
+  for (int32_t k = f0; k < f1; ++k) {
+    npk[k - f0] = k < F ? plan.fronts[k].npiv : xnp[k - F];
+    fk[k - f0] = k < F ? plan.fronts[k].f : xnp[k - F];
+    if (k > f0 && npk[k - f0] > npk[k - f0 - 1]) sorted = false;
+  }
+  unsigned active = nf;
   for (int32_t k0 = 0; k0 < max_np; k0 += kNB) {
-    k_potrf_diag<<<nf, 256, 0, st>>>(fd, f0, k0, fac_d, err_d);
-    const int32_t rows = max_f - k0 - 1;
+    int32_t mf = max_f, mnp = max_np;
+    if (sorted) {
+      while (active > 0 && npk[active - 1] <= k0) --active;
+      mf = 0;
+      for (unsigned q = 0; q < active; ++q) mf = std::max(mf, fk[q]);
+      mnp = npk[0];
+    }
+    if (active == 0) break;
+    k_potrf_diag<<<active, 256, 0, st>>>(fd, f0, k0, fac_d, err_d);
+    const int32_t rows = mf - k0 - 1;
     if (rows > 0) {
       const unsigned rb = static_cast<unsigned>((rows + kTrsmRows - 1) / kTrsmRows);
-      k_trsm_panel<<<dim3(rb, nf), kTrsmRows, 0, st>>>(fd, f0, k0, fac_d);
+      k_trsm_panel<<<dim3(rb, active), kTrsmRows, 0, st>>>(fd, f0, k0, fac_d);
     }
     const int32_t c0 = k0 + kNB;
-    if (c0 < max_np) {
-      const int32_t nct = (max_np - c0 + kTile - 1) / kTile, nrt = (max_f - c0 + kTile - 1) / kTile;
-      k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), nf), 256, 0, st>>>(fd, f0, k0, fac_d);
+    if (c0 < mnp) {
+      const int32_t nct = (mnp - c0 + kTile - 1) / kTile, nrt = (mf - c0 + kTile - 1) / kTile;
+      k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), active), 256, 0, st>>>(fd, f0, k0, fac_d);
     }
   }
   if (max_nu > 0) {

@@ -454,13 +454,20 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
     p.sc_list.resize(tg.size());
     for (size_t i = 0; i < tg.size(); ++i) p.sc_list[i] = tg[i].second;
   }
-  // global front table in level order
-  struct Key { int32_t h, s, i; };
+  // global front table in level order; inside a level by pivot count and
+  // front size, descending, so that each panel step of the factorization can
+  // launch only the prefix of fronts that still have pivots left
+  struct Key { int32_t h, np, f, s, i; };
   std::vector<Key> keys;
   for (int32_t s = 0; s < S; ++s)
-    for (int32_t i = 0; i < static_cast<int32_t>(subf[s].size()); ++i) keys.push_back({subf[s][i].height, s, i});
+    for (int32_t i = 0; i < static_cast<int32_t>(subf[s].size()); ++i) {
+      const LocalFront& lf = subf[s][i];
+      keys.push_back({lf.height, lf.npiv, lf.npiv + static_cast<int32_t>(lf.border.size()), s, i});
+    }
   std::stable_sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) {
     if (a.h != b.h) return a.h < b.h;
+    if (a.np != b.np) return a.np > b.np;
+    if (a.f != b.f) return a.f > b.f;
     if (a.s != b.s) return a.s < b.s;
     return a.i < b.i;
   });
