@@ -97,6 +97,12 @@ SIGNATURES = {
     "emg_fetidp_info": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_stats": ([H, VP, C.c_int32], C.c_int),
     "emg_fetidp_destroy": ([H], None),
+    "emg_fetidp_learned_init": ([H, C.c_uint64], C.c_int),
+    "emg_fetidp_learned_train": ([H, C.c_int32, VP, VP, C.c_float, C.POINTER(C.c_double)], C.c_int),
+    "emg_fetidp_learned_params": ([H, VP, C.POINTER(C.c_int64), C.c_int32], C.c_int),
+    "emg_fetidp_apply": ([H, C.c_int32, VP, VP], C.c_int),
+    "emg_fetidp_lambda_rhs": ([H, VP, VP], C.c_int),
+    "emg_fetidp_duals": ([H, VP, VP, VP, VP], C.c_int),
     "emg_direct_create": ([H, H, VP, C.POINTER(H)], C.c_int),
     "emg_direct_factor": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32], C.c_int),
     "emg_direct_solve": ([H, C.POINTER(KrylovConfig), VP, VP, C.c_int32, C.POINTER(Result)], C.c_int),

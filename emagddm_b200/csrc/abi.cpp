@@ -748,6 +748,54 @@ int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats) {
 
 void emg_fetidp_destroy(emg_fetidp fd) { delete fd; }
 
+int emg_fetidp_learned_init(emg_fetidp fd, uint64_t seed) {
+  return guarded([&]() -> int {
+    if (!fd) { set_error("null FETI-DP handle"); return EMG_INVALID_INPUT; }
+    return emg::learned_init(fd->fd, seed);
+  });
+}
+
+int emg_fetidp_learned_train(emg_fetidp fd, int32_t batch, const double* r_d, const double* t_d, float lr,
+                             double* loss) {
+  return guarded([&]() -> int {
+    if (!fd || !r_d || !t_d) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    return emg::learned_train(fd->fd, batch, r_d, t_d, lr, loss);
+  });
+}
+
+int emg_fetidp_learned_params(emg_fetidp fd, float* params, int64_t* n, int32_t load) {
+  return guarded([&]() -> int {
+    if (!fd) { set_error("null FETI-DP handle"); return EMG_INVALID_INPUT; }
+    return emg::learned_params(fd->fd, params, n, load);
+  });
+}
+
+int emg_fetidp_apply(emg_fetidp fd, int32_t op, const double* in_d, double* out_d) {
+  return guarded([&]() -> int {
+    if (!fd || !in_d || !out_d) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    return fd->fd.apply_op(op, in_d, out_d);
+  });
+}
+
+int emg_fetidp_duals(emg_fetidp fd, int64_t* dual_off, int32_t* dual_lam, int32_t* dual_sign, int32_t* lam_entry) {
+  if (!fd) { set_error("null FETI-DP handle"); return EMG_INVALID_INPUT; }
+  const emg::FetiPlan& p = fd->fd.plan;
+  if (dual_off) std::memcpy(dual_off, p.dual_off.data(), sizeof(int64_t) * p.dual_off.size());
+  if (dual_lam && !p.dual_lam.empty()) std::memcpy(dual_lam, p.dual_lam.data(), sizeof(int32_t) * p.dual_lam.size());
+  if (dual_sign && !p.dual_sign.empty())
+    std::memcpy(dual_sign, p.dual_sign.data(), sizeof(int32_t) * p.dual_sign.size());
+  if (lam_entry && !p.lam_entry.empty())
+    std::memcpy(lam_entry, p.lam_entry.data(), sizeof(int32_t) * p.lam_entry.size());
+  return EMG_SUCCESS;
+}
+
+int emg_fetidp_lambda_rhs(emg_fetidp fd, const double* b_d, double* rhs_d) {
+  return guarded([&]() -> int {
+    if (!fd || !rhs_d) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    return fd->fd.lambda_rhs(b_d, rhs_d);
+  });
+}
+
 int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* out) {
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }

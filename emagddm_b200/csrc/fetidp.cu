@@ -1125,6 +1125,8 @@ unsigned blocks_for(int64_t work, int threads, int cap = 148 * 8) {
 FetiDP::~FetiDP() { release(); }
 
 void FetiDP::release() {
+  free_learn(learn);
+  learn = nullptr;
   if (!dev.empty()) cudaStreamSynchronize(st);
   for (void* p : dev) cudaFree(p);
   dev.clear();
@@ -1328,7 +1330,7 @@ int FetiDP::setup_device() {
       (rc = zalloc(&fXt_d, fsz)) || (rc = zalloc(&fZ_d, fsz)) || (rc = zalloc(&fDa_d, fsz)) ||
       (rc = zalloc(&fDb_d, fsz)) || (rc = zalloc(&c_d, nd)) || (rc = zalloc(&fu_d, P.n_union)) ||
       (rc = zalloc(&xacc_d, P.n_dofs)) || (rc = zalloc(&rglob_d, P.n_dofs)) ||
-      (rc = zalloc(&root_tmp_d, nd * max_ncol)))
+      (rc = zalloc(&root_tmp_d, nd * max_ncol)) || (rc = zalloc(&rold_d, nl)) || (rc = zalloc(&zm_d, nl)))
     return rc;
   if ((rc = zallocf(&S32_d, P.root_off[S])) || (rc = zallocf(&fDa32_d, fsz)) || (rc = zallocf(&fDb32_d, fsz)) ||
       (rc = zallocf(&fDaT32_d, fsz)) || (rc = zallocf(&fDbT32_d, fsz)))
@@ -1514,7 +1516,7 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     return;
   }
   const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
-  if (precond >= 2 && P.n_faces > 0) {
+  if (precond >= 2 && P.n_faces > 0) {  // 4: the Dirichlet part of deluxe + learned
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
     if (precond == 3) {
       k_face_w<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
@@ -1715,6 +1717,7 @@ int FetiDP::prepare_rhs(const double* fu) {
 
 // lambda-PCG on rhs_d; returns the status, sets *iters and *rel.
 int FetiDP::lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel) {
+  if (precond == 4) return lambda_fcg(tol, max_it, iters, rel);
   const int64_t nl = plan.n_lambda;
   LamState* sd = static_cast<LamState*>(state_d);
   LamState hs{};
@@ -1749,6 +1752,110 @@ int FetiDP::lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel) 
   }
   *iters = std::min(it, max_it);
   return status;
+}
+
+__global__ void k_lam_xpby(int64_t n, const double* __restrict__ x, double b, double* __restrict__ y) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = fma(b, y[i], x[i]);
+}
+
+double FetiDP::dot_host(const double* a, const double* b, int64_t n) {
+  dot(a, b, n, 2);
+  LamState hs{};
+  cudaMemcpyAsync(&hs, state_d, sizeof(LamState), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  return hs.rr;
+}
+
+// Flexible CG (Polak-Ribiere beta) with z = M_D r + L(r); where z is not a
+// descent direction (z . r <= 0) the step falls back to the Dirichlet z = M_D r.
+int FetiDP::lambda_fcg(double tol, int32_t max_it, int32_t* iters, double* rel) {
+  const int64_t nl = plan.n_lambda;
+  *iters = 0;
+  *rel = 0.0;
+  if (nl == 0) return EMG_SUCCESS;
+  const unsigned g = blocks_for(nl, 256);
+  EMG_CK(cudaMemsetAsync(lam_d, 0, sizeof(double) * nl, st));
+  EMG_CK(cudaMemcpyAsync(r_d, rhs_d, sizeof(double) * nl, cudaMemcpyDeviceToDevice, st));
+  const double rr0 = dot_host(r_d, r_d, nl);
+  if (!(rr0 > 0.0)) return EMG_SUCCESS;
+  auto precondition = [&](double* rz_out) -> int {
+    apply_M(r_d, zm_d, part_d);
+    int rc = learned_apply(*this, r_d, zm_d, z_d);
+    if (rc) return rc;
+    double rz = dot_host(z_d, r_d, nl);
+    if (!(rz > 0.0) || !std::isfinite(rz)) {
+      EMG_CK(cudaMemcpyAsync(z_d, zm_d, sizeof(double) * nl, cudaMemcpyDeviceToDevice, st));
+      rz = dot_host(z_d, r_d, nl);
+    }
+    *rz_out = rz;
+    return EMG_SUCCESS;
+  };
+  double rz = 0.0;
+  int rc = precondition(&rz);
+  if (rc) return rc;
+  EMG_CK(cudaMemcpyAsync(p_d, z_d, sizeof(double) * nl, cudaMemcpyDeviceToDevice, st));
+  int status = EMG_MAX_ITER_REACHED;
+  int32_t it = 1;
+  for (; it <= max_it; ++it) {
+    apply_F(p_d, q_d, part_d);
+    const double pq = dot_host(p_d, q_d, nl);
+    if (!(pq > 0.0) || !std::isfinite(pq)) { status = EMG_NUMERICAL_ERROR; break; }
+    const double alpha = rz / pq;
+    k_axpy_s<<<g, 256, 0, st>>>(nl, alpha, p_d, lam_d);
+    EMG_CK(cudaMemcpyAsync(rold_d, r_d, sizeof(double) * nl, cudaMemcpyDeviceToDevice, st));
+    k_axpy_s<<<g, 256, 0, st>>>(nl, -alpha, q_d, r_d);
+    const double rr = dot_host(r_d, r_d, nl);
+    *rel = std::sqrt(std::max(rr, 0.0) / rr0);
+    if (!std::isfinite(rr)) { status = EMG_NUMERICAL_ERROR; break; }
+    if (*rel < tol) { status = EMG_SUCCESS; break; }
+    double rz_new = 0.0;
+    rc = precondition(&rz_new);
+    if (rc) return rc;
+    const double zro = dot_host(z_d, rold_d, nl);
+    const double beta = (rz_new - zro) / rz;
+    k_lam_xpby<<<g, 256, 0, st>>>(nl, z_d, beta, p_d);
+    rz = rz_new;
+  }
+  EMG_CK(cudaGetLastError());
+  *iters = std::min(it, max_it);
+  return status;
+}
+
+int FetiDP::apply_op(int32_t op, const double* in, double* out) {
+  if (!factored) { set_error("FETI-DP: factor() has not succeeded"); return EMG_INVALID_INPUT; }
+  if (plan.n_lambda == 0) return EMG_SUCCESS;
+  const int32_t saved = precond;
+  precond = 2;
+  int rc = EMG_SUCCESS;
+  if (op == 0) apply_F(in, out, part_d);
+  else if (op == 1) apply_M(in, out, part_d);
+  else if (op == 2) rc = learned_apply(*this, in, nullptr, out);
+  else if (op == 3) {
+    apply_M(in, zm_d, part_d);
+    rc = learned_apply(*this, in, zm_d, out);
+  } else {
+    set_error("unknown multiplier operator");
+    rc = EMG_INVALID_INPUT;
+  }
+  precond = saved;
+  if (!rc) EMG_CK(cudaGetLastError());
+  return rc;
+}
+
+int FetiDP::lambda_rhs(const double* b, double* out) {
+  if (!factored) { set_error("FETI-DP: factor() has not succeeded"); return EMG_INVALID_INPUT; }
+  const int64_t N = plan.n_dofs;
+  if (b) EMG_CK(cudaMemcpyAsync(bg_d, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+  else k_gather_sum<int32_t><<<blocks_for(N, 256), 256, 0, st>>>(N, d_gptr, d_glist, un.rhs, bg_d);
+  k_distribute<<<blocks_for(N, 256), 256, 0, st>>>(N, d_gptr, d_glist, bg_d, fu_d);
+  int rc = prepare_rhs(fu_d);
+  if (rc) return rc;
+  if (plan.n_lambda > 0)
+    EMG_CK(cudaMemcpyAsync(out, rhs_d, sizeof(double) * plan.n_lambda, cudaMemcpyDeviceToDevice, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  return EMG_SUCCESS;
 }
 
 // Recovery for the union right-hand side fu into xg_d:
@@ -1798,9 +1905,13 @@ int FetiDP::global_residual(const double* b, const double* x, double* rr) {
 int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, emg_result* res) {
   TraceScope tr("fetidp.solve");
   if (!factored) { set_error("FETI-DP: factor() has not succeeded"); return EMG_INVALID_INPUT; }
-  if (cfg.preconditioner < 0 || cfg.preconditioner > 3) {
-    set_error("FETI-DP preconditioner must be 0 (none), 1 (Dirichlet, stiffness scaling), 2 (Dirichlet, deluxe) "
-              "or 3 (Dirichlet, deluxe, FP32 blocks)");
+  if (cfg.preconditioner < 0 || cfg.preconditioner > 4) {
+    set_error("FETI-DP preconditioner must be 0 (none), 1 (Dirichlet, stiffness scaling), 2 (Dirichlet, deluxe), "
+              "3 (Dirichlet, deluxe, FP32 blocks) or 4 (deluxe + learned correction)");
+    return EMG_INVALID_INPUT;
+  }
+  if (cfg.preconditioner == 4 && !learn) {
+    set_error("FETI-DP preconditioner 4 needs a learned preconditioner (emg_fetidp_learned_init)");
     return EMG_INVALID_INPUT;
   }
   precond = cfg.preconditioner;

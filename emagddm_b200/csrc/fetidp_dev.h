@@ -60,15 +60,20 @@ struct FetiStats {
   double factor_ms = 0.0, solve_ms = 0.0;
 };
 
+struct LearnState;
+void free_learn(LearnState* L);
+
 struct FetiDP {
   FetiPlan plan;
+  LearnState* learn = nullptr;  // learned interface preconditioner (learned.cu), optional
   System un;  // block-diagonal union of the subdomain matrices
   cudaStream_t st = nullptr;
   std::vector<void*> dev;
   FrontsDev fd{};
   FacesDev fc{};
   bool factored = false;
-  int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks
+  int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks,
+                        // 4 deluxe + learned correction (flexible CG)
   FetiStats stats;
   // plan tables
   int64_t* d_loc_off = nullptr;
@@ -109,6 +114,7 @@ struct FetiDP {
   double *fSa_d = nullptr, *fSb_d = nullptr, *fX_d = nullptr, *fXt_d = nullptr, *fZ_d = nullptr;
   double *fDa_d = nullptr, *fDb_d = nullptr, *c_d = nullptr;
   double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr, *root_tmp_d = nullptr;
+  double *rold_d = nullptr, *zm_d = nullptr;  // flexible CG
   // FP32 copies of the preconditioner blocks (mixed-precision mode)
   float *S32_d = nullptr, *fDa32_d = nullptr, *fDb32_d = nullptr, *fDaT32_d = nullptr, *fDbT32_d = nullptr;
   void* state_d = nullptr;
@@ -126,6 +132,11 @@ struct FetiDP {
   // assembled F) to the true relative residual cfg.tolerance: FETI-DP passes
   // (lambda-PCG, recovery) with defect correction on the true residual.
   int solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, emg_result* res);
+  // Multiplier-space pieces for training and tests: op 0 F, 1 deluxe M_D,
+  // 2 learned correction L, 3 M_D + L (device vectors of n_lambda).
+  int apply_op(int32_t op, const double* in, double* out);
+  // Right-hand side of the multiplier system for a global b (null = F).
+  int lambda_rhs(const double* b, double* out);
 
  private:
   template <class T>
@@ -144,8 +155,16 @@ struct FetiDP {
   void trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off, double* X);
   int prepare_rhs(const double* fu);
   int lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel);
+  int lambda_fcg(double tol, int32_t max_it, int32_t* iters, double* rel);
+  double dot_host(const double* a, const double* b, int64_t n);
   int recover(const double* fu);
   int global_residual(const double* b, const double* x, double* rr);
 };
+
+// learned.cu
+int learned_init(FetiDP& F, uint64_t seed);
+int learned_apply(FetiDP& F, const double* r, const double* add, double* out);
+int learned_train(FetiDP& F, int32_t B, const double* r, const double* t, float lr, double* loss);
+int learned_params(FetiDP& F, float* host, int64_t* n, int32_t load);
 
 }  // namespace emg

@@ -161,6 +161,20 @@ def gauged_map(m, gauge: int):
     return _MapHandle(h), mh, l2g, nd.value
 
 
+def dual_layout(fd: "FetiDP") -> dict:
+    """The multiplier layout of a FETI-DP solver (emg_fetidp_duals)."""
+    info = fd.info()
+    S, ne, nl = info["n_parts"], info["sum_nD"], info["n_lambda"]
+    dual_off = np.empty(S + 1, np.int64)
+    dual_lam = np.empty(max(ne, 1), np.int32)
+    dual_sign = np.empty(max(ne, 1), np.int32)
+    lam_entry = np.empty((max(nl, 1), 2), np.int32)
+    check(lib().emg_fetidp_duals(fd.h, ptr(dual_off), ptr(dual_lam), ptr(dual_sign), ptr(lam_entry)),
+          "emg_fetidp_duals")
+    return {"n_parts": S, "n_entries": ne, "dual_off": dual_off, "dual_lam": dual_lam[:ne],
+            "dual_sign": dual_sign[:ne], "lam_entry": lam_entry[:nl]}
+
+
 class DirectSolver:
     """GPU sparse direct solver (nested dissection + multifrontal Cholesky,
     iterative refinement) for the gauged system of mesh ``m`` -- the

@@ -201,6 +201,33 @@ int emg_fetidp_solve(emg_fetidp fd, const emg_krylov_config* cfg, double* x, int
  * emg_fetidp_factor. */
 int emg_fetidp_solve_rhs(emg_fetidp fd, const emg_krylov_config* cfg, const double* b, double* x,
                          int32_t on_device, emg_result* out);
+/* ---- Learned interface preconditioner (no reference counterpart): one
+ * 3-layer MLP per subdomain (width 256, BF16 weights, FP32 accumulation)
+ * mapping the subdomain's normalised dual residual to a correction of the
+ * deluxe Dirichlet step; preconditioner EMG_FETI_PRECOND_LEARNED solves with
+ * flexible CG and z = M_D r + L(r), falling back to M_D r where that is not
+ * a descent direction; the true FP64 residual still decides convergence.
+ * Initialised with W3 = 0 (adds nothing until trained). */
+enum { EMG_FETI_PRECOND_LEARNED = 4 };
+int emg_fetidp_learned_init(emg_fetidp fd, uint64_t seed);
+/* One Adam step on `batch` (residual, wanted correction) pairs: r_d, t_d are
+ * device arrays of batch x n_lambda; loss (may be NULL) gets the mean squared
+ * error of the normalised outputs before the step. */
+int emg_fetidp_learned_train(emg_fetidp fd, int32_t batch, const double* r_d, const double* t_d, float lr,
+                             double* loss);
+/* FP32 master parameters (host array of *n floats): load != 0 copies in. */
+int emg_fetidp_learned_params(emg_fetidp fd, float* params, int64_t* n, int32_t load);
+/* Multiplier space, device vectors of n_lambda (emg_fetidp_info[3]):
+ * op 0 F, 1 deluxe Dirichlet M_D, 2 learned correction L, 3 M_D + L. */
+int emg_fetidp_apply(emg_fetidp fd, int32_t op, const double* in_d, double* out_d);
+/* Right-hand side d - G S_cc^-1 g_c of the multiplier system for a global b
+ * (device, n_dofs; NULL = the assembled F) into rhs_d (device, n_lambda). */
+int emg_fetidp_lambda_rhs(emg_fetidp fd, const double* b_d, double* rhs_d);
+/* Dual layout: dual_off (n_parts + 1) over the dual entries (subdomain,
+ * dual DOF), each entry's multiplier and sign (+1 on the lower subdomain),
+ * and lam_entry (2 per multiplier: its + and - entries).  NULL skips. */
+int emg_fetidp_duals(emg_fetidp fd, int64_t* dual_off, int32_t* dual_lam, int32_t* dual_sign, int32_t* lam_entry);
+
 /* info[0..19]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
  * n_levels, max_front, max_pivots, factor doubles, update-pool doubles,
  * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children, and the
