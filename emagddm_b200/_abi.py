@@ -18,6 +18,7 @@ EMG_SUCCESS, EMG_NUMERICAL_ERROR, EMG_DIVERGED, EMG_MAX_ITER_REACHED, EMG_INVALI
 EMG_ERR_CUDA, EMG_ERR_TIMEOUT, EMG_ERR_NOMEM, EMG_ERR_INTERNAL = 5, 6, 7, 8
 GAUGE_NONE, GAUGE_REF, GAUGE_BOUNDARY_FIRST = -1, 0, 1
 FLAG_MASS, FLAG_NO_EDGE_SIGNS, FLAG_PIOLA_LITERAL, FLAG_QUAD3_LITERAL = 1, 2, 4, 8
+ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
 PRECOND_NONE, PRECOND_JACOBI = 0, 1
 
 I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -46,6 +47,9 @@ SIGNATURES = {
     "emg_last_error": ([], C.c_char_p),
     "emg_mesh_create": ([C.c_int64, VP, C.c_int64, VP, VP, C.c_int64, VP, C.c_int32,
                          C.POINTER(H)], C.c_int),
+    "emg_mesh_create_typed": ([C.c_int32, C.c_int64, VP, C.c_int64, VP, VP, C.c_int64, VP, C.c_int32,
+                               C.POINTER(H)], C.c_int),
+    "emg_mesh_elem_type": ([H, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "emg_mesh_destroy": ([H], None),
     "emg_mesh_read_gmsh": ([C.c_char_p, VP, C.c_int32, C.POINTER(H)], C.c_int),
     "emg_mesh_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -64,6 +68,8 @@ SIGNATURES = {
     "emg_system_create": ([C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, VP, C.POINTER(H)], C.c_int),
     "emg_system_create_device": ([C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, VP,
                                   C.POINTER(H)], C.c_int),
+    "emg_system_create_typed": ([C.c_int32, C.c_int64, VP, C.c_int64, VP, VP, VP, C.c_int64, C.c_int32, VP,
+                                 C.POINTER(H)], C.c_int),
     "emg_system_assemble": ([H, VP, VP, C.c_int32, VP, C.c_int32, C.c_int32, VP], C.c_int),
     "emg_system_set_source_map": ([H, VP], C.c_int),
     "emg_system_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),

@@ -73,9 +73,17 @@ class BoundaryMarker:
 @dataclass
 class EMMeshData:
     xyz: np.ndarray                      # (V, 3) node coordinates, node id = row
-    tets: np.ndarray                     # (T, 4) TET4_EDGE elements
+    tets: np.ndarray                     # (T, 4) TET4_EDGE or (T, 8) HEX8_EDGE elements
     material_id: np.ndarray = None       # (T,)
     boundary_markers: list = field(default_factory=list)
+
+    @property
+    def elem_type(self) -> int:
+        """numeric::ElementType of the elements: TET4_EDGE (4 nodes) or HEX8_EDGE (8)."""
+        return _abi.ELEM_HEX8_EDGE if np.asarray(self.tets).shape[1] == 8 else _abi.ELEM_TET4_EDGE
+
+    def edges_per_element(self) -> int:
+        return 12 if self.elem_type == _abi.ELEM_HEX8_EDGE else 6
 
     @classmethod
     def from_cube(cls, mesh) -> "EMMeshData":
@@ -126,9 +134,9 @@ class _Mesh:
         self.material = None if mat is None else np.ascontiguousarray(mat, dtype=np.int32)
         d = np.ascontiguousarray(mesh.dirichlet_pairs(), dtype=np.int32)
         self.h = C.c_void_p()
-        check(L.emg_mesh_create(self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0], ptr(self.tets),
-                                ptr(self.material), d.shape[0], ptr(d) if d.size else None,
-                                mesh.hole_marker_count(), C.byref(self.h)), "emg_mesh_create")
+        check(L.emg_mesh_create_typed(mesh.elem_type, self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0],
+                                      ptr(self.tets), ptr(self.material), d.shape[0], ptr(d) if d.size else None,
+                                      mesh.hole_marker_count(), C.byref(self.h)), "emg_mesh_create_typed")
 
     def __del__(self, _abi=_abi):
         if getattr(self, "h", None) and _abi._LIB is not None:
@@ -149,7 +157,7 @@ class GlobalEdgeIDGenerator:
         n = C.c_int64()
         check(lib().emg_edge_ids(self._mesh.h, None, None, C.byref(n)), "emg_edge_ids")
         T = self.mesh_data.getElementCount()
-        self._elem_edge = np.empty((T, 6), np.int32)
+        self._elem_edge = np.empty((T, self.mesh_data.edges_per_element()), np.int32)
         self._edge_nodes = np.empty((n.value, 2), np.int32)
         check(lib().emg_edge_ids(self._mesh.h, ptr(self._elem_edge), ptr(self._edge_nodes), C.byref(n)),
               "emg_edge_ids")
@@ -190,7 +198,7 @@ class EMDOFManager:
         check(lib().emg_dof_build(self._mesh.h, gauge, C.byref(h)), "emg_dof_build")
         ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
         lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
-        l2g = np.empty((self.mesh_data.getElementCount(), 6), np.int32)
+        l2g = np.empty((self.mesh_data.getElementCount(), self.mesh_data.edges_per_element()), np.int32)
         ed = np.empty(ne.value, np.int32)
         lib().emg_dofmap_export(h, ptr(l2g), ptr(ed))
         if self._map is not None:
@@ -314,7 +322,7 @@ class CsrMatrix:
 
 
 class EMAssembly:
-    """GPU assembly of TET4_EDGE curl-curl systems (EMAssembly::assemble)."""
+    """GPU assembly of TET4_EDGE / HEX8_EDGE curl-curl systems (EMAssembly::assemble)."""
 
     def __init__(self):
         self._sys = None
@@ -341,8 +349,8 @@ class EMAssembly:
             self._stats.error_message = "DOF map shorter than the element list"
             return False
         h = C.c_void_p()
-        rc = L.emg_system_create(xyz.shape[0], ptr(xyz), tets.shape[0], ptr(tets), ptr(mat), ptr(l2g),
-                                 0, None, C.byref(h))
+        rc = L.emg_system_create_typed(mesh_data.elem_type, xyz.shape[0], ptr(xyz), tets.shape[0], ptr(tets),
+                                       ptr(mat), ptr(l2g), 0, 0, None, C.byref(h))
         if rc != 0:
             self._stats.error_message = L.emg_last_error().decode()
             return False

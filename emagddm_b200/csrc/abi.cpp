@@ -76,12 +76,14 @@ int upload(T** dst, const T* src, int64_t count, bool src_on_device, cudaStream_
   return EMG_SUCCESS;
 }
 
-int system_create_impl(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
-                       const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
-                       emg_system* out, bool on_device) {
+int system_create_impl(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                       const int32_t* elems, const int32_t* material, const int32_t* l2g, int64_t n_dofs,
+                       void* stream, emg_system* out, bool on_device) {
   if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
   *out = nullptr;
-  if (n_nodes <= 0 || n_tets <= 0 || !xyz || !tets || !l2g) {
+  if (!emg::valid_elem_type(elem_type)) { set_error("unknown element type"); return EMG_INVALID_INPUT; }
+  const int npe = emg::nodes_per_elem(elem_type), epe = emg::edges_per_elem(elem_type);
+  if (n_nodes <= 0 || n_elems <= 0 || !xyz || !elems || !l2g) {
     set_error("mesh is empty");  // em_assembly.cpp:154-166
     return EMG_INVALID_INPUT;
   }
@@ -90,12 +92,12 @@ int system_create_impl(int64_t n_nodes, const double* xyz, int64_t n_tets, const
     std::vector<int32_t> h;
     const int32_t* src = l2g;
     if (on_device) {
-      h.resize(6 * n_tets);
-      EMG_CK(cudaMemcpy(h.data(), l2g, sizeof(int32_t) * 6 * n_tets, cudaMemcpyDeviceToHost));
+      h.resize(epe * n_elems);
+      EMG_CK(cudaMemcpy(h.data(), l2g, sizeof(int32_t) * epe * n_elems, cudaMemcpyDeviceToHost));
       src = h.data();
     }
     int64_t mx = -1;
-    for (int64_t i = 0; i < 6 * n_tets; ++i) mx = std::max<int64_t>(mx, src[i]);
+    for (int64_t i = 0; i < epe * n_elems; ++i) mx = std::max<int64_t>(mx, src[i]);
     n_dofs = mx + 1;
     if (n_dofs <= 0) { set_error("no free DOF (all constrained)"); return EMG_INVALID_INPUT; }
   }
@@ -103,17 +105,18 @@ int system_create_impl(int64_t n_nodes, const double* xyz, int64_t n_tets, const
   auto* h = new emg_system_t();
   emg::System& s = h->s;
   cudaStream_t st = as_stream(stream);
+  s.elem_type = elem_type;
   s.n_nodes = n_nodes;
-  s.n_tets = n_tets;
+  s.n_elems = n_elems;
   s.n = n_dofs;
   int rc = EMG_SUCCESS;
   if (!rc) rc = upload(&s.xyz, xyz, 3 * n_nodes, on_device, st);
-  if (!rc) rc = upload(&s.tets, tets, 4 * n_tets, on_device, st);
-  if (!rc) rc = upload(&s.l2g, l2g, 6 * n_tets, on_device, st);
+  if (!rc) rc = upload(&s.elems, elems, npe * n_elems, on_device, st);
+  if (!rc) rc = upload(&s.l2g, l2g, epe * n_elems, on_device, st);
   if (!rc) {
-    rc = upload(&s.material, material, n_tets, on_device, st);
+    rc = upload(&s.material, material, n_elems, on_device, st);
     if (!rc && !material) {
-      cudaError_t e = cudaMemsetAsync(s.material, 0, sizeof(int32_t) * n_tets, st);
+      cudaError_t e = cudaMemsetAsync(s.material, 0, sizeof(int32_t) * n_elems, st);
       if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
     }
   }
@@ -200,7 +203,7 @@ void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
 emg::DofMap single_part(const emg::DofMap& d) {
   emg::DofMap s = d;
   s.n_parts = 1;
-  s.tet_part.assign(d.n_tets, 0);
+  s.tet_part.assign(d.n_elems, 0);
   s.dof_primal.assign(d.n_dofs, 0);
   s.n_primal_fix = 0;
   return s;
@@ -217,32 +220,50 @@ const char* emg_last_error(void) { return emg::g_error.c_str(); }
 int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
                     const int32_t* material_id, int64_t n_dirichlet,
                     const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out) {
+  return emg_mesh_create_typed(EMG_ELEM_TET4_EDGE, n_nodes, xyz, n_tets, tets, material_id, n_dirichlet,
+                               dirichlet_pairs, n_hole_markers, out);
+}
+
+int emg_mesh_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                          const int32_t* elems, const int32_t* material_id, int64_t n_dirichlet,
+                          const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out) {
   return guarded([&]() -> int {
     if (!out) { set_error("null output handle"); return EMG_INVALID_INPUT; }
     *out = nullptr;
-    if (n_nodes <= 0 || n_tets <= 0 || !tets) { set_error("mesh is empty"); return EMG_INVALID_INPUT; }
+    if (!emg::valid_elem_type(elem_type)) { set_error("unknown element type"); return EMG_INVALID_INPUT; }
+    const int npe = emg::nodes_per_elem(elem_type);
+    if (n_nodes <= 0 || n_elems <= 0 || !elems) { set_error("mesh is empty"); return EMG_INVALID_INPUT; }
     if (n_dirichlet < 0 || (n_dirichlet > 0 && !dirichlet_pairs)) {
       set_error("bad Dirichlet pair list");
       return EMG_INVALID_INPUT;
     }
-    for (int64_t i = 0; i < 4 * n_tets; ++i)
-      if (tets[i] < 0 || tets[i] >= n_nodes) {
+    for (int64_t i = 0; i < npe * n_elems; ++i)
+      if (elems[i] < 0 || elems[i] >= n_nodes) {
         set_error("element node index out of range");  // em_assembly.cpp:603-608
         return EMG_INVALID_INPUT;
       }
     auto* h = new emg_mesh_t();
     emg::Mesh& m = h->m;
+    m.elem_type = elem_type;
     m.n_nodes = n_nodes;
-    m.n_tets = n_tets;
+    m.n_elems = n_elems;
     if (xyz) m.xyz.assign(xyz, xyz + 3 * n_nodes);
-    m.tets.assign(tets, tets + 4 * n_tets);
-    if (material_id) m.material.assign(material_id, material_id + n_tets);
-    else m.material.assign(n_tets, 0);
+    m.elems.assign(elems, elems + npe * n_elems);
+    if (material_id) m.material.assign(material_id, material_id + n_elems);
+    else m.material.assign(n_elems, 0);
     if (n_dirichlet > 0) m.dirichlet.assign(dirichlet_pairs, dirichlet_pairs + 2 * n_dirichlet);
     m.n_hole_markers = n_hole_markers > 0 ? n_hole_markers : 0;
     *out = h;
     return EMG_SUCCESS;
   });
+}
+
+int emg_mesh_elem_type(emg_mesh mesh, int32_t* elem_type, int32_t* nodes_per_elem, int32_t* edges_per_elem) {
+  if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
+  if (elem_type) *elem_type = mesh->m.elem_type;
+  if (nodes_per_elem) *nodes_per_elem = mesh->m.npe();
+  if (edges_per_elem) *edges_per_elem = mesh->m.epe();
+  return EMG_SUCCESS;
 }
 
 void emg_mesh_destroy(emg_mesh mesh) { delete mesh; }
@@ -262,11 +283,11 @@ int emg_mesh_read_gmsh(const char* path, const int32_t* dirichlet_tags, int32_t 
   });
 }
 
-int emg_mesh_info(emg_mesh mesh, int64_t* n_nodes, int64_t* n_tets, int64_t* n_dirichlet, int32_t* n_materials) {
+int emg_mesh_info(emg_mesh mesh, int64_t* n_nodes, int64_t* n_elems, int64_t* n_dirichlet, int32_t* n_materials) {
   if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
   const emg::Mesh& m = mesh->m;
   if (n_nodes) *n_nodes = m.n_nodes;
-  if (n_tets) *n_tets = m.n_tets;
+  if (n_elems) *n_elems = m.n_elems;
   if (n_dirichlet) *n_dirichlet = static_cast<int64_t>(m.dirichlet.size() / 2);
   if (n_materials) {
     int32_t mx = -1;
@@ -280,7 +301,7 @@ int emg_mesh_export(emg_mesh mesh, double* xyz, int32_t* tets, int32_t* material
   if (!mesh) { set_error("null mesh"); return EMG_INVALID_INPUT; }
   const emg::Mesh& m = mesh->m;
   if (xyz && !m.xyz.empty()) std::memcpy(xyz, m.xyz.data(), sizeof(double) * m.xyz.size());
-  if (tets) std::memcpy(tets, m.tets.data(), sizeof(int32_t) * m.tets.size());
+  if (tets) std::memcpy(tets, m.elems.data(), sizeof(int32_t) * m.elems.size());
   if (material) std::memcpy(material, m.material.data(), sizeof(int32_t) * m.material.size());
   if (dirichlet_pairs && !m.dirichlet.empty())
     std::memcpy(dirichlet_pairs, m.dirichlet.data(), sizeof(int32_t) * m.dirichlet.size());
@@ -376,7 +397,8 @@ int emg_system_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const 
                       const int32_t* material, const int32_t* l2g, int64_t n_dofs, void* stream,
                       emg_system* out) {
   return guarded([&]() -> int {
-    return system_create_impl(n_nodes, xyz, n_tets, tets, material, l2g, n_dofs, stream, out, false);
+    return system_create_impl(EMG_ELEM_TET4_EDGE, n_nodes, xyz, n_tets, tets, material, l2g, n_dofs, stream,
+                              out, false);
   });
 }
 
@@ -384,7 +406,17 @@ int emg_system_create_device(int64_t n_nodes, const double* xyz_d, int64_t n_tet
                              const int32_t* tets_d, const int32_t* material_d,
                              const int32_t* l2g_d, int64_t n_dofs, void* stream, emg_system* out) {
   return guarded([&]() -> int {
-    return system_create_impl(n_nodes, xyz_d, n_tets, tets_d, material_d, l2g_d, n_dofs, stream, out, true);
+    return system_create_impl(EMG_ELEM_TET4_EDGE, n_nodes, xyz_d, n_tets, tets_d, material_d, l2g_d, n_dofs,
+                              stream, out, true);
+  });
+}
+
+int emg_system_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                            const int32_t* elems, const int32_t* material, const int32_t* l2g,
+                            int64_t n_dofs, int32_t on_device, void* stream, emg_system* out) {
+  return guarded([&]() -> int {
+    return system_create_impl(elem_type, n_nodes, xyz, n_elems, elems, material, l2g, n_dofs, stream, out,
+                              on_device != 0);
   });
 }
 
@@ -402,8 +434,8 @@ int emg_system_set_source_map(emg_system sys, const int32_t* tet_source) {
     emg::System& s = sys->s;
     if (s.src_map) { EMG_CK(cudaFreeAsync(s.src_map, 0)); s.src_map = nullptr; }
     if (!tet_source) return EMG_SUCCESS;
-    EMG_CK(cudaMallocAsync(&s.src_map, sizeof(int32_t) * s.n_tets, 0));
-    EMG_CK(cudaMemcpyAsync(s.src_map, tet_source, sizeof(int32_t) * s.n_tets, cudaMemcpyHostToDevice, 0));
+    EMG_CK(cudaMallocAsync(&s.src_map, sizeof(int32_t) * s.n_elems, 0));
+    EMG_CK(cudaMemcpyAsync(s.src_map, tet_source, sizeof(int32_t) * s.n_elems, cudaMemcpyHostToDevice, 0));
     EMG_CK(cudaStreamSynchronize(0));
     return EMG_SUCCESS;
   });
@@ -800,7 +832,8 @@ int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* o
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
     *out = nullptr;
-    if (map->d.n_tets != mesh->m.n_tets || map->d.l2g.size() != static_cast<size_t>(6 * mesh->m.n_tets)) {
+    if (map->d.n_elems != mesh->m.n_elems || map->d.elem_type != mesh->m.elem_type ||
+        map->d.l2g.size() != static_cast<size_t>(mesh->m.epe() * mesh->m.n_elems)) {
       set_error("DOF map does not belong to this mesh");
       return EMG_INVALID_INPUT;
     }

@@ -1,16 +1,17 @@
-// assembly.cu -- EMAssembly::assemble on the GPU for TET4_EDGE elements
-// (reference: src/numeric/em_assembly.cpp:144-420 with the intended
+// assembly.cu -- EMAssembly::assemble on the GPU for TET4_EDGE and HEX8_EDGE
+// elements (reference: src/numeric/em_assembly.cpp:144-420 with the intended
 // MagneticVector3DIntegrator formulas, magnetic_vector_3d_integrator.cpp:139-364).
 //
 // Symbolic phase (once per mesh + DOF map):
 //   k_count_rows / scan / k_fill_incidence / k_sort_incidence build, for every
-//   equation row r, the sorted list of (tet, local edge) slots that map to r;
+//   equation row r, the sorted list of (element, local edge) slots that map to r;
 //   k_row_pattern (count, scan, write) turns those lists into the merged CSR
 //   pattern with ascending columns -- the pattern SparseConverter::to_eigen
 //   produces from the reference's unmerged CSR (sparse_converter.cpp:19-80).
 // Numeric phase:
-//   k_assemble_rows gathers, for each row, the contributions of its incident
-//   tets in ascending tet order and writes the row's values once: no atomics,
+//   k_assemble_rows (tets) / k_assemble_rows_hex gather, for each row, the
+//   contributions of its incident elements in ascending element order and
+//   write the row's values once: no atomics,
 //   deterministic, and every sum is formed in the same order as an element
 //   loop would form it.
 #include <cuda_runtime.h>
@@ -20,6 +21,7 @@
 
 #include "common.cuh"
 #include "device.h"
+#include "internal.h"
 
 namespace emg {
 
@@ -146,11 +148,12 @@ __global__ void k_sort_incidence(const int32_t* __restrict__ inc_ptr, int32_t* _
   }
 }
 
-// Warp per row: candidate columns of all incident tets -> distinct, ranked.
+// Warp per row: candidate columns of all incident elements -> distinct,
+// ranked.  epe = edges per element (slot = epe * element + local edge).
 // write == false: counts[r] = number of distinct columns.
 // write == true : col[row_ptr[r] + rank] = column.
 template <bool kWrite>
-__global__ void __launch_bounds__(128) k_row_pattern(int64_t n, const int32_t* __restrict__ inc_ptr,
+__global__ void __launch_bounds__(128) k_row_pattern(int64_t n, int epe, const int32_t* __restrict__ inc_ptr,
                                                      const int32_t* __restrict__ inc,
                                                      const int32_t* __restrict__ l2g,
                                                      int32_t* __restrict__ counts,
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(128) k_row_pattern(int64_t n, const int32_t* _
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + wib; r < n; r += warps) {
     const int32_t a = inc_ptr[r], b = inc_ptr[r + 1];
-    const int m = 6 * (b - a);
+    const int m = epe * (b - a);
     if (m > kPatternCap) {
       if (lane == 0) {
         atomicOr(err, kErrRowCap);
@@ -174,8 +177,8 @@ __global__ void __launch_bounds__(128) k_row_pattern(int64_t n, const int32_t* _
       continue;
     }
     for (int idx = lane; idx < m; idx += 32) {
-      const int32_t slot = inc[a + idx / 6];
-      cand[idx] = l2g[6 * (slot / 6) + (idx % 6)];
+      const int32_t slot = inc[a + idx / epe];
+      cand[idx] = l2g[epe * (slot / epe) + (idx % epe)];
     }
     __syncwarp();
     for (int idx = lane; idx < m; idx += 32) {  // first occurrence of each valid column
@@ -303,7 +306,7 @@ struct AsmArgs {
   const int32_t* col;
   const int32_t* inc_ptr;
   const int32_t* inc;
-  const int32_t* tets;
+  const int32_t* elems;
   const double* xyz;
   const int32_t* material;
   const int32_t* l2g;
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
       const int32_t mid = A.material ? A.material[t] : 0;
       if (mid < 0 || mid >= A.n_mat) continue;  // em_assembly.cpp:270-276 skips the element
       Tet T;
-      if (!load_tet(A.tets, A.xyz, A.n_nodes, t, T)) { atomicOr(A.err, kErrNode); continue; }
+      if (!load_tet(A.elems, A.xyz, A.n_nodes, t, T)) { atomicOr(A.err, kErrNode); continue; }
       const double adet = fabs(T.det);
       if (adet < 1e-15) continue;  // every quadrature point skipped (:169)
       int sg[6];
@@ -429,6 +432,210 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
   }
 }
 
+// ----------------------------------------------------------- HEX8_EDGE ----
+// Reference hexahedron [-1,1]^3, nodes 0-3 on zeta = -1 (counter-clockwise
+// from (-1,-1)), 4-7 above them (nedelec_element.cpp:506-517).  Edge k runs
+// from local node A to B (ElementGeometry's table, element_geometry.cpp:165-171)
+// along reference axis d; with (p, q) = (d+1, d+2) mod 3 and c_p, c_q the
+// edge's fixed coordinates, its basis (evalHex8Edge, nedelec_element.cpp:519-615) is
+//   W_k = 1/2 s_k (1 + c_p x_p)(1 + c_q x_q) e_d,   s_k = (x_d(B) - x_d(A)) / 2,
+// with curl
+//   curl W_k = 1/2 s_k [c_q (1 + c_p x_p) e_p - c_p (1 + c_q x_q) e_q].
+// (curlHex8Edge, :618-720, has sign / component errors in edges 2, 3, 6, 7;
+// the curl here is the derivative of the reference's own W_k.)  The tables
+// are closed forms, so with k unrolled they fold to compile-time constants.
+__host__ __device__ constexpr int hex_node_coord(int a, int axis) {  // reference coordinate of node a
+  return axis == 0 ? (((a & 3) == 1 || (a & 3) == 2) ? 1 : -1) : axis == 1 ? ((a & 2) ? 1 : -1) : ((a & 4) ? 1 : -1);
+}
+__host__ __device__ constexpr int hex_edge_a(int k) { return k < 8 ? k : k - 8; }
+__host__ __device__ constexpr int hex_edge_b(int k) { return k < 4 ? ((k + 1) & 3) : k < 8 ? 4 + ((k + 1) & 3) : k - 4; }
+__host__ __device__ constexpr int hex_dir(int k) { return k < 8 ? (k & 1) : 2; }
+__host__ __device__ constexpr int hex_sgn(int k) {
+  return (hex_node_coord(hex_edge_b(k), hex_dir(k)) - hex_node_coord(hex_edge_a(k), hex_dir(k))) / 2;
+}
+__host__ __device__ constexpr int hex_cp(int k) { return hex_node_coord(hex_edge_a(k), (hex_dir(k) + 1) % 3); }
+__host__ __device__ constexpr int hex_cq(int k) { return hex_node_coord(hex_edge_a(k), (hex_dir(k) + 2) % 3); }
+static_assert(hex_edge_a(2) == 2 && hex_edge_b(2) == 3 && hex_edge_b(3) == 0 && hex_edge_b(7) == 4 &&
+                  hex_edge_b(11) == 7,
+              "edge table of element_geometry.cpp:165-171");
+static_assert(hex_sgn(2) == -1 && hex_sgn(3) == -1 && hex_sgn(6) == -1 && hex_sgn(7) == -1 && hex_sgn(8) == 1,
+              "basis orientation of nedelec_element.cpp:519-615");
+static_assert(hex_cp(0) == -1 && hex_cq(0) == -1 && hex_cp(1) == -1 && hex_cq(1) == 1 && hex_cp(9) == 1 &&
+                  hex_cq(9) == -1,
+              "edge positions");
+
+// Thread per row, 2x2x2 Gauss-Legendre (points +-1/sqrt 3, weights 1):
+//   K(r, c) = sum_q nu / |det J| (curl_ref_i)^T (J^T J) (curl_ref_j)
+//   M(r, c) = sum_q sigma |det J| f_i f_j [(J^T J)^-1]_{d_i d_j}
+//   F(r)    = sum_q |det J| f_i [J^-1 J_s(x_q)]_{d_i}
+// (curl_phys = J curl_ref / det J, W_phys = J^-T W_ref; EMG_FLAG_PIOLA_LITERAL
+// divides W_phys by det J once more), incident elements in ascending order.
+template <bool kMass>
+__global__ void __launch_bounds__(128) k_assemble_rows_hex(AsmArgs A) {
+  const double g = 0.57735026918962576450914878050195746;  // 1 / sqrt 3
+  const bool want_mass = kMass && A.mval != nullptr;
+  const bool signs = (A.flags & EMG_FLAG_NO_EDGE_SIGNS) == 0;
+  const bool literal = (A.flags & EMG_FLAG_PIOLA_LITERAL) != 0;
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < A.n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s0 = A.row_ptr[r], s1 = A.row_ptr[r + 1];
+    for (int32_t k = s0; k < s1; ++k) {
+      A.kval[k] = 0.0;
+      if (want_mass) A.mval[k] = 0.0;
+    }
+    double f = 0.0;
+    for (int32_t u = A.inc_ptr[r]; u < A.inc_ptr[r + 1]; ++u) {
+      const int32_t slot = A.inc[u];
+      const int64_t t = slot / 12;
+      const int i = slot - 12 * static_cast<int>(t);
+      const int32_t mid = A.material ? A.material[t] : 0;
+      if (mid < 0 || mid >= A.n_mat) continue;  // em_assembly.cpp:270-276 skips the element
+      const int4 n0 = reinterpret_cast<const int4*>(A.elems)[2 * t];
+      const int4 n1 = reinterpret_cast<const int4*>(A.elems)[2 * t + 1];
+      const int32_t node[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};
+      double x[8][3];
+      bool ok = true;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int32_t gn = node[a];
+        if (gn < 0 || gn >= A.n_nodes) { ok = false; break; }
+        x[a][0] = A.xyz[3 * gn]; x[a][1] = A.xyz[3 * gn + 1]; x[a][2] = A.xyz[3 * gn + 2];
+      }
+      if (!ok) { atomicOr(A.err, kErrNode); continue; }
+      int sgi = 1;
+#pragma unroll
+      for (int k = 0; k < 12; ++k)
+        if (k == i && signs) sgi = node[hex_edge_a(k)] < node[hex_edge_b(k)] ? 1 : -1;
+      const double nu = A.nu[mid];
+      const double sig = A.sigma ? A.sigma[mid] : 0.0;
+      const bool do_mass = want_mass && sig > 0.0;
+      const emg_source* tab = c_src;
+      int src_first = 0, src_count = A.n_src;
+      if (A.src_map) {
+        tab = A.src_tab;
+        const int32_t sid = A.src_map[t];
+        src_first = sid;
+        src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
+      }
+      const bool do_src = src_count > 0;
+      int32_t pos[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        const int32_t c = A.l2g[12 * t + j];
+        pos[j] = c >= 0 ? find_slot(A.col, s0, s1, c) : -1;
+        if (c >= 0 && (pos[j] >= s1 || A.col[pos[j]] != c)) {
+          atomicOr(A.err, kErrSlot);
+          pos[j] = -1;
+        }
+      }
+      double krow[12], mrow[kMass ? 12 : 1];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) krow[j] = 0.0;
+#pragma unroll
+      for (int j = 0; j < (kMass ? 12 : 1); ++j) mrow[j] = 0.0;
+      double fi = 0.0;
+      const int di = hex_dir(i);
+      for (int q = 0; q < 8; ++q) {
+        const double xi[3] = {(q & 1) ? g : -g, (q & 2) ? g : -g, (q & 4) ? g : -g};
+        // J[r][c] = dx_r / dxi_c of the trilinear map
+        double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          const double s0 = hex_node_coord(a, 0), s1 = hex_node_coord(a, 1), s2 = hex_node_coord(a, 2);
+          const double l0 = 1.0 + s0 * xi[0], l1 = 1.0 + s1 * xi[1], l2 = 1.0 + s2 * xi[2];
+          const double dn[3] = {0.125 * s0 * l1 * l2, 0.125 * s1 * l0 * l2, 0.125 * s2 * l0 * l1};
+#pragma unroll
+          for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) J[rr][cc] += x[a][rr] * dn[cc];
+        }
+        // adjugate rows: inv(J) = adj / det
+        double adj[3][3];
+        adj[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        adj[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+        adj[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+        adj[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        adj[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+        adj[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+        adj[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        adj[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+        adj[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        const double det = J[0][0] * adj[0][0] + J[0][1] * adj[1][0] + J[0][2] * adj[2][0];
+        // row d_i of adj (J^-1 = adj / det)
+        const double ad[3] = {di == 0 ? adj[0][0] : di == 1 ? adj[1][0] : adj[2][0],
+                              di == 0 ? adj[0][1] : di == 1 ? adj[1][1] : adj[2][1],
+                              di == 0 ? adj[0][2] : di == 1 ? adj[1][2] : adj[2][2]};
+        const double adet = fabs(det);
+        if (adet < 1e-15) continue;  // quadrature point skipped (magnetic_vector_3d_integrator.cpp:169)
+        // Physical curls (without the 1/det) u_k = J curl_ref_k and the
+        // reference basis magnitudes f_k for all 12 edges, the row's own
+        // picked out of the same arrays: every product below is formed from
+        // the same values in row i and row j, so K and M come out exactly
+        // symmetric whatever the contraction into FMAs.
+        double u[12][3], fk[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+          const int dk = hex_dir(k), pk = (dk + 1) % 3, qk = (dk + 2) % 3;
+          const double hk = 0.5 * hex_sgn(k);
+          const double lp = 1.0 + hex_cp(k) * xi[pk], lq = 1.0 + hex_cq(k) * xi[qk];
+          const double cp = hk * hex_cq(k) * lp, cq = -hk * hex_cp(k) * lq;
+#pragma unroll
+          for (int rr = 0; rr < 3; ++rr) u[k][rr] = J[rr][pk] * cp + J[rr][qk] * cq;
+          fk[k] = hk * lp * lq;  // W_ref_k = f_k e_{d_k}
+        }
+        double ui[3] = {0, 0, 0}, fi_q = 0.0;
+#pragma unroll
+        for (int k = 0; k < 12; ++k)
+          if (k == i) { ui[0] = u[k][0]; ui[1] = u[k][1]; ui[2] = u[k][2]; fi_q = fk[k]; }
+        const double kq = nu / adet;
+#pragma unroll
+        for (int j = 0; j < 12; ++j) krow[j] += kq * (ui[0] * u[j][0] + ui[1] * u[j][1] + ui[2] * u[j][2]);
+        if (do_mass || do_src) {
+          const double wscale = literal ? 1.0 / det : 1.0;
+          if (kMass && do_mass) {
+            // W_i . W_j = f_i f_j [adj adj^T]_{d_i d_j} / det^2, the 3x3 Gram
+            // matrix of the adjugate rows formed symmetrically
+            double H[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int b = 0; b < 3; ++b) H[a][b] = adj[a][0] * adj[b][0] + adj[a][1] * adj[b][1] + adj[a][2] * adj[b][2];
+            const double Hi[3] = {di == 0 ? H[0][0] : di == 1 ? H[1][0] : H[2][0],
+                                  di == 0 ? H[0][1] : di == 1 ? H[1][1] : H[2][1],
+                                  di == 0 ? H[0][2] : di == 1 ? H[1][2] : H[2][2]};
+            const double mq = sig * adet * wscale * wscale / (det * det);
+#pragma unroll
+            for (int j = 0; j < (kMass ? 12 : 1); ++j) mrow[j] += (mq * (fi_q * fk[j])) * Hi[hex_dir(j)];
+          }
+          if (do_src) {
+            double xq[3] = {0, 0, 0};
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+              const double na = 0.125 * (1.0 + hex_node_coord(a, 0) * xi[0]) * (1.0 + hex_node_coord(a, 1) * xi[1]) *
+                                (1.0 + hex_node_coord(a, 2) * xi[2]);
+#pragma unroll
+              for (int c = 0; c < 3; ++c) xq[c] += na * x[a][c];
+            }
+            double js[3];
+            source_at(xq, tab, src_first, src_count, js);
+            const double ji = (ad[0] * js[0] + ad[1] * js[1] + ad[2] * js[2]) / det;
+            fi += adet * wscale * fi_q * ji;
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        if (pos[j] < 0) continue;
+        const int sgj = signs ? (node[hex_edge_a(j)] < node[hex_edge_b(j)] ? 1 : -1) : 1;
+        A.kval[pos[j]] += static_cast<double>(sgi * sgj) * krow[j];
+        if (kMass && do_mass) A.mval[pos[j]] += static_cast<double>(sgi * sgj) * mrow[kMass ? j : 0];
+      }
+      f += sgi * fi;
+    }
+    A.rhs[r] = f;
+  }
+}
+
 int grid_for(int64_t work, int threads, int max_blocks = 148 * 16) {
   int64_t b = (work + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -465,7 +672,8 @@ int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, 
 }
 
 int system_build(System& s, cudaStream_t st) {
-  const int64_t m = 6 * s.n_tets, n = s.n;
+  const int epe = edges_per_elem(s.elem_type);
+  const int64_t m = epe * s.n_elems, n = s.n;
   int32_t* cnt = nullptr;
   EMG_CK(cudaMallocAsync(&cnt, sizeof(int32_t) * (n + 1), st));
   EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
@@ -484,7 +692,7 @@ int system_build(System& s, cudaStream_t st) {
   EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
   k_fill_incidence<<<grid_for(m, 256), 256, 0, st>>>(s.l2g, m, s.inc_ptr, cnt, s.inc);
   k_sort_incidence<<<grid_for(n, 128), 128, 0, st>>>(s.inc_ptr, s.inc, n);
-  k_row_pattern<false><<<grid_for(n * 32, 128), 128, 0, st>>>(n, s.inc_ptr, s.inc, s.l2g, cnt,
+  k_row_pattern<false><<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, cnt,
                                                              nullptr, nullptr, s.err);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaMallocAsync(&s.K.row_ptr, sizeof(int32_t) * (n + 1), st));
@@ -499,7 +707,7 @@ int system_build(System& s, cudaStream_t st) {
   s.K.nnz = nnz;
   EMG_CK(cudaMallocAsync(&s.K.col, sizeof(int32_t) * (nnz > 0 ? nnz : 1), st));
   EMG_CK(cudaMallocAsync(&s.K.val, sizeof(double) * (nnz > 0 ? nnz : 1), st));
-  k_row_pattern<true><<<grid_for(n * 32, 128), 128, 0, st>>>(n, s.inc_ptr, s.inc, s.l2g, nullptr,
+  k_row_pattern<true><<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, nullptr,
                                                             s.K.row_ptr, s.K.col, s.err);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaMallocAsync(&s.rhs, sizeof(double) * (n > 0 ? n : 1), st));
@@ -549,11 +757,16 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
   AsmArgs a;
   a.n = s.n; a.n_nodes = s.n_nodes;
   a.row_ptr = s.K.row_ptr; a.col = s.K.col; a.inc_ptr = s.inc_ptr; a.inc = s.inc;
-  a.tets = s.tets; a.xyz = s.xyz; a.material = s.material; a.l2g = s.l2g;
+  a.elems = s.elems; a.xyz = s.xyz; a.material = s.material; a.l2g = s.l2g;
   a.nu = mat; a.sigma = mat + n_mat; a.n_mat = n_mat; a.n_src = n_src; a.flags = flags;
   a.src_tab = src_tab; a.src_map = s.src_map;
   a.kval = s.K.val; a.mval = mass ? s.M.val : nullptr; a.rhs = s.rhs; a.err = s.err;
-  k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
+  if (s.elem_type == EMG_ELEM_HEX8_EDGE && mass)
+    k_assemble_rows_hex<true><<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
+  else if (s.elem_type == EMG_ELEM_HEX8_EDGE)
+    k_assemble_rows_hex<false><<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
+  else
+    k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
   EMG_CK(cudaGetLastError());
   ++s.K.version;
   if (mass) ++s.M.version;
@@ -569,7 +782,7 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
 // Buffers of a System come from the stream-ordered pool (cudaMallocAsync);
 // the owner synchronizes the device before destruction.
 System::~System() {
-  for (void* p : {static_cast<void*>(xyz), static_cast<void*>(tets), static_cast<void*>(material),
+  for (void* p : {static_cast<void*>(xyz), static_cast<void*>(elems), static_cast<void*>(material),
                   static_cast<void*>(l2g), static_cast<void*>(inc_ptr), static_cast<void*>(inc),
                   static_cast<void*>(err), static_cast<void*>(rhs), static_cast<void*>(src_map)})
     if (p) cudaFreeAsync(p, 0);

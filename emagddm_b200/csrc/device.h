@@ -45,16 +45,17 @@ struct DevCsr {
 
 // Assembled system on the device (EMAssembly state).
 struct System {
-  int64_t n_nodes = 0, n_tets = 0, n = 0;
+  int32_t elem_type = EMG_ELEM_TET4_EDGE;
+  int64_t n_nodes = 0, n_elems = 0, n = 0;
   double* xyz = nullptr;       // 3 * n_nodes
-  int32_t* tets = nullptr;     // 4 * n_tets
-  int32_t* material = nullptr; // n_tets
-  int32_t* l2g = nullptr;      // 6 * n_tets
-  int32_t* inc_ptr = nullptr;  // n + 1: incidence of every row (tet-edge slots)
-  int32_t* inc = nullptr;      // sorted slots 6 * t + k per row
+  int32_t* elems = nullptr;    // nodes_per_elem * n_elems
+  int32_t* material = nullptr; // n_elems
+  int32_t* l2g = nullptr;      // edges_per_elem * n_elems
+  int32_t* inc_ptr = nullptr;  // n + 1: incidence of every row (element-edge slots)
+  int32_t* inc = nullptr;      // sorted slots edges_per_elem * t + k per row
   int32_t* err = nullptr;      // device error word
   double* rhs = nullptr;       // n
-  int32_t* src_map = nullptr;  // optional per-tet source index (n_tets)
+  int32_t* src_map = nullptr;  // optional per-element source index (n_elems)
   DevCsr K, M;                 // M shares K's pattern
   bool has_mass = false;
   ~System();

@@ -1169,12 +1169,13 @@ int FetiDP::create(const Mesh& m, const DofMap& d, cudaStream_t stream) {
     int rc = build_feti_plan(m, d, plan);
     if (rc) return rc;
   }
-  // union system: every tet once, its DOFs in its own subdomain's block
+  // union system: every element once, its DOFs in its own subdomain's block
+  un.elem_type = m.elem_type;
   un.n_nodes = m.n_nodes;
-  un.n_tets = m.n_tets;
+  un.n_elems = m.n_elems;
   un.n = plan.n_union;
   std::vector<int32_t> mat = m.material;
-  if (mat.empty()) mat.assign(m.n_tets, 0);
+  if (mat.empty()) mat.assign(m.n_elems, 0);
   int rc = EMG_SUCCESS;
   auto upload = [&](auto** dst, const auto& v) -> int {
     using T = typename std::remove_reference<decltype(v)>::type::value_type;
@@ -1182,7 +1183,7 @@ int FetiDP::create(const Mesh& m, const DofMap& d, cudaStream_t stream) {
     EMG_CK(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
     return EMG_SUCCESS;
   };
-  if ((rc = upload(&un.xyz, m.xyz)) || (rc = upload(&un.tets, m.tets)) || (rc = upload(&un.material, mat)) ||
+  if ((rc = upload(&un.xyz, m.xyz)) || (rc = upload(&un.elems, m.elems)) || (rc = upload(&un.material, mat)) ||
       (rc = upload(&un.l2g, plan.l2g_union)))
     return rc;
   EMG_CK(cudaMallocAsync(&un.err, sizeof(int32_t), st));

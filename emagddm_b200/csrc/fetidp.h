@@ -37,7 +37,7 @@ struct FetiPlan {
   int64_t n_dofs = 0, n_union = 0;
   std::vector<int64_t> loc_off;           // n_parts + 1
   std::vector<int32_t> nI, nD, nP;        // per subdomain
-  std::vector<int32_t> l2g_union;         // 6 * n_tets
+  std::vector<int32_t> l2g_union;         // edges_per_elem * n_elems
   std::vector<int32_t> union_gdof;        // n_union
   std::vector<int64_t> gptr;              // n_dofs + 1
   std::vector<int32_t> glist;             // union positions of each global DOF

@@ -197,13 +197,14 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
     set_error("FETI-DP needs a DOF map from emg_dof_build_partitioned");
     return EMG_INVALID_INPUT;
   }
-  if (!m.edges_built || d.n_tets != m.n_tets || d.n_edges != m.n_edges) {
+  if (!m.edges_built || d.n_elems != m.n_elems || d.elem_type != m.elem_type || d.n_edges != m.n_edges) {
     set_error("FETI-DP: DOF map does not belong to this mesh");
     return EMG_INVALID_INPUT;
   }
   p = FetiPlan{};
   const int32_t S = d.n_parts;
-  const int64_t T = m.n_tets, N = d.n_dofs;
+  const int64_t T = m.n_elems, N = d.n_dofs;
+  const int epe = m.epe();
   p.n_parts = S;
   p.n_dofs = N;
   // subdomains touching every DOF
@@ -211,8 +212,8 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
   std::vector<uint8_t> many(N, 0);
   for (int64_t t = 0; t < T; ++t) {
     const int32_t s = d.tet_part[t];
-    for (int k = 0; k < 6; ++k) {
-      const int32_t g = d.l2g[6 * t + k];
+    for (int k = 0; k < epe; ++k) {
+      const int32_t g = d.l2g[epe * t + k];
       if (g < 0) continue;
       if (q1[g] < 0) q1[g] = s;
       else if (q1[g] != s) {
@@ -255,7 +256,7 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
   p.nI.assign(S, 0);
   p.nD.assign(S, 0);
   p.nP.assign(S, 0);
-  p.l2g_union.assign(6 * T, -1);
+  p.l2g_union.assign(epe * T, -1);
   p.root_front.assign(S, -1);
 
   std::vector<int32_t> stamp(N, -1);
@@ -266,8 +267,8 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
     std::vector<int32_t> I, D, P;
     for (int64_t q = tptr[s]; q < tptr[s + 1]; ++q) {
       const int64_t t = tlist[q];
-      for (int k = 0; k < 6; ++k) {
-        const int32_t g = d.l2g[6 * t + k];
+      for (int k = 0; k < epe; ++k) {
+        const int32_t g = d.l2g[epe * t + k];
         if (g < 0 || stamp[g] == -2) continue;
         stamp[g] = -2;
         (d.dof_primal[g] ? P : (q2[g] >= 0 ? D : I)).push_back(g);
@@ -287,16 +288,16 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
     // adjacency over r DOFs through the subdomain's tets
     w.aptr.assign(static_cast<size_t>(nr) + 1, 0);
     std::vector<std::pair<int32_t, int32_t>> pairs;
-    pairs.reserve(static_cast<size_t>(tptr[s + 1] - tptr[s]) * 30);
+    pairs.reserve(static_cast<size_t>(tptr[s + 1] - tptr[s]) * epe * (epe - 1));
     for (int64_t q = tptr[s]; q < tptr[s + 1]; ++q) {
       const int64_t t = tlist[q];
-      int32_t loc[6];
-      for (int k = 0; k < 6; ++k) {
-        const int32_t g = d.l2g[6 * t + k];
+      int32_t loc[12];
+      for (int k = 0; k < epe; ++k) {
+        const int32_t g = d.l2g[epe * t + k];
         loc[k] = (g >= 0 && stamp[g] < nr) ? stamp[g] : -1;
       }
-      for (int a = 0; a < 6; ++a)
-        for (int b = 0; b < 6; ++b)
+      for (int a = 0; a < epe; ++a)
+        for (int b = 0; b < epe; ++b)
           if (a != b && loc[a] >= 0 && loc[b] >= 0 && loc[a] != loc[b]) pairs.emplace_back(loc[a], loc[b]);
     }
     std::sort(pairs.begin(), pairs.end());
@@ -355,9 +356,9 @@ int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p) {
     for (size_t i = 0; i < pg.size(); ++i) stamp[pg[i]] = static_cast<int32_t>(i);  // global -> position
     for (int64_t q = tptr[s]; q < tptr[s + 1]; ++q) {
       const int64_t t = tlist[q];
-      for (int k = 0; k < 6; ++k) {
-        const int32_t g = d.l2g[6 * t + k];
-        if (g >= 0) p.l2g_union[6 * t + k] = static_cast<int32_t>(p.loc_off[s] + stamp[g]);
+      for (int k = 0; k < epe; ++k) {
+        const int32_t g = d.l2g[epe * t + k];
+        if (g >= 0) p.l2g_union[epe * t + k] = static_cast<int32_t>(p.loc_off[s] + stamp[g]);
       }
     }
     for (size_t i = 0; i < pg.size(); ++i) stamp[pg[i]] = -1;

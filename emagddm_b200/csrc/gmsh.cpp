@@ -221,15 +221,15 @@ int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_
     out = it->second;
     return true;
   };
-  m.n_tets = static_cast<int64_t>(r.tet_phys.size());
-  m.tets.resize(4 * m.n_tets);
+  m.n_elems = static_cast<int64_t>(r.tet_phys.size());
+  m.elems.resize(4 * m.n_elems);
   for (size_t i = 0; i < r.tet_nodes.size(); ++i)
-    if (!idx(r.tet_nodes[i], m.tets[i])) return fail("element references an unknown node");
+    if (!idx(r.tet_nodes[i], m.elems[i])) return fail("element references an unknown node");
   material_tags = r.tet_phys;
   std::sort(material_tags.begin(), material_tags.end());
   material_tags.erase(std::unique(material_tags.begin(), material_tags.end()), material_tags.end());
-  m.material.resize(m.n_tets);
-  for (int64_t t = 0; t < m.n_tets; ++t)
+  m.material.resize(m.n_elems);
+  for (int64_t t = 0; t < m.n_elems; ++t)
     m.material[t] = static_cast<int32_t>(std::lower_bound(material_tags.begin(), material_tags.end(), r.tet_phys[t]) -
                                          material_tags.begin());
   // Dirichlet node pairs
@@ -253,11 +253,11 @@ int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_
   } else {
     // faces of exactly one tetrahedron
     std::vector<std::pair<std::array<int32_t, 3>, int64_t>> faces;
-    faces.reserve(4 * m.n_tets);
+    faces.reserve(4 * m.n_elems);
     const int tf[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
-    for (int64_t t = 0; t < m.n_tets; ++t)
+    for (int64_t t = 0; t < m.n_elems; ++t)
       for (auto& f : tf) {
-        std::array<int32_t, 3> k = {m.tets[4 * t + f[0]], m.tets[4 * t + f[1]], m.tets[4 * t + f[2]]};
+        std::array<int32_t, 3> k = {m.elems[4 * t + f[0]], m.elems[4 * t + f[1]], m.elems[4 * t + f[2]]};
         std::sort(k.begin(), k.end());
         faces.push_back({k, t});
       }

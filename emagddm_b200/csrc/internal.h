@@ -12,32 +12,47 @@ namespace emg {
 // Thread-local error message behind emg_last_error().
 void set_error(const std::string& msg);
 
+// Local node pairs of the element edges, ElementGeometry::get_local_edges
+// (src/fe_em/element_geometry.cpp:115-126 TET4, :161-181 HEX8).
+constexpr int kTetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+constexpr int kHexEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                 {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+
+inline bool valid_elem_type(int32_t t) { return t == EMG_ELEM_TET4_EDGE || t == EMG_ELEM_HEX8_EDGE; }
+inline int nodes_per_elem(int32_t t) { return t == EMG_ELEM_HEX8_EDGE ? 8 : 4; }
+inline int edges_per_elem(int32_t t) { return t == EMG_ELEM_HEX8_EDGE ? 12 : 6; }
+inline const int (*local_edges(int32_t t))[2] { return t == EMG_ELEM_HEX8_EDGE ? kHexEdge : kTetEdge; }
+
 struct Mesh {
+  int32_t elem_type = EMG_ELEM_TET4_EDGE;
   int64_t n_nodes = 0;
-  int64_t n_tets = 0;
+  int64_t n_elems = 0;
   std::vector<double> xyz;        // 3 * n_nodes
-  std::vector<int32_t> tets;      // 4 * n_tets
-  std::vector<int32_t> material;  // n_tets
+  std::vector<int32_t> elems;     // npe() * n_elems
+  std::vector<int32_t> material;  // n_elems
   std::vector<int32_t> dirichlet; // 2 * n_dirichlet
   int32_t n_hole_markers = 0;
   // lazily built edge table
   bool edges_built = false;
   int64_t n_edges = 0;
-  std::vector<int32_t> elem_edge;   // 6 * n_tets
+  std::vector<int32_t> elem_edge;   // epe() * n_elems
   std::vector<int32_t> edge_nodes;  // 2 * n_edges, (lo, hi) global node IDs
+  int npe() const { return nodes_per_elem(elem_type); }
+  int epe() const { return edges_per_elem(elem_type); }
 };
 
 struct DofMap {
-  int64_t n_tets = 0;
+  int32_t elem_type = EMG_ELEM_TET4_EDGE;
+  int64_t n_elems = 0;
   int64_t n_edges = 0;
   int64_t n_free = 0;
   int64_t n_dofs = 0;
   int32_t root = -1;
-  std::vector<int32_t> l2g;       // 6 * n_tets
+  std::vector<int32_t> l2g;       // edges_per_elem * n_elems
   std::vector<int32_t> edge_dof;  // n_edges
   // Set by the partitioned gauge only.
   int32_t n_parts = 0;
-  std::vector<int32_t> tet_part;    // n_tets, subdomain of every tet
+  std::vector<int32_t> tet_part;    // n_elems, subdomain of every element
   std::vector<uint8_t> dof_primal;  // n_dofs, 1 = primal (coarse) DOF
   int64_t n_primal_fix = 0;         // primal DOFs added to connect a subdomain
 };

@@ -18,9 +18,6 @@
 namespace emg {
 namespace {
 
-// TET4 local edges, ElementGeometry::get_local_edges(TET4) (element_geometry.cpp:115-126).
-constexpr int kGeoEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
-
 // Compressed adjacency: for every bucket a contiguous run of entries.
 struct Buckets {
   std::vector<int64_t> ptr;
@@ -37,12 +34,14 @@ struct Buckets {
 // which the reference's hash map assigns new IDs.
 int build_edge_ids(Mesh& m) {
   if (m.edges_built) return EMG_SUCCESS;
-  const int64_t T = m.n_tets, V = m.n_nodes, M = 6 * T;
+  const int npe = m.npe(), epe = m.epe();
+  const int (*le)[2] = local_edges(m.elem_type);
+  const int64_t T = m.n_elems, V = m.n_nodes, M = epe * T;
   Buckets bk;
   bk.ptr.assign(V + 1, 0);
   for (int64_t t = 0; t < T; ++t)
-    for (int k = 0; k < 6; ++k) {
-      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+    for (int k = 0; k < epe; ++k) {
+      int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       bk.ptr[std::min(u, w) + 1]++;
     }
   for (int64_t v = 0; v < V; ++v) bk.ptr[v + 1] += bk.ptr[v];
@@ -50,11 +49,11 @@ int build_edge_ids(Mesh& m) {
   bk.b.resize(M);  // position
   std::vector<int64_t> cur(bk.ptr.begin(), bk.ptr.end() - 1);
   for (int64_t t = 0; t < T; ++t)
-    for (int k = 0; k < 6; ++k) {
-      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+    for (int k = 0; k < epe; ++k) {
+      int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       int64_t s = cur[std::min(u, w)]++;
       bk.a[s] = std::max(u, w);
-      bk.b[s] = static_cast<int32_t>(6 * t + k);
+      bk.b[s] = static_cast<int32_t>(epe * t + k);
     }
   // leader position of every entry
   std::vector<int32_t> leader(M);
@@ -78,9 +77,9 @@ int build_edge_ids(Mesh& m) {
     int32_t id = id_at[leader[p]];
     m.elem_edge[p] = id;
     if (is_leader[p]) {
-      int64_t t = p / 6;
-      int k = static_cast<int>(p % 6);
-      int32_t u = m.tets[4 * t + kGeoEdge[k][0]], w = m.tets[4 * t + kGeoEdge[k][1]];
+      int64_t t = p / epe;
+      int k = static_cast<int>(p % epe);
+      int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       m.edge_nodes[2 * id] = std::min(u, w);
       m.edge_nodes[2 * id + 1] = std::max(u, w);
     }
@@ -104,7 +103,7 @@ struct EdgeGraph {
 EdgeGraph make_graph(const Mesh& m) {
   EdgeGraph g;
   g.compact.assign(m.n_nodes, -1);
-  for (int32_t v : m.tets) g.compact[v] = 0;
+  for (int32_t v : m.elems) g.compact[v] = 0;
   int32_t c = 0;
   for (int64_t v = 0; v < m.n_nodes; ++v)
     if (g.compact[v] == 0) g.compact[v] = c++;
@@ -267,9 +266,10 @@ void mark_constrained(const Mesh& m, std::vector<uint8_t>& constrained) {
 int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
   int rc = build_edge_ids(m);
   if (rc) return rc;
-  const int64_t E = m.n_edges, T = m.n_tets;
+  const int64_t E = m.n_edges, T = m.n_elems;
   out = DofMap{};
-  out.n_tets = T;
+  out.elem_type = m.elem_type;
+  out.n_elems = T;
   out.n_edges = E;
   std::vector<uint8_t> constrained;
   mark_constrained(m, constrained);
@@ -316,12 +316,12 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
     set_error("unknown gauge mode");
     return EMG_INVALID_INPUT;
   }
-  out.l2g.resize(6 * T);
-  for (int64_t p = 0; p < 6 * T; ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  out.l2g.resize(m.elem_edge.size());
+  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
   return EMG_SUCCESS;
 }
 
-// Tree-cotree gauge for a non-overlapping partition of the tets (no
+// Tree-cotree gauge for a non-overlapping partition of the elements (no
 // counterpart in the reference, whose FETI-DP context is a stub:
 // include/fetidp/fetidp_context.hpp:20-66).  Edges are ranked by class:
 //   0 Dirichlet, 1 wire basket (shared by >= 3 subdomains),
@@ -339,7 +339,7 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
 // gradient field vanishing on a connected edge set is zero.  Reduced DOFs
 // are the unconstrained cotree edges in ascending edge ID.
 int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, DofMap& out) {
-  if (n_parts < 1 || (m.n_tets > 0 && tet_part == nullptr)) {
+  if (n_parts < 1 || (m.n_elems > 0 && tet_part == nullptr)) {
     set_error("partitioned gauge: need n_parts >= 1 and a tet_part array");
     return EMG_INVALID_INPUT;
   }
@@ -347,7 +347,7 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
     set_error("partitioned gauge: hole markers (circulation DOFs) are not supported");
     return EMG_INVALID_INPUT;
   }
-  const int64_t T = m.n_tets;
+  const int64_t T = m.n_elems;
   for (int64_t t = 0; t < T; ++t)
     if (tet_part[t] < 0 || tet_part[t] >= n_parts) {
       set_error("partitioned gauge: tet_part[" + std::to_string(t) + "] outside [0, n_parts)");
@@ -356,8 +356,10 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
   int rc = build_edge_ids(m);
   if (rc) return rc;
   const int64_t E = m.n_edges;
+  const int npe = m.npe(), epe = m.epe();
   out = DofMap{};
-  out.n_tets = T;
+  out.elem_type = m.elem_type;
+  out.n_elems = T;
   out.n_edges = E;
   out.n_parts = n_parts;
   out.tet_part.assign(tet_part, tet_part + T);
@@ -368,8 +370,8 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
   std::vector<uint8_t> many(E, 0);
   for (int64_t t = 0; t < T; ++t) {
     const int32_t p = tet_part[t];
-    for (int k = 0; k < 6; ++k) {
-      const int32_t e = m.elem_edge[6 * t + k];
+    for (int k = 0; k < epe; ++k) {
+      const int32_t e = m.elem_edge[epe * t + k];
       if (p1[e] < 0) p1[e] = p;
       else if (p1[e] != p) {
         if (p2[e] < 0) p2[e] = p;
@@ -439,11 +441,11 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
     edges.clear();
     for (int64_t q = tptr[p]; q < tptr[p + 1]; ++q) {
       const int64_t t = tlist[q];
-      for (int a = 0; a < 4; ++a) {
-        const int32_t v = m.tets[4 * t + a];
+      for (int a = 0; a < npe; ++a) {
+        const int32_t v = m.elems[npe * t + a];
         if (node_loc[v] < 0) { node_loc[v] = static_cast<int32_t>(nodes.size()); nodes.push_back(v); }
       }
-      for (int k = 0; k < 6; ++k) edges.push_back(m.elem_edge[6 * t + k]);
+      for (int k = 0; k < epe; ++k) edges.push_back(m.elem_edge[epe * t + k]);
     }
     std::sort(edges.begin(), edges.end());
     edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
@@ -475,8 +477,8 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
     }
   out.n_dofs = nr;
   out.n_primal_fix = fixes;
-  out.l2g.resize(6 * T);
-  for (int64_t p = 0; p < 6 * T; ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  out.l2g.resize(m.elem_edge.size());
+  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
   return EMG_SUCCESS;
 }
 

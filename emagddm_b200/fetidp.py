@@ -1,4 +1,4 @@
-"""FETI-DP solve of the gauged TET4_EDGE curl-curl system on one GPU.
+"""FETI-DP solve of the gauged TET4_EDGE / HEX8_EDGE curl-curl system on one GPU.
 
 The reference declares FETI-DP (``include/fetidp/fetidp_context.hpp:20-66``,
 ``src/fetidp/fetidp_context.cpp:15-45``: a subdomain count and zeroed
@@ -20,7 +20,7 @@ from ._abi import check, lib, ptr
 @dataclass
 class PartitionedMap:
     """Result of the partitioned tree-cotree gauge."""
-    l2g: np.ndarray          # (T, 6) int32, -1 = Dirichlet or tree edge
+    l2g: np.ndarray          # (T, 6 or 12) int32, -1 = Dirichlet or tree edge
     edge_dof: np.ndarray     # (E,) int32
     n_free: int
     n_dofs: int
@@ -36,9 +36,10 @@ class _MeshHandle:
         self.material = np.ascontiguousarray(m.material, np.int32)
         d = np.ascontiguousarray(m.dirichlet, np.int32)
         self.h = C.c_void_p()
-        check(lib().emg_mesh_create(self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0], ptr(self.tets),
-                                    ptr(self.material), d.shape[0], ptr(d) if d.size else None, 0,
-                                    C.byref(self.h)), "emg_mesh_create")
+        et = 1 if self.tets.shape[1] == 8 else 0
+        check(lib().emg_mesh_create_typed(et, self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0],
+                                          ptr(self.tets), ptr(self.material), d.shape[0], ptr(d) if d.size else None,
+                                          0, C.byref(self.h)), "emg_mesh_create_typed")
 
     def __del__(self, _abi=_abi):
         if getattr(self, "h", None) and _abi._LIB is not None:
@@ -66,7 +67,7 @@ def partitioned_dofmap(m, tet_part, n_parts: int, keep_handles: bool = False):
           "emg_dof_build_partitioned")
     ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
     lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
-    l2g = np.empty((m.n_tets, 6), np.int32)
+    l2g = np.empty((m.n_tets, 12 if m.tets.shape[1] == 8 else 6), np.int32)
     ed = np.empty(ne.value, np.int32)
     lib().emg_dofmap_export(h, ptr(l2g), ptr(ed))
     npart, npri, nfix = C.c_int32(), C.c_int64(), C.c_int64()
@@ -150,13 +151,13 @@ class FetiDP:
 
 def gauged_map(m, gauge: int):
     """DOF map of the mesh under a tree gauge (emg_dof_build); returns the
-    map handle owner, the mesh handle owner and the (T, 6) l2g."""
+    map handle owner, the mesh handle owner and the (T, 6 or 12) l2g."""
     mh = _MeshHandle(m)
     h = C.c_void_p()
     check(lib().emg_dof_build(mh.h, int(gauge), C.byref(h)), "emg_dof_build")
     ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
     lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
-    l2g = np.empty((m.n_tets, 6), np.int32)
+    l2g = np.empty((m.n_tets, 12 if m.tets.shape[1] == 8 else 6), np.int32)
     lib().emg_dofmap_export(h, ptr(l2g), None)
     return _MapHandle(h), mh, l2g, nd.value
 

@@ -1,4 +1,4 @@
-"""Synthetic structured tetrahedral meshes of the unit cube.
+"""Synthetic structured tetrahedral and hexahedral meshes of the unit cube.
 
 The reference solve path consumes an ``fe_em::EMMeshData`` (nodes, TET4_EDGE
 elements with a material id, and a DIRICHLET / VECTOR_EDGE_ONLY boundary
@@ -12,6 +12,10 @@ benchmark use:
   (i+1,j+1,k), (i,j+1,k) and the same at k+1;
 * tets per hex {0,1,2,6}, {0,2,3,6}, {0,3,7,6}, {0,7,4,6}, {0,4,5,6}, {0,5,1,6};
 * Dirichlet edges: every mesh edge lying in a boundary face (n x A = 0).
+
+The ``hex_*`` variants keep the hexes themselves as HEX8_EDGE elements
+(vertex order v0..v7 above, ElementGeometry's HEX8 order); a ``CubeMesh``
+whose ``tets`` array has 8 columns is a hex mesh.
 """
 from __future__ import annotations
 
@@ -25,6 +29,12 @@ KUHN = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6],
                  [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]], dtype=np.int64)
 # TET4 local edges, ElementGeometry::get_local_edges(TET4)
 GEO_EDGES = np.array([[0, 1], [1, 2], [0, 2], [0, 3], [1, 3], [2, 3]], dtype=np.int64)
+# HEX8 local edges, ElementGeometry::get_local_edges(HEX8)
+HEX_EDGES = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6], [6, 7], [7, 4],
+                      [0, 4], [1, 5], [2, 6], [3, 7]], dtype=np.int64)
+# Element types (same values as the C ABI's EMG_ELEM_*).
+ELEM_TET4_EDGE = 0
+ELEM_HEX8_EDGE = 1
 
 # Source region kinds (same values as the C ABI's EMG_SRC_*).
 SRC_BOX = 1
@@ -59,7 +69,12 @@ class CubeMesh:
 
     @property
     def n_tets(self) -> int:
+        """Number of elements (tets, or hexes for a hex mesh)."""
         return int(self.tets.shape[0])
+
+    @property
+    def elem_type(self) -> int:
+        return ELEM_HEX8_EDGE if self.tets.shape[1] == 8 else ELEM_TET4_EDGE
 
 
 def cube_topology(n: int):
@@ -80,9 +95,31 @@ def _cube_topology(n: int):
     off = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
     verts = np.stack([(hi + a) + n1 * ((hj + b) + n1 * (hk + c)) for a, b, c in off], axis=1)
     tets = verts[:, KUHN].reshape(-1, 4).astype(np.int32)
-    # boundary-face edges: unique element edges whose two nodes share a
-    # coordinate plane at 0 or n
-    e = tets[:, GEO_EDGES].reshape(-1, 2).astype(np.int64)
+    return xyz, tets, _boundary_pairs(tets, GEO_EDGES, n)
+
+
+@lru_cache(maxsize=64)
+def _hex_topology(n: int):
+    xyz, tets, dirichlet = _cube_topology(n)
+    n1 = n + 1
+    hk, hj, hi = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()
+    off = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    hexes = np.stack([(hi + a) + n1 * ((hj + b) + n1 * (hk + c)) for a, b, c in off], axis=1).astype(np.int32)
+    return xyz, hexes, _boundary_pairs(hexes, HEX_EDGES, n)
+
+
+def hex_topology(n: int):
+    """Nodes, HEX8 elements and boundary-face edge pairs of the n^3 cube."""
+    xyz, hexes, dirichlet = _hex_topology(n)
+    return xyz.copy(), hexes.copy(), dirichlet.copy()
+
+
+def _boundary_pairs(elems, local_edges, n):
+    """Unique element edges whose two nodes share a coordinate plane at 0 or
+    n (grid indices), as sorted node pairs."""
+    n1 = n + 1
+    e = elems[:, local_edges].reshape(-1, 2).astype(np.int64)
     e.sort(axis=1)
     e = np.unique(e[:, 0] * (n1 ** 3) + e[:, 1])
     a, b = e // (n1 ** 3), e % (n1 ** 3)
@@ -91,8 +128,7 @@ def _cube_topology(n: int):
     on = np.zeros(a.shape, dtype=bool)
     for ca, cb in ((ia, ib), (ja, jb), (ka, kb)):
         on |= (ca == cb) & ((ca == 0) | (ca == n))
-    dirichlet = np.stack([a[on], b[on]], axis=1).astype(np.int32)
-    return xyz, tets, dirichlet
+    return np.stack([a[on], b[on]], axis=1).astype(np.int32)
 
 
 def centroids(xyz: np.ndarray, tets: np.ndarray) -> np.ndarray:
@@ -124,6 +160,26 @@ def plain_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
                     sources=[Source(SRC_ANNULUS_Z, (0.0, 0.0, 1.0),
                                     (0.5, 0.5, 0.3, 0.45, 0.2, 0.8))],
                     name=f"cube{n}_iron_coil")
+
+
+def hex_small(n: int = 16) -> CubeMesh:
+    """plain_small on HEX8_EDGE elements (the n^3 grid cells themselves)."""
+    xyz, hexes, dirichlet = hex_topology(n)
+    m = plain_small(1)
+    return CubeMesh(n=n, xyz=xyz, tets=hexes, material=np.zeros(len(hexes), np.int32),
+                    dirichlet=dirichlet, nu=m.nu, sigma=m.sigma, sources=m.sources, name=f"hex{n}_box")
+
+
+def hex_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
+    """plain_scale on HEX8_EDGE elements: iron block by cell centroid, the
+    same coil source."""
+    xyz, hexes, dirichlet = hex_topology(n)
+    c = centroids(xyz, hexes)
+    iron = ((c[:, 0] > 0.25) & (c[:, 0] < 0.75) & (c[:, 1] > 0.25) & (c[:, 1] < 0.75)
+            & (c[:, 2] > 0.4) & (c[:, 2] < 0.6))
+    m = plain_scale(1, mu_iron)
+    return CubeMesh(n=n, xyz=xyz, tets=hexes, material=iron.astype(np.int32), dirichlet=dirichlet,
+                    nu=m.nu, sigma=m.sigma, sources=m.sources, name=f"hex{n}_iron_coil")
 
 
 def jittered_cuts(n: int, parts: int = 4, seed: int = 20261203, jitter: int | None = None):

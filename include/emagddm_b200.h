@@ -52,6 +52,14 @@ enum {
   EMG_GAUGE_BOUNDARY_FIRST = 1  /* tree spans the Dirichlet boundary first    */
 };
 
+/* ---- element types (numeric::ElementType, include/numeric/shape_function_base.hpp:51-57)
+ * One type per mesh.  Local node and edge order follow ElementGeometry
+ * (src/fe_em/element_geometry.cpp:112-126 TET4, :158-181 HEX8). */
+enum {
+  EMG_ELEM_TET4_EDGE = 0,  /* 4 nodes, 6 edges                                     */
+  EMG_ELEM_HEX8_EDGE = 1   /* 8 nodes (bottom face 0-3, top face 4-7 above them), 12 edges */
+};
+
 /* ---- assembly flags ------------------------------------------------------ */
 enum {
   EMG_FLAG_MASS = 1,           /* also assemble M_ij = int sigma W_i . W_j      */
@@ -102,6 +110,19 @@ const char* emg_last_error(void);
 int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
                     const int32_t* material_id, int64_t n_dirichlet,
                     const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out);
+/* Same for a mesh of one element type (EMG_ELEM_*): elems holds
+ * nodes_per_elem * n_elems node indices (4 for TET4_EDGE, 8 for HEX8_EDGE);
+ * emg_mesh_create is elem_type = EMG_ELEM_TET4_EDGE.  Everything downstream
+ * (edge IDs, DOF maps, gauges, systems, the FETI-DP and direct solvers) then
+ * works per element with edges_per_elem (6 or 12) local edges; arrays
+ * documented below as 4*n_tets / 6*n_tets hold nodes_per_elem*n_elems /
+ * edges_per_elem*n_elems entries for such a mesh. */
+int emg_mesh_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                          const int32_t* elems, const int32_t* material_id, int64_t n_dirichlet,
+                          const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out);
+/* Element type, nodes and edges per element of a mesh; any pointer may be NULL. */
+int emg_mesh_elem_type(emg_mesh mesh, int32_t* elem_type, int32_t* nodes_per_elem,
+                       int32_t* edges_per_elem);
 void emg_mesh_destroy(emg_mesh mesh);
 /* Gmsh ASCII mesh (format 2.2 or 4.1; the reference's planned mesh format,
  * mesh/README.md) as an EMMeshData (include/fe_em/em_mesh_data.hpp:90-230):
@@ -280,6 +301,14 @@ int emg_system_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const 
 int emg_system_create_device(int64_t n_nodes, const double* xyz_d, int64_t n_tets,
                              const int32_t* tets_d, const int32_t* material_d,
                              const int32_t* l2g_d, int64_t n_dofs, void* stream, emg_system* out);
+/* Either of the above for elements of type elem_type (EMG_ELEM_*): elems
+ * nodes_per_elem*n_elems, material n_elems, l2g edges_per_elem*n_elems;
+ * on_device selects device (1) or host (0) arrays.  HEX8_EDGE elements are
+ * integrated with the 2x2x2 Gauss-Legendre rule (GaussQuadrature::getHex8Points,
+ * src/numeric/gauss_quadrature.cpp:232-276) on the trilinear map. */
+int emg_system_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                            const int32_t* elems, const int32_t* material, const int32_t* l2g,
+                            int64_t n_dofs, int32_t on_device, void* stream, emg_system* out);
 /* Numeric assembly: nu (1/mu) and sigma per material; sources; EMG_FLAG_*. */
 int emg_system_assemble(emg_system sys, const double* nu_per_material,
                         const double* sigma_per_material, int32_t n_materials,

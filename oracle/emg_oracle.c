@@ -1,6 +1,6 @@
 /*
- * emg_oracle.c -- CPU oracle (test infrastructure only) for the TET4 Nedelec
- * curl-curl solve path of Poofee/emagddm.  See emg_oracle.h for how each part
+ * emg_oracle.c -- CPU oracle (test infrastructure only) for the TET4 / HEX8
+ * Nedelec curl-curl solve path of Poofee/emagddm.  See emg_oracle.h for how each part
  * is pinned.  Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline
  * and the reference arm) load this file's library.
  *
@@ -43,6 +43,13 @@ int orc_num_threads(void) {
 static const int GEO_EDGE[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
 /* Nedelec TET4_EDGE edge table (src/numeric/nedelec_element.cpp:54-60). */
 static const int NED_EDGE[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+/* HEX8 geometry edge table (element_geometry.cpp:161-181); HEX8_EDGE basis k
+ * runs from node [k][0] to node [k][1] (nedelec_element.cpp:506-517). */
+static const int HEX_EDGE[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                    {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+/* HEX8 reference node coordinates (lagrange_element.cpp:765-772). */
+static const double HEX_NODE[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                      {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
 /* Constant reference curls, curlTet4Edge (nedelec_element.cpp:461-505). */
 static const double CURL_REF[6][3] = {{0, 0, -2}, {-2, 0, 0}, {0, -2, 0},
                                       {0, -2, 2}, {2, 0, -2}, {-2, 2, 0}};
@@ -91,13 +98,27 @@ static int radix_sort_u64(int64_t n, uint64_t* key, int64_t* pay, uint64_t max_k
  * map: a stable sort groups equal keys with the first appearance leading its
  * group, and IDs are the prefix count of group leaders by position.
  * ------------------------------------------------------------------------- */
+static int elem_shape(int32_t elem_type, int* npe, int* epe, const int (**tab)[2]) {
+  if (elem_type == ORC_ELEM_TET4_EDGE) { *npe = 4; *epe = 6; *tab = GEO_EDGE; return 0; }
+  if (elem_type == ORC_ELEM_HEX8_EDGE) { *npe = 8; *epe = 12; *tab = HEX_EDGE; return 0; }
+  return ORC_INVALID_INPUT;
+}
+
 int orc_edge_ids(int64_t n_tets, const int32_t* tets, int32_t* elem_edge,
                  int32_t* edge_nodes, int64_t* n_edges) {
-  int64_t m = 6 * n_tets;
+  return orc_edge_ids_typed(ORC_ELEM_TET4_EDGE, n_tets, tets, elem_edge, edge_nodes, n_edges);
+}
+
+int orc_edge_ids_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, int32_t* elem_edge,
+                       int32_t* edge_nodes, int64_t* n_edges) {
+  int npe, epe;
+  const int (*tab)[2];
   *n_edges = 0;
+  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
+  int64_t m = epe * n_tets;
   if (n_tets <= 0) return 0;
   int32_t maxg = 0;
-  for (int64_t i = 0; i < 4 * n_tets; i++) {
+  for (int64_t i = 0; i < npe * n_tets; i++) {
     if (tets[i] < 0) return ORC_INVALID_INPUT;
     if (tets[i] > maxg) maxg = tets[i];
   }
@@ -107,12 +128,12 @@ int orc_edge_ids(int64_t n_tets, const int32_t* tets, int32_t* elem_edge,
   int64_t* id_at = (int64_t*)malloc((size_t)m * sizeof(int64_t));
   if (!key || !pos || !id_at) { free(key); free(pos); free(id_at); return -1; }
   for (int64_t t = 0; t < n_tets; t++)
-    for (int k = 0; k < 6; k++) {
-      uint64_t a = (uint64_t)tets[4 * t + GEO_EDGE[k][0]];
-      uint64_t b = (uint64_t)tets[4 * t + GEO_EDGE[k][1]];
+    for (int k = 0; k < epe; k++) {
+      uint64_t a = (uint64_t)tets[npe * t + tab[k][0]];
+      uint64_t b = (uint64_t)tets[npe * t + tab[k][1]];
       uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
-      key[6 * t + k] = lo * span + hi;
-      pos[6 * t + k] = 6 * t + k;
+      key[epe * t + k] = lo * span + hi;
+      pos[epe * t + k] = epe * t + k;
     }
   if (radix_sort_u64(m, key, pos, span * span - 1)) { free(key); free(pos); free(id_at); return -1; }
   /* leader flags by position */
@@ -160,13 +181,25 @@ int orc_dof_build(int64_t n_tets, const int32_t* tets, const int32_t* elem_edge,
                   const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge,
                   int32_t* l2g, int32_t* edge_dof, int64_t* n_free,
                   int64_t* n_dofs, int32_t* root_node) {
+  return orc_dof_build_typed(ORC_ELEM_TET4_EDGE, n_tets, tets, elem_edge, edge_nodes, n_edges, n_dir,
+                             dir_pairs, n_hole_markers, gauge, l2g, edge_dof, n_free, n_dofs, root_node);
+}
+
+int orc_dof_build_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, const int32_t* elem_edge,
+                        const int32_t* edge_nodes, int64_t n_edges, int64_t n_dir,
+                        const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge,
+                        int32_t* l2g, int32_t* edge_dof, int64_t* n_free,
+                        int64_t* n_dofs, int32_t* root_node) {
   int64_t E = n_edges;
+  int npe, epe;
+  const int (*tab)[2];
   *n_free = 0; *n_dofs = 0;
   if (root_node) *root_node = -1;
+  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
   if (n_tets <= 0 || E <= 0) return ORC_INVALID_INPUT;
   int32_t maxg = 0;
   for (int64_t i = 0; i < 2 * E; i++) if (edge_nodes[i] > maxg) maxg = edge_nodes[i];
-  for (int64_t i = 0; i < 4 * n_tets; i++) if (tets[i] > maxg) maxg = tets[i];
+  for (int64_t i = 0; i < npe * n_tets; i++) if (tets[i] > maxg) maxg = tets[i];
   uint64_t span = (uint64_t)maxg + 1;
 
   /* Edge lookup by sorted node pair (GlobalEdgeIDGenerator::getGlobalEdgeID,
@@ -210,7 +243,7 @@ int orc_dof_build(int64_t n_tets, const int32_t* tets, const int32_t* elem_edge,
      * index = rank of the global node ID among referenced nodes. */
     int32_t* cidx = (int32_t*)malloc((size_t)span * sizeof(int32_t));
     for (uint64_t g = 0; g < span; g++) cidx[g] = -1;
-    for (int64_t i = 0; i < 4 * n_tets; i++) cidx[tets[i]] = 1;
+    for (int64_t i = 0; i < npe * n_tets; i++) cidx[tets[i]] = 1;
     int32_t V = 0;
     for (uint64_t g = 0; g < span; g++) if (cidx[g] == 1) cidx[g] = V++;
     /* sorted adjacency with the edge of each entry */
@@ -375,7 +408,7 @@ int orc_dof_build(int64_t n_tets, const int32_t* tets, const int32_t* elem_edge,
     free(aptr); free(anb); free(aed); free(cidx);
   }
   /* buildVectorElementMapping (em_dof_manager.cpp:353-393) */
-  for (int64_t i = 0; i < 6 * n_tets; i++) l2g[i] = edge_dof[elem_edge[i]];
+  for (int64_t i = 0; i < epe * n_tets; i++) l2g[i] = edge_dof[elem_edge[i]];
   free(skey); free(sid); free(constrained); free(free_of);
   return 0;
 }
@@ -499,14 +532,149 @@ void orc_edge_signs(const int32_t* tet, int32_t* s) {
 }
 
 /* ---------------------------------------------------------------------------
+ * HEX8_EDGE element (MagneticVector3DIntegrator with HEX8_EDGE, intended
+ * formulas: 2x2x2 Gauss-Legendre, GaussQuadrature::getHex8Points,
+ * gauss_quadrature.cpp:247-276; the reference calls getPoints(HEX8_EDGE),
+ * which returns no points (:36-60), so its literal K_e is zero as for tets).
+ * ------------------------------------------------------------------------- */
+void orc_hex_basis(int k, const double* x, double* w) {
+  /* evalHex8Edge (nedelec_element.cpp:519-615) */
+  const double xi = x[0], eta = x[1], zeta = x[2];
+  w[0] = w[1] = w[2] = 0.0;
+  switch (k) {
+    case 0: w[0] = 0.5 * (1.0 - eta) * (1.0 - zeta); break;
+    case 1: w[1] = 0.5 * (1.0 + xi) * (1.0 - zeta); break;
+    case 2: w[0] = -0.5 * (1.0 + eta) * (1.0 - zeta); break;
+    case 3: w[1] = -0.5 * (1.0 - xi) * (1.0 - zeta); break;
+    case 4: w[0] = 0.5 * (1.0 - eta) * (1.0 + zeta); break;
+    case 5: w[1] = 0.5 * (1.0 + xi) * (1.0 + zeta); break;
+    case 6: w[0] = -0.5 * (1.0 + eta) * (1.0 + zeta); break;
+    case 7: w[1] = -0.5 * (1.0 - xi) * (1.0 + zeta); break;
+    case 8: w[2] = 0.5 * (1.0 - xi) * (1.0 - eta); break;
+    case 9: w[2] = 0.5 * (1.0 + xi) * (1.0 - eta); break;
+    case 10: w[2] = 0.5 * (1.0 + xi) * (1.0 + eta); break;
+    default: w[2] = 0.5 * (1.0 - xi) * (1.0 + eta); break;
+  }
+}
+
+void orc_hex_curl(int k, const double* x, double* c) {
+  /* Reference-domain curl of orc_hex_basis, differentiated by hand:
+   * curl(f e_xi) = (0, df/dzeta, -df/deta), curl(f e_eta) = (-df/dzeta, 0, df/dxi),
+   * curl(f e_zeta) = (df/deta, -df/dxi, 0).  Equals curlHex8Edge
+   * (nedelec_element.cpp:618-720) except at edges 2, 3, 6, 7, where that
+   * function has sign and component errors. */
+  const double xi = x[0], eta = x[1], zeta = x[2];
+  c[0] = c[1] = c[2] = 0.0;
+  switch (k) {
+    case 0: c[1] = -0.5 * (1.0 - eta); c[2] = 0.5 * (1.0 - zeta); break;
+    case 1: c[0] = 0.5 * (1.0 + xi); c[2] = 0.5 * (1.0 - zeta); break;
+    case 2: c[1] = 0.5 * (1.0 + eta); c[2] = 0.5 * (1.0 - zeta); break;
+    case 3: c[0] = -0.5 * (1.0 - xi); c[2] = 0.5 * (1.0 - zeta); break;
+    case 4: c[1] = 0.5 * (1.0 - eta); c[2] = 0.5 * (1.0 + zeta); break;
+    case 5: c[0] = -0.5 * (1.0 + xi); c[2] = 0.5 * (1.0 + zeta); break;
+    case 6: c[1] = -0.5 * (1.0 + eta); c[2] = 0.5 * (1.0 + zeta); break;
+    case 7: c[0] = 0.5 * (1.0 - xi); c[2] = 0.5 * (1.0 + zeta); break;
+    case 8: c[0] = -0.5 * (1.0 - xi); c[1] = 0.5 * (1.0 - eta); break;
+    case 9: c[0] = -0.5 * (1.0 + xi); c[1] = -0.5 * (1.0 - eta); break;
+    case 10: c[0] = 0.5 * (1.0 + xi); c[1] = -0.5 * (1.0 + eta); break;
+    default: c[0] = 0.5 * (1.0 - xi); c[1] = 0.5 * (1.0 + eta); break;
+  }
+}
+
+void orc_hex_jacobian(const double* X, const double* x, double* J, double* det) {
+  /* calcJacobian with the HEX8 gradients (evalHex8GradN, lagrange_element.cpp:
+   * 787-846): J[r][c] = sum_a X_a[r] dN_a/dx_c. */
+  for (int i = 0; i < 9; i++) J[i] = 0.0;
+  for (int a = 0; a < 8; a++) {
+    double l[3], dn[3];
+    for (int c = 0; c < 3; c++) l[c] = 1.0 + HEX_NODE[a][c] * x[c];
+    dn[0] = 0.125 * HEX_NODE[a][0] * l[1] * l[2];
+    dn[1] = 0.125 * HEX_NODE[a][1] * l[0] * l[2];
+    dn[2] = 0.125 * HEX_NODE[a][2] * l[0] * l[1];
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) J[3 * r + c] += X[3 * a + r] * dn[c];
+  }
+  *det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+         J[2] * (J[3] * J[7] - J[4] * J[6]);
+}
+
+void orc_element_hex(const double* X, double nu, double sigma, const orc_source* src,
+                     int32_t n_src, int32_t flags, double* Ke, double* Me, double* Fe) {
+  const double g = 1.0 / sqrt(3.0);
+  for (int i = 0; i < 144; i++) { Ke[i] = 0.0; if (Me) Me[i] = 0.0; }
+  if (Fe) for (int i = 0; i < 12; i++) Fe[i] = 0.0;
+  for (int q = 0; q < 8; q++) {
+    /* getHex8Points order: i (xi) outermost, then eta, then zeta; weight 1 */
+    const double x[3] = {(q & 4) ? g : -g, (q & 2) ? g : -g, (q & 1) ? g : -g};
+    double J[9], det;
+    orc_hex_jacobian(X, x, J, &det);
+    const double adet = fabs(det);
+    if (adet < 1e-15) continue; /* magnetic_vector_3d_integrator.cpp:169-176 */
+    double inv[3][3];
+    inv[0][0] = (J[4] * J[8] - J[5] * J[7]) / det;
+    inv[0][1] = (J[2] * J[7] - J[1] * J[8]) / det;
+    inv[0][2] = (J[1] * J[5] - J[2] * J[4]) / det;
+    inv[1][0] = (J[5] * J[6] - J[3] * J[8]) / det;
+    inv[1][1] = (J[0] * J[8] - J[2] * J[6]) / det;
+    inv[1][2] = (J[2] * J[3] - J[0] * J[5]) / det;
+    inv[2][0] = (J[3] * J[7] - J[4] * J[6]) / det;
+    inv[2][1] = (J[1] * J[6] - J[0] * J[7]) / det;
+    inv[2][2] = (J[0] * J[4] - J[1] * J[3]) / det;
+    double c[12][3], W[12][3];
+    for (int k = 0; k < 12; k++) {
+      double cr[3], wr[3];
+      orc_hex_curl(k, x, cr);
+      orc_hex_basis(k, x, wr);
+      for (int r = 0; r < 3; r++) {
+        /* J curl_ref / detJ (nedelec_element.cpp:242-247); J^-T W_ref */
+        c[k][r] = (J[3 * r] * cr[0] + J[3 * r + 1] * cr[1] + J[3 * r + 2] * cr[2]) / det;
+        W[k][r] = inv[0][r] * wr[0] + inv[1][r] * wr[1] + inv[2][r] * wr[2];
+        if (flags & ORC_FLAG_PIOLA_LITERAL) W[k][r] /= det;
+      }
+    }
+    const double wf = adet * nu;
+    for (int i = 0; i < 12; i++)
+      for (int j = i; j < 12; j++) {
+        Ke[12 * i + j] += wf * (c[i][0] * c[j][0] + c[i][1] * c[j][1] + c[i][2] * c[j][2]);
+        if (j != i) Ke[12 * j + i] = Ke[12 * i + j];
+      }
+    if (Me && (flags & ORC_FLAG_MASS) && sigma > 0.0) {
+      const double wm = adet * sigma;
+      for (int i = 0; i < 12; i++)
+        for (int j = i; j < 12; j++) {
+          Me[12 * i + j] += wm * (W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2]);
+          if (j != i) Me[12 * j + i] = Me[12 * i + j];
+        }
+    }
+    if (Fe && n_src > 0) {
+      /* physical position by the HEX8 map (computePhysicalPosition, :437-483) */
+      double p[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < 8; a++) {
+        double N = 0.125 * (1.0 + HEX_NODE[a][0] * x[0]) * (1.0 + HEX_NODE[a][1] * x[1]) *
+                   (1.0 + HEX_NODE[a][2] * x[2]);
+        for (int r = 0; r < 3; r++) p[r] += N * X[3 * a + r];
+      }
+      double js[3];
+      source_at(src, n_src, p, js);
+      for (int i = 0; i < 12; i++) Fe[i] += adet * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
+    }
+  }
+}
+
+void orc_edge_signs_hex(const int32_t* hex, int32_t* s) {
+  for (int k = 0; k < 12; k++) s[k] = hex[HEX_EDGE[k][0]] < hex[HEX_EDGE[k][1]] ? 1 : -1;
+}
+
+/* ---------------------------------------------------------------------------
  * CSR pattern and numeric assembly (EMAssembly::assemble,
  * src/numeric/em_assembly.cpp:144-420, scatter :654-765; duplicates summed
  * as SparseConverter::to_eigen does, sparse_converter.cpp:19-80).
  * ------------------------------------------------------------------------- */
-static int build_incidence(int64_t n_tets, const int32_t* l2g, int64_t n, int64_t** iptr_o, int64_t** ilist_o) {
+static int build_incidence(int epe, int64_t n_tets, const int32_t* l2g, int64_t n, int64_t** iptr_o,
+                           int64_t** ilist_o) {
   int64_t* iptr = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
   if (!iptr) return -1;
-  for (int64_t i = 0; i < 6 * n_tets; i++) {
+  for (int64_t i = 0; i < epe * n_tets; i++) {
     int32_t r = l2g[i];
     if (r >= n) { free(iptr); return ORC_INVALID_INPUT; }
     if (r >= 0) iptr[r + 1]++;
@@ -515,7 +683,7 @@ static int build_incidence(int64_t n_tets, const int32_t* l2g, int64_t n, int64_
   int64_t* ilist = (int64_t*)malloc((size_t)(iptr[n] > 0 ? iptr[n] : 1) * sizeof(int64_t));
   int64_t* fill = (int64_t*)malloc((size_t)(n > 0 ? n : 1) * sizeof(int64_t));
   for (int64_t r = 0; r < n; r++) fill[r] = iptr[r];
-  for (int64_t i = 0; i < 6 * n_tets; i++)
+  for (int64_t i = 0; i < epe * n_tets; i++)
     if (l2g[i] >= 0) ilist[fill[l2g[i]]++] = i;
   free(fill);
   *iptr_o = iptr;
@@ -525,8 +693,16 @@ static int build_incidence(int64_t n_tets, const int32_t* l2g, int64_t n, int64_
 
 int orc_pattern(int64_t n_tets, const int32_t* l2g, int64_t n, int64_t* row_ptr,
                 int32_t* col, int64_t* nnz) {
+  return orc_pattern_typed(ORC_ELEM_TET4_EDGE, n_tets, l2g, n, row_ptr, col, nnz);
+}
+
+int orc_pattern_typed(int32_t elem_type, int64_t n_tets, const int32_t* l2g, int64_t n, int64_t* row_ptr,
+                      int32_t* col, int64_t* nnz) {
+  int npe, epe;
+  const int (*tab)[2];
+  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
   int64_t *iptr, *ilist;
-  int rc = build_incidence(n_tets, l2g, n, &iptr, &ilist);
+  int rc = build_incidence(epe, n_tets, l2g, n, &iptr, &ilist);
   if (rc) return rc;
   row_ptr[0] = 0;
   int64_t total = 0;
@@ -534,9 +710,9 @@ int orc_pattern(int64_t n_tets, const int32_t* l2g, int64_t n, int64_t* row_ptr,
   for (int64_t r = 0; r < n; r++) {
     int m = 0;
     for (int64_t q = iptr[r]; q < iptr[r + 1]; q++) {
-      int64_t t = ilist[q] / 6;
-      for (int k = 0; k < 6; k++) {
-        int32_t c = l2g[6 * t + k];
+      int64_t t = ilist[q] / epe;
+      for (int k = 0; k < epe; k++) {
+        int32_t c = l2g[epe * t + k];
         if (c < 0) continue;
         int found = 0;
         for (int z = 0; z < m; z++) if (buf[z] == c) { found = 1; break; }
@@ -574,33 +750,52 @@ int orc_assemble(int64_t n_nodes, const double* xyz, int64_t n_tets,
                  const orc_source* src, int32_t n_src, int32_t flags, int64_t n,
                  const int64_t* row_ptr, const int32_t* col, double* kval,
                  double* mval, double* rhs) {
+  return orc_assemble_typed(ORC_ELEM_TET4_EDGE, n_nodes, xyz, n_tets, tets, material, l2g, nu_mat, sigma_mat,
+                            n_mat, src, n_src, flags, n, row_ptr, col, kval, mval, rhs);
+}
+
+int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_tets,
+                       const int32_t* tets, const int32_t* material, const int32_t* l2g,
+                       const double* nu_mat, const double* sigma_mat, int32_t n_mat,
+                       const orc_source* src, int32_t n_src, int32_t flags, int64_t n,
+                       const int64_t* row_ptr, const int32_t* col, double* kval,
+                       double* mval, double* rhs) {
+  int npe, epe;
+  const int (*tab)[2];
+  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
   int64_t nnz = row_ptr[n];
   for (int64_t i = 0; i < nnz; i++) { kval[i] = 0.0; if (mval) mval[i] = 0.0; }
   if (rhs) for (int64_t i = 0; i < n; i++) rhs[i] = 0.0;
   for (int64_t t = 0; t < n_tets; t++) {
     int32_t mid = material ? material[t] : 0;
     if (mid < 0 || mid >= n_mat) continue; /* em_assembly.cpp:270-276 */
-    double X[12];
-    for (int a = 0; a < 4; a++) {
-      int32_t g = tets[4 * t + a];
+    double X[24];
+    for (int a = 0; a < npe; a++) {
+      int32_t g = tets[npe * t + a];
       if (g < 0 || g >= n_nodes) return ORC_INVALID_INPUT;
       X[3 * a] = xyz[3 * g]; X[3 * a + 1] = xyz[3 * g + 1]; X[3 * a + 2] = xyz[3 * g + 2];
     }
-    double Ke[36], Me[36], Fe[6];
-    orc_element(X, nu_mat[mid], sigma_mat ? sigma_mat[mid] : 0.0, src, n_src, flags, Ke, Me, Fe);
-    int32_t s[6];
-    orc_edge_signs(tets + 4 * t, s);
-    if (flags & ORC_FLAG_NO_EDGE_SIGNS) for (int k = 0; k < 6; k++) s[k] = 1;
-    const int32_t* L = l2g + 6 * t;
-    for (int i = 0; i < 6; i++) {
+    double Ke[144], Me[144], Fe[12];
+    int32_t s[12];
+    const double sg = sigma_mat ? sigma_mat[mid] : 0.0;
+    if (elem_type == ORC_ELEM_HEX8_EDGE) {
+      orc_element_hex(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
+      orc_edge_signs_hex(tets + npe * t, s);
+    } else {
+      orc_element(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
+      orc_edge_signs(tets + npe * t, s);
+    }
+    if (flags & ORC_FLAG_NO_EDGE_SIGNS) for (int k = 0; k < epe; k++) s[k] = 1;
+    const int32_t* L = l2g + epe * t;
+    for (int i = 0; i < epe; i++) {
       if (L[i] < 0) continue;
       if (rhs) rhs[L[i]] += s[i] * Fe[i];
-      for (int j = 0; j < 6; j++) {
+      for (int j = 0; j < epe; j++) {
         if (L[j] < 0) continue;
         int64_t p = slot_of(row_ptr, col, L[i], L[j]);
         if (p < 0) return ORC_INVALID_INPUT;
-        kval[p] += (double)(s[i] * s[j]) * Ke[6 * i + j];
-        if (mval && (flags & ORC_FLAG_MASS)) mval[p] += (double)(s[i] * s[j]) * Me[6 * i + j];
+        kval[p] += (double)(s[i] * s[j]) * Ke[epe * i + j];
+        if (mval && (flags & ORC_FLAG_MASS)) mval[p] += (double)(s[i] * s[j]) * Me[epe * i + j];
       }
     }
   }

@@ -1,5 +1,5 @@
 /*
- * emg_oracle.h -- CPU oracle for the TET4 Nedelec curl-curl solve path.
+ * emg_oracle.h -- CPU oracle for the TET4 / HEX8 Nedelec curl-curl solve path.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
  * algorithm (Poofee/emagddm) used as the checker for the CUDA product path and
@@ -36,6 +36,9 @@ enum {
   ORC_MAX_ITER_REACHED = 3,
   ORC_INVALID_INPUT = 4
 };
+
+/* Element types (same values as the C ABI's EMG_ELEM_*). */
+enum { ORC_ELEM_TET4_EDGE = 0, ORC_ELEM_HEX8_EDGE = 1 };
 
 /* Gauge modes. */
 enum { ORC_GAUGE_NONE = -1, ORC_GAUGE_REF = 0, ORC_GAUGE_BOUNDARY_FIRST = 1 };
@@ -112,6 +115,37 @@ int orc_bicgstab(int64_t n, const int64_t* row_ptr, const int32_t* col,
                  const double* val, const double* b, double* x, double tol,
                  int32_t max_iter, int32_t precond, int32_t* iterations,
                  double* residual_norm);
+
+/* ---- element-typed variants: elems holds 4 (TET4_EDGE) or 8 (HEX8_EDGE)
+ * nodes per element, elem_edge / l2g 6 or 12 entries per element; the
+ * untyped functions above are elem_type = ORC_ELEM_TET4_EDGE. */
+int orc_edge_ids_typed(int32_t elem_type, int64_t n_elems, const int32_t* elems, int32_t* elem_edge,
+                       int32_t* edge_nodes, int64_t* n_edges);
+int orc_dof_build_typed(int32_t elem_type, int64_t n_elems, const int32_t* elems, const int32_t* elem_edge,
+                        const int32_t* edge_nodes, int64_t n_edges, int64_t n_dir,
+                        const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge,
+                        int32_t* l2g, int32_t* edge_dof, int64_t* n_free,
+                        int64_t* n_dofs, int32_t* root_node);
+int orc_pattern_typed(int32_t elem_type, int64_t n_elems, const int32_t* l2g, int64_t n_dofs,
+                      int64_t* row_ptr, int32_t* col, int64_t* nnz);
+int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
+                       const int32_t* elems, const int32_t* material, const int32_t* l2g,
+                       const double* nu_mat, const double* sigma_mat, int32_t n_mat,
+                       const orc_source* src, int32_t n_src, int32_t flags,
+                       int64_t n_dofs, const int64_t* row_ptr, const int32_t* col,
+                       double* kval, double* mval, double* rhs);
+
+/* HEX8_EDGE: reference-domain basis value and curl of edge k at x (3),
+ * Jacobian (row-major dx_r/dxi_c) and determinant of the trilinear map of
+ * the 8 nodes X (8 x 3), element matrices (144 row-major, Fe 12) and the
+ * edge signs of one element. */
+void orc_hex_basis(int k, const double* x, double* w);
+void orc_hex_curl(int k, const double* x, double* c);
+void orc_hex_jacobian(const double* X, const double* x, double* J, double* det);
+void orc_element_hex(const double* xyz, double nu, double sigma,
+                     const orc_source* src, int32_t n_src, int32_t flags,
+                     double* Ke, double* Me, double* Fe);
+void orc_edge_signs_hex(const int32_t* hex, int32_t* s);
 
 /* Thread count used by the parallel loops (OpenMP when compiled with it). */
 int orc_num_threads(void);

@@ -59,7 +59,32 @@ def lib():
             f.argtypes = [C.c_int64, I64P, I32P, F64P, F64P, F64P, C.c_double, C.c_int32,
                           C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         L.orc_num_threads.restype = C.c_int
+        L.orc_edge_ids_typed.argtypes = [C.c_int32, C.c_int64, I32P, I32P, I32P, C.POINTER(C.c_int64)]
+        L.orc_dof_build_typed.argtypes = [C.c_int32] + L.orc_dof_build.argtypes
+        L.orc_pattern_typed.argtypes = [C.c_int32] + L.orc_pattern.argtypes
+        L.orc_assemble_typed.argtypes = [C.c_int32] + L.orc_assemble.argtypes
+        for f in (L.orc_hex_basis, L.orc_hex_curl):
+            f.argtypes = [C.c_int, F64P, F64P]
+            f.restype = None
+        L.orc_hex_jacobian.argtypes = [F64P, F64P, F64P, C.POINTER(C.c_double)]
+        L.orc_hex_jacobian.restype = None
+        L.orc_element_hex.argtypes = L.orc_element.argtypes
+        L.orc_element_hex.restype = None
+        L.orc_edge_signs_hex.argtypes = [I32P, I32P]
+        L.orc_edge_signs_hex.restype = None
     return _LIB
+
+
+ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
+
+
+def elem_type_of(elems) -> int:
+    """TET4_EDGE for (T, 4) node arrays, HEX8_EDGE for (T, 8)."""
+    return ELEM_HEX8_EDGE if np.asarray(elems).shape[-1] == 8 else ELEM_TET4_EDGE
+
+
+def edges_per_elem(elem_type: int) -> int:
+    return 12 if elem_type == ELEM_HEX8_EDGE else 6
 
 
 def sources_array(sources):
@@ -76,31 +101,36 @@ def sources_array(sources):
 
 
 def edge_ids(tets):
+    """Edge IDs of (T, 4) tets or (T, 8) hexes: (T, 6|12) element edges and
+    the (E, 2) sorted node pairs."""
     tets = np.ascontiguousarray(tets, dtype=np.int32)
-    T = tets.shape[0]
-    elem_edge = np.empty(6 * T, np.int32)
-    edge_nodes = np.empty(12 * T, np.int32)
+    et = elem_type_of(tets)
+    T, epe = tets.shape[0], edges_per_elem(et)
+    elem_edge = np.empty(epe * T, np.int32)
+    edge_nodes = np.empty(2 * epe * T, np.int32)
     ne = C.c_int64()
-    rc = lib().orc_edge_ids(T, tets.ravel(), elem_edge, edge_nodes, C.byref(ne))
+    rc = lib().orc_edge_ids_typed(et, T, tets.ravel(), elem_edge, edge_nodes, C.byref(ne))
     assert rc == 0, rc
-    return elem_edge.reshape(T, 6), edge_nodes[: 2 * ne.value].reshape(-1, 2)
+    return elem_edge.reshape(T, epe), edge_nodes[: 2 * ne.value].reshape(-1, 2)
 
 
 def dof_build(tets, dirichlet, gauge=GAUGE_REF, n_holes=0, elem_edge=None, edge_nodes=None):
     tets = np.ascontiguousarray(tets, dtype=np.int32)
+    et = elem_type_of(tets)
+    epe = edges_per_elem(et)
     if elem_edge is None:
         elem_edge, edge_nodes = edge_ids(tets)
     T, E = tets.shape[0], edge_nodes.shape[0]
     d = np.ascontiguousarray(dirichlet, dtype=np.int32).reshape(-1)
-    l2g = np.empty(6 * T, np.int32)
+    l2g = np.empty(epe * T, np.int32)
     edge_dof = np.empty(E, np.int32)
     nf, nd, root = C.c_int64(), C.c_int64(), C.c_int32()
-    rc = lib().orc_dof_build(T, tets.ravel(), np.ascontiguousarray(elem_edge, np.int32).ravel(),
-                             np.ascontiguousarray(edge_nodes, np.int32).ravel(), E, d.size // 2,
-                             d if d.size else np.zeros(2, np.int32), n_holes, gauge, l2g, edge_dof,
-                             C.byref(nf), C.byref(nd), C.byref(root))
+    rc = lib().orc_dof_build_typed(et, T, tets.ravel(), np.ascontiguousarray(elem_edge, np.int32).ravel(),
+                                   np.ascontiguousarray(edge_nodes, np.int32).ravel(), E, d.size // 2,
+                                   d if d.size else np.zeros(2, np.int32), n_holes, gauge, l2g, edge_dof,
+                                   C.byref(nf), C.byref(nd), C.byref(root))
     assert rc == 0, rc
-    return dict(elem_edge=elem_edge, edge_nodes=edge_nodes, l2g=l2g.reshape(T, 6),
+    return dict(elem_edge=elem_edge, edge_nodes=edge_nodes, l2g=l2g.reshape(T, epe),
                 edge_dof=edge_dof, n_edges=E, n_free=nf.value, n_dofs=nd.value, root=root.value)
 
 
@@ -114,34 +144,73 @@ def element(X, nu=1.0, sigma=0.0, sources=(), flags=0):
 
 
 def edge_signs(tet):
+    if len(tet) == 8:
+        s = np.empty(12, np.int32)
+        lib().orc_edge_signs_hex(np.ascontiguousarray(tet, np.int32), s)
+        return s
     s = np.empty(6, np.int32)
     lib().orc_edge_signs(np.ascontiguousarray(tet, np.int32), s)
     return s
 
 
+def element_hex(X, nu=1.0, sigma=0.0, sources=(), flags=0):
+    """HEX8_EDGE element matrices (12 x 12 K, M; F 12) of the 8 nodes X."""
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(24)
+    K, M, F = np.empty(144), np.empty(144), np.empty(12)
+    arr, ns = sources_array(list(sources))
+    lib().orc_element_hex(X, nu, sigma, C.cast(arr, C.c_void_p) if arr is not None else None, ns,
+                          flags, K, M, F)
+    return K.reshape(12, 12), M.reshape(12, 12), F
+
+
+def hex_basis(x):
+    """(12, 3) reference values and (12, 3) reference curls at x."""
+    x = np.ascontiguousarray(x, np.float64)
+    W, Cu = np.empty((12, 3)), np.empty((12, 3))
+    for k in range(12):
+        w, c = np.empty(3), np.empty(3)
+        lib().orc_hex_basis(k, x, w)
+        lib().orc_hex_curl(k, x, c)
+        W[k], Cu[k] = w, c
+    return W, Cu
+
+
+def hex_jacobian(X, x):
+    J = np.empty(9)
+    det = C.c_double()
+    lib().orc_hex_jacobian(np.ascontiguousarray(X, np.float64).reshape(24), np.ascontiguousarray(x, np.float64),
+                           J, C.byref(det))
+    return J.reshape(3, 3), det.value
+
+
 def pattern(l2g, n):
+    """Merged CSR pattern; l2g is (T, 6) for tets or (T, 12) for hexes (a flat
+    array is read as tets)."""
+    l2g = np.asarray(l2g)
+    et = ELEM_HEX8_EDGE if (l2g.ndim == 2 and l2g.shape[1] == 12) else ELEM_TET4_EDGE
     l2g = np.ascontiguousarray(l2g, dtype=np.int32).ravel()
-    T = l2g.size // 6
+    T = l2g.size // edges_per_elem(et)
     rp = np.empty(n + 1, np.int64)
     nnz = C.c_int64()
-    rc = lib().orc_pattern(T, l2g, n, rp, None, C.byref(nnz))
+    rc = lib().orc_pattern_typed(et, T, l2g, n, rp, None, C.byref(nnz))
     assert rc == 0, rc
     col = np.empty(max(nnz.value, 1), np.int32)
-    rc = lib().orc_pattern(T, l2g, n, rp, col.ctypes.data_as(C.c_void_p), C.byref(nnz))
+    rc = lib().orc_pattern_typed(et, T, l2g, n, rp, col.ctypes.data_as(C.c_void_p), C.byref(nnz))
     assert rc == 0, rc
     return rp, col[: nnz.value]
 
 
 def assemble(mesh, l2g, n, flags=0, rp=None, col=None):
     """Merged CSR (int64 row_ptr, int32 col), K values, M values, rhs."""
+    et = elem_type_of(mesh.tets)
     if rp is None:
-        rp, col = pattern(l2g, n)
+        rp, col = pattern(np.asarray(l2g).reshape(mesh.n_tets, edges_per_elem(et)), n)
     nnz = int(rp[-1])
     kval = np.empty(nnz)
     mval = np.empty(nnz) if flags & FLAG_MASS else None
     rhs = np.empty(n)
     arr, ns = sources_array(mesh.sources)
-    rc = lib().orc_assemble(mesh.n_nodes, np.ascontiguousarray(mesh.xyz).ravel(), mesh.n_tets,
+    rc = lib().orc_assemble_typed(et, mesh.n_nodes, np.ascontiguousarray(mesh.xyz).ravel(), mesh.n_tets,
                             np.ascontiguousarray(mesh.tets, np.int32).ravel(),
                             np.ascontiguousarray(mesh.material, np.int32),
                             np.ascontiguousarray(l2g, np.int32).ravel(),

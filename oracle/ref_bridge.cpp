@@ -8,7 +8,7 @@
 //   EMAssembly::assemble                 (src/numeric/em_assembly.cpp:144)
 //   SparseConverter::to_eigen            (src/numeric/sparse_converter.cpp:19)
 //   CGSolver / BiCGSTABSolver            (src/numeric/iterative_solvers.cpp)
-//   NedelecElement<3>, GaussQuadrature, MagneticVector3DIntegrator.
+//   NedelecElement<3> (TET4_EDGE, HEX8_EDGE), GaussQuadrature, MagneticVector3DIntegrator.
 #include <Eigen/Sparse>
 #include <chrono>
 #include <cstdint>
@@ -25,12 +25,15 @@
 #include "logger_factory.hpp"
 #include "magnetic_vector_3d_integrator.hpp"
 #include "nedelec_element.hpp"
+#include "shape_function_factory.hpp"
 #include "sparse_converter.h"
 
 namespace {
 
 fe_em::EMMeshData make_mesh(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
-                            int64_t n_dir, const int32_t* dir_pairs, int32_t n_hole_markers) {
+                            int64_t n_dir, const int32_t* dir_pairs, int32_t n_hole_markers,
+                            int32_t elem_type = 0) {
+  const int npe = elem_type == 1 ? 8 : 4;
   fe_em::EMMeshData m;
   m.nodes.resize(n_nodes);
   for (int64_t i = 0; i < n_nodes; ++i) {
@@ -41,8 +44,8 @@ fe_em::EMMeshData make_mesh(int64_t n_nodes, const double* xyz, int64_t n_tets, 
   for (int64_t t = 0; t < n_tets; ++t) {
     auto& e = m.elements[t];
     e.id = static_cast<int>(t);
-    e.node_ids = {tets[4 * t], tets[4 * t + 1], tets[4 * t + 2], tets[4 * t + 3]};
-    e.elem_type = numeric::ElementType::TET4_EDGE;
+    e.node_ids.assign(tets + npe * t, tets + npe * (t + 1));
+    e.elem_type = elem_type == 1 ? numeric::ElementType::HEX8_EDGE : numeric::ElementType::TET4_EDGE;
     e.dof_type = fe_em::DOFType::VECTOR_EDGE_ONLY;
     e.material_id = 0;
     e.region_id = 0;
@@ -92,18 +95,35 @@ void refb_quiet(int quiet) {
   FEEM_SET_LEVEL(quiet ? tool::LogLevel::CRITICAL : tool::LogLevel::INFO);
 }
 
-// Edge IDs + DOF map (+ tree gauge when apply_gauge != 0).
+// Edge IDs + DOF map (+ tree gauge when apply_gauge != 0); elem_type 0 =
+// TET4_EDGE (4 nodes, 6 edges per element), 1 = HEX8_EDGE (8 nodes, 12 edges).
+int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, const int32_t* tets, int64_t n_dir,
+                         const int32_t* dir_pairs, int32_t n_hole_markers, int32_t apply_gauge,
+                         int32_t* elem_edge_out, int32_t* l2g_out, int64_t* n_edges, int64_t* n_free,
+                         int64_t* n_dofs);
+
 int refb_dof_build(int64_t n_nodes, int64_t n_tets, const int32_t* tets, int64_t n_dir,
                    const int32_t* dir_pairs, int32_t n_hole_markers, int32_t apply_gauge,
                    int32_t* elem_edge_out, int32_t* l2g_out, int64_t* n_edges, int64_t* n_free,
                    int64_t* n_dofs) {
+  return refb_dof_build_typed(0, n_nodes, n_tets, tets, n_dir, dir_pairs, n_hole_markers, apply_gauge,
+                              elem_edge_out, l2g_out, n_edges, n_free, n_dofs);
+}
+
+int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, const int32_t* tets, int64_t n_dir,
+                         const int32_t* dir_pairs, int32_t n_hole_markers, int32_t apply_gauge,
+                         int32_t* elem_edge_out, int32_t* l2g_out, int64_t* n_edges, int64_t* n_free,
+                         int64_t* n_dofs) {
+  const int epe = elem_type == 1 ? 12 : 6;
   try {
-    auto mesh = make_mesh(n_nodes, nullptr, n_tets, tets, n_dir, dir_pairs, n_hole_markers);
+    auto mesh = make_mesh(n_nodes, nullptr, n_tets, tets, n_dir, dir_pairs, n_hole_markers, elem_type);
     fe_em::GlobalEdgeIDGenerator gen(mesh);
     gen.generate();
     const auto& l2e = gen.getElemLocalToGlobalEdge();
-    for (int64_t t = 0; t < n_tets; ++t)
-      for (int k = 0; k < 6; ++k) elem_edge_out[6 * t + k] = l2e[t][k];
+    for (int64_t t = 0; t < n_tets; ++t) {
+      if (static_cast<int>(l2e[t].size()) != epe) return -3;
+      for (int k = 0; k < epe; ++k) elem_edge_out[epe * t + k] = l2e[t][k];
+    }
     *n_edges = gen.getNumGlobalEdges();
     fe_em::EMDOFManager dm(mesh, l2e, &gen);
     dm.build();
@@ -111,8 +131,10 @@ int refb_dof_build(int64_t n_nodes, int64_t n_tets, const int32_t* tets, int64_t
     if (apply_gauge) dm.applyTreeGauge();
     *n_dofs = dm.getNumFreeDOFs();
     const auto& l2g = dm.getElemLocalToGlobal();
-    for (int64_t t = 0; t < n_tets; ++t)
-      for (int k = 0; k < 6; ++k) l2g_out[6 * t + k] = l2g[t].indices[k];
+    for (int64_t t = 0; t < n_tets; ++t) {
+      if (static_cast<int>(l2g[t].indices.size()) != epe) return -3;
+      for (int k = 0; k < epe; ++k) l2g_out[epe * t + k] = l2g[t].indices[k];
+    }
     return 0;
   } catch (const std::exception&) {
     return -1;
@@ -121,18 +143,29 @@ int refb_dof_build(int64_t n_nodes, int64_t n_tets, const int32_t* tets, int64_t
 
 // Merged CSR pattern via EMAssembly (placeholder integrator) + to_eigen.
 // col_out may be NULL (count only).  raw_nnz = entries before merging.
+int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_tets,
+                       const int32_t* tets, const int32_t* l2g, int64_t* row_ptr_out, int32_t* col_out,
+                       int64_t* nnz, int64_t* raw_nnz, int64_t* n_rows);
+
 int refb_pattern(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
                  const int32_t* l2g, int64_t* row_ptr_out, int32_t* col_out, int64_t* nnz,
                  int64_t* raw_nnz, int64_t* n_rows) {
+  return refb_pattern_typed(0, n_nodes, xyz, n_tets, tets, l2g, row_ptr_out, col_out, nnz, raw_nnz, n_rows);
+}
+
+int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_tets,
+                       const int32_t* tets, const int32_t* l2g, int64_t* row_ptr_out, int32_t* col_out,
+                       int64_t* nnz, int64_t* raw_nnz, int64_t* n_rows) {
+  const int epe = elem_type == 1 ? 12 : 6;
   try {
-    auto mesh = make_mesh(n_nodes, xyz, n_tets, tets, 0, nullptr, 0);
+    auto mesh = make_mesh(n_nodes, xyz, n_tets, tets, 0, nullptr, 0, elem_type);
     std::vector<fe_em::Local2Global> maps(n_tets);
     for (int64_t t = 0; t < n_tets; ++t) {
-      maps[t] = fe_em::Local2Global(6);
-      for (int k = 0; k < 6; ++k) maps[t].indices[k] = l2g[6 * t + k];
+      maps[t] = fe_em::Local2Global(epe);
+      for (int k = 0; k < epe; ++k) maps[t].indices[k] = l2g[epe * t + k];
       maps[t].element_id = static_cast<int>(t);
-      maps[t].num_vector_dofs = 6;
-      maps[t].elem_type = numeric::ElementType::TET4_EDGE;
+      maps[t].num_vector_dofs = epe;
+      maps[t].elem_type = elem_type == 1 ? numeric::ElementType::HEX8_EDGE : numeric::ElementType::TET4_EDGE;
     }
     std::vector<numeric::MaterialProperties> mats(1);
     numeric::EMAssembly as;
@@ -239,6 +272,77 @@ int refb_integrator_k(const double* xyz /*4 nodes x 3*/, double mu, double* K_ou
     if (K.rows() != 6 || K.cols() != 6) return -2;
     for (int i = 0; i < 6; ++i)
       for (int j = 0; j < 6; ++j) K_out[6 * i + j] = K(i, j);
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
+
+// HEX8_EDGE reference-domain values and curls at one point: w_out[12*3], c_out[12*3].
+void refb_nedelec_hex8(double xi, double eta, double zeta, double* w_out, double* c_out) {
+  numeric::NedelecElement<3> ned(numeric::ElementType::HEX8_EDGE);
+  numeric::LocalPoint p(xi, eta, zeta);
+  for (int k = 0; k < 12; ++k) {
+    Eigen::Vector3d w = ned.evalEdgeFunction(k, p);
+    Eigen::Vector3d c = ned.evalCurlEdge(k, p);
+    for (int r = 0; r < 3; ++r) { w_out[3 * k + r] = w[r]; c_out[3 * k + r] = c[r]; }
+  }
+}
+
+// Jacobian (row-major dx_r/dxi_c) and determinant of the HEX8 Lagrange map
+// of the 8 nodes X (node a at X[3a..3a+2]) at one point, through
+// ShapeFunctionFactory::create("HEX8")->calcJacobian -- the geometry map the
+// integrator uses for positions (computePhysicalPosition).  (NedelecElement's
+// own calcJacobian multiplies the 3 x 8 node matrix by its zero 12 x 3
+// evalGradN, a dimension mismatch, and is not called here.)
+int refb_hex8_jacobian(const double* X, double xi, double eta, double zeta, double* J_out, double* det_out) {
+  try {
+    auto sf = numeric::ShapeFunctionFactory::create("HEX8");
+    if (!sf) return -2;
+    numeric::LocalPoint p(xi, eta, zeta);
+    Eigen::MatrixXd N(3, 8);
+    for (int a = 0; a < 8; ++a)
+      for (int r = 0; r < 3; ++r) N(r, a) = X[3 * a + r];
+    numeric::JacobianResult jr = sf->calcJacobian(p, N);
+    if (jr.jacobian.rows() != 3 || jr.jacobian.cols() != 3) return -3;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) J_out[3 * r + c] = jr.jacobian(r, c);
+    *det_out = jr.det_j;
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
+
+// GaussQuadrature::getPoints(type, order) for HEX8 (edge_type 0) or
+// HEX8_EDGE (edge_type 1): up to 8 points (x, y, z, w) into pts_out.
+int refb_quadrature_hex(int32_t edge_type, int32_t order, double* pts_out /*8*4*/) {
+  auto pts = numeric::GaussQuadrature::getPoints(
+      edge_type ? numeric::ElementType::HEX8_EDGE : numeric::ElementType::HEX8, order);
+  int n = static_cast<int>(pts.size());
+  for (int i = 0; i < n && i < 8; ++i) {
+    pts_out[4 * i] = pts[i].coords[0];
+    pts_out[4 * i + 1] = pts[i].coords[1];
+    pts_out[4 * i + 2] = pts[i].coords[2];
+    pts_out[4 * i + 3] = pts[i].weight;
+  }
+  return n;
+}
+
+// The reference's own MagneticVector3DIntegrator K for one HEX8_EDGE element.
+int refb_integrator_k_hex(const double* xyz /*8 nodes x 3*/, double mu, double* K_out /*144*/) {
+  try {
+    numeric::MagneticVector3DIntegrator it(numeric::ElementType::HEX8_EDGE);
+    numeric::MaterialProperties mp;
+    mp.mu = mu;
+    it.setMaterialProperties(mp);
+    Eigen::MatrixXd X(3, 8);
+    for (int a = 0; a < 8; ++a)
+      for (int r = 0; r < 3; ++r) X(r, a) = xyz[3 * a + r];
+    Eigen::MatrixXd K = it.computeStiffnessMatrix(X);
+    if (K.rows() != 12 || K.cols() != 12) return -2;
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 12; ++j) K_out[12 * i + j] = K(i, j);
     return 0;
   } catch (const std::exception&) {
     return -1;

@@ -46,38 +46,54 @@ def lib():
         L.refb_nedelec_tet4.restype = None
         L.refb_quadrature.argtypes = [C.c_int32, C.c_int32, F64P]
         L.refb_integrator_k.argtypes = [F64P, C.c_double, F64P]
+        L.refb_dof_build_typed.argtypes = [C.c_int32] + L.refb_dof_build.argtypes
+        L.refb_pattern_typed.argtypes = [C.c_int32] + L.refb_pattern.argtypes
+        L.refb_nedelec_hex8.argtypes = [C.c_double, C.c_double, C.c_double, F64P, F64P]
+        L.refb_nedelec_hex8.restype = None
+        L.refb_hex8_jacobian.argtypes = [F64P, C.c_double, C.c_double, C.c_double, F64P, C.POINTER(C.c_double)]
+        L.refb_quadrature_hex.argtypes = [C.c_int32, C.c_int32, F64P]
+        L.refb_integrator_k_hex.argtypes = [F64P, C.c_double, F64P]
         L.refb_quiet(1)
     return _LIB
 
 
+def _elem_type(tets) -> int:
+    return 1 if np.asarray(tets).shape[1] == 8 else 0
+
+
 def dof_build(n_nodes, tets, dirichlet, gauge=True, n_holes=0):
+    """GlobalEdgeIDGenerator + EMDOFManager on (T, 4) TET4_EDGE or (T, 8)
+    HEX8_EDGE elements."""
     tets = np.ascontiguousarray(tets, np.int32)
+    et = _elem_type(tets)
+    epe = 12 if et else 6
     T = tets.shape[0]
     d = np.ascontiguousarray(dirichlet, np.int32).reshape(-1)
-    ee = np.empty(6 * T, np.int32)
-    l2g = np.empty(6 * T, np.int32)
+    ee = np.empty(epe * T, np.int32)
+    l2g = np.empty(epe * T, np.int32)
     ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
-    rc = lib().refb_dof_build(n_nodes, T, tets.ravel(), d.size // 2,
-                              d if d.size else np.zeros(2, np.int32), n_holes, int(gauge), ee,
-                              l2g, C.byref(ne), C.byref(nf), C.byref(nd))
+    rc = lib().refb_dof_build_typed(et, n_nodes, T, tets.ravel(), d.size // 2,
+                                    d if d.size else np.zeros(2, np.int32), n_holes, int(gauge), ee,
+                                    l2g, C.byref(ne), C.byref(nf), C.byref(nd))
     assert rc == 0, rc
-    return dict(elem_edge=ee.reshape(T, 6), l2g=l2g.reshape(T, 6), n_edges=ne.value,
+    return dict(elem_edge=ee.reshape(T, epe), l2g=l2g.reshape(T, epe), n_edges=ne.value,
                 n_free=nf.value, n_dofs=nd.value)
 
 
 def pattern(xyz, tets, l2g):
     tets = np.ascontiguousarray(tets, np.int32)
+    et = _elem_type(tets)
     l2g = np.ascontiguousarray(l2g, np.int32).ravel()
     xyz = np.ascontiguousarray(xyz, np.float64).ravel()
     nnz, raw, nr = C.c_int64(), C.c_int64(), C.c_int64()
-    rc = lib().refb_pattern(xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g, None, None,
-                            C.byref(nnz), C.byref(raw), C.byref(nr))
+    rc = lib().refb_pattern_typed(et, xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g, None, None,
+                                  C.byref(nnz), C.byref(raw), C.byref(nr))
     assert rc == 0, rc
     rp = np.empty(nr.value + 1, np.int64)
     col = np.empty(nnz.value, np.int32)
-    rc = lib().refb_pattern(xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g,
-                            rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
-                            C.byref(nnz), C.byref(raw), C.byref(nr))
+    rc = lib().refb_pattern_typed(et, xyz.size // 3, xyz, tets.shape[0], tets.ravel(), l2g,
+                                  rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                                  C.byref(nnz), C.byref(raw), C.byref(nr))
     assert rc == 0, rc
     return rp, col, raw.value
 
@@ -112,3 +128,32 @@ def integrator_k(X, mu=1.0):
     rc = lib().refb_integrator_k(np.ascontiguousarray(X, np.float64).ravel(), mu, K)
     assert rc == 0, rc
     return K.reshape(6, 6)
+
+
+def nedelec_hex8(xi, eta, zeta):
+    """evalEdgeFunction / evalCurlEdge of HEX8_EDGE: (12, 3) values, (12, 3) curls."""
+    w, c = np.empty(36), np.empty(36)
+    lib().refb_nedelec_hex8(xi, eta, zeta, w, c)
+    return w.reshape(12, 3), c.reshape(12, 3)
+
+
+def hex8_jacobian(X, xi, eta, zeta):
+    """HEX8 Lagrange calcJacobian of the 8 nodes X: (3, 3) J, det J."""
+    J = np.empty(9)
+    det = C.c_double()
+    rc = lib().refb_hex8_jacobian(np.ascontiguousarray(X, np.float64).ravel(), xi, eta, zeta, J, C.byref(det))
+    assert rc == 0, rc
+    return J.reshape(3, 3), det.value
+
+
+def quadrature_hex(edge_type, order):
+    p = np.zeros(32)
+    n = lib().refb_quadrature_hex(edge_type, order, p)
+    return p.reshape(8, 4)[:n]
+
+
+def integrator_k_hex(X, mu=1.0):
+    K = np.empty(144)
+    rc = lib().refb_integrator_k_hex(np.ascontiguousarray(X, np.float64).ravel(), mu, K)
+    assert rc == 0, rc
+    return K.reshape(12, 12)

@@ -5,9 +5,10 @@ reference sources (`make -C oracle -f Makefile.ref`).  Every fixture comes
 from the reference's own code path (GlobalEdgeIDGenerator, EMDOFManager,
 TreeGauge, EMAssembly + SparseConverter, CGSolver, BiCGSTABSolver,
 NedelecElement, GaussQuadrature, MagneticVector3DIntegrator) on the synthetic
-Kuhn-split cube meshes of emagddm_b200.mesh:
+Kuhn-split cube meshes of emagddm_b200.mesh, and the HEX8_EDGE fixtures on
+the hex grids of the same module:
 
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py [--hex-only]
 """
 from __future__ import annotations
 
@@ -26,8 +27,59 @@ from oracle import oracle as O  # noqa: E402
 from oracle import refbridge as R  # noqa: E402
 
 
+def hex_fixtures():
+    """HEX8_EDGE fixtures (reference_hex_fixtures.npz / reference_hex_counts.json)
+    on the n^3 hex grids of emagddm_b200.mesh.hex_topology."""
+    counts = {}
+    arrays = {}
+    for n in (1, 2, 3, 4, 6):
+        xyz, hexes, d = mesh.hex_topology(n)
+        for holes in (0, 2):
+            r0 = R.dof_build(len(xyz), hexes, d, gauge=False, n_holes=holes)
+            r1 = R.dof_build(len(xyz), hexes, d, gauge=True, n_holes=holes)
+            key = f"hex_n{n}_h{holes}"
+            counts[key] = dict(n_edges=r1["n_edges"], n_free=r1["n_free"], n_dofs=r1["n_dofs"],
+                               n_dirichlet=int(len(d)))
+            if n in (2, 3, 4):
+                arrays[f"{key}_elem_edge"] = r1["elem_edge"].astype(np.int32)
+                arrays[f"{key}_l2g_free"] = r0["l2g"].astype(np.int32)
+                arrays[f"{key}_l2g_gauge"] = r1["l2g"].astype(np.int32)
+    # every third Dirichlet pair only (a partly clamped boundary)
+    xyz, hexes, d = mesh.hex_topology(3)
+    r1 = R.dof_build(len(xyz), hexes, d[::3], gauge=True)
+    arrays["hex_n3_partial_l2g_gauge"] = r1["l2g"].astype(np.int32)
+    counts["hex_n3_partial"] = dict(n_edges=r1["n_edges"], n_free=r1["n_free"], n_dofs=r1["n_dofs"])
+    # merged CSR pattern of the gauged n=3 system
+    r1 = R.dof_build(len(xyz), hexes, d, gauge=True)
+    rp, col, raw = R.pattern(xyz, hexes, r1["l2g"])
+    arrays["hex_n3_pattern_row_ptr"] = rp.astype(np.int64)
+    arrays["hex_n3_pattern_col"] = col.astype(np.int32)
+    counts["hex_n3_h0"]["raw_nnz"] = int(raw)
+    counts["hex_n3_h0"]["nnz"] = int(rp[-1])
+    # basis, quadrature, Jacobian, integrator known answers
+    w, c = R.nedelec_hex8(0.3, -0.2, 0.5)
+    arrays["hex_w_at_0.3_-0.2_0.5"] = w
+    arrays["hex_curl_at_0.3_-0.2_0.5"] = c
+    arrays["quad_hex8_order8"] = R.quadrature_hex(0, 8)
+    arrays["quad_hex8edge_order8"] = R.quadrature_hex(1, 8).reshape(-1, 4)
+    X = np.array([[0, 0, 0], [1, 0.1, 0], [1.2, 1, 0.1], [0, 0.9, 0], [0.1, 0, 1], [1, 0, 1.1],
+                  [1, 1.1, 1], [0, 1, 0.9]])
+    J, det = R.hex8_jacobian(X, 0.1, 0.2, -0.3)
+    arrays["hex_distorted_nodes"] = X
+    arrays["hex_distorted_jacobian_at_0.1_0.2_-0.3"] = J
+    arrays["hex_distorted_det"] = np.array([det])
+    arrays["integrator_k_unit_hex"] = R.integrator_k_hex(mesh.hex_topology(1)[0], 1.0)
+    np.savez_compressed(os.path.join(HERE, "reference_hex_fixtures.npz"), **arrays)
+    with open(os.path.join(HERE, "reference_hex_counts.json"), "w") as f:
+        json.dump(counts, f, indent=1, sort_keys=True)
+    print("wrote", len(arrays), "hex arrays and", len(counts), "hex count records")
+
+
 def main():
     assert R.available(), "build oracle/_ref first (make -C oracle -f Makefile.ref)"
+    if "--hex-only" in sys.argv:
+        hex_fixtures()
+        return
     counts = {}
     arrays = {}
     for n in (1, 2, 3, 4, 6, 8):
@@ -76,6 +128,7 @@ def main():
     with open(os.path.join(HERE, "reference_counts.json"), "w") as f:
         json.dump(counts, f, indent=1, sort_keys=True)
     print("wrote", len(arrays), "arrays and", len(counts), "count records")
+    hex_fixtures()
 
 
 if __name__ == "__main__":

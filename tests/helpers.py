@@ -27,9 +27,10 @@ class System:
         tets = np.ascontiguousarray(m.tets, np.int32)
         mat = np.ascontiguousarray(m.material, np.int32)
         self.h = C.c_void_p()
-        _abi.check(lib().emg_system_create(xyz.shape[0], _abi.ptr(xyz), tets.shape[0], _abi.ptr(tets),
-                                           _abi.ptr(mat), _abi.ptr(self.l2g), n_dofs, None,
-                                           C.byref(self.h)), "emg_system_create")
+        et = 1 if tets.shape[1] == 8 else 0
+        _abi.check(lib().emg_system_create_typed(et, xyz.shape[0], _abi.ptr(xyz), tets.shape[0], _abi.ptr(tets),
+                                                 _abi.ptr(mat), _abi.ptr(self.l2g), n_dofs, 0, None,
+                                                 C.byref(self.h)), "emg_system_create_typed")
         self.nu = np.ascontiguousarray(m.nu, np.float64)
         self.sigma = np.ascontiguousarray(m.sigma if sigma is None else sigma, np.float64)
         self.flags = flags
