@@ -10,7 +10,8 @@ host integer setup done once per mesh (reported as setup_dof_ms).
 
 `value` times the step with inputs resident in HBM (emg_system_create_device
 + emg_system_assemble + emg_system_solve); `e2e` times the same C-ABI calls
-with host buffers (geometry and DOF map copied in, solution copied out).
+with pinned host buffers (geometry and DOF map copied in, solution copied
+out).
 Both in solves/s; ms_per_step is the time to a 1e-8 residual.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -171,7 +172,11 @@ def run_ours(args, rank, world, local_rank):
     d_xyz, d_tets = torch.from_numpy(xyz).to(dev), torch.from_numpy(tets).to(dev)
     d_mat, d_l2g = torch.from_numpy(mat).to(dev), torch.from_numpy(l2g).to(dev)
     d_x = torch.empty(n_dofs, dtype=torch.float64, device=dev)
-    h_x = np.empty(n_dofs)
+    # e2e inputs and result live in pinned host memory (page-locked copies)
+    pinned = [torch.from_numpy(a).pin_memory() for a in (xyz, tets, mat, l2g)]
+    p_xyz, p_tets, p_mat, p_l2g = (t.numpy() for t in pinned)
+    h_x_t = torch.empty(n_dofs, dtype=torch.float64).pin_memory()
+    h_x = h_x_t.numpy()
     stream = torch.cuda.current_stream(dev)
     sp = C.c_void_p(stream.cuda_stream)
     src, nsrc = _abi.sources_array(m.sources)
@@ -201,8 +206,8 @@ def run_ours(args, rank, world, local_rank):
                                             C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
                                             C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h))
         else:
-            rc = L.emg_system_create(xyz.shape[0], _abi.ptr(xyz), tets.shape[0], _abi.ptr(tets),
-                                     _abi.ptr(mat), _abi.ptr(l2g), n_dofs, sp, C.byref(h))
+            rc = L.emg_system_create(p_xyz.shape[0], _abi.ptr(p_xyz), p_tets.shape[0], _abi.ptr(p_tets),
+                                     _abi.ptr(p_mat), _abi.ptr(p_l2g), n_dofs, sp, C.byref(h))
         _abi.check(rc, "emg_system_create")
         _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
                    "emg_system_assemble")

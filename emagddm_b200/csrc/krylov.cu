@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -361,6 +362,76 @@ __global__ void k_sell_values(int64_t slots, const int32_t* __restrict__ src,
     const int32_t s = src[i];
     val[i] = s >= 0 ? cval[s] : 0.0;
   }
+}
+
+// Warp per window of kWindow rows: the stable counting sort of the rows by
+// descending length.  Lengths of kLenCap - 1 and more share the last bucket
+// (kept in row order): the order only decides the padding, never the result.
+constexpr int kLenCap = 1024;
+__global__ void __launch_bounds__(32) k_sell_window_perm(int64_t n, const int32_t* __restrict__ rp,
+                                                         int32_t* __restrict__ perm) {
+  __shared__ int32_t cur[kLenCap];  // bucket 0 = longest rows
+  const int lane = threadIdx.x;
+  const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kWindow;
+  const int64_t w1 = w0 + kWindow < n ? w0 + kWindow : n;
+  for (int b = lane; b < kLenCap; b += 32) cur[b] = 0;
+  __syncwarp();
+  for (int64_t i = w0 + lane; i < w1; i += 32) {
+    const int len = rp[i + 1] - rp[i];
+    atomicAdd(&cur[kLenCap - 1 - (len < kLenCap - 1 ? len : kLenCap - 1)], 1);
+  }
+  __syncwarp();
+  // exclusive scan: lane l owns buckets [l * 32, l * 32 + 32)
+  constexpr int kPer = kLenCap / 32;
+  int local = 0;
+  for (int k = 0; k < kPer; ++k) local += cur[lane * kPer + k];
+  int incl = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  int run = incl - local;
+  for (int k = 0; k < kPer; ++k) {
+    const int c = cur[lane * kPer + k];
+    cur[lane * kPer + k] = run;
+    run += c;
+  }
+  __syncwarp();
+  // 32 rows a round in ascending order; equal buckets ranked by lane
+  for (int64_t base = w0; base < w1; base += 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < w1;
+    int b = -1 - lane;  // unique key for lanes past the window
+    if (valid) {
+      const int len = rp[i + 1] - rp[i];
+      b = kLenCap - 1 - (len < kLenCap - 1 ? len : kLenCap - 1);
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, b);
+    const int rank = __popc(grp & ((1u << lane) - 1u));
+    const int pos = valid ? cur[b] + rank : 0;
+    __syncwarp();
+    if (valid && rank == 0) cur[b] += __popc(grp);
+    __syncwarp();
+    if (valid) perm[w0 + pos] = static_cast<int32_t>(i);
+  }
+}
+
+// Slots of every slice: 32 x the longest row it holds.
+__global__ void k_sell_slice_slots(int64_t n, int64_t nslices, const int32_t* __restrict__ rp,
+                                   const int32_t* __restrict__ perm, int32_t* __restrict__ slots) {
+  for (int64_t s = gtid(); s < nslices; s += gstride()) {
+    int32_t len = 0;
+    const int64_t r1 = (s + 1) * kSliceRows < n ? (s + 1) * kSliceRows : n;
+    for (int64_t r = s * kSliceRows; r < r1; ++r) {
+      const int32_t o = perm[r];
+      len = max(len, rp[o + 1] - rp[o]);
+    }
+    slots[s] = kSliceRows * len;
+  }
+}
+
+__global__ void k_widen(int64_t n, const int32_t* __restrict__ in, int64_t* __restrict__ out) {
+  for (int64_t i = gtid(); i < n; i += gstride()) out[i] = in[i];
 }
 
 __global__ void k_invert_perm(int64_t n, const int32_t* __restrict__ perm, int32_t* __restrict__ iperm) {
@@ -750,56 +821,55 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   Sell& S = *A.sell;
   const int64_t n = A.n;
   S.n = n;
-  std::vector<int32_t> rp(n + 1);
-  EMG_CK(cudaMemcpyAsync(rp.data(), A.row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
-  EMG_CK(cudaStreamSynchronize(st));
-  std::vector<int32_t> perm(n);
-  int32_t maxlen = 0;
-  for (int64_t i = 0; i < n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
-  std::vector<int64_t> cnt(static_cast<size_t>(maxlen) + 2);
-  for (int64_t w0 = 0; w0 < n; w0 += kWindow) {
-    const int64_t w1 = std::min<int64_t>(n, w0 + kWindow);
-    std::fill(cnt.begin(), cnt.end(), 0);
-    for (int64_t i = w0; i < w1; ++i) cnt[maxlen - (rp[i + 1] - rp[i]) + 1]++;  // descending
-    for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
-    for (int64_t i = w0; i < w1; ++i) perm[w0 + cnt[maxlen - (rp[i + 1] - rp[i])]++] = static_cast<int32_t>(i);
-  }
+  // Permutation and slice offsets on the device: a warp per window sorts
+  // its rows, a thread per slice takes the longest row, a scan gives offsets.
+  const int g = grid_size();
   S.nslices = (n + kSliceRows - 1) / kSliceRows;
-  std::vector<int64_t> sp(S.nslices + 1, 0);
-  for (int64_t s = 0; s < S.nslices; ++s) {
-    int32_t len = 0;
-    for (int64_t r = s * kSliceRows; r < std::min<int64_t>(n, (s + 1) * kSliceRows); ++r)
-      len = std::max(len, rp[perm[r] + 1] - rp[perm[r]]);
-    sp[s + 1] = sp[s] + static_cast<int64_t>(kSliceRows) * len;
+  EMG_CK(cudaMallocAsync(&S.perm, sizeof(int32_t) * n, st));
+  EMG_CK(cudaMallocAsync(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), st));
+  int32_t *slice_slots = nullptr, *slice_off = nullptr;
+  EMG_CK(cudaMallocAsync(&slice_slots, sizeof(int32_t) * S.nslices, st));
+  EMG_CK(cudaMallocAsync(&slice_off, sizeof(int32_t) * (S.nslices + 1), st));
+  const int64_t windows = (n + kWindow - 1) / kWindow;
+  k_sell_window_perm<<<static_cast<unsigned>(windows), 32, 0, st>>>(n, A.row_ptr, S.perm);
+  k_sell_slice_slots<<<g, kThreads, 0, st>>>(n, S.nslices, A.row_ptr, S.perm, slice_slots);
+  EMG_CK(cudaGetLastError());
+  int64_t total = 0;
+  int rc = scan_counts(slice_slots, slice_off, S.nslices, &total, st);
+  if (rc) return rc;
+  if (total >= (int64_t(1) << 31)) {
+    cudaFreeAsync(slice_slots, st);
+    cudaFreeAsync(slice_off, st);
+    set_error("matrix too large for the solver format");
+    return EMG_INVALID_INPUT;
   }
-  S.slots = sp[S.nslices];
-  if (S.slots >= (int64_t(1) << 31)) { set_error("matrix too large for the solver format"); return EMG_INVALID_INPUT; }
+  k_widen<<<g, kThreads, 0, st>>>(S.nslices + 1, slice_off, S.slice_ptr);
+  EMG_CK(cudaFreeAsync(slice_slots, st));
+  EMG_CK(cudaFreeAsync(slice_off, st));
+  S.slots = total;
   int32_t* iperm = nullptr;
   const size_t ns = static_cast<size_t>(std::max<int64_t>(S.slots, 1));
-  EMG_CK(cudaMallocAsync(&S.perm, sizeof(int32_t) * n, st));
   EMG_CK(cudaMallocAsync(&iperm, sizeof(int32_t) * n, st));
-  EMG_CK(cudaMallocAsync(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), st));
   EMG_CK(cudaMallocAsync(&S.col, sizeof(int32_t) * ns, st));
   EMG_CK(cudaMallocAsync(&S.src, sizeof(int32_t) * ns, st));
   EMG_CK(cudaMallocAsync(&S.val, sizeof(double) * ns, st));
-  EMG_CK(cudaMemcpyAsync(S.perm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemcpyAsync(S.slice_ptr, sp.data(), sizeof(int64_t) * (S.nslices + 1), cudaMemcpyHostToDevice, st));
-  const int g = grid_size();
   k_invert_perm<<<g, kThreads, 0, st>>>(n, S.perm, iperm);
   k_sell_fill<<<g, kThreads, 0, st>>>(n, S.nslices, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col, S.src);
   EMG_CK(cudaGetLastError());
-  EMG_CK(cudaStreamSynchronize(st));
   EMG_CK(cudaFreeAsync(iperm, st));
   S.version = ~uint64_t(0);
-  // bulk-copy pipeline: tiles of 8 slices, kStages stages in shared memory
   S.max_tile_slots = 0;
-  for (int64_t s0 = 0; s0 < S.nslices; s0 += tma::kWarps) {
-    const int64_t s1 = std::min<int64_t>(S.nslices, s0 + tma::kWarps);
-    S.max_tile_slots = std::max<int64_t>(S.max_tile_slots, sp[s1] - sp[s0]);
-  }
   S.tma = false;
 #if EMG_SELL_TMA
   {
+    // bulk-copy pipeline: tiles of 8 slices, kStages stages in shared memory
+    std::vector<int64_t> sp(S.nslices + 1);
+    EMG_CK(cudaMemcpyAsync(sp.data(), S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    for (int64_t s0 = 0; s0 < S.nslices; s0 += tma::kWarps) {
+      const int64_t s1 = std::min<int64_t>(S.nslices, s0 + tma::kWarps);
+      S.max_tile_slots = std::max<int64_t>(S.max_tile_slots, sp[s1] - sp[s0]);
+    }
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -862,6 +932,44 @@ void free_sell(Sell* s) {
   delete s;
 }
 
+// Pinned host blocks for the solver-state read-back, recycled for the life of
+// the process: page-locking and releasing a block per solver
+// (cudaMallocHost / cudaFreeHost) costs about a millisecond per solve and,
+// measured on B200 boxes, occasionally 50-500 ms inside cudaFreeHost.
+// The pool is never destroyed, so workspaces released during process exit
+// still find it.
+constexpr size_t kPinnedBlock = 256;
+static_assert(sizeof(SolverState) <= kPinnedBlock, "solver state must fit a pinned block");
+struct PinnedPool {
+  std::mutex mu;
+  std::vector<void*> free;
+};
+PinnedPool& pinned_pool() {
+  static PinnedPool* p = new PinnedPool();
+  return *p;
+}
+
+int pinned_state_alloc(SolverState** out) {
+  PinnedPool& pool = pinned_pool();
+  std::lock_guard<std::mutex> lock(pool.mu);
+  if (pool.free.empty()) {
+    constexpr int kBlocks = 64;
+    char* chunk = nullptr;
+    EMG_CK(cudaMallocHost(&chunk, kPinnedBlock * kBlocks));
+    for (int b = kBlocks - 1; b >= 0; --b) pool.free.push_back(chunk + kPinnedBlock * b);
+  }
+  *out = static_cast<SolverState*>(pool.free.back());
+  pool.free.pop_back();
+  return EMG_SUCCESS;
+}
+
+void pinned_state_free(SolverState* p) {
+  if (!p) return;
+  PinnedPool& pool = pinned_pool();
+  std::lock_guard<std::mutex> lock(pool.mu);
+  pool.free.push_back(p);
+}
+
 // Workspace vectors come from the stream-ordered pool (allocated on `st`,
 // returned with cudaFreeAsync once the device is idle).
 int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
@@ -877,7 +985,7 @@ int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
     EMG_CK(cudaMallocAsync(&w.state, sizeof(SolverState), st));
     EMG_CK(cudaStreamSynchronize(st));
     EMG_CK(cudaMemset(w.state, 0, sizeof(SolverState)));
-    EMG_CK(cudaMallocHost(&w.state_h, sizeof(SolverState)));
+    if (int rc = pinned_state_alloc(&w.state_h)) return rc;
     EMG_CK(cudaStreamCreate(&w.cap));
     EMG_CK(cudaEventCreate(&w.ev0));
     EMG_CK(cudaEventCreate(&w.ev1));
@@ -1189,7 +1297,7 @@ void free_workspace(KrylovWorkspace* w) {
   }
   {
     TraceScope t("free_workspace.host_state");
-    if (w->state_h) cudaFreeHost(w->state_h);
+    pinned_state_free(w->state_h);
   }
   {
     TraceScope t("free_workspace.stream_events");
