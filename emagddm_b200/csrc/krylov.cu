@@ -3,10 +3,12 @@
 // 343-503 and :869-1118), with the same iteration, stopping and failure rules.
 //
 // Matrix format inside the solvers: SELL-32-sigma.  Rows are sorted by length
-// (descending) inside windows of 4096 rows, cut into slices of 32 rows, and
-// each slice is stored column-major and padded to its longest row, so one warp
-// reads a slice with 256-byte coalesced loads and every lane has a whole row
-// (no shuffles, many independent loads in flight).  The solvers run in the
+// (descending) inside windows of 4096 rows and cut into slices of 32 rows; the
+// 8 slices of a 256-row group are padded to the group's longest row and
+// stored entry-interleaved (entry j of the 8 slices is one 2 KB run of
+// values), so one warp reads a slice with 256-byte coalesced loads, every lane
+// has a whole row (no shuffles, many independent loads in flight), and the 8
+// warps of a block stream one contiguous run together.  The solvers run in the
 // permuted numbering (P A P^T, P b): all vector kernels stay contiguous; b is
 // permuted on entry and x on exit.  The CSR handed in stays the exported form.
 //
@@ -55,13 +57,14 @@ struct SolverState {
   int32_t copy_err;    // a bounded wait on a bulk copy ran out
 };
 
-// SELL-32-sigma copy of a DevCsr in the permuted numbering.
+// SELL-32-sigma copy of a DevCsr in the permuted numbering, slices in
+// interleaved groups of kGroup.
 struct Sell {
-  int64_t n = 0, nslices = 0, slots = 0;
+  int64_t n = 0, nslices = 0, ngroups = 0, slots = 0;
   int64_t max_tile_slots = 0;    // largest 8-slice tile (bulk-copy stage size)
   bool tma = false;              // stages of the bulk-copy kernels fit in shared memory
   int32_t* perm = nullptr;       // new row -> old row
-  int64_t* slice_ptr = nullptr;  // nslices + 1 slot offsets (multiples of 32)
+  int64_t* slice_ptr = nullptr;  // ngroups + 1 slot offsets of the slice groups (multiples of 32 kGroup)
   int16_t* dcol = nullptr;       // column - row of every slot, when all fit in 16 bits
   bool narrow = false;           // dcol in use (col freed): 10 bytes per slot instead of 12
   int32_t* col = nullptr;        // permuted column of every slot
@@ -123,6 +126,31 @@ __device__ __forceinline__ int64_t gstride() {
 #ifndef EMG_SELL_UNROLL
 #define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
 #endif
+// Slices per group: the kGroup slices of a group share one length and are
+// interleaved entry by entry (slot of entry j, slice w, lane l at
+// group_base + 32 kGroup j + 32 w + l), so the kGroup warps of a block that
+// work on one group read one contiguous 32 kGroup-slot run per entry.
+#ifndef EMG_SELL_GROUP
+#define EMG_SELL_GROUP 1
+#endif
+// Slice order over the warps: 0 = the warps of a block take adjacent slices
+// (slice = global warp id + k * warps); 1 = they take slices gridDim.x apart,
+// which spreads the concurrent streams of an SM over memory (64.1 vs 65.6 us
+// for the 64^3 CG matrix on B200; interleaving the slices of a block instead,
+// EMG_SELL_GROUP=8, was slower: 75.5 us).
+#ifndef EMG_SELL_SPREAD
+#define EMG_SELL_SPREAD 1
+#endif
+constexpr int kGroup = EMG_SELL_GROUP;
+constexpr int kGroupStride = 32 * kGroup;
+
+// Base slot (entry 0, lane 0) and entry count of slice s.
+__device__ __forceinline__ void slice_span(const int64_t* __restrict__ gp, int64_t s, int64_t& base, int& len) {
+  const int64_t g = s / kGroup;
+  const int64_t b0 = gp[g];
+  len = static_cast<int>((gp[g + 1] - b0) / kGroupStride);
+  base = b0 + 32 * (s - g * kGroup);
+}
 
 // Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
 // out(row, y_row) for every real row.  Entries of a row are summed in CSR
@@ -131,7 +159,9 @@ __device__ __forceinline__ int64_t gstride() {
 template <bool kNarrow, class Out>
 __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
   const int lane = threadIdx.x & 31;
-  const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+  const int64_t nwarps = gstride() >> 5;
+  const int64_t warp = EMG_SELL_SPREAD ? static_cast<int64_t>(threadIdx.x >> 5) * gridDim.x + blockIdx.x
+                                       : gtid() >> 5;
   const uint64_t pol = evict_first_policy();
   const int64_t* __restrict__ sp = A.slice_ptr;
   const int32_t* __restrict__ col = A.col;
@@ -142,20 +172,21 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     else return ld_stream(col + k, pol);
   };
   for (int64_t s = warp; s < A.nslices; s += nwarps) {
-    const int64_t b0 = sp[s], b1 = sp[s + 1];
-    const int len = static_cast<int>((b1 - b0) >> 5);
-    const int64_t base = b0 + lane;
+    int64_t base;
+    int len;
+    slice_span(sp, s, base, len);
+    base += lane;
     const int row32 = static_cast<int>(s * kSliceRows + lane);
     double sum = 0.0;
     int j = 0;
     for (; j + EMG_SELL_UNROLL <= len; j += EMG_SELL_UNROLL) {
-      const int64_t k = base + 32 * j;
+      const int64_t k = base + static_cast<int64_t>(kGroupStride) * j;
       int c[EMG_SELL_UNROLL];
       double v[EMG_SELL_UNROLL], xv[EMG_SELL_UNROLL];
 #pragma unroll
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) {
-        c[u] = column(k + 32 * u, row32);
-        v[u] = ld_stream(val + k + 32 * u, pol);
+        c[u] = column(k + kGroupStride * u, row32);
+        v[u] = ld_stream(val + k + kGroupStride * u, pol);
       }
 #pragma unroll
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) xv[u] = x[c[u]];
@@ -163,7 +194,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) sum += v[u] * xv[u];
     }
     for (; j < len; ++j) {
-      const int64_t k = base + 32 * j;
+      const int64_t k = base + static_cast<int64_t>(kGroupStride) * j;
       sum += ld_stream(val + k, pol) * x[column(k, row32)];
     }
     const int64_t row = s * kSliceRows + lane;
@@ -304,7 +335,8 @@ __device__ __forceinline__ bool reduce_partials(const double (&vals)[kVals], dou
 }
 
 // ------------------------------------------------------------ SELL build ----
-// Warp per slice: column index (permuted) and CSR source of every slot.
+// Warp per slice: column index (permuted) and CSR source of every slot; rows
+// at or past n are all padding.
 __global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restrict__ sp,
                             const int32_t* __restrict__ perm, const int32_t* __restrict__ iperm,
                             const int32_t* __restrict__ rp, const int32_t* __restrict__ ccol,
@@ -312,8 +344,9 @@ __global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restric
   const int lane = threadIdx.x & 31;
   const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   for (int64_t s = warp; s < nslices; s += nwarps) {
-    const int64_t b0 = sp[s];
-    const int len = static_cast<int>((sp[s + 1] - b0) >> 5);
+    int64_t b0;
+    int len;
+    slice_span(sp, s, b0, len);
     const int64_t row = s * kSliceRows + lane;
     int32_t a = 0, rl = 0;
     const int32_t self = static_cast<int32_t>(row < n ? row : n - 1);
@@ -323,7 +356,7 @@ __global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restric
       rl = rp[old + 1] - a;
     }
     for (int j = 0; j < len; ++j) {
-      const int64_t k = b0 + 32 * j + lane;
+      const int64_t k = b0 + static_cast<int64_t>(kGroupStride) * j + lane;
       if (j < rl) {
         col[k] = iperm[ccol[a + j]];
         src[k] = a + j;
@@ -342,12 +375,13 @@ __global__ void k_sell_narrow(int64_t nslices, const int64_t* __restrict__ sp,
   const int lane = threadIdx.x & 31;
   const int64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   for (int64_t s = warp; s < nslices; s += nwarps) {
-    const int64_t b0 = sp[s];
-    const int len = static_cast<int>((sp[s + 1] - b0) >> 5);
+    int64_t b0;
+    int len;
+    slice_span(sp, s, b0, len);
     const int64_t row = s * kSliceRows + lane;
     bool bad = false;
     for (int j = 0; j < len; ++j) {
-      const int64_t k = b0 + 32 * j + lane;
+      const int64_t k = b0 + static_cast<int64_t>(kGroupStride) * j + lane;
       const int64_t d = static_cast<int64_t>(col[k]) - row;
       bad |= d < -32768 || d > 32767;
       dcol[k] = static_cast<int16_t>(d);
@@ -416,17 +450,18 @@ __global__ void __launch_bounds__(32) k_sell_window_perm(int64_t n, const int32_
   }
 }
 
-// Slots of every slice: 32 x the longest row it holds.
-__global__ void k_sell_slice_slots(int64_t n, int64_t nslices, const int32_t* __restrict__ rp,
+// Slots of every group: 32 kGroup x the longest row it holds.
+__global__ void k_sell_group_slots(int64_t n, int64_t ngroups, const int32_t* __restrict__ rp,
                                    const int32_t* __restrict__ perm, int32_t* __restrict__ slots) {
-  for (int64_t s = gtid(); s < nslices; s += gstride()) {
+  for (int64_t g = gtid(); g < ngroups; g += gstride()) {
     int32_t len = 0;
-    const int64_t r1 = (s + 1) * kSliceRows < n ? (s + 1) * kSliceRows : n;
-    for (int64_t r = s * kSliceRows; r < r1; ++r) {
+    const int64_t r0 = g * kGroupStride;
+    const int64_t r1 = r0 + kGroupStride < n ? r0 + kGroupStride : n;
+    for (int64_t r = r0; r < r1; ++r) {
       const int32_t o = perm[r];
       len = max(len, rp[o + 1] - rp[o]);
     }
-    slots[s] = kSliceRows * len;
+    slots[g] = kGroupStride * len;
   }
 }
 
@@ -548,7 +583,31 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, double* __res
   if (st->done) return;
   const double a = st->alpha;
   double acc[2] = {0.0, 0.0};
-  for (int64_t i = gtid(); i < n; i += gstride()) {
+  // pairs of entries per 16-byte access, the odd last entry by thread 0
+  const int64_t n2 = n >> 1;
+  double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+  double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+  double2* __restrict__ z2 = reinterpret_cast<double2*>(z);
+  const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
+  const double2* __restrict__ q2 = reinterpret_cast<const double2*>(q);
+  const double2* __restrict__ d2 = reinterpret_cast<const double2*>(dinv);
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    const double2 pv = p2[i], qv = q2[i], dv = d2[i];
+    double2 xv = x2[i], rv = r2[i], zv;
+    xv.x += a * pv.x;
+    xv.y += a * pv.y;
+    rv.x -= a * qv.x;
+    rv.y -= a * qv.y;
+    zv.x = dv.x * rv.x;
+    zv.y = dv.y * rv.y;
+    x2[i] = xv;
+    r2[i] = rv;
+    z2[i] = zv;
+    acc[0] += rv.x * zv.x + rv.y * zv.y;
+    acc[1] += rv.x * rv.x + rv.y * rv.y;
+  }
+  if ((n & 1) && gtid() == 0) {
+    const int64_t i = n - 1;
     x[i] += a * p[i];
     const double ri = r[i] - a * q[i];
     const double zi = dinv[i] * ri;
@@ -583,7 +642,17 @@ __global__ void __launch_bounds__(kThreads) k_cg_direction(int64_t n, double* __
                                                            const SolverState* st) {
   if (st->done) return;
   const double b = st->beta;
-  for (int64_t i = gtid(); i < n; i += gstride()) p[i] = z[i] + b * p[i];
+  const int64_t n2 = n >> 1;
+  double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
+  const double2* __restrict__ z2 = reinterpret_cast<const double2*>(z);
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    const double2 zv = z2[i];
+    double2 pv = p2[i];
+    pv.x = zv.x + b * pv.x;
+    pv.y = zv.y + b * pv.y;
+    p2[i] = pv;
+  }
+  if ((n & 1) && gtid() == 0) p[n - 1] = z[n - 1] + b * p[n - 1];
 }
 
 // ----------------------------------------------------------- BiCGSTAB ----
@@ -825,17 +894,18 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   // its rows, a thread per slice takes the longest row, a scan gives offsets.
   const int g = grid_size();
   S.nslices = (n + kSliceRows - 1) / kSliceRows;
+  S.ngroups = (S.nslices + kGroup - 1) / kGroup;
   EMG_CK(cudaMallocAsync(&S.perm, sizeof(int32_t) * n, st));
-  EMG_CK(cudaMallocAsync(&S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), st));
+  EMG_CK(cudaMallocAsync(&S.slice_ptr, sizeof(int64_t) * (S.ngroups + 1), st));
   int32_t *slice_slots = nullptr, *slice_off = nullptr;
-  EMG_CK(cudaMallocAsync(&slice_slots, sizeof(int32_t) * S.nslices, st));
-  EMG_CK(cudaMallocAsync(&slice_off, sizeof(int32_t) * (S.nslices + 1), st));
+  EMG_CK(cudaMallocAsync(&slice_slots, sizeof(int32_t) * S.ngroups, st));
+  EMG_CK(cudaMallocAsync(&slice_off, sizeof(int32_t) * (S.ngroups + 1), st));
   const int64_t windows = (n + kWindow - 1) / kWindow;
   k_sell_window_perm<<<static_cast<unsigned>(windows), 32, 0, st>>>(n, A.row_ptr, S.perm);
-  k_sell_slice_slots<<<g, kThreads, 0, st>>>(n, S.nslices, A.row_ptr, S.perm, slice_slots);
+  k_sell_group_slots<<<g, kThreads, 0, st>>>(n, S.ngroups, A.row_ptr, S.perm, slice_slots);
   EMG_CK(cudaGetLastError());
   int64_t total = 0;
-  int rc = scan_counts(slice_slots, slice_off, S.nslices, &total, st);
+  int rc = scan_counts(slice_slots, slice_off, S.ngroups, &total, st);
   if (rc) return rc;
   if (total >= (int64_t(1) << 31)) {
     cudaFreeAsync(slice_slots, st);
@@ -843,7 +913,7 @@ int build_sell(DevCsr& A, cudaStream_t st) {
     set_error("matrix too large for the solver format");
     return EMG_INVALID_INPUT;
   }
-  k_widen<<<g, kThreads, 0, st>>>(S.nslices + 1, slice_off, S.slice_ptr);
+  k_widen<<<g, kThreads, 0, st>>>(S.ngroups + 1, slice_off, S.slice_ptr);
   EMG_CK(cudaFreeAsync(slice_slots, st));
   EMG_CK(cudaFreeAsync(slice_off, st));
   S.slots = total;
@@ -854,13 +924,16 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   EMG_CK(cudaMallocAsync(&S.src, sizeof(int32_t) * ns, st));
   EMG_CK(cudaMallocAsync(&S.val, sizeof(double) * ns, st));
   k_invert_perm<<<g, kThreads, 0, st>>>(n, S.perm, iperm);
-  k_sell_fill<<<g, kThreads, 0, st>>>(n, S.nslices, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col, S.src);
+  // every slot of every group is written: slices past the last row are padding
+  k_sell_fill<<<g, kThreads, 0, st>>>(n, S.ngroups * kGroup, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col,
+                                      S.src);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaFreeAsync(iperm, st));
   S.version = ~uint64_t(0);
   S.max_tile_slots = 0;
   S.tma = false;
 #if EMG_SELL_TMA
+  static_assert(kGroup == 1, "the bulk-copy pipeline reads contiguous per-slice runs (EMG_SELL_GROUP=1)");
   {
     // bulk-copy pipeline: tiles of 8 slices, kStages stages in shared memory
     std::vector<int64_t> sp(S.nslices + 1);
