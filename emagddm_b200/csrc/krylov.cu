@@ -144,6 +144,17 @@ __device__ __forceinline__ int64_t gstride() {
 constexpr int kGroup = EMG_SELL_GROUP;
 constexpr int kGroupStride = 32 * kGroup;
 
+// Packed slots: every 32-slot chunk (one warp's entry) is stored as 256 B of
+// values followed by 128 B of columns, one stream per warp instead of two.
+#ifndef EMG_SELL_PACKED
+#define EMG_SELL_PACKED 0
+#endif
+constexpr int kChunkBytes = 384;
+__host__ __device__ __forceinline__ int64_t packed_val_index(int64_t k) { return (k >> 5) * (kChunkBytes / 8) + (k & 31); }
+__host__ __device__ __forceinline__ int64_t packed_col_index(int64_t k) {
+  return (k >> 5) * (kChunkBytes / 4) + 64 + (k & 31);
+}
+
 // Base slot (entry 0, lane 0) and entry count of slice s.
 __device__ __forceinline__ void slice_span(const int64_t* __restrict__ gp, int64_t s, int64_t& base, int& len) {
   const int64_t g = s / kGroup;
@@ -169,7 +180,12 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
   const double* __restrict__ val = A.val;
   auto column = [&](int64_t k, int row) -> int {
     if constexpr (kNarrow) return row + ld_stream(dcol + k, pol);
+    else if constexpr (EMG_SELL_PACKED) return ld_stream(col + packed_col_index(k), pol);
     else return ld_stream(col + k, pol);
+  };
+  auto value = [&](int64_t k) -> double {
+    if constexpr (EMG_SELL_PACKED) return ld_stream(val + packed_val_index(k), pol);
+    else return ld_stream(val + k, pol);
   };
   for (int64_t s = warp; s < A.nslices; s += nwarps) {
     int64_t base;
@@ -186,7 +202,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
 #pragma unroll
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) {
         c[u] = column(k + kGroupStride * u, row32);
-        v[u] = ld_stream(val + k + kGroupStride * u, pol);
+        v[u] = value(k + kGroupStride * u);
       }
 #pragma unroll
       for (int u = 0; u < EMG_SELL_UNROLL; ++u) xv[u] = x[c[u]];
@@ -195,7 +211,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     }
     for (; j < len; ++j) {
       const int64_t k = base + static_cast<int64_t>(kGroupStride) * j;
-      sum += ld_stream(val + k, pol) * x[column(k, row32)];
+      sum += value(k) * x[column(k, row32)];
     }
     const int64_t row = s * kSliceRows + lane;
     if (row < A.n) out(row, sum);
@@ -357,11 +373,12 @@ __global__ void k_sell_fill(int64_t n, int64_t nslices, const int64_t* __restric
     }
     for (int j = 0; j < len; ++j) {
       const int64_t k = b0 + static_cast<int64_t>(kGroupStride) * j + lane;
+      const int64_t kc = EMG_SELL_PACKED ? packed_col_index(k) : k;
       if (j < rl) {
-        col[k] = iperm[ccol[a + j]];
+        col[kc] = iperm[ccol[a + j]];
         src[k] = a + j;
       } else {
-        col[k] = self;  // padding reads a valid entry and multiplies it by 0
+        col[kc] = self;  // padding reads a valid entry and multiplies it by 0
         src[k] = -1;
       }
     }
@@ -394,7 +411,7 @@ __global__ void k_sell_values(int64_t slots, const int32_t* __restrict__ src,
                               const double* __restrict__ cval, double* __restrict__ val) {
   for (int64_t i = gtid(); i < slots; i += gstride()) {
     const int32_t s = src[i];
-    val[i] = s >= 0 ? cval[s] : 0.0;
+    val[EMG_SELL_PACKED ? packed_val_index(i) : i] = s >= 0 ? cval[s] : 0.0;
   }
 }
 
@@ -920,9 +937,14 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   int32_t* iperm = nullptr;
   const size_t ns = static_cast<size_t>(std::max<int64_t>(S.slots, 1));
   EMG_CK(cudaMallocAsync(&iperm, sizeof(int32_t) * n, st));
-  EMG_CK(cudaMallocAsync(&S.col, sizeof(int32_t) * ns, st));
   EMG_CK(cudaMallocAsync(&S.src, sizeof(int32_t) * ns, st));
-  EMG_CK(cudaMallocAsync(&S.val, sizeof(double) * ns, st));
+  if (EMG_SELL_PACKED) {  // one buffer: 32-slot chunks of values then columns
+    EMG_CK(cudaMallocAsync(&S.val, (sizeof(double) + sizeof(int32_t)) * ns, st));
+    S.col = reinterpret_cast<int32_t*>(S.val);
+  } else {
+    EMG_CK(cudaMallocAsync(&S.col, sizeof(int32_t) * ns, st));
+    EMG_CK(cudaMallocAsync(&S.val, sizeof(double) * ns, st));
+  }
   k_invert_perm<<<g, kThreads, 0, st>>>(n, S.perm, iperm);
   // every slot of every group is written: slices past the last row are padding
   k_sell_fill<<<g, kThreads, 0, st>>>(n, S.ngroups * kGroup, S.slice_ptr, S.perm, iperm, A.row_ptr, A.col, S.col,
@@ -933,7 +955,8 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   S.max_tile_slots = 0;
   S.tma = false;
 #if EMG_SELL_TMA
-  static_assert(kGroup == 1, "the bulk-copy pipeline reads contiguous per-slice runs (EMG_SELL_GROUP=1)");
+  static_assert(kGroup == 1 && !EMG_SELL_PACKED,
+                "the bulk-copy pipeline reads contiguous per-slice runs of separate arrays");
   {
     // bulk-copy pipeline: tiles of 8 slices, kStages stages in shared memory
     std::vector<int64_t> sp(S.nslices + 1);
@@ -960,7 +983,7 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   // 16-bit column offsets when every |column - row| fits (banded numberings,
   // e.g. first-appearance edge IDs of structured meshes): 10 bytes per slot.
   S.narrow = false;
-  if (EMG_SELL_NARROW && !S.tma && S.slots > 0) {
+  if (EMG_SELL_NARROW && !EMG_SELL_PACKED && !S.tma && S.slots > 0) {
     int32_t* overflow = nullptr;
     EMG_CK(cudaMallocAsync(&S.dcol, sizeof(int16_t) * S.slots, st));
     EMG_CK(cudaMallocAsync(&overflow, sizeof(int32_t), st));
@@ -998,9 +1021,9 @@ int ensure_sell(DevCsr& A, cudaStream_t st) {
 
 void free_sell(Sell* s) {
   if (!s) return;
-  for (void* p : {static_cast<void*>(s->perm), static_cast<void*>(s->slice_ptr),
-                  static_cast<void*>(s->col), static_cast<void*>(s->dcol), static_cast<void*>(s->src),
-                  static_cast<void*>(s->val)})
+  void* col = static_cast<void*>(s->col) == static_cast<void*>(s->val) ? nullptr : static_cast<void*>(s->col);
+  for (void* p : {static_cast<void*>(s->perm), static_cast<void*>(s->slice_ptr), col,
+                  static_cast<void*>(s->dcol), static_cast<void*>(s->src), static_cast<void*>(s->val)})
     if (p) cudaFreeAsync(p, 0);
   delete s;
 }
