@@ -2,16 +2,18 @@
 //
 // The reference plans Gmsh .msh files as its mesh format (mesh/README.md) and
 // consumes meshes as fe_em::EMMeshData (include/fe_em/em_mesh_data.hpp:90-230):
-// nodes, TET4 elements with a material id, and a DIRICHLET / VECTOR_EDGE_ONLY
-// boundary marker whose targets are edge node pairs.  This reader produces
-// exactly those arrays:
+// nodes, TET4 / HEX8 elements with a material id, and a DIRICHLET /
+// VECTOR_EDGE_ONLY boundary marker whose targets are edge node pairs.  This
+// reader produces exactly those arrays:
 //   * nodes in ascending Gmsh tag order (index = rank of the tag);
-//   * 4-node tetrahedra (element type 4) in file order; material id = rank of
-//     the element's physical tag among the distinct physical tags of the
-//     tetrahedra (ascending); higher-order tetrahedra are rejected;
-//   * Dirichlet node pairs = the edges of the triangles (type 2) whose
-//     physical tag is listed, or, with no list, the edges of every boundary
-//     face (a face of exactly one tetrahedron).
+//   * 4-node tetrahedra (element type 4) or 8-node hexahedra (type 5, Gmsh's
+//     vertex order = ElementGeometry's HEX8 order) in file order, one type per
+//     file; material id = rank of the element's physical tag among the
+//     distinct physical tags of the volume elements (ascending); higher-order,
+//     prism and pyramid volumes are rejected;
+//   * Dirichlet node pairs = the edges of the triangles (type 2) and
+//     quadrangles (type 3) whose physical tag is listed, or, with no list, the
+//     edges of every boundary face (a face of exactly one volume element).
 #include <algorithm>
 #include <array>
 #include <cstdio>
@@ -30,10 +32,13 @@ namespace {
 struct Raw {
   std::vector<int64_t> node_tag;
   std::vector<double> xyz;
-  std::vector<int64_t> tet_nodes;  // 4 per tet, Gmsh node tags
-  std::vector<int32_t> tet_phys;
+  int vol_type = 0;                // Gmsh type of the volume elements: 4 or 5
+  std::vector<int64_t> vol_nodes;  // 4 or 8 per element, Gmsh node tags
+  std::vector<int32_t> vol_phys;
   std::vector<int64_t> tri_nodes;  // 3 per triangle
   std::vector<int32_t> tri_phys;
+  std::vector<int64_t> quad_nodes;  // 4 per quadrangle
+  std::vector<int32_t> quad_phys;
 };
 
 bool seek(std::istream& in, const std::string& section) {
@@ -48,6 +53,46 @@ bool seek(std::istream& in, const std::string& section) {
 int fail(const std::string& what) {
   set_error("gmsh: " + what);
   return EMG_INVALID_INPUT;
+}
+
+// One element of Gmsh type `type` with nodes v: kept, skipped, or rejected.
+int take(Raw& r, int64_t type, const int64_t* v, int32_t phys) {
+  if (type == 4 || type == 5) {
+    if (r.vol_type && r.vol_type != type) return fail("tetrahedra and hexahedra in one mesh are not supported");
+    r.vol_type = static_cast<int>(type);
+    r.vol_nodes.insert(r.vol_nodes.end(), v, v + (type == 4 ? 4 : 8));
+    r.vol_phys.push_back(phys);
+  } else if (type == 2) {
+    r.tri_nodes.insert(r.tri_nodes.end(), v, v + 3);
+    r.tri_phys.push_back(phys);
+  } else if (type == 3) {
+    r.quad_nodes.insert(r.quad_nodes.end(), v, v + 4);
+    r.quad_phys.push_back(phys);
+  } else if (type == 11 || type == 29 || type == 30 || type == 31) {
+    return fail("higher-order tetrahedra are not TET4_EDGE meshes");
+  } else if (type == 12 || type == 17 || type == 92 || type == 93) {
+    return fail("higher-order hexahedra are not HEX8_EDGE meshes");
+  } else if (type == 6 || type == 7 || type == 13 || type == 14 || type == 18 || type == 19) {
+    return fail("prism and pyramid elements are not supported");
+  }
+  return EMG_SUCCESS;
+}
+
+// Nodes of Gmsh element types the reader has to step over.
+int node_count(int64_t type) {
+  switch (type) {
+    case 15: return 1;
+    case 1: return 2;
+    case 2: case 8: return 3;
+    case 3: case 4: return 4;
+    case 7: return 5;
+    case 6: case 9: return 6;
+    case 5: return 8;
+    case 16: return 8;
+    case 10: return 9;
+    case 11: return 10;
+    default: return -1;
+  }
 }
 
 int parse_v2(std::istream& in, Raw& r) {
@@ -76,20 +121,14 @@ int parse_v2(std::istream& in, Raw& r) {
     std::vector<int64_t> tags(ntags);
     for (auto& t : tags) ls >> t;
     const int32_t phys = ntags > 0 ? static_cast<int32_t>(tags[0]) : 0;
-    if (type == 4) {
-      int64_t v[4];
-      ls >> v[0] >> v[1] >> v[2] >> v[3];
-      if (!ls) return fail("bad tetrahedron line");
-      r.tet_nodes.insert(r.tet_nodes.end(), v, v + 4);
-      r.tet_phys.push_back(phys);
-    } else if (type == 2) {
-      int64_t v[3];
-      ls >> v[0] >> v[1] >> v[2];
-      if (!ls) return fail("bad triangle line");
-      r.tri_nodes.insert(r.tri_nodes.end(), v, v + 3);
-      r.tri_phys.push_back(phys);
-    } else if (type == 11 || type == 29 || type == 30 || type == 31) {
-      return fail("higher-order tetrahedra are not TET4_EDGE meshes");
+    if (type == 2 || type == 3 || type == 4 || type == 5) {
+      const int nv = node_count(type);
+      int64_t v[8];
+      for (int k = 0; k < nv; ++k) ls >> v[k];
+      if (!ls) return fail("bad element line");
+      if (int rc = take(r, type, v, phys)) return rc;
+    } else if (int rc = take(r, type, nullptr, phys)) {
+      return rc;
     }
   }
   return EMG_SUCCESS;
@@ -163,21 +202,15 @@ int parse_v4(std::istream& in, Raw& r) {
     in >> dim >> tag >> type >> cnt;
     const auto it = phys.find({dim, tag});
     const int32_t p = it == phys.end() ? 0 : it->second;
-    const int nv = type == 4 ? 4 : type == 2 ? 3 : type == 1 ? 2 : type == 15 ? 1 : type == 3 ? 4 : type == 5 ? 8 :
-                   type == 6 ? 6 : type == 7 ? 5 : type == 11 ? 10 : type == 9 ? 6 : type == 8 ? 3 : -1;
+    if (int rc = take(r, type == 2 || type == 3 || type == 4 || type == 5 ? 0 : type, nullptr, p)) return rc;
+    const int nv = node_count(type);
     if (nv < 0) return fail("unsupported element type " + std::to_string(type));
-    if (type == 11) return fail("higher-order tetrahedra are not TET4_EDGE meshes");
     for (int64_t i = 0; i < cnt; ++i) {
       int64_t id = 0, v[10];
       in >> id;
       for (int k = 0; k < nv; ++k) in >> v[k];
-      if (type == 4) {
-        r.tet_nodes.insert(r.tet_nodes.end(), v, v + 4);
-        r.tet_phys.push_back(p);
-      } else if (type == 2) {
-        r.tri_nodes.insert(r.tri_nodes.end(), v, v + 3);
-        r.tri_phys.push_back(p);
-      }
+      if (type == 2 || type == 3 || type == 4 || type == 5)
+        if (int rc = take(r, type, v, p)) return rc;
     }
   }
   if (!in) return fail("truncated $Elements");
@@ -200,7 +233,7 @@ int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_
   Raw r;
   int rc = version >= 4.0 ? parse_v4(in, r) : version >= 2.0 ? parse_v2(in, r) : fail("unsupported version");
   if (rc) return rc;
-  if (r.tet_phys.empty()) return fail("no 4-node tetrahedra");
+  if (r.vol_phys.empty()) return fail("no 4-node tetrahedra or 8-node hexahedra");
   // node index = rank of the tag
   std::vector<int64_t> order(r.node_tag.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int64_t>(i);
@@ -221,23 +254,27 @@ int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_
     out = it->second;
     return true;
   };
-  m.n_elems = static_cast<int64_t>(r.tet_phys.size());
-  m.elems.resize(4 * m.n_elems);
-  for (size_t i = 0; i < r.tet_nodes.size(); ++i)
-    if (!idx(r.tet_nodes[i], m.elems[i])) return fail("element references an unknown node");
-  material_tags = r.tet_phys;
+  const bool hex = r.vol_type == 5;
+  m.elem_type = hex ? EMG_ELEM_HEX8_EDGE : EMG_ELEM_TET4_EDGE;
+  const int npe = m.npe();
+  m.n_elems = static_cast<int64_t>(r.vol_phys.size());
+  m.elems.resize(npe * m.n_elems);
+  for (size_t i = 0; i < r.vol_nodes.size(); ++i)
+    if (!idx(r.vol_nodes[i], m.elems[i])) return fail("element references an unknown node");
+  material_tags = r.vol_phys;
   std::sort(material_tags.begin(), material_tags.end());
   material_tags.erase(std::unique(material_tags.begin(), material_tags.end()), material_tags.end());
   m.material.resize(m.n_elems);
   for (int64_t t = 0; t < m.n_elems; ++t)
-    m.material[t] = static_cast<int32_t>(std::lower_bound(material_tags.begin(), material_tags.end(), r.tet_phys[t]) -
+    m.material[t] = static_cast<int32_t>(std::lower_bound(material_tags.begin(), material_tags.end(), r.vol_phys[t]) -
                                          material_tags.begin());
-  // Dirichlet node pairs
-  auto add_face = [&](const int32_t* v) {
-    const int e[3][2] = {{0, 1}, {1, 2}, {0, 2}};
-    for (auto& p : e) {
-      m.dirichlet.push_back(v[p[0]]);
-      m.dirichlet.push_back(v[p[1]]);
+  // Dirichlet node pairs: a triangle's 3 corner pairs (0,1), (1,2), (0,2);
+  // a quadrangle's 4 sides from its corners in cyclic order (no diagonals)
+  auto add_face = [&](const int32_t* v, int nv) {
+    const int tri[3][2] = {{0, 1}, {1, 2}, {0, 2}};
+    for (int k = 0; k < nv; ++k) {
+      m.dirichlet.push_back(nv == 3 ? v[tri[k][0]] : v[k]);
+      m.dirichlet.push_back(nv == 3 ? v[tri[k][1]] : v[(k + 1) % nv]);
     }
   };
   if (n_tags > 0) {
@@ -248,25 +285,41 @@ int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_
       int32_t v[3];
       for (int k = 0; k < 3; ++k)
         if (!idx(r.tri_nodes[3 * f + k], v[k])) return fail("triangle references an unknown node");
-      add_face(v);
+      add_face(v, 3);
+    }
+    for (size_t f = 0; f < r.quad_phys.size(); ++f) {
+      if (!std::binary_search(want.begin(), want.end(), r.quad_phys[f])) continue;
+      int32_t v[4];
+      for (int k = 0; k < 4; ++k)
+        if (!idx(r.quad_nodes[4 * f + k], v[k])) return fail("quadrangle references an unknown node");
+      add_face(v, 4);
     }
   } else {
-    // faces of exactly one tetrahedron
-    std::vector<std::pair<std::array<int32_t, 3>, int64_t>> faces;
-    faces.reserve(4 * m.n_elems);
-    const int tf[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    // faces of exactly one volume element, corners in cyclic order
+    // (ElementGeometry's TET4 / HEX8 faces, element_geometry.cpp:112-181)
+    const int tf[4][4] = {{0, 1, 2, -1}, {0, 1, 3, -1}, {0, 2, 3, -1}, {1, 2, 3, -1}};
+    const int hf[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {2, 3, 7, 6}, {0, 3, 7, 4}, {1, 2, 6, 5}};
+    const int nf = hex ? 6 : 4, nv = hex ? 4 : 3;
+    struct Face {
+      std::array<int32_t, 4> key;  // sorted corners (-1 padded)
+      std::array<int32_t, 4> cyc;  // corners in cyclic order
+    };
+    std::vector<Face> faces;
+    faces.reserve(static_cast<size_t>(nf) * m.n_elems);
     for (int64_t t = 0; t < m.n_elems; ++t)
-      for (auto& f : tf) {
-        std::array<int32_t, 3> k = {m.elems[4 * t + f[0]], m.elems[4 * t + f[1]], m.elems[4 * t + f[2]]};
-        std::sort(k.begin(), k.end());
-        faces.push_back({k, t});
+      for (int f = 0; f < nf; ++f) {
+        Face fc;
+        fc.cyc = {-1, -1, -1, -1};
+        for (int k = 0; k < nv; ++k) fc.cyc[k] = m.elems[npe * t + (hex ? hf[f][k] : tf[f][k])];
+        fc.key = fc.cyc;
+        std::sort(fc.key.begin(), fc.key.begin() + nv);
+        faces.push_back(fc);
       }
-    std::sort(faces.begin(), faces.end(),
-              [](const auto& x, const auto& y) { return x.first < y.first; });
+    std::sort(faces.begin(), faces.end(), [](const Face& x, const Face& y) { return x.key < y.key; });
     for (size_t i = 0; i < faces.size();) {
       size_t j = i;
-      while (j < faces.size() && faces[j].first == faces[i].first) ++j;
-      if (j - i == 1) add_face(faces[i].first.data());
+      while (j < faces.size() && faces[j].key == faces[i].key) ++j;
+      if (j - i == 1) add_face(nv == 3 ? faces[i].key.data() : faces[i].cyc.data(), nv);
       i = j;
     }
   }

@@ -238,15 +238,28 @@ def perturbed(m: CubeMesh, amplitude: float = 0.2, seed: int = 0) -> CubeMesh:
     return CubeMesh(**{**m.__dict__, "xyz": xyz, "name": m.name + f"_perturbed{seed}"})
 
 
+HEX_FACES = np.array([[0, 1, 2, 3], [4, 5, 6, 7], [0, 1, 5, 4], [2, 3, 7, 6], [0, 3, 7, 4], [1, 2, 6, 5]])
+
+
 def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2), boundary_tag: int = 100):
     """Write the mesh as an ASCII Gmsh file (2.2 or 4.1): node tags 1..V,
-    the tetrahedra with physical tag volume_tags[material], and every
-    boundary face as a triangle with physical tag `boundary_tag`."""
+    the tetrahedra (type 4) or hexahedra (type 5) with physical tag
+    volume_tags[material], and every boundary face as a triangle (type 2) or
+    a quadrangle (type 3, corners in cyclic order) with physical tag
+    `boundary_tag`."""
     tets = np.asarray(m.tets, np.int64)
-    faces = np.sort(tets[:, [[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]]].reshape(-1, 3), axis=1)
-    uf, cnt = np.unique(faces, axis=0, return_counts=True)
-    bfaces = uf[cnt == 1]
+    hexa = tets.shape[1] == 8
+    if hexa:
+        cyc = tets[:, HEX_FACES].reshape(-1, 4)
+        _, first, cnt = np.unique(np.sort(cyc, axis=1), axis=0, return_index=True, return_counts=True)
+        bfaces = cyc[np.sort(first[cnt == 1])]
+    else:
+        faces = np.sort(tets[:, [[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]]].reshape(-1, 3), axis=1)
+        uf, cnt = np.unique(faces, axis=0, return_counts=True)
+        bfaces = uf[cnt == 1]
+    ftype, vtype = (3, 5) if hexa else (2, 4)
     vt = np.asarray(volume_tags)[np.asarray(m.material)]
+    nodes = lambda row: " ".join(str(int(v) + 1) for v in row)
     with open(path, "w") as f:
         if version.startswith("2"):
             f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % m.n_nodes)
@@ -254,11 +267,11 @@ def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2),
                 f.write(f"{i + 1} {float(x)!r} {float(y)!r} {float(z)!r}\n")
             f.write("$EndNodes\n$Elements\n%d\n" % (len(bfaces) + len(tets)))
             eid = 1
-            for a, b, c in bfaces:
-                f.write(f"{eid} 2 2 {boundary_tag} 1 {a + 1} {b + 1} {c + 1}\n")
+            for fc in bfaces:
+                f.write(f"{eid} {ftype} 2 {boundary_tag} 1 {nodes(fc)}\n")
                 eid += 1
             for t, tag in zip(tets, vt):
-                f.write(f"{eid} 4 2 {int(tag)} {int(tag)} {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
+                f.write(f"{eid} {vtype} 2 {int(tag)} {int(tag)} {nodes(t)}\n")
                 eid += 1
             f.write("$EndElements\n")
         else:
@@ -273,15 +286,15 @@ def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2),
             f.write("$EndNodes\n$Elements\n%d %d 1 %d\n" % (1 + len(vols), len(bfaces) + len(tets),
                                                            len(bfaces) + len(tets)))
             eid = 1
-            f.write(f"2 1 2 {len(bfaces)}\n")
-            for a, b, c in bfaces:
-                f.write(f"{eid} {a + 1} {b + 1} {c + 1}\n")
+            f.write(f"2 1 {ftype} {len(bfaces)}\n")
+            for fc in bfaces:
+                f.write(f"{eid} {nodes(fc)}\n")
                 eid += 1
             for v in vols:
                 sel = tets[vt == v]
-                f.write(f"3 {v} 4 {len(sel)}\n")
+                f.write(f"3 {v} {vtype} {len(sel)}\n")
                 for t in sel:
-                    f.write(f"{eid} {t[0] + 1} {t[1] + 1} {t[2] + 1} {t[3] + 1}\n")
+                    f.write(f"{eid} {nodes(t)}\n")
                     eid += 1
             f.write("$EndElements\n")
 
@@ -301,8 +314,10 @@ def read_gmsh(path: str, dirichlet_tags=None, nu=None, sigma=None, sources=None)
     try:
         nn, nt, nd, nm = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
         L.emg_mesh_info(h, C.byref(nn), C.byref(nt), C.byref(nd), C.byref(nm))
+        npe = C.c_int32()
+        L.emg_mesh_elem_type(h, None, C.byref(npe), None)
         xyz = np.empty((nn.value, 3))
-        tets = np.empty((nt.value, 4), np.int32)
+        tets = np.empty((nt.value, npe.value), np.int32)
         mat = np.empty(nt.value, np.int32)
         dp = np.empty((nd.value, 2), np.int32)
         L.emg_mesh_export(h, _abi.ptr(xyz), _abi.ptr(tets), _abi.ptr(mat), _abi.ptr(dp))

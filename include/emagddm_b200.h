@@ -126,12 +126,15 @@ int emg_mesh_elem_type(emg_mesh mesh, int32_t* elem_type, int32_t* nodes_per_ele
 void emg_mesh_destroy(emg_mesh mesh);
 /* Gmsh ASCII mesh (format 2.2 or 4.1; the reference's planned mesh format,
  * mesh/README.md) as an EMMeshData (include/fe_em/em_mesh_data.hpp:90-230):
- * nodes in ascending Gmsh tag order, the 4-node tetrahedra (type 4) in file
- * order with material id = rank of their physical tag among the tetrahedra's
- * distinct physical tags, Dirichlet node pairs = edges of the triangles whose
- * physical tag is in dirichlet_tags, or of every boundary face (a face of one
- * tetrahedron) when n_tags == 0.  Binary files and higher-order tetrahedra are
- * rejected with EMG_INVALID_INPUT. */
+ * nodes in ascending Gmsh tag order, the 4-node tetrahedra (type 4) or the
+ * 8-node hexahedra (type 5; one volume type per file; emg_mesh_elem_type
+ * tells which) in file order with material id = rank of their physical tag
+ * among the volume elements' distinct physical tags, Dirichlet node pairs =
+ * edges of the triangles / quadrangles (types 2 / 3) whose physical tag is in
+ * dirichlet_tags, or of every boundary face (a face of one volume element)
+ * when n_tags == 0.  Binary files, mixed tetrahedra and hexahedra,
+ * higher-order, prism and pyramid volumes are rejected with
+ * EMG_INVALID_INPUT. */
 int emg_mesh_read_gmsh(const char* path, const int32_t* dirichlet_tags, int32_t n_tags, emg_mesh* out);
 /* Sizes of a mesh handle; any pointer may be NULL. */
 int emg_mesh_info(emg_mesh mesh, int64_t* n_nodes, int64_t* n_tets, int64_t* n_dirichlet_pairs,
