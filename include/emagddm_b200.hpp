@@ -39,34 +39,41 @@ struct SolverResult {
 
 inline std::string last_error() { return emg_last_error(); }
 
-// fe_em::EMMeshData restricted to the edge path: nodes (id = index), TET4_EDGE
-// elements with material ids, Dirichlet edge node pairs, hole-marker count.
+// fe_em::EMMeshData restricted to the edge path: nodes (id = index), elements
+// of one type (TET4_EDGE: 4 nodes each, HEX8_EDGE: 8) with material ids,
+// Dirichlet edge node pairs, hole-marker count.
 class Mesh {
  public:
-  Mesh(std::vector<double> xyz, std::vector<int32_t> tets, std::vector<int32_t> material,
-       std::vector<int32_t> dirichlet_pairs, int32_t n_hole_markers = 0)
-      : xyz_(std::move(xyz)), tets_(std::move(tets)), material_(std::move(material)) {
-    const int rc = emg_mesh_create(static_cast<int64_t>(xyz_.size() / 3), xyz_.data(),
-                                   static_cast<int64_t>(tets_.size() / 4), tets_.data(),
-                                   material_.empty() ? nullptr : material_.data(),
-                                   static_cast<int64_t>(dirichlet_pairs.size() / 2),
-                                   dirichlet_pairs.empty() ? nullptr : dirichlet_pairs.data(),
-                                   n_hole_markers, &h_);
-    if (rc != EMG_SUCCESS) throw std::invalid_argument("emg_mesh_create: " + last_error());
+  Mesh(std::vector<double> xyz, std::vector<int32_t> elems, std::vector<int32_t> material,
+       std::vector<int32_t> dirichlet_pairs, int32_t n_hole_markers = 0,
+       int32_t elem_type = EMG_ELEM_TET4_EDGE)
+      : xyz_(std::move(xyz)), elems_(std::move(elems)), material_(std::move(material)), type_(elem_type) {
+    const int rc = emg_mesh_create_typed(type_, static_cast<int64_t>(xyz_.size() / 3), xyz_.data(),
+                                         getElementCount(), elems_.data(),
+                                         material_.empty() ? nullptr : material_.data(),
+                                         static_cast<int64_t>(dirichlet_pairs.size() / 2),
+                                         dirichlet_pairs.empty() ? nullptr : dirichlet_pairs.data(),
+                                         n_hole_markers, &h_);
+    if (rc != EMG_SUCCESS) throw std::invalid_argument("emg_mesh_create_typed: " + last_error());
   }
   ~Mesh() { emg_mesh_destroy(h_); }
   Mesh(const Mesh&) = delete;
   Mesh& operator=(const Mesh&) = delete;
   emg_mesh handle() const { return h_; }
+  int32_t elementType() const { return type_; }
+  int nodesPerElement() const { return type_ == EMG_ELEM_HEX8_EDGE ? 8 : 4; }
+  int edgesPerElement() const { return type_ == EMG_ELEM_HEX8_EDGE ? 12 : 6; }
   int64_t getNodeCount() const { return static_cast<int64_t>(xyz_.size() / 3); }
-  int64_t getElementCount() const { return static_cast<int64_t>(tets_.size() / 4); }
+  int64_t getElementCount() const { return static_cast<int64_t>(elems_.size() / nodesPerElement()); }
   const std::vector<double>& xyz() const { return xyz_; }
-  const std::vector<int32_t>& tets() const { return tets_; }
+  const std::vector<int32_t>& elements() const { return elems_; }
+  const std::vector<int32_t>& tets() const { return elems_; }  // TET4_EDGE meshes
   const std::vector<int32_t>& material() const { return material_; }
 
  private:
   std::vector<double> xyz_;
-  std::vector<int32_t> tets_, material_;
+  std::vector<int32_t> elems_, material_;
+  int32_t type_ = EMG_ELEM_TET4_EDGE;
   emg_mesh h_ = nullptr;
 };
 
@@ -78,12 +85,13 @@ class GlobalEdgeIDGenerator {
     int64_t n = 0;
     if (emg_edge_ids(mesh_.handle(), nullptr, nullptr, &n) != EMG_SUCCESS)
       throw std::invalid_argument("GlobalEdgeIDGenerator::generate: " + last_error());
-    elem_edge_.resize(6 * mesh_.getElementCount());
+    elem_edge_.resize(mesh_.edgesPerElement() * mesh_.getElementCount());
     edge_nodes_.resize(2 * n);
     emg_edge_ids(mesh_.handle(), elem_edge_.data(), edge_nodes_.data(), &n);
   }
   int getNumGlobalEdges() const { return static_cast<int>(edge_nodes_.size() / 2); }
-  // element-major, 6 local edges per element (ElementGeometry TET4 order)
+  // element-major, 6 (TET4) or 12 (HEX8) local edges per element in
+  // ElementGeometry's order
   const std::vector<int32_t>& getElemLocalToGlobalEdge() const { return elem_edge_; }
   const std::vector<int32_t>& getEdgeNodes() const { return edge_nodes_; }
 
@@ -100,7 +108,7 @@ class EMDOFManager {
   EMDOFManager(const EMDOFManager&) = delete;
   EMDOFManager& operator=(const EMDOFManager&) = delete;
   void build() { run(EMG_GAUGE_NONE); gauged_ = false; }
-  // Tree gauge for a partition of the tets (FETI-DP); replaces any gauge.
+  // Tree gauge for a partition of the elements (FETI-DP); replaces any gauge.
   void applyPartitionedGauge(const std::vector<int32_t>& tet_part, int32_t n_parts) {
     emg_dofmap m = nullptr;
     if (emg_dof_build_partitioned(mesh_.handle(), tet_part.data(), n_parts, &m) != EMG_SUCCESS)
@@ -137,7 +145,7 @@ class EMDOFManager {
     map_ = m;
     int64_t ne = 0, nf = 0;
     emg_dofmap_info(map_, &ne, &nf, &n_dofs_);
-    l2g_.resize(6 * mesh_.getElementCount());
+    l2g_.resize(mesh_.edgesPerElement() * mesh_.getElementCount());
     edge_dof_.resize(ne);
     emg_dofmap_export(map_, l2g_.data(), edge_dof_.data());
   }
@@ -148,7 +156,7 @@ class EMDOFManager {
   std::vector<int32_t> l2g_, edge_dof_;
 };
 
-// numeric::EMAssembly for TET4_EDGE on the GPU (src/numeric/em_assembly.cpp:144-420).
+// numeric::EMAssembly for TET4_EDGE / HEX8_EDGE on the GPU (src/numeric/em_assembly.cpp:144-420).
 // Materials are reluctivity nu = 1/mu and conductivity sigma per material id.
 class GpuEMAssembly {
  public:
@@ -158,9 +166,10 @@ class GpuEMAssembly {
                 const std::vector<emg_source>& sources = {}, bool is_transient = false,
                 int32_t flags = 0) {
     clear();
-    int rc = emg_system_create(mesh.getNodeCount(), mesh.xyz().data(), mesh.getElementCount(),
-                               mesh.tets().data(), mesh.material().empty() ? nullptr : mesh.material().data(),
-                               elem_local_to_global.data(), 0, nullptr, &sys_);
+    int rc = emg_system_create_typed(mesh.elementType(), mesh.getNodeCount(), mesh.xyz().data(),
+                                     mesh.getElementCount(), mesh.elements().data(),
+                                     mesh.material().empty() ? nullptr : mesh.material().data(),
+                                     elem_local_to_global.data(), 0, 0, nullptr, &sys_);
     if (rc == EMG_SUCCESS)
       rc = emg_system_assemble(sys_, nu.data(), sigma.empty() ? nullptr : sigma.data(),
                                static_cast<int32_t>(nu.size()), sources.empty() ? nullptr : sources.data(),

@@ -3,8 +3,12 @@
 // reference caller would write it:
 //   GlobalEdgeIDGenerator -> EMDOFManager::build/applyTreeGauge
 //   -> GpuEMAssembly::assemble -> GpuCGSolver::set_matrix/solve,
-// or (--direct) the GPU direct backend on the same gauged system.
-// Usage: solve_cube <n> [--numbering-only] [--direct] [--x out.bin]
+// or (--direct) the GPU direct backend on the same gauged system.  --hex keeps
+// the hexes as HEX8_EDGE elements; --wiggle moves every interior node by
+// 0.2 h sin(...) per coordinate (a deterministic non-affine geometry) and
+// --xyz writes the node coordinates used.
+// Usage: solve_cube <n> [--numbering-only] [--direct] [--hex] [--wiggle]
+//                       [--x out.bin] [--xyz out.bin]
 // Prints one line of key=value pairs.
 #include <cmath>
 #include <cstdio>
@@ -16,41 +20,62 @@
 
 int main(int argc, char** argv) {
   const int n = argc > 1 ? std::atoi(argv[1]) : 4;
-  bool numbering_only = false, direct = false;
+  bool numbering_only = false, direct = false, hex = false, wiggle = false;
   const char* xout = nullptr;
+  const char* xyzout = nullptr;
   for (int i = 2; i < argc; ++i) {
     if (!std::strcmp(argv[i], "--numbering-only")) numbering_only = true;
     if (!std::strcmp(argv[i], "--direct")) direct = true;
+    if (!std::strcmp(argv[i], "--hex")) hex = true;
+    if (!std::strcmp(argv[i], "--wiggle")) wiggle = true;
     if (!std::strcmp(argv[i], "--x") && i + 1 < argc) xout = argv[++i];
+    if (!std::strcmp(argv[i], "--xyz") && i + 1 < argc) xyzout = argv[++i];
   }
   const int n1 = n + 1;
   std::vector<double> xyz;
   for (int k = 0; k < n1; ++k)
     for (int j = 0; j < n1; ++j)
       for (int i = 0; i < n1; ++i) {
-        xyz.push_back(double(i) / n);
-        xyz.push_back(double(j) / n);
-        xyz.push_back(double(k) / n);
+        const bool interior = i > 0 && i < n && j > 0 && j < n && k > 0 && k < n;
+        const double h = 0.2 / n, w = wiggle && interior ? 1.0 : 0.0;
+        xyz.push_back(double(i) / n + w * h * std::sin(1.3 * i + 2.1 * j + 0.7 * k));
+        xyz.push_back(double(j) / n + w * h * std::sin(0.4 * i + 1.7 * j + 2.9 * k));
+        xyz.push_back(double(k) / n + w * h * std::sin(2.3 * i + 0.9 * j + 1.1 * k));
       }
+  if (xyzout) {
+    FILE* f = std::fopen(xyzout, "wb");
+    if (f) {
+      std::fwrite(xyz.data(), sizeof(double), xyz.size(), f);
+      std::fclose(f);
+    }
+  }
   auto gid = [&](int i, int j, int k) { return i + n1 * (j + n1 * k); };
   const int kuhn[6][4] = {{0, 1, 2, 6}, {0, 2, 3, 6}, {0, 3, 7, 6}, {0, 7, 4, 6}, {0, 4, 5, 6}, {0, 5, 1, 6}};
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
   std::vector<int32_t> tets;
   for (int k = 0; k < n; ++k)
     for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i)
+      for (int i = 0; i < n; ++i) {
+        if (hex) {
+          for (auto& o : off) tets.push_back(gid(i + o[0], j + o[1], k + o[2]));
+          continue;
+        }
         for (auto& t : kuhn)
           for (int a = 0; a < 4; ++a) {
             const int* o = off[t[a]];
             tets.push_back(gid(i + o[0], j + o[1], k + o[2]));
           }
+      }
   // Dirichlet: every element edge lying in a boundary face (duplicates are fine)
   const int ge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  const int he[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  const int npe = hex ? 8 : 4, epe = hex ? 12 : 6;
   std::vector<int32_t> dir;
   auto coord = [&](int g, int c) { return c == 0 ? g % n1 : c == 1 ? (g / n1) % n1 : g / (n1 * n1); };
-  for (size_t t = 0; t < tets.size() / 4; ++t)
-    for (auto& e : ge) {
-      const int a = tets[4 * t + e[0]], b = tets[4 * t + e[1]];
+  for (size_t t = 0; t < tets.size() / npe; ++t)
+    for (int q = 0; q < epe; ++q) {
+      const int* e = hex ? he[q] : ge[q];
+      const int a = tets[npe * t + e[0]], b = tets[npe * t + e[1]];
       for (int c = 0; c < 3; ++c)
         if (coord(a, c) == coord(b, c) && (coord(a, c) == 0 || coord(a, c) == n)) {
           dir.push_back(a);
@@ -58,7 +83,8 @@ int main(int argc, char** argv) {
           break;
         }
     }
-  emg::Mesh mesh(xyz, tets, std::vector<int32_t>(tets.size() / 4, 0), dir);
+  emg::Mesh mesh(xyz, tets, std::vector<int32_t>(tets.size() / npe, 0), dir, 0,
+                 hex ? EMG_ELEM_HEX8_EDGE : EMG_ELEM_TET4_EDGE);
   emg::GlobalEdgeIDGenerator gen(mesh);
   gen.generate();
   emg::EMDOFManager dofs(mesh);

@@ -63,3 +63,36 @@ def test_cpp_direct_backend_matches_oracle(tmp_path):
     xo, st, it, res = O.pcg(rp, col, kv_, rhs, tol=1e-12, max_iter=10000, precond=1)
     x = np.fromfile(xfile, dtype=np.float64)
     assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("n", [2, 3, 5])
+def test_cpp_hex_numbering_matches_oracle(n):
+    rc, kv = run(n, "--numbering-only", "--hex")
+    assert rc == 0
+    xyz, hexes, d = mesh.hex_topology(n)
+    o = O.dof_build(hexes, d, gauge=O.GAUGE_REF)
+    assert int(kv["edges"]) == o["n_edges"]
+    assert int(kv["free"]) == o["n_free"]
+    assert int(kv["dofs"]) == o["n_dofs"]
+    assert int(kv["l2g_sum"]) == int(o["l2g"].astype(np.int64).sum())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("direct", [False, True])
+def test_cpp_hex_chain_matches_oracle(tmp_path, direct):
+    """HEX8_EDGE through the C++ adapters on a non-affine (wiggled) grid."""
+    n = 6
+    xfile, gfile = tmp_path / "x.bin", tmp_path / "xyz.bin"
+    args = [n, "--hex", "--wiggle", "--x", xfile, "--xyz", gfile] + (["--direct"] if direct else [])
+    rc, kv = run(*args)
+    assert rc == 0, kv
+    _, hexes, d = mesh.hex_topology(n)
+    xyz = np.fromfile(gfile, dtype=np.float64).reshape(-1, 3)
+    m = mesh.CubeMesh(n=n, xyz=xyz, tets=hexes, material=np.zeros(len(hexes), np.int32), dirichlet=d,
+                      nu=np.array([1.0]), sigma=np.array([0.0]), sources=mesh.plain_small(n).sources)
+    o = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
+    rp, col, kv_, _, rhs = O.assemble(m, o["l2g"], o["n_dofs"])
+    assert np.abs(rhs).max() > 1e-6
+    xo, st, it, res = O.pcg(rp, col, kv_, rhs, tol=1e-12, max_iter=20000, precond=1)
+    x = np.fromfile(xfile, dtype=np.float64)
+    assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
