@@ -8,8 +8,8 @@ gauge (bit-exact numbering), FP64 assembly on the GPU (CSR pattern + K + F),
 then Jacobi-PCG to a relative residual of 1e-8.  The edge numbering / gauge is
 host integer setup done once per mesh (reported as setup_dof_ms).
 
-`value` times the step with inputs resident in HBM (emg_system_create_device
-+ emg_system_assemble + emg_system_solve); `e2e` times the same C-ABI calls
+`value` times the step with inputs resident in HBM (emg_system_create_typed on
+device arrays + emg_system_assemble + emg_system_solve); `e2e` times the same C-ABI calls
 with pinned host buffers (geometry and DOF map copied in, solution copied
 out).
 Both in solves/s; ms_per_step is the time to a 1e-8 residual.
@@ -47,11 +47,13 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="iterations in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline (profiling runs)")
-    ap.add_argument("--workload", default="cube64", choices=["cube64", "batch512", "fetidp64", "learned64"],
+    ap.add_argument("--workload", default="cube64",
+                    choices=["cube64", "hex64", "batch512", "fetidp64", "learned64"],
                     help="cube64: the plain method at scale (default line); batch512: 512 "
                          "independent 8^3..32^3 instances solved in one lockstep device loop; "
                          "fetidp64: the 64^3 problem split into 64 jittered box subdomains, "
-                         "FETI-DP (factor + solve) next to plain PCG on the same gauged system")
+                         "FETI-DP (factor + solve) next to plain PCG on the same gauged system; "
+                         "hex64: the cube64 physics on 64^3 perturbed HEX8_EDGE elements")
     ap.add_argument("--parts", type=int, default=4, help="fetidp64: subdomains per axis")
     ap.add_argument("--train-fields", type=int, default=200, help="learned64: training fields (seeds 1000+)")
     ap.add_argument("--eval-fields", type=int, default=50, help="learned64: held-out fields (seeds 2000+)")
@@ -64,17 +66,31 @@ def parse():
     return ap.parse_args()
 
 
-def workload(n):
+HEX_AMPLITUDE = 0.2  # hex64: interior nodes moved by up to 0.2 cell widths (seeded)
+
+
+def workload(n, kind="cube64"):
     from emagddm_b200 import mesh
+    if kind == "hex64":
+        # On the unperturbed grid the ref tree takes every z-directed edge and
+        # the z-directed coil current leaves F = 0; perturbed geometry keeps it.
+        return mesh.perturbed(mesh.hex_scale(n), amplitude=HEX_AMPLITUDE, seed=n)
     return mesh.plain_scale(n)
 
 
-def workload_config(n, n_dofs=None, nnz=None):
-    cfg = {"workload": f"cube{n}_iron_coil: {n}^3 hex x 6 TET4_EDGE ({6 * n ** 3} tets), mu_r 1000 "
-                       f"block, annulus coil J_z, ref tree gauge, FP64 GPU assembly + Jacobi-PCG "
-                       f"to 1e-8",
-           "n": n, "tets": 6 * n ** 3, "gauge": "ref", "tol": TOL, "precond": "jacobi",
-           "l2": "inputs larger than L2 (CSR values+indices > 126 MB), no flush"}
+def workload_config(n, n_dofs=None, nnz=None, kind="cube64"):
+    if kind == "hex64":
+        cfg = {"workload": f"hex{n}_iron_coil: {n}^3 HEX8_EDGE elements, interior nodes perturbed by up to "
+                           f"{HEX_AMPLITUDE} cell (seed {n}), mu_r 1000 block, annulus coil J_z, ref tree gauge, "
+                           f"FP64 GPU assembly (2x2x2 Gauss) + Jacobi-PCG to 1e-8",
+               "n": n, "hexes": n ** 3, "gauge": "ref", "tol": TOL, "precond": "jacobi",
+               "l2": "inputs larger than L2 (CSR values+indices > 126 MB), no flush"}
+    else:
+        cfg = {"workload": f"cube{n}_iron_coil: {n}^3 hex x 6 TET4_EDGE ({6 * n ** 3} tets), mu_r 1000 "
+                           f"block, annulus coil J_z, ref tree gauge, FP64 GPU assembly + Jacobi-PCG "
+                           f"to 1e-8",
+               "n": n, "tets": 6 * n ** 3, "gauge": "ref", "tol": TOL, "precond": "jacobi",
+               "l2": "inputs larger than L2 (CSR values+indices > 126 MB), no flush"}
     if n_dofs is not None:
         cfg["dofs"] = int(n_dofs)
     if nnz is not None:
@@ -157,7 +173,8 @@ def run_ours(args, rank, world, local_rank):
     L = _abi.lib()
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    m = workload(args.n)
+    m = workload(args.n, args.workload)
+    et = m.elem_type
     md = api.EMMeshData.from_cube(m)
     t0 = time.perf_counter()
     dm = api.EMDOFManager(md)
@@ -188,9 +205,9 @@ def run_ours(args, rank, world, local_rank):
 
     if args.kernels_only:
         h = C.c_void_p()
-        _abi.check(L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
-                                              C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
-                                              C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h)), "create")
+        _abi.check(L.emg_system_create_typed(et, xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                             C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                             C.c_void_p(d_l2g.data_ptr()), n_dofs, 1, sp, C.byref(h)), "create")
         _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
                    "assemble")
         kt = (C.c_double * 3)()
@@ -202,12 +219,12 @@ def run_ours(args, rank, world, local_rank):
     def step(resident: bool):
         h = C.c_void_p()
         if resident:
-            rc = L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
-                                            C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
-                                            C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h))
+            rc = L.emg_system_create_typed(et, xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                           C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                           C.c_void_p(d_l2g.data_ptr()), n_dofs, 1, sp, C.byref(h))
         else:
-            rc = L.emg_system_create(p_xyz.shape[0], _abi.ptr(p_xyz), p_tets.shape[0], _abi.ptr(p_tets),
-                                     _abi.ptr(p_mat), _abi.ptr(p_l2g), n_dofs, sp, C.byref(h))
+            rc = L.emg_system_create_typed(et, p_xyz.shape[0], _abi.ptr(p_xyz), p_tets.shape[0], _abi.ptr(p_tets),
+                                           _abi.ptr(p_mat), _abi.ptr(p_l2g), n_dofs, 0, sp, C.byref(h))
         _abi.check(rc, "emg_system_create")
         _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
                    "emg_system_assemble")
@@ -227,18 +244,21 @@ def run_ours(args, rank, world, local_rank):
         info["solve_ms"] = out.solve_time_ms
         L.emg_system_destroy(h)
 
+    step_ms = {}
+
     def timed(resident, k, w):
         for _ in range(w):
             step(resident)
         barrier()
         torch.cuda.synchronize(dev)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(k):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
+        ev[0].record(stream)
+        for i in range(k):
             step(resident)
-        e1.record(stream)
+            ev[i + 1].record(stream)
         torch.cuda.synchronize(dev)
-        ms = e0.elapsed_time(e1)
+        step_ms["resident" if resident else "e2e"] = [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(k)]
+        ms = ev[0].elapsed_time(ev[k])
         return max_over_ranks(ms)
 
     def barrier():
@@ -257,14 +277,14 @@ def run_ours(args, rank, world, local_rank):
     with Clocks(local_rank) as clk:
         total_ms = timed(True, args.steps, args.warmup)
     iters = info["iters"]
-    total_e2e = timed(False, args.steps, 1)
+    total_e2e = timed(False, args.steps, args.warmup)
     e2e_iters = info["iters"]
 
     # roofline of the dominant kernel (SpMV + p.q of CG), live CUDA-event times
     h = C.c_void_p()
-    _abi.check(L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
-                                          C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
-                                          C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h)), "create")
+    _abi.check(L.emg_system_create_typed(et, xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                                         C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                                         C.c_void_p(d_l2g.data_ptr()), n_dofs, 1, sp, C.byref(h)), "create")
     _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp), "asm")
     kt = (C.c_double * 3)()
     Kh = L.emg_system_matrix(h, 0)
@@ -277,9 +297,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
     h = C.c_void_p()
-    L.emg_system_create_device(xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
-                               C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
-                               C.c_void_p(d_l2g.data_ptr()), n_dofs, sp, C.byref(h))
+    L.emg_system_create_typed(et, xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
+                              C.c_void_p(d_tets.data_ptr()), C.c_void_p(d_mat.data_ptr()),
+                              C.c_void_p(d_l2g.data_ptr()), n_dofs, 1, sp, C.byref(h))
     torch.cuda.synchronize(dev)
     phases["create_symbolic"] = (time.perf_counter() - t) * 1e3
     t = time.perf_counter()
@@ -312,13 +332,15 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seedless structured cube mesh; iron block + annulus coil)",
-        "config": {**workload_config(args.n, n_dofs, nnz), "parallelism": f"replicas{world}",
+        "data": ("synthetic (structured hex grid, interior nodes perturbed, seed n; iron block + annulus coil)"
+                 if args.workload == "hex64" else
+                 "synthetic (seedless structured cube mesh; iron block + annulus coil)"),
+        "config": {**workload_config(args.n, n_dofs, nnz, args.workload), "parallelism": f"replicas{world}",
                    "pcg_iterations": iters, "final_residual": info["res"],
                    "setup_dof_ms": setup_dof_ms,
                    "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]},
                    "cg_iteration_ms_kernels": it_ms,
-                   "solve_ms": info["solve_ms"], "phase_ms": phases,
+                   "solve_ms": info["solve_ms"], "phase_ms": phases, "step_ms": step_ms,
                    "solver_format": {"kind": "SELL-32-sigma4096", "slots": slots.value,
                                      "padding": slots.value / nnz - 1.0}},
         "clocks": clk.summary(),

@@ -5,9 +5,10 @@
 // Symbolic phase (once per mesh + DOF map):
 //   k_count_rows / scan / k_fill_incidence / k_sort_incidence build, for every
 //   equation row r, the sorted list of (element, local edge) slots that map to r;
-//   k_row_pattern (count, scan, write) turns those lists into the merged CSR
-//   pattern with ascending columns -- the pattern SparseConverter::to_eigen
-//   produces from the reference's unmerged CSR (sparse_converter.cpp:19-80).
+//   k_row_unique (sorted distinct columns of each row into scratch, counts),
+//   a scan and k_row_columns turn those lists into the merged CSR pattern with
+//   ascending columns -- the pattern SparseConverter::to_eigen produces from
+//   the reference's unmerged CSR (sparse_converter.cpp:19-80).
 // Numeric phase:
 //   k_assemble_rows (tets) / k_assemble_rows_hex gather, for each row, the
 //   contributions of its incident elements in ascending element order and
@@ -148,31 +149,81 @@ __global__ void k_sort_incidence(const int32_t* __restrict__ inc_ptr, int32_t* _
   }
 }
 
-// Warp per row: candidate columns of all incident elements -> distinct,
-// ranked.  epe = edges per element (slot = epe * element + local edge).
-// write == false: counts[r] = number of distinct columns.
-// write == true : col[row_ptr[r] + rank] = column.
-template <bool kWrite>
-__global__ void __launch_bounds__(128) k_row_pattern(int64_t n, int epe, const int32_t* __restrict__ inc_ptr,
-                                                     const int32_t* __restrict__ inc,
-                                                     const int32_t* __restrict__ l2g,
-                                                     int32_t* __restrict__ counts,
-                                                     const int32_t* __restrict__ row_ptr,
-                                                     int32_t* __restrict__ col,
-                                                     int32_t* __restrict__ err) {
+// Sorts the 64 values v0 (index lane) and v1 (index lane + 32) of a warp
+// ascending with a bitonic network in registers.
+__device__ __forceinline__ void warp_sort64(int32_t& v0, int32_t& v1) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32) {  // pairs (lane, lane + 32), k == 64: ascending
+        const int32_t lo = min(v0, v1), hi = max(v0, v1);
+        v0 = lo;
+        v1 = hi;
+      } else {
+        const int32_t p0 = __shfl_xor_sync(0xffffffffu, v0, j);
+        const int32_t p1 = __shfl_xor_sync(0xffffffffu, v1, j);
+        const bool lower = (lane & j) == 0;
+        const bool up0 = (lane & k) == 0, up1 = ((lane + 32) & k) == 0;
+        v0 = (lower == up0) ? min(v0, p0) : max(v0, p0);
+        v1 = (lower == up1) ? min(v1, p1) : max(v1, p1);
+      }
+    }
+  }
+}
+
+// Warp per row: the distinct columns of all incident elements (slot = epe *
+// element + local edge), ascending, into tmp[inc_ptr[r] * epe ...] (room for
+// every candidate of the row), and their count into counts[r].  Rows of up to
+// 64 candidates are sorted in registers; longer rows (up to kPatternCap) go
+// through shared memory.
+__global__ void __launch_bounds__(128) k_row_unique(int64_t n, int epe, const int32_t* __restrict__ inc_ptr,
+                                                    const int32_t* __restrict__ inc,
+                                                    const int32_t* __restrict__ l2g,
+                                                    int32_t* __restrict__ counts, int32_t* __restrict__ tmp,
+                                                    int32_t* __restrict__ err) {
   __shared__ int32_t cand_all[4][kPatternCap];
   __shared__ uint8_t first_all[4][kPatternCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   int32_t* cand = cand_all[wib];
   uint8_t* first = first_all[wib];
+  const unsigned lt = (1u << lane) - 1u;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + wib; r < n; r += warps) {
     const int32_t a = inc_ptr[r], b = inc_ptr[r + 1];
     const int m = epe * (b - a);
+    int32_t* out = tmp + static_cast<int64_t>(a) * epe;
+    if (m <= 64) {
+      int32_t v0 = INT32_MAX, v1 = INT32_MAX;
+      if (lane < m) {
+        const int32_t slot = inc[a + lane / epe];
+        v0 = l2g[epe * (slot / epe) + (lane % epe)];
+      }
+      if (lane + 32 < m) {
+        const int32_t slot = inc[a + (lane + 32) / epe];
+        v1 = l2g[epe * (slot / epe) + ((lane + 32) % epe)];
+      }
+      if (v0 < 0) v0 = INT32_MAX;  // constrained / gauged-out local edges
+      if (v1 < 0) v1 = INT32_MAX;
+      warp_sort64(v0, v1);
+      // every lane takes part in each shuffle; lane 0 then swaps in v0 of lane 31
+      const int32_t prev0 = __shfl_up_sync(0xffffffffu, v0, 1);
+      const int32_t last0 = __shfl_sync(0xffffffffu, v0, 31);
+      const int32_t up1 = __shfl_up_sync(0xffffffffu, v1, 1);
+      const int32_t prev1 = lane ? up1 : last0;
+      const bool keep0 = v0 != INT32_MAX && (lane == 0 || v0 != prev0);
+      const bool keep1 = v1 != INT32_MAX && v1 != prev1;
+      const unsigned b0 = __ballot_sync(0xffffffffu, keep0), b1 = __ballot_sync(0xffffffffu, keep1);
+      if (keep0) out[__popc(b0 & lt)] = v0;
+      if (keep1) out[__popc(b0) + __popc(b1 & lt)] = v1;
+      if (lane == 0) counts[r] = __popc(b0) + __popc(b1);
+      continue;
+    }
     if (m > kPatternCap) {
       if (lane == 0) {
         atomicOr(err, kErrRowCap);
-        if (!kWrite) counts[r] = 0;
+        counts[r] = 0;
       }
       continue;
     }
@@ -193,23 +244,40 @@ __global__ void __launch_bounds__(128) k_row_pattern(int64_t n, int epe, const i
       const int idx = base + lane;
       const bool keep = idx < m && first[idx];
       kept += __popc(__ballot_sync(0xffffffffu, keep));
-      if (kWrite && keep) {
+      if (keep) {
         const int32_t c = cand[idx];
         int rank = 0;  // distinct columns smaller than c
         for (int j = 0; j < m; ++j) rank += (first[j] && cand[j] < c) ? 1 : 0;
-        col[row_ptr[r] + rank] = c;
+        out[rank] = c;
       }
     }
-    if (!kWrite && lane == 0) counts[r] = kept;
+    if (lane == 0) counts[r] = kept;
     __syncwarp();
+  }
+}
+
+// Warp per row: the row's columns from the scratch rows into the CSR.
+__global__ void __launch_bounds__(128) k_row_columns(int64_t n, int epe, const int32_t* __restrict__ inc_ptr,
+                                                     const int32_t* __restrict__ tmp,
+                                                     const int32_t* __restrict__ row_ptr,
+                                                     int32_t* __restrict__ col) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int32_t* src = tmp + static_cast<int64_t>(inc_ptr[r]) * epe;
+    const int32_t c0 = row_ptr[r], len = row_ptr[r + 1] - c0;
+    for (int k = lane; k < len; k += 32) col[c0 + k] = src[k];
   }
 }
 
 // --------------------------------------------------------------- numeric ----
 // Nedelec TET4_EDGE edge table (nedelec_element.cpp:54-60): basis k is
-// lambda_b grad(lambda_a) - lambda_a grad(lambda_b) for (a, b) = kNed[k].
-__constant__ int kNedA[6] = {0, 1, 2, 0, 1, 2};
-__constant__ int kNedB[6] = {1, 2, 0, 3, 3, 3};
+// lambda_b grad(lambda_a) - lambda_a grad(lambda_b) for (a, b) = (ned_a(k), ned_b(k)).
+// Closed forms of kNed = {(0,1),(1,2),(2,0),(0,3),(1,3),(2,3)}: with k unrolled
+// they fold to constants, so no per-thread array is indexed at run time.
+__host__ __device__ constexpr int ned_a(int k) { return k < 3 ? k : k - 3; }
+__host__ __device__ constexpr int ned_b(int k) { return k < 3 ? (k + 1) % 3 : 3; }
+static_assert(ned_a(2) == 2 && ned_b(2) == 0 && ned_a(4) == 1 && ned_b(4) == 3, "nedelec_element.cpp:54-60");
 
 struct Tet {
   double d[3][3];  // d[c] = x_c - x_3 (Jacobian columns)
@@ -353,10 +421,15 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
       if (!load_tet(A.elems, A.xyz, A.n_nodes, t, T)) { atomicOr(A.err, kErrNode); continue; }
       const double adet = fabs(T.det);
       if (adet < 1e-15) continue;  // every quadrature point skipped (:169)
-      int sg[6];
+      // the row's own local edge, picked out with compile-time indices
+      int sgi = 1;
+      double ci[3] = {0, 0, 0};
 #pragma unroll
       for (int k = 0; k < 6; ++k)
-        sg[k] = signs ? (T.node[kNedB[k]] < T.node[kNedA[k]] ? 1 : -1) : 1;
+        if (k == i) {
+          if (signs) sgi = T.node[ned_b(k)] < T.node[ned_a(k)] ? 1 : -1;
+          ci[0] = T.c[k][0]; ci[1] = T.c[k][1]; ci[2] = T.c[k][2];
+        }
       const double kf = nq * w * adet * A.nu[mid];
       const double sig = A.sigma ? A.sigma[mid] : 0.0;
       const bool do_mass = want_mass && sig > 0.0;
@@ -369,13 +442,12 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
         src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
       }
       const bool do_src = src_count > 0;
-      int32_t cj[6];
       int32_t pos[6];
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        cj[j] = A.l2g[6 * t + j];
-        pos[j] = cj[j] >= 0 ? find_slot(A.col, s0, s1, cj[j]) : -1;
-        if (cj[j] >= 0 && (pos[j] >= s1 || A.col[pos[j]] != cj[j])) {
+        const int32_t cj = A.l2g[6 * t + j];
+        pos[j] = cj >= 0 ? find_slot(A.col, s0, s1, cj) : -1;
+        if (cj >= 0 && (pos[j] >= s1 || A.col[pos[j]] != cj)) {
           atomicOr(A.err, kErrSlot);
           pos[j] = -1;
         }
@@ -383,8 +455,9 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         if (pos[j] < 0) continue;
-        const double d = T.c[i][0] * T.c[j][0] + T.c[i][1] * T.c[j][1] + T.c[i][2] * T.c[j][2];
-        A.kval[pos[j]] += static_cast<double>(sg[i] * sg[j]) * (kf * d);
+        const int sgj = signs ? (T.node[ned_b(j)] < T.node[ned_a(j)] ? 1 : -1) : 1;
+        const double d = ci[0] * T.c[j][0] + ci[1] * T.c[j][1] + ci[2] * T.c[j][2];
+        A.kval[pos[j]] += static_cast<double>(sgi * sgj) * (kf * d);
       }
       if (do_mass || do_src) {
         double mrow[6] = {0, 0, 0, 0, 0, 0};
@@ -396,20 +469,20 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
           else if (qq == 2 && !quad3) { lam[0] = qb; lam[1] = qa; lam[2] = qa; }
           else { lam[0] = qa; lam[1] = qa; lam[2] = qa; }
           lam[3] = 1.0 - lam[0] - lam[1] - lam[2];
-          double W[6][3];
+          double W[6][3], Wi[3] = {0, 0, 0};
 #pragma unroll
           for (int k = 0; k < 6; ++k) {
-            const int a = kNedA[k], b = kNedB[k];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              W[k][c] = lam[b] * T.g[a][c] - lam[a] * T.g[b][c];
+              W[k][c] = lam[ned_b(k)] * T.g[ned_a(k)][c] - lam[ned_a(k)] * T.g[ned_b(k)][c];
               if (literal) W[k][c] /= T.det;
             }
+            if (k == i) { Wi[0] = W[k][0]; Wi[1] = W[k][1]; Wi[2] = W[k][2]; }
           }
           if (do_mass) {
 #pragma unroll
             for (int j = 0; j < 6; ++j)
-              mrow[j] += w * adet * sig * (W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2]);
+              mrow[j] += w * adet * sig * (Wi[0] * W[j][0] + Wi[1] * W[j][1] + Wi[2] * W[j][2]);
           }
           if (do_src) {
             double x[3], js[3];
@@ -417,15 +490,18 @@ __global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
             for (int c = 0; c < 3; ++c)
               x[c] = T.x3[c] + lam[0] * T.d[0][c] + lam[1] * T.d[1][c] + lam[2] * T.d[2][c];
             source_at(x, tab, src_first, src_count, js);
-            fi += w * adet * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
+            fi += w * adet * (Wi[0] * js[0] + Wi[1] * js[1] + Wi[2] * js[2]);
           }
         }
         if (do_mass) {
 #pragma unroll
           for (int j = 0; j < 6; ++j)
-            if (pos[j] >= 0) A.mval[pos[j]] += static_cast<double>(sg[i] * sg[j]) * mrow[j];
+            if (pos[j] >= 0) {
+              const int sgj = signs ? (T.node[ned_b(j)] < T.node[ned_a(j)] ? 1 : -1) : 1;
+              A.mval[pos[j]] += static_cast<double>(sgi * sgj) * mrow[j];
+            }
         }
-        f += sg[i] * fi;
+        f += sgi * fi;
       }
     }
     A.rhs[r] = f;
@@ -692,24 +768,36 @@ int system_build(System& s, cudaStream_t st) {
   EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
   k_fill_incidence<<<grid_for(m, 256), 256, 0, st>>>(s.l2g, m, s.inc_ptr, cnt, s.inc);
   k_sort_incidence<<<grid_for(n, 128), 128, 0, st>>>(s.inc_ptr, s.inc, n);
-  k_row_pattern<false><<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, cnt,
-                                                             nullptr, nullptr, s.err);
+  int32_t* tmp = nullptr;  // every row's candidates: epe per incident slot
+  EMG_CK(cudaMallocAsync(&tmp, sizeof(int32_t) * (inc_total > 0 ? inc_total * epe : 1), st));
+  k_row_unique<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, cnt, tmp, s.err);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaMallocAsync(&s.K.row_ptr, sizeof(int32_t) * (n + 1), st));
   int64_t nnz = 0;
   rc = scan_counts(cnt, s.K.row_ptr, n, &nnz, st);
-  if (rc) return rc;
-  EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  EMG_CK(cudaStreamSynchronize(st));
-  if (herr) { set_error("system build:" + err_text(herr)); return EMG_INVALID_INPUT; }
-  if (nnz >= (int64_t(1) << 31)) { set_error("nnz exceeds int32 range"); return EMG_INVALID_INPUT; }
+  if (!rc) {
+    EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    if (herr) {
+      set_error("system build:" + err_text(herr));
+      rc = EMG_INVALID_INPUT;
+    } else if (nnz >= (int64_t(1) << 31)) {
+      set_error("nnz exceeds int32 range");
+      rc = EMG_INVALID_INPUT;
+    }
+  }
+  if (rc) {
+    cudaFreeAsync(tmp, st);
+    cudaFreeAsync(cnt, st);
+    return rc;
+  }
   s.K.n = n;
   s.K.nnz = nnz;
   EMG_CK(cudaMallocAsync(&s.K.col, sizeof(int32_t) * (nnz > 0 ? nnz : 1), st));
   EMG_CK(cudaMallocAsync(&s.K.val, sizeof(double) * (nnz > 0 ? nnz : 1), st));
-  k_row_pattern<true><<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, nullptr,
-                                                            s.K.row_ptr, s.K.col, s.err);
+  k_row_columns<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, tmp, s.K.row_ptr, s.K.col);
   EMG_CK(cudaGetLastError());
+  EMG_CK(cudaFreeAsync(tmp, st));
   EMG_CK(cudaMallocAsync(&s.rhs, sizeof(double) * (n > 0 ? n : 1), st));
   EMG_CK(cudaMemsetAsync(s.rhs, 0, sizeof(double) * (n > 0 ? n : 1), st));
   EMG_CK(cudaMemsetAsync(s.K.val, 0, sizeof(double) * (nnz > 0 ? nnz : 1), st));
