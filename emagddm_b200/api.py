@@ -423,7 +423,7 @@ class IterativeSolverConfig:
     tolerance: float = 1e-8
     max_iterations: int = 1000
     residual_monitor_interval: int = 10
-    preconditioner: str = "NONE"  # NONE | JACOBI
+    preconditioner: str = "NONE"  # NONE | JACOBI (ILU0 is reported as INVALID_INPUT)
 
 
 CGConfig = IterativeSolverConfig
@@ -468,9 +468,11 @@ class _KrylovSolver:
         if b.shape[0] != self._A.rows():
             res.error_msg = "right-hand side length does not match the matrix"
             return res
+        # PreconditionerType values of iterative_solvers.h:59-76; the library
+        # rejects ILU0 (2) and unknown names rather than substituting one
+        kinds = {"NONE": _abi.PRECOND_NONE, "JACOBI": _abi.PRECOND_JACOBI, "ILU0": 2}
         cfg = _abi.KrylovConfig(self.config.tolerance, self.config.max_iterations,
-                                _abi.PRECOND_JACOBI if self.config.preconditioner == "JACOBI"
-                                else _abi.PRECOND_NONE)
+                                kinds.get(str(self.config.preconditioner).upper(), -1))
         out = _abi.Result()
         x = np.empty_like(b)
         fn = lib().emg_bicgstab_solve if self._bicg else lib().emg_cg_solve
@@ -480,7 +482,7 @@ class _KrylovSolver:
         res.iterations = out.iterations
         res.residual_norm = out.residual_norm
         res.solve_time_ms = out.solve_time_ms
-        if rc > 4:
+        if rc > 4 or rc == _abi.EMG_INVALID_INPUT:
             res.error_msg = lib().emg_last_error().decode()
         cap = max(out.iterations, 1)
         hist = np.empty(cap)

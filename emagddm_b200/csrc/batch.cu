@@ -561,6 +561,7 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
     set_error("batch solve: bad arguments");
     return EMG_INVALID_INPUT;
   }
+  if (check_krylov_precond(cfg.preconditioner)) return EMG_INVALID_INPUT;
   std::vector<int64_t> blocks(blocks_in, blocks_in + nb + 1);
   if (blocks[0] != 0 || blocks[nb] != A.n) {
     set_error("batch solve: block partition must start at 0 and end at n");

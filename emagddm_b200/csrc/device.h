@@ -67,6 +67,15 @@ int system_build(System& s, cudaStream_t st);
 int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_mat,
                     const emg_source* src, int32_t n_src, int32_t flags, cudaStream_t st);
 
+// EMG_PRECOND_NONE / _JACOBI, else EMG_INVALID_INPUT with a message (no
+// silent substitution for the reference's ILU0).
+inline int check_krylov_precond(int32_t p) {
+  if (p == EMG_PRECOND_NONE || p == EMG_PRECOND_JACOBI) return EMG_SUCCESS;
+  set_error("preconditioner " + std::to_string(p) +
+            ": only EMG_PRECOND_NONE (0) and EMG_PRECOND_JACOBI (1) exist on the GPU path");
+  return EMG_INVALID_INPUT;
+}
+
 // Exclusive scan of n int32 counts into out[0..n]; returns the total.
 int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, cudaStream_t st);
 

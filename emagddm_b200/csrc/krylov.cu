@@ -1199,6 +1199,7 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   res->status = EMG_INVALID_INPUT;
   if (!b || !x) { set_error("null vector"); return EMG_INVALID_INPUT; }
   if (A.n <= 0) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
+  if (check_krylov_precond(cfg.preconditioner)) return EMG_INVALID_INPUT;
   const int32_t max_iter = cfg.max_iterations;
   int rc;
   {

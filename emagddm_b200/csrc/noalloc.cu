@@ -261,6 +261,7 @@ int cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* c
     set_error("emg_cg_solve_noalloc: null array or empty matrix");
     return EMG_INVALID_INPUT;
   }
+  if (check_krylov_precond(cfg.preconditioner)) return EMG_INVALID_INPUT;
   if (n > kMaxRows) {
     set_error("emg_cg_solve_noalloc: n = " + std::to_string(n) + " exceeds the no-allocation scratch limit of " +
               std::to_string(kMaxRows) + " rows; use emg_cg_solve_device");

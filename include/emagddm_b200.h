@@ -78,6 +78,12 @@ typedef struct {
 } emg_source;
 
 /* ---- solver configuration and result ------------------------------------ */
+/* CGConfig / BiCGSTABConfig::PreconditionerType (iterative_solvers.h:59-76).
+ * The reference's third value, ILU0 (= 2), is Eigen::IncompleteLUT (fill
+ * factor 10, drop tolerance 1e-12, AMD ordering; iterative_solvers.h:324,
+ * .cpp:277-286): a sequential host factorization with no GPU counterpart
+ * here.  The solvers reject any value other than the two below with
+ * EMG_INVALID_INPUT instead of substituting another preconditioner. */
 enum { EMG_PRECOND_NONE = 0, EMG_PRECOND_JACOBI = 1 };
 typedef struct {
   double tolerance;          /* ||r||/||b|| stop threshold (IterativeSolverConfig, default 1e-8) */
