@@ -126,6 +126,11 @@ __device__ __forceinline__ int64_t gstride() {
 #ifndef EMG_SELL_UNROLL
 #define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
 #endif
+// 1: the next batch of columns / values is loaded while the current batch's
+// x entries are gathered (two batches in flight per lane).
+#ifndef EMG_SELL_PIPE
+#define EMG_SELL_PIPE 1
+#endif
 // Slices per group: the kGroup slices of a group share one length and are
 // interleaved entry by entry (slot of entry j, slice w, lane l at
 // group_base + 32 kGroup j + 32 w + l), so the kGroup warps of a block that
@@ -195,6 +200,39 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     const int row32 = static_cast<int>(s * kSliceRows + lane);
     double sum = 0.0;
     int j = 0;
+#if EMG_SELL_PIPE
+    // software pipeline: the next batch's columns and values are in flight
+    // while this batch's x entries are gathered; entries past the row length
+    // are masked (value 0, column 0) and add +0 after the real ones
+    {
+      constexpr int U = EMG_SELL_UNROLL;
+      const int nb = (len + U - 1) / U;
+      int cn[U];
+      double vn[U];
+      auto fetch = [&](int jb, int (&c)[U], double (&v)[U]) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = jb + u < len;
+          const int64_t k = base + static_cast<int64_t>(kGroupStride) * (jb + u);
+          c[u] = in ? column(k, row32) : 0;
+          v[u] = in ? value(k) : 0.0;
+        }
+      };
+      if (nb > 0) fetch(0, cn, vn);
+      for (int bt = 0; bt < nb; ++bt) {
+        int c[U];
+        double v[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
+        if (bt + 1 < nb) fetch((bt + 1) * U, cn, vn);
+#pragma unroll
+        for (int u = 0; u < U; ++u) xv[u] = x[c[u]];
+#pragma unroll
+        for (int u = 0; u < U; ++u) sum += v[u] * xv[u];
+      }
+      j = len;
+    }
+#endif
     for (; j + EMG_SELL_UNROLL <= len; j += EMG_SELL_UNROLL) {
       const int64_t k = base + static_cast<int64_t>(kGroupStride) * j;
       int c[EMG_SELL_UNROLL];
