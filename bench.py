@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import statistics
@@ -216,7 +217,10 @@ def run_ours(args, rank, world, local_rank):
         return {"mode": "kernels-only", "iterations": args.kernels_only,
                 "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]}}
 
+    phase_log = []  # per step: host ms of create, assemble, solve, destroy; device ms of the solve
+
     def step(resident: bool):
+        t0 = time.perf_counter()
         h = C.c_void_p()
         if resident:
             rc = L.emg_system_create_typed(et, xyz.shape[0], C.c_void_p(d_xyz.data_ptr()), tets.shape[0],
@@ -226,8 +230,10 @@ def run_ours(args, rank, world, local_rank):
             rc = L.emg_system_create_typed(et, p_xyz.shape[0], _abi.ptr(p_xyz), p_tets.shape[0], _abi.ptr(p_tets),
                                            _abi.ptr(p_mat), _abi.ptr(p_l2g), n_dofs, 0, sp, C.byref(h))
         _abi.check(rc, "emg_system_create")
+        t1 = time.perf_counter()
         _abi.check(L.emg_system_assemble(h, _abi.ptr(nu), _abi.ptr(sigma), len(nu), srcp, nsrc, 0, sp),
                    "emg_system_assemble")
+        t2 = time.perf_counter()
         out = _abi.Result()
         if resident:
             rc = L.emg_system_solve(h, 0, C.byref(cfg), C.c_void_p(d_x.data_ptr()), 1, sp, C.byref(out))
@@ -242,7 +248,11 @@ def run_ours(args, rank, world, local_rank):
         info["iters"] = out.iterations
         info["res"] = out.residual_norm
         info["solve_ms"] = out.solve_time_ms
+        t3 = time.perf_counter()
         L.emg_system_destroy(h)
+        t4 = time.perf_counter()
+        phase_log.append([round((b - a) * 1e3, 2) for a, b in ((t0, t1), (t1, t2), (t2, t3), (t3, t4))]
+                         + [round(out.solve_time_ms, 2)])
 
     step_ms = {}
 
@@ -252,12 +262,18 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         torch.cuda.synchronize(dev)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
+        del phase_log[:]
+        gc.collect()
+        gc.disable()  # no collector pass inside the timed steps (they create no cycles)
         ev[0].record(stream)
         for i in range(k):
             step(resident)
             ev[i + 1].record(stream)
         torch.cuda.synchronize(dev)
-        step_ms["resident" if resident else "e2e"] = [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(k)]
+        gc.enable()
+        arm = "resident" if resident else "e2e"
+        step_ms[arm] = [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(k)]
+        step_ms[arm + "_phases"] = list(phase_log)
         ms = ev[0].elapsed_time(ev[k])
         return max_over_ranks(ms)
 
@@ -341,6 +357,7 @@ def run_ours(args, rank, world, local_rank):
                    "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]},
                    "cg_iteration_ms_kernels": it_ms,
                    "solve_ms": info["solve_ms"], "phase_ms": phases, "step_ms": step_ms,
+                   "median_step_ms": {a: statistics.median(step_ms[a]) for a in ("resident", "e2e")},
                    "solver_format": {"kind": "SELL-32-sigma4096", "slots": slots.value,
                                      "padding": slots.value / nnz - 1.0}},
         "clocks": clk.summary(),

@@ -125,6 +125,7 @@ int system_create_impl(int32_t elem_type, int64_t n_nodes, const double* xyz, in
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = EMG_ERR_CUDA; }
   }
   if (!rc) {
+    emg::trace_mark(st, "create.upload");
     emg::TraceScope t("system_create.build");
     rc = emg::system_build(s, st);
   }

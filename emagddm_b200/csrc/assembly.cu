@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "device.h"
 #include "internal.h"
+#include "trace.h"
 
 namespace emg {
 
@@ -748,6 +749,8 @@ int scan_counts(const int32_t* counts, int32_t* out, int64_t n, int64_t* total, 
 }
 
 int system_build(System& s, cudaStream_t st) {
+  trace_pool("system_build.begin");
+  trace_mark(st, "build.begin");
   const int epe = edges_per_elem(s.elem_type);
   const int64_t m = epe * s.n_elems, n = s.n;
   int32_t* cnt = nullptr;
@@ -760,6 +763,7 @@ int system_build(System& s, cudaStream_t st) {
   int64_t inc_total = 0;
   int rc = scan_counts(cnt, s.inc_ptr, n, &inc_total, st);
   if (rc) return rc;
+  trace_mark(st, "build.count_scan");
   int32_t herr = 0;
   EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   EMG_CK(cudaStreamSynchronize(st));
@@ -768,13 +772,22 @@ int system_build(System& s, cudaStream_t st) {
   EMG_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st));
   k_fill_incidence<<<grid_for(m, 256), 256, 0, st>>>(s.l2g, m, s.inc_ptr, cnt, s.inc);
   k_sort_incidence<<<grid_for(n, 128), 128, 0, st>>>(s.inc_ptr, s.inc, n);
+  trace_mark(st, "build.fill_sort");
   int32_t* tmp = nullptr;  // every row's candidates: epe per incident slot
-  EMG_CK(cudaMallocAsync(&tmp, sizeof(int32_t) * (inc_total > 0 ? inc_total * epe : 1), st));
-  k_row_unique<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, cnt, tmp, s.err);
+  {
+    TraceScope t("build.tmp_malloc_call");
+    EMG_CK(cudaMallocAsync(&tmp, sizeof(int32_t) * (inc_total > 0 ? inc_total * epe : 1), st));
+  }
+  {
+    TraceScope t("build.row_unique_launch_call");
+    k_row_unique<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, s.inc, s.l2g, cnt, tmp, s.err);
+  }
   EMG_CK(cudaGetLastError());
+  trace_mark(st, "build.row_unique");
   EMG_CK(cudaMallocAsync(&s.K.row_ptr, sizeof(int32_t) * (n + 1), st));
   int64_t nnz = 0;
   rc = scan_counts(cnt, s.K.row_ptr, n, &nnz, st);
+  trace_mark(st, "build.scan2");
   if (!rc) {
     EMG_CK(cudaMemcpyAsync(&herr, s.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     EMG_CK(cudaStreamSynchronize(st));
@@ -793,8 +806,11 @@ int system_build(System& s, cudaStream_t st) {
   }
   s.K.n = n;
   s.K.nnz = nnz;
-  EMG_CK(cudaMallocAsync(&s.K.col, sizeof(int32_t) * (nnz > 0 ? nnz : 1), st));
-  EMG_CK(cudaMallocAsync(&s.K.val, sizeof(double) * (nnz > 0 ? nnz : 1), st));
+  {
+    TraceScope t("build.colval_malloc_call");
+    EMG_CK(cudaMallocAsync(&s.K.col, sizeof(int32_t) * (nnz > 0 ? nnz : 1), st));
+    EMG_CK(cudaMallocAsync(&s.K.val, sizeof(double) * (nnz > 0 ? nnz : 1), st));
+  }
   k_row_columns<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, tmp, s.K.row_ptr, s.K.col);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaFreeAsync(tmp, st));
@@ -803,6 +819,7 @@ int system_build(System& s, cudaStream_t st) {
   EMG_CK(cudaMemsetAsync(s.K.val, 0, sizeof(double) * (nnz > 0 ? nnz : 1), st));
   EMG_CK(cudaFreeAsync(cnt, st));
   EMG_CK(cudaStreamSynchronize(st));
+  trace_mark(st, "build.end");
   // M shares the pattern of K
   s.M.n = n;
   s.M.nnz = nnz;
@@ -906,6 +923,28 @@ int check_csr(int64_t n, const int32_t* rp, const int32_t* col, int64_t nnz, cud
   if (h & 1) { set_error("row_ptr is not a valid offset array"); return EMG_INVALID_INPUT; }
   if (h & 2) { set_error("columns out of range or not strictly ascending in a row"); return EMG_INVALID_INPUT; }
   return EMG_SUCCESS;
+}
+
+void trace_pool(const char* where) {
+  if (!trace_enabled()) return;
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+  uint64_t reserved = 0, used = 0;
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  std::fprintf(stderr, "emg-trace-pool %s %llu %llu\n", where, static_cast<unsigned long long>(reserved),
+               static_cast<unsigned long long>(used));
+}
+
+void trace_mark(void* stream, const char* label) {
+  if (!trace_enabled()) return;
+  static thread_local std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
+  cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  const auto now = std::chrono::steady_clock::now();
+  std::fprintf(stderr, "emg-trace-mark %s %.3f\n", label,
+               std::chrono::duration<double, std::milli>(now - last).count());
+  last = now;
 }
 
 void keep_pool_memory() {

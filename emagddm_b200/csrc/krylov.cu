@@ -1248,9 +1248,11 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   KrylovWorkspace& w = *A.ws;
   cudaStream_t st = user ? user : w.cap;
   {
+    trace_pool("solve.sell.begin");
     TraceScope t("solve.sell");
     rc = ensure_sell(A, st);
   }
+  trace_pool("solve.sell.end");
   if (rc) { res->status = rc; return rc; }
   // Preferred: the whole solve as one graph with a device while-loop; else
   // host-polled chunks of kChunk iterations.

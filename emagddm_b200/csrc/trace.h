@@ -16,6 +16,13 @@ inline bool trace_enabled() {
   return on;
 }
 
+// With tracing on: the reserved and used bytes of the current device's
+// default stream-ordered memory pool, as "emg-trace-pool <where> <reserved> <used>".
+void trace_pool(const char* where);
+// With tracing on: synchronizes the stream (a cudaStream_t) and prints the
+// wall time since the previous mark of this thread, "emg-trace-mark <label> <ms>".
+void trace_mark(void* stream, const char* label);
+
 class TraceScope {
  public:
   explicit TraceScope(const char* name) : name_(name) {
