@@ -601,7 +601,18 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* _
 }
 
 template <int kMode>
-__global__ void __launch_bounds__(kThreads) k_cg_spmv_dot(Sell A, const double* __restrict__ p,
+// Minimum resident blocks per SM asked of the compiler for the CG SpMV
+// kernel (0 = no register cap).
+#ifndef EMG_SPMV_MINB
+#define EMG_SPMV_MINB 0
+#endif
+#if EMG_SPMV_MINB
+#define EMG_SPMV_BOUNDS __launch_bounds__(kThreads, EMG_SPMV_MINB)
+#else
+#define EMG_SPMV_BOUNDS __launch_bounds__(kThreads)
+#endif
+
+__global__ void EMG_SPMV_BOUNDS k_cg_spmv_dot(Sell A, const double* __restrict__ p,
                                                           double* __restrict__ q, double* partial,
                                                           SolverState* st) {
   if (st->done) return;
