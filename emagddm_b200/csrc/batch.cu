@@ -206,6 +206,12 @@ __global__ void __launch_bounds__(kBThreads) k_b_init(View B, const double* __re
 }
 
 // q = A p and p.q per block -> alpha (or breakdown)
+// 1: the batched SpMV keeps the next batch of loads in flight (as the
+// single-system SELL kernel does); 0: one batch at a time.
+#ifndef EMG_BATCH_PIPE
+#define EMG_BATCH_PIPE 1
+#endif
+
 __global__ void __launch_bounds__(kBThreads) k_b_spmv_dot(View B) {
   if (B.ctl[1] == 0) return;
   const uint64_t pol = evict_first_policy();
@@ -216,6 +222,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_spmv_dot(View B) {
         const int len = static_cast<int>((B.slice_ptr[s + 1] - b0) >> 5);
         const int64_t base = b0 + lane;
         double sum = 0.0;
+#if !EMG_BATCH_PIPE
         int j = 0;
         for (; j + 4 <= len; j += 4) {
           const int64_t k = base + 32 * j;
@@ -235,6 +242,34 @@ __global__ void __launch_bounds__(kBThreads) k_b_spmv_dot(View B) {
           const int64_t k = base + 32 * j;
           sum += ld_stream(B.val + k, pol) * B.p[ld_stream(B.col + k, pol)];
         }
+#else
+        // the next batch of 4 columns / values is in flight while this batch
+        // gathers p; entries past the row length are masked and add +0 last
+        const int nbt = (len + 3) >> 2;
+        int cn[4];
+        double vn[4];
+        auto fetch = [&](int jb) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const bool in = jb + u < len;
+            const int64_t k = base + 32 * static_cast<int64_t>(jb + u);
+            cn[u] = in ? ld_stream(B.col + k, pol) : 0;
+            vn[u] = in ? ld_stream(B.val + k, pol) : 0.0;
+          }
+        };
+        if (nbt > 0) fetch(0);
+        for (int bt = 0; bt < nbt; ++bt) {
+          int cc[4];
+          double vv[4], xx[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) { cc[u] = cn[u]; vv[u] = vn[u]; }
+          if (bt + 1 < nbt) fetch(4 * (bt + 1));
+#pragma unroll
+          for (int u = 0; u < 4; ++u) xx[u] = B.p[cc[u]];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) sum += vv[u] * xx[u];
+        }
+#endif
         const int64_t row = static_cast<int64_t>(s) * 32 + lane;
         B.q[row] = sum;
         v[0] = B.p[row] * sum;
