@@ -91,6 +91,7 @@ struct KrylovWorkspace {
   cudaGraphExec_t bi_loop = nullptr;
   bool loop_unavailable = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int dev = -1;  // device of cap / ev0 / ev1
 };
 
 namespace {
@@ -1115,6 +1116,65 @@ void pinned_state_free(SolverState* p) {
   pool.free.push_back(p);
 }
 
+// Capture streams and timing events of released workspaces, kept per device
+// and handed to the next workspace instead of being destroyed and created
+// for every solve (never destroyed, like the pinned blocks above).
+struct HandlePool {
+  std::mutex mu;
+  std::vector<std::pair<int, cudaStream_t>> streams;
+  std::vector<std::pair<int, cudaEvent_t>> events;
+};
+HandlePool& handle_pool() {
+  static HandlePool* p = new HandlePool();
+  return *p;
+}
+
+int take_stream(cudaStream_t* out) {
+  int dev = 0;
+  EMG_CK(cudaGetDevice(&dev));
+  {
+    HandlePool& hp = handle_pool();
+    std::lock_guard<std::mutex> lock(hp.mu);
+    for (size_t i = 0; i < hp.streams.size(); ++i)
+      if (hp.streams[i].first == dev) {
+        *out = hp.streams[i].second;
+        hp.streams.erase(hp.streams.begin() + static_cast<int64_t>(i));
+        return EMG_SUCCESS;
+      }
+  }
+  EMG_CK(cudaStreamCreate(out));
+  return EMG_SUCCESS;
+}
+
+int take_event(cudaEvent_t* out) {
+  int dev = 0;
+  EMG_CK(cudaGetDevice(&dev));
+  {
+    HandlePool& hp = handle_pool();
+    std::lock_guard<std::mutex> lock(hp.mu);
+    for (size_t i = 0; i < hp.events.size(); ++i)
+      if (hp.events[i].first == dev) {
+        *out = hp.events[i].second;
+        hp.events.erase(hp.events.begin() + static_cast<int64_t>(i));
+        return EMG_SUCCESS;
+      }
+  }
+  EMG_CK(cudaEventCreate(out));
+  return EMG_SUCCESS;
+}
+
+// Returns a stream / events of device `dev` to the pool; the stream is first
+// drained so that the next owner starts on an idle stream.
+void give_back(int dev, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+  if (dev < 0) return;
+  if (s) cudaStreamSynchronize(s);
+  HandlePool& hp = handle_pool();
+  std::lock_guard<std::mutex> lock(hp.mu);
+  if (s) hp.streams.emplace_back(dev, s);
+  for (cudaEvent_t e : {e0, e1})
+    if (e) hp.events.emplace_back(dev, e);
+}
+
 // Workspace vectors come from the stream-ordered pool (allocated on `st`,
 // returned with cudaFreeAsync once the device is idle).
 int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
@@ -1131,9 +1191,10 @@ int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
     EMG_CK(cudaStreamSynchronize(st));
     EMG_CK(cudaMemset(w.state, 0, sizeof(SolverState)));
     if (int rc = pinned_state_alloc(&w.state_h)) return rc;
-    EMG_CK(cudaStreamCreate(&w.cap));
-    EMG_CK(cudaEventCreate(&w.ev0));
-    EMG_CK(cudaEventCreate(&w.ev1));
+    EMG_CK(cudaGetDevice(&w.dev));
+    if (int rc = take_stream(&w.cap)) return rc;
+    if (int rc = take_event(&w.ev0)) return rc;
+    if (int rc = take_event(&w.ev1)) return rc;
   }
   KrylovWorkspace& w = *A.ws;
   if (bicg && !w.rh) {
@@ -1449,9 +1510,7 @@ void free_workspace(KrylovWorkspace* w) {
   }
   {
     TraceScope t("free_workspace.stream_events");
-    if (w->cap) cudaStreamDestroy(w->cap);
-    if (w->ev0) cudaEventDestroy(w->ev0);
-    if (w->ev1) cudaEventDestroy(w->ev1);
+    give_back(w->dev, w->cap, w->ev0, w->ev1);
   }
   delete w;
 }
