@@ -127,10 +127,17 @@ __device__ __forceinline__ int64_t gstride() {
 #ifndef EMG_SELL_UNROLL
 #define EMG_SELL_UNROLL 4  // row entries per batch of loads in the plain SELL loop
 #endif
-// 1: the next batch of columns / values is loaded while the current batch's
-// x entries are gathered (two batches in flight per lane).
+// Load pipeline of the plain SELL loop.  0: one batch of EMG_SELL_UNROLL
+// loads at a time; 1: the next batch of the same slice is loaded while the
+// current batch's x entries are gathered; 2: one pipeline across all slices
+// of a warp, batches of EMG_SELL_BATCH entries (51.7 vs 60.3 us for 1 with
+// 8 entries, 63.6 us with 4, for the 64^3 CG matrix on B200, each with the
+// one-wave grid of EMG_SPMV_RESIDENT).
 #ifndef EMG_SELL_PIPE
-#define EMG_SELL_PIPE 1
+#define EMG_SELL_PIPE 2
+#endif
+#ifndef EMG_SELL_BATCH
+#define EMG_SELL_BATCH 8
 #endif
 // Slices per group: the kGroup slices of a group share one length and are
 // interleaved entry by entry (slot of entry j, slice w, lane l at
@@ -169,12 +176,90 @@ __device__ __forceinline__ void slice_span(const int64_t* __restrict__ gp, int64
   base = b0 + 32 * (s - g * kGroup);
 }
 
+// Warp per slice, lane per row, as one software pipeline over all slices of
+// the warp: the batch of EMG_SELL_BATCH entries after the current one --
+// possibly the first batch of the warp's next slice -- is in flight while
+// the current batch's x entries are gathered, and the span of the slice
+// after the one being fetched is read one slice ahead, so no slice starts
+// with an exposed load.  A slice without entries takes one batch of masked
+// loads; entries past a row's length are masked (value 0, column 0) and add
+// +0 after the real ones, so every row is summed in CSR order.  Calls
+// out(row, y_row) for every real row.  32-bit columns, unpacked slots.
+template <class Out>
+__device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __restrict__ x, Out out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = gstride() >> 5;
+  const int64_t warp = EMG_SELL_SPREAD ? static_cast<int64_t>(threadIdx.x >> 5) * gridDim.x + blockIdx.x
+                                       : gtid() >> 5;
+  const uint64_t pol = evict_first_policy();
+  const int64_t* __restrict__ sp = A.slice_ptr;
+  const int32_t* __restrict__ col = A.col;
+  const double* __restrict__ val = A.val;
+  constexpr int U = EMG_SELL_BATCH;
+  int64_t cs = warp;  // slice whose batch is being summed
+  if (cs >= A.nslices) return;
+  int64_t fs = cs;  // slice being fetched, its lane base, length, next entry
+  int64_t fbase;
+  int flen;
+  slice_span(sp, fs, fbase, flen);
+  fbase += lane;
+  int fj = 0;
+  int64_t nbase = 0;  // span of slice fs + nwarps
+  int nlen = 0;
+  if (fs + nwarps < A.nslices) slice_span(sp, fs + nwarps, nbase, nlen);
+  bool more = true;
+  auto fetch = [&](int (&c)[U], double (&v)[U], bool& last) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool in = fj + u < flen;
+      const int64_t k = fbase + static_cast<int64_t>(kGroupStride) * (fj + u);
+      c[u] = in ? ld_stream(col + k, pol) : 0;
+      v[u] = in ? ld_stream(val + k, pol) : 0.0;
+    }
+    fj += U;
+    last = fj >= flen;
+    if (last) {
+      fs += nwarps;
+      more = fs < A.nslices;
+      fbase = nbase + lane;
+      flen = nlen;
+      fj = 0;
+      if (fs + nwarps < A.nslices) slice_span(sp, fs + nwarps, nbase, nlen);
+    }
+  };
+  int cn[U];
+  double vn[U];
+  bool lastn;
+  fetch(cn, vn, lastn);
+  double sum = 0.0;
+  for (;;) {
+    int c[U];
+    double v[U], xv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
+    const bool last = lastn;
+    if (more) fetch(cn, vn, lastn);
+#pragma unroll
+    for (int u = 0; u < U; ++u) xv[u] = x[c[u]];
+#pragma unroll
+    for (int u = 0; u < U; ++u) sum += v[u] * xv[u];
+    if (last) {
+      const int64_t row = cs * kSliceRows + lane;
+      if (row < A.n) out(row, sum);
+      sum = 0.0;
+      cs += nwarps;
+      if (cs >= A.nslices) break;
+    }
+  }
+}
+
 // Warp per slice, lane per row: y_row = sum_j val * x[col].  Calls
 // out(row, y_row) for every real row.  Entries of a row are summed in CSR
-// order, four loads in flight per lane at a time.
+// order, EMG_SELL_UNROLL loads in flight per lane at a time (with
+// EMG_SELL_PIPE=1 the next batch of the same slice as well).
 // kNarrow: columns are stored as 16-bit offsets from the row (A.dcol).
 template <bool kNarrow, class Out>
-__device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
+__device__ __forceinline__ void sell_rows_sliced(const Sell& A, const double* __restrict__ x, Out out) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gstride() >> 5;
   const int64_t warp = EMG_SELL_SPREAD ? static_cast<int64_t>(threadIdx.x >> 5) * gridDim.x + blockIdx.x
@@ -201,7 +286,7 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     const int row32 = static_cast<int>(s * kSliceRows + lane);
     double sum = 0.0;
     int j = 0;
-#if EMG_SELL_PIPE
+#if EMG_SELL_PIPE == 1
     // software pipeline: the next batch's columns and values are in flight
     // while this batch's x entries are gathered; entries past the row length
     // are masked (value 0, column 0) and add +0 after the real ones
@@ -255,6 +340,12 @@ __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restric
     const int64_t row = s * kSliceRows + lane;
     if (row < A.n) out(row, sum);
   }
+}
+
+template <bool kNarrow, class Out>
+__device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
+  if constexpr (!kNarrow && !EMG_SELL_PACKED && EMG_SELL_PIPE == 2) sell_rows_stream(A, x, out);
+  else sell_rows_sliced<kNarrow>(A, x, out);
 }
 
 // Same product with the slices streamed through shared memory by bulk
@@ -601,7 +692,6 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int64_t n, const double* _
   }
 }
 
-template <int kMode>
 // Minimum resident blocks per SM asked of the compiler for the CG SpMV
 // kernel (0 = no register cap).
 #ifndef EMG_SPMV_MINB
@@ -613,6 +703,7 @@ template <int kMode>
 #define EMG_SPMV_BOUNDS __launch_bounds__(kThreads)
 #endif
 
+template <int kMode>
 __global__ void EMG_SPMV_BOUNDS k_cg_spmv_dot(Sell A, const double* __restrict__ p,
                                                           double* __restrict__ q, double* partial,
                                                           SolverState* st) {
@@ -939,6 +1030,33 @@ SpmvShape spmv_shape(const Sell& S, int plain_grid) {
   return {plain_grid, 0};
 }
 
+// Grid of a grid-stride solver kernel (SELL SpMV, CG / BiCGSTAB vector
+// updates): with EMG_SPMV_RESIDENT, as many blocks as fit on the GPU at once
+// (occupancy x SMs, at most `g`), so the loop runs in one wave; otherwise
+// `g` (8 blocks per SM, of which 4-5 of the SpMV fit: a second partial wave,
+// 63.6 instead of 54.4 us for the 64^3 CG matrix on B200 with the same loop).
+#ifndef EMG_SPMV_RESIDENT
+#define EMG_SPMV_RESIDENT 1
+#endif
+template <auto Kernel>
+int resident_grid(int g) {
+#if EMG_SPMV_RESIDENT
+  static int resident = 0;
+  if (!resident) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, Kernel, kThreads, 0) != cudaSuccess ||
+        per_sm < 1 || sms < 1)
+      return g;
+    resident = per_sm * sms;
+  }
+  return resident < g ? resident : g;
+#else
+  return g;
+#endif
+}
+
 int grid_size() {
   static int g = 0;
   if (!g) {
@@ -1257,16 +1375,16 @@ int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
 // Launches KERNEL<mode> for the storage format of S: the bulk-copy pipeline
 // (mode 2, persistent grid + dynamic shared memory), 16-bit column offsets
 // (mode 1) or 32-bit columns (mode 0).
-#define EMG_LAUNCH_SPMV(KERNEL, S, g, st, ...)                            \
-  do {                                                                    \
-    if ((S).tma) {                                                        \
-      const SpmvShape sh_ = spmv_shape(S, g);                             \
-      KERNEL<2><<<sh_.grid, kThreads, sh_.smem, st>>>(__VA_ARGS__);       \
-    } else if ((S).narrow) {                                              \
-      KERNEL<1><<<g, kThreads, 0, st>>>(__VA_ARGS__);                     \
-    } else {                                                              \
-      KERNEL<0><<<g, kThreads, 0, st>>>(__VA_ARGS__);                     \
-    }                                                                     \
+#define EMG_LAUNCH_SPMV(KERNEL, S, g, st, ...)                                        \
+  do {                                                                                \
+    if ((S).tma) {                                                                    \
+      const SpmvShape sh_ = spmv_shape(S, g);                                         \
+      KERNEL<2><<<sh_.grid, kThreads, sh_.smem, st>>>(__VA_ARGS__);                   \
+    } else if ((S).narrow) {                                                          \
+      KERNEL<1><<<resident_grid<KERNEL<1>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
+    } else {                                                                          \
+      KERNEL<0><<<resident_grid<KERNEL<0>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
+    }                                                                                 \
   } while (0)
 
 void launch_iterations(DevCsr& A, bool bicg, int count) {
@@ -1276,15 +1394,15 @@ void launch_iterations(DevCsr& A, bool bicg, int count) {
   for (int c = 0; c < count; ++c) {
     if (!bicg) {
       EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, w.cap, S, w.p, w.q, w.partial, w.state);
-      k_cg_update<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
+      k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                              w.hist, w.hist_cap);
-      k_cg_direction<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
+      k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
     } else {
-      k_bi_p<<<g, kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
+      k_bi_p<<<resident_grid<k_bi_p>(g), kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
       EMG_LAUNCH_SPMV(k_bi_v, S, g, w.cap, S, w.p, w.v, w.rh, w.partial, w.state);
-      k_bi_s<<<g, kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
+      k_bi_s<<<resident_grid<k_bi_s>(g), kThreads, 0, w.cap>>>(A.n, w.r, w.v, w.dinv, w.s, w.z, w.partial, w.state);
       EMG_LAUNCH_SPMV(k_bi_t, S, g, w.cap, S, w.z, w.t, w.partial, w.state);
-      k_bi_x<<<g, kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
+      k_bi_x<<<resident_grid<k_bi_x>(g), kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.p, w.z, w.s, w.t, w.rh, w.partial, w.state,
                                         w.hist, w.hist_cap);
     }
   }
@@ -1453,10 +1571,10 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
     EMG_CK(cudaEventRecord(ev[4 * i], st));
     EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, st, S, w.p, w.q, w.partial, w.state);
     EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
-    k_cg_update<<<g, kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
+    k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
                                         w.hist, w.hist_cap);
     EMG_CK(cudaEventRecord(ev[4 * i + 2], st));
-    k_cg_direction<<<g, kThreads, 0, st>>>(A.n, w.p, w.z, w.state);
+    k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, st>>>(A.n, w.p, w.z, w.state);
     EMG_CK(cudaEventRecord(ev[4 * i + 3], st));
   }
   EMG_CK(cudaGetLastError());
