@@ -54,7 +54,8 @@ struct SolverState {
   uint32_t ticket;
   int32_t loops;       // device-loop bodies executed in this solve
   int32_t loop_limit;  // hard bound on loop bodies (stops the loop without `done`)
-  int32_t copy_err;    // a bounded wait on a bulk copy ran out
+  int32_t copy_err;    // a bounded wait (bulk copy, grid barrier) ran out
+  uint32_t gen;        // grid-barrier generation of the fused CG update
 };
 
 // SELL-32-sigma copy of a DevCsr in the permuted numbering, slices in
@@ -92,6 +93,11 @@ struct KrylovWorkspace {
   bool loop_unavailable = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int dev = -1;  // device of cap / ev0 / ev1
+  // fused CG update + direction (one cooperative launch per iteration)
+  bool fuse = false;
+  int fuse_grid = 0;
+  size_t fuse_smem = 0;
+  int64_t fuse_stash = 0;  // entry pairs of a block kept in shared memory
 };
 
 namespace {
@@ -184,8 +190,9 @@ __device__ __forceinline__ void slice_span(const int64_t* __restrict__ gp, int64
 // with an exposed load.  A slice without entries takes one batch of masked
 // loads; entries past a row's length are masked (value 0, column 0) and add
 // +0 after the real ones, so every row is summed in CSR order.  Calls
-// out(row, y_row) for every real row.  32-bit columns, unpacked slots.
-template <class Out>
+// out(row, y_row) for every real row.  Unpacked slots; kNarrow: columns as
+// 16-bit offsets from the row (A.dcol).
+template <bool kNarrow, class Out>
 __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __restrict__ x, Out out) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gstride() >> 5;
@@ -194,6 +201,7 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
   const uint64_t pol = evict_first_policy();
   const int64_t* __restrict__ sp = A.slice_ptr;
   const int32_t* __restrict__ col = A.col;
+  const int16_t* __restrict__ dcol = A.dcol;
   const double* __restrict__ val = A.val;
   constexpr int U = EMG_SELL_BATCH;
   int64_t cs = warp;  // slice whose batch is being summed
@@ -213,7 +221,8 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
     for (int u = 0; u < U; ++u) {
       const bool in = fj + u < flen;
       const int64_t k = fbase + static_cast<int64_t>(kGroupStride) * (fj + u);
-      c[u] = in ? ld_stream(col + k, pol) : 0;
+      if constexpr (kNarrow) c[u] = in ? static_cast<int>(fs * kSliceRows + lane) + ld_stream(dcol + k, pol) : 0;
+      else c[u] = in ? ld_stream(col + k, pol) : 0;
       v[u] = in ? ld_stream(val + k, pol) : 0.0;
     }
     fj += U;
@@ -344,7 +353,7 @@ __device__ __forceinline__ void sell_rows_sliced(const Sell& A, const double* __
 
 template <bool kNarrow, class Out>
 __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
-  if constexpr (!kNarrow && !EMG_SELL_PACKED && EMG_SELL_PIPE == 2) sell_rows_stream(A, x, out);
+  if constexpr (!EMG_SELL_PACKED && EMG_SELL_PIPE == 2) sell_rows_stream<kNarrow>(A, x, out);
   else sell_rows_sliced<kNarrow>(A, x, out);
 }
 
@@ -811,6 +820,155 @@ __global__ void __launch_bounds__(kThreads) k_cg_direction(int64_t n, double* __
     p2[i] = pv;
   }
   if ((n & 1) && gtid() == 0) p[n - 1] = z[n - 1] + b * p[n - 1];
+}
+
+// CG update and direction in one cooperative launch (one block of
+// kFuseThreads per SM, all resident):
+//   x += alpha p,  r -= alpha q,  z = D^-1 r,  partial sums of r.z and r.r;
+//   grid barrier: the block that arrives last forms the sums, the residual
+//   test and beta (as k_cg_update) and then releases the others;
+//   p = z + beta p.
+// Every block owns a contiguous run of entry pairs and keeps z and the old p
+// of the first `stash` pairs of its run in shared memory, so z is neither
+// written nor read back and p is read once (8 vector passes per iteration
+// instead of the 11 of k_cg_update + k_cg_direction).  Pairs past the stash
+// go through z in global memory.  The barrier wait is bounded: a block that
+// gives up raises st->copy_err and skips the direction step; the next SpMV
+// then ends the solve with EMG_ERR_TIMEOUT.
+constexpr int kFuseThreads = 1024;
+constexpr int kBarrierSpins = 1 << 21;  // x >= 100 ns per poll: well over 0.2 s
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
+
+__global__ void __launch_bounds__(kFuseThreads, 1) k_cg_update_dir(
+    int64_t n, double* __restrict__ x, double* __restrict__ r, double* __restrict__ z,
+    double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ dinv,
+    double* partial, SolverState* st, double* hist, int32_t hist_cap, int64_t stash) {
+  extern __shared__ __align__(16) double2 keep[];  // [stash] z, then [stash] old p
+  __shared__ double red[kFuseThreads / 32];
+  __shared__ double sh_beta;
+  __shared__ int sh_go;
+  __shared__ int sh_last;
+  __shared__ uint32_t sh_gen;
+  if (st->done) return;
+  const double a = st->alpha;
+  const int64_t n2 = n >> 1;
+  const int64_t per = (n2 + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = min(n2, static_cast<int64_t>(blockIdx.x) * per);
+  const int64_t hi = min(n2, lo + per);
+  double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+  double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+  double2* __restrict__ z2 = reinterpret_cast<double2*>(z);
+  double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
+  const double2* __restrict__ q2 = reinterpret_cast<const double2*>(q);
+  const double2* __restrict__ d2 = reinterpret_cast<const double2*>(dinv);
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kFuseThreads) {
+    const double2 pv = p2[i], qv = q2[i], dv = d2[i];
+    double2 xv = x2[i], rv = r2[i], zv;
+    xv.x += a * pv.x;
+    xv.y += a * pv.y;
+    rv.x -= a * qv.x;
+    rv.y -= a * qv.y;
+    zv.x = dv.x * rv.x;
+    zv.y = dv.y * rv.y;
+    x2[i] = xv;
+    r2[i] = rv;
+    const int64_t li = i - lo;
+    if (li < stash) {
+      keep[li] = zv;
+      keep[stash + li] = pv;
+    } else {
+      z2[i] = zv;
+    }
+    rz += rv.x * zv.x + rv.y * zv.y;
+    rr += rv.x * rv.x + rv.y * rv.y;
+  }
+  const bool odd = (n & 1) && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0;
+  if (odd) {
+    const int64_t i = n - 1;
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    const double zi = dinv[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  const double brz = block_sum(rz, red);
+  const double brr = block_sum(rr, red);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = brz;
+    partial[gridDim.x + blockIdx.x] = brr;
+    sh_gen = ld_volatile(&st->gen);  // read before this block's ticket
+    __threadfence();
+    sh_last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (sh_last) {
+    __threadfence();
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += kFuseThreads) {
+      t0 += ld_l2(partial + i);
+      t1 += ld_l2(partial + gridDim.x + i);
+    }
+    const double tot0 = block_sum(t0, red);
+    const double tot1 = block_sum(t1, red);
+    if (threadIdx.x == 0) {
+      const int it = st->iter;
+      const double res = sqrt(tot1) / st->bnorm;
+      st->res = res;
+      if (it - 1 < hist_cap) hist[it - 1] = res;
+      if (res < st->tol) {
+        st->status = EMG_SUCCESS; st->done = 1;
+      } else if (it > 10 && res > st->prev * 1000.0) {  // iterative_solvers.cpp:477-483
+        st->status = EMG_DIVERGED; st->done = 1;
+      } else {
+        st->beta = tot0 / st->rz;
+        st->rz = tot0;
+        st->prev = res;
+        if (it >= st->max_iter) { st->status = EMG_MAX_ITER_REACHED; st->done = 1; }
+        else st->iter = it + 1;
+      }
+      sh_beta = st->beta;
+      sh_go = !st->done;
+      st->ticket = 0;
+      __threadfence();
+      atomicAdd(&st->gen, 1u);  // release the other blocks
+    }
+  } else if (threadIdx.x == 0) {
+    bool ok = false;
+    for (int k = 0; k < kBarrierSpins; ++k) {
+      if (ld_volatile(&st->gen) != sh_gen) { ok = true; break; }
+      __nanosleep(100);
+    }
+    __threadfence();
+    if (ok) {
+      sh_beta = *reinterpret_cast<const volatile double*>(&st->beta);
+      sh_go = !*reinterpret_cast<const volatile int32_t*>(&st->done);
+    } else {
+      atomicOr(&st->copy_err, 1);
+      sh_go = 0;
+    }
+  }
+  __syncthreads();
+  if (!sh_go) return;
+  const double b = sh_beta;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kFuseThreads) {
+    const int64_t li = i - lo;
+    double2 zv, pv;
+    if (li < stash) {
+      zv = keep[li];
+      pv = keep[stash + li];
+    } else {
+      zv = z2[i];
+      pv = p2[i];
+    }
+    pv.x = zv.x + b * pv.x;
+    pv.y = zv.y + b * pv.y;
+    p2[i] = pv;
+  }
+  if (odd) p[n - 1] = z[n - 1] + b * p[n - 1];
 }
 
 // ----------------------------------------------------------- BiCGSTAB ----
@@ -1295,6 +1453,63 @@ void give_back(int dev, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
 
 // Workspace vectors come from the stream-ordered pool (allocated on `st`,
 // returned with cudaFreeAsync once the device is idle).
+// Fused CG update + direction: used when the device takes cooperative
+// launches and one block of kFuseThreads with its shared-memory stash fits
+// on every SM; otherwise the two-kernel update stays.
+#ifndef EMG_CG_FUSE
+#define EMG_CG_FUSE 1
+#endif
+void setup_fuse(KrylovWorkspace& w) {
+  w.fuse = false;
+  if (!EMG_CG_FUSE || w.n < 2) return;
+  int dev = 0, coop = 0, sms = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      !coop || sms < 1) {
+    cudaGetLastError();
+    return;
+  }
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_cg_update_dir) != cudaSuccess) { cudaGetLastError(); return; }
+  const int64_t room = (static_cast<int64_t>(optin) - static_cast<int64_t>(fa.sharedSizeBytes)) / 32;
+  if (room < 1) return;
+  const int64_t n2 = w.n / 2;
+  const int64_t per = (n2 + sms - 1) / sms;
+  const int64_t stash = per < room ? per : room;
+  const size_t smem = static_cast<size_t>(stash) * 32;
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(k_cg_update_dir, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(room * 32)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_update_dir, kFuseThreads, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return;
+  }
+  w.fuse_grid = sms;  // one block per SM: at most the co-resident count
+  w.fuse_smem = smem;
+  w.fuse_stash = stash;
+  w.fuse = w.fuse_grid <= 4 * w.grid;  // the partial sums fit w.partial
+}
+
+// One fused CG update + direction (cooperative: all blocks co-resident).
+void launch_update_dir(KrylovWorkspace& w, int64_t n, cudaStream_t st) {
+  cudaLaunchConfig_t c = {};
+  c.gridDim = dim3(static_cast<unsigned>(w.fuse_grid));
+  c.blockDim = dim3(kFuseThreads);
+  c.dynamicSmemBytes = w.fuse_smem;
+  c.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  c.attrs = at;
+  c.numAttrs = 1;
+  cudaLaunchKernelEx(&c, k_cg_update_dir, n, w.x, w.r, w.z, w.p, static_cast<const double*>(w.q),
+                     static_cast<const double*>(w.dinv), w.partial, w.state, w.hist, w.hist_cap,
+                     w.fuse_stash);
+}
+
 int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
   if (!A.ws) {
     A.ws = new KrylovWorkspace();
@@ -1310,6 +1525,7 @@ int ensure_ws(DevCsr& A, bool bicg, int32_t max_iter, cudaStream_t st) {
     EMG_CK(cudaMemset(w.state, 0, sizeof(SolverState)));
     if (int rc = pinned_state_alloc(&w.state_h)) return rc;
     EMG_CK(cudaGetDevice(&w.dev));
+    setup_fuse(w);
     if (int rc = take_stream(&w.cap)) return rc;
     if (int rc = take_event(&w.ev0)) return rc;
     if (int rc = take_event(&w.ev1)) return rc;
@@ -1394,9 +1610,13 @@ void launch_iterations(DevCsr& A, bool bicg, int count) {
   for (int c = 0; c < count; ++c) {
     if (!bicg) {
       EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, w.cap, S, w.p, w.q, w.partial, w.state);
-      k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, w.cap>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
-                                             w.hist, w.hist_cap);
-      k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
+      if (w.fuse) {
+        launch_update_dir(w, A.n, w.cap);
+      } else {
+        k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, w.cap>>>(
+            A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state, w.hist, w.hist_cap);
+        k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, w.cap>>>(A.n, w.p, w.z, w.state);
+      }
     } else {
       k_bi_p<<<resident_grid<k_bi_p>(g), kThreads, 0, w.cap>>>(A.n, w.p, w.r, w.v, w.state);
       EMG_LAUNCH_SPMV(k_bi_v, S, g, w.cap, S, w.p, w.v, w.rh, w.partial, w.state);
@@ -1449,7 +1669,13 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   cudaGraphExec_t* loop = bicg ? &w.bi_loop : &w.cg_loop;
   if (!*loop && !w.loop_unavailable) {
     TraceScope t("solve.capture_loop");
-    if (capture_loop(A, bicg, loop) != EMG_SUCCESS) {
+    int crc = capture_loop(A, bicg, loop);
+    if (crc != EMG_SUCCESS && w.fuse && !bicg) {  // retry with the two-kernel update
+      w.fuse = false;
+      *loop = nullptr;
+      crc = capture_loop(A, bicg, loop);
+    }
+    if (crc != EMG_SUCCESS) {
       w.loop_unavailable = true;
       *loop = nullptr;
     }
@@ -1457,6 +1683,11 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   cudaGraphExec_t* exec = bicg ? &w.bi_exec : &w.cg_exec;
   if (!*loop && !*exec) {
     rc = capture_chunk(A, bicg, exec);
+    if (rc && w.fuse && !bicg) {
+      w.fuse = false;
+      *exec = nullptr;
+      rc = capture_chunk(A, bicg, exec);
+    }
     if (rc) { res->status = rc; return rc; }
   }
   const Sell& S = *A.sell;
@@ -1571,10 +1802,15 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms
     EMG_CK(cudaEventRecord(ev[4 * i], st));
     EMG_LAUNCH_SPMV(k_cg_spmv_dot, S, g, st, S, w.p, w.q, w.partial, w.state);
     EMG_CK(cudaEventRecord(ev[4 * i + 1], st));
-    k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, st>>>(A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state,
-                                        w.hist, w.hist_cap);
-    EMG_CK(cudaEventRecord(ev[4 * i + 2], st));
-    k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, st>>>(A.n, w.p, w.z, w.state);
+    if (w.fuse) {  // the fused update + direction counts as the update
+      launch_update_dir(w, A.n, st);
+      EMG_CK(cudaEventRecord(ev[4 * i + 2], st));
+    } else {
+      k_cg_update<<<resident_grid<k_cg_update>(g), kThreads, 0, st>>>(
+          A.n, w.x, w.r, w.z, w.p, w.q, w.dinv, w.partial, w.state, w.hist, w.hist_cap);
+      EMG_CK(cudaEventRecord(ev[4 * i + 2], st));
+      k_cg_direction<<<resident_grid<k_cg_direction>(g), kThreads, 0, st>>>(A.n, w.p, w.z, w.state);
+    }
     EMG_CK(cudaEventRecord(ev[4 * i + 3], st));
   }
   EMG_CK(cudaGetLastError());

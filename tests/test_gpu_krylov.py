@@ -181,3 +181,41 @@ def test_ilu0_and_unknown_preconditioners_are_rejected():
     cg.set_matrix(A)
     r = cg.solve(rhs)
     assert r.status == api.SolverStatus.INVALID_INPUT and "preconditioner 2" in r.error_msg
+
+
+@pytest.mark.parametrize("n", [2_500_001, 1_000_000])
+def test_large_tridiagonal_cg_matches_oracle(n):
+    """CG on tridiag(-1, 4 + (i mod 7)/10, -1): at 2,500,001 unknowns the
+    fused update + direction keeps only part of each block's run in shared
+    memory (the rest goes through z in global memory) and the odd last entry
+    takes its own path; 1,000,000 fits entirely."""
+    i = np.arange(n)
+    diag = 4.0 + (i % 7) * 0.1
+    rp = np.zeros(n + 1, np.int64)
+    counts = np.full(n, 3)
+    counts[0] = counts[-1] = 2
+    rp[1:] = np.cumsum(counts)
+    col = np.empty(rp[-1], np.int32)
+    val = np.empty(rp[-1], np.float64)
+    starts = rp[:-1]
+    # row i: (i-1, -1), (i, diag), (i+1, -1) in column order
+    has_lo = i > 0
+    k = starts.copy()
+    col[k[has_lo]] = i[has_lo] - 1
+    val[k[has_lo]] = -1.0
+    k[has_lo] += 1
+    col[k] = i
+    val[k] = diag
+    k += 1
+    has_hi = i < n - 1
+    col[k[has_hi]] = i[has_hi] + 1
+    val[k[has_hi]] = -1.0
+    b = np.random.default_rng(n).standard_normal(n)
+    A = HostCsr(rp.astype(np.int32), col, val)
+    x, out = solve(A.h, b, "cg", tol=1e-10, max_iter=500, precond=1)
+    xo, st, it, res = O.pcg(rp, col, val, b, tol=1e-10, max_iter=500, precond=1)
+    assert out.status == st == 0
+    assert abs(out.iterations - it) <= 2
+    assert rel(x, xo) <= 1e-9
+    r = b - O.spmv(rp, col, val, x)
+    assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b)
