@@ -37,16 +37,30 @@ __device__ __forceinline__ uint64_t evict_first_policy() {
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
+// EMG_LD_PREFETCH: 1 asks L2 to fetch 256-byte blocks for these loads.
+#ifndef EMG_LD_PREFETCH
+#define EMG_LD_PREFETCH 0
+#endif
 __device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
   double v;
+#if EMG_LD_PREFETCH
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.L2::256B.f64 %0, [%1], %2;"
+               : "=d"(v) : "l"(p), "l"(pol));
+#else
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
                : "=d"(v) : "l"(p), "l"(pol));
+#endif
   return v;
 }
 __device__ __forceinline__ int ld_stream(const int* p, uint64_t pol) {
   int v;
+#if EMG_LD_PREFETCH
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.L2::256B.s32 %0, [%1], %2;"
+               : "=r"(v) : "l"(p), "l"(pol));
+#else
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
                : "=r"(v) : "l"(p), "l"(pol));
+#endif
   return v;
 }
 // 16-bit signed load, sign-extended to int.
