@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="hex grid size (64 = the quoted workload)")
-    ap.add_argument("--cpu-iters", type=int, default=20, help="iterations in the CPU sample")
+    ap.add_argument("--cpu-iters", type=int, default=250,
+                    help="iterations in the CPU sample (about 10 s of 1-thread work at 64^3)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--workload", default="cube64",
