@@ -19,6 +19,7 @@ EMG_ERR_CUDA, EMG_ERR_TIMEOUT, EMG_ERR_NOMEM, EMG_ERR_INTERNAL = 5, 6, 7, 8
 GAUGE_NONE, GAUGE_REF, GAUGE_BOUNDARY_FIRST = -1, 0, 1
 FLAG_MASS, FLAG_NO_EDGE_SIGNS, FLAG_PIOLA_LITERAL, FLAG_QUAD3_LITERAL = 1, 2, 4, 8
 ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
+DOF_SCALAR_ONLY, DOF_VECTOR_EDGE_ONLY, DOF_MIXED_AV, DOF_ABSENT = 0, 1, 2, -2
 PRECOND_NONE, PRECOND_JACOBI = 0, 1
 
 I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -58,6 +59,8 @@ SIGNATURES = {
     "emg_mesh_material_tags": ([H, VP], C.c_int),
     "emg_edge_ids": ([H, VP, VP, C.POINTER(C.c_int64)], C.c_int),
     "emg_dof_build": ([H, C.c_int32, C.POINTER(H)], C.c_int),
+    "emg_dof_build_av": ([H, VP, C.c_int64, VP, C.c_int32, VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                          C.POINTER(C.c_int64)], C.c_int),
     "emg_dofmap_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "emg_dofmap_export": ([H, VP, VP], C.c_int),
     "emg_dofmap_expand": ([H, VP, VP], C.c_int),

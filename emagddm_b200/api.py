@@ -76,6 +76,9 @@ class EMMeshData:
     tets: np.ndarray                     # (T, 4) TET4_EDGE or (T, 8) HEX8_EDGE elements
     material_id: np.ndarray = None       # (T,)
     boundary_markers: list = field(default_factory=list)
+    # Element::dof_type per element (DOFType values or names); None = all
+    # VECTOR_EDGE_ONLY
+    dof_type: object = None
 
     @property
     def elem_type(self) -> int:
@@ -105,6 +108,27 @@ class EMMeshData:
                  if m.bnd_type == "DIRICHLET" and m.dof_type in ("VECTOR_EDGE_ONLY", "MIXED_AV")
                  and m.target_ids is not None and np.asarray(m.target_ids).ndim == 2]
         return np.concatenate(pairs) if pairs else np.zeros((0, 2), np.int32)
+
+    def dof_types(self):
+        """Element::dof_type of every element as DOFType values, or None when
+        every element is VECTOR_EDGE_ONLY."""
+        if self.dof_type is None:
+            return None
+        names = {"SCALAR_ONLY": _abi.DOF_SCALAR_ONLY, "VECTOR_EDGE_ONLY": _abi.DOF_VECTOR_EDGE_ONLY,
+                 "MIXED_AV": _abi.DOF_MIXED_AV}
+        t = [names[v] if isinstance(v, str) else int(v) for v in np.asarray(self.dof_type).ravel()]
+        t = np.ascontiguousarray(t, dtype=np.int32)
+        if t.shape[0] != self.getElementCount():
+            raise ValueError("dof_type needs one entry per element")
+        return None if np.all(t == _abi.DOF_VECTOR_EDGE_ONLY) else t
+
+    def scalar_dirichlet_nodes(self) -> np.ndarray:
+        """Node IDs of every DIRICHLET marker on scalar DOFs
+        (markConstrainedDOFs, em_dof_manager.cpp:163-177)."""
+        nodes = [np.asarray(m.target_ids, dtype=np.int32).ravel() for m in self.boundary_markers
+                 if m.bnd_type == "DIRICHLET" and m.dof_type in ("SCALAR_ONLY", "MIXED_AV")
+                 and m.target_ids is not None and np.asarray(m.target_ids).ndim == 1]
+        return np.concatenate(nodes) if nodes else np.zeros(0, np.int32)
 
     def hole_marker_count(self) -> int:
         """Markers the reference's heuristic counts as holes
@@ -194,6 +218,9 @@ class EMDOFManager:
     def _run(self, gauge: int):
         if self._mesh is None:
             self._mesh = _Mesh(self.mesh_data)
+        types = self.mesh_data.dof_types()
+        if types is not None:
+            return self._run_av(gauge, types)
         h = C.c_void_p()
         check(lib().emg_dof_build(self._mesh.h, gauge, C.byref(h)), "emg_dof_build")
         ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
@@ -205,6 +232,19 @@ class EMDOFManager:
             lib().emg_dofmap_destroy(self._map)
         self._map = h
         return l2g, ed, nf.value, nd.value
+
+    def _run_av(self, gauge: int, types: np.ndarray):
+        """Scalar / edge / A-V elements: rows of nodes + edges entries,
+        Local2Global::indices padded with DOF_ABSENT."""
+        md = self.mesh_data
+        sd = np.ascontiguousarray(md.scalar_dirichlet_nodes(), dtype=np.int32)
+        w = np.asarray(md.tets).shape[1] + md.edges_per_element()
+        l2g = np.empty((md.getElementCount(), w), np.int32)
+        ns, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().emg_dof_build_av(self._mesh.h, ptr(types), sd.size, ptr(sd) if sd.size else None, gauge,
+                                     ptr(l2g), C.byref(ns), C.byref(nf), C.byref(nd)), "emg_dof_build_av")
+        self._n_scalar_free = ns.value
+        return l2g, None, nf.value, nd.value
 
     def build(self) -> None:
         self._l2g, self._edge_dof, self._n_free, self._n_dofs = self._run(_abi.GAUGE_NONE)
@@ -225,12 +265,24 @@ class EMDOFManager:
         return self._n_free
 
     def getElemLocalToGlobal(self) -> np.ndarray:
+        """(T, epe) for edge-only meshes; with per-element DOF types (T,
+        nodes + edges), each row Local2Global::indices padded with DOF_ABSENT."""
         return self._l2g
+
+    def getElemLocalToGlobalList(self) -> list:
+        """Local2Global::indices of every element, without padding."""
+        return [row[row != _abi.DOF_ABSENT] for row in self._l2g]
+
+    def getNumScalarFreeDOFs(self) -> int:
+        """Free nodal (scalar) DOFs; they take equations 0 .. n - 1."""
+        return getattr(self, "_n_scalar_free", 0)
 
     def getEdgeToDOF(self) -> np.ndarray:
         return self._edge_dof
 
     def mapReducedSolutionToFull(self, reduced) -> np.ndarray:
+        if self._map is None:
+            raise RuntimeError("mapReducedSolutionToFull needs an edge-only map built by build()")
         reduced = np.ascontiguousarray(reduced, dtype=np.float64)
         full = np.empty(self._edge_dof.shape[0])
         check(lib().emg_dofmap_expand(self._map, ptr(reduced), ptr(full)), "emg_dofmap_expand")

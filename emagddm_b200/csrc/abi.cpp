@@ -340,6 +340,24 @@ int emg_dof_build(emg_mesh mesh, int32_t gauge_mode, emg_dofmap* out) {
   });
 }
 
+int emg_dof_build_av(emg_mesh mesh, const int32_t* dof_type, int64_t n_scalar_dirichlet,
+                     const int32_t* scalar_dirichlet, int32_t gauge_mode, int32_t* l2g,
+                     int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs) {
+  return guarded([&]() -> int {
+    if (!mesh) { set_error("null handle"); return EMG_INVALID_INPUT; }
+    std::vector<int32_t> rows;
+    int64_t ns = 0, nf = 0, nd = 0;
+    int rc = emg::build_dofmap_av(mesh->m, dof_type, n_scalar_dirichlet, scalar_dirichlet, gauge_mode, rows,
+                                  ns, nf, nd);
+    if (rc) return rc;
+    if (l2g && !rows.empty()) std::memcpy(l2g, rows.data(), sizeof(int32_t) * rows.size());
+    if (n_scalar_free) *n_scalar_free = ns;
+    if (n_free) *n_free = nf;
+    if (n_dofs) *n_dofs = nd;
+    return EMG_SUCCESS;
+  });
+}
+
 int emg_dofmap_info(emg_dofmap map, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs) {
   if (!map) { set_error("null dofmap"); return EMG_INVALID_INPUT; }
   if (n_edges) *n_edges = map->d.n_edges;

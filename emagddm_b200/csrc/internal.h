@@ -61,6 +61,11 @@ struct DofMap {
 int build_edge_ids(Mesh& m);
 int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out);
 int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, DofMap& out);
+// EMDOFManager with per-element DOF types (SCALAR_ONLY / VECTOR_EDGE_ONLY /
+// MIXED_AV); l2g rows of npe + epe entries padded with EMG_DOF_ABSENT.
+int build_dofmap_av(const Mesh& m, const int32_t* dof_type, int64_t n_sdir, const int32_t* sdir,
+                    int32_t gauge_mode, std::vector<int32_t>& l2g, int64_t& n_scalar_free, int64_t& n_free,
+                    int64_t& n_dofs);
 // Gmsh ASCII reader (gmsh.cpp); material_tags[i] = physical tag of material i.
 int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_tags, Mesh& m,
               std::vector<int32_t>& material_tags);

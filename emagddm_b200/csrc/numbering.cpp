@@ -321,6 +321,90 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
   return EMG_SUCCESS;
 }
 
+// Per-element DOF types (Element::dof_type, include/fe_em/em_mesh_data.hpp:45-49).
+// Scalar unknowns: the nodes of SCALAR_ONLY / MIXED_AV elements, prenumbered
+// in ascending node ID (assignPrenumbering, em_dof_manager.cpp:91-150),
+// constrained by the scalar Dirichlet node list (markConstrainedDOFs,
+// :152-243) and ranked first among the free DOFs (renumberFreeDOFs,
+// :245-286).  Edge unknowns: GlobalEdgeIDGenerator and the tree gauge see
+// only VECTOR_EDGE_ONLY / MIXED_AV elements (global_edge_id_generator.cpp:44-53,
+// mesh_graph_extractor.cpp:78), so they are the edge numbering of that
+// sub-mesh (same node IDs, Dirichlet pairs and hole markers) shifted past
+// the free scalars, both before the gauge and after it
+// (renumberVectorDOFsWithTreeGauge, :501-626).  Element rows follow
+// buildScalar/Vector/MixedAVElementMapping (:318-446).
+int build_dofmap_av(const Mesh& m, const int32_t* dof_type, int64_t n_sdir, const int32_t* sdir,
+                    int32_t gauge_mode, std::vector<int32_t>& l2g, int64_t& n_scalar_free, int64_t& n_free,
+                    int64_t& n_dofs) {
+  const int npe = m.npe(), epe = m.epe(), w = npe + epe;
+  const int64_t T = m.n_elems;
+  if (gauge_mode != EMG_GAUGE_NONE && gauge_mode != EMG_GAUGE_REF && gauge_mode != EMG_GAUGE_BOUNDARY_FIRST) {
+    set_error("unknown gauge mode");
+    return EMG_INVALID_INPUT;
+  }
+  if (n_sdir < 0 || (n_sdir > 0 && !sdir)) {
+    set_error("scalar Dirichlet list: negative count or null pointer");
+    return EMG_INVALID_INPUT;
+  }
+  auto type_of = [&](int64_t e) { return dof_type ? dof_type[e] : static_cast<int32_t>(EMG_DOF_MIXED_AV); };
+  Mesh sub;
+  sub.elem_type = m.elem_type;
+  sub.n_nodes = m.n_nodes;
+  sub.dirichlet = m.dirichlet;
+  sub.n_hole_markers = m.n_hole_markers;
+  std::vector<uint8_t> scalar_node(static_cast<size_t>(m.n_nodes), 0);
+  for (int64_t e = 0; e < T; ++e) {
+    const int32_t t = type_of(e);
+    if (t != EMG_DOF_SCALAR_ONLY && t != EMG_DOF_VECTOR_EDGE_ONLY && t != EMG_DOF_MIXED_AV) {
+      set_error("dof_type of element " + std::to_string(e) + " is not SCALAR_ONLY, VECTOR_EDGE_ONLY or MIXED_AV");
+      return EMG_INVALID_INPUT;
+    }
+    const int32_t* nodes = m.elems.data() + static_cast<size_t>(npe) * e;
+    if (t != EMG_DOF_VECTOR_EDGE_ONLY)
+      for (int i = 0; i < npe; ++i) scalar_node[nodes[i]] = 1;
+    if (t != EMG_DOF_SCALAR_ONLY) {
+      sub.elems.insert(sub.elems.end(), nodes, nodes + npe);
+      sub.n_elems++;
+    }
+  }
+  // Node IDs outside the mesh or on no scalar element constrain nothing, as
+  // in the reference (the marker's node is not among the prenumbers).
+  for (int64_t i = 0; i < n_sdir; ++i)
+    if (sdir[i] >= 0 && sdir[i] < m.n_nodes && scalar_node[sdir[i]]) scalar_node[sdir[i]] = 2;
+  std::vector<int32_t> sfree(static_cast<size_t>(m.n_nodes), -1);
+  int64_t ns = 0;
+  for (int64_t v = 0; v < m.n_nodes; ++v)
+    if (scalar_node[v] == 1) sfree[v] = static_cast<int32_t>(ns++);
+  DofMap vm;
+  if (sub.n_elems > 0) {
+    if (int rc = build_dofmap(sub, gauge_mode, vm)) return rc;
+  }
+  if (ns + vm.n_free > INT32_MAX) {
+    set_error("too many DOFs for 32-bit indices");
+    return EMG_INVALID_INPUT;
+  }
+  l2g.assign(static_cast<size_t>(w) * T, EMG_DOF_ABSENT);
+  int64_t se = 0;
+  for (int64_t e = 0; e < T; ++e) {
+    const int32_t t = type_of(e);
+    int32_t* row = l2g.data() + static_cast<size_t>(w) * e;
+    int c = 0;
+    if (t != EMG_DOF_VECTOR_EDGE_ONLY)
+      for (int i = 0; i < npe; ++i) row[c++] = sfree[m.elems[static_cast<size_t>(npe) * e + i]];
+    if (t != EMG_DOF_SCALAR_ONLY) {
+      for (int j = 0; j < epe; ++j) {
+        const int32_t d = vm.l2g[static_cast<size_t>(epe) * se + j];
+        row[c++] = d < 0 ? -1 : static_cast<int32_t>(d + ns);
+      }
+      ++se;
+    }
+  }
+  n_scalar_free = ns;
+  n_free = ns + vm.n_free;
+  n_dofs = ns + vm.n_dofs;
+  return EMG_SUCCESS;
+}
+
 // Tree-cotree gauge for a non-overlapping partition of the elements (no
 // counterpart in the reference, whose FETI-DP context is a stub:
 // include/fetidp/fetidp_context.hpp:20-66).  Edges are ranked by class:

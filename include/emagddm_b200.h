@@ -169,6 +169,30 @@ int emg_dofmap_export(emg_dofmap map, int32_t* l2g, int32_t* edge_dof);
 int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full);
 void emg_dofmap_destroy(emg_dofmap map);
 
+/* ---- Per-element DOF types: EMDOFManager::build with Element::dof_type
+ * (include/fe_em/em_mesh_data.hpp:45-49).  SCALAR_ONLY elements carry nodal
+ * DOFs, VECTOR_EDGE_ONLY edge DOFs, MIXED_AV both (the A-V formulation):
+ * assignPrenumbering (src/fe_em/em_dof_manager.cpp:91-150) numbers the nodes
+ * of the scalar-carrying elements in ascending ID, then the edges of the
+ * vector-carrying elements by first appearance; markConstrainedDOFs
+ * (:152-243) takes the scalar_dirichlet node IDs and the mesh's Dirichlet
+ * edge pairs; renumberFreeDOFs (:245-286) ranks the unconstrained, scalars
+ * first; the element maps (:288-446) list node DOFs, edge DOFs, or node then
+ * edge DOFs.  For gauge_mode >= 0, applyTreeGauge (:448-626) gauges the edge
+ * DOFs with the tree of the vector-carrying elements; they keep following
+ * the free scalar DOFs.
+ * dof_type: n_elems values, or NULL for all MIXED_AV.
+ * l2g: (nodes_per_elem + edges_per_elem) * n_elems or NULL; row e holds
+ *   Local2Global::indices of element e, padded with EMG_DOF_ABSENT
+ *   (-1 = constrained DOF or tree edge, as everywhere).
+ * n_scalar_free: free scalar DOFs, equations 0 .. n_scalar_free - 1;
+ * n_free: free DOFs before the gauge; n_dofs: equations.  Any output may be
+ * NULL.  EMG_INVALID_INPUT for a dof_type value outside the enum. */
+enum { EMG_DOF_SCALAR_ONLY = 0, EMG_DOF_VECTOR_EDGE_ONLY = 1, EMG_DOF_MIXED_AV = 2, EMG_DOF_ABSENT = -2 };
+int emg_dof_build_av(emg_mesh mesh, const int32_t* dof_type, int64_t n_scalar_dirichlet,
+                     const int32_t* scalar_dirichlet, int32_t gauge_mode, int32_t* l2g,
+                     int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs);
+
 /* ---- Tree-cotree gauge for a non-overlapping partition of the tets, the
  * numbering the FETI-DP solver below works on.  No reference counterpart:
  * the reference's FETI-DP layer is a stub (include/fetidp/fetidp_context.hpp:20-66,

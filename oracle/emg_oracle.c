@@ -960,3 +960,79 @@ int orc_bicgstab(int64_t n, const int64_t* rp, const int32_t* col, const double*
   free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv);
   return status;
 }
+
+/* ------------------------------------------------------------------------
+ * Per-element DOF types (MIXED_AV): see emg_oracle.h.  The scalar part is
+ * restated here; the edge part runs the edge-ID and DOF/gauge restatement
+ * above on the vector-carrying elements in their order, which is the mesh
+ * GlobalEdgeIDGenerator and MeshGraphExtractor see
+ * (mesh_graph_extractor.cpp:78, :182). */
+int orc_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems,
+                     const int32_t* dof_type, int64_t n_dir, const int32_t* dir_pairs, int64_t n_sdir,
+                     const int32_t* sdir_nodes, int32_t n_hole_markers, int32_t gauge, int32_t* l2g,
+                     int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs) {
+  const int npe = elem_type == ORC_ELEM_HEX8_EDGE ? 8 : 4, epe = elem_type == ORC_ELEM_HEX8_EDGE ? 12 : 6;
+  const int w = npe + epe;
+  int64_t i, e, nv = 0, nsf = 0, ne = 0, vf = 0, vd = 0, k = 0;
+  int32_t root = -1;
+  int rc = 0;
+  for (e = 0; e < n_elems; ++e) {
+    if (dof_type[e] < 0 || dof_type[e] > 2) return -1;
+    if (dof_type[e] != ORC_DOF_SCALAR_ONLY) nv++;
+  }
+  /* scalar prenumbers: nodes of SCALAR_ONLY / MIXED_AV elements, ascending */
+  uint8_t* ref = calloc((size_t)(n_nodes > 0 ? n_nodes : 1), 1);
+  uint8_t* con = calloc((size_t)(n_nodes > 0 ? n_nodes : 1), 1);
+  int32_t* sfree = malloc(sizeof(int32_t) * (size_t)(n_nodes > 0 ? n_nodes : 1));
+  int32_t* vel = malloc(sizeof(int32_t) * (size_t)(npe * (nv > 0 ? nv : 1)));
+  int32_t* vee = malloc(sizeof(int32_t) * (size_t)(epe * (nv > 0 ? nv : 1)));
+  int32_t* vl2g = malloc(sizeof(int32_t) * (size_t)(epe * (nv > 0 ? nv : 1)));
+  int32_t* ven = malloc(sizeof(int32_t) * (size_t)(2 * epe * (nv > 0 ? nv : 1)));
+  int32_t* vdof = malloc(sizeof(int32_t) * (size_t)(epe * (nv > 0 ? nv : 1)));
+  if (!ref || !con || !sfree || !vel || !vee || !vl2g || !ven || !vdof) { rc = -2; goto done; }
+  for (e = 0; e < n_elems; ++e)
+    if (dof_type[e] != ORC_DOF_VECTOR_EDGE_ONLY)
+      for (i = 0; i < npe; ++i) {
+        const int32_t v = elems[npe * e + i];
+        if (v < 0 || v >= n_nodes) { rc = -1; goto done; }
+        ref[v] = 1;
+      }
+  for (i = 0; i < n_sdir; ++i)
+    if (sdir_nodes[i] >= 0 && sdir_nodes[i] < n_nodes) con[sdir_nodes[i]] = 1;
+  for (i = 0; i < n_nodes; ++i) sfree[i] = (ref[i] && !con[i]) ? (int32_t)nsf++ : -1;
+  /* edge part on the vector-carrying elements */
+  for (e = 0; e < n_elems; ++e)
+    if (dof_type[e] != ORC_DOF_SCALAR_ONLY) {
+      memcpy(vel + npe * k, elems + npe * e, sizeof(int32_t) * (size_t)npe);
+      k++;
+    }
+  if (nv > 0) {
+    rc = orc_edge_ids_typed(elem_type, nv, vel, vee, ven, &ne);
+    if (!rc)
+      rc = orc_dof_build_typed(elem_type, nv, vel, vee, ven, ne, n_dir, dir_pairs, n_hole_markers, gauge, vl2g,
+                               vdof, &vf, &vd, &root);
+    if (rc) goto done;
+  }
+  /* rows: node DOFs, then edge DOFs offset by the free scalars, then -2 */
+  k = 0;
+  for (e = 0; e < n_elems; ++e) {
+    int32_t* row = l2g + (int64_t)w * e;
+    int c = 0;
+    for (i = 0; i < w; ++i) row[i] = -2;
+    if (dof_type[e] != ORC_DOF_VECTOR_EDGE_ONLY)
+      for (i = 0; i < npe; ++i) row[c++] = sfree[elems[npe * e + i]];
+    if (dof_type[e] != ORC_DOF_SCALAR_ONLY) {
+      for (i = 0; i < epe; ++i) {
+        const int32_t d = vl2g[epe * k + i];
+        row[c++] = d < 0 ? -1 : (int32_t)(d + nsf);
+      }
+      k++;
+    }
+  }
+  *n_scalar_free = nsf;
+  *n_free = nsf + vf;
+  *n_dofs = nsf + vd;
+done:
+  free(ref); free(con); free(sfree); free(vel); free(vee); free(vl2g); free(ven); free(vdof);
+  return rc;
+}

@@ -128,6 +128,29 @@ int orc_dof_build_typed(int32_t elem_type, int64_t n_elems, const int32_t* elems
                         int64_t* n_dofs, int32_t* root_node);
 int orc_pattern_typed(int32_t elem_type, int64_t n_elems, const int32_t* l2g, int64_t n_dofs,
                       int64_t* row_ptr, int32_t* col, int64_t* nnz);
+
+/* EMDOFManager::build (+ applyTreeGauge when gauge >= 0) with per-element
+ * Element::dof_type (ORC_DOF_SCALAR_ONLY / VECTOR_EDGE_ONLY / MIXED_AV,
+ * include/fe_em/em_mesh_data.hpp:45-49):
+ *   assignPrenumbering  (src/fe_em/em_dof_manager.cpp:91-150): nodes of the
+ *     scalar-carrying elements in ascending node ID, then the edges of the
+ *     vector-carrying elements by first appearance (GlobalEdgeIDGenerator
+ *     skips scalar-only elements, global_edge_id_generator.cpp:44-53);
+ *   markConstrainedDOFs (:152-243): scalar_dirichlet node IDs, dir_pairs edges;
+ *   renumberFreeDOFs    (:245-286): free index = rank among the unconstrained
+ *     prenumbers (scalars first);
+ *   buildMappingTables  (:288-446): node DOFs, edge DOFs, or node then edge
+ *     DOFs per element;
+ *   renumberVectorDOFsWithTreeGauge (:501-626): the tree gauge of the
+ *     vector-carrying elements, edge DOF = n_scalar_free + reduced index.
+ * l2g: (npe + epe) * n_elems, each row Local2Global::indices padded with -2. */
+#define ORC_DOF_SCALAR_ONLY 0
+#define ORC_DOF_VECTOR_EDGE_ONLY 1
+#define ORC_DOF_MIXED_AV 2
+int orc_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems,
+                     const int32_t* dof_type, int64_t n_dir, const int32_t* dir_pairs, int64_t n_sdir,
+                     const int32_t* sdir_nodes, int32_t n_hole_markers, int32_t gauge, int32_t* l2g,
+                     int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs);
 int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,
                        const int32_t* elems, const int32_t* material, const int32_t* l2g,
                        const double* nu_mat, const double* sigma_mat, int32_t n_mat,

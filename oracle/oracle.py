@@ -134,6 +134,30 @@ def dof_build(tets, dirichlet, gauge=GAUGE_REF, n_holes=0, elem_edge=None, edge_
                 edge_dof=edge_dof, n_edges=E, n_free=nf.value, n_dofs=nd.value, root=root.value)
 
 
+def dof_build_av(elems, dof_type, dirichlet, scalar_dirichlet, gauge=GAUGE_REF, n_holes=0, n_nodes=None):
+    """EMDOFManager with per-element DOFType (0 SCALAR_ONLY, 1 VECTOR_EDGE_ONLY,
+    2 MIXED_AV): rows of npe + epe entries (Local2Global::indices, padded -2)."""
+    elems = np.ascontiguousarray(elems, dtype=np.int32)
+    et = elem_type_of(elems)
+    w = elems.shape[1] + edges_per_elem(et)
+    T = elems.shape[0]
+    if n_nodes is None:
+        n_nodes = int(elems.max()) + 1 if elems.size else 0
+    dt = np.ascontiguousarray(dof_type, np.int32)
+    d = np.ascontiguousarray(dirichlet, dtype=np.int32).reshape(-1)
+    sd = np.ascontiguousarray(scalar_dirichlet, dtype=np.int32).reshape(-1)
+    l2g = np.empty(w * T, np.int32)
+    nsf, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+    L = lib()
+    L.orc_dof_build_av.argtypes = [C.c_int32, C.c_int64, C.c_int64, I32P, I32P, C.c_int64, I32P, C.c_int64, I32P,
+                                   C.c_int32, C.c_int32, I32P, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = L.orc_dof_build_av(et, n_nodes, T, elems.ravel(), dt, d.size // 2, d if d.size else np.zeros(2, np.int32),
+                            sd.size, sd if sd.size else np.zeros(1, np.int32), n_holes, gauge, l2g,
+                            C.byref(nsf), C.byref(nf), C.byref(nd))
+    assert rc == 0, rc
+    return dict(l2g=l2g.reshape(T, w), n_scalar_free=nsf.value, n_free=nf.value, n_dofs=nd.value)
+
+
 def element(X, nu=1.0, sigma=0.0, sources=(), flags=0):
     X = np.ascontiguousarray(X, dtype=np.float64).reshape(12)
     K, M, F = np.empty(36), np.empty(36), np.empty(6)

@@ -141,6 +141,48 @@ int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, con
   }
 }
 
+// EMDOFManager::build (+ applyTreeGauge) on elements with per-element
+// Element::dof_type (0 SCALAR_ONLY, 1 VECTOR_EDGE_ONLY, 2 MIXED_AV) and a
+// DIRICHLET marker on scalar DOFs (node IDs) next to the one on edges.
+// l2g_out rows hold npe + epe entries: Local2Global::indices, the rest -2.
+int refb_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems,
+                      const int32_t* dof_type, int64_t n_dir, const int32_t* dir_pairs, int64_t n_sdir,
+                      const int32_t* sdir_nodes, int32_t n_hole_markers, int32_t apply_gauge,
+                      int32_t* l2g_out, int64_t* n_free, int64_t* n_dofs) {
+  const int npe = elem_type == 1 ? 8 : 4, epe = elem_type == 1 ? 12 : 6;
+  try {
+    auto mesh = make_mesh(n_nodes, nullptr, n_elems, elems, n_dir, dir_pairs, n_hole_markers, elem_type);
+    for (int64_t t = 0; t < n_elems; ++t)
+      mesh.elements[t].dof_type = dof_type[t] == 0   ? fe_em::DOFType::SCALAR_ONLY
+                                  : dof_type[t] == 1 ? fe_em::DOFType::VECTOR_EDGE_ONLY
+                                                     : fe_em::DOFType::MIXED_AV;
+    fe_em::EMBoundaryMarker sm;
+    sm.id = 100;
+    sm.bnd_type = tool::BndType::DIRICHLET;
+    sm.dof_type = fe_em::DOFType::SCALAR_ONLY;
+    sm.target_ids = std::vector<int>(sdir_nodes, sdir_nodes + n_sdir);
+    sm.value = 0.0;
+    sm.name = "outer_potential";
+    mesh.boundary_markers.push_back(sm);
+    fe_em::GlobalEdgeIDGenerator gen(mesh);
+    gen.generate();
+    fe_em::EMDOFManager dm(mesh, gen.getElemLocalToGlobalEdge(), &gen);
+    dm.build();
+    *n_free = dm.getNumFreeDOFs();
+    if (apply_gauge) dm.applyTreeGauge();
+    *n_dofs = dm.getNumFreeDOFs();
+    const auto& l2g = dm.getElemLocalToGlobal();
+    for (int64_t t = 0; t < n_elems; ++t) {
+      const auto& ix = l2g[t].indices;
+      if (static_cast<int>(ix.size()) > npe + epe) return -3;
+      for (int k = 0; k < npe + epe; ++k) l2g_out[(npe + epe) * t + k] = k < static_cast<int>(ix.size()) ? ix[k] : -2;
+    }
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
+
 // Merged CSR pattern via EMAssembly (placeholder integrator) + to_eigen.
 // col_out may be NULL (count only).  raw_nnz = entries before merging.
 int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_tets,

@@ -80,6 +80,29 @@ def dof_build(n_nodes, tets, dirichlet, gauge=True, n_holes=0):
                 n_free=nf.value, n_dofs=nd.value)
 
 
+def dof_build_av(n_nodes, elems, dof_type, dirichlet, scalar_dirichlet, gauge=True, n_holes=0):
+    """EMDOFManager with per-element DOFType (0 SCALAR_ONLY, 1 VECTOR_EDGE_ONLY,
+    2 MIXED_AV) and a scalar DIRICHLET marker on `scalar_dirichlet` nodes.
+    Rows of l2g: npe + epe entries, Local2Global::indices padded with -2."""
+    elems = np.ascontiguousarray(elems, np.int32)
+    et = _elem_type(elems)
+    w = (8 + 12) if et else (4 + 6)
+    T = elems.shape[0]
+    dt = np.ascontiguousarray(dof_type, np.int32)
+    d = np.ascontiguousarray(dirichlet, np.int32).reshape(-1)
+    sd = np.ascontiguousarray(scalar_dirichlet, np.int32).reshape(-1)
+    l2g = np.empty(w * T, np.int32)
+    nf, nd = C.c_int64(), C.c_int64()
+    L = lib()
+    L.refb_dof_build_av.argtypes = [C.c_int32, C.c_int64, C.c_int64, I32P, I32P, C.c_int64, I32P, C.c_int64,
+                                    I32P, C.c_int32, C.c_int32, I32P, C.c_void_p, C.c_void_p]
+    rc = L.refb_dof_build_av(et, n_nodes, T, elems.ravel(), dt, d.size // 2, d if d.size else np.zeros(2, np.int32),
+                             sd.size, sd if sd.size else np.zeros(1, np.int32), n_holes, int(gauge), l2g,
+                             C.byref(nf), C.byref(nd))
+    assert rc == 0, rc
+    return dict(l2g=l2g.reshape(T, w), n_free=nf.value, n_dofs=nd.value)
+
+
 def pattern(xyz, tets, l2g):
     tets = np.ascontiguousarray(tets, np.int32)
     et = _elem_type(tets)

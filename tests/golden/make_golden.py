@@ -5,10 +5,11 @@ reference sources (`make -C oracle -f Makefile.ref`).  Every fixture comes
 from the reference's own code path (GlobalEdgeIDGenerator, EMDOFManager,
 TreeGauge, EMAssembly + SparseConverter, CGSolver, BiCGSTABSolver,
 NedelecElement, GaussQuadrature, MagneticVector3DIntegrator) on the synthetic
-Kuhn-split cube meshes of emagddm_b200.mesh, and the HEX8_EDGE fixtures on
-the hex grids of the same module:
+Kuhn-split cube meshes of emagddm_b200.mesh, the HEX8_EDGE fixtures on the
+hex grids of the same module, and the per-element DOF-type (MIXED_AV)
+fixtures on both:
 
-  python tests/golden/make_golden.py [--hex-only]
+  python tests/golden/make_golden.py [--hex-only | --av-only]
 """
 from __future__ import annotations
 
@@ -75,10 +76,52 @@ def hex_fixtures():
     print("wrote", len(arrays), "hex arrays and", len(counts), "hex count records")
 
 
+def av_patterns(T):
+    """Element::dof_type patterns of the per-element DOF-type fixtures
+    (0 SCALAR_ONLY, 1 VECTOR_EDGE_ONLY, 2 MIXED_AV)."""
+    half = np.arange(T) < T // 2
+    return {"all_av": np.full(T, 2, np.int32),
+            "cycle": (np.arange(T) % 3).astype(np.int32),
+            "av_vector": np.where(half, 2, 1).astype(np.int32),
+            "av_scalar": np.where(half, 2, 0).astype(np.int32)}
+
+
+def av_meshes():
+    m = mesh.plain_small(3)
+    yield "tet3", m.xyz, m.tets, m.dirichlet
+    xyz, hexes, d = mesh.hex_topology(3)
+    yield "hex3", xyz, hexes, d
+
+
+def av_fixtures():
+    """Per-element DOF types (reference_av_fixtures.npz / reference_av_counts.json):
+    EMDOFManager with SCALAR_ONLY / VECTOR_EDGE_ONLY / MIXED_AV elements and a
+    scalar DIRICHLET marker on every second boundary node."""
+    counts = {}
+    arrays = {}
+    for name, xyz, el, d in av_meshes():
+        bnd = np.unique(np.asarray(d).ravel()).astype(np.int32)[::2]
+        for pat, dt in av_patterns(el.shape[0]).items():
+            for holes in (0, 2):
+                for gauge in (False, True):
+                    r = R.dof_build_av(len(xyz), el, dt, d, bnd, gauge=gauge, n_holes=holes)
+                    key = f"{name}_{pat}_h{holes}_{'gauge' if gauge else 'free'}"
+                    arrays[key] = r["l2g"].astype(np.int32)
+                    counts[key] = dict(n_free=r["n_free"], n_dofs=r["n_dofs"])
+    np.savez_compressed(os.path.join(HERE, "reference_av_fixtures.npz"), **arrays)
+    with open(os.path.join(HERE, "reference_av_counts.json"), "w") as f:
+        json.dump(counts, f, indent=1, sort_keys=True)
+    print("wrote", len(arrays), "per-element DOF-type arrays")
+
+
 def main():
     assert R.available(), "build oracle/_ref first (make -C oracle -f Makefile.ref)"
+    R.lib().refb_quiet(1)
     if "--hex-only" in sys.argv:
         hex_fixtures()
+        return
+    if "--av-only" in sys.argv:
+        av_fixtures()
         return
     counts = {}
     arrays = {}
@@ -129,6 +172,7 @@ def main():
         json.dump(counts, f, indent=1, sort_keys=True)
     print("wrote", len(arrays), "arrays and", len(counts), "count records")
     hex_fixtures()
+    av_fixtures()
 
 
 if __name__ == "__main__":
