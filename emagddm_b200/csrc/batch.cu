@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "device.h"
+#include "trace.h"
 
 namespace emg {
 
@@ -36,6 +37,13 @@ constexpr int kBWarps = kBThreads / 32;
 constexpr int kMaxLocal = 64;   // blocks touched by one CTA
 constexpr int kWindowB = 4096;  // length-sort window (inside a block)
 constexpr int kBodyB = 4;       // iterations per while-loop body
+// CTAs per SM the slices are split into (each CTA ~ the same number of
+// slots).  A CTA whose blocks have all converged returns at once, so more,
+// smaller CTAs let the block scheduler spread the blocks still iterating
+// over the whole GPU.
+#ifndef EMG_BATCH_CTAS_PER_SM
+#define EMG_BATCH_CTAS_PER_SM 4
+#endif
 
 }  // namespace
 
@@ -388,13 +396,18 @@ __global__ void k_b_values(int64_t slots, const int32_t* __restrict__ src, const
 }
 
 // Every column of a row lies inside the row's block.
+// *bad = 1 if a row has a column outside its block (blocks: nb + 1 row
+// offsets; the block of row i is the last k with blocks[k] <= i).
 __global__ void k_b_check(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                          const int32_t* __restrict__ row_block, const int64_t* __restrict__ blocks,
-                          int32_t* __restrict__ bad) {
+                          int32_t nb, const int64_t* __restrict__ blocks, int32_t* __restrict__ bad) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t k = row_block[i];
-    const int64_t lo = blocks[k], hi = blocks[k + 1];
+    int32_t a = 0, b = nb;  // blocks[a] <= i < blocks[b]
+    while (b - a > 1) {
+      const int32_t m = (a + b) >> 1;
+      if (blocks[m] <= i) a = m; else b = m;
+    }
+    const int64_t lo = blocks[a], hi = blocks[a + 1];
     for (int32_t e = rp[i]; e < rp[i + 1]; ++e)
       if (col[e] < lo || col[e] >= hi) { atomicOr(bad, 1); break; }
   }
@@ -405,6 +418,81 @@ __global__ void k_b_scatter(int64_t N, const int32_t* __restrict__ perm, const d
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < N;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     if (perm[i] >= 0) out[perm[i]] = in[i];
+}
+
+// Plan on the device.  Window w holds rows [row0[w], row0[w] + nrows[w]) of
+// one block (at most kWindowB); a warp sorts them by descending length,
+// stably (lengths of kLenCapB - 1 and more share the last bucket: the order
+// only decides the padding), into perm[out0[w] ...].
+constexpr int kLenCapB = 1024;
+__global__ void __launch_bounds__(32) k_b_window_perm(const int64_t* __restrict__ row0,
+                                                      const int32_t* __restrict__ nrows,
+                                                      const int64_t* __restrict__ out0,
+                                                      const int32_t* __restrict__ rp, int32_t* __restrict__ perm) {
+  __shared__ int32_t cur[kLenCapB];  // bucket 0 = longest rows
+  const int lane = threadIdx.x;
+  const int64_t w0 = row0[blockIdx.x], w1 = w0 + nrows[blockIdx.x], o0 = out0[blockIdx.x];
+  for (int b = lane; b < kLenCapB; b += 32) cur[b] = 0;
+  __syncwarp();
+  for (int64_t i = w0 + lane; i < w1; i += 32) {
+    const int len = rp[i + 1] - rp[i];
+    atomicAdd(&cur[kLenCapB - 1 - (len < kLenCapB - 1 ? len : kLenCapB - 1)], 1);
+  }
+  __syncwarp();
+  constexpr int kPer = kLenCapB / 32;  // lane l owns buckets [l kPer, (l + 1) kPer)
+  int local = 0;
+  for (int k = 0; k < kPer; ++k) local += cur[lane * kPer + k];
+  int incl = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  int run = incl - local;
+  for (int k = 0; k < kPer; ++k) {
+    const int c = cur[lane * kPer + k];
+    cur[lane * kPer + k] = run;
+    run += c;
+  }
+  __syncwarp();
+  for (int64_t base = w0; base < w1; base += 32) {  // 32 rows a round, ties ranked by lane
+    const int64_t i = base + lane;
+    const bool valid = i < w1;
+    int b = -1 - lane;
+    if (valid) {
+      const int len = rp[i + 1] - rp[i];
+      b = kLenCapB - 1 - (len < kLenCapB - 1 ? len : kLenCapB - 1);
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, b);
+    const int rank = __popc(grp & ((1u << lane) - 1u));
+    const int pos = valid ? cur[b] + rank : 0;
+    __syncwarp();
+    if (valid && rank == 0) cur[b] += __popc(grp);
+    __syncwarp();
+    if (valid) perm[o0 + pos] = static_cast<int32_t>(i);
+  }
+}
+
+// Warp per slice: slots = 32 x the longest row of the slice (padding rows,
+// perm -1, count 0).
+__global__ void k_b_slice_slots(int64_t ns, const int32_t* __restrict__ perm, const int32_t* __restrict__ rp,
+                                int32_t* __restrict__ slots) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; s < ns; s += nw) {
+    const int32_t o = perm[s * 32 + lane];
+    const int len = o >= 0 ? rp[o + 1] - rp[o] : 0;
+    const int mx = __reduce_max_sync(0xffffffffu, len);
+    if (lane == 0) slots[s] = 32 * mx;
+  }
+}
+
+__global__ void k_b_widen_iperm(int64_t ns, const int32_t* __restrict__ off, int64_t* __restrict__ sp,
+                                int64_t N, const int32_t* __restrict__ perm, int32_t* __restrict__ iperm) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  for (int64_t i = t0; i <= ns; i += stride) sp[i] = off[i];
+  for (int64_t i = t0; i < N; i += stride)
+    if (perm[i] >= 0) iperm[perm[i]] = static_cast<int32_t>(i);
 }
 
 int launch_grid(int64_t work) {
@@ -422,54 +510,80 @@ int dalloc(T** p, int64_t count, cudaStream_t st) {
 int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, BatchPlan& P) {
   const int64_t n = A.n;
   const int32_t nb = static_cast<int32_t>(blocks.size()) - 1;
-  std::vector<int32_t> rp(n + 1);
-  EMG_CK(cudaMemcpyAsync(rp.data(), A.row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
-  EMG_CK(cudaStreamSynchronize(st));
-  auto len = [&](int64_t o) { return rp[o + 1] - rp[o]; };
-  int32_t maxlen = 0;
-  for (int64_t i = 0; i < n; ++i) maxlen = std::max(maxlen, len(i));
-  // new numbering
+  // new numbering: every block padded to a multiple of 32 rows
   std::vector<int64_t> nstart(nb + 1, 0);
   for (int32_t k = 0; k < nb; ++k) nstart[k + 1] = nstart[k] + ((blocks[k + 1] - blocks[k] + 31) / 32) * 32;
   const int64_t N = nstart[nb];
-  std::vector<int32_t> perm(N, -1), iperm(n, 0);
-  std::vector<int64_t> cnt(static_cast<size_t>(maxlen) + 2);
-  for (int32_t k = 0; k < nb; ++k) {
-    int64_t out = nstart[k];
-    for (int64_t w0 = blocks[k]; w0 < blocks[k + 1]; w0 += kWindowB) {
-      const int64_t w1 = std::min<int64_t>(blocks[k + 1], w0 + kWindowB);
-      std::fill(cnt.begin(), cnt.end(), 0);
-      for (int64_t i = w0; i < w1; ++i) cnt[maxlen - len(i) + 1]++;
-      for (size_t b = 1; b < cnt.size(); ++b) cnt[b] += cnt[b - 1];
-      for (int64_t i = w0; i < w1; ++i) perm[out + cnt[maxlen - len(i)]++] = static_cast<int32_t>(i);
-      out += w1 - w0;
-    }
-  }
-  for (int64_t i = 0; i < N; ++i)
-    if (perm[i] >= 0) iperm[perm[i]] = static_cast<int32_t>(i);
   const int64_t ns = N / 32;
+  if (N >= (int64_t(1) << 31)) {
+    set_error("batch too large for the solver format");
+    return EMG_INVALID_INPUT;
+  }
+  // length-sort windows inside the blocks
+  std::vector<int64_t> wrow, wout;
+  std::vector<int32_t> wlen;
+  for (int32_t k = 0; k < nb; ++k)
+    for (int64_t w0 = blocks[k]; w0 < blocks[k + 1]; w0 += kWindowB) {
+      wrow.push_back(w0);
+      wlen.push_back(static_cast<int32_t>(std::min<int64_t>(blocks[k + 1] - w0, kWindowB)));
+      wout.push_back(nstart[k] + (w0 - blocks[k]));
+    }
+  const int64_t nwin = static_cast<int64_t>(wrow.size());
+  int32_t *d_iperm = nullptr, *d_slots = nullptr, *d_off = nullptr, *d_wlen = nullptr;
+  int64_t *d_wrow = nullptr, *d_wout = nullptr;
+  int rc = dalloc(&P.perm, N, st);
+  if (!rc) rc = dalloc(&d_iperm, n, st);
+  if (!rc) rc = dalloc(&P.slice_ptr, ns + 1, st);
+  if (!rc) rc = dalloc(&d_slots, ns, st);
+  if (!rc) rc = dalloc(&d_off, ns + 1, st);
+  if (!rc) rc = dalloc(&d_wrow, nwin, st);
+  if (!rc) rc = dalloc(&d_wout, nwin, st);
+  if (!rc) rc = dalloc(&d_wlen, nwin, st);
+  if (rc) return rc;
+  EMG_CK(cudaMemsetAsync(P.perm, 0xff, sizeof(int32_t) * std::max<int64_t>(N, 1), st));
+  if (nwin > 0) {
+    EMG_CK(cudaMemcpyAsync(d_wrow, wrow.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st));
+    EMG_CK(cudaMemcpyAsync(d_wout, wout.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st));
+    EMG_CK(cudaMemcpyAsync(d_wlen, wlen.data(), sizeof(int32_t) * nwin, cudaMemcpyHostToDevice, st));
+    k_b_window_perm<<<static_cast<unsigned>(nwin), 32, 0, st>>>(d_wrow, d_wlen, d_wout, A.row_ptr, P.perm);
+  }
+  if (ns > 0) k_b_slice_slots<<<launch_grid(ns * 32), 256, 0, st>>>(ns, P.perm, A.row_ptr, d_slots);
+  EMG_CK(cudaGetLastError());
+  int64_t total = 0;
+  rc = scan_counts(d_slots, d_off, ns, &total, st);
+  if (!rc && total >= (int64_t(1) << 31)) {
+    set_error("batch too large for the solver format");
+    rc = EMG_INVALID_INPUT;
+  }
+  if (!rc) {
+    k_b_widen_iperm<<<launch_grid(N), 256, 0, st>>>(ns, d_off, P.slice_ptr, N, P.perm, d_iperm);
+    if (cudaGetLastError() != cudaSuccess) { set_error("batch plan launch failed"); rc = EMG_ERR_CUDA; }
+  }
   std::vector<int64_t> sp(ns + 1, 0);
+  if (!rc && cudaMemcpyAsync(sp.data(), P.slice_ptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, st) !=
+                 cudaSuccess) {
+    set_error("batch plan copy failed");
+    rc = EMG_ERR_CUDA;
+  }
+  for (void* p : {static_cast<void*>(d_slots), static_cast<void*>(d_off), static_cast<void*>(d_wrow),
+                  static_cast<void*>(d_wout), static_cast<void*>(d_wlen)})
+    cudaFreeAsync(p, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) { set_error("batch plan failed"); rc = EMG_ERR_CUDA; }
+  if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
   std::vector<int32_t> sinst(ns);
   {
     int32_t k = 0;
-    for (int64_t s = 0; s < ns; ++s) {
-      while (s * 32 >= nstart[k + 1]) ++k;
-      sinst[s] = k;
-      int32_t l = 0;
-      for (int64_t r = s * 32; r < s * 32 + 32; ++r)
-        if (perm[r] >= 0) l = std::max(l, len(perm[r]));
-      sp[s + 1] = sp[s] + 32 * static_cast<int64_t>(l);
+    for (int64_t s2 = 0; s2 < ns; ++s2) {
+      while (s2 * 32 >= nstart[k + 1]) ++k;
+      sinst[s2] = k;
     }
-  }
-  if (sp[ns] >= (int64_t(1) << 31) || ns >= (int64_t(1) << 31)) {
-    set_error("batch too large for the solver format");
-    return EMG_INVALID_INPUT;
   }
   // CTA ranges: contiguous slices, ~equal slots, at most kMaxLocal blocks each
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t target = std::max<int64_t>(1, (sp[ns] + 4 * sms - 1) / (4 * sms));
+  const int64_t parts = static_cast<int64_t>(EMG_BATCH_CTAS_PER_SM) * sms;
+  const int64_t target = std::max<int64_t>(1, (sp[ns] + parts - 1) / parts);
   std::vector<int32_t> cs{0}, cseg;
   std::vector<int32_t> iseg_cnt(nb, 0);
   {
@@ -495,11 +609,6 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
   // a block without rows has no segments; its sums are 0 and it finishes at once
   P.n = n; P.N = N; P.nslices = ns; P.slots = sp[ns]; P.nb = nb; P.nctas = nctas; P.nsegs = nsegs;
   P.blocks = blocks;
-  int rc = EMG_SUCCESS;
-  int32_t* d_iperm = nullptr;
-  if (!rc) rc = dalloc(&P.perm, N, st);
-  if (!rc) rc = dalloc(&d_iperm, n, st);
-  if (!rc) rc = dalloc(&P.slice_ptr, ns + 1, st);
   if (!rc) rc = dalloc(&P.slice_inst, ns, st);
   if (!rc) rc = dalloc(&P.cta_slice, nctas + 1, st);
   if (!rc) rc = dalloc(&P.cta_seg, nctas, st);
@@ -516,10 +625,7 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
     if (!rc) rc = dalloc(v, nb, st);
   if (!rc) rc = dalloc(&P.ctl, 8, st);
   if (!rc) rc = dalloc(&P.tol, 1, st);
-  if (rc) return rc;
-  EMG_CK(cudaMemcpyAsync(P.perm, perm.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemcpyAsync(d_iperm, iperm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemcpyAsync(P.slice_ptr, sp.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, st));
+  if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
   if (ns > 0) EMG_CK(cudaMemcpyAsync(P.slice_inst, sinst.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
   EMG_CK(cudaMemcpyAsync(P.cta_slice, cs.data(), sizeof(int32_t) * (nctas + 1), cudaMemcpyHostToDevice, st));
   if (nctas > 0) EMG_CK(cudaMemcpyAsync(P.cta_seg, cseg.data(), sizeof(int32_t) * nctas, cudaMemcpyHostToDevice, st));
@@ -606,27 +712,23 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
     if (blocks[k + 1] < blocks[k]) { set_error("batch solve: block partition not monotone"); return EMG_INVALID_INPUT; }
   cudaStream_t st = user;
   if (!A.batch || A.batch->blocks != blocks) {
+    TraceScope trace_setup("batch.setup");
     // block-diagonal check on the device
-    std::vector<int32_t> rb(A.n);
-    for (int32_t k = 0; k < nb; ++k)
-      for (int64_t i = blocks[k]; i < blocks[k + 1]; ++i) rb[i] = k;
-    int32_t *d_rb = nullptr, *d_bad = nullptr;
+    int32_t* d_bad = nullptr;
     int64_t* d_blocks = nullptr;
-    EMG_CK(cudaMallocAsync(&d_rb, sizeof(int32_t) * std::max<int64_t>(A.n, 1), st));
     EMG_CK(cudaMallocAsync(&d_blocks, sizeof(int64_t) * (nb + 1), st));
     EMG_CK(cudaMallocAsync(&d_bad, sizeof(int32_t), st));
-    EMG_CK(cudaMemcpyAsync(d_rb, rb.data(), sizeof(int32_t) * A.n, cudaMemcpyHostToDevice, st));
     EMG_CK(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, st));
     EMG_CK(cudaMemsetAsync(d_bad, 0, sizeof(int32_t), st));
-    k_b_check<<<launch_grid(A.n), 256, 0, st>>>(A.n, A.row_ptr, A.col, d_rb, d_blocks, d_bad);
+    k_b_check<<<launch_grid(A.n), 256, 0, st>>>(A.n, A.row_ptr, A.col, nb, d_blocks, d_bad);
     int32_t bad = 0;
     EMG_CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     EMG_CK(cudaStreamSynchronize(st));
-    for (void* p : {static_cast<void*>(d_rb), static_cast<void*>(d_blocks), static_cast<void*>(d_bad)})
-      EMG_CK(cudaFreeAsync(p, st));
+    for (void* p : {static_cast<void*>(d_blocks), static_cast<void*>(d_bad)}) EMG_CK(cudaFreeAsync(p, st));
     if (bad) { set_error("batch solve: the matrix couples different blocks"); return EMG_INVALID_INPUT; }
     free_batch(A.batch);
     A.batch = new BatchPlan();
+    TraceScope trace_plan("batch.plan");
     int rc = build_plan(A, blocks, st, *A.batch);
     if (rc) { free_batch(A.batch); A.batch = nullptr; return rc; }
   }
@@ -637,6 +739,7 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
     P.version = A.version;
   }
   if (!P.loop) {
+    TraceScope trace_capture("batch.capture");
     int rc = capture_batch_loop(P);
     if (rc) return rc;
   }
