@@ -10,11 +10,13 @@
 // Layout: SELL-32 per block.  Rows of each block are sorted by length inside
 // windows of 4096 rows that never cross a block boundary, and each block is
 // padded to a multiple of 32 rows, so every 32-row slice belongs to exactly
-// one block.  A CTA owns a contiguous range of slices (balanced by stored
-// slots, at most kMaxLocal blocks per CTA); per-block dot products are summed
-// per CTA in a fixed order, written as one partial per (CTA, block) segment,
-// and the last CTA to finish (atomic ticket) sums each block's segments in
-// order -- deterministic results for a fixed partition.
+// one block.  The blocks still iterating are listed once per loop body (a
+// block that finishes inside a body is skipped until the next list); the
+// slices of the listed blocks are split into equal contiguous shares, one
+// per warp of a one-wave grid, so the remaining work always spreads over the
+// whole GPU.  Every slice writes its own dot-product partials; a warp per
+// block then adds them in slice order -- results do not depend on the grid
+// or on which blocks are still iterating.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,44 +34,36 @@ namespace emg {
 
 namespace {
 
-constexpr int kBThreads = 512;
-constexpr int kBWarps = kBThreads / 32;
-constexpr int kMaxLocal = 64;   // blocks touched by one CTA
+constexpr int kBT = 256;        // threads of the slice kernels
 constexpr int kWindowB = 4096;  // length-sort window (inside a block)
 constexpr int kBodyB = 4;       // iterations per while-loop body
-// CTAs per SM the slices are split into (each CTA ~ the same number of
-// slots).  A CTA whose blocks have all converged returns at once, so more,
-// smaller CTAs let the block scheduler spread the blocks still iterating
-// over the whole GPU.
-#ifndef EMG_BATCH_CTAS_PER_SM
-#define EMG_BATCH_CTAS_PER_SM 4
-#endif
 
 }  // namespace
 
 struct BatchPlan {
   int64_t n = 0, N = 0, nslices = 0, slots = 0;
-  int32_t nb = 0, nctas = 0, nsegs = 0;
-  std::vector<int64_t> blocks;   // host copy of the block row partition
+  int32_t nb = 0;
+  int grid_spmv = 0, grid_vec = 0;  // one-wave grids of the slice kernels
+  std::vector<int64_t> blocks;      // host copy of the block row partition
   uint64_t version = ~uint64_t(0);
   // device arrays
   int32_t* perm = nullptr;        // new row -> old row, -1 = padding (N)
   int64_t* slice_ptr = nullptr;   // nslices + 1
-  int32_t* slice_inst = nullptr;  // block of every slice
-  int32_t* cta_slice = nullptr;   // nctas + 1 slice ranges
-  int32_t* cta_seg = nullptr;     // first segment id of every CTA
-  int32_t* inst_seg = nullptr;    // nb + 1 segment ranges per block
+  int32_t* inst_slice = nullptr;  // nb + 1: slices of block k are [inst_slice[k], inst_slice[k + 1])
+  int32_t* act_inst = nullptr;    // nb: blocks still iterating, ascending
+  int32_t* act_start = nullptr;   // nb + 1: their first slice in the active-slice numbering
   int32_t* col = nullptr;
   int32_t* src = nullptr;
   double* val = nullptr;
   // workspace
   double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
-  double* partial = nullptr;      // 2 * nsegs
+  double* partial = nullptr;      // 2 * nslices: per-slice sums
   // per-block state (structure of arrays)
   double *bnorm = nullptr, *rz = nullptr, *alpha = nullptr, *beta = nullptr, *res = nullptr,
          *prev = nullptr;
   int32_t *iter = nullptr, *status = nullptr, *done = nullptr;
-  int32_t* ctl = nullptr;         // [0] ticket, [1] active, [2] loops, [3] loop limit, [4] max_iter
+  // [1] active blocks, [2] loops, [3] loop limit, [4] max_iter, [5] listed blocks, [6] listed slices
+  int32_t* ctl = nullptr;
   double* tol = nullptr;          // [0]
   cudaStream_t cap = nullptr;
   cudaGraphExec_t loop = nullptr;
@@ -83,10 +77,9 @@ struct View {
   int32_t nb;
   const int32_t* perm;
   const int64_t* slice_ptr;
-  const int32_t* slice_inst;
-  const int32_t* cta_slice;
-  const int32_t* cta_seg;
-  const int32_t* inst_seg;
+  const int32_t* inst_slice;
+  int32_t* act_inst;
+  int32_t* act_start;
   const int32_t* col;
   const double* val;
   double *x, *r, *z, *p, *q, *dinv, *partial;
@@ -97,72 +90,81 @@ struct View {
 
 View view_of(const BatchPlan& P) {
   View v;
-  v.N = P.N; v.nb = P.nb; v.perm = P.perm; v.slice_ptr = P.slice_ptr; v.slice_inst = P.slice_inst;
-  v.cta_slice = P.cta_slice; v.cta_seg = P.cta_seg; v.inst_seg = P.inst_seg; v.col = P.col; v.val = P.val;
+  v.N = P.N; v.nb = P.nb; v.perm = P.perm; v.slice_ptr = P.slice_ptr; v.inst_slice = P.inst_slice;
+  v.act_inst = P.act_inst; v.act_start = P.act_start; v.col = P.col; v.val = P.val;
   v.x = P.x; v.r = P.r; v.z = P.z; v.p = P.p; v.q = P.q; v.dinv = P.dinv; v.partial = P.partial;
   v.bnorm = P.bnorm; v.rz = P.rz; v.alpha = P.alpha; v.beta = P.beta; v.res = P.res; v.prev = P.prev;
   v.iter = P.iter; v.status = P.status; v.done = P.done; v.ctl = P.ctl; v.tol = P.tol;
   return v;
 }
 
-// Per-CTA accumulation of per-block sums: acc[warp][local][k] in shared memory.
-template <int K>
-struct Acc {
-  double (*a)[kMaxLocal][K];
-  int first;  // first block of this CTA
-};
+// The slices of the listed blocks (ctl[6] of them, numbered block after
+// block) are split into equal contiguous shares, one per warp of the grid,
+// so the work of the blocks still iterating spreads over the whole GPU
+// however few they are.  body(slice, block, lane) runs for every slice of a
+// block that is not done (blocks finish only between launches).
+template <class Body>
+__device__ __forceinline__ void active_slices(const View& B, Body body) {
+  const int64_t total = B.ctl[6];
+  const int nact = B.ctl[5];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const int64_t gw = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t a = total * gw / nw, b = total * (gw + 1) / nw;
+  if (a >= b) return;
+  int lo = 0, hi = nact;  // act_start[lo] <= a < act_start[hi]
+  while (hi - lo > 1) {
+    const int m = (lo + hi) >> 1;
+    if (B.act_start[m] <= a) lo = m; else hi = m;
+  }
+  int j = lo;
+  int inst = B.act_inst[j];
+  int64_t next = B.act_start[j + 1];
+  int64_t s = B.inst_slice[inst] + (a - B.act_start[j]);
+  bool live = !B.done[inst];
+  for (int64_t t = a; t < b; ++t, ++s) {
+    if (t == next) {
+      ++j;
+      inst = B.act_inst[j];
+      next = B.act_start[j + 1];
+      s = B.inst_slice[inst];
+      live = !B.done[inst];
+    }
+    if (live) body(s, inst, lane);
+  }
+}
 
-// Runs body(slice, block, local, lane) -> contributions[K] for every slice of
-// this CTA whose block is still active (or every slice when all_blocks), adds
-// the warp-reduced contributions per block, and on the last CTA calls
-// fin(block, totals) for every block.  Returns after fin has run.
-template <int K, bool kAll, class Body, class Fin>
-__device__ __forceinline__ void sweep(const View& B, Body body, Fin fin) {
-  __shared__ double acc[kBWarps][kMaxLocal][K];
-  __shared__ bool last;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x;
-  const int s0 = B.cta_slice[c], s1 = B.cta_slice[c + 1];
-  const int first = s0 < s1 ? B.slice_inst[s0] : 0;
-  const int nlocal = s0 < s1 ? B.slice_inst[s1 - 1] - first + 1 : 0;
-  for (int i = threadIdx.x; i < kBWarps * kMaxLocal * K; i += blockDim.x) (&acc[0][0][0])[i] = 0.0;
-  __syncthreads();
-  for (int s = s0 + w; s < s1; s += kBWarps) {
-    const int inst = B.slice_inst[s];
+// Warp per listed block that is not done: the block's per-slice sums added
+// in slice order (lane-strided, then a fixed butterfly), then fin(block, tot).
+template <int K, bool kAll, class Fin>
+__device__ __forceinline__ void finish_blocks(const View& B, Fin fin) {
+  const int lane = threadIdx.x & 31;
+  const int nact = B.ctl[5];
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; j < nact; j += nw) {
+    const int inst = B.act_inst[j];
     if (!kAll && B.done[inst]) continue;
-    double v[K];
-    body(s, inst, lane, v);
+    double t[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
-    if (lane == 0)
+    for (int k = 0; k < K; ++k) t[k] = 0.0;
+    // 8 slices a lane in flight, added in slice order
+    constexpr int kU = 8;
+    const int64_t s1 = B.inst_slice[inst + 1];
+    for (int64_t s0 = B.inst_slice[inst] + lane; s0 < s1; s0 += 32 * kU) {
+      double v[kU][K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) acc[w][inst - first][k] += v[k];
+      for (int u = 0; u < kU; ++u)
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[u][k] = s0 + 32 * u < s1 ? B.partial[(s0 + 32 * u) * K + k] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+#pragma unroll
+        for (int k = 0; k < K; ++k) t[k] += v[u][k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) t[k] = warp_sum(t[k]);
+    if (lane == 0) fin(inst, t);
   }
-  __syncthreads();
-  for (int t = threadIdx.x; t < nlocal * K; t += blockDim.x) {
-    const int l = t / K, k = t % K;
-    double s = 0.0;
-    for (int ww = 0; ww < kBWarps; ++ww) s += acc[ww][l][k];
-    B.partial[(B.cta_seg[c] + l) * K + k] = s;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(reinterpret_cast<unsigned*>(&B.ctl[0]), 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int i = threadIdx.x; i < B.nb; i += blockDim.x) {
-    if (!kAll && B.done[i]) continue;
-    double tot[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) tot[k] = 0.0;
-    for (int sg = B.inst_seg[i]; sg < B.inst_seg[i + 1]; ++sg)
-#pragma unroll
-      for (int k = 0; k < K; ++k) tot[k] += ld_l2(B.partial + sg * K + k);
-    fin(i, tot);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) B.ctl[0] = 0;
 }
 
 __global__ void k_b_jacobi(View B, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
@@ -184,185 +186,262 @@ __global__ void k_b_jacobi(View B, const int32_t* __restrict__ rp, const int32_t
   }
 }
 
-__global__ void __launch_bounds__(kBThreads) k_b_init(View B, const double* __restrict__ b) {
-  sweep<2, true>(
-      B,
-      [&](int s, int, int lane, double* v) {
-        const int64_t row = static_cast<int64_t>(s) * 32 + lane;
-        const int32_t o = B.perm[row];
-        const double bi = o >= 0 ? b[o] : 0.0, zi = B.dinv[row] * bi;
-        B.x[row] = 0.0; B.r[row] = bi; B.z[row] = zi; B.p[row] = zi; B.q[row] = 0.0;
-        v[0] = bi * bi;
-        v[1] = bi * zi;
-      },
-      [&](int i, const double* tot) {
-        const double bn = sqrt(tot[0]);
-        const int32_t max_iter = B.ctl[4];
-        B.bnorm[i] = bn;
-        B.rz[i] = tot[1];
-        B.iter[i] = 1;
-        B.status[i] = EMG_MAX_ITER_REACHED;
-        B.done[i] = 0;
-        if (bn < 1e-15) {  // iterative_solvers.cpp:440-446
-          B.status[i] = EMG_SUCCESS; B.iter[i] = 0; B.res[i] = 0.0; B.done[i] = 1;
-        } else {
-          B.res[i] = sqrt(tot[0]) / bn;
-          B.prev[i] = B.res[i];
-          if (max_iter < 1) { B.iter[i] = max_iter; B.done[i] = 1; }
-        }
-      });
-}
-
-// q = A p and p.q per block -> alpha (or breakdown)
-// 1: the batched SpMV keeps the next batch of loads in flight (as the
-// single-system SELL kernel does); 0: one batch at a time.
-#ifndef EMG_BATCH_PIPE
-#define EMG_BATCH_PIPE 1
-#endif
-
-__global__ void __launch_bounds__(kBThreads) k_b_spmv_dot(View B) {
-  if (B.ctl[1] == 0) return;
-  const uint64_t pol = evict_first_policy();
-  sweep<1, false>(
-      B,
-      [&](int s, int, int lane, double* v) {
-        const int64_t b0 = B.slice_ptr[s];
-        const int len = static_cast<int>((B.slice_ptr[s + 1] - b0) >> 5);
-        const int64_t base = b0 + lane;
-        double sum = 0.0;
-#if !EMG_BATCH_PIPE
-        int j = 0;
-        for (; j + 4 <= len; j += 4) {
-          const int64_t k = base + 32 * j;
-          int cc[4];
-          double vv[4], xx[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            cc[u] = ld_stream(B.col + k + 32 * u, pol);
-            vv[u] = ld_stream(B.val + k + 32 * u, pol);
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) xx[u] = B.p[cc[u]];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) sum += vv[u] * xx[u];
-        }
-        for (; j < len; ++j) {
-          const int64_t k = base + 32 * j;
-          sum += ld_stream(B.val + k, pol) * B.p[ld_stream(B.col + k, pol)];
-        }
-#else
-        // the next batch of 4 columns / values is in flight while this batch
-        // gathers p; entries past the row length are masked and add +0 last
-        const int nbt = (len + 3) >> 2;
-        int cn[4];
-        double vn[4];
-        auto fetch = [&](int jb) {
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const bool in = jb + u < len;
-            const int64_t k = base + 32 * static_cast<int64_t>(jb + u);
-            cn[u] = in ? ld_stream(B.col + k, pol) : 0;
-            vn[u] = in ? ld_stream(B.val + k, pol) : 0.0;
-          }
-        };
-        if (nbt > 0) fetch(0);
-        for (int bt = 0; bt < nbt; ++bt) {
-          int cc[4];
-          double vv[4], xx[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) { cc[u] = cn[u]; vv[u] = vn[u]; }
-          if (bt + 1 < nbt) fetch(4 * (bt + 1));
-#pragma unroll
-          for (int u = 0; u < 4; ++u) xx[u] = B.p[cc[u]];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) sum += vv[u] * xx[u];
-        }
-#endif
-        const int64_t row = static_cast<int64_t>(s) * 32 + lane;
-        B.q[row] = sum;
-        v[0] = B.p[row] * sum;
-      },
-      [&](int i, const double* tot) {
-        if (fabs(tot[0]) < 1e-30) {  // :453-457
-          B.status[i] = EMG_NUMERICAL_ERROR;
-          B.done[i] = 1;
-        } else {
-          B.alpha[i] = B.rz[i] / tot[0];
-        }
-      });
-}
-
-__global__ void __launch_bounds__(kBThreads) k_b_update(View B) {
-  if (B.ctl[1] == 0) return;
-  sweep<2, false>(
-      B,
-      [&](int s, int inst, int lane, double* v) {
-        const int64_t row = static_cast<int64_t>(s) * 32 + lane;
-        const double a = B.alpha[inst];
-        B.x[row] += a * B.p[row];
-        const double ri = B.r[row] - a * B.q[row];
-        const double zi = B.dinv[row] * ri;
-        B.r[row] = ri;
-        B.z[row] = zi;
-        v[0] = ri * zi;
-        v[1] = ri * ri;
-      },
-      [&](int i, const double* tot) {
-        const int it = B.iter[i];
-        const double res = sqrt(tot[1]) / B.bnorm[i];
-        B.res[i] = res;
-        if (res < B.tol[0]) {
-          B.status[i] = EMG_SUCCESS; B.done[i] = 1;
-        } else if (it > 10 && res > B.prev[i] * 1000.0) {  // :477-483
-          B.status[i] = EMG_DIVERGED; B.done[i] = 1;
-        } else {
-          B.beta[i] = tot[0] / B.rz[i];
-          B.rz[i] = tot[0];
-          B.prev[i] = res;
-          if (it >= B.ctl[4]) { B.status[i] = EMG_MAX_ITER_REACHED; B.done[i] = 1; }
-          else B.iter[i] = it + 1;
-        }
-      });
-}
-
-__global__ void __launch_bounds__(kBThreads) k_b_direction(View B) {
-  if (B.ctl[1] == 0) return;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x;
-  for (int s = B.cta_slice[c] + w; s < B.cta_slice[c + 1]; s += kBWarps) {
-    const int inst = B.slice_inst[s];
-    if (B.done[inst]) continue;
-    const int64_t row = static_cast<int64_t>(s) * 32 + lane;
-    B.p[row] = B.z[row] + B.beta[inst] * B.p[row];
+// Lists the blocks that are not done (act_inst, act_start, ctl[5], ctl[6]),
+// sets ctl[1] = their count and, with kSteer, counts a loop body and steers
+// the device while-loop.  One CTA of 1024 threads, blocks in chunks of 1024.
+template <bool kSteer>
+__global__ void __launch_bounds__(1024) k_b_list(View B, cudaGraphConditionalHandle handle) {
+  __shared__ int32_t wc[32], ws[32];
+  __shared__ int32_t carry_c, carry_s;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) { carry_c = 0; carry_s = 0; }
+  __syncthreads();
+  for (int base = 0; base < B.nb; base += 1024) {
+    const int i = base + static_cast<int>(threadIdx.x);
+    const int f = (i < B.nb && !B.done[i]) ? 1 : 0;
+    const int sl = f ? B.inst_slice[i + 1] - B.inst_slice[i] : 0;
+    int ic = f, is = sl;  // warp inclusive scans
+    for (int o = 1; o < 32; o <<= 1) {
+      const int vc = __shfl_up_sync(0xffffffffu, ic, o), vs = __shfl_up_sync(0xffffffffu, is, o);
+      if (lane >= o) { ic += vc; is += vs; }
+    }
+    if (lane == 31) { wc[w] = ic; ws[w] = is; }
+    __syncthreads();
+    if (w == 0) {
+      int c = wc[lane], t = ws[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int vc = __shfl_up_sync(0xffffffffu, c, o), vs = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) { c += vc; t += vs; }
+      }
+      wc[lane] = c - wc[lane];  // exclusive warp offsets
+      ws[lane] = t - ws[lane];
+    }
+    __syncthreads();
+    if (f) {
+      const int pc = carry_c + wc[w] + ic - f;
+      B.act_inst[pc] = i;
+      B.act_start[pc] = carry_s + ws[w] + is - sl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 1023) { carry_c += wc[w] + ic; carry_s += ws[w] + is; }
+    __syncthreads();
   }
-}
-
-// Counts active blocks and steers the device while-loop.
-__global__ void k_b_control(View B, cudaGraphConditionalHandle handle) {
-  __shared__ int cnt;
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  int mine = 0;
-  for (int i = threadIdx.x; i < B.nb; i += blockDim.x) mine += B.done[i] ? 0 : 1;
-  atomicAdd(&cnt, mine);
-  __syncthreads();
   if (threadIdx.x == 0) {
-    B.ctl[1] = cnt;
-    const int loops = B.ctl[2] + 1;
-    B.ctl[2] = loops;
-    cudaGraphSetConditional(handle, (cnt > 0 && loops < B.ctl[3]) ? 1u : 0u);
+    B.act_start[carry_c] = carry_s;
+    B.ctl[5] = carry_c;
+    B.ctl[6] = carry_s;
+    B.ctl[1] = carry_c;
+    if constexpr (kSteer) {
+      const int loops = B.ctl[2] + 1;
+      B.ctl[2] = loops;
+      cudaGraphSetConditional(handle, (carry_c > 0 && loops < B.ctl[3]) ? 1u : 0u);
+    }
   }
 }
 
-__global__ void k_b_active(View B) {
-  __shared__ int cnt;
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  int mine = 0;
-  for (int i = threadIdx.x; i < B.nb; i += blockDim.x) mine += B.done[i] ? 0 : 1;
-  atomicAdd(&cnt, mine);
-  __syncthreads();
-  if (threadIdx.x == 0) B.ctl[1] = cnt;
+// x = 0, r = b, z = p = D^-1 b; per-slice b.b and b.z
+__global__ void __launch_bounds__(kBT) k_b_init(View B, const double* __restrict__ b) {
+  active_slices(B, [&](int64_t s, int, int lane) {
+    const int64_t row = s * 32 + lane;
+    const int32_t o = B.perm[row];
+    const double bi = o >= 0 ? b[o] : 0.0, zi = B.dinv[row] * bi;
+    B.x[row] = 0.0; B.r[row] = bi; B.z[row] = zi; B.p[row] = zi; B.q[row] = 0.0;
+    const double bb = warp_sum(bi * bi), bz = warp_sum(bi * zi);
+    if (lane == 0) { B.partial[2 * s] = bb; B.partial[2 * s + 1] = bz; }
+  });
+}
+
+__global__ void __launch_bounds__(kBT) k_b_fin_init(View B) {
+  finish_blocks<2, true>(B, [&](int i, const double* tot) {
+    const double bn = sqrt(tot[0]);
+    const int32_t max_iter = B.ctl[4];
+    B.bnorm[i] = bn;
+    B.rz[i] = tot[1];
+    B.iter[i] = 1;
+    B.status[i] = EMG_MAX_ITER_REACHED;
+    B.done[i] = 0;
+    if (bn < 1e-15) {  // iterative_solvers.cpp:440-446
+      B.status[i] = EMG_SUCCESS; B.iter[i] = 0; B.res[i] = 0.0; B.done[i] = 1;
+    } else {
+      B.res[i] = sqrt(tot[0]) / bn;
+      B.prev[i] = B.res[i];
+      if (max_iter < 1) { B.iter[i] = max_iter; B.done[i] = 1; }
+    }
+  });
+}
+
+// Walks the warp's share of the listed slices (as active_slices), stopping
+// only at slices of blocks that are not done.
+struct SliceCursor {
+  int64_t t, end, next, s;
+  int j, inst;
+  __device__ __forceinline__ bool init(const View& B) {
+    const int64_t total = B.ctl[6];
+    const int nact = B.ctl[5];
+    const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int64_t gw = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    t = total * gw / nw;
+    end = total * (gw + 1) / nw;
+    if (t >= end) return false;
+    int lo = 0, hi = nact;
+    while (hi - lo > 1) {
+      const int m = (lo + hi) >> 1;
+      if (B.act_start[m] <= t) lo = m; else hi = m;
+    }
+    j = lo;
+    inst = B.act_inst[j];
+    next = B.act_start[j + 1];
+    s = B.inst_slice[inst] + (t - B.act_start[j]);
+    return live(B);
+  }
+  // moves to the next slice of a live block; false past the end
+  __device__ __forceinline__ bool live(const View& B) {
+    while (t < end) {
+      if (!B.done[inst]) return true;
+      t = next;  // skip the rest of this block
+      if (t >= end) break;
+      ++j;
+      inst = B.act_inst[j];
+      next = B.act_start[j + 1];
+      s = B.inst_slice[inst];
+    }
+    return false;
+  }
+  __device__ __forceinline__ bool step(const View& B) {
+    ++t;
+    ++s;
+    if (t < end && t == next) {
+      ++j;
+      inst = B.act_inst[j];
+      next = B.act_start[j + 1];
+      s = B.inst_slice[inst];
+    }
+    return live(B);
+  }
+};
+
+// q = A p and the slice's p.q for every live slice of the warp's share: one
+// software pipeline over the share -- the next batch of kBatchB columns /
+// values, possibly of the next slice, is in flight while the current batch
+// gathers p (entries of a row summed in CSR order; masked entries add +0
+// after the real ones).
+#ifndef EMG_BATCH_ENTRIES
+#define EMG_BATCH_ENTRIES 4
+#endif
+constexpr int kBatchB = EMG_BATCH_ENTRIES;
+__global__ void __launch_bounds__(kBT) k_b_spmv_dot(View B) {
+  const uint64_t pol = evict_first_policy();
+  const int lane = threadIdx.x & 31;
+  SliceCursor F;  // fetch cursor
+  bool more = F.init(B);
+  if (!more) return;
+  int64_t fbase = B.slice_ptr[F.s];
+  int flen = static_cast<int>((B.slice_ptr[F.s + 1] - fbase) >> 5);
+  fbase += lane;
+  int fj = 0;
+  auto fetch = [&](int (&c)[kBatchB], double (&v)[kBatchB], bool& last, int64_t& sl) {
+#pragma unroll
+    for (int u = 0; u < kBatchB; ++u) {
+      const bool in = fj + u < flen;
+      const int64_t k = fbase + 32 * static_cast<int64_t>(fj + u);
+      c[u] = in ? ld_stream(B.col + k, pol) : 0;
+      v[u] = in ? ld_stream(B.val + k, pol) : 0.0;
+    }
+    sl = F.s;
+    fj += kBatchB;
+    last = fj >= flen;
+    if (last) {
+      more = F.step(B);
+      if (more) {
+        fbase = B.slice_ptr[F.s];
+        flen = static_cast<int>((B.slice_ptr[F.s + 1] - fbase) >> 5);
+        fbase += lane;
+        fj = 0;
+      }
+    }
+  };
+  int cn[kBatchB];
+  double vn[kBatchB];
+  bool lastn;
+  int64_t sn;
+  fetch(cn, vn, lastn, sn);
+  double sum = 0.0;
+  for (;;) {
+    int c[kBatchB];
+    double v[kBatchB], xv[kBatchB];
+#pragma unroll
+    for (int u = 0; u < kBatchB; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
+    const bool last = lastn;
+    const int64_t sl = sn;
+    const bool had_more = more;
+    if (more) fetch(cn, vn, lastn, sn);
+#pragma unroll
+    for (int u = 0; u < kBatchB; ++u) xv[u] = B.p[c[u]];
+#pragma unroll
+    for (int u = 0; u < kBatchB; ++u) sum += v[u] * xv[u];
+    if (last) {
+      const int64_t row = sl * 32 + lane;
+      B.q[row] = sum;
+      const double pq = warp_sum(B.p[row] * sum);
+      if (lane == 0) B.partial[sl] = pq;
+      sum = 0.0;
+      if (!had_more) break;
+    }
+  }
+}
+
+// alpha (or breakdown) per block
+__global__ void __launch_bounds__(kBT) k_b_fin_alpha(View B) {
+  finish_blocks<1, false>(B, [&](int i, const double* tot) {
+    if (fabs(tot[0]) < 1e-30) {  // :453-457
+      B.status[i] = EMG_NUMERICAL_ERROR;
+      B.done[i] = 1;
+    } else {
+      B.alpha[i] = B.rz[i] / tot[0];
+    }
+  });
+}
+
+// x += alpha p, r -= alpha q, z = D^-1 r; per-slice r.z and r.r
+__global__ void __launch_bounds__(kBT) k_b_update(View B) {
+  active_slices(B, [&](int64_t s, int inst, int lane) {
+    const int64_t row = s * 32 + lane;
+    const double a = B.alpha[inst];
+    B.x[row] += a * B.p[row];
+    const double ri = B.r[row] - a * B.q[row];
+    const double zi = B.dinv[row] * ri;
+    B.r[row] = ri;
+    B.z[row] = zi;
+    const double rz = warp_sum(ri * zi), rr = warp_sum(ri * ri);
+    if (lane == 0) { B.partial[2 * s] = rz; B.partial[2 * s + 1] = rr; }
+  });
+}
+
+// residual test and beta per block (CGSolver::solve_with_jacobi, :459-495)
+__global__ void __launch_bounds__(kBT) k_b_fin_beta(View B) {
+  finish_blocks<2, false>(B, [&](int i, const double* tot) {
+    const int it = B.iter[i];
+    const double res = sqrt(tot[1]) / B.bnorm[i];
+    B.res[i] = res;
+    if (res < B.tol[0]) {
+      B.status[i] = EMG_SUCCESS; B.done[i] = 1;
+    } else if (it > 10 && res > B.prev[i] * 1000.0) {  // :477-483
+      B.status[i] = EMG_DIVERGED; B.done[i] = 1;
+    } else {
+      B.beta[i] = tot[0] / B.rz[i];
+      B.rz[i] = tot[0];
+      B.prev[i] = res;
+      if (it >= B.ctl[4]) { B.status[i] = EMG_MAX_ITER_REACHED; B.done[i] = 1; }
+      else B.iter[i] = it + 1;
+    }
+  });
+}
+
+__global__ void __launch_bounds__(kBT) k_b_direction(View B) {
+  active_slices(B, [&](int64_t s, int inst, int lane) {
+    const int64_t row = s * 32 + lane;
+    B.p[row] = B.z[row] + B.beta[inst] * B.p[row];
+  });
 }
 
 // Warp per slice: permuted column (via iperm) and CSR source per slot.
@@ -559,66 +638,35 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
     k_b_widen_iperm<<<launch_grid(N), 256, 0, st>>>(ns, d_off, P.slice_ptr, N, P.perm, d_iperm);
     if (cudaGetLastError() != cudaSuccess) { set_error("batch plan launch failed"); rc = EMG_ERR_CUDA; }
   }
-  std::vector<int64_t> sp(ns + 1, 0);
-  if (!rc && cudaMemcpyAsync(sp.data(), P.slice_ptr, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, st) !=
-                 cudaSuccess) {
-    set_error("batch plan copy failed");
-    rc = EMG_ERR_CUDA;
-  }
   for (void* p : {static_cast<void*>(d_slots), static_cast<void*>(d_off), static_cast<void*>(d_wrow),
                   static_cast<void*>(d_wout), static_cast<void*>(d_wlen)})
     cudaFreeAsync(p, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) { set_error("batch plan failed"); rc = EMG_ERR_CUDA; }
   if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
-  std::vector<int32_t> sinst(ns);
-  {
-    int32_t k = 0;
-    for (int64_t s2 = 0; s2 < ns; ++s2) {
-      while (s2 * 32 >= nstart[k + 1]) ++k;
-      sinst[s2] = k;
-    }
-  }
-  // CTA ranges: contiguous slices, ~equal slots, at most kMaxLocal blocks each
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t parts = static_cast<int64_t>(EMG_BATCH_CTAS_PER_SM) * sms;
-  const int64_t target = std::max<int64_t>(1, (sp[ns] + parts - 1) / parts);
-  std::vector<int32_t> cs{0}, cseg;
-  std::vector<int32_t> iseg_cnt(nb, 0);
-  {
-    int64_t acc = 0;
-    int32_t first = ns > 0 ? sinst[0] : 0;
-    for (int64_t s = 0; s < ns; ++s) {
-      const bool split = s > cs.back() && (acc >= target || sinst[s] - first >= kMaxLocal);
-      if (split) { cs.push_back(static_cast<int32_t>(s)); acc = 0; first = sinst[s]; }
-      acc += sp[s + 1] - sp[s];
-    }
-    if (ns > 0) cs.push_back(static_cast<int32_t>(ns));
-  }
-  const int32_t nctas = static_cast<int32_t>(cs.size()) - 1;
-  int32_t nsegs = 0;
-  for (int32_t c = 0; c < nctas; ++c) {
-    cseg.push_back(nsegs);
-    const int32_t f = sinst[cs[c]], l = sinst[cs[c + 1] - 1];
-    for (int32_t k = f; k <= l; ++k) iseg_cnt[k]++;
-    nsegs += l - f + 1;
-  }
-  std::vector<int32_t> iseg(nb + 1, 0);
-  for (int32_t k = 0; k < nb; ++k) iseg[k + 1] = iseg[k] + iseg_cnt[k];
-  // a block without rows has no segments; its sums are 0 and it finishes at once
-  P.n = n; P.N = N; P.nslices = ns; P.slots = sp[ns]; P.nb = nb; P.nctas = nctas; P.nsegs = nsegs;
+  // slices of every block; a block without rows has none, sums 0 and
+  // finishes at once
+  std::vector<int32_t> islice(nb + 1);
+  for (int32_t k = 0; k <= nb; ++k) islice[k] = static_cast<int32_t>(nstart[k] / 32);
+  P.n = n; P.N = N; P.nslices = ns; P.slots = total; P.nb = nb;
   P.blocks = blocks;
-  if (!rc) rc = dalloc(&P.slice_inst, ns, st);
-  if (!rc) rc = dalloc(&P.cta_slice, nctas + 1, st);
-  if (!rc) rc = dalloc(&P.cta_seg, nctas, st);
-  if (!rc) rc = dalloc(&P.inst_seg, nb + 1, st);
+  {
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_spmv_dot, kBT, 0) != cudaSuccess || per < 1) per = 4;
+    P.grid_spmv = per * sms;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_update, kBT, 0) != cudaSuccess || per < 1) per = 4;
+    P.grid_vec = per * sms;
+    cudaGetLastError();
+  }
+  if (!rc) rc = dalloc(&P.inst_slice, nb + 1, st);
+  if (!rc) rc = dalloc(&P.act_inst, nb, st);
+  if (!rc) rc = dalloc(&P.act_start, nb + 1, st);
   if (!rc) rc = dalloc(&P.col, P.slots, st);
   if (!rc) rc = dalloc(&P.src, P.slots, st);
   if (!rc) rc = dalloc(&P.val, P.slots, st);
   for (double** v : {&P.x, &P.r, &P.z, &P.p, &P.q, &P.dinv})
     if (!rc) rc = dalloc(v, N, st);
-  if (!rc) rc = dalloc(&P.partial, 2 * static_cast<int64_t>(std::max(nsegs, 1)), st);
+  if (!rc) rc = dalloc(&P.partial, 2 * ns, st);
   for (double** v : {&P.bnorm, &P.rz, &P.alpha, &P.beta, &P.res, &P.prev})
     if (!rc) rc = dalloc(v, nb, st);
   for (int32_t** v : {&P.iter, &P.status, &P.done})
@@ -626,10 +674,7 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
   if (!rc) rc = dalloc(&P.ctl, 8, st);
   if (!rc) rc = dalloc(&P.tol, 1, st);
   if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
-  if (ns > 0) EMG_CK(cudaMemcpyAsync(P.slice_inst, sinst.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemcpyAsync(P.cta_slice, cs.data(), sizeof(int32_t) * (nctas + 1), cudaMemcpyHostToDevice, st));
-  if (nctas > 0) EMG_CK(cudaMemcpyAsync(P.cta_seg, cseg.data(), sizeof(int32_t) * nctas, cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemcpyAsync(P.inst_seg, iseg.data(), sizeof(int32_t) * (nb + 1), cudaMemcpyHostToDevice, st));
+  EMG_CK(cudaMemcpyAsync(P.inst_slice, islice.data(), sizeof(int32_t) * (nb + 1), cudaMemcpyHostToDevice, st));
   EMG_CK(cudaMemsetAsync(P.ctl, 0, sizeof(int32_t) * 8, st));
   if (ns > 0)
     k_b_fill<<<launch_grid(ns * 32), 256, 0, st>>>(ns, P.slice_ptr, P.perm, d_iperm, A.row_ptr, A.col, P.col, P.src);
@@ -639,6 +684,11 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
   EMG_CK(cudaStreamCreate(&P.cap));
   P.version = ~uint64_t(0);
   return EMG_SUCCESS;
+}
+
+// Warp per block for the per-block sums.
+int fin_grid(int32_t nb) {
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((nb + kBT / 32 - 1) / (kBT / 32), 148 * 8)));
 }
 
 int capture_batch_loop(BatchPlan& P) {
@@ -658,12 +708,15 @@ int capture_batch_loop(BatchPlan& P) {
     e = cudaStreamBeginCaptureToGraph(P.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       const View v = view_of(P);
+      const int gf = fin_grid(P.nb);
       for (int k = 0; k < kBodyB; ++k) {
-        k_b_spmv_dot<<<P.nctas, kBThreads, 0, P.cap>>>(v);
-        k_b_update<<<P.nctas, kBThreads, 0, P.cap>>>(v);
-        k_b_direction<<<P.nctas, kBThreads, 0, P.cap>>>(v);
+        k_b_spmv_dot<<<P.grid_spmv, kBT, 0, P.cap>>>(v);
+        k_b_fin_alpha<<<gf, kBT, 0, P.cap>>>(v);
+        k_b_update<<<P.grid_vec, kBT, 0, P.cap>>>(v);
+        k_b_fin_beta<<<gf, kBT, 0, P.cap>>>(v);
+        k_b_direction<<<P.grid_vec, kBT, 0, P.cap>>>(v);
       }
-      k_b_control<<<1, 256, 0, P.cap>>>(v, handle);
+      k_b_list<true><<<1, 1024, 0, P.cap>>>(v, handle);
       e = cudaStreamEndCapture(P.cap, &body);
     }
   }
@@ -681,9 +734,8 @@ int capture_batch_loop(BatchPlan& P) {
 
 BatchPlan::~BatchPlan() {
   if (loop) cudaGraphExecDestroy(loop);
-  for (void* p : {static_cast<void*>(perm), static_cast<void*>(slice_ptr), static_cast<void*>(slice_inst),
-                  static_cast<void*>(cta_slice), static_cast<void*>(cta_seg), static_cast<void*>(inst_seg),
-                  static_cast<void*>(col), static_cast<void*>(src), static_cast<void*>(val),
+  for (void* p : {static_cast<void*>(perm), static_cast<void*>(slice_ptr), static_cast<void*>(inst_slice),
+                  static_cast<void*>(act_inst), static_cast<void*>(act_start), static_cast<void*>(col), static_cast<void*>(src), static_cast<void*>(val),
                   static_cast<void*>(x), static_cast<void*>(r), static_cast<void*>(z), static_cast<void*>(p),
                   static_cast<void*>(q), static_cast<void*>(dinv), static_cast<void*>(partial),
                   static_cast<void*>(bnorm), static_cast<void*>(rz), static_cast<void*>(alpha),
@@ -754,8 +806,11 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
   EMG_CK(cudaMemcpyAsync(P.tol, &cfg.tolerance, sizeof(double), cudaMemcpyHostToDevice, st));
   const View v = view_of(P);
   k_b_jacobi<<<launch_grid(P.N), 256, 0, st>>>(v, A.row_ptr, A.col, A.val, cfg.preconditioner);
-  if (P.nctas > 0) k_b_init<<<P.nctas, kBThreads, 0, st>>>(v, b);
-  k_b_active<<<1, 256, 0, st>>>(v);
+  EMG_CK(cudaMemsetAsync(P.done, 0, sizeof(int32_t) * nb, st));
+  k_b_list<false><<<1, 1024, 0, st>>>(v, cudaGraphConditionalHandle{});  // every block
+  k_b_init<<<P.grid_vec, kBT, 0, st>>>(v, b);
+  k_b_fin_init<<<fin_grid(nb), kBT, 0, st>>>(v);
+  k_b_list<false><<<1, 1024, 0, st>>>(v, cudaGraphConditionalHandle{});  // blocks with b != 0
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaGraphLaunch(P.loop, st));
   k_b_scatter<<<launch_grid(P.N), 256, 0, st>>>(P.N, P.perm, P.x, x);

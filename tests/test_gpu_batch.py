@@ -78,3 +78,44 @@ def test_batch_statuses_and_coupling_check():
                                      C.byref(cfg), None, out)
     assert rc == _abi.EMG_INVALID_INPUT
     assert b"couples" in L.emg_last_error()
+
+
+@pytest.mark.gpu
+def test_batch_zero_block_rhs_finishes_at_once():
+    """A block whose right-hand side is zero finishes in the first list
+    (SUCCESS, 0 iterations, x = 0) while the others iterate to the oracle's
+    solutions; blocks leave the active list as they converge."""
+    import torch
+    b = batch.build_batch(instances(), threads=2)
+    S = batch.BatchSystem(b)
+    rp, col, kv, rhs = S.export()
+    r0, r1 = b.block_row_ptr[2], b.block_row_ptr[3]
+    rhs = rhs.copy()
+    rhs[r0:r1] = 0.0
+    bd = torch.from_numpy(rhs).cuda()
+    x = torch.full((b.n_rows,), 7.0, dtype=torch.float64, device="cuda")
+    L = _abi.lib()
+    nb = len(b.instances)
+    out = (_abi.Result * nb)()
+    cfg = _abi.KrylovConfig(1e-10, 20000, 1)
+    rc = L.emg_batch_cg_solve_device(L.emg_system_matrix(S.h, 0), nb, _abi.ptr(b.block_row_ptr),
+                                     C.c_void_p(bd.data_ptr()), C.c_void_p(x.data_ptr()), C.byref(cfg), None, out)
+    torch.cuda.synchronize()
+    assert rc == _abi.EMG_SUCCESS, L.emg_last_error()
+    xs = x.cpu().numpy()
+    assert out[2].status == _abi.EMG_SUCCESS and out[2].iterations == 0
+    assert np.all(xs[r0:r1] == 0.0)
+    its = []
+    for k in range(nb):
+        if k == 2:
+            continue
+        a0, a1 = b.block_row_ptr[k], b.block_row_ptr[k + 1]
+        blk = slice(rp[a0], rp[a1])
+        orp = (rp[a0:a1 + 1] - rp[a0]).astype(np.int64)
+        ocol = (col[blk] - a0).astype(np.int32)
+        xo, st, it, _ = O.pcg(orp, ocol, kv[blk], rhs[a0:a1], tol=1e-10, max_iter=20000, precond=1)
+        assert out[k].status == st == 0
+        assert abs(out[k].iterations - it) <= max(3, 0.15 * it)
+        assert np.linalg.norm(xs[a0:a1] - xo) <= 1e-8 * np.linalg.norm(xo)
+        its.append(out[k].iterations)
+    assert len(set(its)) > 3  # blocks finish at different iterations
