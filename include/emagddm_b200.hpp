@@ -123,6 +123,29 @@ class EMDOFManager {
     run(mode);
     gauged_ = true;
   }
+  // Elements with Element::dof_type SCALAR_ONLY / VECTOR_EDGE_ONLY / MIXED_AV
+  // (EMG_DOF_*), scalar Dirichlet node IDs: EMDOFManager::build (+
+  // applyTreeGauge for mode >= 0).  Returns Local2Global::indices per
+  // element (node DOFs, edge DOFs, or node then edge DOFs).
+  std::vector<std::vector<int32_t>> buildWithDofTypes(const std::vector<int32_t>& dof_type,
+                                                      const std::vector<int32_t>& scalar_dirichlet,
+                                                      int32_t mode = EMG_GAUGE_REF) {
+    int32_t et = 0, npe = 0, epe = 0;
+    emg_mesh_elem_type(mesh_.handle(), &et, &npe, &epe);
+    const size_t ne = dof_type.size(), w = static_cast<size_t>(npe + epe);
+    std::vector<int32_t> rows(w * ne);
+    int64_t ns = 0, nf = 0, nd = 0;
+    if (emg_dof_build_av(mesh_.handle(), dof_type.data(), static_cast<int64_t>(scalar_dirichlet.size()),
+                         scalar_dirichlet.data(), mode, rows.data(), &ns, &nf, &nd) != EMG_SUCCESS)
+      throw std::invalid_argument("EMDOFManager: " + last_error());
+    std::vector<std::vector<int32_t>> out(ne);
+    for (size_t e = 0; e < ne; ++e)
+      for (size_t k = 0; k < w && rows[w * e + k] != EMG_DOF_ABSENT; ++k) out[e].push_back(rows[w * e + k]);
+    n_dofs_ = nd;
+    n_scalar_free_ = ns;
+    return out;
+  }
+  int getNumScalarFreeDOFs() const { return static_cast<int>(n_scalar_free_); }
   int getNumFreeDOFs() const { return static_cast<int>(n_dofs_); }
   const std::vector<int32_t>& getElemLocalToGlobal() const { return l2g_; }
   const std::vector<int32_t>& getEdgeToDOF() const { return edge_dof_; }
@@ -152,6 +175,7 @@ class EMDOFManager {
   const Mesh& mesh_;
   emg_dofmap map_ = nullptr;
   int64_t n_dofs_ = 0;
+  int64_t n_scalar_free_ = 0;
   bool gauged_ = false;
   std::vector<int32_t> l2g_, edge_dof_;
 };

@@ -7,7 +7,7 @@
 // the hexes as HEX8_EDGE elements; --wiggle moves every interior node by
 // 0.2 h sin(...) per coordinate (a deterministic non-affine geometry) and
 // --xyz writes the node coordinates used.
-// Usage: solve_cube <n> [--numbering-only] [--direct] [--hex] [--wiggle]
+// Usage: solve_cube <n> [--numbering-only] [--direct] [--hex] [--wiggle] [--av]
 //                       [--x out.bin] [--xyz out.bin]
 // Prints one line of key=value pairs.
 #include <cmath>
@@ -20,7 +20,7 @@
 
 int main(int argc, char** argv) {
   const int n = argc > 1 ? std::atoi(argv[1]) : 4;
-  bool numbering_only = false, direct = false, hex = false, wiggle = false;
+  bool numbering_only = false, direct = false, hex = false, wiggle = false, av = false;
   const char* xout = nullptr;
   const char* xyzout = nullptr;
   for (int i = 2; i < argc; ++i) {
@@ -28,6 +28,7 @@ int main(int argc, char** argv) {
     if (!std::strcmp(argv[i], "--direct")) direct = true;
     if (!std::strcmp(argv[i], "--hex")) hex = true;
     if (!std::strcmp(argv[i], "--wiggle")) wiggle = true;
+    if (!std::strcmp(argv[i], "--av")) av = true;
     if (!std::strcmp(argv[i], "--x") && i + 1 < argc) xout = argv[++i];
     if (!std::strcmp(argv[i], "--xyz") && i + 1 < argc) xyzout = argv[++i];
   }
@@ -95,6 +96,22 @@ int main(int argc, char** argv) {
   for (int32_t v : dofs.getElemLocalToGlobal()) l2g_sum += v;
   std::printf("n=%d edges=%d free=%d dofs=%d l2g_sum=%lld", n, gen.getNumGlobalEdges(), n_free,
               dofs.getNumFreeDOFs(), l2g_sum);
+  if (av) {
+    // element DOF types SCALAR_ONLY / VECTOR_EDGE_ONLY / MIXED_AV in turn,
+    // scalar Dirichlet on every boundary node
+    std::vector<int32_t> types, phi;
+    for (size_t t = 0; t < tets.size() / npe; ++t) types.push_back(static_cast<int32_t>(t % 3));
+    for (int g = 0; g < n1 * n1 * n1; ++g)
+      for (int c = 0; c < 3; ++c)
+        if (coord(g, c) == 0 || coord(g, c) == n) { phi.push_back(g); break; }
+    emg::EMDOFManager av_dofs(mesh);
+    const auto rows = av_dofs.buildWithDofTypes(types, phi, EMG_GAUGE_REF);
+    long long av_sum = 0, av_len = 0;
+    for (const auto& r : rows)
+      for (int32_t v : r) { av_sum += v; ++av_len; }
+    std::printf(" av_dofs=%d av_scalar=%d av_sum=%lld av_len=%lld", av_dofs.getNumFreeDOFs(),
+                av_dofs.getNumScalarFreeDOFs(), av_sum, av_len);
+  }
   if (numbering_only) {
     std::printf("\n");
     return 0;

@@ -65,6 +65,26 @@ def test_cpp_direct_backend_matches_oracle(tmp_path):
     assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
 
 
+@pytest.mark.parametrize("n,hexes", [(3, False), (4, True)])
+def test_cpp_dof_types_match_oracle(n, hexes):
+    """EMDOFManager::buildWithDofTypes (per-element SCALAR_ONLY /
+    VECTOR_EDGE_ONLY / MIXED_AV) from C++ against the oracle."""
+    rc, kv = run(n, "--numbering-only", "--av", *(["--hex"] if hexes else []))
+    assert rc == 0
+    if hexes:
+        xyz, el, d = mesh.hex_topology(n)
+    else:
+        m = mesh.plain_small(n)
+        xyz, el, d = m.xyz, m.tets, m.dirichlet
+    t = (np.arange(el.shape[0]) % 3).astype(np.int32)
+    bnd = np.where(np.any((xyz < 1e-12) | (xyz > 1 - 1e-12), axis=1))[0].astype(np.int32)
+    o = O.dof_build_av(el, t, d, bnd, gauge=O.GAUGE_REF, n_nodes=len(xyz))
+    rows = o["l2g"]
+    assert int(kv["av_dofs"]) == o["n_dofs"] and int(kv["av_scalar"]) == o["n_scalar_free"]
+    assert int(kv["av_sum"]) == int(rows[rows != -2].astype(np.int64).sum())
+    assert int(kv["av_len"]) == int((rows != -2).sum())
+
+
 @pytest.mark.parametrize("n", [2, 3, 5])
 def test_cpp_hex_numbering_matches_oracle(n):
     rc, kv = run(n, "--numbering-only", "--hex")

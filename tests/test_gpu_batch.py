@@ -119,3 +119,28 @@ def test_batch_zero_block_rhs_finishes_at_once():
         assert np.linalg.norm(xs[a0:a1] - xo) <= 1e-8 * np.linalg.norm(xo)
         its.append(out[k].iterations)
     assert len(set(its)) > 3  # blocks finish at different iterations
+
+
+@pytest.mark.gpu
+def test_batch_more_blocks_than_one_list_chunk():
+    """1,100 small blocks: the active list is built in chunks of 1,024 blocks;
+    every block converges and a sample matches the oracle's own solves."""
+    import torch
+    inst = [mesh.random_instance(2 + (k % 3), 1000 + k) for k in range(1100)]
+    b = batch.build_batch(inst, threads=4)
+    S = batch.BatchSystem(b)
+    rp, col, kv, rhs = S.export()
+    x = torch.zeros(b.n_rows, dtype=torch.float64, device="cuda")
+    rc, res = S.solve(x.data_ptr(), tol=1e-10, max_iter=5000)
+    torch.cuda.synchronize()
+    assert rc == _abi.EMG_SUCCESS, (rc, _abi.lib().emg_last_error())
+    assert all(r["status"] == _abi.EMG_SUCCESS for r in res)
+    xs = x.cpu().numpy()
+    for k in (0, 511, 1023, 1024, 1099):
+        a0, a1 = b.block_row_ptr[k], b.block_row_ptr[k + 1]
+        blk = slice(rp[a0], rp[a1])
+        orp = (rp[a0:a1 + 1] - rp[a0]).astype(np.int64)
+        ocol = (col[blk] - a0).astype(np.int32)
+        xo, st, it, _ = O.pcg(orp, ocol, kv[blk], rhs[a0:a1], tol=1e-10, max_iter=5000, precond=1)
+        assert st == 0 and abs(res[k]["iterations"] - it) <= max(3, 0.15 * it)
+        assert np.linalg.norm(xs[a0:a1] - xo) <= 1e-8 * max(np.linalg.norm(xo), 1e-300)
