@@ -123,7 +123,7 @@ __device__ __forceinline__ void active_slices(const View& B, Body body) {
   int64_t s = B.inst_slice[inst] + (a - B.act_start[j]);
   bool live = !B.done[inst];
   for (int64_t t = a; t < b; ++t, ++s) {
-    if (t == next) {
+    while (t == next) {  // a listed block without rows is passed over
       ++j;
       inst = B.act_inst[j];
       next = B.act_start[j + 1];
@@ -310,7 +310,7 @@ struct SliceCursor {
   __device__ __forceinline__ bool step(const View& B) {
     ++t;
     ++s;
-    if (t < end && t == next) {
+    while (t < end && t == next) {  // a listed block without rows is passed over
       ++j;
       inst = B.act_inst[j];
       next = B.act_start[j + 1];

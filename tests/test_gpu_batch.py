@@ -144,3 +144,32 @@ def test_batch_more_blocks_than_one_list_chunk():
         xo, st, it, _ = O.pcg(orp, ocol, kv[blk], rhs[a0:a1], tol=1e-10, max_iter=5000, precond=1)
         assert st == 0 and abs(res[k]["iterations"] - it) <= max(3, 0.15 * it)
         assert np.linalg.norm(xs[a0:a1] - xo) <= 1e-8 * max(np.linalg.norm(xo), 1e-300)
+
+
+@pytest.mark.gpu
+def test_batch_with_empty_blocks():
+    """Instances without free DOFs (n = 1 cubes, every edge on the boundary)
+    give empty blocks, two of them adjacent: they finish at once and the
+    blocks around them still match the oracle."""
+    import torch
+    inst = [mesh.random_instance(3, 1), mesh.random_instance(1, 2), mesh.random_instance(1, 3),
+            mesh.random_instance(4, 4), mesh.random_instance(1, 5)]
+    b = batch.build_batch(inst, threads=2)
+    assert b.block_row_ptr[1] == b.block_row_ptr[3] and b.block_row_ptr[4] == b.block_row_ptr[5]
+    S = batch.BatchSystem(b)
+    rp, col, kv, rhs = S.export()
+    x = torch.zeros(b.n_rows, dtype=torch.float64, device="cuda")
+    rc, res = S.solve(x.data_ptr(), tol=1e-10, max_iter=5000)
+    torch.cuda.synchronize()
+    assert rc == _abi.EMG_SUCCESS, (rc, _abi.lib().emg_last_error())
+    for k in (1, 2, 4):
+        assert res[k]["status"] == _abi.EMG_SUCCESS and res[k]["iterations"] == 0
+    xs = x.cpu().numpy()
+    for k in (0, 3):
+        a0, a1 = b.block_row_ptr[k], b.block_row_ptr[k + 1]
+        blk = slice(rp[a0], rp[a1])
+        orp = (rp[a0:a1 + 1] - rp[a0]).astype(np.int64)
+        ocol = (col[blk] - a0).astype(np.int32)
+        xo, st, it, _ = O.pcg(orp, ocol, kv[blk], rhs[a0:a1], tol=1e-10, max_iter=5000, precond=1)
+        assert res[k]["status"] == st == 0 and abs(res[k]["iterations"] - it) <= max(3, 0.15 * it)
+        assert np.linalg.norm(xs[a0:a1] - xo) <= 1e-8 * np.linalg.norm(xo)
