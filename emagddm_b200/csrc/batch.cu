@@ -618,16 +618,31 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
   if (!rc) rc = dalloc(&d_wrow, nwin, st);
   if (!rc) rc = dalloc(&d_wout, nwin, st);
   if (!rc) rc = dalloc(&d_wlen, nwin, st);
-  if (rc) return rc;
-  EMG_CK(cudaMemsetAsync(P.perm, 0xff, sizeof(int32_t) * std::max<int64_t>(N, 1), st));
-  if (nwin > 0) {
-    EMG_CK(cudaMemcpyAsync(d_wrow, wrow.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st));
-    EMG_CK(cudaMemcpyAsync(d_wout, wout.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st));
-    EMG_CK(cudaMemcpyAsync(d_wlen, wlen.data(), sizeof(int32_t) * nwin, cudaMemcpyHostToDevice, st));
-    k_b_window_perm<<<static_cast<unsigned>(nwin), 32, 0, st>>>(d_wrow, d_wlen, d_wout, A.row_ptr, P.perm);
+  // scratch goes back on every exit (the plan's own arrays go with the plan)
+  auto release = [&](bool with_iperm) {
+    for (void* q : {static_cast<void*>(d_slots), static_cast<void*>(d_off), static_cast<void*>(d_wrow),
+                    static_cast<void*>(d_wout), static_cast<void*>(d_wlen)})
+      if (q) cudaFreeAsync(q, st);
+    d_slots = d_off = d_wlen = nullptr;
+    d_wrow = d_wout = nullptr;
+    if (with_iperm && d_iperm) cudaFreeAsync(d_iperm, st);
+  };
+  if (rc) { release(true); return rc; }
+  cudaError_t e = cudaMemsetAsync(P.perm, 0xff, sizeof(int32_t) * std::max<int64_t>(N, 1), st);
+  if (e == cudaSuccess && nwin > 0) {
+    e = cudaMemcpyAsync(d_wrow, wrow.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_wout, wout.data(), sizeof(int64_t) * nwin, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_wlen, wlen.data(), sizeof(int32_t) * nwin, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      k_b_window_perm<<<static_cast<unsigned>(nwin), 32, 0, st>>>(d_wrow, d_wlen, d_wout, A.row_ptr, P.perm);
   }
-  if (ns > 0) k_b_slice_slots<<<launch_grid(ns * 32), 256, 0, st>>>(ns, P.perm, A.row_ptr, d_slots);
-  EMG_CK(cudaGetLastError());
+  if (e == cudaSuccess && ns > 0) k_b_slice_slots<<<launch_grid(ns * 32), 256, 0, st>>>(ns, P.perm, A.row_ptr, d_slots);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    release(true);
+    set_error(std::string("batch plan: ") + cudaGetErrorString(e));
+    return EMG_ERR_CUDA;
+  }
   int64_t total = 0;
   rc = scan_counts(d_slots, d_off, ns, &total, st);
   if (!rc && total >= (int64_t(1) << 31)) {
@@ -638,10 +653,8 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
     k_b_widen_iperm<<<launch_grid(N), 256, 0, st>>>(ns, d_off, P.slice_ptr, N, P.perm, d_iperm);
     if (cudaGetLastError() != cudaSuccess) { set_error("batch plan launch failed"); rc = EMG_ERR_CUDA; }
   }
-  for (void* p : {static_cast<void*>(d_slots), static_cast<void*>(d_off), static_cast<void*>(d_wrow),
-                  static_cast<void*>(d_wout), static_cast<void*>(d_wlen)})
-    cudaFreeAsync(p, st);
-  if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
+  release(rc != EMG_SUCCESS);
+  if (rc) return rc;
   // slices of every block; a block without rows has none, sums 0 and
   // finishes at once
   std::vector<int32_t> islice(nb + 1);
@@ -674,13 +687,18 @@ int build_plan(DevCsr& A, const std::vector<int64_t>& blocks, cudaStream_t st, B
   if (!rc) rc = dalloc(&P.ctl, 8, st);
   if (!rc) rc = dalloc(&P.tol, 1, st);
   if (rc) { cudaFreeAsync(d_iperm, st); return rc; }
-  EMG_CK(cudaMemcpyAsync(P.inst_slice, islice.data(), sizeof(int32_t) * (nb + 1), cudaMemcpyHostToDevice, st));
-  EMG_CK(cudaMemsetAsync(P.ctl, 0, sizeof(int32_t) * 8, st));
-  if (ns > 0)
+  e = cudaMemcpyAsync(P.inst_slice, islice.data(), sizeof(int32_t) * (nb + 1), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.ctl, 0, sizeof(int32_t) * 8, st);
+  if (e == cudaSuccess && ns > 0) {
     k_b_fill<<<launch_grid(ns * 32), 256, 0, st>>>(ns, P.slice_ptr, P.perm, d_iperm, A.row_ptr, A.col, P.col, P.src);
-  EMG_CK(cudaGetLastError());
-  EMG_CK(cudaFreeAsync(d_iperm, st));
-  EMG_CK(cudaStreamSynchronize(st));
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(d_iperm, st);  // the plan's own arrays go with the plan
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    set_error(std::string("batch plan: ") + cudaGetErrorString(e));
+    return EMG_ERR_CUDA;
+  }
   EMG_CK(cudaStreamCreate(&P.cap));
   P.version = ~uint64_t(0);
   return EMG_SUCCESS;
@@ -768,15 +786,24 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
     // block-diagonal check on the device
     int32_t* d_bad = nullptr;
     int64_t* d_blocks = nullptr;
-    EMG_CK(cudaMallocAsync(&d_blocks, sizeof(int64_t) * (nb + 1), st));
-    EMG_CK(cudaMallocAsync(&d_bad, sizeof(int32_t), st));
-    EMG_CK(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, st));
-    EMG_CK(cudaMemsetAsync(d_bad, 0, sizeof(int32_t), st));
-    k_b_check<<<launch_grid(A.n), 256, 0, st>>>(A.n, A.row_ptr, A.col, nb, d_blocks, d_bad);
     int32_t bad = 0;
-    EMG_CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    EMG_CK(cudaStreamSynchronize(st));
-    for (void* p : {static_cast<void*>(d_blocks), static_cast<void*>(d_bad)}) EMG_CK(cudaFreeAsync(p, st));
+    cudaError_t e = cudaMallocAsync(&d_blocks, sizeof(int64_t) * (nb + 1), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_bad, sizeof(int32_t), st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int32_t), st);
+    if (e == cudaSuccess) {
+      k_b_check<<<launch_grid(A.n), 256, 0, st>>>(A.n, A.row_ptr, A.col, nb, d_blocks, d_bad);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    for (void* p : {static_cast<void*>(d_blocks), static_cast<void*>(d_bad)})
+      if (p) cudaFreeAsync(p, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      set_error(std::string("batch solve: block check: ") + cudaGetErrorString(e));
+      return EMG_ERR_CUDA;
+    }
     if (bad) { set_error("batch solve: the matrix couples different blocks"); return EMG_INVALID_INPUT; }
     free_batch(A.batch);
     A.batch = new BatchPlan();

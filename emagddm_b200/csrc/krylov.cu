@@ -64,6 +64,10 @@ struct Sell {
   int64_t n = 0, nslices = 0, ngroups = 0, slots = 0;
   int64_t max_tile_slots = 0;    // largest 8-slice tile (bulk-copy stage size)
   bool tma = false;              // stages of the bulk-copy kernels fit in shared memory
+  bool ws = false;               // warp-specialized bulk-copy SpMV in use
+  uint32_t ws_stage_bytes = 0;   // one slice (largest) of values + columns, 128-byte multiple
+  int ws_grid = 0;
+  size_t ws_smem = 0;
   int32_t* perm = nullptr;       // new row -> old row
   int64_t* slice_ptr = nullptr;  // ngroups + 1 slot offsets of the slice groups (multiples of 32 kGroup)
   int16_t* dcol = nullptr;       // column - row of every slot, when all fit in 16 bits
@@ -123,6 +127,18 @@ __device__ __forceinline__ int64_t gstride() {
 // build-time option (-DEMG_SELL_TMA=1) rather than the default.
 #ifndef EMG_SELL_TMA
 #define EMG_SELL_TMA 0
+#endif
+// Warp-specialized bulk-copy SpMV (-DEMG_SELL_WS=1): warp 0 of a block
+// streams the slices of the other warps into per-warp rings of kWsStages
+// shared-memory stages; those warps only gather x.
+#ifndef EMG_SELL_WS
+#define EMG_SELL_WS 0
+#endif
+#ifndef EMG_SELL_WS_CONTIG
+#define EMG_SELL_WS_CONTIG 0
+#endif
+#ifndef EMG_SELL_WS_STAGES
+#define EMG_SELL_WS_STAGES 2
 #endif
 // 16-bit column offsets (10 instead of 12 bytes per slot) when the matrix
 // bandwidth allows: fewer bytes, but measured slower than 32-bit columns on
@@ -204,17 +220,28 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
   const int16_t* __restrict__ dcol = A.dcol;
   const double* __restrict__ val = A.val;
   constexpr int U = EMG_SELL_BATCH;
+#if EMG_SELL_SPREAD == 2
+  // contiguous share of slices per warp
+  const int64_t gwc = gtid() >> 5;
+  const int64_t s_end = A.nslices * (gwc + 1) / nwarps;
+  const int64_t step = 1;
+  int64_t cs = A.nslices * gwc / nwarps;
+  if (cs >= s_end) return;
+#else
+  const int64_t s_end = A.nslices;
+  const int64_t step = nwarps;
   int64_t cs = warp;  // slice whose batch is being summed
   if (cs >= A.nslices) return;
+#endif
   int64_t fs = cs;  // slice being fetched, its lane base, length, next entry
   int64_t fbase;
   int flen;
   slice_span(sp, fs, fbase, flen);
   fbase += lane;
   int fj = 0;
-  int64_t nbase = 0;  // span of slice fs + nwarps
+  int64_t nbase = 0;  // span of slice fs + step
   int nlen = 0;
-  if (fs + nwarps < A.nslices) slice_span(sp, fs + nwarps, nbase, nlen);
+  if (fs + step < s_end) slice_span(sp, fs + step, nbase, nlen);
   bool more = true;
   auto fetch = [&](int (&c)[U], double (&v)[U], bool& last) {
 #pragma unroll
@@ -228,12 +255,12 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
     fj += U;
     last = fj >= flen;
     if (last) {
-      fs += nwarps;
-      more = fs < A.nslices;
+      fs += step;
+      more = fs < s_end;
       fbase = nbase + lane;
       flen = nlen;
       fj = 0;
-      if (fs + nwarps < A.nslices) slice_span(sp, fs + nwarps, nbase, nlen);
+      if (fs + step < s_end) slice_span(sp, fs + step, nbase, nlen);
     }
   };
   int cn[U];
@@ -256,8 +283,8 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
       const int64_t row = cs * kSliceRows + lane;
       if (row < A.n) out(row, sum);
       sum = 0.0;
-      cs += nwarps;
-      if (cs >= A.nslices) break;
+      cs += step;
+      if (cs >= s_end) break;
     }
   }
 }
@@ -453,12 +480,116 @@ __device__ __forceinline__ void sell_rows_tma(const Sell& A, const double* __res
   }
 }
 
+// Warp-specialized bulk-copy SpMV.  Block = 1 producer warp + kWsC
+// consumer warps; consumer c of block b takes slices b kWsC + c + k (kWsC
+// gridDim.x), k = 0, 1, ...; producer lane c copies consumer c's next
+// slices (values, then columns, one byte range each) into c's ring of
+// kWsS stages and the consumer, once a stage's full barrier completes, sums
+// its rows from shared memory (entries in CSR order, kWsU gathers of x in
+// flight per lane) and releases the stage on its empty barrier.  Every wait
+// is bounded: a producer that gives up raises *err and waits (bounded) for
+// the copies it already issued; a consumer that gives up raises *err and
+// stops.
+constexpr int kWsC = kThreads / 32 - 1;
+constexpr int kWsS = EMG_SELL_WS_STAGES;
+constexpr int kWsU = 16;
+__host__ __device__ inline size_t ws_smem_bytes(uint32_t stage_bytes) {
+  return static_cast<size_t>(kWsC) * kWsS * stage_bytes + sizeof(uint64_t) * 2 * kWsC * kWsS +
+         sizeof(uint32_t) * kWsC * kWsS;
+}
+template <class Out>
+__device__ __forceinline__ void sell_rows_ws(const Sell& A, const double* __restrict__ x, Out out,
+                                             int32_t* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const uint32_t sb = A.ws_stage_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + static_cast<size_t>(kWsC) * kWsS * sb);
+  uint64_t* empty = full + kWsC * kWsS;
+  uint32_t* slots_of = reinterpret_cast<uint32_t*>(empty + kWsC * kWsS);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < kWsC * kWsS) {
+    tma::mbar_init(&full[threadIdx.x], 1);
+    tma::mbar_init(&empty[threadIdx.x], 1);
+  }
+  tma::fence_mbar_init();
+  __syncthreads();
+  const int64_t nc = static_cast<int64_t>(gridDim.x) * kWsC;
+  const int64_t* __restrict__ sp = A.slice_ptr;
+  if (warp == 0) {
+    if (lane < kWsC) {
+      const uint64_t pol = evict_first_policy();
+      int k = 0;
+      bool ok = true;
+#if EMG_SELL_WS_CONTIG
+      const int64_t gc = static_cast<int64_t>(blockIdx.x) * kWsC + lane;
+      const int64_t s_end = A.nslices * (gc + 1) / nc;
+      for (int64_t s = A.nslices * gc / nc; s < s_end; ++s, ++k) {
+#else
+      for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWsC + lane; s < A.nslices; s += nc, ++k) {
+#endif
+        const int q = lane * kWsS + k % kWsS;
+        if (k >= kWsS && !tma::mbar_wait(&empty[q], ((k / kWsS) & 1u) ^ 1u)) { ok = false; break; }
+        const int64_t b0 = sp[s];
+        const uint32_t slots = static_cast<uint32_t>(sp[s + 1] - b0);
+        unsigned char* base = smem + static_cast<size_t>(q) * sb;
+        slots_of[q] = slots;
+        tma::fence_proxy_async();
+        tma::mbar_expect_tx(&full[q], slots * 12u);
+        if (slots > 0) {
+          tma::bulk_g2s(base, A.val + b0, slots * 8u, &full[q], pol);
+          tma::bulk_g2s(base + slots * 8u, A.col + b0, slots * 4u, &full[q], pol);
+        }
+      }
+      if (!ok) {
+        atomicOr(err, 1);
+        // the copies issued for the last kWsS slices may still be in flight
+        for (int j = k - kWsS; j < k; ++j)
+          if (j >= 0) tma::mbar_wait(&full[lane * kWsS + j % kWsS], (j / kWsS) & 1u);
+      }
+    }
+    return;
+  }
+  const int c = warp - 1;
+  int k = 0;
+#if EMG_SELL_WS_CONTIG
+  const int64_t gcc = static_cast<int64_t>(blockIdx.x) * kWsC + c;
+  const int64_t c_end = A.nslices * (gcc + 1) / nc;
+  for (int64_t s = A.nslices * gcc / nc; s < c_end; ++s, ++k) {
+#else
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * kWsC + c; s < A.nslices; s += nc, ++k) {
+#endif
+    const int q = c * kWsS + k % kWsS;
+    if (!tma::mbar_wait(&full[q], (k / kWsS) & 1u)) {
+      if (lane == 0) atomicOr(err, 1);
+      break;
+    }
+    const int len = static_cast<int>(slots_of[q] >> 5);
+    const double* sv = reinterpret_cast<const double*>(smem + static_cast<size_t>(q) * sb) + lane;
+    const int32_t* sc =
+        reinterpret_cast<const int32_t*>(smem + static_cast<size_t>(q) * sb + static_cast<size_t>(len) * 256) + lane;
+    double sum = 0.0;
+    for (int j0 = 0; j0 < len; j0 += kWsU) {
+      double xv[kWsU];
+#pragma unroll
+      for (int u = 0; u < kWsU; ++u) xv[u] = j0 + u < len ? x[sc[32 * (j0 + u)]] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kWsU; ++u)
+        if (j0 + u < len) sum += sv[32 * (j0 + u)] * xv[u];
+    }
+    __syncwarp();
+    if (lane == 0) tma::mbar_arrive(&empty[q]);
+    const int64_t row = s * kSliceRows + lane;
+    if (row < A.n) out(row, sum);
+  }
+}
+
 // Row kernels: kMode 0 = SELL with 32-bit columns, 1 = SELL with 16-bit
-// column offsets, 2 = bulk-copy pipeline (32-bit columns).
+// column offsets, 2 = bulk-copy pipeline (32-bit columns), 3 = warp-
+// specialized bulk-copy pipeline.
 template <int kMode, class Out>
 __device__ __forceinline__ void spmv_rows(const Sell& A, const double* __restrict__ x, Out out,
                                           int32_t* err) {
   if constexpr (kMode == 2) sell_rows_tma(A, x, out, err);
+  else if constexpr (kMode == 3) sell_rows_ws(A, x, out, err);
   else sell_rows<kMode == 1>(A, x, out);
 }
 
@@ -1306,10 +1437,41 @@ int build_sell(DevCsr& A, cudaStream_t st) {
     }
   }
 #endif
+  S.ws = false;
+#if EMG_SELL_WS
+  static_assert(kGroup == 1 && !EMG_SELL_PACKED, "the warp-specialized SpMV copies per-slice runs");
+  if (!S.tma && S.nslices > 0) {
+    std::vector<int64_t> sp(S.nslices + 1);
+    EMG_CK(cudaMemcpyAsync(sp.data(), S.slice_ptr, sizeof(int64_t) * (S.nslices + 1), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    int64_t mx = 0;
+    for (int64_t s = 0; s < S.nslices; ++s) mx = std::max<int64_t>(mx, sp[s + 1] - sp[s]);
+    const uint32_t sb = static_cast<uint32_t>(((12 * mx + 127) / 128) * 128);
+    const size_t need = ws_smem_bytes(sb);
+    int dev = 0, optin = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (mx > 0 && need <= static_cast<size_t>(optin)) {
+      const int b = static_cast<int>(need);
+      EMG_CK(cudaFuncSetAttribute(k_cg_spmv_dot<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_v<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_bi_t<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaFuncSetAttribute(k_spmv<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+      EMG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg_spmv_dot<3>, kThreads, need));
+      if (per > 0) {
+        S.ws = true;
+        S.ws_stage_bytes = sb;
+        S.ws_smem = need;
+        S.ws_grid = std::min(per * sms, grid_size());
+      }
+    }
+  }
+#endif
   // 16-bit column offsets when every |column - row| fits (banded numberings,
   // e.g. first-appearance edge IDs of structured meshes): 10 bytes per slot.
   S.narrow = false;
-  if (EMG_SELL_NARROW && !EMG_SELL_PACKED && !S.tma && S.slots > 0) {
+  if (EMG_SELL_NARROW && !EMG_SELL_PACKED && !S.tma && !S.ws && S.slots > 0) {
     int32_t* overflow = nullptr;
     EMG_CK(cudaMallocAsync(&S.dcol, sizeof(int16_t) * S.slots, st));
     EMG_CK(cudaMallocAsync(&overflow, sizeof(int32_t), st));
@@ -1596,12 +1758,20 @@ int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
     if ((S).tma) {                                                                    \
       const SpmvShape sh_ = spmv_shape(S, g);                                         \
       KERNEL<2><<<sh_.grid, kThreads, sh_.smem, st>>>(__VA_ARGS__);                   \
+    } else if (EMG_WS_LAUNCH(KERNEL, S, st, __VA_ARGS__)) {                           \
     } else if ((S).narrow) {                                                          \
       KERNEL<1><<<resident_grid<KERNEL<1>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
     } else {                                                                          \
       KERNEL<0><<<resident_grid<KERNEL<0>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
     }                                                                                 \
   } while (0)
+
+#if EMG_SELL_WS
+#define EMG_WS_LAUNCH(KERNEL, S, st, ...) \
+  ((S).ws ? (KERNEL<3><<<(S).ws_grid, kThreads, (S).ws_smem, st>>>(__VA_ARGS__), true) : false)
+#else
+#define EMG_WS_LAUNCH(KERNEL, S, st, ...) false
+#endif
 
 void launch_iterations(DevCsr& A, bool bicg, int count) {
   KrylovWorkspace& w = *A.ws;
