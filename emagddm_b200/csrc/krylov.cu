@@ -249,8 +249,9 @@ __device__ __forceinline__ void sell_rows_stream(const Sell& A, const double* __
       const bool in = fj + u < flen;
       const int64_t k = fbase + static_cast<int64_t>(kGroupStride) * (fj + u);
       if constexpr (kNarrow) c[u] = in ? static_cast<int>(fs * kSliceRows + lane) + ld_stream(dcol + k, pol) : 0;
+      else if constexpr (EMG_SELL_PACKED) c[u] = in ? ld_stream(col + packed_col_index(k), pol) : 0;
       else c[u] = in ? ld_stream(col + k, pol) : 0;
-      v[u] = in ? ld_stream(val + k, pol) : 0.0;
+      v[u] = in ? ld_stream(val + (EMG_SELL_PACKED ? packed_val_index(k) : k), pol) : 0.0;
     }
     fj += U;
     last = fj >= flen;
@@ -380,7 +381,7 @@ __device__ __forceinline__ void sell_rows_sliced(const Sell& A, const double* __
 
 template <bool kNarrow, class Out>
 __device__ __forceinline__ void sell_rows(const Sell& A, const double* __restrict__ x, Out out) {
-  if constexpr (!EMG_SELL_PACKED && EMG_SELL_PIPE == 2) sell_rows_stream<kNarrow>(A, x, out);
+  if constexpr (EMG_SELL_PIPE == 2) sell_rows_stream<kNarrow>(A, x, out);
   else sell_rows_sliced<kNarrow>(A, x, out);
 }
 
