@@ -168,6 +168,31 @@ def ncu_traffic():
 
 
 # --------------------------------------------------------------------------- ours
+def bind_to_gpu_numa(local_rank):
+    """Restrict this process to the host CPUs NVML reports as local to the
+    GPU, so that the pinned host buffers of the end-to-end arm (allocated
+    afterwards, first touch) sit on the GPU's NUMA node.  Returns a short
+    description for the JSON line; leaves the affinity alone when NVML, the
+    PCI lookup or the intersection with the allowed CPUs comes up empty."""
+    import torch
+    try:
+        import pynvml as N
+        p = torch.cuda.get_device_properties(local_rank)
+        bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        N.nvmlInit()
+        h = N.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        words = (os.cpu_count() + 63) // 64
+        mask = N.nvmlDeviceGetCpuAffinity(h, words)
+        local = {64 * w + b for w, m in enumerate(mask) for b in range(64) if (m >> b) & 1}
+        cpus = local & os.sched_getaffinity(0)
+        if not cpus:
+            return "unbound (no GPU-local CPU allowed)"
+        os.sched_setaffinity(0, cpus)
+        return f"GPU-local NUMA CPUs ({len(cpus)})"
+    except Exception as e:  # NVML missing or refused: measure unbound
+        return f"unbound ({type(e).__name__})"
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -175,6 +200,7 @@ def run_ours(args, rank, world, local_rank):
     L = _abi.lib()
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    host_binding = bind_to_gpu_numa(local_rank)
     m = workload(args.n, args.workload)
     et = m.elem_type
     md = api.EMMeshData.from_cube(m)
@@ -361,7 +387,8 @@ def run_ours(args, rank, world, local_rank):
                    "solve_ms": info["solve_ms"], "phase_ms": phases, "step_ms": step_ms,
                    "median_step_ms": {a: statistics.median(step_ms[a]) for a in ("resident", "e2e")},
                    "solver_format": {"kind": "SELL-32-sigma4096", "slots": slots.value,
-                                     "padding": slots.value / nnz - 1.0}},
+                                     "padding": slots.value / nnz - 1.0},
+                   "host_cpus": host_binding},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h_x.nbytes), "ms_per_step": total_e2e / args.steps,
