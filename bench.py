@@ -369,8 +369,11 @@ def run_ours(args, rank, world, local_rank):
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms * 1e-3)
     e2e_value = world * args.steps / (total_e2e * 1e-3)
-    chunks = -(-iters // 16)
-    launches_per_step = 11 + 1 + 2 + chunks * 16 * 3
+    # per step: 23 launches of create + assemble + SELL build + Jacobi + CG
+    # init (the committed launch list), the solution scatter, and the device
+    # while-loop: bodies of 4 iterations x (SpMV, fused update) + 1 control
+    bodies = -(-iters // 4)
+    launches_per_step = 23 + 1 + bodies * (4 * 2 + 1)
     h2d = xyz.nbytes + tets.nbytes + mat.nbytes + l2g.nbytes
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
