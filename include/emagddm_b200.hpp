@@ -132,6 +132,8 @@ class EMDOFManager {
                                                       int32_t mode = EMG_GAUGE_REF) {
     int32_t et = 0, npe = 0, epe = 0;
     emg_mesh_elem_type(mesh_.handle(), &et, &npe, &epe);
+    if (static_cast<int64_t>(dof_type.size()) != static_cast<int64_t>(mesh_.getElementCount()))
+      throw std::invalid_argument("EMDOFManager: dof_type needs one entry per element");
     const size_t ne = dof_type.size(), w = static_cast<size_t>(npe + epe);
     std::vector<int32_t> rows(w * ne);
     int64_t ns = 0, nf = 0, nd = 0;
