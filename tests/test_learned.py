@@ -1,7 +1,7 @@
 """Learned interface preconditioner: data generation on the CPU (random
 fields, divergence-free curl-T sources) and, on the GPU, the MLP inference
 kernel against a NumPy restatement with BF16-rounded weights, training and
-flexible-CG solves judged by the true FP64 residual."""
+flexible-CG solves checked by the true FP64 residual."""
 import ctypes as C
 
 import numpy as np

@@ -48,7 +48,7 @@ def test_pattern_matches_reference(n):
     np.testing.assert_array_equal(col, FIX[f"n{n}_pattern_col"])
 
 
-def test_survey_counts_16():
+def test_gauged_counts_16():
     m = mesh.plain_small(16)
     g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)
     b = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_BOUNDARY_FIRST)
