@@ -293,6 +293,94 @@ __device__ __forceinline__ void tile_update(double* __restrict__ C, int64_t ldc,
   }
 }
 
+// The same tile product on the FP64 tensor cores: 256 threads, warp w owns
+// rows 8w .. 8w+7 of the tile (eight 8x8 blocks across its 64 columns) and
+// issues mma.sync m8n8k4 FP64 per 4-wide step of k; k-chunks of 16 staged by
+// cp.async, double-buffered, rows padded by 4 doubles so that a fragment
+// load (4 k-rows x 8 rows) hits distinct banks.  16 accumulator doubles a
+// thread instead of 64: four blocks of 256 threads fit an SM.
+#ifndef EMG_FETI_DMMA
+#define EMG_FETI_DMMA 1
+#endif
+constexpr int kMmaThreads = 256;
+constexpr int kMmaPad = kTile + 4;
+struct TileSmemMma {
+  double a[2][kGK][kMmaPad];
+  double b[2][kGK][kMmaPad];
+};
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+template <bool kOverwrite = false>
+__device__ __forceinline__ void tile_update_mma(double* __restrict__ C, int64_t ldc, int mr, int mc,
+                                                const double* __restrict__ A, int64_t lda,
+                                                const double* __restrict__ B, int64_t ldb, int K,
+                                                TileSmemMma& sm) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  double acc[8][2];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+  const int nk = (K + kGK - 1) / kGK;
+  auto load = [&](int chunk, int buf) {
+    const int k0 = chunk * kGK;
+#pragma unroll
+    for (int i = 0; i < (kGK * kTile) / kMmaThreads; ++i) {
+      const int e = t + kMmaThreads * i;
+      const int c = e / kTile, r = e - c * kTile;
+      const bool kin = k0 + c < K;
+      const bool va = kin && r < mr, vb = kin && r < mc;
+      cp_async8(&sm.a[buf][c][r], va ? A + r + static_cast<int64_t>(k0 + c) * lda : A, va);
+      cp_async8(&sm.b[buf][c][r], vb ? B + r + static_cast<int64_t>(k0 + c) * ldb : B, vb);
+    }
+    cp_async_commit();
+  };
+  if (nk > 0) load(0, 0);
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row / k of this lane
+  for (int i = 0; i < nk; ++i) {
+    if (i + 1 < nk) {
+      load(i + 1, (i + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int buf = i & 1;
+#pragma unroll
+    for (int kk = 0; kk < kGK; kk += 4) {
+      const double a = sm.a[buf][kk + fk][8 * w + fr];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[j], a, sm.b[buf][kk + fk][8 * j + fr]);
+    }
+    __syncthreads();
+  }
+  const int rr = 8 * w + fr;
+  if (rr >= mr) return;
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int cc = 8 * j + 2 * fk + q;
+      if (cc < mc) {
+        if (kOverwrite) C[rr + static_cast<int64_t>(cc) * ldc] = acc[j][q];
+        else C[rr + static_cast<int64_t>(cc) * ldc] -= acc[j][q];
+      }
+    }
+}
+#if EMG_FETI_DMMA
+constexpr int kTileThreads = kMmaThreads;
+using TileSmemT = TileSmemMma;
+#define EMG_TILE_UPDATE tile_update_mma
+#else
+constexpr int kTileThreads = 64;
+using TileSmemT = TileSmem;
+#define EMG_TILE_UPDATE tile_update
+#endif
+
+#if !EMG_FETI_DMMA
 // C[0:mr, 0:mc] -= A[0:mr, 0:K] * B[0:mc, 0:K]^T for one 64x64 tile with 256
 // threads (4 x 4 registers each, rows 4*tx.., columns 4*ty..), for small K
 // where the update is bound by the C read-modify-write and wants many
@@ -340,11 +428,17 @@ __device__ __forceinline__ void tile_update_wide(double* __restrict__ C, int64_t
   }
 }
 
+#endif
+
 // Right-looking update of the remaining pivot columns [k0+nb, npiv), rows >= column.
 __global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0, int32_t k0,
                                                         double* __restrict__ fac) {
+#if EMG_FETI_DMMA
+  __shared__ TileSmemMma sm;
+#else
   __shared__ double As[kKC][kTile + 1];
   __shared__ double Bs[kKC][kTile + 1];
+#endif
   const int32_t k = f0 + blockIdx.y;
   const int32_t np = F.npiv[k];
   if (k0 >= np) return;
@@ -359,14 +453,21 @@ __global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0,
   if (rs + kTile <= cs) return;  // strictly above the diagonal
   const int mc = min(kTile, np - cs), mr = min(kTile, fs - rs);
   double* A = fac + F.fac[k];
+#if EMG_FETI_DMMA
+  static_assert(kMmaThreads == 256, "k_update_pivcols runs 256 threads");
+  tile_update_mma(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
+                  A + cs + static_cast<int64_t>(k0) * fs, fs, nb, sm);
+#else
   tile_update_wide(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
                    A + cs + static_cast<int64_t>(k0) * fs, fs, nb, As, Bs);
+#endif
 }
 
 // Update block: U -= L21 L21^T (lower tiles), K = npiv.
-__global__ void __launch_bounds__(64) k_syrk_update(FrontsDev F, int32_t f0, const double* __restrict__ fac,
-                                                    double* __restrict__ upd) {
-  __shared__ TileSmem sm;
+__global__ void __launch_bounds__(kTileThreads) k_syrk_update(FrontsDev F, int32_t f0,
+                                                              const double* __restrict__ fac,
+                                                              double* __restrict__ upd) {
+  __shared__ TileSmemT sm;
   const int32_t k = f0 + blockIdx.y;
   const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np;
   if (nu <= 0) return;
@@ -382,7 +483,7 @@ __global__ void __launch_bounds__(64) k_syrk_update(FrontsDev F, int32_t f0, con
   const int mr = min(kTile, nu - rs), mc = min(kTile, nu - cs);
   const double* L = fac + F.fac[k];
   double* U = upd + F.upd[k];
-  tile_update(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, sm);
+  EMG_TILE_UPDATE(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, sm);
 }
 
 // --------------------------------------------------- triangular inverse
@@ -407,9 +508,12 @@ __global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t*
   const int32_t w = min(kTB, n - c0);
   const double* L = Lbase + l_off[m];
   double* X = Xbase + x_off[m];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x;
+#if !EMG_FETI_DMMA
+  const int tx = tid & 15, ty = tid >> 4;
   double (*As)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);               // [kKC][kTB+1]
   double (*Bs)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kKC * (kTB + 1));
+#endif
   double (*T)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);                // [kTB][kTB+1]
   double (*Ls)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kTB * (kTB + 1));
   for (int64_t e = tid; e < static_cast<int64_t>(c0) * w; e += blockDim.x) {
@@ -419,6 +523,45 @@ __global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t*
   const int32_t nb = (n + kTB - 1) / kTB;
   for (int32_t I = blockIdx.x; I < nb; ++I) {
     const int32_t r0 = I * kTB, h = min(kTB, n - r0);
+#if EMG_FETI_DMMA
+    // E_IJ - sum_K L_IK X_KJ on the FP64 tensor cores: warp wp owns rows
+    // 8 wp .. 8 wp + 7 of the 64 x 64 block (fragments of mma m8n8k4)
+    {
+      static_assert(kTB == kTile && kKC % 4 == 0 && 2 * kKC * kMmaPad <= 2 * kTB * (kTB + 1),
+                    "staging of the tensor-core product");
+      const int lane = tid & 31, wp = tid >> 5, fr = lane >> 2, fk = lane & 3;
+      double (*As2)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(sm);
+      double (*Bs2)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(sm + kKC * kMmaPad);
+      double acc2[8][2];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) acc2[j][q] = (r0 == c0 && 8 * wp + fr == 8 * j + 2 * fk + q) ? 1.0 : 0.0;
+      for (int32_t k0 = c0; k0 < r0; k0 += kKC) {  // K blocks left of I are full
+        __syncthreads();
+        for (int e = tid; e < kKC * kTB; e += blockDim.x) {
+          const int k = e / kTB, r = e - k * kTB;
+          As2[k][r] = r < h ? L[(r0 + r) + static_cast<int64_t>(k0 + k) * n] : 0.0;
+        }
+        for (int e = tid; e < kKC * kTB; e += blockDim.x) {
+          const int c = e / kKC, k = e - c * kKC;
+          Bs2[k][c] = c < w ? X[(k0 + k) + static_cast<int64_t>(c0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kKC; kk += 4) {
+          const double a = -As2[kk + fk][8 * wp + fr];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dmma_8x8x4(acc2[j], a, Bs2[kk + fk][8 * j + fr]);
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) T[8 * wp + fr][8 * j + 2 * fk + q] = acc2[j][q];
+    }
+#else
     double acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -451,6 +594,7 @@ __global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t*
     for (int x = 0; x < 4; ++x)
 #pragma unroll
       for (int y = 0; y < 4; ++y) T[4 * tx + x][4 * ty + y] = acc[x][y];
+#endif
     for (int e = tid; e < kTB * kTB; e += blockDim.x) {
       const int q = e / kTB, r = e - q * kTB;
       Ls[r][q] = (r < h && q < h && r >= q) ? L[(r0 + r) + static_cast<int64_t>(r0 + q) * n] : 0.0;
@@ -892,9 +1036,10 @@ __global__ void k_face_transpose(FacesDev Fc, const double* __restrict__ X, doub
 }
 
 // C_f = A_f B_f^T for every face (n x n, column-major, same offsets).
-__global__ void __launch_bounds__(64) k_face_gemm_nt(FacesDev Fc, const double* __restrict__ A,
-                                                     const double* __restrict__ B, double* __restrict__ C) {
-  __shared__ TileSmem sm;
+__global__ void __launch_bounds__(kTileThreads) k_face_gemm_nt(FacesDev Fc, const double* __restrict__ A,
+                                                               const double* __restrict__ B,
+                                                               double* __restrict__ C) {
+  __shared__ TileSmemT sm;
   const int32_t f = blockIdx.y;
   const int32_t n = Fc.dim[f];
   const int32_t nt = (n + kTile - 1) / kTile;
@@ -904,7 +1049,7 @@ __global__ void __launch_bounds__(64) k_face_gemm_nt(FacesDev Fc, const double* 
   const int32_t rs = tr * kTile, cs = tc * kTile;
   const int mr = min(kTile, n - rs), mc = min(kTile, n - cs);
   const int64_t o = Fc.off[f];
-  tile_update<true>(C + o + rs + static_cast<int64_t>(cs) * n, n, mr, mc, A + o + rs, n, B + o + cs, n, n, sm);
+  EMG_TILE_UPDATE<true>(C + o + rs + static_cast<int64_t>(cs) * n, n, mr, mc, A + o + rs, n, B + o + cs, n, n, sm);
 }
 
 // w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
@@ -1424,7 +1569,7 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   }
   if (max_nu > 0) {
     const int32_t nt = (max_nu + kTile - 1) / kTile;
-    k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), 64, 0, st>>>(fd, f0, fac_d, upd_d);
+    k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), kTileThreads, 0, st>>>(fd, f0, fac_d, upd_d);
   }
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -1559,9 +1704,9 @@ int FetiDP::setup_deluxe() {
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);
   const int32_t nt = (max_fdim + kTile - 1) / kTile;
   const dim3 g(static_cast<unsigned>(nt * nt), nf);
-  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
-  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
-  k_face_gemm_nt<<<g, 64, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
+  k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
+  k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
+  k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
   // transposes for the row pass, in the buffers of X and X^T (no longer needed)
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
