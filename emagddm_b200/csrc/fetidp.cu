@@ -33,7 +33,10 @@
 namespace emg {
 namespace {
 
-constexpr int kNB = 32;       // panel width of the partial Cholesky
+#ifndef EMG_FETI_NB
+#define EMG_FETI_NB 64
+#endif
+constexpr int kNB = EMG_FETI_NB;  // panel width of the partial Cholesky
 constexpr int kTile = 64;     // output tile of the rank-k updates
 constexpr int kKC = 32;       // k-chunk of the rank-k updates
 constexpr int kTrsmRows = 128;
@@ -184,10 +187,13 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int
 }
 
 // Panel rows below the diagonal block: X L_kk^T = F[i, k0:k0+nb].
+constexpr size_t kTrsmSmem = sizeof(double) * (static_cast<size_t>(kNB) * (kNB + 1) +
+                                               static_cast<size_t>(kNB) * kTrsmRows);
 __global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(FrontsDev F, int32_t f0, int32_t k0,
                                                           double* __restrict__ fac) {
-  __shared__ double D[kNB][kNB + 1];
-  __shared__ double X[kNB][kTrsmRows];
+  extern __shared__ double trsm_sm[];
+  double (*D)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(trsm_sm);
+  double (*X)[kTrsmRows] = reinterpret_cast<double (*)[kTrsmRows]>(trsm_sm + kNB * (kNB + 1));
   const int32_t k = f0 + blockIdx.y;
   const int32_t np = F.npiv[k];
   if (k0 >= np) return;
@@ -1546,6 +1552,9 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
     if (k > f0 && npk[k - f0] > npk[k - f0 - 1]) sorted = false;
   }
   unsigned active = nf;
+  if (kTrsmSmem > 48 * 1024)
+    EMG_CK(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kTrsmSmem)));
   for (int32_t k0 = 0; k0 < max_np; k0 += kNB) {
     int32_t mf = max_f, mnp = max_np;
     if (sorted) {
@@ -1559,7 +1568,7 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
     const int32_t rows = mf - k0 - 1;
     if (rows > 0) {
       const unsigned rb = static_cast<unsigned>((rows + kTrsmRows - 1) / kTrsmRows);
-      k_trsm_panel<<<dim3(rb, active), kTrsmRows, 0, st>>>(fd, f0, k0, fac_d);
+      k_trsm_panel<<<dim3(rb, active), kTrsmRows, kTrsmSmem, st>>>(fd, f0, k0, fac_d);
     }
     const int32_t c0 = k0 + kNB;
     if (c0 < mnp) {
