@@ -207,6 +207,24 @@ __global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(FrontsDev F, int32_t f
   }
   const int32_t i = r0 + threadIdx.x;
   const bool live = i < fs;
+  if (nb == kNB) {
+    // full panel: the row in registers (the same operations in the same order)
+    __syncthreads();
+    double xr[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) xr[c] = live ? A[i + static_cast<int64_t>(k0 + c) * fs] : 0.0;
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) {
+      double v = xr[c];
+#pragma unroll
+      for (int q = 0; q < c; ++q) v -= xr[q] * D[c][q];
+      xr[c] = v / D[c][c];
+    }
+    if (live)
+#pragma unroll
+      for (int c = 0; c < kNB; ++c) A[i + static_cast<int64_t>(k0 + c) * fs] = xr[c];
+    return;
+  }
   for (int c = 0; c < nb; ++c) X[c][threadIdx.x] = live ? A[i + static_cast<int64_t>(k0 + c) * fs] : 0.0;
   __syncthreads();
   for (int c = 0; c < nb; ++c) {
