@@ -690,6 +690,10 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
   });
 }
 
+int emg_test_set_barrier_spins(int32_t spins) {
+  return guarded([&]() -> int { return emg::set_barrier_spins(spins); });
+}
+
 int emg_batch_cg_solve_device(emg_csr A, int32_t n_blocks, const int64_t* block_row_ptr,
                               const double* b_d, double* x_d, const emg_krylov_config* cfg,
                               void* stream, emg_result* results) {

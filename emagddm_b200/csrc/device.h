@@ -94,6 +94,7 @@ int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_confi
                    cudaStream_t st, emg_result* res);
 int csr_history(DevCsr& A, double* out, int32_t cap);
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
+int set_barrier_spins(int32_t spins);
 void free_workspace(KrylovWorkspace* ws);
 void free_batch(BatchPlan* p);
 // Lockstep CG over the diagonal blocks [blocks[k], blocks[k+1]) of A (batch.cu).

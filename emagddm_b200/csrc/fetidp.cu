@@ -1603,16 +1603,18 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
 }
 
 // X = L^-1 for n_mat lower factors stored in fac_d (blocked kernel).
-void FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
-                   double* X) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrtriSmem));
-    attr = true;
-  }
-  if (n_mat == 0 || max_n == 0) return;
+// The shared-memory limit is a per-device attribute of the kernel: set it
+// on every call (cheap), so a solve on another device or thread launches
+// with it too.
+int FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
+                  double* X) {
+  if (n_mat == 0 || max_n == 0) return EMG_SUCCESS;
+  EMG_CK(cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(kTrtriSmem)));
   k_trtri_blk<<<dim3(static_cast<unsigned>((max_n + kTB - 1) / kTB), static_cast<unsigned>(n_mat)), 256, kTrtriSmem,
                 st>>>(n_mat, dim, l_off, x_off, fac_d, X);
+  EMG_CK(cudaGetLastError());
+  return EMG_SUCCESS;
 }
 
 // Multifrontal forward / backward solve of K_rr x = b for ncol right-hand
@@ -1727,7 +1729,8 @@ int FetiDP::setup_deluxe() {
   int rc = factor_range(F + 1, F + 1 + NF);
   if (!rc) rc = check_err("FETI-DP face factorization");
   if (rc) return rc;
-  trtri(NF, max_fdim, fc.dim, fc.fac, fc.off, fX_d);
+  rc = trtri(NF, max_fdim, fc.dim, fc.fac, fc.off, fX_d);
+  if (rc) return rc;
   k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);
   const int32_t nt = (max_fdim + kTile - 1) / kTile;
   const dim3 g(static_cast<unsigned>(nt * nt), nf);
@@ -1814,7 +1817,8 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   if (!rc) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
   if (n_roots > 0) {
-    trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);
+    rc = trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);
+    if (rc) return rc;
     k_mirror_lower<<<dim3(blocks_for(static_cast<int64_t>(max_nD) * max_nD, 256, 256),
                           static_cast<unsigned>(n_roots)), 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d);
   }
@@ -1838,7 +1842,8 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     rc = factor_range(F, F + 1);
     if (!rc) rc = check_err("FETI-DP coarse factorization");
     if (rc) return rc;
-    trtri(1, static_cast<int32_t>(nc), d_cdim, d_cfac, d_czero, Lcc_d);
+    rc = trtri(1, static_cast<int32_t>(nc), d_cdim, d_cfac, d_czero, Lcc_d);
+    if (rc) return rc;
     k_mirror_lower<<<dim3(blocks_for(nc * nc, 256, 256), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d);
   }
   const int64_t ne = P.dual_off[S];

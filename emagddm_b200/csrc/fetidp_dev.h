@@ -152,7 +152,7 @@ struct FetiDP {
   void apply_M(const double* r, double* z, double* part);
   int dot(const double* a, const double* b, int64_t n, int which);
   int setup_deluxe();
-  void trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off, double* X);
+  int trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off, double* X);
   int prepare_rhs(const double* fu);
   int lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel);
   int lambda_fcg(double tol, int32_t max_it, int32_t* iters, double* rel);

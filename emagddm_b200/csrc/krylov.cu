@@ -969,6 +969,9 @@ __global__ void __launch_bounds__(kThreads) k_cg_direction(int64_t n, double* __
 // then ends the solve with EMG_ERR_TIMEOUT.
 constexpr int kFuseThreads = 1024;
 constexpr int kBarrierSpins = 1 << 21;  // x >= 100 ns per poll: well over 0.2 s
+// Polls a waiting block makes before it gives up; kBarrierSpins unless a
+// test lowers it (emg_test_set_barrier_spins) to make the wait run out.
+__device__ int32_t g_barrier_spins = kBarrierSpins;
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
 
@@ -1070,7 +1073,8 @@ __global__ void __launch_bounds__(kFuseThreads, 1) k_cg_update_dir(
     }
   } else if (threadIdx.x == 0) {
     bool ok = false;
-    for (int k = 0; k < kBarrierSpins; ++k) {
+    const int32_t spins = g_barrier_spins;
+    for (int k = 0; k < spins; ++k) {
       if (ld_volatile(&st->gen) != sh_gen) { ok = true; break; }
       __nanosleep(100);
     }
@@ -1943,6 +1947,12 @@ int cg_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg
 int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
                    cudaStream_t st, emg_result* res) {
   return run_solver(A, b, x, cfg, st, res, true);
+}
+
+int set_barrier_spins(int32_t spins) {
+  const int32_t v = spins < 0 ? kBarrierSpins : spins;
+  EMG_CK(cudaMemcpyToSymbol(g_barrier_spins, &v, sizeof(v)));
+  return EMG_SUCCESS;
 }
 
 int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t user, double* ms) {

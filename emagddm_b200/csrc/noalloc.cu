@@ -22,6 +22,10 @@
 // on each device (with that device current) looks the address up with
 // cudaGetSymbolAddress and caches it; that first call should come before any
 // stream capture.
+//
+// Every call blocks the calling host thread until the solve has finished: it
+// synchronizes the stream after the input check and then reads the solver
+// state back every kPollEvery iterations to decide whether to launch more.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -113,7 +117,10 @@ __global__ void k_na_reset(NaState* st, double tol, int32_t max_iter) {
 }
 
 // Input check before any indexed access: offsets monotone and inside
-// [0, nnz], columns inside [0, n).  Flags land in st->pad[0].
+// [0, nnz], columns inside [0, n) and strictly ascending within each row (a
+// merged CSR, the form emg_csr_create_device takes; with it the Jacobi
+// diagonal below is the row's single diagonal entry, as in
+// emg_cg_solve_device).  Flags land in st->pad[0].
 __global__ void k_na_check(int64_t n, int64_t nnz, const int32_t* __restrict__ rp,
                            const int32_t* __restrict__ col, NaState* st) {
   for (int64_t i = tid(); i < n; i += nthreads()) {
@@ -122,8 +129,10 @@ __global__ void k_na_check(int64_t n, int64_t nnz, const int32_t* __restrict__ r
       atomicOr(&st->pad[0], 1);
       continue;
     }
-    for (int32_t k = a; k < b; ++k)
+    for (int32_t k = a; k < b; ++k) {
       if (col[k] < 0 || col[k] >= n) { atomicOr(&st->pad[0], 2); break; }
+      if (k > a && col[k] <= col[k - 1]) { atomicOr(&st->pad[0], 4); break; }
+    }
   }
 }
 
@@ -270,6 +279,9 @@ int cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* c
   double* base = nullptr;
   int rc = scratch_base(&base);
   if (rc) { res->status = rc; return rc; }
+  // From here every early return through EMG_CK is a CUDA error; the paths
+  // that end otherwise overwrite the status.
+  res->status = EMG_ERR_CUDA;
   const Scratch s = carve(base);
   const auto t0 = std::chrono::steady_clock::now();
   k_na_reset<<<1, 32, 0, st>>>(s.st, cfg.tolerance, cfg.max_iterations);
@@ -279,8 +291,10 @@ int cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* c
   EMG_CK(cudaMemcpyAsync(&h, s.st, sizeof(NaState), cudaMemcpyDeviceToHost, st));
   EMG_CK(cudaStreamSynchronize(st));
   if (h.pad[0]) {
-    set_error(h.pad[0] & 1 ? "emg_cg_solve_noalloc: row_ptr is not a valid offset array"
-                           : "emg_cg_solve_noalloc: column index out of range");
+    set_error(h.pad[0] & 1   ? "emg_cg_solve_noalloc: row_ptr is not a valid offset array"
+              : h.pad[0] & 2 ? "emg_cg_solve_noalloc: column index out of range"
+                             : "emg_cg_solve_noalloc: columns of a row are not strictly ascending (unmerged CSR)");
+    res->status = EMG_INVALID_INPUT;
     return EMG_INVALID_INPUT;
   }
   k_na_init<<<kGrid, kThreads, 0, st>>>(n, rp, col, val, b, cfg.preconditioner, x, s);

@@ -405,6 +405,13 @@ int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg,
  * b = ones, each launch bracketed by CUDA events on `stream`. */
 int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms);
 
+/* Test hook (no counterpart in the reference): polls a block of the fused
+ * CG update makes at its grid barrier before giving up (default 2^21, about
+ * 0.2 s or more; a negative value restores it) on the current device.  A
+ * block that gives up ends the solve with EMG_ERR_TIMEOUT instead of
+ * waiting on; tests lower the limit to make that wait run out. */
+int emg_test_set_barrier_spins(int32_t spins);
+
 /* Solver storage of A (SELL-32-sigma copy built at the first solve or SpMV):
  * stored slots including padding and number of 32-row slices; -1 before the
  * first solve. */
@@ -430,13 +437,17 @@ int emg_batch_cg_solve_device(emg_csr A, int32_t n_blocks, const int64_t* block_
  * CUDA allocator after start-up (cudaMalloc/cudaFree synchronize the device
  * and take unbounded time).  Same iteration, stopping and failure rules as
  * emg_cg_solve_device, on a caller-owned merged CSR in device memory
- * (row_ptr_d n+1, col_d/val_d nnz; b_d, x_d n).  Allocates nothing: the work
+ * (row_ptr_d n+1, col_d/val_d nnz, columns strictly ascending within each
+ * row; b_d, x_d n; an unmerged CSR returns EMG_INVALID_INPUT).  Allocates
+ * nothing: the work
  * vectors live in a fixed scratch array inside the library (about 10 MiB,
  * held by every GPU that loads the library until exit), so n is limited to
  * 262,144 rows; larger n returns EMG_INVALID_INPUT.  The first call on a
  * device looks up the scratch address and should come before any stream
- * capture.  Calls share the scratch: calls that overlap on the GPU (other
- * streams or threads) race.  solve_time_ms is host wall time. */
+ * capture.  Every call blocks the host until the solve ends: it synchronizes
+ * the stream and reads the solver state back every 16 iterations.  Calls
+ * share the scratch: calls that overlap on the GPU (other streams or
+ * threads) race.  solve_time_ms is host wall time. */
 int emg_cg_solve_noalloc(int64_t n, int64_t nnz, const int32_t* row_ptr_d, const int32_t* col_d,
                          const double* val_d, const double* b_d, double* x_d,
                          const emg_krylov_config* cfg, void* stream, emg_result* out);

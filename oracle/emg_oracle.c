@@ -845,8 +845,21 @@ static void jacobi_inverse(int64_t n, const int64_t* rp, const int32_t* col,
 int orc_pcg(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
             const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
             int32_t* iterations, double* residual_norm) {
+  return orc_pcg_snap(n, rp, col, val, b, x, tol, max_iter, precond, iterations, residual_norm,
+                      0.0, NULL, NULL);
+}
+
+/* orc_pcg with a snapshot: the first iterate whose relative residual is
+ * below snap_tol is copied to x_snap (its iteration to *snap_iter, -1 if
+ * never), so one run to a tight tolerance also gives the iterate at which a
+ * solve to snap_tol stops (same sequence of iterates). */
+int orc_pcg_snap(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
+                 const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
+                 int32_t* iterations, double* residual_norm, double snap_tol, double* x_snap,
+                 int32_t* snap_iter) {
   *iterations = 0;
   *residual_norm = 0.0;
+  if (snap_iter) *snap_iter = -1;
   if (n <= 0) return ORC_INVALID_INPUT;
   double* r = (double*)malloc((size_t)n * sizeof(double));
   double* z = (double*)malloc((size_t)n * sizeof(double));
@@ -879,6 +892,10 @@ int orc_pcg(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
     }
     double rz_new = vdot(n, r, z);
     res = sqrt(vdot(n, r, r)) / bnorm;
+    if (x_snap && snap_iter && *snap_iter < 0 && res < snap_tol) {
+      memcpy(x_snap, x, (size_t)n * sizeof(double));
+      *snap_iter = it;
+    }
     if (res < tol) { status = ORC_SUCCESS; break; }
     if (it > 10 && res > prev * 1000.0) { status = ORC_DIVERGED; break; }
     double beta = rz_new / rz;

@@ -109,6 +109,14 @@ int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col,
             int32_t max_iter, int32_t precond, int32_t* iterations,
             double* residual_norm);
 
+/* orc_pcg that also copies the first iterate whose relative residual is
+ * below snap_tol into x_snap (its iteration into *snap_iter, -1 if none). */
+int orc_pcg_snap(int64_t n, const int64_t* row_ptr, const int32_t* col,
+                 const double* val, const double* b, double* x, double tol,
+                 int32_t max_iter, int32_t precond, int32_t* iterations,
+                 double* residual_norm, double snap_tol, double* x_snap,
+                 int32_t* snap_iter);
+
 /* BiCGSTABSolver::solve_no_preconditioner / solve_with_jacobi
  * (src/numeric/iterative_solvers.cpp:869-1118). */
 int orc_bicgstab(int64_t n, const int64_t* row_ptr, const int32_t* col,

@@ -58,6 +58,7 @@ def lib():
         for f in (L.orc_pcg, L.orc_bicgstab):
             f.argtypes = [C.c_int64, I64P, I32P, F64P, F64P, F64P, C.c_double, C.c_int32,
                           C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.orc_pcg_snap.argtypes = L.orc_pcg.argtypes + [C.c_double, F64P, C.POINTER(C.c_int32)]
         L.orc_num_threads.restype = C.c_int
         L.orc_edge_ids_typed.argtypes = [C.c_int32, C.c_int64, I32P, I32P, I32P, C.POINTER(C.c_int64)]
         L.orc_dof_build_typed.argtypes = [C.c_int32] + L.orc_dof_build.argtypes
@@ -265,6 +266,17 @@ def _krylov(fn, rp, col, val, b, tol, max_iter, precond):
 
 def pcg(rp, col, val, b, tol=1e-8, max_iter=1000, precond=1):
     return _krylov(lib().orc_pcg, rp, col, val, b, tol, max_iter, precond)
+
+
+def pcg_snap(rp, col, val, b, tol=1e-12, snap_tol=1e-8, max_iter=1000, precond=1):
+    """pcg to `tol` that also returns the iterate at which a solve to
+    `snap_tol` stops: (x, status, iterations, residual, x_snap, snap_iter)."""
+    n = rp.size - 1
+    x, xs = np.empty(n), np.empty(n)
+    it, res, sit = C.c_int32(), C.c_double(), C.c_int32()
+    st = lib().orc_pcg_snap(n, rp, col, val, np.ascontiguousarray(b, np.float64), x, tol, max_iter, precond,
+                            C.byref(it), C.byref(res), snap_tol, xs, C.byref(sit))
+    return x, st, it.value, res.value, xs, sit.value
 
 
 def bicgstab(rp, col, val, b, tol=1e-8, max_iter=1000, precond=1):

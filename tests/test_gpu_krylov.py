@@ -77,6 +77,34 @@ def test_cg_tight_solution_within_1e8_of_oracle():
     assert rel(x, xo) <= 1e-8
 
 
+def test_config_plain_small_16_to_1e10():
+    """The 'plain method, small' configuration exactly: 16^3 x 6 tets, nu = 1,
+    J_z in [0.375, 0.625]^3, ref tree gauge, GPU assembly + Jacobi-PCG to
+    1e-10 through emg_system_solve, against the oracle's own assembly and
+    solve (iterations within the usual margin, solution within 1e-8 of the
+    oracle's 1e-12 solution)."""
+    import ctypes as C
+    m = mesh.plain_small(16)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    n = int(l2g.max()) + 1
+    assert n == 22320 and m.n_tets == 24576
+    s = System(m, l2g)
+    rp, col, kv, _, rhs = oracle_system(m, l2g)
+    cfg = _abi.KrylovConfig(1e-10, 20000, _abi.PRECOND_JACOBI)
+    out = _abi.Result()
+    x = np.empty(n)
+    rc = lib().emg_system_solve(s.h, 0, C.byref(cfg), _abi.ptr(x), 0, None, C.byref(out))
+    assert rc == out.status == 0, lib().emg_last_error()
+    xo, st, it, res, xt, _ = O.pcg_snap(rp, col, kv, rhs, tol=1e-12, snap_tol=1e-10, max_iter=50000, precond=1)
+    _, st10, it10, _ = O.pcg(rp, col, kv, rhs, tol=1e-10, max_iter=50000, precond=1)
+    assert st == st10 == 0
+    assert abs(out.iterations - it10) <= max(3, 0.15 * it10)
+    assert out.residual_norm < 1e-10
+    assert np.linalg.norm(rhs - O.spmv(rp, col, kv, x)) / np.linalg.norm(rhs) <= 2e-10
+    assert rel(x, xo) <= 1e-8
+    assert rel(x, xt) <= 1e-8  # the oracle's own iterate at 1e-10 (same algorithm)
+
+
 def test_zero_rhs_and_iteration_limits():
     m = mesh.plain_small(4)
     l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]

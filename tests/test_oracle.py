@@ -161,3 +161,15 @@ def test_partial_dirichlet_and_unknown_pairs():
     r = R.dof_build(m.n_nodes, m.tets, np.zeros((0, 2), np.int32), gauge=True)
     o = O.dof_build(m.tets, np.zeros((0, 2), np.int32), gauge=O.GAUGE_REF)
     np.testing.assert_array_equal(r["l2g"], o["l2g"])
+
+
+def test_pcg_snapshot_is_the_iterate_of_the_looser_solve():
+    m = mesh.plain_scale(8)
+    l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
+    rp, col, kv, _, rhs = O.assemble(m, l2g, int(l2g.max()) + 1)
+    x8, st8, it8, _ = O.pcg(rp, col, kv, rhs, tol=1e-8, max_iter=5000)
+    x, st, it, res, xs, sit = O.pcg_snap(rp, col, kv, rhs, tol=1e-12, snap_tol=1e-8, max_iter=5000)
+    assert st == st8 == 0 and sit == it8 and it > it8 and res < 1e-12
+    np.testing.assert_array_equal(xs, x8)
+    _, _, _, _, _, never = O.pcg_snap(rp, col, kv, rhs, tol=1e-6, snap_tol=1e-9, max_iter=5000)
+    assert never == -1

@@ -82,5 +82,16 @@ def test_noalloc_rejects_oversize_and_bad_input():
     bad[5] = n + 7  # out-of-range column: rejected before any indexed access
     rc = lib().emg_cg_solve_noalloc(n, nnz, _p(t["rp"]), _p(bad), _p(t["val"]), _p(t["b"]), _p(x),
                                     C.byref(cfg), None, C.byref(r))
-    assert rc == _abi.EMG_INVALID_INPUT
+    assert rc == r.status == _abi.EMG_INVALID_INPUT
     assert b"column" in lib().emg_last_error()
+    # a row whose columns are swapped (unmerged form): rejected, since the
+    # Jacobi diagonal is defined on a merged CSR
+    rp = t["rp"].cpu().numpy()
+    row = int(np.argmax(np.diff(rp) >= 2))
+    k = int(rp[row])
+    swapped = t["col"].clone()
+    swapped[k], swapped[k + 1] = t["col"][k + 1], t["col"][k]
+    rc = lib().emg_cg_solve_noalloc(n, nnz, _p(t["rp"]), _p(swapped), _p(t["val"]), _p(t["b"]), _p(x),
+                                    C.byref(cfg), None, C.byref(r))
+    assert rc == r.status == _abi.EMG_INVALID_INPUT
+    assert b"ascending" in lib().emg_last_error()
