@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--eval-fields", type=int, default=50, help="learned64: held-out fields (seeds 2000+)")
     ap.add_argument("--feti-precond", type=int, default=2,
                     help="fetidp64: 2 deluxe (FP64 blocks), 3 deluxe with FP32 blocks (mixed precision)")
+    ap.add_argument("--feti-variants", default=",".join(["fp64", "fp32_precond", "tf32_factor",
+                                                           "tf32_factor_fp32_precond"]),
+                    help="cube64 north-star comparison: FETI-DP variants to time (comma-separated)")
+    ap.add_argument("--mixed", action="store_true",
+                    help="fetidp64: mixed-precision factor (TF32 tensor-core contractions, FP64 refinement)")
     ap.add_argument("--instances", type=int, default=512, help="batch512: number of instances")
     ap.add_argument("--no-oracle", action="store_true",
                     help="cube64: skip the full-size FP64 oracle check after the timed region")
@@ -601,9 +606,14 @@ def run_batch(args, rank, world, local_rank):
     }
 
 
+FLAG_FACTOR_TF32 = 16
 FETI_VARIANTS = {
     "fp64": ("FP64 factor, deluxe-scaled Dirichlet preconditioner with FP64 blocks", 2, 0),
     "fp32_precond": ("FP64 factor, deluxe preconditioner blocks read in FP32", 3, 0),
+    "tf32_factor": ("mixed-precision factor: update-block and pivot-column contractions on the tcgen05 tensor "
+                    "cores (two-term TF32, FP32 accumulation), FP64 refinement on the true residual",
+                    2, FLAG_FACTOR_TF32),
+    "tf32_factor_fp32_precond": ("mixed-precision factor and FP32 preconditioner blocks", 3, FLAG_FACTOR_TF32),
 }
 
 
@@ -632,10 +642,22 @@ def fetidp_variants(fd, names, steps, warmup, stream, dev):
             if k >= warmup:
                 per.append(e0.elapsed_time(e1))
                 st = fd.stats()
+        its = max(int(st["iterations"]), 1)
+        # dense blocks read per multiplier iteration: L^-1 (lower, then upper
+        # mirror: the whole n_D^2 block once) and S_DD (whole block; FP32
+        # copies with the FP32 preconditioner)
+        nb = fd.info()["dual_block_doubles"] * (8 + (4 if precond == 3 else 8))
+        peak, _ = measured_peak()
+        per_it = st["lambda_ms"] / its
         res[name] = {"what": what, "ms": statistics.mean(per), "ms_steps": [round(v, 3) for v in per],
                      "factor_ms": st["factor_ms"], "solve_ms": st["solve_ms"],
                      "lambda_iterations": int(st["iterations"]), "passes": int(st["passes"]),
-                     "true_residual": st["residual"], "_x": x}
+                     "true_residual": st["residual"],
+                     "solve_phases_ms": {"lambda_iterations": st["lambda_ms"], "front_solves": st["fronts_ms"]},
+                     "lambda_iteration": {"ms": per_it, "dense_block_bytes": nb,
+                                          "achieved_gbs": nb / (per_it * 1e-3) / 1e9,
+                                          "frac_of_measured_hbm": nb / (per_it * 1e-3) / 1e9 / peak},
+                     "_x": x}
     return res
 
 
@@ -691,7 +713,10 @@ def north_star(args, local_rank):
     fd = fetidp.FetiDP(m, part, 64)
     setup_ms = (time.perf_counter() - t0) * 1e3
     info = fd.info()
-    var = fetidp_variants(fd, list(FETI_VARIANTS), steps=3, warmup=2, stream=stream, dev=dev)
+    names = [v for v in args.feti_variants.split(",") if v in FETI_VARIANTS]
+    if "fp64" not in names:
+        names.insert(0, "fp64")
+    var = fetidp_variants(fd, names, steps=3, warmup=2, stream=stream, dev=dev)
     x_feti = var["fp64"].pop("_x")
     for v in var.values():
         v.pop("_x", None)
@@ -738,7 +763,8 @@ def run_fetidp(args, rank, world, local_rank):
     setup_ms = (time.perf_counter() - t0) * 1e3
     info = fd.info()
     stream = torch.cuda.current_stream(dev)
-    name = {2: "fp64", 3: "fp32_precond"}.get(args.feti_precond)
+    name = {(2, 0): "fp64", (3, 0): "fp32_precond", (2, 1): "tf32_factor",
+            (3, 1): "tf32_factor_fp32_precond"}.get((args.feti_precond, int(args.mixed)))
     if name is None:
         raise SystemExit(f"--feti-precond {args.feti_precond}: use 2 or 3")
     with Clocks(local_rank) as clk:

@@ -93,6 +93,8 @@ SIGNATURES = {
                           C.POINTER(Result)], C.c_int),
     "emg_cg_kernel_times": ([H, C.c_int32, VP, VP], C.c_int),
     "emg_test_set_barrier_spins": ([C.c_int32], C.c_int),
+    "emg_test_tc_tile": ([C.c_int32, C.c_int32, C.c_int32, VP, C.c_int64, VP, C.c_int64, VP, C.c_int64, VP],
+                         C.c_int),
     "emg_system_combine": ([H, C.c_double, C.c_double, C.POINTER(H)], C.c_int),
     "emg_batch_cg_solve_device": ([H, C.c_int32, VP, VP, VP, C.POINTER(KrylovConfig), VP, VP], C.c_int),
     "emg_cg_solve_noalloc": ([C.c_int64, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(KrylovConfig), VP,

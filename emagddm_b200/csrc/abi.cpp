@@ -690,6 +690,11 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
   });
 }
 
+int emg_test_tc_tile(int32_t mr, int32_t mc, int32_t k, const double* a_d, int64_t lda, const double* b_d,
+                     int64_t ldb, double* c_d, int64_t ldc, void* stream) {
+  return guarded([&]() -> int { return emg::tc_tile_test(mr, mc, k, a_d, lda, b_d, ldb, c_d, ldc, as_stream(stream)); });
+}
+
 int emg_test_set_barrier_spins(int32_t spins) {
   return guarded([&]() -> int { return emg::set_barrier_spins(spins); });
 }
@@ -817,9 +822,9 @@ int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info) {
 int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats) {
   if (!fd || (!stats && n_stats > 0)) { set_error("null argument"); return EMG_INVALID_INPUT; }
   const emg::FetiStats& s = fd->fd.stats;
-  const double v[6] = {s.factor_ms, s.solve_ms, static_cast<double>(s.iterations), s.lambda_residual, s.residual,
-                       static_cast<double>(s.refinements)};
-  for (int32_t i = 0; i < n_stats && i < 6; ++i) stats[i] = v[i];
+  const double v[8] = {s.factor_ms, s.solve_ms, static_cast<double>(s.iterations), s.lambda_residual, s.residual,
+                       static_cast<double>(s.refinements), s.lambda_ms, s.fronts_ms};
+  for (int32_t i = 0; i < n_stats && i < 8; ++i) stats[i] = v[i];
   return EMG_SUCCESS;
 }
 

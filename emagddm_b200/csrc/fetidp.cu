@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -28,6 +29,7 @@
 #include "device.h"
 #include "fetidp.h"
 #include "fetidp_dev.h"
+#include "tc_tile.cuh"
 #include "trace.h"
 
 namespace emg {
@@ -42,7 +44,7 @@ constexpr int kKC = 32;       // k-chunk of the rank-k updates
 constexpr int kTrsmRows = 128;
 constexpr double kMinInnerTol = 1e-12;  // floor of a pass's multiplier tolerance
 
-enum : int32_t { kErrPivot = 1, kErrAsm = 2 };
+enum : int32_t { kErrPivot = 1, kErrAsm = 2, kErrTc = 4 };
 
 #define EMG_CK_VOID(call)                                                         \
   do {                                                                            \
@@ -510,6 +512,67 @@ __global__ void __launch_bounds__(kTileThreads) k_syrk_update(FrontsDev F, int32
   EMG_TILE_UPDATE(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np, sm);
 }
 
+// Mixed-precision variants of the two contractions of the factor (the
+// update block and the pivot-column update) on the 5th-generation tensor
+// cores: 128 x 128 tiles, FP64 operands split into two TF32 terms, FP32
+// accumulation in tensor memory (tc_tile.cuh).  Subdomain fronts only; the
+// coarse matrix and the deluxe face sums keep the FP64 kernels.
+__global__ void __launch_bounds__(tc::kThreads) k_syrk_update_tc(FrontsDev F, int32_t f0,
+                                                                 const double* __restrict__ fac,
+                                                                 double* __restrict__ upd, int32_t* __restrict__ err) {
+  extern __shared__ uint8_t tc_dyn[];
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np;
+  if (nu <= 0 || np <= 0) return;
+  const int32_t nt = (nu + tc::kM - 1) / tc::kM;
+  const int32_t t = blockIdx.x;
+  if (t >= nt * (nt + 1) / 2) return;
+  int32_t tr = static_cast<int32_t>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((tr + 1) * (tr + 2) / 2 <= t) ++tr;
+  while (tr * (tr + 1) / 2 > t) --tr;
+  const int32_t tcol = t - tr * (tr + 1) / 2;
+  const int32_t rs = tr * tc::kM, cs = tcol * tc::kN;
+  const int mr = min(tc::kM, nu - rs), mc = min(tc::kN, nu - cs);
+  const double* L = fac + F.fac[k];
+  double* U = upd + F.upd[k];
+  if (!tc::tile_update(U + rs + static_cast<int64_t>(cs) * nu, nu, mr, mc, L + np + rs, fs, L + np + cs, fs, np,
+                       tc_dyn) &&
+      threadIdx.x == 0)
+    atomicOr(err, kErrTc);
+}
+
+__global__ void __launch_bounds__(tc::kThreads) k_update_pivcols_tc(FrontsDev F, int32_t f0, int32_t k0,
+                                                                    double* __restrict__ fac,
+                                                                    int32_t* __restrict__ err) {
+  extern __shared__ uint8_t tc_dyn[];
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k];
+  if (k0 >= np) return;
+  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
+  const int32_t c0 = k0 + nb;
+  if (c0 >= np) return;
+  const int32_t nct = (np - c0 + tc::kN - 1) / tc::kN, nrt = (fs - c0 + tc::kM - 1) / tc::kM;
+  const int32_t t = blockIdx.x;
+  if (t >= nct * nrt) return;
+  const int32_t tcol = t % nct, tr = t / nct;
+  const int32_t cs = c0 + tcol * tc::kN, rs = c0 + tr * tc::kM;
+  if (rs + tc::kM <= cs) return;  // strictly above the diagonal
+  const int mc = min(tc::kN, np - cs), mr = min(tc::kM, fs - rs);
+  double* A = fac + F.fac[k];
+  if (!tc::tile_update(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs,
+                       fs, A + cs + static_cast<int64_t>(k0) * fs, fs, nb, tc_dyn) &&
+      threadIdx.x == 0)
+    atomicOr(err, kErrTc);
+}
+
+// One tile C -= A B^T (device arrays) for the tile's own test.
+__global__ void __launch_bounds__(tc::kThreads) k_tc_tile_test(double* C, int64_t ldc, int mr, int mc,
+                                                               const double* A, int64_t lda, const double* B,
+                                                               int64_t ldb, int K, int32_t* err) {
+  extern __shared__ uint8_t tc_dyn[];
+  if (!tc::tile_update(C, ldc, mr, mc, A, lda, B, ldb, K, tc_dyn) && threadIdx.x == 0) atomicOr(err, kErrTc);
+}
+
 // --------------------------------------------------- triangular inverse
 
 // Blocked X = L^-1: one CTA per 64-column block J of one matrix; row blocks
@@ -824,6 +887,11 @@ __global__ void k_mirror_lower(int32_t n_mat, const int32_t* __restrict__ dim, c
 
 // Column-dot mat-vec of dense blocks: y_c = sum over rows r in the range of
 // column c of M[r, c] w_r; range 0: r <= c, 1: r >= c, 2: all rows.
+// y[c] = column c of block m (rows lo..hi) . w, one warp per column.  range
+// 0: rows 0..c (the mirrored upper part of L^-1: y = L^-1 w), 1: rows c..n-1
+// (y = L^-T w), 2: all rows.  The column is read with 16-byte loads (after a
+// scalar head up to the first aligned element), four vectors in flight per
+// lane; w, which every column of the block reads, stays in L1/L2.
 template <class T>
 __global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int32_t* __restrict__ dim,
                                                        const int64_t* __restrict__ m_off,
@@ -831,23 +899,50 @@ __global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int3
                                                        const int64_t* __restrict__ v_off,
                                                        const double* __restrict__ w, double* __restrict__ y,
                                                        int range) {
+  constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
+  using Vec = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
   const int32_t m = blockIdx.y;
   if (m >= n_mat) return;
   const int32_t n = dim[m];
   const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (c >= n) return;
   const int lane = threadIdx.x & 31;
-  const T* Mc = M + m_off[m] + static_cast<int64_t>(c) * n;
+  const int64_t col0 = m_off[m] + static_cast<int64_t>(c) * n;  // element index of the column start
+  const T* Mc = M + col0;
   const double* wm = w + v_off[m];
   const int32_t lo = range == 1 ? c : 0, hi = range == 0 ? c + 1 : n;
-  double a0 = 0.0, a1 = 0.0;
-  int32_t i = lo + lane;
-  for (; i + 32 < hi; i += 64) {
-    a0 = fma(static_cast<double>(Mc[i]), wm[i], a0);
-    a1 = fma(static_cast<double>(Mc[i + 32]), wm[i + 32], a1);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  // scalar head: up to the first element on a 16-byte boundary
+  const int32_t head = min(hi, lo + static_cast<int32_t>((V - ((col0 + lo) % V)) % V));
+  if (lo + lane < head) a0 = fma(static_cast<double>(Mc[lo + lane]), wm[lo + lane], a0);
+  const int32_t nv = (hi - head) / V;  // whole vectors
+  const Vec* Mv = reinterpret_cast<const Vec*>(Mc + head);
+  const double* wv = wm + head;
+  int32_t v = lane;
+  for (; v + 96 < nv; v += 128) {
+    const Vec x0 = Mv[v], x1 = Mv[v + 32], x2 = Mv[v + 64], x3 = Mv[v + 96];
+    const T* e0 = reinterpret_cast<const T*>(&x0);
+    const T* e1 = reinterpret_cast<const T*>(&x1);
+    const T* e2 = reinterpret_cast<const T*>(&x2);
+    const T* e3 = reinterpret_cast<const T*>(&x3);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      a0 = fma(static_cast<double>(e0[j]), wv[V * v + j], a0);
+      a1 = fma(static_cast<double>(e1[j]), wv[V * (v + 32) + j], a1);
+      a2 = fma(static_cast<double>(e2[j]), wv[V * (v + 64) + j], a2);
+      a3 = fma(static_cast<double>(e3[j]), wv[V * (v + 96) + j], a3);
+    }
   }
-  if (i < hi) a0 = fma(static_cast<double>(Mc[i]), wm[i], a0);
-  const double acc = warp_sum(a0 + a1);
+  for (; v < nv; v += 32) {
+    const Vec x0 = Mv[v];
+    const T* e0 = reinterpret_cast<const T*>(&x0);
+#pragma unroll
+    for (int j = 0; j < V; ++j) a0 = fma(static_cast<double>(e0[j]), wv[V * v + j], a0);
+  }
+  // scalar tail
+  const int32_t t0 = head + V * nv;
+  if (t0 + lane < hi) a1 = fma(static_cast<double>(Mc[t0 + lane]), wm[t0 + lane], a1);
+  const double acc = warp_sum((a0 + a1) + (a2 + a3));
   if (lane == 0) y[v_off[m] + c] = acc;
 }
 
@@ -1174,6 +1269,9 @@ __global__ void k_to_f32(int64_t n, const double* __restrict__ x, float* __restr
 
 struct LamState {
   double rz, rz_old, pq, rr, rr0, alpha, beta;
+  // device-side loop of the multiplier iteration (k_lam_control)
+  double tol;
+  int32_t it, max_it, done, status, loops, loop_limit;
 };
 
 __global__ void __launch_bounds__(256) k_dot_part(int64_t n, const double* __restrict__ a,
@@ -1210,6 +1308,34 @@ __global__ void k_lam_update(int64_t n, const LamState* __restrict__ st, double*
     x[i] = fma(a, p[i], x[i]);
     r[i] = fma(-a, q[i], r[i]);
   }
+}
+
+__global__ void k_lam_loop_init(LamState* st, double tol, int32_t max_it) {
+  if (threadIdx.x != 0) return;
+  st->tol = tol;
+  st->max_it = max_it;
+  st->it = 0;
+  st->done = 0;
+  st->status = EMG_MAX_ITER_REACHED;
+  st->loops = 0;
+  st->loop_limit = max_it + 2;
+}
+
+// Last node of the multiplier loop's body: the host loop's tests (breakdown
+// or non-finite residual, convergence, iteration limit) on the device.  The
+// body-count bound does not depend on the solver state, so the loop ends
+// even if that state were wrong.
+__global__ void k_lam_control(LamState* st, cudaGraphConditionalHandle handle) {
+  if (threadIdx.x != 0) return;
+  const int32_t it = st->it + 1;
+  st->it = it;
+  const double rr = st->rr;
+  if (!(st->pq > 0.0) || !isfinite(rr)) { st->status = EMG_NUMERICAL_ERROR; st->done = 1; }
+  else if (sqrt(fmax(rr, 0.0) / st->rr0) < st->tol) { st->status = EMG_SUCCESS; st->done = 1; }
+  else if (it >= st->max_it) { st->status = EMG_MAX_ITER_REACHED; st->done = 1; }
+  const int32_t loops = st->loops + 1;
+  st->loops = loops;
+  cudaGraphSetConditional(handle, (!st->done && loops < st->loop_limit) ? 1u : 0u);
 }
 
 __global__ void k_lam_direction(int64_t n, const LamState* __restrict__ st, double* __restrict__ p,
@@ -1297,6 +1423,9 @@ void FetiDP::release() {
   free_learn(learn);
   learn = nullptr;
   if (!dev.empty()) cudaStreamSynchronize(st);
+  for (cudaGraphExec_t& g : lam_exec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (cap_st) { cudaStreamDestroy(cap_st); cap_st = nullptr; }
   for (void* p : dev) cudaFree(p);
   dev.clear();
 }
@@ -1538,6 +1667,10 @@ int FetiDP::check_err(const char* where) {
     set_error(std::string(where) + ": non-positive pivot (a subdomain matrix is not positive definite)");
     return EMG_NUMERICAL_ERROR;
   }
+  if (e & kErrTc) {
+    set_error(std::string(where) + ": a tensor-core tile gave up waiting for its MMAs");
+    return EMG_ERR_TIMEOUT;
+  }
   if (e) {
     set_error(std::string(where) + ": front assembly lookup failed");
     return EMG_ERR_INTERNAL;
@@ -1573,6 +1706,14 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   if (kTrsmSmem > 48 * 1024)
     EMG_CK(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kTrsmSmem)));
+  // mixed precision: the subdomain fronts' contractions on the TF32 tensor cores
+  const bool tc_here = tc_factor && f1 <= F;
+  if (tc_here) {
+    EMG_CK(cudaFuncSetAttribute(k_syrk_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc::kSmemBytes)));
+    EMG_CK(cudaFuncSetAttribute(k_update_pivcols_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc::kSmemBytes)));
+  }
   for (int32_t k0 = 0; k0 < max_np; k0 += kNB) {
     int32_t mf = max_f, mnp = max_np;
     if (sorted) {
@@ -1589,12 +1730,20 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
       k_trsm_panel<<<dim3(rb, active), kTrsmRows, kTrsmSmem, st>>>(fd, f0, k0, fac_d);
     }
     const int32_t c0 = k0 + kNB;
-    if (c0 < mnp) {
+    if (c0 < mnp && tc_here) {
+      const int32_t nct = (mnp - c0 + tc::kN - 1) / tc::kN, nrt = (mf - c0 + tc::kM - 1) / tc::kM;
+      k_update_pivcols_tc<<<dim3(static_cast<unsigned>(nct * nrt), active), tc::kThreads, tc::kSmemBytes, st>>>(
+          fd, f0, k0, fac_d, err_d);
+    } else if (c0 < mnp) {
       const int32_t nct = (mnp - c0 + kTile - 1) / kTile, nrt = (mf - c0 + kTile - 1) / kTile;
       k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), active), 256, 0, st>>>(fd, f0, k0, fac_d);
     }
   }
-  if (max_nu > 0) {
+  if (max_nu > 0 && tc_here) {
+    const int32_t nt = (max_nu + tc::kM - 1) / tc::kM;
+    k_syrk_update_tc<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), tc::kThreads, tc::kSmemBytes, st>>>(
+        fd, f0, fac_d, upd_d, err_d);
+  } else if (max_nu > 0) {
     const int32_t nt = (max_nu + kTile - 1) / kTile;
     k_syrk_update<<<dim3(static_cast<unsigned>(nt * (nt + 1) / 2), nf), kTileThreads, 0, st>>>(fd, f0, fac_d, upd_d);
   }
@@ -1774,6 +1923,8 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
                    int32_t flags) {
   TraceScope tr("fetidp.factor");
   factored = false;
+  tc_factor = (flags & EMG_FLAG_FACTOR_TF32) != 0;
+  flags &= ~EMG_FLAG_FACTOR_TF32;
   const FetiPlan& P = plan;
   const int32_t S = P.n_parts;
   const int32_t F = static_cast<int32_t>(P.fronts.size());
@@ -1893,6 +2044,73 @@ int FetiDP::prepare_rhs(const double* fu) {
   return EMG_SUCCESS;
 }
 
+// One multiplier-CG iteration after the start (q = F p, alpha, lambda and r,
+// r.r, z = M r, beta, p), every scalar through the device state.
+void FetiDP::lambda_body(void* state) {
+  const int64_t nl = plan.n_lambda;
+  LamState* sd = static_cast<LamState*>(state);
+  apply_F(p_d, q_d, part_d);
+  k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 0);
+  k_lam_update<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, lam_d, r_d, p_d, q_d);
+  dot(r_d, r_d, nl, 2);
+  apply_M(r_d, z_d, part_d);
+  k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 1);
+  k_lam_direction<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, p_d, z_d, 0);
+}
+
+// The multiplier loop as one graph: a conditional while-node whose body is
+// lambda_body + k_lam_control, captured once per preconditioner (the
+// buffers it names live as long as the solver).  Null where conditional
+// nodes or the capture are unavailable (the host loop runs instead), or when
+// EMG_FETI_GRAPH=0.
+cudaGraphExec_t FetiDP::lambda_loop_graph() {
+  if (precond < 0 || precond > 3) return nullptr;
+  static const bool off = [] {
+    const char* e = std::getenv("EMG_FETI_GRAPH");
+    return e && e[0] == '0';
+  }();
+  if (off || graph_failed) return nullptr;
+  if (lam_exec[precond]) return lam_exec[precond];
+  if (!cap_st && cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    graph_failed = true;
+    return nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  if (cudaGraphCreate(&graph, 0) != cudaSuccess) { cudaGetLastError(); graph_failed = true; return nullptr; }
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const cudaStream_t saved = st;
+    st = cap_st;
+    e = cudaStreamBeginCaptureToGraph(cap_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      lambda_body(state_d);
+      k_lam_control<<<1, 32, 0, st>>>(static_cast<LamState*>(state_d), handle);
+      e = cudaStreamEndCapture(cap_st, &body);
+    }
+    st = saved;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    graph_failed = true;
+    return nullptr;
+  }
+  lam_exec[precond] = exec;
+  return exec;
+}
+
 // lambda-PCG on rhs_d; returns the status, sets *iters and *rel.
 int FetiDP::lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel) {
   if (precond == 4) return lambda_fcg(tol, max_it, iters, rel);
@@ -1912,16 +2130,21 @@ int FetiDP::lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel) 
   EMG_CK(cudaStreamSynchronize(st));
   const double rr0 = hs.rr0;
   if (!(rr0 > 0.0)) return EMG_SUCCESS;
+  // the whole loop on the device: one graph launch, one read-back
+  cudaGraphExec_t loop = max_it > 0 ? lambda_loop_graph() : nullptr;
+  if (loop) {
+    k_lam_loop_init<<<1, 32, 0, st>>>(sd, tol, max_it);
+    EMG_CK(cudaGraphLaunch(loop, st));
+    EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaStreamSynchronize(st));
+    *iters = std::min(hs.it, max_it);
+    *rel = std::sqrt(std::max(hs.rr, 0.0) / rr0);
+    return hs.status;
+  }
   int status = EMG_MAX_ITER_REACHED;
   int32_t it = 1;
   for (; it <= max_it; ++it) {
-    apply_F(p_d, q_d, part_d);
-    k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 0);
-    k_lam_update<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, lam_d, r_d, p_d, q_d);
-    dot(r_d, r_d, nl, 2);
-    apply_M(r_d, z_d, part_d);
-    k_reduce_state<<<1, 1024, 0, st>>>(part_d, kParts, sd, 1);
-    k_lam_direction<<<blocks_for(nl, 256), 256, 0, st>>>(nl, sd, p_d, z_d, 0);
+    lambda_body(sd);
     EMG_CK(cudaMemcpyAsync(&hs, sd, sizeof(LamState), cudaMemcpyDeviceToHost, st));
     EMG_CK(cudaStreamSynchronize(st));
     *rel = std::sqrt(std::max(hs.rr, 0.0) / rr0);
@@ -2118,23 +2341,42 @@ int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, 
   // multiplier tolerance is the reduction still needed divided by amp, with a
   // safety factor of 10 and a floor of kMinInnerTol.  A pass that does not
   // halve the true residual is undone and retried 1000x tighter.
-  constexpr int kMaxPasses = 6;
+  // The mixed-precision factor leaves a relative error of about 1e-7 kappa in
+  // each pass, so it may take several refinement passes where the FP64
+  // factor takes one.
+  const int kMaxPasses = tc_factor ? 40 : 6;
   double amp = 1e4;  // true-residual reduction / multiplier-residual reduction, updated per pass
+  // per-phase device time: right-hand side and recovery (multifrontal front
+  // solves, coarse solves) vs the multiplier iterations
+  EventPair ph0, ph1;
+  double lambda_ms = 0.0, fronts_ms = 0.0;
   while (bb > 0.0 && refinements < kMaxPasses) {
+    EMG_CK(cudaEventRecord(ph0.a, st));
     k_distribute<<<blocks_for(N, 256), 256, 0, st>>>(N, d_gptr, d_glist, rglob_d, fu_d);
     int rc = prepare_rhs(fu_d);
     if (rc) return rc;
+    EMG_CK(cudaEventRecord(ph0.b, st));
     int32_t it = 0;
     const double want = 0.1 * cfg.tolerance / std::max(rel, 1e-300) / amp;
     status = lambda_pcg(std::min(1e-2, std::max(kMinInnerTol, want)), cfg.max_iterations - total, &it, &lam_rel);
     total += it;
     ++refinements;
+    EMG_CK(cudaEventRecord(ph1.a, st));
     rc = recover(fu_d);
     if (rc) return rc;
+    EMG_CK(cudaEventRecord(ph1.b, st));
     k_axpy_s<<<blocks_for(N, 256), 256, 0, st>>>(N, 1.0, xg_d, xacc_d);
     double rr = 0.0;
     rc = global_residual(bg_d, xacc_d, &rr);
     if (rc) return rc;
+    {  // global_residual synchronized the stream: all four events are complete
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, ph0.a, ph0.b);
+      cudaEventElapsedTime(&b, ph0.b, ph1.a);
+      cudaEventElapsedTime(&c, ph1.a, ph1.b);
+      fronts_ms += a + c;
+      lambda_ms += b;
+    }
     const double rel_new = std::sqrt(rr / bb);
     if (status == EMG_NUMERICAL_ERROR) break;
     if (!(rel_new < 0.5 * rel)) {
@@ -2161,6 +2403,8 @@ int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, 
   stats.lambda_residual = lam_rel;
   stats.residual = bb > 0.0 ? rel : 0.0;
   stats.solve_ms = ev.ms();
+  stats.lambda_ms = lambda_ms;
+  stats.fronts_ms = fronts_ms;
   if (res) {
     res->status = status;
     res->iterations = total;
@@ -2168,6 +2412,29 @@ int FetiDP::solve(const emg_krylov_config& cfg, const double* b_d, double* x_d, 
     res->solve_time_ms = stats.solve_ms;
   }
   return status;
+}
+
+int tc_tile_test(int32_t mr, int32_t mc, int32_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
+                 double* C, int64_t ldc, cudaStream_t st) {
+  if (mr < 1 || mc < 1 || mr > tc::kM || mc > tc::kN || K < 0 || lda < mr || ldb < mc || ldc < mr || !A || !B ||
+      !C) {
+    set_error("emg_test_tc_tile: tile sizes must be 1..128 and leading dimensions at least the rows");
+    return EMG_INVALID_INPUT;
+  }
+  int32_t* err = nullptr;
+  EMG_CK(cudaMallocAsync(&err, sizeof(int32_t), st));
+  EMG_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+  EMG_CK(cudaFuncSetAttribute(k_tc_tile_test, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(tc::kSmemBytes)));
+  k_tc_tile_test<<<1, tc::kThreads, tc::kSmemBytes, st>>>(C, ldc, mr, mc, A, lda, B, ldb, K, err);
+  int32_t e = 0;
+  const cudaError_t le = cudaGetLastError();
+  EMG_CK(cudaMemcpyAsync(&e, err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  cudaFreeAsync(err, st);
+  EMG_CK(le);
+  if (e) { set_error("emg_test_tc_tile: a wait ran out"); return EMG_ERR_TIMEOUT; }
+  return EMG_SUCCESS;
 }
 
 }  // namespace emg

@@ -9,6 +9,8 @@
 // numbering places subdomain s at loc_off[s] .. loc_off[s+1].
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -77,5 +79,8 @@ struct FetiPlan {
 int build_feti_plan(const Mesh& m, const DofMap& d, FetiPlan& p);
 // Checks every index of the plan against the sizes it addresses.
 int validate_feti_plan(const FetiPlan& p);
+// One 128 x 128 tensor-core tile C -= A B^T (device arrays; test hook).
+int tc_tile_test(int32_t mr, int32_t mc, int32_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
+                 double* C, int64_t ldc, cudaStream_t st);
 
 }  // namespace emg

@@ -58,6 +58,8 @@ struct FetiStats {
   double lambda_residual = 0.0;   // ||r_lambda|| / ||r_lambda,0||
   double residual = 0.0;          // true ||b - A x|| / ||b|| of the global system
   double factor_ms = 0.0, solve_ms = 0.0;
+  double lambda_ms = 0.0;  // device time of the multiplier iterations
+  double fronts_ms = 0.0;  // device time of the right-hand sides and recoveries (front and coarse solves)
 };
 
 struct LearnState;
@@ -72,6 +74,7 @@ struct FetiDP {
   FrontsDev fd{};
   FacesDev fc{};
   bool factored = false;
+  bool tc_factor = false;  // factor contractions on the TF32 tensor cores (EMG_FLAG_FACTOR_TF32)
   int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks,
                         // 4 deluxe + learned correction (flexible CG)
   FetiStats stats;
@@ -119,6 +122,10 @@ struct FetiDP {
   float *S32_d = nullptr, *fDa32_d = nullptr, *fDb32_d = nullptr, *fDaT32_d = nullptr, *fDbT32_d = nullptr;
   void* state_d = nullptr;
   int32_t* err_d = nullptr;
+  // device-side multiplier loop: one while-loop graph per preconditioner 0..3
+  cudaGraphExec_t lam_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t cap_st = nullptr;
+  bool graph_failed = false;
   static constexpr int kParts = 592;
 
   ~FetiDP();
@@ -155,6 +162,8 @@ struct FetiDP {
   int trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off, double* X);
   int prepare_rhs(const double* fu);
   int lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel);
+  void lambda_body(void* state);
+  cudaGraphExec_t lambda_loop_graph();
   int lambda_fcg(double tol, int32_t max_it, int32_t* iters, double* rel);
   double dot_host(const double* a, const double* b, int64_t n);
   int recover(const double* fu);

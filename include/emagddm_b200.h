@@ -65,7 +65,11 @@ enum {
   EMG_FLAG_MASS = 1,           /* also assemble M_ij = int sigma W_i . W_j      */
   EMG_FLAG_NO_EDGE_SIGNS = 2,  /* scatter unsigned element matrices            */
   EMG_FLAG_PIOLA_LITERAL = 4,  /* W_phys = J^-T W_ref / detJ (reference text)   */
-  EMG_FLAG_QUAD3_LITERAL = 8   /* the reference's 3-point TET4 rule             */
+  EMG_FLAG_QUAD3_LITERAL = 8,  /* the reference's 3-point TET4 rule             */
+  EMG_FLAG_FACTOR_TF32 = 16    /* FETI-DP / direct factor: subdomain contractions
+                                  on the TF32 tensor cores (two-term split, FP32
+                                  accumulation); FP64 refinement on the true
+                                  residual restores full accuracy */
 };
 
 /* ---- source regions: J evaluated at quadrature points ------------------- */
@@ -288,8 +292,9 @@ int emg_fetidp_duals(emg_fetidp fd, int64_t* dual_off, int32_t* dual_lam, int32_
  * flops of the numeric phase: front panels, front update blocks, inverse
  * factors + deluxe weights. */
 int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
-/* stats[0..5]: factor ms, solve ms, iterations, multiplier residual, true
- * residual, FETI-DP passes. */
+/* stats[0..7]: factor ms, solve ms, iterations, multiplier residual, true
+ * residual, FETI-DP passes, and the solve's device ms split into the
+ * multiplier iterations and the right-hand-side / recovery front solves. */
 int emg_fetidp_stats(emg_fetidp fd, double* stats, int32_t n_stats);
 void emg_fetidp_destroy(emg_fetidp fd);
 /* Host-only symbolic analysis (no GPU needed): the info[] of the plan; a map
@@ -411,6 +416,14 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
  * block that gives up ends the solve with EMG_ERR_TIMEOUT instead of
  * waiting on; tests lower the limit to make that wait run out. */
 int emg_test_set_barrier_spins(int32_t spins);
+
+/* Test hook (no counterpart in the reference): one tile of the
+ * mixed-precision factor's tensor-core contraction, C -= A B^T with A
+ * (mr x k, leading dimension lda), B (mc x k, ldb), C (mr x mc, ldc), all
+ * column-major FP64 device arrays, 1 <= mr, mc <= 128; the tile splits each
+ * value into two TF32 terms and accumulates in FP32 (EMG_FLAG_FACTOR_TF32). */
+int emg_test_tc_tile(int32_t mr, int32_t mc, int32_t k, const double* a_d, int64_t lda, const double* b_d,
+                     int64_t ldb, double* c_d, int64_t ldc, void* stream);
 
 /* Solver storage of A (SELL-32-sigma copy built at the first solve or SpMV):
  * stored slots including padding and number of 32-row slices; -1 before the
