@@ -20,7 +20,7 @@ GAUGE_NONE, GAUGE_REF, GAUGE_BOUNDARY_FIRST = -1, 0, 1
 FLAG_MASS, FLAG_NO_EDGE_SIGNS, FLAG_PIOLA_LITERAL, FLAG_QUAD3_LITERAL = 1, 2, 4, 8
 ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
 DOF_SCALAR_ONLY, DOF_VECTOR_EDGE_ONLY, DOF_MIXED_AV, DOF_ABSENT = 0, 1, 2, -2
-PRECOND_NONE, PRECOND_JACOBI = 0, 1
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 
 I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

@@ -475,7 +475,7 @@ class IterativeSolverConfig:
     tolerance: float = 1e-8
     max_iterations: int = 1000
     residual_monitor_interval: int = 10
-    preconditioner: str = "NONE"  # NONE | JACOBI (ILU0 is reported as INVALID_INPUT)
+    preconditioner: str = "NONE"  # NONE | JACOBI | ILU0
 
 
 CGConfig = IterativeSolverConfig
@@ -502,7 +502,8 @@ class _KrylovSolver:
         self._history = []
 
     def get_solver_name(self) -> str:
-        return f"{self._base}_{'Jacobi' if self.config.preconditioner == 'JACOBI' else 'None'}"
+        name = {"JACOBI": "Jacobi", "ILU0": "ILU0"}.get(str(self.config.preconditioner).upper(), "None")
+        return f"{self._base}_{name}"
 
     def clear(self):
         self._A = None
@@ -520,9 +521,9 @@ class _KrylovSolver:
         if b.shape[0] != self._A.rows():
             res.error_msg = "right-hand side length does not match the matrix"
             return res
-        # PreconditionerType values of iterative_solvers.h:59-76; the library
-        # rejects ILU0 (2) and unknown names rather than substituting one
-        kinds = {"NONE": _abi.PRECOND_NONE, "JACOBI": _abi.PRECOND_JACOBI, "ILU0": 2}
+        # PreconditionerType values of iterative_solvers.h:59-76; unknown names
+        # are rejected by the library rather than substituted
+        kinds = {"NONE": _abi.PRECOND_NONE, "JACOBI": _abi.PRECOND_JACOBI, "ILU0": _abi.PRECOND_ILU0}
         cfg = _abi.KrylovConfig(self.config.tolerance, self.config.max_iterations,
                                 kinds.get(str(self.config.preconditioner).upper(), -1))
         out = _abi.Result()

@@ -24,6 +24,7 @@ void set_error(const std::string& msg);
 struct KrylovWorkspace;
 struct Sell;
 struct BatchPlan;
+struct IluState;
 
 // Device CSR matrix (int32 row_ptr / col, fp64 values, rows sorted, merged).
 // `version` changes whenever the values change (re-assembly), so derived
@@ -40,6 +41,7 @@ struct DevCsr {
   KrylovWorkspace* ws = nullptr;
   Sell* sell = nullptr;
   BatchPlan* batch = nullptr;  // lockstep batch layout (batch.cu)
+  IluState* ilu = nullptr;     // ILU(0) factor, level schedules and Krylov state (ilu.cu)
   ~DevCsr();
 };
 
@@ -67,12 +69,13 @@ int system_build(System& s, cudaStream_t st);
 int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_mat,
                     const emg_source* src, int32_t n_src, int32_t flags, cudaStream_t st);
 
-// EMG_PRECOND_NONE / _JACOBI, else EMG_INVALID_INPUT with a message (no
-// silent substitution for the reference's ILU0).
-inline int check_krylov_precond(int32_t p) {
-  if (p == EMG_PRECOND_NONE || p == EMG_PRECOND_JACOBI) return EMG_SUCCESS;
+// EMG_PRECOND_NONE / _JACOBI (and _ILU0 where the solver has it), else
+// EMG_INVALID_INPUT with a message (no silent substitution).
+inline int check_krylov_precond(int32_t p, bool ilu0_allowed = false) {
+  if (p == EMG_PRECOND_NONE || p == EMG_PRECOND_JACOBI || (ilu0_allowed && p == EMG_PRECOND_ILU0)) return EMG_SUCCESS;
   set_error("preconditioner " + std::to_string(p) +
-            ": only EMG_PRECOND_NONE (0) and EMG_PRECOND_JACOBI (1) exist on the GPU path");
+            (ilu0_allowed ? ": use EMG_PRECOND_NONE (0), EMG_PRECOND_JACOBI (1) or EMG_PRECOND_ILU0 (2)"
+                          : ": this solver takes EMG_PRECOND_NONE (0) or EMG_PRECOND_JACOBI (1)"));
   return EMG_INVALID_INPUT;
 }
 
@@ -97,6 +100,10 @@ int cg_kernel_times(DevCsr& A, int32_t iterations, cudaStream_t st, double* ms);
 int set_barrier_spins(int32_t spins);
 void free_workspace(KrylovWorkspace* ws);
 void free_batch(BatchPlan* p);
+void free_ilu(IluState* s);
+// CG / BiCGSTAB with the ILU(0) preconditioner (ilu.cu).
+int ilu_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg, cudaStream_t st,
+              emg_result* res, bool bicg);
 // Lockstep CG over the diagonal blocks [blocks[k], blocks[k+1]) of A (batch.cu).
 int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks, const double* b, double* x,
                    const emg_krylov_config& cfg, cudaStream_t st, emg_result* results);

@@ -118,6 +118,7 @@ struct FetiDP {
   double *fDa_d = nullptr, *fDb_d = nullptr, *c_d = nullptr;
   double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr, *root_tmp_d = nullptr;
   double *rold_d = nullptr, *zm_d = nullptr;  // flexible CG
+  double *fp_d = nullptr, *fq_d = nullptr, *fr0_d = nullptr;  // global flexible CG (mixed factor)
   // FP32 copies of the preconditioner blocks (mixed-precision mode)
   float *S32_d = nullptr, *fDa32_d = nullptr, *fDb32_d = nullptr, *fDaT32_d = nullptr, *fDbT32_d = nullptr;
   void* state_d = nullptr;
@@ -168,6 +169,8 @@ struct FetiDP {
   double dot_host(const double* a, const double* b, int64_t n);
   int recover(const double* fu);
   int global_residual(const double* b, const double* x, double* rr);
+  int fcg(const emg_krylov_config& cfg, double bb, int* status, int32_t* total, int32_t* outer, double* rel,
+          double* lam_rel, double* lambda_ms, double* fronts_ms);
 };
 
 // learned.cu

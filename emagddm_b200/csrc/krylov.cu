@@ -1822,7 +1822,7 @@ int run_solver(DevCsr& A, const double* b, double* x, const emg_krylov_config& c
   res->status = EMG_INVALID_INPUT;
   if (!b || !x) { set_error("null vector"); return EMG_INVALID_INPUT; }
   if (A.n <= 0) { set_error("empty matrix"); return EMG_INVALID_INPUT; }
-  if (check_krylov_precond(cfg.preconditioner)) return EMG_INVALID_INPUT;
+  if (check_krylov_precond(cfg.preconditioner, true)) return EMG_INVALID_INPUT;
   const int32_t max_iter = cfg.max_iterations;
   int rc;
   {
@@ -1941,11 +1941,13 @@ int csr_spmv(DevCsr& A, const double* x, double* y, cudaStream_t st) {
 
 int cg_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg, cudaStream_t st,
              emg_result* res) {
+  if (cfg.preconditioner == EMG_PRECOND_ILU0) return ilu_solve(A, b, x, cfg, st, res, false);
   return run_solver(A, b, x, cfg, st, res, false);
 }
 
 int bicgstab_solve(DevCsr& A, const double* b, double* x, const emg_krylov_config& cfg,
                    cudaStream_t st, emg_result* res) {
+  if (cfg.preconditioner == EMG_PRECOND_ILU0) return ilu_solve(A, b, x, cfg, st, res, true);
   return run_solver(A, b, x, cfg, st, res, true);
 }
 
@@ -2052,6 +2054,7 @@ void free_workspace(KrylovWorkspace* w) {
 
 // Pattern and values come from the stream-ordered pool (cudaMallocAsync).
 DevCsr::~DevCsr() {
+  free_ilu(ilu);
   free_workspace(ws);
   free_sell(sell);
   free_batch(batch);

@@ -83,12 +83,17 @@ typedef struct {
 
 /* ---- solver configuration and result ------------------------------------ */
 /* CGConfig / BiCGSTABConfig::PreconditionerType (iterative_solvers.h:59-76).
- * The reference's third value, ILU0 (= 2), is Eigen::IncompleteLUT (fill
- * factor 10, drop tolerance 1e-12, AMD ordering; iterative_solvers.h:324,
- * .cpp:277-286): a sequential host factorization with no GPU counterpart
- * here.  The solvers reject any value other than the two below with
- * EMG_INVALID_INPUT instead of substituting another preconditioner. */
-enum { EMG_PRECOND_NONE = 0, EMG_PRECOND_JACOBI = 1 };
+ * ILU0: the reference factors Eigen::IncompleteLUT (fill factor 10, drop
+ * tolerance 1e-12; iterative_solvers.h:324, .cpp:277-286); the GPU solvers
+ * factor ILU(0) on the matrix's own pattern (level-scheduled kernels, the
+ * factor kept with the matrix until its values change) and run the
+ * reference's CG / BiCGSTAB ILU0 iterations (.cpp:505-585, :1121-1243).  The
+ * fill differs, so iteration counts differ; a factorization that breaks down
+ * (missing diagonal, zero or non-finite pivot) leaves the solve without a
+ * preconditioner, as the reference's does.  Any other value is rejected with
+ * EMG_INVALID_INPUT; the batched and allocation-free solvers take NONE and
+ * JACOBI only. */
+enum { EMG_PRECOND_NONE = 0, EMG_PRECOND_JACOBI = 1, EMG_PRECOND_ILU0 = 2 };
 typedef struct {
   double tolerance;          /* ||r||/||b|| stop threshold (IterativeSolverConfig, default 1e-8) */
   int32_t max_iterations;    /* default 1000                                          */

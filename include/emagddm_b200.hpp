@@ -238,9 +238,11 @@ class GpuEMAssembly {
 template <bool kBiCG>
 class GpuKrylovSolver {
  public:
+  // preconditioner: EMG_PRECOND_NONE (0), _JACOBI (1) or _ILU0 (2), the
+  // values of PreconditionerType (a bool `jacobi` converts to 0 / 1)
   explicit GpuKrylovSolver(double tolerance = 1e-8, int32_t max_iterations = 1000,
-                           bool jacobi = false)
-      : cfg_{tolerance, max_iterations, jacobi ? EMG_PRECOND_JACOBI : EMG_PRECOND_NONE} {}
+                           int32_t preconditioner = EMG_PRECOND_NONE)
+      : cfg_{tolerance, max_iterations, preconditioner} {}
   ~GpuKrylovSolver() { clear(); }
   // CsrMatrix<double> from host arrays (duplicates summed, as to_eigen does).
   void set_matrix(int64_t n, const std::vector<int32_t>& row_ptr, const std::vector<int32_t>& col,
@@ -274,7 +276,9 @@ class GpuKrylovSolver {
   }
   std::string get_solver_name() const {
     return std::string(kBiCG ? "BiCGSTABSolver" : "CGSolver") +
-           (cfg_.preconditioner == EMG_PRECOND_JACOBI ? "_Jacobi" : "_None");
+           (cfg_.preconditioner == EMG_PRECOND_JACOBI ? "_Jacobi"
+            : cfg_.preconditioner == EMG_PRECOND_ILU0 ? "_ILU0"
+                                                      : "_None");
   }
   void clear() {
     if (owned_) emg_csr_destroy(owned_);

@@ -842,6 +842,101 @@ static void jacobi_inverse(int64_t n, const int64_t* rp, const int32_t* col,
   }
 }
 
+/* Preconditioners of CGSolver / BiCGSTABSolver: 0 none, 1 Jacobi
+ * (setup_preconditioner, iterative_solvers.cpp:261-292), 2 ILU0.  The
+ * reference's ILU0 is Eigen's IncompleteLUT (:277-286); this restatement
+ * uses ILU(0) on the matrix's own pattern -- the IKJ elimination (Saad,
+ * Iterative Methods for Sparse Linear Systems, 2nd ed., Algorithm 10.4)
+ * restricted to that pattern, as the GPU solver does -- and, like the
+ * reference, runs without a preconditioner when the factorization fails
+ * (:279-282): a row without a diagonal entry, columns not ascending, or a
+ * zero / non-finite pivot. */
+typedef struct {
+  int kind;        /* 0 none, 1 Jacobi, 2 ILU(0) */
+  double* dinv;    /* Jacobi */
+  double* lu;      /* ILU(0): unit L below, U on and above the diagonal */
+  int64_t* diag;
+  double* y;
+} OrcPrec;
+
+static void prec_free(OrcPrec* P) {
+  free(P->dinv); free(P->lu); free(P->diag); free(P->y);
+  P->dinv = P->lu = P->y = NULL;
+  P->diag = NULL;
+}
+
+static int ilu0_factor(int64_t n, const int64_t* rp, const int32_t* col, const double* val, OrcPrec* P) {
+  P->lu = (double*)malloc((size_t)(rp[n] > 0 ? rp[n] : 1) * sizeof(double));
+  P->diag = (int64_t*)malloc((size_t)n * sizeof(int64_t));
+  P->y = (double*)malloc((size_t)n * sizeof(double));
+  int64_t* where = (int64_t*)malloc((size_t)n * sizeof(int64_t));
+  if (!P->lu || !P->diag || !P->y || !where) { free(where); return 0; }
+  memcpy(P->lu, val, (size_t)rp[n] * sizeof(double));
+  for (int64_t i = 0; i < n; i++) where[i] = -1;
+  int ok = 1;
+  for (int64_t i = 0; i < n && ok; i++) {
+    P->diag[i] = -1;
+    for (int64_t q = rp[i]; q < rp[i + 1]; q++) {
+      if (q > rp[i] && col[q] <= col[q - 1]) ok = 0;
+      if (col[q] == i) P->diag[i] = q;
+    }
+    if (P->diag[i] < 0) ok = 0;
+  }
+  for (int64_t i = 0; i < n && ok; i++) {
+    for (int64_t q = rp[i]; q < rp[i + 1]; q++) where[col[q]] = q;
+    for (int64_t p = rp[i]; p < P->diag[i]; p++) {
+      const int64_t k = col[p];
+      const double l = P->lu[p] / P->lu[P->diag[k]];
+      P->lu[p] = l;
+      for (int64_t q = P->diag[k] + 1; q < rp[k + 1]; q++) {
+        const int64_t w = where[col[q]];
+        if (w >= 0) P->lu[w] -= l * P->lu[q];
+      }
+    }
+    for (int64_t q = rp[i]; q < rp[i + 1]; q++) where[col[q]] = -1;
+    const double u = P->lu[P->diag[i]];
+    if (!(fabs(u) > 0.0) || !isfinite(u)) ok = 0;
+  }
+  free(where);
+  return ok;
+}
+
+static int prec_setup(OrcPrec* P, int64_t n, const int64_t* rp, const int32_t* col, const double* val,
+                      int32_t precond) {
+  memset(P, 0, sizeof(*P));
+  P->kind = precond == 1 ? 1 : precond == 2 ? 2 : 0;
+  if (P->kind == 1) {
+    P->dinv = (double*)malloc((size_t)n * sizeof(double));
+    if (!P->dinv) return -1;
+    jacobi_inverse(n, rp, col, val, P->dinv);
+  } else if (P->kind == 2 && !ilu0_factor(n, rp, col, val, P)) {
+    prec_free(P);
+    P->kind = 0;  /* the reference falls back to no preconditioner */
+  }
+  return 0;
+}
+
+/* out = M^-1 in */
+static void prec_apply(const OrcPrec* P, int64_t n, const int64_t* rp, const int32_t* col, const double* in,
+                       double* out) {
+  if (P->kind == 1) {
+    for (int64_t i = 0; i < n; i++) out[i] = P->dinv[i] * in[i];
+  } else if (P->kind == 2) {
+    for (int64_t i = 0; i < n; i++) {
+      double s = 0.0;
+      for (int64_t p = rp[i]; p < P->diag[i]; p++) s += P->lu[p] * P->y[col[p]];
+      P->y[i] = in[i] - s;
+    }
+    for (int64_t i = n - 1; i >= 0; i--) {
+      double s = 0.0;
+      for (int64_t p = P->diag[i] + 1; p < rp[i + 1]; p++) s += P->lu[p] * out[col[p]];
+      out[i] = (P->y[i] - s) / P->lu[P->diag[i]];
+    }
+  } else {
+    for (int64_t i = 0; i < n; i++) out[i] = in[i];
+  }
+}
+
 int orc_pcg(int64_t n, const int64_t* rp, const int32_t* col, const double* val,
             const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
             int32_t* iterations, double* residual_norm) {
@@ -865,16 +960,16 @@ int orc_pcg_snap(int64_t n, const int64_t* rp, const int32_t* col, const double*
   double* z = (double*)malloc((size_t)n * sizeof(double));
   double* p = (double*)malloc((size_t)n * sizeof(double));
   double* q = (double*)malloc((size_t)n * sizeof(double));
-  double* dinv = (double*)malloc((size_t)n * sizeof(double));
-  if (!r || !z || !p || !q || !dinv) return -1;
-  if (precond) jacobi_inverse(n, rp, col, val, dinv);
-  else for (int64_t i = 0; i < n; i++) dinv[i] = 1.0;
-  for (int64_t i = 0; i < n; i++) { x[i] = 0.0; r[i] = b[i]; z[i] = dinv[i] * r[i]; p[i] = z[i]; }
+  OrcPrec M;
+  if (!r || !z || !p || !q || prec_setup(&M, n, rp, col, val, precond)) return -1;
+  for (int64_t i = 0; i < n; i++) { x[i] = 0.0; r[i] = b[i]; }
+  prec_apply(&M, n, rp, col, r, z);
+  for (int64_t i = 0; i < n; i++) p[i] = z[i];
   double rz = vdot(n, r, z);
   double bnorm = sqrt(vdot(n, b, b));
   int status = ORC_MAX_ITER_REACHED;
   if (bnorm < 1e-15) { /* :361-367 / :440-446 */
-    free(r); free(z); free(p); free(q); free(dinv);
+    free(r); free(z); free(p); free(q); prec_free(&M);
     return ORC_SUCCESS;
   }
   double res = sqrt(vdot(n, r, r)) / bnorm, prev = res;
@@ -888,8 +983,8 @@ int orc_pcg_snap(int64_t n, const int64_t* rp, const int32_t* col, const double*
     for (int64_t i = 0; i < n; i++) {
       x[i] += alpha * p[i];
       r[i] -= alpha * q[i];
-      z[i] = dinv[i] * r[i];
     }
+    prec_apply(&M, n, rp, col, r, z);
     double rz_new = vdot(n, r, z);
     res = sqrt(vdot(n, r, r)) / bnorm;
     if (x_snap && snap_iter && *snap_iter < 0 && res < snap_tol) {
@@ -906,7 +1001,7 @@ int orc_pcg_snap(int64_t n, const int64_t* rp, const int32_t* col, const double*
   }
   *iterations = it <= max_iter ? it : max_iter;
   *residual_norm = res;
-  free(r); free(z); free(p); free(q); free(dinv);
+  free(r); free(z); free(p); free(q); prec_free(&M);
   return status;
 }
 
@@ -918,15 +1013,14 @@ int orc_bicgstab(int64_t n, const int64_t* rp, const int32_t* col, const double*
   if (n <= 0) return ORC_INVALID_INPUT;
   size_t sz = (size_t)n * sizeof(double);
   double *r = malloc(sz), *rh = malloc(sz), *p = malloc(sz), *v = malloc(sz);
-  double *s = malloc(sz), *z = malloc(sz), *t = malloc(sz), *dinv = malloc(sz);
-  if (!r || !rh || !p || !v || !s || !z || !t || !dinv) return -1;
-  if (precond) jacobi_inverse(n, rp, col, val, dinv);
-  else for (int64_t i = 0; i < n; i++) dinv[i] = 1.0;
+  double *s = malloc(sz), *z = malloc(sz), *t = malloc(sz);
+  OrcPrec M;
+  if (!r || !rh || !p || !v || !s || !z || !t || prec_setup(&M, n, rp, col, val, precond)) return -1;
   for (int64_t i = 0; i < n; i++) { x[i] = 0.0; r[i] = b[i]; rh[i] = b[i]; p[i] = b[i]; v[i] = 0.0; }
   double rho = vdot(n, r, rh), alpha = 1.0, omega = 1.0;
   double bnorm = sqrt(vdot(n, b, b));
   int status = ORC_MAX_ITER_REACHED;
-  if (bnorm < 1e-15) { free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv); return ORC_SUCCESS; }
+  if (bnorm < 1e-15) { free(r); free(rh); free(p); free(v); free(s); free(z); free(t); prec_free(&M); return ORC_SUCCESS; }
   double res = sqrt(vdot(n, r, r)) / bnorm, prev = res;
   int dcount = 0;
   int32_t it;
@@ -949,11 +1043,11 @@ int orc_bicgstab(int64_t n, const int64_t* rp, const int32_t* col, const double*
       for (int64_t i = 0; i < n; i++) x[i] += alpha * p[i];
       *iterations = it;
       *residual_norm = res;
-      free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv);
+      free(r); free(rh); free(p); free(v); free(s); free(z); free(t); prec_free(&M);
       return ORC_SUCCESS;
     }
-    /* precondition s only (:1061) */
-    for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * s[i];
+    /* precondition s only (:1061, :1186) */
+    prec_apply(&M, n, rp, col, s, z);
     orc_spmv(n, rp, col, val, z, t);
     double tt = vdot(n, t, t);
     omega = fabs(tt) < 1e-30 ? 0.0 : vdot(n, z, t) / tt;
@@ -974,7 +1068,7 @@ int orc_bicgstab(int64_t n, const int64_t* rp, const int32_t* col, const double*
   }
   *iterations = it <= max_iter ? it : max_iter;
   *residual_norm = res;
-  free(r); free(rh); free(p); free(v); free(s); free(z); free(t); free(dinv);
+  free(r); free(rh); free(p); free(v); free(s); free(z); free(t); prec_free(&M);
   return status;
 }
 

@@ -102,8 +102,10 @@ int orc_assemble(int64_t n_nodes, const double* xyz, int64_t n_tets,
 void orc_spmv(int64_t n, const int64_t* row_ptr, const int32_t* col,
               const double* val, const double* x, double* y);
 
-/* CGSolver::solve_no_preconditioner / solve_with_jacobi
- * (src/numeric/iterative_solvers.cpp:343-503).  precond: 0 none, 1 jacobi. */
+/* CGSolver::solve_no_preconditioner / solve_with_jacobi / solve_with_ilu0
+ * (src/numeric/iterative_solvers.cpp:343-585).  precond: 0 none, 1 jacobi,
+ * 2 ILU0 (restated as ILU(0) on the matrix's pattern; the reference's is
+ * Eigen's IncompleteLUT). */
 int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col,
             const double* val, const double* b, double* x, double tol,
             int32_t max_iter, int32_t precond, int32_t* iterations,

@@ -230,7 +230,8 @@ int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, in
 }
 
 // CGSolver / BiCGSTABSolver on a host CSR.  kind: 0 = CG, 1 = BiCGSTAB.
-// precond: 0 none, 1 jacobi.  Returns SolverStatus; times set_matrix and solve.
+// precond: 0 none, 1 jacobi, 2 ILU0 (Eigen IncompleteLUT inside the
+// reference).  Returns SolverStatus; times set_matrix and solve.
 int refb_krylov(int32_t kind, int64_t n, const int64_t* rp, const int32_t* col, const double* val,
                 const double* b, double* x, double tol, int32_t max_iter, int32_t precond,
                 int32_t* iterations, double* residual, double* setup_ms, double* solve_ms) {
@@ -243,8 +244,9 @@ int refb_krylov(int32_t kind, int64_t n, const int64_t* rp, const int32_t* col, 
       numeric::CGConfig cfg;
       cfg.tolerance = tol;
       cfg.max_iterations = max_iter;
-      cfg.preconditioner = precond ? numeric::CGConfig::PreconditionerType::JACOBI
-                                   : numeric::CGConfig::PreconditionerType::NONE;
+      cfg.preconditioner = precond == 2   ? numeric::CGConfig::PreconditionerType::ILU0
+                           : precond == 1 ? numeric::CGConfig::PreconditionerType::JACOBI
+                                          : numeric::CGConfig::PreconditionerType::NONE;
       numeric::CGSolver s(cfg);
       s.set_matrix(A);
       auto t1 = std::chrono::steady_clock::now();
@@ -256,8 +258,9 @@ int refb_krylov(int32_t kind, int64_t n, const int64_t* rp, const int32_t* col, 
       numeric::BiCGSTABConfig cfg;
       cfg.tolerance = tol;
       cfg.max_iterations = max_iter;
-      cfg.preconditioner = precond ? numeric::BiCGSTABConfig::PreconditionerType::JACOBI
-                                   : numeric::BiCGSTABConfig::PreconditionerType::NONE;
+      cfg.preconditioner = precond == 2   ? numeric::BiCGSTABConfig::PreconditionerType::ILU0
+                           : precond == 1 ? numeric::BiCGSTABConfig::PreconditionerType::JACOBI
+                                          : numeric::BiCGSTABConfig::PreconditionerType::NONE;
       numeric::BiCGSTABSolver s(cfg);
       s.set_matrix(A);
       auto t1 = std::chrono::steady_clock::now();

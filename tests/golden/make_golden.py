@@ -9,7 +9,7 @@ Kuhn-split cube meshes of emagddm_b200.mesh, the HEX8_EDGE fixtures on the
 hex grids of the same module, and the per-element DOF-type (MIXED_AV)
 fixtures on both:
 
-  python tests/golden/make_golden.py [--hex-only | --av-only]
+  python tests/golden/make_golden.py [--hex-only | --av-only | --ilu0-only]
 """
 from __future__ import annotations
 
@@ -114,9 +114,35 @@ def av_fixtures():
     print("wrote", len(arrays), "per-element DOF-type arrays")
 
 
+def ilu0_fixtures():
+    """The reference's CGSolver / BiCGSTABSolver with PreconditionerType::ILU0
+    (Eigen IncompleteLUT inside) on the restated n=4 box-source system and the
+    n=6 iron-block / coil system (reference_ilu0_fixtures.npz /
+    reference_ilu0_counts.json)."""
+    arrays, counts = {}, {}
+    for tag, m in (("n4", mesh.plain_small(4)), ("s6", mesh.plain_scale(6))):
+        r1 = R.dof_build(m.n_nodes, m.tets, m.dirichlet, gauge=True)
+        rp, col, kv, _, rhs = O.assemble(m, r1["l2g"], r1["n_dofs"])
+        arrays[f"{tag}_row_ptr"] = rp.astype(np.int64)
+        arrays[f"{tag}_col"] = col.astype(np.int32)
+        arrays[f"{tag}_val"] = kv
+        arrays[f"{tag}_rhs"] = rhs
+        for kind, name in ((0, "cg"), (1, "bicgstab")):
+            x, st, it, res, _, _ = R.krylov(kind, rp, col, kv, rhs, tol=1e-10, max_iter=1000, precond=2)
+            arrays[f"{tag}_{name}_ilu0_x"] = x
+            counts[f"{tag}_{name}_ilu0"] = dict(status=int(st), iterations=int(it), residual=float(res))
+    np.savez_compressed(os.path.join(HERE, "reference_ilu0_fixtures.npz"), **arrays)
+    with open(os.path.join(HERE, "reference_ilu0_counts.json"), "w") as f:
+        json.dump(counts, f, indent=1, sort_keys=True)
+    print("wrote", len(arrays), "ILU0 arrays:", counts)
+
+
 def main():
     assert R.available(), "build oracle/_ref first (make -C oracle -f Makefile.ref)"
     R.lib().refb_quiet(1)
+    if "--ilu0-only" in sys.argv:
+        ilu0_fixtures()
+        return
     if "--hex-only" in sys.argv:
         hex_fixtures()
         return
@@ -173,6 +199,7 @@ def main():
     print("wrote", len(arrays), "arrays and", len(counts), "count records")
     hex_fixtures()
     av_fixtures()
+    ilu0_fixtures()
 
 
 if __name__ == "__main__":

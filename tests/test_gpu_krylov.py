@@ -190,25 +190,24 @@ def test_history_records_every_iteration():
     assert h[-1] == out.residual_norm and h[-1] < 1e-9 <= h[-2]
 
 
-def test_ilu0_and_unknown_preconditioners_are_rejected():
-    """The reference's third preconditioner (ILU0 = Eigen's IncompleteLUT) has
-    no GPU counterpart: value 2 and unknown values are INVALID_INPUT, never a
-    silent substitute."""
+def test_unknown_preconditioners_are_rejected():
+    """Only the reference's three PreconditionerType values exist; anything
+    else is INVALID_INPUT, never a silent substitute."""
     from emagddm_b200 import api
     m = mesh.plain_small(3)
     l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
     s = System(m, l2g)
     _, _, _, _, rhs = oracle_system(m, l2g)
-    for pc in (2, 7, -1):
+    for pc in (3, 7, -1):
         for kind in ("cg", "bicgstab"):
             _, out = solve(s.matrix(0), rhs, kind, precond=pc)
             assert out.status == _abi.EMG_INVALID_INPUT
-            assert b"EMG_PRECOND_JACOBI" in lib().emg_last_error()
+            assert b"EMG_PRECOND_ILU0" in lib().emg_last_error()
     A = api.CsrMatrix(s.matrix(0), owner=s)
-    cg = api.CGSolver(api.IterativeSolverConfig(preconditioner="ILU0"))
+    cg = api.CGSolver(api.IterativeSolverConfig(preconditioner="SSOR"))
     cg.set_matrix(A)
     r = cg.solve(rhs)
-    assert r.status == api.SolverStatus.INVALID_INPUT and "preconditioner 2" in r.error_msg
+    assert r.status == api.SolverStatus.INVALID_INPUT and "preconditioner -1" in r.error_msg
 
 
 @pytest.mark.parametrize("n", [2_500_001, 1_000_000])

@@ -34,8 +34,9 @@ def test_tc_tile_matches_fp64(mr, mc, k, scale):
     rng = np.random.default_rng(mr * 7 + mc * 3 + k)
     lda, ldb, ldc = mr + 5, mc + 3, mr + 9
     # column-major storage: (k, ld) in C order is (ld, k) column-major
-    A = rng.standard_normal((k, lda))
-    B = rng.standard_normal((k, ldb))
+    # (at least one column allocated: k = 0 still passes valid pointers)
+    A = rng.standard_normal((max(k, 1), lda))
+    B = rng.standard_normal((max(k, 1), ldb))
     if scale:  # rows spanning +-scale decades
         A *= 10.0 ** rng.uniform(-scale, scale, size=(1, lda))
         B *= 10.0 ** rng.uniform(-scale, scale, size=(1, ldb))
@@ -46,7 +47,7 @@ def test_tc_tile_matches_fp64(mr, mc, k, scale):
     torch.cuda.synchronize()
     assert rc == _abi.EMG_SUCCESS, lib().emg_last_error()
     out = dC.cpu().numpy()
-    a, b = A[:, :mr].T, B[:, :mc].T            # (mr, k), (mc, k)
+    a, b = A[:k, :mr].T, B[:k, :mc].T          # (mr, k), (mc, k)
     want = Cm[:mc, :mr] - (a @ b.T).T           # C stored (mc, ldc): [col, row]
     bound = 4e-6 * (np.abs(a) @ np.abs(b).T).T + 1e-300
     assert np.all(np.abs(out[:mc, :mr] - want) <= bound), np.max(np.abs(out[:mc, :mr] - want) / bound)
@@ -72,14 +73,16 @@ def test_mixed_factor_fetidp_matches_oracle(kind, n, parts):
     part = mesh.jittered_partition(m, parts)
     fd = fetidp.FetiDP(m, part, parts ** 3)
     assert fd.factor(flags=FLAG_TF32) == _abi.EMG_SUCCESS, lib().emg_last_error()
-    x, rc, out = fd.solve(tol=1e-10, max_iter=3000)
+    # residuals well below the solution bar on both sides, so that the
+    # comparison measures the solvers, not their stopping points
+    x, rc, out = fd.solve(tol=1e-11, max_iter=5000)
     assert rc == _abi.EMG_SUCCESS, (rc, lib().emg_last_error())
-    assert out.residual_norm <= 1e-10
-    xo = _monolithic(m, fd.map.l2g)
+    assert out.residual_norm <= 1e-11
+    xo = _monolithic(m, fd.map.l2g, tol=1e-13)
     assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
     # the FP64 factor of the same plan gives the same solution
     assert fd.factor() == _abi.EMG_SUCCESS
-    x64, rc, _ = fd.solve(tol=1e-10, max_iter=3000)
+    x64, rc, _ = fd.solve(tol=1e-11, max_iter=5000)
     assert rc == 0 and np.linalg.norm(x - x64) <= 1e-8 * np.linalg.norm(x64)
 
 

@@ -173,3 +173,34 @@ def test_pcg_snapshot_is_the_iterate_of_the_looser_solve():
     np.testing.assert_array_equal(xs, x8)
     _, _, _, _, _, never = O.pcg_snap(rp, col, kv, rhs, tol=1e-6, snap_tol=1e-9, max_iter=5000)
     assert never == -1
+
+
+def test_oracle_ilu0_cg_reaches_the_reference_solution():
+    """The oracle's ILU(0) restatement (CG solve_with_ilu0 steps) converges to
+    the solution the reference's CGSolver with IncompleteLUT returns; ILU(0)
+    of a tridiagonal matrix is exact (one iteration)."""
+    import json as _json
+    F = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_ilu0_fixtures.npz"))
+    for tag in ("n4", "s6"):
+        rp, col, kv, b = F[f"{tag}_row_ptr"], F[f"{tag}_col"], F[f"{tag}_val"], F[f"{tag}_rhs"]
+        x, st, it, res = O.pcg(rp, col, kv, b, tol=1e-10, max_iter=1000, precond=2)
+        xr = F[f"{tag}_cg_ilu0_x"]
+        assert st == 0 and np.linalg.norm(x - xr) <= 1e-8 * np.linalg.norm(xr)
+        _, _, itj, _ = O.pcg(rp, col, kv, b, tol=1e-10, max_iter=1000, precond=1)
+        assert it < itj
+    n = 300
+    i = np.arange(n)
+    rows = np.concatenate([i, i[1:], i[:-1]])
+    cols = np.concatenate([i, i[:-1], i[1:]])
+    vals = np.concatenate([4.0 + (i % 3), -np.ones(n - 1), -np.ones(n - 1)])
+    o = np.lexsort((cols, rows))
+    rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int64)
+    x, st, it, _ = O.pcg(rp, cols[o].astype(np.int32), vals[o], np.ones(n), tol=1e-12, max_iter=50, precond=2)
+    assert st == 0 and it == 1
+    # a zero pivot: the solve runs without a preconditioner, as the reference's does
+    rp2 = np.array([0, 2, 4], np.int64)
+    c2 = np.array([0, 1, 0, 1], np.int32)
+    v2 = np.array([1.0, 2.0, 2.0, 4.0])
+    a = O.pcg(rp2, c2, v2, np.array([1.0, 0.5]), tol=1e-10, max_iter=20, precond=2)
+    b_ = O.pcg(rp2, c2, v2, np.array([1.0, 0.5]), tol=1e-10, max_iter=20, precond=0)
+    assert a[1:] == b_[1:] and np.array_equal(a[0], b_[0])
