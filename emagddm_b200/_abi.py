@@ -93,6 +93,8 @@ SIGNATURES = {
                           C.POINTER(Result)], C.c_int),
     "emg_cg_kernel_times": ([H, C.c_int32, VP, VP], C.c_int),
     "emg_test_set_barrier_spins": ([C.c_int32], C.c_int),
+    "emg_tune_enable": ([C.c_int32], C.c_int),
+    "emg_tune_report": ([C.c_char_p, C.c_int32], C.c_int32),
     "emg_test_tc_tile": ([C.c_int32, C.c_int32, C.c_int32, VP, C.c_int64, VP, C.c_int64, VP, C.c_int64, VP],
                          C.c_int),
     "emg_system_combine": ([H, C.c_double, C.c_double, C.POINTER(H)], C.c_int),
@@ -172,3 +174,12 @@ def sources_array(sources):
         for i in range(6):
             arr[k].p[i] = float(s.p[i])
     return arr, len(sources)
+
+
+def tune_report() -> dict:
+    """The autotuner's decisions so far (emg_tune_report), as a dict."""
+    import json
+    n = lib().emg_tune_report(None, 0)
+    buf = C.create_string_buffer(int(n))
+    lib().emg_tune_report(buf, n)
+    return json.loads(buf.value.decode() or "{}")

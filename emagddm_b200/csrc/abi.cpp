@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "device.h"
+#include "tune.h"
 #include "fetidp_dev.h"
 #include "internal.h"
 #include "trace.h"
@@ -693,6 +694,21 @@ int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms)
 int emg_test_tc_tile(int32_t mr, int32_t mc, int32_t k, const double* a_d, int64_t lda, const double* b_d,
                      int64_t ldb, double* c_d, int64_t ldc, void* stream) {
   return guarded([&]() -> int { return emg::tc_tile_test(mr, mc, k, a_d, lda, b_d, ldb, c_d, ldc, as_stream(stream)); });
+}
+
+int emg_tune_enable(int32_t on) {
+  emg::tune::set_enabled(on != 0);
+  return EMG_SUCCESS;
+}
+
+int32_t emg_tune_report(char* buf, int32_t cap) {
+  const std::string r = emg::tune::report();
+  if (buf && cap > 0) {
+    const size_t n = std::min<size_t>(r.size(), static_cast<size_t>(cap - 1));
+    std::memcpy(buf, r.data(), n);
+    buf[n] = '\0';
+  }
+  return static_cast<int32_t>(r.size() + 1);
 }
 
 int emg_test_set_barrier_spins(int32_t spins) {

@@ -28,6 +28,7 @@
 
 #include "common.cuh"
 #include "device.h"
+#include "tune.h"
 #include "trace.h"
 
 namespace emg {
@@ -44,6 +45,7 @@ struct BatchPlan {
   int64_t n = 0, N = 0, nslices = 0, slots = 0;
   int32_t nb = 0;
   int grid_spmv = 0, grid_vec = 0;  // one-wave grids of the slice kernels
+  bool tuned = false;               // grid_spmv chosen by the autotuner (first solve)
   std::vector<int64_t> blocks;      // host copy of the block row partition
   uint64_t version = ~uint64_t(0);
   // device arrays
@@ -839,6 +841,31 @@ int batch_cg_solve(DevCsr& A, int32_t nb, const int64_t* blocks_in, const double
   k_b_fin_init<<<fin_grid(nb), kBT, 0, st>>>(v);
   k_b_list<false><<<1, 1024, 0, st>>>(v, cudaGraphConditionalHandle{});  // blocks with b != 0
   EMG_CK(cudaGetLastError());
+  if (!P.tuned) {
+    // Warps sharing the slices of the SpMV: one resident wave (default) or
+    // one or two blocks per SM fewer, timed on this batch's first SpMV (its
+    // q and partials are overwritten by the loop's own first SpMV).
+    P.tuned = true;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per = std::max(1, P.grid_spmv / std::max(sms, 1));
+    std::vector<int> cand{P.grid_spmv};
+    for (int d = 1; d <= 2; ++d)
+      if (per - d >= 1) cand.push_back((per - d) * sms);
+    const std::string key = "nb" + std::to_string(nb) + "N" + std::to_string(P.N) + "slots" + std::to_string(P.slots);
+    const int g = tune::pick("batch.spmv_grid", key, cand, [&](int gv, cudaStream_t s2) {
+      k_b_spmv_dot<<<gv, kBT, 0, s2>>>(v);
+    }, st);
+    cudaGetLastError();
+    if (g != P.grid_spmv) {
+      P.grid_spmv = g;
+      cudaGraphExecDestroy(P.loop);
+      P.loop = nullptr;
+      int rc = capture_batch_loop(P);
+      if (rc) return rc;
+    }
+  }
   EMG_CK(cudaGraphLaunch(P.loop, st));
   k_b_scatter<<<launch_grid(P.N), 256, 0, st>>>(P.N, P.perm, P.x, x);
   EMG_CK(cudaEventRecord(e1, st));

@@ -31,6 +31,7 @@
 #include "fetidp_dev.h"
 #include "tc_tile.cuh"
 #include "trace.h"
+#include "tune.h"
 
 namespace emg {
 namespace {
@@ -711,11 +712,22 @@ __global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t*
 // skipped (they are solved with L^-1).  Forward: per block of 32 pivots one
 // warp solves the diagonal block, then all warps update the rows below it.
 constexpr int kSB = 32;
+constexpr int kPivMax = 1024;     // pivot-block kernels: one CTA per (front, column), up to 1024 threads
+constexpr int kUpdMax = 512;      // forward update rows: one row per thread, up to 512 a CTA
+constexpr int kXChunk = 2048;     // pivot values staged in shared memory per pass
 
-__global__ void __launch_bounds__(256) k_front_fwd_blk(FrontsDev F, int32_t f0, RhsDev R,
-                                                       const int32_t* __restrict__ nI,
-                                                       const int32_t* __restrict__ nD,
-                                                       const double* __restrict__ fac) {
+// Every level's front solve is split in two: the pivot block L11 (a
+// sequential chain of 32-pivot panels, one wide CTA per front and column)
+// and the update rows L21 (a GEMV, spread over many CTAs per front), so
+// that the top levels, with few large fronts, still cover the GPU.
+
+// Forward, pivot block: the children's update vectors into x / V, then
+// L11 y = x_piv panel by panel (one warp solves a 32 x 32 block, all warps
+// update the pivot rows below it).
+__global__ void __launch_bounds__(kPivMax) k_front_fwd_piv(FrontsDev F, int32_t f0, RhsDev R,
+                                                               const int32_t* __restrict__ nI,
+                                                               const int32_t* __restrict__ nD,
+                                                               const double* __restrict__ fac) {
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
@@ -760,22 +772,95 @@ __global__ void __launch_bounds__(256) k_front_fwd_blk(FrontsDev F, int32_t f0, 
       if (lane < nb) { x[p0 + jb + lane] = v; yb[lane] = v; }
     }
     __syncthreads();
-    for (int32_t i = jb + nb + tid; i < fs; i += blockDim.x) {
+    for (int32_t i = jb + nb + tid; i < np; i += blockDim.x) {
       double acc = 0.0;
       for (int32_t j = 0; j < nb; ++j) acc = fma(L[i + static_cast<int64_t>(jb + j) * fs], yb[j], acc);
-      if (i < np) x[p0 + i] -= acc;
-      else V[i - np] -= acc;
+      x[p0 + i] -= acc;
     }
     __syncthreads();
   }
 }
 
-// Backward: per block (last first) the warps form the dot products with the
-// rows below the block, then one warp solves the diagonal block.
-__global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, RhsDev R,
+// Forward, update rows: V[i - np] -= sum_j L[i, j] y_j for the rows
+// np .. fs-1, one row per thread (grid: row chunk, front, column); the
+// pivot values are staged in shared memory.
+__global__ void __launch_bounds__(kUpdMax) k_front_fwd_upd(FrontsDev F, int32_t f0, RhsDev R,
+                                                            const int32_t* __restrict__ nI,
+                                                            const int32_t* __restrict__ nD,
+                                                            const double* __restrict__ fac) {
+  const int32_t k = f0 + blockIdx.y;
+  if (F.is_root[k]) return;
+  const int32_t s = F.sub[k];
+  const int32_t col = blockIdx.z;
+  if (col >= R.ncol[s]) return;
+  const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
+  const int32_t r0 = blockIdx.x * blockDim.x;
+  if (r0 >= nu || np == 0) return;
+  __shared__ double xs[kXChunk];
+  const int32_t ld = nI[s] + nD[s];
+  const double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
+  const int32_t i = np + r0 + threadIdx.x;
+  const bool live = i < fs;
+  const double* L = fac + F.fac[k] + (live ? i : np);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  for (int32_t c0 = 0; c0 < np; c0 += kXChunk) {
+    const int32_t cw = min(kXChunk, np - c0);
+    __syncthreads();
+    for (int32_t e = threadIdx.x; e < cw; e += blockDim.x) xs[e] = x[p0 + c0 + e];
+    __syncthreads();
+    if (live) {
+      const double* Lc = L + static_cast<int64_t>(c0) * fs;
+      int32_t j = 0;
+      for (; j + 3 < cw; j += 4) {
+        a0 = fma(Lc[static_cast<int64_t>(j) * fs], xs[j], a0);
+        a1 = fma(Lc[static_cast<int64_t>(j + 1) * fs], xs[j + 1], a1);
+        a2 = fma(Lc[static_cast<int64_t>(j + 2) * fs], xs[j + 2], a2);
+        a3 = fma(Lc[static_cast<int64_t>(j + 3) * fs], xs[j + 3], a3);
+      }
+      for (; j < cw; ++j) a0 = fma(Lc[static_cast<int64_t>(j) * fs], xs[j], a0);
+    }
+  }
+  if (live) V[i - np] -= (a0 + a1) + (a2 + a3);
+}
+
+// Backward, update rows: x_j -= sum_{i >= np} L[i, j] x[row i] for every
+// pivot column j, a warp per column (grid: column chunk, front, rhs column).
+__global__ void __launch_bounds__(256) k_front_bwd_upd(FrontsDev F, int32_t f0, RhsDev R,
                                                        const int32_t* __restrict__ nI,
                                                        const int32_t* __restrict__ nD,
                                                        const double* __restrict__ fac) {
+  const int32_t k = f0 + blockIdx.y;
+  if (F.is_root[k]) return;
+  const int32_t s = F.sub[k];
+  const int32_t col = blockIdx.z;
+  if (col >= R.ncol[s]) return;
+  const int lane = threadIdx.x & 31;
+  const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
+  const int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= np || fs == np) return;
+  const int32_t ld = nI[s] + nD[s];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  const int32_t* rows = F.rows_v + F.rows[k];
+  const double* Lj = fac + F.fac[k] + static_cast<int64_t>(j) * fs;
+  double a0 = 0.0, a1 = 0.0;
+  int32_t i = np + lane;
+  for (; i + 32 < fs; i += 64) {
+    a0 = fma(Lj[i], x[rows[i]], a0);
+    a1 = fma(Lj[i + 32], x[rows[i + 32]], a1);
+  }
+  if (i < fs) a0 = fma(Lj[i], x[rows[i]], a0);
+  const double acc = warp_sum(a0 + a1);
+  if (lane == 0) x[p0 + j] -= acc;
+}
+
+// Backward, pivot block: per 32-pivot panel (last first) the warps form the
+// dot products of the panel's columns with the pivot rows below it, then one
+// warp solves the diagonal block.
+__global__ void __launch_bounds__(kPivMax) k_front_bwd_piv(FrontsDev F, int32_t f0, RhsDev R,
+                                                               const int32_t* __restrict__ nI,
+                                                               const int32_t* __restrict__ nD,
+                                                               const double* __restrict__ fac) {
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
@@ -785,7 +870,6 @@ __global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, 
   const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
   const int32_t ld = nI[s] + nD[s];
   double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
-  const int32_t* rows = F.rows_v + F.rows[k];
   const double* L = fac + F.fac[k];
   __shared__ double tb[kSB];
   __shared__ double Db[kSB][kSB + 1];
@@ -798,7 +882,7 @@ __global__ void __launch_bounds__(256) k_front_bwd_blk(FrontsDev F, int32_t f0, 
     for (int32_t j = wid; j < nb; j += nw) {
       const double* Lj = L + static_cast<int64_t>(jb + j) * fs;
       double acc = 0.0;
-      for (int32_t i = jb + nb + lane; i < fs; i += 32) acc = fma(Lj[i], x[i < np ? p0 + i : rows[i]], acc);
+      for (int32_t i = jb + nb + lane; i < np; i += 32) acc = fma(Lj[i], x[p0 + i], acc);
       acc = warp_sum(acc);
       if (lane == 0) tb[j] = acc;
     }
@@ -1771,11 +1855,26 @@ int FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_
 // their explicit inverse factors.
 int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   const int32_t nlev = static_cast<int32_t>(plan.level_ptr.size()) - 1;
+  if (static_cast<int32_t>(lvl_max_np.size()) != nlev) {  // largest pivot / update counts per level
+    lvl_max_np.assign(nlev, 0);
+    lvl_max_nu.assign(nlev, 0);
+    for (int32_t h = 0; h < nlev; ++h)
+      for (int32_t k = plan.level_ptr[h]; k < plan.level_ptr[h + 1]; ++k) {
+        const FetiFront& x = plan.fronts[k];
+        if (x.is_root) continue;
+        lvl_max_np[h] = std::max(lvl_max_np[h], x.npiv);
+        lvl_max_nu[h] = std::max(lvl_max_nu[h], x.f - x.npiv);
+      }
+  }
+  const unsigned nc = static_cast<unsigned>(ncol);
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
-    if (nf > 0)
-      k_front_fwd_blk<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 256, 0, st>>>(fd, f0, R, d_nI,
-                                                                                                    d_nD, fac_d);
+    if (nf == 0) continue;  // (a front without pivots still gathers its children)
+    k_front_fwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
+    if (lvl_max_nu[h] > 0)
+      k_front_fwd_upd<<<dim3(static_cast<unsigned>((lvl_max_nu[h] + upd_rows - 1) / upd_rows),
+                             static_cast<unsigned>(nf), nc),
+                        upd_rows, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
   }
   if (n_roots > 0) {
     const unsigned rc = static_cast<unsigned>(n_roots * ncol);
@@ -1789,9 +1888,11 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   }
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
-    if (nf > 0)
-      k_front_bwd_blk<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(nf)), 256, 0, st>>>(fd, f0, R, d_nI,
-                                                                                                    d_nD, fac_d);
+    if (nf == 0 || lvl_max_np[h] == 0) continue;
+    if (lvl_max_nu[h] > 0)
+      k_front_bwd_upd<<<dim3(static_cast<unsigned>((lvl_max_np[h] + 7) / 8), static_cast<unsigned>(nf), nc), 256, 0,
+                        st>>>(fd, f0, R, d_nI, d_nD, fac_d);
+    k_front_bwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
   }
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
@@ -1801,9 +1902,9 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
 void FetiDP::coarse_solve(const double* t, double* u) {
   const int32_t nc = plan.n_coarse;
   if (nc == 0) return;
-  const dim3 g(static_cast<unsigned>((nc + 7) / 8), 1);
-  k_block_colgemv<double><<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t, t2_d, 0);
-  k_block_colgemv<double><<<g, 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t2_d, u, 1);
+  const dim3 g(static_cast<unsigned>((nc + gemv_warps - 1) / gemv_warps), 1);
+  k_block_colgemv<double><<<g, 32 * gemv_warps, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t, t2_d, 0);
+  k_block_colgemv<double><<<g, 32 * gemv_warps, 0, st>>>(1, d_cdim, d_czero, Lcc_d, d_czero, t2_d, u, 1);
 }
 
 // q = (F_rr + G S_cc^-1 G^T) p, part = per-block partials of p . q
@@ -1812,9 +1913,9 @@ void FetiDP::apply_F(const double* p, double* q, double* part) {
   const int64_t ne = P.dual_off[P.n_parts];
   RhsDev R{phi_d, d_roff_s, d_ncol_s, d_voff_s, vs_d};
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, p, w_d);
-  const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
-  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
-  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
+  const dim3 gr(static_cast<unsigned>((max_nD + gemv_warps - 1) / gemv_warps), static_cast<unsigned>(n_roots));
+  k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
+  k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
   if (P.n_coarse > 0) {
     k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
         P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, nullptr, t_d);
@@ -1839,13 +1940,13 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     k_dot_part<<<kParts, 256, 0, st>>>(P.n_lambda, r, z, part);
     return;
   }
-  const dim3 gr(static_cast<unsigned>((max_nD + 7) / 8), static_cast<unsigned>(n_roots));
+  const dim3 gr(static_cast<unsigned>((max_nD + gemv_warps - 1) / gemv_warps), static_cast<unsigned>(n_roots));
   if (precond >= 2 && P.n_faces > 0) {  // 4: the Dirichlet part of deluxe + learned
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
     if (precond == 3) {
       k_face_w<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
           fc, d_lam_entry, fDaT32_d, fDbT32_d, r, w_d);
-      k_block_colgemv<float><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S32_d, d_rvoff, w_d, y_d, 2);
+      k_block_colgemv<float><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S32_d, d_rvoff, w_d, y_d, 2);
       k_face_c<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
           fc, d_lam_entry, fDa32_d, fDb32_d, y_d, c_d);
       k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
@@ -1853,14 +1954,14 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     }
     k_face_w<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fX_d,
                                                                                           fXt_d, r, w_d);
-    k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+    k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
     k_face_c<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
                                                                                   y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, wt_d, r, w_d);
-  k_block_colgemv<double><<<gr, 256, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+  k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
   k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, wt_d, y_d, z, r, part);
 }
 
@@ -2012,7 +2113,38 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   EMG_CK(cudaEventSynchronize(ev.b));
   stats.factor_ms = ev.ms();
   factored = true;
+  if (!tuned) {  // once per solver, after its first factorization (not in factor_ms)
+    tuned = true;
+    tune_solve_kernels();
+  }
   return EMG_SUCCESS;
+}
+
+// CTA widths of the solve kernels, chosen by the autotuner on this plan's
+// shape (tune.h): the pivot-block and update-row kernels of the front
+// solves (a single-column solve into scratch vectors) and the dense column
+// dots of the multiplier iteration (an S_DD pass).  The values of the
+// vectors do not matter for the timing; the kernels read and write only the
+// solver's own scratch.
+void FetiDP::tune_solve_kernels() {
+  const std::string key = "u" + std::to_string(plan.n_union) + "f" + std::to_string(plan.fronts.size()) + "s" +
+                          std::to_string(plan.n_parts);
+  RhsDev R1{xu_d, d_roff1, d_ncol1, d_voff1, v1_d};
+  const int32_t saved_upd = upd_rows;
+  piv_threads = tune::pick("feti.front_pivot_threads", key, {512, 256, 1024}, [&](int v, cudaStream_t) {
+    piv_threads = v;
+    solve_fronts(R1, 1);
+  }, st);
+  upd_rows = tune::pick("feti.front_update_rows", key, {saved_upd, 128, 512}, [&](int v, cudaStream_t) {
+    upd_rows = v;
+    solve_fronts(R1, 1);
+  }, st);
+  if (n_roots > 0)
+    gemv_warps = tune::pick("feti.dense_column_warps", key, {8, 4, 16}, [&](int v, cudaStream_t) {
+      const dim3 gr(static_cast<unsigned>((max_nD + v - 1) / v), static_cast<unsigned>(n_roots));
+      k_block_colgemv<double><<<gr, 32 * v, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+    }, st);
+  cudaGetLastError();
 }
 
 // Right-hand side of the multiplier system for the union right-hand side fu:

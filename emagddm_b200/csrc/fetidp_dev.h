@@ -75,6 +75,9 @@ struct FetiDP {
   FacesDev fc{};
   bool factored = false;
   bool tc_factor = false;  // factor contractions on the TF32 tensor cores (EMG_FLAG_FACTOR_TF32)
+  // CTA widths of the solve kernels (autotuned after the first factorization)
+  int32_t piv_threads = 512, upd_rows = 256, gemv_warps = 8;
+  bool tuned = false;
   int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks,
                         // 4 deluxe + learned correction (flexible CG)
   FetiStats stats;
@@ -101,6 +104,7 @@ struct FetiDP {
   int64_t coarse_fac = 0;
   // extra fronts after the plan's: [0] the coarse matrix, [1 + f] face f's S_a + S_b
   std::vector<int32_t> xnp;
+  std::vector<int32_t> lvl_max_np, lvl_max_nu;  // per level, non-root fronts: largest pivot / update counts
   int32_t max_fdim = 0;
   // solve layouts
   int64_t *d_roff_s = nullptr, *d_roff1 = nullptr, *d_voff_s = nullptr, *d_voff1 = nullptr;
@@ -160,6 +164,7 @@ struct FetiDP {
   void apply_M(const double* r, double* z, double* part);
   int dot(const double* a, const double* b, int64_t n, int which);
   int setup_deluxe();
+  void tune_solve_kernels();
   int trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off, double* X);
   int prepare_rhs(const double* fu);
   int lambda_pcg(double tol, int32_t max_it, int32_t* iters, double* rel);

@@ -32,6 +32,7 @@
 
 #include "common.cuh"
 #include "device.h"
+#include "tune.h"
 #include "sell_tma.cuh"
 #include "trace.h"
 
@@ -76,6 +77,7 @@ struct Sell {
   int32_t* src = nullptr;        // CSR index of every slot, -1 = padding
   double* val = nullptr;
   uint64_t version = ~uint64_t(0);
+  int grid = 0;                  // autotuned grid of the register-pipeline SpMV kernels (0: one resident wave)
 };
 
 struct KrylovWorkspace {
@@ -1351,6 +1353,14 @@ int resident_grid(int g) {
 #endif
 }
 
+// The SpMV grid: one resident wave, or the autotuned grid of the matrix when
+// it is smaller (tune_sell_grid).
+template <auto Kernel>
+int sell_grid(const Sell& S, int g) {
+  const int r = resident_grid<Kernel>(g);
+  return S.grid > 0 && S.grid < r ? S.grid : r;
+}
+
 int grid_size() {
   static int g = 0;
   if (!g) {
@@ -1498,10 +1508,14 @@ int build_sell(DevCsr& A, cudaStream_t st) {
   return EMG_SUCCESS;
 }
 
+void tune_sell_grid(DevCsr& A, cudaStream_t st);
+
 int ensure_sell(DevCsr& A, cudaStream_t st) {
+  bool fresh = false;
   if (!A.sell) {
     int rc = build_sell(A, st);
     if (rc) return rc;
+    fresh = true;
   }
   Sell& S = *A.sell;
   if (S.version != A.version) {
@@ -1509,6 +1523,7 @@ int ensure_sell(DevCsr& A, cudaStream_t st) {
     EMG_CK(cudaGetLastError());
     S.version = A.version;
   }
+  if (fresh && A.ws) tune_sell_grid(A, st);
   return EMG_SUCCESS;
 }
 
@@ -1765,9 +1780,9 @@ int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
       KERNEL<2><<<sh_.grid, kThreads, sh_.smem, st>>>(__VA_ARGS__);                   \
     } else if (EMG_WS_LAUNCH(KERNEL, S, st, __VA_ARGS__)) {                           \
     } else if ((S).narrow) {                                                          \
-      KERNEL<1><<<resident_grid<KERNEL<1>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
+      KERNEL<1><<<sell_grid<KERNEL<1>>(S, g), kThreads, 0, st>>>(__VA_ARGS__);         \
     } else {                                                                          \
-      KERNEL<0><<<resident_grid<KERNEL<0>>(g), kThreads, 0, st>>>(__VA_ARGS__);       \
+      KERNEL<0><<<sell_grid<KERNEL<0>>(S, g), kThreads, 0, st>>>(__VA_ARGS__);         \
     }                                                                                 \
   } while (0)
 
@@ -1777,6 +1792,27 @@ int capture_loop(DevCsr& A, bool bicg, cudaGraphExec_t* out) {
 #else
 #define EMG_WS_LAUNCH(KERNEL, S, st, ...) false
 #endif
+
+// Blocks per SM of the register-pipeline SpMV (the SELL kernel without the
+// solver's dot product, whose loads and occupancy are the same), chosen by
+// the autotuner for this matrix shape: one resident wave (the default) or
+// one or two blocks per SM fewer, timed on the matrix itself.
+void tune_sell_grid(DevCsr& A, cudaStream_t st) {
+  Sell& S = *A.sell;
+  if (S.tma || S.ws) return;
+  const int g = grid_size(), sms = num_sms();
+  const int r = S.narrow ? resident_grid<k_spmv<1>>(g) : resident_grid<k_spmv<0>>(g);
+  std::vector<int> cand{r};
+  for (int d = 1; d <= 2; ++d)
+    if (r - d * sms >= sms) cand.push_back(r - d * sms);
+  int32_t* err = &A.ws->state->copy_err;
+  const std::string key = "n" + std::to_string(A.n) + "slots" + std::to_string(S.slots);
+  S.grid = tune::pick("sell.spmv_grid", key, cand, [&](int v, cudaStream_t s) {
+    if (S.narrow) k_spmv<1><<<v, kThreads, 0, s>>>(S, A.ws->p, A.ws->q, err);
+    else k_spmv<0><<<v, kThreads, 0, s>>>(S, A.ws->p, A.ws->q, err);
+  }, st);
+  cudaGetLastError();
+}
 
 void launch_iterations(DevCsr& A, bool bicg, int count) {
   KrylovWorkspace& w = *A.ws;

@@ -415,6 +415,20 @@ int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg,
  * b = ones, each launch bracketed by CUDA events on `stream`. */
 int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms);
 
+/* ---- Launch-configuration autotuner (no counterpart in the reference) ----
+ * The library times candidate launch configurations of some kernels on the
+ * device the first time it meets a problem shape and keeps the fastest:
+ * the grid of the SELL SpMV of each matrix, and the CTA widths of the
+ * FETI-DP / direct solve kernels after a solver's first factorization.
+ * Tuning is on by default (EMG_TUNE=0 in the environment turns it off:
+ * built-in defaults); EMG_TUNE_CACHE=<file> keeps the decisions between
+ * processes.  emg_tune_enable switches it for the rest of the process. */
+int emg_tune_enable(int32_t on);
+/* The decisions so far as JSON ({"family|shape": {"value": v,
+ * "candidates_ms": {...}}}) into buf (cap bytes, NUL-terminated); returns the
+ * length needed including the NUL. */
+int32_t emg_tune_report(char* buf, int32_t cap);
+
 /* Test hook (no counterpart in the reference): polls a block of the fused
  * CG update makes at its grid barrier before giving up (default 2^21, about
  * 0.2 s or more; a negative value restores it) on the current device.  A
