@@ -61,8 +61,11 @@ def parse():
     ap.add_argument("--eval-fields", type=int, default=50, help="learned64: held-out fields (seeds 2000+)")
     ap.add_argument("--feti-precond", type=int, default=2,
                     help="fetidp64: 2 deluxe (FP64 blocks), 3 deluxe with FP32 blocks (mixed precision)")
-    ap.add_argument("--feti-variants", default=",".join(["fp64", "fp32_precond", "tf32_factor",
-                                                           "tf32_factor_fp32_precond"]),
+    ap.add_argument("--ns-train-fields", type=int, default=12,
+                    help="cube64 north-star comparison: training fields of the learned preconditioner")
+    ap.add_argument("--ns-eval-fields", type=int, default=3,
+                    help="cube64 north-star comparison: held-out fields of the learned preconditioner")
+    ap.add_argument("--feti-variants", default=",".join(["fp64", "fp32_precond", "tf32_factor"]),
                     help="cube64 north-star comparison: FETI-DP variants to time (comma-separated)")
     ap.add_argument("--mixed", action="store_true",
                     help="fetidp64: mixed-precision factor (TF32 tensor-core contractions, FP64 refinement)")
@@ -400,7 +403,8 @@ def run_ours(args, rank, world, local_rank):
                    "median_step_ms": {a: statistics.median(step_ms[a]) for a in ("resident", "e2e")},
                    "solver_format": {"kind": "SELL-32-sigma4096", "slots": slots.value,
                                      "padding": slots.value / nnz - 1.0},
-                   "host_cpus": host_binding},
+                   "host_cpus": host_binding,
+                   "autotune": _abi.tune_report()},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h_x.nbytes), "ms_per_step": total_e2e / args.steps,
@@ -538,17 +542,24 @@ def run_batch(args, rank, world, local_rank):
         info["res"] = res
         del S
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local_rank) as clk:
+    def timed_steps():
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / args.steps
+
+    # the built-in launch configuration first (autotuner off), then the tuned one
+    L.emg_tune_enable(0)
+    ms_default = timed_steps()
+    L.emg_tune_enable(1)
+    with Clocks(local_rank) as clk:
+        ms = timed_steps()
     iters = [r["iterations"] for r in info["res"]]
     # plain path: the same instances one at a time (a sample, projected)
     sample = list(range(0, len(inst), max(1, len(inst) // 16)))
@@ -601,7 +612,9 @@ def run_batch(args, rank, world, local_rank):
                    "batched_vs_plain": value / world / (1e3 / plain_per_inst_ms),
                    "oracle_rel_error_sample_max": max(errs), "oracle_rel_error_sample_median": float(np.median(errs)),
                    "oracle_sample": len(errs), "oracle_sample_instances": "every 16th (0, 16, ..., 496)",
-                   "oracle_ms": oracle_ms, "oracle_threads": O.num_threads()},
+                   "oracle_ms": oracle_ms, "oracle_threads": O.num_threads(),
+                   "autotune": {"decisions": _abi.tune_report(), "ms_per_step_default": ms_default,
+                                "ms_per_step_tuned": ms, "tuned_vs_default": ms_default / ms}},
         "clocks": clk.summary(),
     }
 
@@ -707,7 +720,7 @@ def north_star(args, local_rank):
     Jacobi-PCG solve to 1e-12."""
     import torch
 
-    from emagddm_b200 import fetidp, mesh
+    from emagddm_b200 import _abi, fetidp, mesh
     from oracle import oracle as O
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream(dev)
@@ -729,6 +742,8 @@ def north_star(args, local_rank):
     pcg, sols = pcg_same_gauge(m, fd.map.l2g, n_dofs, (TOL, 1e-12), dev)
     orp, ocol, okv, _, orhs = O.assemble(m, fd.map.l2g, n_dofs)
     r = orhs - O.spmv(orp, ocol, okv, x_feti)
+    del fd
+    learned = north_star_learned(args, local_rank) if args.ns_train_fields > 0 else None
     plain_fetidp = var["fp64"]["ms"]
     plain_pcg = pcg[f"{TOL:g}"]["ms"]
     best = min(timed, key=lambda k: timed[k]["ms"])
@@ -737,16 +752,57 @@ def north_star(args, local_rank):
                     "tree gauge, time to a true FP64 relative residual of 1e-8",
         "dofs": n_dofs, "n_lambda": info["n_lambda"], "n_coarse": info["n_coarse"],
         "setup_host_ms": setup_ms, "fetidp": var, "plain_pcg_same_gauge": pcg,
+        "learned": learned,
+        "combination": "mixed factor + learned + graph loop: not run, the mixed-precision factor does not converge "
+                       "at 64^3 (fetidp.tf32_factor above)",
         "best": best, "best_ms": var[best]["ms"],
         "speedup_vs_plain_fetidp": plain_fetidp / var[best]["ms"],
         "speedup_vs_plain_pcg": plain_pcg / var[best]["ms"],
         "plain_fetidp_vs_plain_pcg": plain_pcg / plain_fetidp,
         "target": "additions >= 5x faster than the plain GPU FETI-DP/PCG path",
+        "autotune": _abi.tune_report(),
         "oracle": {"true_residual_on_oracle_matrix": float(np.linalg.norm(r) / np.linalg.norm(orhs)),
                    "rel_diff_vs_gpu_pcg_1e-12": rel_err(x_feti, sols[1e-12]),
                    "what": "FP64 FETI-DP solution: residual on the CPU oracle's own assembly of the partition-"
                            "gauged system, and difference from the GPU Jacobi-PCG solution to 1e-12"},
     }
+
+
+def north_star_learned(args, local_rank):
+    """The learned interface preconditioner on its own configuration (64^3,
+    64 jittered boxes, random log-normal mu_r fields, curl-T sources), with a
+    reduced training set so that it fits the default run: training pairs from
+    `ns_train_fields` fields (seeds 1000+), 20 epochs, then `ns_eval_fields`
+    held-out fields (seeds 2000+) solved with deluxe alone and deluxe +
+    learned (flexible CG) to a true residual of 1e-8."""
+    import torch
+
+    from emagddm_b200 import learned
+    t0 = time.perf_counter()
+    tr = learned.Trainer(n=64, parts=4, seed=1)
+    R, T = [], []
+    for k in range(args.ns_train_fields):
+        r, t = tr.pairs(np.random.default_rng(1000 + k), per_solve=8, stride=3)
+        R += r
+        T += t
+    losses = tr.train(R, T, epochs=20, batch=32, lr=1e-3)
+    torch.cuda.synchronize()
+    prep_ms = (time.perf_counter() - t0) * 1e3
+    rows = []
+    for k in range(args.ns_eval_fields):
+        o = tr.evaluate(np.random.default_rng(2000 + k), tol=TOL)
+        rows.append((o[2]["iterations"], o[4]["iterations"], o[2]["ms"], o[4]["ms"], o[2]["residual"],
+                     o[4]["residual"], o[2]["status"], o[4]["status"]))
+    a = np.array(rows, dtype=float)
+    return {"what": "deluxe vs deluxe + learned MLP correction (flexible CG), random mu_r fields; reduced training "
+                    "set (the learned64 workload trains on 200 fields)",
+            "train_fields": args.ns_train_fields, "pairs": len(R), "eval_fields": args.ns_eval_fields,
+            "prep_ms": prep_ms, "loss_first_last": [losses[0], losses[-1]],
+            "iterations_mean": {"deluxe": a[:, 0].mean(), "deluxe_plus_learned": a[:, 1].mean()},
+            "solve_ms_mean": {"deluxe": a[:, 2].mean(), "deluxe_plus_learned": a[:, 3].mean()},
+            "true_residual_max": {"deluxe": a[:, 4].max(), "deluxe_plus_learned": a[:, 5].max()},
+            "all_converged": bool((a[:, 6] == 0).all() and (a[:, 7] == 0).all()),
+            "learned_vs_deluxe_time": a[:, 2].mean() / a[:, 3].mean()}
 
 
 def run_fetidp(args, rank, world, local_rank):
@@ -761,13 +817,22 @@ def run_fetidp(args, rank, world, local_rank):
     from emagddm_b200 import fetidp, mesh
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    from emagddm_b200 import _abi
     m = workload(args.n)
     part = mesh.jittered_partition(m, args.parts)
+    stream = torch.cuda.current_stream(dev)
+    default = None
+    if not args.mixed:  # the built-in solve-kernel widths (autotuner off) on a solver of their own
+        _abi.lib().emg_tune_enable(0)
+        fd0 = fetidp.FetiDP(m, part, args.parts ** 3)
+        default = fetidp_variants(fd0, ["fp64"], steps=args.steps, warmup=args.warmup, stream=stream, dev=dev)["fp64"]
+        default.pop("_x", None)
+        del fd0
+        _abi.lib().emg_tune_enable(1)
     t0 = time.perf_counter()
     fd = fetidp.FetiDP(m, part, args.parts ** 3)
     setup_ms = (time.perf_counter() - t0) * 1e3
     info = fd.info()
-    stream = torch.cuda.current_stream(dev)
     name = {(2, 0): "fp64", (3, 0): "fp32_precond", (2, 1): "tf32_factor",
             (3, 1): "tf32_factor_fp32_precond"}.get((args.feti_precond, int(args.mixed)))
     if name is None:
@@ -797,7 +862,11 @@ def run_fetidp(args, rank, world, local_rank):
                    "device_gb": 8e-9 * (info["factor_doubles"] + info["update_pool_doubles"]
                                         + 2 * info["dual_block_doubles"]),
                    "plain_pcg_same_gauge": pcg, "rel_diff_vs_pcg_1e-12": rel_err(x, sols[1e-12]),
-                   "fetidp_vs_plain_pcg": pcg[f"{TOL:g}"]["ms"] / ms},
+                   "fetidp_vs_plain_pcg": pcg[f"{TOL:g}"]["ms"] / ms,
+                   "autotune": {"decisions": _abi.tune_report(),
+                                "default_widths": {k: default[k] for k in ("ms", "factor_ms", "solve_ms",
+                                                                           "solve_phases_ms")} if default else None,
+                                "tuned_vs_default": default["ms"] / ms if default else None}},
         "clocks": clk.summary(),
     }
 
