@@ -84,7 +84,7 @@ __global__ void k_front_scatter(FrontsDev F, int32_t f0, const int64_t* __restri
                                 const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
                                 const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
                                 const double* __restrict__ val, double* __restrict__ fac,
-                                int32_t* __restrict__ err) {
+                                double* __restrict__ diag0, int32_t* __restrict__ err) {
   const int32_t k = f0 + blockIdx.y;
   const int32_t lane = threadIdx.x & 31;
   const int32_t a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -103,6 +103,7 @@ __global__ void k_front_scatter(FrontsDev F, int32_t f0, const int64_t* __restri
     const int32_t pj = j < p0 + np ? j - p0 : find_row(rows, fs, j);
     if (pj < 0) { atomicOr(err, kErrAsm); continue; }
     col_a[pj] = val[q];
+    if (j == i) diag0[u] = val[q];  // the pivot test of k_potrf_diag is relative to it
   }
 }
 
@@ -151,14 +152,26 @@ __global__ void k_copy_roots(FrontsDev F, int32_t f0, const int64_t* __restrict_
 
 // ----------------------------------------------------- partial Cholesky
 
+// Pivots below kPivRel times the matrix's own diagonal entry (a condition
+// number beyond 1e11: numerically singular in FP64) count as breakdowns, as
+// do non-positive ones; the singular systems of an ungauged curl-curl
+// problem leave round-off-sized pivots of either sign.
+constexpr double kPivRel = 1e-11;
+
 // Diagonal block [k0, k0+nb) of every front in the range with npiv > k0.
+// diag0 (null for the coarse matrix and the face sums) holds the original
+// diagonal of the subdomain matrices in union numbering.
 __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
+                                                    const double* __restrict__ diag0,
+                                                    const int64_t* __restrict__ loc_off, int32_t n_plan,
                                                     int32_t* __restrict__ err) {
   __shared__ double D[kNB][kNB + 1];
   __shared__ double piv;
   const int32_t k = f0 + blockIdx.x;
   const int32_t np = F.npiv[k];
   if (k0 >= np) return;
+  const bool rel = diag0 != nullptr && k < n_plan;
+  const int64_t u0 = rel ? loc_off[F.sub[k]] + F.p0[k] + k0 : 0;
   const int32_t nb = min(kNB, np - k0), fs = F.f[k];
   double* A = fac + F.fac[k] + k0 + static_cast<int64_t>(k0) * fs;
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
@@ -169,7 +182,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int
   for (int c = 0; c < nb; ++c) {
     if (threadIdx.x == 0) {
       double d = D[c][c];
-      if (!(d > 0.0)) { atomicOr(err, kErrPivot); d = 1.0; }
+      if (!(d > 0.0) || (rel && !(d > kPivRel * fabs(diag0[u0 + c])))) { atomicOr(err, kErrPivot); d = 1.0; }
       piv = sqrt(d);
       D[c][c] = piv;
     }
@@ -782,8 +795,11 @@ __global__ void __launch_bounds__(kPivMax) k_front_fwd_piv(FrontsDev F, int32_t 
 }
 
 // Forward, update rows: V[i - np] -= sum_j L[i, j] y_j for the rows
-// np .. fs-1, one row per thread (grid: row chunk, front, column); the
-// pivot values are staged in shared memory.
+// np .. fs-1, one row per thread, up to kColB right-hand-side columns per CTA
+// so that L21 is read once per kColB columns (grid: row chunk, front, column
+// group); the pivot values of the group are staged in shared memory.
+constexpr int kColB = 8;
+constexpr int kXChunkB = kXChunk / kColB;
 __global__ void __launch_bounds__(kUpdMax) k_front_fwd_upd(FrontsDev F, int32_t f0, RhsDev R,
                                                             const int32_t* __restrict__ nI,
                                                             const int32_t* __restrict__ nD,
@@ -791,41 +807,58 @@ __global__ void __launch_bounds__(kUpdMax) k_front_fwd_upd(FrontsDev F, int32_t 
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
-  const int32_t col = blockIdx.z;
-  if (col >= R.ncol[s]) return;
+  const int32_t c0 = blockIdx.z * kColB;
+  const int32_t nc = min(kColB, R.ncol[s] - c0);
+  if (nc <= 0) return;
   const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
   const int32_t r0 = blockIdx.x * blockDim.x;
   if (r0 >= nu || np == 0) return;
-  __shared__ double xs[kXChunk];
+  __shared__ double xs[kColB][kXChunkB];
   const int32_t ld = nI[s] + nD[s];
-  const double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
-  double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
+  const double* x = R.x + R.off[s] + static_cast<int64_t>(c0) * ld;
+  double* V = R.v + R.voff[k] + static_cast<int64_t>(c0) * nu;
   const int32_t i = np + r0 + threadIdx.x;
   const bool live = i < fs;
   const double* L = fac + F.fac[k] + (live ? i : np);
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  for (int32_t c0 = 0; c0 < np; c0 += kXChunk) {
-    const int32_t cw = min(kXChunk, np - c0);
+  double acc[kColB];
+#pragma unroll
+  for (int c = 0; c < kColB; ++c) acc[c] = 0.0;
+  for (int32_t j0 = 0; j0 < np; j0 += kXChunkB) {
+    const int32_t jw = min(kXChunkB, np - j0);
     __syncthreads();
-    for (int32_t e = threadIdx.x; e < cw; e += blockDim.x) xs[e] = x[p0 + c0 + e];
+    for (int32_t e = threadIdx.x; e < nc * jw; e += blockDim.x) {
+      const int32_t c = e / jw, j = e - c * jw;
+      xs[c][j] = x[static_cast<int64_t>(c) * ld + p0 + j0 + j];
+    }
     __syncthreads();
     if (live) {
-      const double* Lc = L + static_cast<int64_t>(c0) * fs;
+      const double* Lc = L + static_cast<int64_t>(j0) * fs;
       int32_t j = 0;
-      for (; j + 3 < cw; j += 4) {
-        a0 = fma(Lc[static_cast<int64_t>(j) * fs], xs[j], a0);
-        a1 = fma(Lc[static_cast<int64_t>(j + 1) * fs], xs[j + 1], a1);
-        a2 = fma(Lc[static_cast<int64_t>(j + 2) * fs], xs[j + 2], a2);
-        a3 = fma(Lc[static_cast<int64_t>(j + 3) * fs], xs[j + 3], a3);
+      for (; j + 3 < jw; j += 4) {  // four loads of L in flight
+        const double l0 = Lc[static_cast<int64_t>(j) * fs], l1 = Lc[static_cast<int64_t>(j + 1) * fs];
+        const double l2 = Lc[static_cast<int64_t>(j + 2) * fs], l3 = Lc[static_cast<int64_t>(j + 3) * fs];
+#pragma unroll
+        for (int c = 0; c < kColB; ++c)
+          if (c < nc)
+            acc[c] = fma(l3, xs[c][j + 3], fma(l2, xs[c][j + 2], fma(l1, xs[c][j + 1], fma(l0, xs[c][j], acc[c]))));
       }
-      for (; j < cw; ++j) a0 = fma(Lc[static_cast<int64_t>(j) * fs], xs[j], a0);
+      for (; j < jw; ++j) {
+        const double l = Lc[static_cast<int64_t>(j) * fs];
+#pragma unroll
+        for (int c = 0; c < kColB; ++c)
+          if (c < nc) acc[c] = fma(l, xs[c][j], acc[c]);
+      }
     }
   }
-  if (live) V[i - np] -= (a0 + a1) + (a2 + a3);
+  if (live)
+#pragma unroll
+    for (int c = 0; c < kColB; ++c)
+      if (c < nc) V[static_cast<int64_t>(c) * nu + (i - np)] -= acc[c];
 }
 
 // Backward, update rows: x_j -= sum_{i >= np} L[i, j] x[row i] for every
-// pivot column j, a warp per column (grid: column chunk, front, rhs column).
+// pivot column j, a warp per column and up to kColB right-hand-side columns
+// per warp (grid: column chunk, front, column group).
 __global__ void __launch_bounds__(256) k_front_bwd_upd(FrontsDev F, int32_t f0, RhsDev R,
                                                        const int32_t* __restrict__ nI,
                                                        const int32_t* __restrict__ nD,
@@ -833,25 +866,32 @@ __global__ void __launch_bounds__(256) k_front_bwd_upd(FrontsDev F, int32_t f0, 
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
-  const int32_t col = blockIdx.z;
-  if (col >= R.ncol[s]) return;
+  const int32_t c0 = blockIdx.z * kColB;
+  const int32_t nc = min(kColB, R.ncol[s] - c0);
+  if (nc <= 0) return;
   const int lane = threadIdx.x & 31;
   const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
   const int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (j >= np || fs == np) return;
   const int32_t ld = nI[s] + nD[s];
-  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  double* x = R.x + R.off[s] + static_cast<int64_t>(c0) * ld;
   const int32_t* rows = F.rows_v + F.rows[k];
   const double* Lj = fac + F.fac[k] + static_cast<int64_t>(j) * fs;
-  double a0 = 0.0, a1 = 0.0;
-  int32_t i = np + lane;
-  for (; i + 32 < fs; i += 64) {
-    a0 = fma(Lj[i], x[rows[i]], a0);
-    a1 = fma(Lj[i + 32], x[rows[i + 32]], a1);
+  double acc[kColB];
+#pragma unroll
+  for (int c = 0; c < kColB; ++c) acc[c] = 0.0;
+  for (int32_t i = np + lane; i < fs; i += 32) {
+    const double l = Lj[i];
+    const int32_t r = rows[i];
+#pragma unroll
+    for (int c = 0; c < kColB; ++c)
+      if (c < nc) acc[c] = fma(l, x[static_cast<int64_t>(c) * ld + r], acc[c]);
   }
-  if (i < fs) a0 = fma(Lj[i], x[rows[i]], a0);
-  const double acc = warp_sum(a0 + a1);
-  if (lane == 0) x[p0 + j] -= acc;
+#pragma unroll
+  for (int c = 0; c < kColB; ++c) {
+    const double a = warp_sum(acc[c]);
+    if (lane == 0 && c < nc) x[static_cast<int64_t>(c) * ld + p0 + j] -= a;
+  }
 }
 
 // Backward, pivot block: per 32-pivot panel (last first) the warps form the
@@ -977,7 +1017,7 @@ __global__ void k_mirror_lower(int32_t n_mat, const int32_t* __restrict__ dim, c
 // scalar head up to the first aligned element), four vectors in flight per
 // lane; w, which every column of the block reads, stays in L1/L2.
 template <class T>
-__global__ void __launch_bounds__(256) k_block_colgemv(int32_t n_mat, const int32_t* __restrict__ dim,
+__global__ void __launch_bounds__(512) k_block_colgemv(int32_t n_mat, const int32_t* __restrict__ dim,
                                                        const int64_t* __restrict__ m_off,
                                                        const T* __restrict__ M,
                                                        const int64_t* __restrict__ v_off,
@@ -1724,6 +1764,7 @@ int FetiDP::setup_device() {
       (rc = zalloc(&v1_d, P.vec_rows)) || (rc = zalloc(&cblk_d, P.cblk_off[S])) ||
       (rc = zalloc(&h_d, P.pri_off[S])) || (rc = zalloc(&gc_d, nc)) || (rc = zalloc(&uc_d, nc)) ||
       (rc = zalloc(&t_d, nc)) || (rc = zalloc(&t2_d, nc)) || (rc = zalloc(&rho_d, nd)) ||
+      (rc = zalloc(&diag0_d, P.n_union)) ||
       (rc = zalloc(&wt_d, nd)) || (rc = zalloc(&w_d, nd)) || (rc = zalloc(&y_d, nd)) || (rc = zalloc(&y2_d, nd)) ||
       (rc = zalloc(&xu_d, P.n_union)) || (rc = zalloc(&ru_d, P.n_union)) || (rc = zalloc(&xg_d, P.n_dofs)) ||
       (rc = zalloc(&rg_d, P.n_dofs)) || (rc = zalloc(&bg_d, P.n_dofs)) || (rc = zalloc(&lam_d, nl)) ||
@@ -1748,7 +1789,8 @@ int FetiDP::check_err(const char* where) {
   EMG_CK(cudaStreamSynchronize(st));
   EMG_CK(cudaGetLastError());
   if (e & kErrPivot) {
-    set_error(std::string(where) + ": non-positive pivot (a subdomain matrix is not positive definite)");
+    set_error(std::string(where) + ": non-positive or vanishing pivot (a subdomain matrix is singular or not "
+                                    "positive definite)");
     return EMG_NUMERICAL_ERROR;
   }
   if (e & kErrTc) {
@@ -1807,7 +1849,7 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
       mnp = npk[0];
     }
     if (active == 0) break;
-    k_potrf_diag<<<active, 256, 0, st>>>(fd, f0, k0, fac_d, err_d);
+    k_potrf_diag<<<active, 256, 0, st>>>(fd, f0, k0, fac_d, diag0_d, d_loc_off, F, err_d);
     const int32_t rows = mf - k0 - 1;
     if (rows > 0) {
       const unsigned rb = static_cast<unsigned>((rows + kTrsmRows - 1) / kTrsmRows);
@@ -1867,13 +1909,14 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
       }
   }
   const unsigned nc = static_cast<unsigned>(ncol);
+  const unsigned ngroups = static_cast<unsigned>((ncol + kColB - 1) / kColB);
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0) continue;  // (a front without pivots still gathers its children)
     k_front_fwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
     if (lvl_max_nu[h] > 0)
       k_front_fwd_upd<<<dim3(static_cast<unsigned>((lvl_max_nu[h] + upd_rows - 1) / upd_rows),
-                             static_cast<unsigned>(nf), nc),
+                             static_cast<unsigned>(nf), ngroups),
                         upd_rows, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
   }
   if (n_roots > 0) {
@@ -1890,8 +1933,8 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0 || lvl_max_np[h] == 0) continue;
     if (lvl_max_nu[h] > 0)
-      k_front_bwd_upd<<<dim3(static_cast<unsigned>((lvl_max_np[h] + 7) / 8), static_cast<unsigned>(nf), nc), 256, 0,
-                        st>>>(fd, f0, R, d_nI, d_nD, fac_d);
+      k_front_bwd_upd<<<dim3(static_cast<unsigned>((lvl_max_np[h] + 7) / 8), static_cast<unsigned>(nf), ngroups), 256,
+                        0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
     k_front_bwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
   }
   EMG_CK(cudaGetLastError());
@@ -2058,7 +2101,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     }
     k_front_zero<<<dim3(blocks_for(max_el, 256, 512), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
     k_front_scatter<<<dim3(static_cast<unsigned>((max_np + 7) / 8), nf), 256, 0, st>>>(
-        fd, f0, d_loc_off, d_nI, d_nD, rp, cl, vl, fac_d, err_d);
+        fd, f0, d_loc_off, d_nI, d_nD, rp, cl, vl, fac_d, diag0_d, err_d);
     for (int32_t slot = 0; slot < max_ch; ++slot)
       k_extend_add<<<dim3(blocks_for(max_cu, 256, 512), nf), 256, 0, st>>>(fd, f0, slot, fac_d, upd_d);
     if (max_root > 0)

@@ -123,6 +123,7 @@ struct FetiDP {
   double *fu_d = nullptr, *xacc_d = nullptr, *rglob_d = nullptr, *root_tmp_d = nullptr;
   double *rold_d = nullptr, *zm_d = nullptr;  // flexible CG
   double *fp_d = nullptr, *fq_d = nullptr, *fr0_d = nullptr;  // global flexible CG (mixed factor)
+  double* diag0_d = nullptr;  // original diagonal of the subdomain matrices (union numbering), pivot scale
   // FP32 copies of the preconditioner blocks (mixed-precision mode)
   float *S32_d = nullptr, *fDa32_d = nullptr, *fDb32_d = nullptr, *fDaT32_d = nullptr, *fDbT32_d = nullptr;
   void* state_d = nullptr;

@@ -60,3 +60,23 @@ def test_grid_barrier_wait_runs_out_with_timeout_status():
     rp, col, kv, _, rhs = oracle_system(m, l2g)
     _, st, it, _ = O.pcg(rp, col, kv, rhs, tol=1e-8, max_iter=5000)
     assert abs(out.iterations - it) <= max(3, 0.15 * it)
+
+
+def test_singular_system_factor_reports_numerical_error():
+    """The direct backend on the ungauged curl-curl system (GAUGE_NONE: the
+    discrete gradients of the interior nodes are in the kernel of K): the
+    multifrontal Cholesky meets round-off-sized pivots and reports
+    NUMERICAL_ERROR instead of returning a NaN or garbage solution; a solve
+    without a successful factorization is INVALID_INPUT."""
+    from emagddm_b200 import fetidp
+    m = mesh.plain_scale(6)
+    ds = fetidp.DirectSolver(m, gauge=_abi.GAUGE_NONE)
+    assert ds.factor() == _abi.EMG_NUMERICAL_ERROR
+    assert b"pivot" in lib().emg_last_error()
+    _, rc, _ = ds.solve()
+    assert rc == _abi.EMG_INVALID_INPUT
+    # the same mesh gauged is regular: the factor succeeds and solves
+    ok = fetidp.DirectSolver(m)
+    assert ok.factor() == 0
+    _, rc, out = ok.solve(tol=1e-12)
+    assert rc == 0 and out.residual_norm < 1e-12
