@@ -1549,6 +1549,8 @@ void FetiDP::release() {
   if (!dev.empty()) cudaStreamSynchronize(st);
   for (cudaGraphExec_t& g : lam_exec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (cudaGraphExec_t& g : fac_exec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   if (cap_st) { cudaStreamDestroy(cap_st); cap_st = nullptr; }
   for (void* p : dev) cudaFree(p);
   dev.clear();
@@ -1829,12 +1831,12 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
     if (k > f0 && npk[k - f0] > npk[k - f0 - 1]) sorted = false;
   }
   unsigned active = nf;
-  if (kTrsmSmem > 48 * 1024)
+  if (kTrsmSmem > 48 * 1024 && !capturing)  // (set by the eager factorization before any capture)
     EMG_CK(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kTrsmSmem)));
   // mixed precision: the subdomain fronts' contractions on the TF32 tensor cores
   const bool tc_here = tc_factor && f1 <= F;
-  if (tc_here) {
+  if (tc_here && !capturing) {
     EMG_CK(cudaFuncSetAttribute(k_syrk_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc::kSmemBytes)));
     EMG_CK(cudaFuncSetAttribute(k_update_pivcols_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1884,8 +1886,9 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
 int FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
                   double* X) {
   if (n_mat == 0 || max_n == 0) return EMG_SUCCESS;
-  EMG_CK(cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(kTrtriSmem)));
+  if (!capturing)
+    EMG_CK(cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kTrtriSmem)));
   k_trtri_blk<<<dim3(static_cast<unsigned>((max_n + kTB - 1) / kTB), static_cast<unsigned>(n_mat)), 256, kTrtriSmem,
                 st>>>(n_mat, dim, l_off, x_off, fac_d, X);
   EMG_CK(cudaGetLastError());
@@ -2018,9 +2021,9 @@ int FetiDP::setup_deluxe() {
   const int64_t f2 = static_cast<int64_t>(max_fdim) * max_fdim;
   k_face_gather<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, d_lam_entry, d_dual_off, d_root_off, d_nD,
                                                                      S_d, fac_d, fSa_d, fSb_d);
-  EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
+  if (!capturing) EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
   int rc = factor_range(F + 1, F + 1 + NF);
-  if (!rc) rc = check_err("FETI-DP face factorization");
+  if (!rc && !capturing) rc = check_err("FETI-DP face factorization");
   if (rc) return rc;
   rc = trtri(NF, max_fdim, fc.dim, fc.fac, fc.off, fX_d);
   if (rc) return rc;
@@ -2069,13 +2072,75 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   factored = false;
   tc_factor = (flags & EMG_FLAG_FACTOR_TF32) != 0;
   flags &= ~EMG_FLAG_FACTOR_TF32;
-  const FetiPlan& P = plan;
-  const int32_t S = P.n_parts;
-  const int32_t F = static_cast<int32_t>(P.fronts.size());
   EventPair ev;
   EMG_CK(cudaEventRecord(ev.a, st));
   int rc = system_assemble(un, nu, sigma, n_mat, src, n_src, flags & ~EMG_FLAG_MASS, st);
   if (rc) return rc;
+  // The numeric factorization after the union assembly is the same launch
+  // sequence for every factorization of this plan: the first one runs
+  // eagerly (and the autotuner fixes the solve kernels' widths after it),
+  // the second is captured as one CUDA graph, later ones replay it.  While
+  // capturing, the breakdown checks are deferred to one read at the end.
+  static const bool graph_off = [] {
+    const char* e = std::getenv("EMG_FETI_GRAPH");
+    return e && e[0] == '0';
+  }();
+  cudaGraphExec_t& fg = fac_exec[tc_factor ? 1 : 0];
+  if (!graph_off && !fac_graph_failed && tuned && !fg) {
+    if (!cap_st && cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      fac_graph_failed = true;
+    } else {
+      cudaGraph_t g = nullptr;
+      const cudaStream_t saved = st;
+      st = cap_st;
+      capturing = true;
+      cudaError_t e = cudaStreamBeginCapture(cap_st, cudaStreamCaptureModeThreadLocal);
+      int brc = EMG_SUCCESS;
+      if (e == cudaSuccess) {
+        brc = factor_device();
+        e = cudaStreamEndCapture(cap_st, &g);
+      }
+      capturing = false;
+      st = saved;
+      if (e == cudaSuccess && brc == EMG_SUCCESS) e = cudaGraphInstantiate(&fg, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess || brc != EMG_SUCCESS) {
+        cudaGetLastError();
+        fg = nullptr;
+        fac_graph_failed = true;
+      }
+    }
+  }
+  if (fg) {
+    EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
+    EMG_CK(cudaGraphLaunch(fg, st));
+    rc = check_err("FETI-DP factorization (subdomain, coarse or face matrices)");
+  } else {
+    rc = factor_device();
+  }
+  if (rc) return rc;
+  EMG_CK(cudaGetLastError());
+  EMG_CK(cudaEventRecord(ev.b, st));
+  EMG_CK(cudaEventSynchronize(ev.b));
+  stats.factor_ms = ev.ms();
+  factored = true;
+  if (!tuned) {  // once per solver, after its first factorization (not in factor_ms)
+    tuned = true;
+    tune_solve_kernels();
+  }
+  return EMG_SUCCESS;
+}
+
+// Everything of the numeric factorization after the union assembly: the
+// multifrontal levels, the inverse factors of the dual blocks, the coarse
+// basis and matrix, the deluxe weights.  Breakdown checks read the error word
+// after each phase, unless a capture defers them.
+int FetiDP::factor_device() {
+  const FetiPlan& P = plan;
+  const int32_t S = P.n_parts;
+  const int32_t F = static_cast<int32_t>(P.fronts.size());
+  int rc = EMG_SUCCESS;
   const int32_t* rp = un.K.row_ptr;
   const int32_t* cl = un.K.col;
   const double* vl = un.K.val;
@@ -2109,7 +2174,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
           fd, f0, d_root_off, fac_d, S_d);
     rc = factor_range(f0, f1);
   }
-  if (!rc) rc = check_err("FETI-DP factorization");
+  if (!rc && !capturing) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
   if (n_roots > 0) {
     rc = trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);
@@ -2133,9 +2198,9 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     k_gather_sum<int64_t><<<blocks_for(nc * nc, 256), 256, 0, st>>>(nc * nc, d_sc_ptr, d_sc_list, cblk_d,
                                                                      fac_d + coarse_fac);
     k_gather_sum<int32_t><<<blocks_for(nc, 256), 256, 0, st>>>(nc, d_coarse_ptr, d_coarse_list, h_d, gc_d);
-    EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
+    if (!capturing) EMG_CK(cudaMemsetAsync(err_d, 0, sizeof(int32_t), st));
     rc = factor_range(F, F + 1);
-    if (!rc) rc = check_err("FETI-DP coarse factorization");
+    if (!rc && !capturing) rc = check_err("FETI-DP coarse factorization");
     if (rc) return rc;
     rc = trtri(1, static_cast<int32_t>(nc), d_cdim, d_cfac, d_czero, Lcc_d);
     if (rc) return rc;
@@ -2152,14 +2217,6 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     if (rc) return rc;
   }
   EMG_CK(cudaGetLastError());
-  EMG_CK(cudaEventRecord(ev.b, st));
-  EMG_CK(cudaEventSynchronize(ev.b));
-  stats.factor_ms = ev.ms();
-  factored = true;
-  if (!tuned) {  // once per solver, after its first factorization (not in factor_ms)
-    tuned = true;
-    tune_solve_kernels();
-  }
   return EMG_SUCCESS;
 }
 

@@ -132,6 +132,10 @@ struct FetiDP {
   cudaGraphExec_t lam_exec[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaStream_t cap_st = nullptr;
   bool graph_failed = false;
+  // the numeric factorization as one graph per factor mode (FP64, mixed)
+  cudaGraphExec_t fac_exec[2] = {nullptr, nullptr};
+  bool fac_graph_failed = false;
+  bool capturing = false;  // a capture is recording: defer checks, no attribute calls
   static constexpr int kParts = 592;
 
   ~FetiDP();
@@ -159,6 +163,7 @@ struct FetiDP {
   int setup_device();
   int check_err(const char* where);
   int factor_range(int32_t f0, int32_t f1);
+  int factor_device();
   int solve_fronts(const RhsDev& R, int32_t ncol);
   void coarse_solve(const double* t, double* u);
   void apply_F(const double* p, double* q, double* part);

@@ -132,3 +132,21 @@ def test_direct_solver_on_reference_gauge(kind, n):
     assert rc == 0 and out2.residual_norm <= 1e-12
     rp, col, kv, _, _ = oracle_system(m, ds.l2g)
     assert np.linalg.norm(b2 - O.spmv(rp, col, kv, x2)) <= 1e-11 * np.linalg.norm(b2)
+
+
+def test_factor_graph_replay_matches_the_eager_factorization():
+    """The first factorization of a plan runs eagerly, the second is captured
+    as one CUDA graph, later ones replay it: the same kernels in the same
+    order, so the solutions agree bit for bit (and a different material set
+    between them is picked up by the replay)."""
+    m, part, k = make("scale", 8, 2)
+    fd = fetidp.FetiDP(m, part, k)
+    xs = []
+    for nu in (None, None, np.array([1.0, 0.01]), None):
+        assert fd.factor(nu=nu) == 0, _abi.lib().emg_last_error()
+        x, rc, _ = fd.solve(tol=1e-10, max_iter=1000)
+        assert rc == 0
+        xs.append(x)
+    np.testing.assert_array_equal(xs[0], xs[1])
+    np.testing.assert_array_equal(xs[0], xs[3])
+    assert np.linalg.norm(xs[2] - xs[0]) > 1e-3 * np.linalg.norm(xs[0])
