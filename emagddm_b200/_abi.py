@@ -94,6 +94,16 @@ SIGNATURES = {
     "emg_cg_kernel_times": ([H, C.c_int32, VP, VP], C.c_int),
     "emg_test_set_barrier_spins": ([C.c_int32], C.c_int),
     "emg_tune_enable": ([C.c_int32], C.c_int),
+    "emg_aedt_read": ([C.c_char_p, C.POINTER(H)], C.c_int),
+    "emg_aedt_info": ([H, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+    "emg_aedt_material": ([H, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                           C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+    "emg_aedt_bh_curve": ([H, C.c_int32, VP, VP, C.c_int32], C.c_int),
+    "emg_aedt_object": ([H, C.c_int32, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)],
+                        C.c_int),
+    "emg_aedt_boundary": ([H, C.c_int32, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32],
+                          C.c_int),
+    "emg_aedt_destroy": ([H], None),
     "emg_tune_report": ([C.c_char_p, C.c_int32], C.c_int32),
     "emg_test_tc_tile": ([C.c_int32, C.c_int32, C.c_int32, VP, C.c_int64, VP, C.c_int64, VP, C.c_int64, VP],
                          C.c_int),

@@ -696,6 +696,95 @@ int emg_test_tc_tile(int32_t mr, int32_t mc, int32_t k, const double* a_d, int64
   return guarded([&]() -> int { return emg::tc_tile_test(mr, mc, k, a_d, lda, b_d, ldb, c_d, ldc, as_stream(stream)); });
 }
 
+struct emg_aedt_t {
+  emg::AedtProject p;
+};
+
+namespace {
+void copy_str(const std::string& s, char* buf, int32_t cap) {
+  if (!buf || cap <= 0) return;
+  const size_t n = std::min<size_t>(s.size(), static_cast<size_t>(cap - 1));
+  std::memcpy(buf, s.data(), n);
+  buf[n] = '\0';
+}
+}  // namespace
+
+int emg_aedt_read(const char* path, emg_aedt* out) {
+  return guarded([&]() -> int {
+    if (!path || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
+    *out = nullptr;
+    auto* h = new emg_aedt_t();
+    const int rc = emg::aedt_read(path, h->p);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return EMG_SUCCESS;
+  });
+}
+
+int emg_aedt_info(emg_aedt a, int32_t* n_materials, int32_t* n_objects, int32_t* n_boundaries) {
+  if (!a) { set_error("null AEDT handle"); return EMG_INVALID_INPUT; }
+  if (n_materials) *n_materials = static_cast<int32_t>(a->p.materials.size());
+  if (n_objects) *n_objects = static_cast<int32_t>(a->p.objects.size());
+  if (n_boundaries) *n_boundaries = static_cast<int32_t>(a->p.boundaries.size());
+  return EMG_SUCCESS;
+}
+
+int emg_aedt_material(emg_aedt a, int32_t k, char* name, int32_t cap, double* mu_r, double* sigma,
+                      int32_t* flags, int32_t* n_bh) {
+  if (!a || k < 0 || k >= static_cast<int32_t>(a->p.materials.size())) {
+    set_error("AEDT material index out of range");
+    return EMG_INVALID_INPUT;
+  }
+  const auto& m = a->p.materials[k];
+  copy_str(m.name, name, cap);
+  if (mu_r) *mu_r = m.mu_r;
+  if (sigma) *sigma = m.sigma;
+  if (flags) *flags = m.flags;
+  if (n_bh) *n_bh = static_cast<int32_t>(m.h.size());
+  return EMG_SUCCESS;
+}
+
+int emg_aedt_bh_curve(emg_aedt a, int32_t k, double* h, double* b, int32_t cap) {
+  if (!a || k < 0 || k >= static_cast<int32_t>(a->p.materials.size())) {
+    set_error("AEDT material index out of range");
+    return EMG_INVALID_INPUT;
+  }
+  const auto& m = a->p.materials[k];
+  for (int32_t i = 0; i < cap && i < static_cast<int32_t>(m.h.size()); ++i) {
+    if (h) h[i] = m.h[i];
+    if (b) b[i] = m.b[i];
+  }
+  return EMG_SUCCESS;
+}
+
+int emg_aedt_object(emg_aedt a, int32_t k, char* name, int32_t cap, char* material, int32_t mcap,
+                    int32_t* solve_inside) {
+  if (!a || k < 0 || k >= static_cast<int32_t>(a->p.objects.size())) {
+    set_error("AEDT object index out of range");
+    return EMG_INVALID_INPUT;
+  }
+  const auto& o = a->p.objects[k];
+  copy_str(o.name, name, cap);
+  copy_str(o.material, material, mcap);
+  if (solve_inside) *solve_inside = o.solve_inside;
+  return EMG_SUCCESS;
+}
+
+int emg_aedt_boundary(emg_aedt a, int32_t k, char* name, int32_t cap, char* type, int32_t tcap, char* value,
+                      int32_t vcap) {
+  if (!a || k < 0 || k >= static_cast<int32_t>(a->p.boundaries.size())) {
+    set_error("AEDT boundary index out of range");
+    return EMG_INVALID_INPUT;
+  }
+  const auto& b = a->p.boundaries[k];
+  copy_str(b.name, name, cap);
+  copy_str(b.type, type, tcap);
+  copy_str(b.value, value, vcap);
+  return EMG_SUCCESS;
+}
+
+void emg_aedt_destroy(emg_aedt a) { delete a; }
+
 int emg_tune_enable(int32_t on) {
   emg::tune::set_enabled(on != 0);
   return EMG_SUCCESS;

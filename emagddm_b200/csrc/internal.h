@@ -70,4 +70,26 @@ int build_dofmap_av(const Mesh& m, const int32_t* dof_type, int64_t n_sdir, cons
 int read_gmsh(const std::string& path, const int32_t* dirichlet_tags, int32_t n_tags, Mesh& m,
               std::vector<int32_t>& material_tags);
 
+// Materials, objects and boundaries of an Ansys Maxwell project file
+// (aedt.cpp).
+struct AedtProject {
+  struct Material {
+    std::string name;
+    double mu_r = 1.0, sigma = 0.0;
+    int32_t flags = 0;  // 1 nonlinear (BH curve), 2 permeability not a number, 4 conductivity not a number
+    std::vector<double> h, b;  // BH curve of a nonlinear material
+  };
+  struct Object {
+    std::string name, material;
+    int32_t solve_inside = 1;
+  };
+  struct Boundary {
+    std::string name, type, value;
+  };
+  std::vector<Material> materials;
+  std::vector<Object> objects;
+  std::vector<Boundary> boundaries;
+};
+int aedt_read(const std::string& path, AedtProject& out);
+
 }  // namespace emg

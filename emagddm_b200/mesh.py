@@ -241,12 +241,14 @@ def perturbed(m: CubeMesh, amplitude: float = 0.2, seed: int = 0) -> CubeMesh:
 HEX_FACES = np.array([[0, 1, 2, 3], [4, 5, 6, 7], [0, 1, 5, 4], [2, 3, 7, 6], [0, 3, 7, 4], [1, 2, 6, 5]])
 
 
-def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2), boundary_tag: int = 100):
+def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2), boundary_tag: int = 100,
+               names=None):
     """Write the mesh as an ASCII Gmsh file (2.2 or 4.1): node tags 1..V,
     the tetrahedra (type 4) or hexahedra (type 5) with physical tag
     volume_tags[material], and every boundary face as a triangle (type 2) or
     a quadrangle (type 3, corners in cyclic order) with physical tag
-    `boundary_tag`."""
+    `boundary_tag`.  `names` ({physical tag: name}) adds a $PhysicalNames
+    section (dimension 3 for the volume tags, 2 for the boundary tag)."""
     tets = np.asarray(m.tets, np.int64)
     hexa = tets.shape[1] == 8
     if hexa:
@@ -260,9 +262,13 @@ def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2),
     ftype, vtype = (3, 5) if hexa else (2, 4)
     vt = np.asarray(volume_tags)[np.asarray(m.material)]
     nodes = lambda row: " ".join(str(int(v) + 1) for v in row)
+    pn = ""
+    if names:
+        rows = [f'{2 if int(t) == boundary_tag else 3} {int(t)} "{n}"' for t, n in sorted(names.items())]
+        pn = "$PhysicalNames\n%d\n%s\n$EndPhysicalNames\n" % (len(rows), "\n".join(rows))
     with open(path, "w") as f:
         if version.startswith("2"):
-            f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % m.n_nodes)
+            f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n" + pn + "$Nodes\n%d\n" % m.n_nodes)
             for i, (x, y, z) in enumerate(m.xyz):
                 f.write(f"{i + 1} {float(x)!r} {float(y)!r} {float(z)!r}\n")
             f.write("$EndNodes\n$Elements\n%d\n" % (len(bfaces) + len(tets)))
@@ -276,7 +282,7 @@ def write_gmsh(m: CubeMesh, path: str, version: str = "2.2", volume_tags=(1, 2),
             f.write("$EndElements\n")
         else:
             vols = sorted(set(int(v) for v in vt))
-            f.write("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Entities\n0 0 1 %d\n" % len(vols))
+            f.write("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n" + pn + "$Entities\n0 0 1 %d\n" % len(vols))
             f.write(f"1 0 0 0 1 1 1 1 {boundary_tag} 0\n")
             for v in vols:
                 f.write(f"{v} 0 0 0 1 1 1 1 {v} 0\n")
@@ -331,4 +337,25 @@ def read_gmsh(path: str, dirichlet_tags=None, nu=None, sigma=None, sources=None)
                  sigma=np.zeros(k) if sigma is None else np.asarray(sigma, np.float64),
                  sources=list(sources or []), name=path)
     m.material_tags = mtags[:k]
+    names = physical_names(path)
+    m.physical_names = names
+    # the name of every material (physical volume), in material-id order
+    m.material_names = [names.get((3, int(t))) for t in m.material_tags]
     return m
+
+
+def physical_names(path: str) -> dict:
+    """{(dimension, physical tag): name} from a Gmsh file's $PhysicalNames
+    section (empty without one)."""
+    out = {}
+    with open(path) as f:
+        for line in f:
+            if line.strip() == "$PhysicalNames":
+                n = int(f.readline())
+                for _ in range(n):
+                    dim, tag, rest = f.readline().split(None, 2)
+                    out[(int(dim), int(tag))] = rest.strip().strip('"')
+                break
+            if line.strip() == "$Nodes":
+                break
+    return out

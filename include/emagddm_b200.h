@@ -415,6 +415,32 @@ int emg_system_solve(emg_system sys, int32_t kind, const emg_krylov_config* cfg,
  * b = ones, each launch bracketed by CUDA events on `stream`. */
 int emg_cg_kernel_times(emg_csr A, int32_t iterations, void* stream, double* ms);
 
+/* ---- Ansys Maxwell project input (MaxwellParserImpl / AedtProjectLoader,
+ * src/tool/maxwell_parser_impl.cpp, src/tool/aedt_project_loader.cpp:60-130)
+ * The materials, geometry parts (objects) and boundaries of an .aedt text
+ * project.  The mesh is not stored in .aedt files: a mesh read with
+ * emg_mesh_read_gmsh whose physical volumes carry the objects' names takes
+ * nu / sigma from here (Python: emagddm_b200.aedt). */
+typedef struct emg_aedt_t* emg_aedt;
+int emg_aedt_read(const char* path, emg_aedt* out);
+int emg_aedt_info(emg_aedt a, int32_t* n_materials, int32_t* n_objects, int32_t* n_boundaries);
+/* Material k: name (NUL-terminated, at most cap bytes), relative permeability
+ * (a nonlinear material: its initial permeability, the first BH point with
+ * H > 0 as B / (mu0 H)), conductivity [S/m], flags (1 nonlinear, 2
+ * permeability not a number, 4 conductivity not a number) and the number of
+ * BH-curve points. */
+int emg_aedt_material(emg_aedt a, int32_t k, char* name, int32_t cap, double* mu_r, double* sigma,
+                      int32_t* flags, int32_t* n_bh);
+/* BH curve of material k: H [A/m] and B [T], at most cap points. */
+int emg_aedt_bh_curve(emg_aedt a, int32_t k, double* h, double* b, int32_t cap);
+/* Object k: name, material name, solve-inside flag. */
+int emg_aedt_object(emg_aedt a, int32_t k, char* name, int32_t cap, char* material, int32_t mcap,
+                    int32_t* solve_inside);
+/* Boundary k: name, type ('Vector Potential', 'Coil', ...), value. */
+int emg_aedt_boundary(emg_aedt a, int32_t k, char* name, int32_t cap, char* type, int32_t tcap, char* value,
+                      int32_t vcap);
+void emg_aedt_destroy(emg_aedt a);
+
 /* ---- Launch-configuration autotuner (no counterpart in the reference) ----
  * The library times candidate launch configurations of some kernels on the
  * device the first time it meets a problem shape and keeps the fastest:
