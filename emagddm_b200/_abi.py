@@ -18,7 +18,7 @@ EMG_SUCCESS, EMG_NUMERICAL_ERROR, EMG_DIVERGED, EMG_MAX_ITER_REACHED, EMG_INVALI
 EMG_ERR_CUDA, EMG_ERR_TIMEOUT, EMG_ERR_NOMEM, EMG_ERR_INTERNAL = 5, 6, 7, 8
 GAUGE_NONE, GAUGE_REF, GAUGE_BOUNDARY_FIRST = -1, 0, 1
 FLAG_MASS, FLAG_NO_EDGE_SIGNS, FLAG_PIOLA_LITERAL, FLAG_QUAD3_LITERAL = 1, 2, 4, 8
-ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
+ELEM_TET4_EDGE, ELEM_HEX8_EDGE, ELEM_PRISM6_EDGE, ELEM_PYRAMID5_EDGE = 0, 1, 2, 3
 DOF_SCALAR_ONLY, DOF_VECTOR_EDGE_ONLY, DOF_MIXED_AV, DOF_ABSENT = 0, 1, 2, -2
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 

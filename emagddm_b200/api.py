@@ -32,7 +32,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _abi
+from . import _abi, mesh
 from ._abi import check, lib, ptr
 
 
@@ -83,10 +83,10 @@ class EMMeshData:
     @property
     def elem_type(self) -> int:
         """numeric::ElementType of the elements: TET4_EDGE (4 nodes) or HEX8_EDGE (8)."""
-        return _abi.ELEM_HEX8_EDGE if np.asarray(self.tets).shape[1] == 8 else _abi.ELEM_TET4_EDGE
+        return mesh.TYPE_OF_NODES[np.asarray(self.tets).shape[1]]
 
     def edges_per_element(self) -> int:
-        return 12 if self.elem_type == _abi.ELEM_HEX8_EDGE else 6
+        return mesh.EDGES_OF_TYPE[self.elem_type]
 
     @classmethod
     def from_cube(cls, mesh) -> "EMMeshData":

@@ -1,5 +1,5 @@
-// assembly.cu -- EMAssembly::assemble on the GPU for TET4_EDGE and HEX8_EDGE
-// elements (reference: src/numeric/em_assembly.cpp:144-420 with the intended
+// assembly.cu -- EMAssembly::assemble on the GPU for TET4_EDGE, HEX8_EDGE,
+// PRISM6_EDGE and PYRAMID5_EDGE elements (reference: src/numeric/em_assembly.cpp:144-420 with the intended
 // MagneticVector3DIntegrator formulas, magnetic_vector_3d_integrator.cpp:139-364).
 //
 // Symbolic phase (once per mesh + DOF map):
@@ -10,19 +10,26 @@
 //   ascending columns -- the pattern SparseConverter::to_eigen produces from
 //   the reference's unmerged CSR (sparse_converter.cpp:19-80).
 // Numeric phase:
-//   k_assemble_rows (tets) / k_assemble_rows_hex gather, for each row, the
-//   contributions of its incident elements in ascending element order and
-//   write the row's values once: no atomics,
-//   deterministic, and every sum is formed in the same order as an element
-//   loop would form it.
+//   tets: k_tet_terms forms every tet's element terms once (the packed 6x6
+//   stiffness and mass blocks, the source vector, signs folded in) and
+//   k_rows_gather sums, for each row, the terms of its incident tets in
+//   ascending element order at column positions k_slot_positions recorded
+//   in the symbolic phase (k_rows_from_terms for rows longer than 64);
+//   hexahedra, prisms, pyramids: k_elem_terms runs the quadrature loop once
+//   per element (elem_shapes.cuh) and k_rows_from_terms gathers the rows.
+//   Every row's values are written once: no atomics, deterministic, and
+//   every sum is formed in the same order as an element loop would form it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <vector>
 
 #include "common.cuh"
 #include "device.h"
 #include "internal.h"
+#include "elem_shapes.cuh"
 #include "trace.h"
 
 namespace emg {
@@ -271,6 +278,52 @@ __global__ void __launch_bounds__(128) k_row_columns(int64_t n, int epe, const i
   }
 }
 
+// Thread per row (TET4_EDGE): for every incidence slot q of the row, element t,
+// the positions of the element's columns l2g[6 t + j] inside the row, as bytes
+// pos[8 q + j] (0xFF for a constrained edge or a row longer than 254), byte
+// pos[8 q + 6] = 1 when two of them coincide (a DOF map that sends two local
+// edges of one tet to one DOF), and the longest row into *max_len.
+__global__ void k_slot_positions(int64_t n, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc,
+                                 const int32_t* __restrict__ l2g, const int32_t* __restrict__ row_ptr,
+                                 const int32_t* __restrict__ col, uint8_t* __restrict__ pos,
+                                 int32_t* __restrict__ max_len) {
+  int32_t longest = 0;
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s0 = row_ptr[r], s1 = row_ptr[r + 1];
+    longest = max(longest, s1 - s0);
+    for (int32_t q = inc_ptr[r]; q < inc_ptr[r + 1]; ++q) {
+      const int64_t t = inc[q] / 6;
+      uint8_t b[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = 0xFF;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int32_t c = l2g[6 * t + j];
+        if (c < 0) continue;
+        int32_t lo = s0, hi = s1;
+        while (lo < hi) {
+          const int32_t mid = (lo + hi) >> 1;
+          if (col[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        if (lo < s1 && col[lo] == c && lo - s0 < 0xFF) b[j] = static_cast<uint8_t>(lo - s0);
+      }
+      uint8_t dup = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j)
+#pragma unroll
+        for (int k = j + 1; k < 6; ++k) dup |= (b[j] != 0xFF && b[j] == b[k]) ? 1 : 0;
+      b[6] = dup;
+      uint2 w;
+      w.x = b[0] | (b[1] << 8) | (b[2] << 16) | (static_cast<uint32_t>(b[3]) << 24);
+      w.y = b[4] | (b[5] << 8) | (b[6] << 16) | (static_cast<uint32_t>(b[7]) << 24);
+      reinterpret_cast<uint2*>(pos)[q] = w;
+    }
+  }
+  longest = __reduce_max_sync(0xffffffffu, longest);
+  if ((threadIdx.x & 31) == 0) atomicMax(max_len, longest);
+}
+
 // --------------------------------------------------------------- numeric ----
 // Nedelec TET4_EDGE edge table (nedelec_element.cpp:54-60): basis k is
 // lambda_b grad(lambda_a) - lambda_a grad(lambda_b) for (a, b) = (ned_a(k), ned_b(k)).
@@ -390,328 +443,516 @@ struct AsmArgs {
   int32_t* err;
 };
 
-// Thread per row: K(r, c) = sum over incident tets of
-//   nu |det| wsum s_i s_j curl_i . curl_j
+// Packed upper triangle of a symmetric 6x6 element matrix: entry (i, j),
+// i <= j, at i (11 - i) / 2 + j.
+__host__ __device__ constexpr int ke_index(int i, int j) { return i * (11 - i) / 2 + j; }
+static_assert(ke_index(0, 5) == 5 && ke_index(1, 1) == 6 && ke_index(2, 2) == 11 && ke_index(4, 5) == 19 &&
+                  ke_index(5, 5) == 20,
+              "packed 6x6 upper triangle");
+constexpr int kKe = 21;
+constexpr int kTermTile = 128;  // tets per block pass of k_tet_terms
+
+// Copies a block's staged per-tet terms (cnt tets x width doubles, in shared
+// memory) to out[t0 * width ...] with consecutive threads on consecutive
+// doubles.
+__device__ __forceinline__ void store_staged(const double* stage, double* __restrict__ out, int64_t t0, int cnt,
+                                             int width) {
+  __syncthreads();
+  for (int x = threadIdx.x; x < cnt * width; x += blockDim.x) out[t0 * width + x] = stage[x];
+  __syncthreads();
+}
+
+// Thread per tet, once per tet, the element loop of em_assembly.cpp:144-420:
+//   ke[21 t + (i, j)] = s_i s_j nu |det| wsum curl_i . curl_j
 // where curl_k = J curl_ref_k / det is constant per tet, so the quadrature
 // sum collapses to the weight sum (1/6 for the Hammer rule, 1/8 for the
-// reference's 3-point rule).  M and F are integrated at the quadrature points.
-__global__ void __launch_bounds__(128) k_assemble_rows(AsmArgs A) {
+// reference's 3-point rule);
+//   me[21 t + (i, j)] = s_i s_j sum_q w |det| sigma W_i(x_q) . W_j(x_q)
+//   fe[6 t + i]       = s_i sum_q w |det| W_i(x_q) . J_s(x_q)
+// (s_k the edge sign).  Tets the element loop skips (material id out of
+// range, |det| < 1e-15) get zeros, which leave every sum they join unchanged.
+// The terms are staged in shared memory and written coalesced.
+// kK selects the stiffness terms, kMass / kSrc the quadrature terms: the two
+// groups run as separate launches, which keeps each one's registers low.
+template <bool kK, bool kMass, bool kSrc>
+__global__ void __launch_bounds__(kTermTile, 4) k_tet_terms(AsmArgs A, int64_t n_tets, double* __restrict__ ke,
+                                                            double* __restrict__ me, double* __restrict__ fe) {
+  __shared__ double stage[kTermTile * kKe];
   const double qa = 0.13819660112501051517954131656343619;   // (5 - sqrt 5) / 20
   const double qb = 0.58541019662496845446137605030969143;   // (5 + 3 sqrt 5) / 20
   const bool quad3 = (A.flags & EMG_FLAG_QUAD3_LITERAL) != 0;
   const int nq = quad3 ? 3 : 4;
   const double w = 1.0 / 24.0;
-  const bool want_mass = (A.flags & EMG_FLAG_MASS) != 0 && A.mval != nullptr;
   const bool signs = (A.flags & EMG_FLAG_NO_EDGE_SIGNS) == 0;
   const bool literal = (A.flags & EMG_FLAG_PIOLA_LITERAL) != 0;
-  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < A.n;
-       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t s0 = A.row_ptr[r], s1 = A.row_ptr[r + 1];
-    for (int32_t k = s0; k < s1; ++k) {
-      A.kval[k] = 0.0;
-      if (want_mass) A.mval[k] = 0.0;
+  for (int64_t t0 = static_cast<int64_t>(blockIdx.x) * kTermTile; t0 < n_tets;
+       t0 += static_cast<int64_t>(gridDim.x) * kTermTile) {
+    const int cnt = static_cast<int>(n_tets - t0 < kTermTile ? n_tets - t0 : kTermTile);
+    const int64_t t = t0 + threadIdx.x;
+    const int32_t mid = t < n_tets ? (A.material ? A.material[t] : 0) : -1;
+    Tet T;
+    bool use = mid >= 0 && mid < A.n_mat;  // em_assembly.cpp:270-276 skips the element
+    if (use && !load_tet(A.elems, A.xyz, A.n_nodes, t, T)) {
+      atomicOr(A.err, kErrNode);
+      use = false;
     }
-    double f = 0.0;
-    for (int32_t q = A.inc_ptr[r]; q < A.inc_ptr[r + 1]; ++q) {
-      const int32_t slot = A.inc[q];
-      const int64_t t = slot / 6;
-      const int i = slot - 6 * static_cast<int>(t);
-      const int32_t mid = A.material ? A.material[t] : 0;
-      if (mid < 0 || mid >= A.n_mat) continue;  // em_assembly.cpp:270-276 skips the element
-      Tet T;
-      if (!load_tet(A.elems, A.xyz, A.n_nodes, t, T)) { atomicOr(A.err, kErrNode); continue; }
-      const double adet = fabs(T.det);
-      if (adet < 1e-15) continue;  // every quadrature point skipped (:169)
-      // the row's own local edge, picked out with compile-time indices
-      int sgi = 1;
-      double ci[3] = {0, 0, 0};
+    use = use && !(fabs(T.det) < 1e-15);  // every quadrature point skipped (:169)
+    double sg[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k)
-        if (k == i) {
-          if (signs) sgi = T.node[ned_b(k)] < T.node[ned_a(k)] ? 1 : -1;
-          ci[0] = T.c[k][0]; ci[1] = T.c[k][1]; ci[2] = T.c[k][2];
+    for (int k = 0; k < 6; ++k) sg[k] = (!use || !signs || T.node[ned_b(k)] < T.node[ned_a(k)]) ? 1.0 : -1.0;
+    const double adet = use ? fabs(T.det) : 0.0;
+    if (kK) {
+      const double kf = use ? nq * w * adet * A.nu[mid] : 0.0;
+      double* st = stage + threadIdx.x * kKe;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = i; j < 6; ++j) {
+          const double d = use ? T.c[i][0] * T.c[j][0] + T.c[i][1] * T.c[j][1] + T.c[i][2] * T.c[j][2] : 0.0;
+          st[ke_index(i, j)] = (sg[i] * sg[j]) * (kf * d);
         }
-      const double kf = nq * w * adet * A.nu[mid];
-      const double sig = A.sigma ? A.sigma[mid] : 0.0;
-      const bool do_mass = want_mass && sig > 0.0;
-      const emg_source* tab = c_src;
-      int src_first = 0, src_count = A.n_src;
-      if (A.src_map) {
-        tab = A.src_tab;
-        const int32_t sid = A.src_map[t];
-        src_first = sid;
-        src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
-      }
-      const bool do_src = src_count > 0;
-      int32_t pos[6];
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const int32_t cj = A.l2g[6 * t + j];
-        pos[j] = cj >= 0 ? find_slot(A.col, s0, s1, cj) : -1;
-        if (cj >= 0 && (pos[j] >= s1 || A.col[pos[j]] != cj)) {
-          atomicOr(A.err, kErrSlot);
-          pos[j] = -1;
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        if (pos[j] < 0) continue;
-        const int sgj = signs ? (T.node[ned_b(j)] < T.node[ned_a(j)] ? 1 : -1) : 1;
-        const double d = ci[0] * T.c[j][0] + ci[1] * T.c[j][1] + ci[2] * T.c[j][2];
-        A.kval[pos[j]] += static_cast<double>(sgi * sgj) * (kf * d);
-      }
-      if (do_mass || do_src) {
-        double mrow[6] = {0, 0, 0, 0, 0, 0};
-        double fi = 0.0;
-        for (int qq = 0; qq < nq; ++qq) {
-          double lam[4];
-          if (qq == 0) { lam[0] = qa; lam[1] = qa; lam[2] = qb; }
-          else if (qq == 1) { lam[0] = qa; lam[1] = qb; lam[2] = qa; }
-          else if (qq == 2 && !quad3) { lam[0] = qb; lam[1] = qa; lam[2] = qa; }
-          else { lam[0] = qa; lam[1] = qa; lam[2] = qa; }
-          lam[3] = 1.0 - lam[0] - lam[1] - lam[2];
-          double W[6][3], Wi[3] = {0, 0, 0};
-#pragma unroll
-          for (int k = 0; k < 6; ++k) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              W[k][c] = lam[ned_b(k)] * T.g[ned_a(k)][c] - lam[ned_a(k)] * T.g[ned_b(k)][c];
-              if (literal) W[k][c] /= T.det;
-            }
-            if (k == i) { Wi[0] = W[k][0]; Wi[1] = W[k][1]; Wi[2] = W[k][2]; }
-          }
-          if (do_mass) {
-#pragma unroll
-            for (int j = 0; j < 6; ++j)
-              mrow[j] += w * adet * sig * (Wi[0] * W[j][0] + Wi[1] * W[j][1] + Wi[2] * W[j][2]);
-          }
-          if (do_src) {
-            double x[3], js[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              x[c] = T.x3[c] + lam[0] * T.d[0][c] + lam[1] * T.d[1][c] + lam[2] * T.d[2][c];
-            source_at(x, tab, src_first, src_count, js);
-            fi += w * adet * (Wi[0] * js[0] + Wi[1] * js[1] + Wi[2] * js[2]);
-          }
-        }
-        if (do_mass) {
-#pragma unroll
-          for (int j = 0; j < 6; ++j)
-            if (pos[j] >= 0) {
-              const int sgj = signs ? (T.node[ned_b(j)] < T.node[ned_a(j)] ? 1 : -1) : 1;
-              A.mval[pos[j]] += static_cast<double>(sgi * sgj) * mrow[j];
-            }
-        }
-        f += sgi * fi;
       }
     }
-    A.rhs[r] = f;
+    double mt[kMass ? kKe : 1], ft[kSrc ? 6 : 1];
+#pragma unroll
+    for (int e = 0; e < (kMass ? kKe : 1); ++e) mt[e] = 0.0;
+#pragma unroll
+    for (int e = 0; e < (kSrc ? 6 : 1); ++e) ft[e] = 0.0;
+    const double sig = use && A.sigma ? A.sigma[mid] : 0.0;
+    const bool do_mass = kMass && sig > 0.0;
+    const emg_source* tab = c_src;
+    int src_first = 0, src_count = use ? A.n_src : 0;
+    if (use && A.src_map) {
+      tab = A.src_tab;
+      const int32_t sid = A.src_map[t];
+      src_first = sid;
+      src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
+    }
+    const bool do_src = kSrc && src_count > 0;
+    if (do_mass || do_src) {
+      for (int qq = 0; qq < nq; ++qq) {
+        double lam[4];
+        if (qq == 0) { lam[0] = qa; lam[1] = qa; lam[2] = qb; }
+        else if (qq == 1) { lam[0] = qa; lam[1] = qb; lam[2] = qa; }
+        else if (qq == 2 && !quad3) { lam[0] = qb; lam[1] = qa; lam[2] = qa; }
+        else { lam[0] = qa; lam[1] = qa; lam[2] = qa; }
+        lam[3] = 1.0 - lam[0] - lam[1] - lam[2];
+        double js[3] = {0.0, 0.0, 0.0};
+        if (kSrc && do_src) {
+          double x[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            x[c] = T.x3[c] + lam[0] * T.d[0][c] + lam[1] * T.d[1][c] + lam[2] * T.d[2][c];
+          source_at(x, tab, src_first, src_count, js);
+        }
+        // a point outside every source region adds nothing to F
+        if (!(kMass && do_mass) && js[0] == 0.0 && js[1] == 0.0 && js[2] == 0.0) continue;
+        double W[6][3];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            W[k][c] = lam[ned_b(k)] * T.g[ned_a(k)][c] - lam[ned_a(k)] * T.g[ned_b(k)][c];
+            if (literal) W[k][c] /= T.det;
+          }
+        }
+        if (kMass && do_mass) {
+#pragma unroll
+          for (int i = 0; i < 6; ++i) {
+#pragma unroll
+            for (int j = i; j < 6; ++j)
+              mt[kMass ? ke_index(i, j) : 0] +=
+                  w * adet * sig * (W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2]);
+          }
+        }
+        if (kSrc && do_src) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k)
+            ft[kSrc ? k : 0] += w * adet * (W[k][0] * js[0] + W[k][1] * js[1] + W[k][2] * js[2]);
+        }
+      }
+    }
+    if (kK) store_staged(stage, ke, t0, cnt, kKe);
+    if (kMass) {
+      double* st = stage + threadIdx.x * kKe;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = i; j < 6; ++j) st[ke_index(i, j)] = (sg[i] * sg[j]) * mt[kMass ? ke_index(i, j) : 0];
+      }
+      store_staged(stage, me, t0, cnt, kKe);
+    }
+    if (kSrc) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) stage[threadIdx.x * 6 + k] = sg[k] * ft[kSrc ? k : 0];
+      store_staged(stage, fe, t0, cnt, 6);
+    }
   }
 }
 
-// ----------------------------------------------------------- HEX8_EDGE ----
-// Reference hexahedron [-1,1]^3, nodes 0-3 on zeta = -1 (counter-clockwise
-// from (-1,-1)), 4-7 above them (nedelec_element.cpp:506-517).  Edge k runs
-// from local node A to B (ElementGeometry's table, element_geometry.cpp:165-171)
-// along reference axis d; with (p, q) = (d+1, d+2) mod 3 and c_p, c_q the
-// edge's fixed coordinates, its basis (evalHex8Edge, nedelec_element.cpp:519-615) is
-//   W_k = 1/2 s_k (1 + c_p x_p)(1 + c_q x_q) e_d,   s_k = (x_d(B) - x_d(A)) / 2,
-// with curl
-//   curl W_k = 1/2 s_k [c_q (1 + c_p x_p) e_p - c_p (1 + c_q x_q) e_q].
-// (curlHex8Edge, :618-720, has sign / component errors in edges 2, 3, 6, 7;
-// the curl here is the derivative of the reference's own W_k.)  The tables
-// are closed forms, so with k unrolled they fold to compile-time constants.
-__host__ __device__ constexpr int hex_node_coord(int a, int axis) {  // reference coordinate of node a
-  return axis == 0 ? (((a & 3) == 1 || (a & 3) == 2) ? 1 : -1) : axis == 1 ? ((a & 2) ? 1 : -1) : ((a & 4) ? 1 : -1);
-}
-__host__ __device__ constexpr int hex_edge_a(int k) { return k < 8 ? k : k - 8; }
-__host__ __device__ constexpr int hex_edge_b(int k) { return k < 4 ? ((k + 1) & 3) : k < 8 ? 4 + ((k + 1) & 3) : k - 4; }
-__host__ __device__ constexpr int hex_dir(int k) { return k < 8 ? (k & 1) : 2; }
-__host__ __device__ constexpr int hex_sgn(int k) {
-  return (hex_node_coord(hex_edge_b(k), hex_dir(k)) - hex_node_coord(hex_edge_a(k), hex_dir(k))) / 2;
-}
-__host__ __device__ constexpr int hex_cp(int k) { return hex_node_coord(hex_edge_a(k), (hex_dir(k) + 1) % 3); }
-__host__ __device__ constexpr int hex_cq(int k) { return hex_node_coord(hex_edge_a(k), (hex_dir(k) + 2) % 3); }
-static_assert(hex_edge_a(2) == 2 && hex_edge_b(2) == 3 && hex_edge_b(3) == 0 && hex_edge_b(7) == 4 &&
-                  hex_edge_b(11) == 7,
-              "edge table of element_geometry.cpp:165-171");
-static_assert(hex_sgn(2) == -1 && hex_sgn(3) == -1 && hex_sgn(6) == -1 && hex_sgn(7) == -1 && hex_sgn(8) == 1,
-              "basis orientation of nedelec_element.cpp:519-615");
-static_assert(hex_cp(0) == -1 && hex_cq(0) == -1 && hex_cp(1) == -1 && hex_cq(1) == 1 && hex_cp(9) == 1 &&
-                  hex_cq(9) == -1,
-              "edge positions");
+// Packed upper triangle of a symmetric E x E element matrix: entry (i, j),
+// i <= j, at i (2E - 1 - i) / 2 + j.
+__host__ __device__ constexpr int packed_index(int e, int i, int j) { return i * (2 * e - 1 - i) / 2 + j; }
+static_assert(packed_index(6, 2, 3) == ke_index(2, 3) && packed_index(12, 11, 11) == 77 &&
+                  packed_index(9, 8, 8) == 44 && packed_index(8, 0, 7) == 7,
+              "packed upper triangle");
 
-// Thread per row, 2x2x2 Gauss-Legendre (points +-1/sqrt 3, weights 1):
-//   K(r, c) = sum_q nu / |det J| (curl_ref_i)^T (J^T J) (curl_ref_j)
-//   M(r, c) = sum_q sigma |det J| f_i f_j [(J^T J)^-1]_{d_i d_j}
-//   F(r)    = sum_q |det J| f_i [J^-1 J_s(x_q)]_{d_i}
-// (curl_phys = J curl_ref / det J, W_phys = J^-T W_ref; EMG_FLAG_PIOLA_LITERAL
-// divides W_phys by det J once more), incident elements in ascending order.
-template <bool kMass>
-__global__ void __launch_bounds__(128) k_assemble_rows_hex(AsmArgs A) {
-  const double g = 0.57735026918962576450914878050195746;  // 1 / sqrt 3
-  const bool want_mass = kMass && A.mval != nullptr;
+// Sixteen lanes per row, lane k owning the row's column col[s0 + k] (longer
+// rows in passes of sixteen columns), for elements of kEpe edges.  For every
+// incident slot (t, i) of the row, in ascending element order, a lane adds
+// the entries (i, j) of element t whose column l2g[kEpe t + j] is its own, in
+// ascending j: the order in which the element loop forms every sum.  Each
+// value is written once, coalesced, without atomics, and K(r, c) and
+// K(c, r) add the same terms in the same order, so K is exactly symmetric.
+template <int kEpe, bool kMass, bool kSrc>
+__global__ void __launch_bounds__(256, 4) k_rows_from_terms(AsmArgs A, const double* __restrict__ ke,
+                                                            const double* __restrict__ me,
+                                                            const double* __restrict__ fe) {
+  constexpr int kP = kEpe * (kEpe + 1) / 2;
+  const int sub = threadIdx.x & 15;
+  const unsigned half = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const int64_t stride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 4;
+  for (int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 4; r < A.n; r += stride) {
+    const int32_t s0 = A.row_ptr[r], s1 = A.row_ptr[r + 1];
+    const int32_t a = A.inc_ptr[r], m = A.inc_ptr[r + 1] - a;
+    double f = 0.0;
+    for (int32_t cb = s0; cb < s1; cb += 16) {
+      const int32_t k = cb + sub;
+      const int32_t c = k < s1 ? A.col[k] : -2;  // -2 matches no l2g entry
+      double acc = 0.0, accm = 0.0;
+      for (int32_t qb = 0; qb < m; qb += 16) {
+        const int32_t mine = qb + sub < m ? A.inc[a + qb + sub] : 0;
+        const int nu = min(16, m - qb);
+        for (int u = 0; u < nu; ++u) {
+          const int32_t slot = __shfl_sync(half, mine, u, 16);
+          const int32_t t = slot / kEpe;
+          const int i = slot - kEpe * t;
+          const int32_t* lg = A.l2g + static_cast<int64_t>(kEpe) * t;
+          unsigned hit = 0;
+#pragma unroll
+          for (int j = 0; j < kEpe; ++j) hit |= (lg[j] == c ? 1u : 0u) << j;
+          const int64_t base = static_cast<int64_t>(kP) * t;
+          while (hit) {
+            const int j = __ffs(hit) - 1;
+            hit &= hit - 1;
+            const int e = i <= j ? packed_index(kEpe, i, j) : packed_index(kEpe, j, i);
+            acc += ke[base + e];
+            if (kMass) accm += me[base + e];
+          }
+          if (kSrc && cb == s0) f += fe[static_cast<int64_t>(kEpe) * t + i];
+        }
+      }
+      if (k < s1) {
+        A.kval[k] = acc;
+        if (kMass) A.mval[k] = accm;
+      }
+    }
+    if (sub == 0) A.rhs[r] = f;
+  }
+}
+
+constexpr int kGatherRows = 5;  // rows per warp, six lanes (local columns j) each
+constexpr int kGatherCap = 64;  // longest row k_rows_gather takes
+
+// Five rows per warp, lane (rho, j) handling local column j of row r0 + rho.
+// Step q visits the q-th incident slot (t, i) of every row at once (slots
+// ascend in element order): the lane adds the tet's entry (i, j) into the
+// row's accumulator at the column position the symbolic phase recorded,
+// pos[8 q + j].  Within a step the six columns of one tet are distinct, so
+// lanes never collide (a DOF map that sends two local edges of one tet to
+// the same column is detected and handled one lane at a time); across steps
+// each position receives its terms in ascending element order, the order of
+// the element loop.  Rows are then written once from shared memory.
+template <bool kMass, bool kSrc>
+__global__ void __launch_bounds__(256) k_rows_gather(AsmArgs A, const uint8_t* __restrict__ pos,
+                                                     const double* __restrict__ ke, const double* __restrict__ me,
+                                                     const double* __restrict__ fe) {
+  // rows kGatherCap + 1 doubles apart: the rows of a warp start in different banks
+  constexpr int kStride = kGatherCap + 1;
+  __shared__ double acc_k[8][kGatherRows * kStride];
+  __shared__ double acc_m[kMass ? 8 : 1][kMass ? kGatherRows * kStride : 1];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int rho = lane / 6, j = lane - 6 * rho;  // rho == 5: lanes 30, 31 idle
+  double* rk = acc_k[wib] + (rho < kGatherRows ? rho : 0) * kStride;
+  double* rm = kMass ? acc_m[kMass ? wib : 0] + (rho < kGatherRows ? rho : 0) * kStride : nullptr;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r0 = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + wib) * kGatherRows; r0 < A.n;
+       r0 += warps * kGatherRows) {
+    const int64_t r = r0 + rho;
+    const bool live = rho < kGatherRows && r < A.n;
+    int32_t s0 = 0, len = 0, a = 0, m = 0;
+    if (live) {
+      s0 = A.row_ptr[r];
+      len = A.row_ptr[r + 1] - s0;
+      a = A.inc_ptr[r];
+      m = A.inc_ptr[r + 1] - a;
+      for (int k = j; k < len; k += 6) {
+        rk[k] = 0.0;
+        if (kMass) rm[k] = 0.0;
+      }
+    }
+    const int steps = __reduce_max_sync(0xffffffffu, m);
+    __syncwarp();
+    double f = 0.0;
+    const int src0 = (rho < kGatherRows ? rho : 0) * 6;
+    for (int q0 = 0; q0 < steps; q0 += 12) {
+      // the row's next twelve incidence slots, two per lane of its group
+      const int32_t lo = live && q0 + j < m ? A.inc[a + q0 + j] : 0;
+      const int32_t hi = live && q0 + 6 + j < m ? A.inc[a + q0 + 6 + j] : 0;
+      const int nq = min(12, steps - q0);
+      for (int u = 0; u < nq; ++u) {
+        const int q = q0 + u;
+        const int32_t slot = __shfl_sync(0xffffffffu, u < 6 ? lo : hi, src0 + (u < 6 ? u : u - 6));
+        const bool act = live && q < m;
+        const int64_t t = slot / 6;
+        const int i = slot - 6 * static_cast<int>(t);
+        const uint8_t* pq = pos + 8 * static_cast<int64_t>(a + q);
+        const int p = act ? pq[j] : 0xFF;
+        const bool clash = __any_sync(0xffffffffu, act && j == 0 && pq[6] != 0);
+        const bool add = p != 0xFF;
+        const int e = i <= j ? ke_index(i, j) : ke_index(j, i);
+        double vk = 0.0, vm = 0.0;
+        if (add) {
+          vk = ke[kKe * t + e];
+          if (kMass) vm = me[kKe * t + e];
+        }
+        if (kSrc && act && j == 0) f += fe[6 * t + i];
+        if (!clash) {
+          if (add) {
+            rk[p] += vk;
+            if (kMass) rm[p] += vm;
+          }
+        } else {  // two local edges of one tet on one column: add one lane at a time, ascending j
+          for (int jj = 0; jj < 6; ++jj) {
+            if (add && j == jj) {
+              rk[p] += vk;
+              if (kMass) rm[p] += vm;
+            }
+            __syncwarp();
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (live) {
+      for (int k = j; k < len; k += 6) {
+        A.kval[s0 + k] = rk[k];
+        if (kMass) A.mval[s0 + k] = rm[k];
+      }
+      if (j == 0) A.rhs[r] = f;
+    }
+    __syncwarp();
+  }
+}
+
+template <bool kMass, bool kSrc>
+void launch_tet_assembly(const AsmArgs& a, int64_t n_tets, const uint8_t* slot_pos, int32_t max_row_len,
+                         double* ke, double* me, double* fe, cudaStream_t st) {
+  const int64_t tiles = (n_tets + kTermTile - 1) / kTermTile;
+  const unsigned gt = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(tiles, 148 * 16)));
+  k_tet_terms<true, false, false><<<gt, kTermTile, 0, st>>>(a, n_tets, ke, me, fe);
+  if (kMass || kSrc) k_tet_terms<false, kMass, kSrc><<<gt, kTermTile, 0, st>>>(a, n_tets, ke, me, fe);
+  if (slot_pos && max_row_len <= kGatherCap) {
+    const int64_t rb = (a.n + 8 * kGatherRows - 1) / (8 * kGatherRows);  // 8 warps of 5 rows per block
+    const unsigned gr = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(rb, 148 * 64)));
+    k_rows_gather<kMass, kSrc><<<gr, 256, 0, st>>>(a, slot_pos, ke, me, fe);
+  } else {  // rows longer than the gather kernel's shared-memory rows
+    const int64_t rb = (a.n * 16 + 255) / 256;
+    const unsigned gr = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(rb, 148 * 64)));
+    k_rows_from_terms<6, kMass, kSrc><<<gr, 256, 0, st>>>(a, ke, me, fe);
+  }
+}
+
+// ------------------------------------------ HEX8 / PRISM6 / PYRAMID5 ----
+constexpr int kElemTile = 64;  // elements per block pass of k_elem_terms
+
+// Thread per element of shape S (elem_shapes.cuh), once per element, the
+// quadrature loop of MagneticVector3DIntegrator (computeStiffnessMatrix /
+// computeMassMatrix / computeSourceVector, magnetic_vector_3d_integrator.cpp:
+// 139-364) with curl_phys = J curl_ref / det J and W_phys = J^-T W_ref
+// (divided by det J once more under EMG_FLAG_PIOLA_LITERAL):
+//   kK:    ke[P t + (i, j)] = s_i s_j sum_q w_q |det J| nu curl_i . curl_j
+//   kMass: me[P t + (i, j)] = s_i s_j sum_q w_q |det J| sigma W_i . W_j
+//   kSrc:  fe[E t + i]      = s_i sum_q w_q |det J| W_i . J_s(x_q)
+// (P = E (E + 1) / 2 packed upper-triangle entries, s_k the edge sign;
+// quadrature points with |det J| < 1e-15 are skipped, elements with a
+// material id out of range get zeros).  The stiffness and the quadrature
+// terms run as separate launches; the packed sums accumulate in shared
+// memory, entry-major so that a warp's lanes touch consecutive words, and are
+// written coalesced.
+template <class S, bool kK, bool kMass, bool kSrc>
+__global__ void __launch_bounds__(kElemTile) k_elem_terms(AsmArgs A, int64_t n_el, double* __restrict__ ke,
+                                                          double* __restrict__ me, double* __restrict__ fe) {
+  constexpr int E = S::kEdges, N = S::kNodes, P = E * (E + 1) / 2;
+  constexpr int W = (kK || kMass) ? P : E;  // entries staged per element
+  __shared__ double acc[W * kElemTile];
   const bool signs = (A.flags & EMG_FLAG_NO_EDGE_SIGNS) == 0;
   const bool literal = (A.flags & EMG_FLAG_PIOLA_LITERAL) != 0;
-  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < A.n;
-       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t s0 = A.row_ptr[r], s1 = A.row_ptr[r + 1];
-    for (int32_t k = s0; k < s1; ++k) {
-      A.kval[k] = 0.0;
-      if (want_mass) A.mval[k] = 0.0;
+  const int tid = threadIdx.x;
+  for (int64_t t0 = static_cast<int64_t>(blockIdx.x) * kElemTile; t0 < n_el;
+       t0 += static_cast<int64_t>(gridDim.x) * kElemTile) {
+    const int cnt = static_cast<int>(n_el - t0 < kElemTile ? n_el - t0 : kElemTile);
+    const int64_t t = t0 + tid;
+#pragma unroll 1
+    for (int e = 0; e < W; ++e) acc[e * kElemTile + tid] = 0.0;
+    double ft[kSrc ? E : 1];
+#pragma unroll
+    for (int k = 0; k < (kSrc ? E : 1); ++k) ft[k] = 0.0;
+    const int32_t mid = t < n_el ? (A.material ? A.material[t] : 0) : -1;
+    bool use = mid >= 0 && mid < A.n_mat;  // em_assembly.cpp:270-276 skips the element
+    int32_t node[N];
+    double X[N][3];
+    if (use) {
+#pragma unroll
+      for (int a = 0; a < N; ++a) {
+        node[a] = A.elems[static_cast<int64_t>(N) * t + a];
+        if (node[a] < 0 || node[a] >= A.n_nodes) use = false;
+      }
+      if (!use) atomicOr(A.err, kErrNode);
     }
-    double f = 0.0;
-    for (int32_t u = A.inc_ptr[r]; u < A.inc_ptr[r + 1]; ++u) {
-      const int32_t slot = A.inc[u];
-      const int64_t t = slot / 12;
-      const int i = slot - 12 * static_cast<int>(t);
-      const int32_t mid = A.material ? A.material[t] : 0;
-      if (mid < 0 || mid >= A.n_mat) continue;  // em_assembly.cpp:270-276 skips the element
-      const int4 n0 = reinterpret_cast<const int4*>(A.elems)[2 * t];
-      const int4 n1 = reinterpret_cast<const int4*>(A.elems)[2 * t + 1];
-      const int32_t node[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};
-      double x[8][3];
-      bool ok = true;
+    if (use) {
 #pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        const int32_t gn = node[a];
-        if (gn < 0 || gn >= A.n_nodes) { ok = false; break; }
-        x[a][0] = A.xyz[3 * gn]; x[a][1] = A.xyz[3 * gn + 1]; x[a][2] = A.xyz[3 * gn + 2];
-      }
-      if (!ok) { atomicOr(A.err, kErrNode); continue; }
-      int sgi = 1;
+      for (int a = 0; a < N; ++a)
 #pragma unroll
-      for (int k = 0; k < 12; ++k)
-        if (k == i && signs) sgi = node[hex_edge_a(k)] < node[hex_edge_b(k)] ? 1 : -1;
-      const double nu = A.nu[mid];
-      const double sig = A.sigma ? A.sigma[mid] : 0.0;
-      const bool do_mass = want_mass && sig > 0.0;
-      const emg_source* tab = c_src;
-      int src_first = 0, src_count = A.n_src;
-      if (A.src_map) {
-        tab = A.src_tab;
-        const int32_t sid = A.src_map[t];
-        src_first = sid;
-        src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
-      }
-      const bool do_src = src_count > 0;
-      int32_t pos[12];
+        for (int r = 0; r < 3; ++r) X[a][r] = A.xyz[3 * static_cast<int64_t>(node[a]) + r];
+    }
+    const double nu = use ? A.nu[mid] : 0.0;
+    const double sig = use && A.sigma ? A.sigma[mid] : 0.0;
+    const emg_source* tab = c_src;
+    int src_first = 0, src_count = use ? A.n_src : 0;
+    if (use && A.src_map) {
+      tab = A.src_tab;
+      const int32_t sid = A.src_map[t];
+      src_first = sid;
+      src_count = (sid >= 0 && sid < A.n_src) ? 1 : 0;
+    }
+    const bool run = use && (kK || (kMass && sig > 0.0) || (kSrc && src_count > 0));
+    if (run) {
+#pragma unroll 1
+      for (int q = 0; q < S::kPoints; ++q) {
+        double x[3], wq, J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        S::point(q, x, &wq);
 #pragma unroll
-      for (int j = 0; j < 12; ++j) {
-        const int32_t c = A.l2g[12 * t + j];
-        pos[j] = c >= 0 ? find_slot(A.col, s0, s1, c) : -1;
-        if (c >= 0 && (pos[j] >= s1 || A.col[pos[j]] != c)) {
-          atomicOr(A.err, kErrSlot);
-          pos[j] = -1;
+        for (int a = 0; a < N; ++a) {
+          double d[3];
+          S::dn(a, x, d);
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) J[r][c] += X[a][r] * d[c];
         }
-      }
-      double krow[12], mrow[kMass ? 12 : 1];
-#pragma unroll
-      for (int j = 0; j < 12; ++j) krow[j] = 0.0;
-#pragma unroll
-      for (int j = 0; j < (kMass ? 12 : 1); ++j) mrow[j] = 0.0;
-      double fi = 0.0;
-      const int di = hex_dir(i);
-      for (int q = 0; q < 8; ++q) {
-        const double xi[3] = {(q & 1) ? g : -g, (q & 2) ? g : -g, (q & 4) ? g : -g};
-        // J[r][c] = dx_r / dxi_c of the trilinear map
-        double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const double s0 = hex_node_coord(a, 0), s1 = hex_node_coord(a, 1), s2 = hex_node_coord(a, 2);
-          const double l0 = 1.0 + s0 * xi[0], l1 = 1.0 + s1 * xi[1], l2 = 1.0 + s2 * xi[2];
-          const double dn[3] = {0.125 * s0 * l1 * l2, 0.125 * s1 * l0 * l2, 0.125 * s2 * l0 * l1};
-#pragma unroll
-          for (int rr = 0; rr < 3; ++rr)
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) J[rr][cc] += x[a][rr] * dn[cc];
-        }
-        // adjugate rows: inv(J) = adj / det
-        double adj[3][3];
-        adj[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-        adj[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
-        adj[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
-        adj[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-        adj[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
-        adj[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
-        adj[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-        adj[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
-        adj[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-        const double det = J[0][0] * adj[0][0] + J[0][1] * adj[1][0] + J[0][2] * adj[2][0];
-        // row d_i of adj (J^-1 = adj / det)
-        const double ad[3] = {di == 0 ? adj[0][0] : di == 1 ? adj[1][0] : adj[2][0],
-                              di == 0 ? adj[0][1] : di == 1 ? adj[1][1] : adj[2][1],
-                              di == 0 ? adj[0][2] : di == 1 ? adj[1][2] : adj[2][2]};
+        const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                           J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
         const double adet = fabs(det);
-        if (adet < 1e-15) continue;  // quadrature point skipped (magnetic_vector_3d_integrator.cpp:169)
-        // Physical curls (without the 1/det) u_k = J curl_ref_k and the
-        // reference basis magnitudes f_k for all 12 edges, the row's own
-        // picked out of the same arrays: every product below is formed from
-        // the same values in row i and row j, so K and M come out exactly
-        // symmetric whatever the contraction into FMAs.
-        double u[12][3], fk[12];
+        if (adet < 1e-15) continue;  // magnetic_vector_3d_integrator.cpp:169-176
+        if (kK) {
+          double c[E][3];
 #pragma unroll
-        for (int k = 0; k < 12; ++k) {
-          const int dk = hex_dir(k), pk = (dk + 1) % 3, qk = (dk + 2) % 3;
-          const double hk = 0.5 * hex_sgn(k);
-          const double lp = 1.0 + hex_cp(k) * xi[pk], lq = 1.0 + hex_cq(k) * xi[qk];
-          const double cp = hk * hex_cq(k) * lp, cq = -hk * hex_cp(k) * lq;
+          for (int k = 0; k < E; ++k) {
+            double cr[3];
+            S::curl(k, x, cr);
 #pragma unroll
-          for (int rr = 0; rr < 3; ++rr) u[k][rr] = J[rr][pk] * cp + J[rr][qk] * cq;
-          fk[k] = hk * lp * lq;  // W_ref_k = f_k e_{d_k}
-        }
-        double ui[3] = {0, 0, 0}, fi_q = 0.0;
-#pragma unroll
-        for (int k = 0; k < 12; ++k)
-          if (k == i) { ui[0] = u[k][0]; ui[1] = u[k][1]; ui[2] = u[k][2]; fi_q = fk[k]; }
-        const double kq = nu / adet;
-#pragma unroll
-        for (int j = 0; j < 12; ++j) krow[j] += kq * (ui[0] * u[j][0] + ui[1] * u[j][1] + ui[2] * u[j][2]);
-        if (do_mass || do_src) {
-          const double wscale = literal ? 1.0 / det : 1.0;
-          if (kMass && do_mass) {
-            // W_i . W_j = f_i f_j [adj adj^T]_{d_i d_j} / det^2, the 3x3 Gram
-            // matrix of the adjugate rows formed symmetrically
-            double H[3][3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int b = 0; b < 3; ++b) H[a][b] = adj[a][0] * adj[b][0] + adj[a][1] * adj[b][1] + adj[a][2] * adj[b][2];
-            const double Hi[3] = {di == 0 ? H[0][0] : di == 1 ? H[1][0] : H[2][0],
-                                  di == 0 ? H[0][1] : di == 1 ? H[1][1] : H[2][1],
-                                  di == 0 ? H[0][2] : di == 1 ? H[1][2] : H[2][2]};
-            const double mq = sig * adet * wscale * wscale / (det * det);
-#pragma unroll
-            for (int j = 0; j < (kMass ? 12 : 1); ++j) mrow[j] += (mq * (fi_q * fk[j])) * Hi[hex_dir(j)];
+            for (int r = 0; r < 3; ++r) c[k][r] = (J[r][0] * cr[0] + J[r][1] * cr[1] + J[r][2] * cr[2]) / det;
           }
-          if (do_src) {
-            double xq[3] = {0, 0, 0};
+          const double wk = wq * adet * nu;
+          int e = 0;
 #pragma unroll
-            for (int a = 0; a < 8; ++a) {
-              const double na = 0.125 * (1.0 + hex_node_coord(a, 0) * xi[0]) * (1.0 + hex_node_coord(a, 1) * xi[1]) *
-                                (1.0 + hex_node_coord(a, 2) * xi[2]);
+          for (int i = 0; i < E; ++i)
 #pragma unroll
-              for (int c = 0; c < 3; ++c) xq[c] += na * x[a][c];
+            for (int j = i; j < E; ++j, ++e)
+              acc[e * kElemTile + tid] += wk * (c[i][0] * c[j][0] + c[i][1] * c[j][1] + c[i][2] * c[j][2]);
+        } else {
+          double inv[3][3];
+          inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+          inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+          inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+          inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+          inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+          inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+          inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+          inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+          inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+          double Wp[E][3];
+#pragma unroll
+          for (int k = 0; k < E; ++k) {
+            double wr[3];
+            S::basis(k, x, wr);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              Wp[k][r] = inv[0][r] * wr[0] + inv[1][r] * wr[1] + inv[2][r] * wr[2];
+              if (literal) Wp[k][r] /= det;
             }
-            double js[3];
-            source_at(xq, tab, src_first, src_count, js);
-            const double ji = (ad[0] * js[0] + ad[1] * js[1] + ad[2] * js[2]) / det;
-            fi += adet * wscale * fi_q * ji;
+          }
+          if (kMass && sig > 0.0) {
+            const double wm = wq * adet * sig;
+            int e = 0;
+#pragma unroll
+            for (int i = 0; i < E; ++i)
+#pragma unroll
+              for (int j = i; j < E; ++j, ++e)
+                acc[e * kElemTile + tid] += wm * (Wp[i][0] * Wp[j][0] + Wp[i][1] * Wp[j][1] + Wp[i][2] * Wp[j][2]);
+          }
+          if (kSrc && src_count > 0) {
+            double p[3] = {0.0, 0.0, 0.0}, js[3];
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+              const double na = S::n(a, x);
+#pragma unroll
+              for (int r = 0; r < 3; ++r) p[r] += na * X[a][r];
+            }
+            source_at(p, tab, src_first, src_count, js);
+#pragma unroll
+            for (int k = 0; k < (kSrc ? E : 1); ++k)
+              ft[k] += wq * adet * (Wp[k][0] * js[0] + Wp[k][1] * js[1] + Wp[k][2] * js[2]);
           }
         }
       }
-#pragma unroll
-      for (int j = 0; j < 12; ++j) {
-        if (pos[j] < 0) continue;
-        const int sgj = signs ? (node[hex_edge_a(j)] < node[hex_edge_b(j)] ? 1 : -1) : 1;
-        A.kval[pos[j]] += static_cast<double>(sgi * sgj) * krow[j];
-        if (kMass && do_mass) A.mval[pos[j]] += static_cast<double>(sgi * sgj) * mrow[kMass ? j : 0];
-      }
-      f += sgi * fi;
     }
-    A.rhs[r] = f;
+    double sg[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) sg[k] = (!use || !signs || node[S::edge_a(k)] < node[S::edge_b(k)]) ? 1.0 : -1.0;
+    if (kK || kMass) {
+      int e = 0;
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+#pragma unroll
+        for (int j = i; j < E; ++j, ++e) acc[e * kElemTile + tid] *= sg[i] * sg[j];
+      __syncthreads();
+      double* out = kK ? ke : me;
+      for (int x = tid; x < cnt * P; x += kElemTile) out[t0 * P + x] = acc[(x % P) * kElemTile + x / P];
+      __syncthreads();
+    }
+    if (kSrc && !kK) {
+#pragma unroll
+      for (int k = 0; k < (kSrc ? E : 1); ++k) acc[k * kElemTile + tid] = sg[k] * ft[k];
+      __syncthreads();
+      for (int x = tid; x < cnt * E; x += kElemTile) fe[t0 * E + x] = acc[(x % E) * kElemTile + x / E];
+      __syncthreads();
+    }
   }
 }
+
+template <class S, bool kMass, bool kSrc>
+void launch_elem_assembly(const AsmArgs& a, int64_t n_el, double* ke, double* me, double* fe, cudaStream_t st) {
+  const int64_t tiles = (n_el + kElemTile - 1) / kElemTile;
+  const unsigned g = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(tiles, 148 * 32)));
+  k_elem_terms<S, true, false, false><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
+  if (kMass || kSrc) k_elem_terms<S, false, kMass, kSrc><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
+  const int64_t rb = (a.n * 16 + 255) / 256;
+  const unsigned gr = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(rb, 148 * 64)));
+  k_rows_from_terms<S::kEdges, kMass, kSrc><<<gr, 256, 0, st>>>(a, ke, me, fe);
+}
+
+template <class S>
+void launch_elem_assembly(const AsmArgs& a, int64_t n_el, bool mass, bool srcs, double* ke, double* me, double* fe,
+                          cudaStream_t st) {
+  if (mass && srcs) launch_elem_assembly<S, true, true>(a, n_el, ke, me, fe, st);
+  else if (mass) launch_elem_assembly<S, true, false>(a, n_el, ke, me, fe, st);
+  else if (srcs) launch_elem_assembly<S, false, true>(a, n_el, ke, me, fe, st);
+  else launch_elem_assembly<S, false, false>(a, n_el, ke, me, fe, st);
+}
+
 
 int grid_for(int64_t work, int threads, int max_blocks = 148 * 16) {
   int64_t b = (work + threads - 1) / threads;
@@ -814,6 +1055,17 @@ int system_build(System& s, cudaStream_t st) {
   k_row_columns<<<grid_for(n * 32, 128), 128, 0, st>>>(n, epe, s.inc_ptr, tmp, s.K.row_ptr, s.K.col);
   EMG_CK(cudaGetLastError());
   EMG_CK(cudaFreeAsync(tmp, st));
+  if (epe == 6) {  // TET4_EDGE: column positions of every incidence slot, for the numeric gather
+    int32_t* dmax = nullptr;
+    EMG_CK(cudaMallocAsync(&dmax, sizeof(int32_t), st));
+    EMG_CK(cudaMemsetAsync(dmax, 0, sizeof(int32_t), st));
+    EMG_CK(cudaMallocAsync(&s.slot_pos, 8 * std::max<int64_t>(inc_total, 1), st));
+    k_slot_positions<<<grid_for(n, 128), 128, 0, st>>>(n, s.inc_ptr, s.inc, s.l2g, s.K.row_ptr, s.K.col,
+                                                       s.slot_pos, dmax);
+    EMG_CK(cudaGetLastError());
+    EMG_CK(cudaMemcpyAsync(&s.max_row_len, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaFreeAsync(dmax, st));
+  }
   EMG_CK(cudaMallocAsync(&s.rhs, sizeof(double) * (n > 0 ? n : 1), st));
   EMG_CK(cudaMemsetAsync(s.rhs, 0, sizeof(double) * (n > 0 ? n : 1), st));
   EMG_CK(cudaMemsetAsync(s.K.val, 0, sizeof(double) * (nnz > 0 ? nnz : 1), st));
@@ -866,13 +1118,42 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
   a.nu = mat; a.sigma = mat + n_mat; a.n_mat = n_mat; a.n_src = n_src; a.flags = flags;
   a.src_tab = src_tab; a.src_map = s.src_map;
   a.kval = s.K.val; a.mval = mass ? s.M.val : nullptr; a.rhs = s.rhs; a.err = s.err;
-  if (s.elem_type == EMG_ELEM_HEX8_EDGE && mass)
-    k_assemble_rows_hex<true><<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
-  else if (s.elem_type == EMG_ELEM_HEX8_EDGE)
-    k_assemble_rows_hex<false><<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
-  else
-    k_assemble_rows<<<grid_for(s.n, 128, 148 * 32), 128, 0, st>>>(a);
+  // per-element terms: packed K and M (P = E (E + 1) / 2 each, M with the
+  // mass matrix) and F (E, with sources)
+  double* terms = nullptr;
+  const bool srcs = n_src > 0;
+  if (s.elem_type != EMG_ELEM_TET4_EDGE) {
+    const int64_t T = s.n_elems, E = edges_per_elem(s.elem_type), P = E * (E + 1) / 2;
+    const int64_t width = P + (mass ? P : 0) + (srcs ? E : 0);
+    EMG_CK(cudaMallocAsync(&terms, sizeof(double) * std::max<int64_t>(width * T, 1), st));
+    double* ke = terms;
+    double* me = mass ? terms + P * T : nullptr;
+    double* fe = srcs ? terms + (mass ? 2 * P : P) * T : nullptr;
+    if (s.elem_type == EMG_ELEM_HEX8_EDGE) launch_elem_assembly<shape::Hex>(a, T, mass, srcs, ke, me, fe, st);
+    else if (s.elem_type == EMG_ELEM_PRISM6_EDGE) launch_elem_assembly<shape::Prism>(a, T, mass, srcs, ke, me, fe, st);
+    else launch_elem_assembly<shape::Pyramid>(a, T, mass, srcs, ke, me, fe, st);
+  } else {
+    if (reinterpret_cast<uintptr_t>(s.l2g) % 8 != 0) {
+      cudaFreeAsync(mat, st);
+      if (src_tab) cudaFreeAsync(src_tab, st);
+      set_error("assembly: the DOF map must be 8-byte aligned");
+      return EMG_INVALID_INPUT;
+    }
+    const int64_t T = s.n_elems;
+    const int64_t width = kKe + (mass ? kKe : 0) + (srcs ? 6 : 0);
+    EMG_CK(cudaMallocAsync(&terms, sizeof(double) * std::max<int64_t>(width * T, 1), st));
+    double* ke = terms;
+    double* me = mass ? terms + kKe * T : nullptr;
+    double* fe = srcs ? terms + (mass ? 2 * kKe : kKe) * T : nullptr;
+    const uint8_t* sp = s.slot_pos;
+    const int32_t ml = s.max_row_len;
+    if (mass && srcs) launch_tet_assembly<true, true>(a, T, sp, ml, ke, me, fe, st);
+    else if (mass) launch_tet_assembly<true, false>(a, T, sp, ml, ke, me, fe, st);
+    else if (srcs) launch_tet_assembly<false, true>(a, T, sp, ml, ke, me, fe, st);
+    else launch_tet_assembly<false, false>(a, T, sp, ml, ke, me, fe, st);
+  }
   EMG_CK(cudaGetLastError());
+  if (terms) EMG_CK(cudaFreeAsync(terms, st));
   ++s.K.version;
   if (mass) ++s.M.version;
   int32_t herr = 0;
@@ -889,7 +1170,8 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
 System::~System() {
   for (void* p : {static_cast<void*>(xyz), static_cast<void*>(elems), static_cast<void*>(material),
                   static_cast<void*>(l2g), static_cast<void*>(inc_ptr), static_cast<void*>(inc),
-                  static_cast<void*>(err), static_cast<void*>(rhs), static_cast<void*>(src_map)})
+                  static_cast<void*>(err), static_cast<void*>(rhs), static_cast<void*>(src_map),
+                  static_cast<void*>(slot_pos)})
     if (p) cudaFreeAsync(p, 0);
 }
 

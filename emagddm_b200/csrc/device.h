@@ -58,6 +58,10 @@ struct System {
   int32_t* err = nullptr;      // device error word
   double* rhs = nullptr;       // n
   int32_t* src_map = nullptr;  // optional per-element source index (n_elems)
+  // TET4_EDGE: for every incidence slot (8 bytes each), the position of the
+  // slot's element columns 0..5 inside the row (0xFF: constrained edge)
+  uint8_t* slot_pos = nullptr;
+  int32_t max_row_len = 0;     // longest CSR row
   DevCsr K, M;                 // M shares K's pattern
   bool has_mass = false;
   ~System();

@@ -13,15 +13,30 @@ namespace emg {
 void set_error(const std::string& msg);
 
 // Local node pairs of the element edges, ElementGeometry::get_local_edges
-// (src/fe_em/element_geometry.cpp:115-126 TET4, :161-181 HEX8).
+// (src/fe_em/element_geometry.cpp:115-126 TET4, :161-181 HEX8, :214-237
+// PRISM6, :268-289 PYRAMID5).
 constexpr int kTetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
 constexpr int kHexEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+constexpr int kPrismEdge[9][2] = {{0, 1}, {1, 2}, {0, 2}, {3, 4}, {4, 5}, {3, 5}, {0, 3}, {1, 4}, {2, 5}};
+constexpr int kPyramidEdge[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 4}, {2, 4}, {3, 4}};
 
-inline bool valid_elem_type(int32_t t) { return t == EMG_ELEM_TET4_EDGE || t == EMG_ELEM_HEX8_EDGE; }
-inline int nodes_per_elem(int32_t t) { return t == EMG_ELEM_HEX8_EDGE ? 8 : 4; }
-inline int edges_per_elem(int32_t t) { return t == EMG_ELEM_HEX8_EDGE ? 12 : 6; }
-inline const int (*local_edges(int32_t t))[2] { return t == EMG_ELEM_HEX8_EDGE ? kHexEdge : kTetEdge; }
+inline bool valid_elem_type(int32_t t) {
+  return t == EMG_ELEM_TET4_EDGE || t == EMG_ELEM_HEX8_EDGE || t == EMG_ELEM_PRISM6_EDGE ||
+         t == EMG_ELEM_PYRAMID5_EDGE;
+}
+inline int nodes_per_elem(int32_t t) {
+  return t == EMG_ELEM_HEX8_EDGE ? 8 : t == EMG_ELEM_PRISM6_EDGE ? 6 : t == EMG_ELEM_PYRAMID5_EDGE ? 5 : 4;
+}
+inline int edges_per_elem(int32_t t) {
+  return t == EMG_ELEM_HEX8_EDGE ? 12 : t == EMG_ELEM_PRISM6_EDGE ? 9 : t == EMG_ELEM_PYRAMID5_EDGE ? 8 : 6;
+}
+inline const int (*local_edges(int32_t t))[2] {
+  return t == EMG_ELEM_HEX8_EDGE       ? kHexEdge
+         : t == EMG_ELEM_PRISM6_EDGE   ? kPrismEdge
+         : t == EMG_ELEM_PYRAMID5_EDGE ? kPyramidEdge
+                                       : kTetEdge;
+}
 
 struct Mesh {
   int32_t elem_type = EMG_ELEM_TET4_EDGE;

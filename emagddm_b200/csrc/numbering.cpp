@@ -55,15 +55,23 @@ int build_edge_ids(Mesh& m) {
       bk.a[s] = std::max(u, w);
       bk.b[s] = static_cast<int32_t>(epe * t + k);
     }
-  // leader position of every entry
+  // leader position of every entry: the bucket's distinct hi nodes so far
+  // (a handful per node) are searched instead of all its earlier entries
   std::vector<int32_t> leader(M);
   std::vector<uint8_t> is_leader(M, 0);
+  std::vector<int32_t> seen_hi, seen_pos;
   for (int64_t v = 0; v < V; ++v) {
+    seen_hi.clear();
+    seen_pos.clear();
     for (int64_t s = bk.ptr[v]; s < bk.ptr[v + 1]; ++s) {
-      int64_t f = bk.ptr[v];
-      while (bk.a[f] != bk.a[s]) ++f;  // first entry with the same hi
-      leader[bk.b[s]] = bk.b[f];
-      if (f == s) is_leader[bk.b[s]] = 1;
+      size_t f = 0;
+      while (f < seen_hi.size() && seen_hi[f] != bk.a[s]) ++f;
+      if (f == seen_hi.size()) {  // first entry with this hi
+        seen_hi.push_back(bk.a[s]);
+        seen_pos.push_back(bk.b[s]);
+        is_leader[bk.b[s]] = 1;
+      }
+      leader[bk.b[s]] = seen_pos[f];
     }
   }
   std::vector<int32_t> id_at(M, -1);

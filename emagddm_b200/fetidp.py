@@ -13,7 +13,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import _abi
+from . import _abi, mesh
 from ._abi import check, lib, ptr
 
 
@@ -36,7 +36,7 @@ class _MeshHandle:
         self.material = np.ascontiguousarray(m.material, np.int32)
         d = np.ascontiguousarray(m.dirichlet, np.int32)
         self.h = C.c_void_p()
-        et = 1 if self.tets.shape[1] == 8 else 0
+        et = mesh.TYPE_OF_NODES[self.tets.shape[1]]
         check(lib().emg_mesh_create_typed(et, self.xyz.shape[0], ptr(self.xyz), self.tets.shape[0],
                                           ptr(self.tets), ptr(self.material), d.shape[0], ptr(d) if d.size else None,
                                           0, C.byref(self.h)), "emg_mesh_create_typed")
@@ -67,7 +67,7 @@ def partitioned_dofmap(m, tet_part, n_parts: int, keep_handles: bool = False):
           "emg_dof_build_partitioned")
     ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
     lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
-    l2g = np.empty((m.n_tets, 12 if m.tets.shape[1] == 8 else 6), np.int32)
+    l2g = np.empty((m.n_tets, mesh.EDGES_OF_TYPE[m.elem_type]), np.int32)
     ed = np.empty(ne.value, np.int32)
     lib().emg_dofmap_export(h, ptr(l2g), ptr(ed))
     npart, npri, nfix = C.c_int32(), C.c_int64(), C.c_int64()
@@ -158,7 +158,7 @@ def gauged_map(m, gauge: int):
     check(lib().emg_dof_build(mh.h, int(gauge), C.byref(h)), "emg_dof_build")
     ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
     lib().emg_dofmap_info(h, C.byref(ne), C.byref(nf), C.byref(nd))
-    l2g = np.empty((m.n_tets, 12 if m.tets.shape[1] == 8 else 6), np.int32)
+    l2g = np.empty((m.n_tets, mesh.EDGES_OF_TYPE[m.elem_type]), np.int32)
     lib().emg_dofmap_export(h, ptr(l2g), None)
     return _MapHandle(h), mh, l2g, nd.value
 

@@ -15,7 +15,12 @@ benchmark use:
 
 The ``hex_*`` variants keep the hexes themselves as HEX8_EDGE elements
 (vertex order v0..v7 above, ElementGeometry's HEX8 order); a ``CubeMesh``
-whose ``tets`` array has 8 columns is a hex mesh.
+whose ``tets`` array has 8 columns is a hex mesh.  The ``prism_*`` variants
+split every hex into two PRISM6_EDGE elements (triangles (v0, v1, v2) and
+(v0, v2, v3) extruded along z; nodes bottom 0-2, top 3-5), the ``pyramid_*``
+variants into six PYRAMID5_EDGE elements, one per hex face, with the apex at
+an added node in the hex centre (gid (n+1)^3 + hex index).  The element
+type follows the number of columns of ``tets``: 4, 8, 6 or 5.
 """
 from __future__ import annotations
 
@@ -32,9 +37,18 @@ GEO_EDGES = np.array([[0, 1], [1, 2], [0, 2], [0, 3], [1, 3], [2, 3]], dtype=np.
 # HEX8 local edges, ElementGeometry::get_local_edges(HEX8)
 HEX_EDGES = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6], [6, 7], [7, 4],
                       [0, 4], [1, 5], [2, 6], [3, 7]], dtype=np.int64)
+# PRISM6 and PYRAMID5 local edges, ElementGeometry::get_local_edges
+PRISM_EDGES = np.array([[0, 1], [1, 2], [0, 2], [3, 4], [4, 5], [3, 5], [0, 3], [1, 4], [2, 5]], dtype=np.int64)
+PYRAMID_EDGES = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [0, 4], [1, 4], [2, 4], [3, 4]], dtype=np.int64)
 # Element types (same values as the C ABI's EMG_ELEM_*).
 ELEM_TET4_EDGE = 0
 ELEM_HEX8_EDGE = 1
+ELEM_PRISM6_EDGE = 2
+ELEM_PYRAMID5_EDGE = 3
+TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE}
+EDGES_OF_TYPE = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8}
+LOCAL_EDGES = {ELEM_TET4_EDGE: GEO_EDGES, ELEM_HEX8_EDGE: HEX_EDGES, ELEM_PRISM6_EDGE: PRISM_EDGES,
+               ELEM_PYRAMID5_EDGE: PYRAMID_EDGES}
 
 # Source region kinds (same values as the C ABI's EMG_SRC_*).
 SRC_BOX = 1
@@ -74,7 +88,7 @@ class CubeMesh:
 
     @property
     def elem_type(self) -> int:
-        return ELEM_HEX8_EDGE if self.tets.shape[1] == 8 else ELEM_TET4_EDGE
+        return TYPE_OF_NODES[self.tets.shape[1]]
 
 
 def cube_topology(n: int):
@@ -115,11 +129,40 @@ def hex_topology(n: int):
     return xyz.copy(), hexes.copy(), dirichlet.copy()
 
 
+def prism_topology(n: int):
+    """Nodes, PRISM6 elements (two per grid cell) and boundary-face edge pairs
+    of the n^3 cube."""
+    xyz, hexes, _ = _hex_topology(n)
+    # ElementGeometry's PRISM6 order with the reference's PRISM6 map (node 0 at
+    # area coordinate xi, node 1 at eta, node 2 at the right angle) gives a
+    # positive Jacobian for these triangles
+    a = hexes[:, [0, 1, 2, 4, 5, 6]]
+    b = hexes[:, [0, 2, 3, 4, 6, 7]]
+    prisms = np.stack([a, b], axis=1).reshape(-1, 6).astype(np.int32)
+    return xyz.copy(), prisms, _boundary_pairs(prisms, PRISM_EDGES, n)
+
+
+def pyramid_topology(n: int):
+    """Nodes (the grid plus one centre node per cell), PYRAMID5 elements (six
+    per cell, base = a cell face ordered so that the apex lies on the side the
+    reference map puts it) and boundary-face edge pairs of the n^3 cube."""
+    xyz, hexes, _ = _hex_topology(n)
+    n1 = n + 1
+    centres = xyz[hexes].mean(axis=1)
+    cid = (n1 ** 3 + np.arange(len(hexes))).astype(np.int32)
+    faces = [[0, 1, 2, 3], [4, 7, 6, 5], [0, 4, 5, 1], [3, 2, 6, 7], [0, 3, 7, 4], [1, 5, 6, 2]]
+    pyr = np.stack([np.concatenate([hexes[:, f], cid[:, None]], axis=1) for f in faces], axis=1)
+    return np.vstack([xyz, centres]), pyr.reshape(-1, 5).astype(np.int32), _boundary_pairs(pyr.reshape(-1, 5),
+                                                                                           PYRAMID_EDGES, n)
+
+
 def _boundary_pairs(elems, local_edges, n):
     """Unique element edges whose two nodes share a coordinate plane at 0 or
-    n (grid indices), as sorted node pairs."""
+    n (grid indices), as sorted node pairs (nodes beyond the grid, such as
+    cell centres, lie on no boundary)."""
     n1 = n + 1
     e = elems[:, local_edges].reshape(-1, 2).astype(np.int64)
+    e = e[(e < n1 ** 3).all(axis=1)]
     e.sort(axis=1)
     e = np.unique(e[:, 0] * (n1 ** 3) + e[:, 1])
     a, b = e // (n1 ** 3), e % (n1 ** 3)
@@ -180,6 +223,40 @@ def hex_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
     m = plain_scale(1, mu_iron)
     return CubeMesh(n=n, xyz=xyz, tets=hexes, material=iron.astype(np.int32), dirichlet=dirichlet,
                     nu=m.nu, sigma=m.sigma, sources=m.sources, name=f"hex{n}_iron_coil")
+
+
+def _on_cells(kind: str, n: int, mu_iron: float, small: bool) -> CubeMesh:
+    xyz, elems, dirichlet = prism_topology(n) if kind == "prism" else pyramid_topology(n)
+    if small:
+        m = plain_small(1)
+        mat = np.zeros(len(elems), np.int32)
+    else:
+        m = plain_scale(1, mu_iron)
+        c = centroids(xyz, elems)
+        mat = ((c[:, 0] > 0.25) & (c[:, 0] < 0.75) & (c[:, 1] > 0.25) & (c[:, 1] < 0.75)
+               & (c[:, 2] > 0.4) & (c[:, 2] < 0.6)).astype(np.int32)
+    return CubeMesh(n=n, xyz=xyz, tets=elems, material=mat, dirichlet=dirichlet, nu=m.nu, sigma=m.sigma,
+                    sources=m.sources, name=f"{kind}{n}_{'box' if small else 'iron_coil'}")
+
+
+def prism_small(n: int = 16) -> CubeMesh:
+    """plain_small on PRISM6_EDGE elements."""
+    return _on_cells("prism", n, 1.0, True)
+
+
+def prism_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
+    """plain_scale on PRISM6_EDGE elements (iron block by element centroid)."""
+    return _on_cells("prism", n, mu_iron, False)
+
+
+def pyramid_small(n: int = 16) -> CubeMesh:
+    """plain_small on PYRAMID5_EDGE elements."""
+    return _on_cells("pyramid", n, 1.0, True)
+
+
+def pyramid_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
+    """plain_scale on PYRAMID5_EDGE elements (iron block by element centroid)."""
+    return _on_cells("pyramid", n, mu_iron, False)
 
 
 def jittered_cuts(n: int, parts: int = 4, seed: int = 20261203, jitter: int | None = None):

@@ -54,10 +54,13 @@ enum {
 
 /* ---- element types (numeric::ElementType, include/numeric/shape_function_base.hpp:51-57)
  * One type per mesh.  Local node and edge order follow ElementGeometry
- * (src/fe_em/element_geometry.cpp:112-126 TET4, :158-181 HEX8). */
+ * (src/fe_em/element_geometry.cpp:112-126 TET4, :158-181 HEX8, :214-237
+ * PRISM6, :268-289 PYRAMID5). */
 enum {
-  EMG_ELEM_TET4_EDGE = 0,  /* 4 nodes, 6 edges                                     */
-  EMG_ELEM_HEX8_EDGE = 1   /* 8 nodes (bottom face 0-3, top face 4-7 above them), 12 edges */
+  EMG_ELEM_TET4_EDGE = 0,    /* 4 nodes, 6 edges                                     */
+  EMG_ELEM_HEX8_EDGE = 1,    /* 8 nodes (bottom face 0-3, top face 4-7 above them), 12 edges */
+  EMG_ELEM_PRISM6_EDGE = 2,  /* 6 nodes (bottom triangle 0-2, top 3-5 above them), 9 edges */
+  EMG_ELEM_PYRAMID5_EDGE = 3 /* 5 nodes (base quadrilateral 0-3, apex 4), 8 edges    */
 };
 
 /* ---- assembly flags ------------------------------------------------------ */
@@ -126,10 +129,11 @@ int emg_mesh_create(int64_t n_nodes, const double* xyz, int64_t n_tets, const in
                     const int32_t* material_id, int64_t n_dirichlet,
                     const int32_t* dirichlet_pairs, int32_t n_hole_markers, emg_mesh* out);
 /* Same for a mesh of one element type (EMG_ELEM_*): elems holds
- * nodes_per_elem * n_elems node indices (4 for TET4_EDGE, 8 for HEX8_EDGE);
+ * nodes_per_elem * n_elems node indices (4 TET4_EDGE, 8 HEX8_EDGE, 6 PRISM6_EDGE,
+ * 5 PYRAMID5_EDGE);
  * emg_mesh_create is elem_type = EMG_ELEM_TET4_EDGE.  Everything downstream
  * (edge IDs, DOF maps, gauges, systems, the FETI-DP and direct solvers) then
- * works per element with edges_per_elem (6 or 12) local edges; arrays
+ * works per element with edges_per_elem (6, 12, 9 or 8) local edges; arrays
  * documented below as 4*n_tets / 6*n_tets hold nodes_per_elem*n_elems /
  * edges_per_elem*n_elems entries for such a mesh. */
 int emg_mesh_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_elems,

@@ -40,7 +40,8 @@ struct SolverResult {
 inline std::string last_error() { return emg_last_error(); }
 
 // fe_em::EMMeshData restricted to the edge path: nodes (id = index), elements
-// of one type (TET4_EDGE: 4 nodes each, HEX8_EDGE: 8) with material ids,
+// of one type (TET4_EDGE: 4 nodes each, HEX8_EDGE: 8, PRISM6_EDGE: 6,
+// PYRAMID5_EDGE: 5) with material ids,
 // Dirichlet edge node pairs, hole-marker count.
 class Mesh {
  public:
@@ -61,8 +62,12 @@ class Mesh {
   Mesh& operator=(const Mesh&) = delete;
   emg_mesh handle() const { return h_; }
   int32_t elementType() const { return type_; }
-  int nodesPerElement() const { return type_ == EMG_ELEM_HEX8_EDGE ? 8 : 4; }
-  int edgesPerElement() const { return type_ == EMG_ELEM_HEX8_EDGE ? 12 : 6; }
+  int nodesPerElement() const {
+    return type_ == EMG_ELEM_HEX8_EDGE ? 8 : type_ == EMG_ELEM_PRISM6_EDGE ? 6 : type_ == EMG_ELEM_PYRAMID5_EDGE ? 5 : 4;
+  }
+  int edgesPerElement() const {
+    return type_ == EMG_ELEM_HEX8_EDGE ? 12 : type_ == EMG_ELEM_PRISM6_EDGE ? 9 : type_ == EMG_ELEM_PYRAMID5_EDGE ? 8 : 6;
+  }
   int64_t getNodeCount() const { return static_cast<int64_t>(xyz_.size() / 3); }
   int64_t getElementCount() const { return static_cast<int64_t>(elems_.size() / nodesPerElement()); }
   const std::vector<double>& xyz() const { return xyz_; }
@@ -90,7 +95,7 @@ class GlobalEdgeIDGenerator {
     emg_edge_ids(mesh_.handle(), elem_edge_.data(), edge_nodes_.data(), &n);
   }
   int getNumGlobalEdges() const { return static_cast<int>(edge_nodes_.size() / 2); }
-  // element-major, 6 (TET4) or 12 (HEX8) local edges per element in
+  // element-major, 6 (TET4), 12 (HEX8), 9 (PRISM6) or 8 (PYRAMID5) local edges per element in
   // ElementGeometry's order
   const std::vector<int32_t>& getElemLocalToGlobalEdge() const { return elem_edge_; }
   const std::vector<int32_t>& getEdgeNodes() const { return edge_nodes_; }
@@ -182,7 +187,8 @@ class EMDOFManager {
   std::vector<int32_t> l2g_, edge_dof_;
 };
 
-// numeric::EMAssembly for TET4_EDGE / HEX8_EDGE on the GPU (src/numeric/em_assembly.cpp:144-420).
+// numeric::EMAssembly for TET4_EDGE / HEX8_EDGE / PRISM6_EDGE / PYRAMID5_EDGE on the GPU
+// (src/numeric/em_assembly.cpp:144-420).
 // Materials are reluctivity nu = 1/mu and conductivity sigma per material id.
 class GpuEMAssembly {
  public:

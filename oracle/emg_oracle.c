@@ -47,6 +47,10 @@ static const int NED_EDGE[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3
  * runs from node [k][0] to node [k][1] (nedelec_element.cpp:506-517). */
 static const int HEX_EDGE[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                     {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+/* PRISM6 and PYRAMID5 geometry edge tables (element_geometry.cpp:214-237,
+ * :268-289); the basis of edge k runs from node [k][0] to node [k][1]. */
+static const int PRISM_EDGE[9][2] = {{0, 1}, {1, 2}, {0, 2}, {3, 4}, {4, 5}, {3, 5}, {0, 3}, {1, 4}, {2, 5}};
+static const int PYR_EDGE[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 4}, {2, 4}, {3, 4}};
 /* HEX8 reference node coordinates (lagrange_element.cpp:765-772). */
 static const double HEX_NODE[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
                                       {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
@@ -101,6 +105,8 @@ static int radix_sort_u64(int64_t n, uint64_t* key, int64_t* pay, uint64_t max_k
 static int elem_shape(int32_t elem_type, int* npe, int* epe, const int (**tab)[2]) {
   if (elem_type == ORC_ELEM_TET4_EDGE) { *npe = 4; *epe = 6; *tab = GEO_EDGE; return 0; }
   if (elem_type == ORC_ELEM_HEX8_EDGE) { *npe = 8; *epe = 12; *tab = HEX_EDGE; return 0; }
+  if (elem_type == ORC_ELEM_PRISM6_EDGE) { *npe = 6; *epe = 9; *tab = PRISM_EDGE; return 0; }
+  if (elem_type == ORC_ELEM_PYRAMID5_EDGE) { *npe = 5; *epe = 8; *tab = PYR_EDGE; return 0; }
   return ORC_INVALID_INPUT;
 }
 
@@ -666,6 +672,240 @@ void orc_edge_signs_hex(const int32_t* hex, int32_t* s) {
 }
 
 /* ---------------------------------------------------------------------------
+ * PRISM6_EDGE and PYRAMID5_EDGE elements.  The reference calls
+ * getPoints(PRISM6_EDGE / PYRAMID5_EDGE), which returns no points
+ * (gauss_quadrature.cpp:36-60): its literal K_e is zero.  Intended
+ * formulas, restated here independently of the library's kernels:
+ *  - prism: PRISM6 Lagrange map (lagrange_element.cpp:458-522: node a < 3
+ *    has area coordinate L_a, L_0 = xi, L_1 = eta, L_2 = 1 - xi - eta, at
+ *    zeta = -1, node a + 3 the same at zeta = +1), the basis forms of
+ *    evalPrism6Edge (nedelec_element.cpp:744-792) placed on their own edges
+ *    with unit circulation, the reference's 6-point rule
+ *    (gauss_quadrature.cpp:304-345);
+ *  - pyramid: PYRAMID5 Lagrange map (lagrange_element.cpp:51-135: base
+ *    corners N_a = (1 - zeta) P_a(xi, eta), apex N_4 = zeta, zeta in
+ *    [0, 1]), a conforming basis (base edges 1/4 (1 +- x_perp)(1 - zeta)^2
+ *    along the edge, slant edges N_a grad N_4 - N_4 grad N_a), 2 x 2 x 3
+ *    Gauss-Legendre points on [-1, 1]^2 x [0, 1].
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int npe, epe, nq;
+  void (*point)(int q, double* x, double* w);
+  void (*grad)(int a, const double* x, double* d);     /* dN_a / d(xi, eta, zeta) */
+  double (*value)(int a, const double* x);              /* N_a */
+  void (*basis)(int k, const double* x, double* w);    /* W_k, reference components */
+  void (*curl)(int k, const double* x, double* c);     /* reference curl of W_k */
+} orc_shape;
+
+static const double PR_DL[3][2] = {{1.0, 0.0}, {0.0, 1.0}, {-1.0, -1.0}};
+static double pr_l(int a, const double* x) { return a == 0 ? x[0] : a == 1 ? x[1] : 1.0 - x[0] - x[1]; }
+static void pr_point(int q, double* x, double* w) {
+  static const double tri[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
+  const double g = 1.0 / sqrt(3.0);
+  x[0] = tri[q % 3][0];
+  x[1] = tri[q % 3][1];
+  x[2] = q < 3 ? -g : g; /* zeta outer loop, triangle points inner */
+  *w = 1.0 / 6.0;
+}
+static double pr_value(int a, const double* x) {
+  return pr_l(a % 3, x) * (a < 3 ? 0.5 * (1.0 - x[2]) : 0.5 * (1.0 + x[2]));
+}
+static void pr_grad(int a, const double* x, double* d) {
+  const double h = a < 3 ? 0.5 * (1.0 - x[2]) : 0.5 * (1.0 + x[2]);
+  d[0] = h * PR_DL[a % 3][0];
+  d[1] = h * PR_DL[a % 3][1];
+  d[2] = (a < 3 ? -0.5 : 0.5) * pr_l(a % 3, x);
+}
+static void pr_basis(int k, const double* x, double* w) {
+  if (k >= 6) { w[0] = 0.0; w[1] = 0.0; w[2] = 0.5 * pr_l(k - 6, x); return; }
+  const int a = PRISM_EDGE[k][0] % 3, b = PRISM_EDGE[k][1] % 3;
+  const double h = k < 3 ? 0.5 * (1.0 - x[2]) : 0.5 * (1.0 + x[2]);
+  for (int c = 0; c < 2; c++) w[c] = h * (pr_l(a, x) * PR_DL[b][c] - pr_l(b, x) * PR_DL[a][c]);
+  w[2] = 0.0;
+}
+static void pr_curl(int k, const double* x, double* c) {
+  if (k >= 6) { c[0] = 0.5 * PR_DL[k - 6][1]; c[1] = -0.5 * PR_DL[k - 6][0]; c[2] = 0.0; return; }
+  const int a = PRISM_EDGE[k][0] % 3, b = PRISM_EDGE[k][1] % 3;
+  const double h = k < 3 ? 0.5 * (1.0 - x[2]) : 0.5 * (1.0 + x[2]), dh = k < 3 ? -0.5 : 0.5;
+  double wv[2];
+  for (int i = 0; i < 2; i++) wv[i] = pr_l(a, x) * PR_DL[b][i] - pr_l(b, x) * PR_DL[a][i];
+  /* grad(h) x w + h curl(w), curl(w) = 2 grad L_a x grad L_b */
+  c[0] = -dh * wv[1];
+  c[1] = dh * wv[0];
+  c[2] = 2.0 * h * (PR_DL[a][0] * PR_DL[b][1] - PR_DL[a][1] * PR_DL[b][0]);
+}
+
+static const double PY_C[4][2] = {{-1.0, -1.0}, {1.0, -1.0}, {1.0, 1.0}, {-1.0, 1.0}};
+static void py_point(int q, double* x, double* w) {
+  const double g = 1.0 / sqrt(3.0), s = sqrt(0.6);
+  const double zt[3] = {-s, 0.0, s}, zw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  x[0] = (q / 6) ? g : -g;
+  x[1] = ((q / 3) % 2) ? g : -g;
+  x[2] = 0.5 * (1.0 + zt[q % 3]);
+  *w = 0.5 * zw[q % 3];
+}
+static double py_p(int a, const double* x) { return 0.25 * (1.0 + PY_C[a][0] * x[0]) * (1.0 + PY_C[a][1] * x[1]); }
+static double py_value(int a, const double* x) { return a == 4 ? x[2] : (1.0 - x[2]) * py_p(a, x); }
+static void py_grad(int a, const double* x, double* d) {
+  if (a == 4) { d[0] = 0.0; d[1] = 0.0; d[2] = 1.0; return; }
+  d[0] = (1.0 - x[2]) * 0.25 * PY_C[a][0] * (1.0 + PY_C[a][1] * x[1]);
+  d[1] = (1.0 - x[2]) * 0.25 * PY_C[a][1] * (1.0 + PY_C[a][0] * x[0]);
+  d[2] = -py_p(a, x);
+}
+static void py_basis(int k, const double* x, double* w) {
+  const double r2 = (1.0 - x[2]) * (1.0 - x[2]);
+  w[0] = w[1] = w[2] = 0.0;
+  if (k < 4) {
+    /* along +-e_xi (edges 0, 2) or +-e_eta (1, 3), vanishing on the opposite side */
+    const int axis = k & 1;
+    const double dir = PY_C[PYR_EDGE[k][1]][axis] - PY_C[PYR_EDGE[k][0]][axis]; /* +-2 */
+    const double side = PY_C[PYR_EDGE[k][0]][1 - axis];                           /* fixed coordinate */
+    w[axis] = 0.125 * dir * (1.0 + side * x[1 - axis]) * r2;
+    return;
+  }
+  const int a = k - 4;
+  double d[3];
+  py_grad(a, x, d);
+  /* N_a grad N_4 - N_4 grad N_a */
+  const double na = py_value(a, x), n4 = x[2];
+  w[0] = -n4 * d[0];
+  w[1] = -n4 * d[1];
+  w[2] = na - n4 * d[2];
+}
+static void py_curl(int k, const double* x, double* c) {
+  const double r = 1.0 - x[2];
+  if (k < 4) {
+    const int axis = k & 1;
+    const double dir = PY_C[PYR_EDGE[k][1]][axis] - PY_C[PYR_EDGE[k][0]][axis];
+    const double side = PY_C[PYR_EDGE[k][0]][1 - axis];
+    const double f = 0.125 * dir * (1.0 + side * x[1 - axis]); /* W_axis = f r^2 */
+    const double df = 0.125 * dir * side;                      /* d f / d x_other */
+    /* curl (0-form components): axis 0: (0, dW0/dz, -dW0/dy); axis 1: (-dW1/dz, 0, dW1/dx) */
+    if (axis == 0) { c[0] = 0.0; c[1] = -2.0 * f * r; c[2] = -df * r * r; }
+    else { c[0] = 2.0 * f * r; c[1] = 0.0; c[2] = df * r * r; }
+    return;
+  }
+  /* 2 grad N_a x grad N_4 */
+  double d[3];
+  py_grad(k - 4, x, d);
+  c[0] = 2.0 * d[1];
+  c[1] = -2.0 * d[0];
+  c[2] = 0.0;
+}
+
+static const orc_shape ORC_PRISM = {6, 9, 6, pr_point, pr_grad, pr_value, pr_basis, pr_curl};
+static const orc_shape ORC_PYRAMID = {5, 8, 12, py_point, py_grad, py_value, py_basis, py_curl};
+
+/* K_e, M_e, F_e of a quadrature element (the HEX8_EDGE transforms above):
+ * curl_phys = J curl_ref / det, W_phys = J^-T W_ref (divided by det once
+ * more under ORC_FLAG_PIOLA_LITERAL), weights w_q |det J|. */
+static void orc_element_shape(const orc_shape* S, const double* X, double nu, double sigma,
+                              const orc_source* src, int32_t n_src, int32_t flags, double* Ke, double* Me,
+                              double* Fe) {
+  const int E = S->epe;
+  for (int i = 0; i < E * E; i++) { Ke[i] = 0.0; Me[i] = 0.0; }
+  for (int i = 0; i < E; i++) Fe[i] = 0.0;
+  for (int q = 0; q < S->nq; q++) {
+    double x[3], wq, J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    S->point(q, x, &wq);
+    for (int a = 0; a < S->npe; a++) {
+      double d[3];
+      S->grad(a, x, d);
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) J[3 * r + c] += X[3 * a + r] * d[c];
+    }
+    const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                       J[2] * (J[3] * J[7] - J[4] * J[6]);
+    const double adet = fabs(det);
+    if (adet < 1e-15) continue;
+    double inv[3][3];
+    inv[0][0] = (J[4] * J[8] - J[5] * J[7]) / det;
+    inv[0][1] = (J[2] * J[7] - J[1] * J[8]) / det;
+    inv[0][2] = (J[1] * J[5] - J[2] * J[4]) / det;
+    inv[1][0] = (J[5] * J[6] - J[3] * J[8]) / det;
+    inv[1][1] = (J[0] * J[8] - J[2] * J[6]) / det;
+    inv[1][2] = (J[2] * J[3] - J[0] * J[5]) / det;
+    inv[2][0] = (J[3] * J[7] - J[4] * J[6]) / det;
+    inv[2][1] = (J[1] * J[6] - J[0] * J[7]) / det;
+    inv[2][2] = (J[0] * J[4] - J[1] * J[3]) / det;
+    double c[12][3], W[12][3];
+    for (int k = 0; k < E; k++) {
+      double cr[3], wr[3];
+      S->curl(k, x, cr);
+      S->basis(k, x, wr);
+      for (int r = 0; r < 3; r++) {
+        c[k][r] = (J[3 * r] * cr[0] + J[3 * r + 1] * cr[1] + J[3 * r + 2] * cr[2]) / det;
+        W[k][r] = inv[0][r] * wr[0] + inv[1][r] * wr[1] + inv[2][r] * wr[2];
+        if (flags & ORC_FLAG_PIOLA_LITERAL) W[k][r] /= det;
+      }
+    }
+    for (int i = 0; i < E; i++)
+      for (int j = 0; j < E; j++) {
+        Ke[E * i + j] += wq * adet * nu * (c[i][0] * c[j][0] + c[i][1] * c[j][1] + c[i][2] * c[j][2]);
+        if ((flags & ORC_FLAG_MASS) && sigma > 0.0)
+          Me[E * i + j] += wq * adet * sigma * (W[i][0] * W[j][0] + W[i][1] * W[j][1] + W[i][2] * W[j][2]);
+      }
+    if (n_src > 0) {
+      double p[3] = {0.0, 0.0, 0.0}, js[3];
+      for (int a = 0; a < S->npe; a++) {
+        const double N = S->value(a, x);
+        for (int r = 0; r < 3; r++) p[r] += N * X[3 * a + r];
+      }
+      source_at(src, n_src, p, js);
+      for (int i = 0; i < E; i++) Fe[i] += wq * adet * (W[i][0] * js[0] + W[i][1] * js[1] + W[i][2] * js[2]);
+    }
+  }
+}
+
+/* Reference-element checks for the tests: circulation of W_k along edge e
+ * (midpoint rule, n segments, reference coordinates; the pyramid's slant
+ * edges are the collapsed cube's vertical edges) and the largest difference
+ * between grad N_a and the edge-basis combination sum_k (N_a(b_k) -
+ * N_a(a_k)) W_k at point x. */
+static void shape_node(int32_t elem_type, int a, double* x) {
+  if (elem_type == ORC_ELEM_PRISM6_EDGE) {
+    const double v[3][2] = {{1.0, 0.0}, {0.0, 1.0}, {0.0, 0.0}};
+    x[0] = v[a % 3][0]; x[1] = v[a % 3][1]; x[2] = a < 3 ? -1.0 : 1.0;
+  } else {
+    x[0] = a == 4 ? 0.0 : PY_C[a][0]; x[1] = a == 4 ? 0.0 : PY_C[a][1]; x[2] = a == 4 ? 1.0 : 0.0;
+  }
+}
+double orc_shape_circulation(int32_t elem_type, int k, int e, int n) {
+  const orc_shape* S = elem_type == ORC_ELEM_PRISM6_EDGE ? &ORC_PRISM : &ORC_PYRAMID;
+  const int (*tab)[2] = elem_type == ORC_ELEM_PRISM6_EDGE ? PRISM_EDGE : PYR_EDGE;
+  double xa[3], xb[3], s = 0.0;
+  shape_node(elem_type, tab[e][0], xa);
+  shape_node(elem_type, tab[e][1], xb);
+  if (elem_type == ORC_ELEM_PYRAMID5_EDGE && tab[e][1] == 4) { xb[0] = xa[0]; xb[1] = xa[1]; }
+  (void)S;
+  for (int i = 0; i < n; i++) {
+    double x[3], w[3];
+    const double t = (i + 0.5) / n;
+    for (int c = 0; c < 3; c++) x[c] = xa[c] + t * (xb[c] - xa[c]);
+    S->basis(k, x, w);
+    for (int c = 0; c < 3; c++) s += w[c] * (xb[c] - xa[c]) / n;
+  }
+  return s;
+}
+double orc_shape_grad_residual(int32_t elem_type, const double* x) {
+  const orc_shape* S = elem_type == ORC_ELEM_PRISM6_EDGE ? &ORC_PRISM : &ORC_PYRAMID;
+  const int (*tab)[2] = elem_type == ORC_ELEM_PRISM6_EDGE ? PRISM_EDGE : PYR_EDGE;
+  double worst = 0.0;
+  for (int a = 0; a < S->npe; a++) {
+    double g[3], sum[3] = {0.0, 0.0, 0.0};
+    S->grad(a, x, g);
+    for (int k = 0; k < S->epe; k++) {
+      double w[3];
+      const double coef = (tab[k][1] == a) - (tab[k][0] == a);
+      S->basis(k, x, w);
+      for (int r = 0; r < 3; r++) sum[r] += coef * w[r];
+    }
+    for (int r = 0; r < 3; r++) worst = fmax(worst, fabs(g[r] - sum[r]));
+  }
+  return worst;
+}
+
+/* ---------------------------------------------------------------------------
  * CSR pattern and numeric assembly (EMAssembly::assemble,
  * src/numeric/em_assembly.cpp:144-420, scatter :654-765; duplicates summed
  * as SparseConverter::to_eigen does, sparse_converter.cpp:19-80).
@@ -781,6 +1021,10 @@ int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, in
     if (elem_type == ORC_ELEM_HEX8_EDGE) {
       orc_element_hex(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
       orc_edge_signs_hex(tets + npe * t, s);
+    } else if (elem_type == ORC_ELEM_PRISM6_EDGE || elem_type == ORC_ELEM_PYRAMID5_EDGE) {
+      orc_element_shape(elem_type == ORC_ELEM_PRISM6_EDGE ? &ORC_PRISM : &ORC_PYRAMID, X, nu_mat[mid], sg, src,
+                        n_src, flags, Ke, Me, Fe);
+      for (int k = 0; k < epe; k++) s[k] = tets[npe * t + tab[k][0]] < tets[npe * t + tab[k][1]] ? 1 : -1;
     } else {
       orc_element(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
       orc_edge_signs(tets + npe * t, s);
@@ -1082,7 +1326,9 @@ int orc_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const 
                      const int32_t* dof_type, int64_t n_dir, const int32_t* dir_pairs, int64_t n_sdir,
                      const int32_t* sdir_nodes, int32_t n_hole_markers, int32_t gauge, int32_t* l2g,
                      int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs) {
-  const int npe = elem_type == ORC_ELEM_HEX8_EDGE ? 8 : 4, epe = elem_type == ORC_ELEM_HEX8_EDGE ? 12 : 6;
+  int npe, epe;
+  const int (*tab)[2];
+  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
   const int w = npe + epe;
   int64_t i, e, nv = 0, nsf = 0, ne = 0, vf = 0, vd = 0, k = 0;
   int32_t root = -1;

@@ -38,7 +38,7 @@ enum {
 };
 
 /* Element types (same values as the C ABI's EMG_ELEM_*). */
-enum { ORC_ELEM_TET4_EDGE = 0, ORC_ELEM_HEX8_EDGE = 1 };
+enum { ORC_ELEM_TET4_EDGE = 0, ORC_ELEM_HEX8_EDGE = 1, ORC_ELEM_PRISM6_EDGE = 2, ORC_ELEM_PYRAMID5_EDGE = 3 };
 
 /* Gauge modes. */
 enum { ORC_GAUGE_NONE = -1, ORC_GAUGE_REF = 0, ORC_GAUGE_BOUNDARY_FIRST = 1 };
@@ -126,8 +126,9 @@ int orc_bicgstab(int64_t n, const int64_t* row_ptr, const int32_t* col,
                  int32_t max_iter, int32_t precond, int32_t* iterations,
                  double* residual_norm);
 
-/* ---- element-typed variants: elems holds 4 (TET4_EDGE) or 8 (HEX8_EDGE)
- * nodes per element, elem_edge / l2g 6 or 12 entries per element; the
+/* ---- element-typed variants: elems holds 4 (TET4_EDGE), 8 (HEX8_EDGE),
+ * 6 (PRISM6_EDGE) or 5 (PYRAMID5_EDGE) nodes per element, elem_edge / l2g
+ * 6, 12, 9 or 8 entries per element; the
  * untyped functions above are elem_type = ORC_ELEM_TET4_EDGE. */
 int orc_edge_ids_typed(int32_t elem_type, int64_t n_elems, const int32_t* elems, int32_t* elem_edge,
                        int32_t* edge_nodes, int64_t* n_edges);
@@ -179,6 +180,11 @@ void orc_element_hex(const double* xyz, double nu, double sigma,
                      const orc_source* src, int32_t n_src, int32_t flags,
                      double* Ke, double* Me, double* Fe);
 void orc_edge_signs_hex(const int32_t* hex, int32_t* s);
+/* PRISM6_EDGE / PYRAMID5_EDGE reference-element checks: circulation of basis
+ * k along edge e (n midpoint segments), and max |grad N_a - sum_k (N_a(b_k) -
+ * N_a(a_k)) W_k| over the nodes a at reference point x. */
+double orc_shape_circulation(int32_t elem_type, int k, int e, int n);
+double orc_shape_grad_residual(int32_t elem_type, const double* x);
 
 /* Thread count used by the parallel loops (OpenMP when compiled with it). */
 int orc_num_threads(void);

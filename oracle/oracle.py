@@ -73,19 +73,37 @@ def lib():
         L.orc_element_hex.restype = None
         L.orc_edge_signs_hex.argtypes = [I32P, I32P]
         L.orc_edge_signs_hex.restype = None
+        L.orc_shape_circulation.argtypes = [C.c_int32, C.c_int, C.c_int, C.c_int]
+        L.orc_shape_circulation.restype = C.c_double
+        L.orc_shape_grad_residual.argtypes = [C.c_int32, F64P]
+        L.orc_shape_grad_residual.restype = C.c_double
     return _LIB
 
 
-ELEM_TET4_EDGE, ELEM_HEX8_EDGE = 0, 1
+ELEM_TET4_EDGE, ELEM_HEX8_EDGE, ELEM_PRISM6_EDGE, ELEM_PYRAMID5_EDGE = 0, 1, 2, 3
+_TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE}
+_EDGES = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8}
+_TYPE_OF_EDGES = {v: k for k, v in _EDGES.items()}
 
 
 def elem_type_of(elems) -> int:
-    """TET4_EDGE for (T, 4) node arrays, HEX8_EDGE for (T, 8)."""
-    return ELEM_HEX8_EDGE if np.asarray(elems).shape[-1] == 8 else ELEM_TET4_EDGE
+    """Element type of a (T, nodes) array: 4 TET4_EDGE, 8 HEX8_EDGE, 6
+    PRISM6_EDGE, 5 PYRAMID5_EDGE."""
+    return _TYPE_OF_NODES[np.asarray(elems).shape[-1]]
 
 
 def edges_per_elem(elem_type: int) -> int:
-    return 12 if elem_type == ELEM_HEX8_EDGE else 6
+    return _EDGES[elem_type]
+
+
+def shape_circulation(elem_type, k, e, n=2000):
+    """Circulation of PRISM6_EDGE / PYRAMID5_EDGE basis k along edge e."""
+    return lib().orc_shape_circulation(elem_type, k, e, n)
+
+
+def shape_grad_residual(elem_type, x):
+    """max |grad N_a - sum_k (N_a(b_k) - N_a(a_k)) W_k| at reference point x."""
+    return lib().orc_shape_grad_residual(elem_type, np.ascontiguousarray(x, np.float64))
 
 
 def sources_array(sources):
@@ -212,7 +230,7 @@ def pattern(l2g, n):
     """Merged CSR pattern; l2g is (T, 6) for tets or (T, 12) for hexes (a flat
     array is read as tets)."""
     l2g = np.asarray(l2g)
-    et = ELEM_HEX8_EDGE if (l2g.ndim == 2 and l2g.shape[1] == 12) else ELEM_TET4_EDGE
+    et = _TYPE_OF_EDGES[l2g.shape[1]] if l2g.ndim == 2 else ELEM_TET4_EDGE
     l2g = np.ascontiguousarray(l2g, dtype=np.int32).ravel()
     T = l2g.size // edges_per_elem(et)
     rp = np.empty(n + 1, np.int64)

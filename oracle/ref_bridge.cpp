@@ -30,10 +30,20 @@
 
 namespace {
 
+// Element types of the C ABI (EMG_ELEM_*) as the reference's ElementType.
+static int bridge_npe(int32_t t) { return t == 1 ? 8 : t == 2 ? 6 : t == 3 ? 5 : 4; }
+static int bridge_epe(int32_t t) { return t == 1 ? 12 : t == 2 ? 9 : t == 3 ? 8 : 6; }
+static numeric::ElementType bridge_type(int32_t t) {
+  return t == 1   ? numeric::ElementType::HEX8_EDGE
+         : t == 2 ? numeric::ElementType::PRISM6_EDGE
+         : t == 3 ? numeric::ElementType::PYRAMID5_EDGE
+                  : numeric::ElementType::TET4_EDGE;
+}
+
 fe_em::EMMeshData make_mesh(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32_t* tets,
                             int64_t n_dir, const int32_t* dir_pairs, int32_t n_hole_markers,
                             int32_t elem_type = 0) {
-  const int npe = elem_type == 1 ? 8 : 4;
+  const int npe = bridge_npe(elem_type);
   fe_em::EMMeshData m;
   m.nodes.resize(n_nodes);
   for (int64_t i = 0; i < n_nodes; ++i) {
@@ -45,7 +55,7 @@ fe_em::EMMeshData make_mesh(int64_t n_nodes, const double* xyz, int64_t n_tets, 
     auto& e = m.elements[t];
     e.id = static_cast<int>(t);
     e.node_ids.assign(tets + npe * t, tets + npe * (t + 1));
-    e.elem_type = elem_type == 1 ? numeric::ElementType::HEX8_EDGE : numeric::ElementType::TET4_EDGE;
+    e.elem_type = bridge_type(elem_type);
     e.dof_type = fe_em::DOFType::VECTOR_EDGE_ONLY;
     e.material_id = 0;
     e.region_id = 0;
@@ -114,7 +124,7 @@ int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, con
                          const int32_t* dir_pairs, int32_t n_hole_markers, int32_t apply_gauge,
                          int32_t* elem_edge_out, int32_t* l2g_out, int64_t* n_edges, int64_t* n_free,
                          int64_t* n_dofs) {
-  const int epe = elem_type == 1 ? 12 : 6;
+  const int epe = bridge_epe(elem_type);
   try {
     auto mesh = make_mesh(n_nodes, nullptr, n_tets, tets, n_dir, dir_pairs, n_hole_markers, elem_type);
     fe_em::GlobalEdgeIDGenerator gen(mesh);
@@ -149,7 +159,7 @@ int refb_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const
                       const int32_t* dof_type, int64_t n_dir, const int32_t* dir_pairs, int64_t n_sdir,
                       const int32_t* sdir_nodes, int32_t n_hole_markers, int32_t apply_gauge,
                       int32_t* l2g_out, int64_t* n_free, int64_t* n_dofs) {
-  const int npe = elem_type == 1 ? 8 : 4, epe = elem_type == 1 ? 12 : 6;
+  const int npe = bridge_npe(elem_type), epe = bridge_epe(elem_type);
   try {
     auto mesh = make_mesh(n_nodes, nullptr, n_elems, elems, n_dir, dir_pairs, n_hole_markers, elem_type);
     for (int64_t t = 0; t < n_elems; ++t)
@@ -198,7 +208,7 @@ int refb_pattern(int64_t n_nodes, const double* xyz, int64_t n_tets, const int32
 int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, int64_t n_tets,
                        const int32_t* tets, const int32_t* l2g, int64_t* row_ptr_out, int32_t* col_out,
                        int64_t* nnz, int64_t* raw_nnz, int64_t* n_rows) {
-  const int epe = elem_type == 1 ? 12 : 6;
+  const int epe = bridge_epe(elem_type);
   try {
     auto mesh = make_mesh(n_nodes, xyz, n_tets, tets, 0, nullptr, 0, elem_type);
     std::vector<fe_em::Local2Global> maps(n_tets);
@@ -207,7 +217,7 @@ int refb_pattern_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, in
       for (int k = 0; k < epe; ++k) maps[t].indices[k] = l2g[epe * t + k];
       maps[t].element_id = static_cast<int>(t);
       maps[t].num_vector_dofs = epe;
-      maps[t].elem_type = elem_type == 1 ? numeric::ElementType::HEX8_EDGE : numeric::ElementType::TET4_EDGE;
+      maps[t].elem_type = bridge_type(elem_type);
     }
     std::vector<numeric::MaterialProperties> mats(1);
     numeric::EMAssembly as;

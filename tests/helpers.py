@@ -27,7 +27,7 @@ class System:
         tets = np.ascontiguousarray(m.tets, np.int32)
         mat = np.ascontiguousarray(m.material, np.int32)
         self.h = C.c_void_p()
-        et = 1 if tets.shape[1] == 8 else 0
+        et = mesh.TYPE_OF_NODES[tets.shape[1]]
         _abi.check(lib().emg_system_create_typed(et, xyz.shape[0], _abi.ptr(xyz), tets.shape[0], _abi.ptr(tets),
                                                  _abi.ptr(mat), _abi.ptr(self.l2g), n_dofs, 0, None,
                                                  C.byref(self.h)), "emg_system_create_typed")

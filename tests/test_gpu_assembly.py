@@ -81,6 +81,53 @@ def test_flags_match_oracle(flags):
         assert close(mv, omv)
 
 
+def fan_mesh(k=40):
+    """k tets around the axis edge (0,0,0)-(0,0,1): that edge's row has
+    2k + 3 columns, longer than the shared-memory rows of the gather kernel."""
+    ang = np.linspace(0.0, 2 * np.pi, k, endpoint=False)
+    ring = np.stack([np.cos(ang), np.sin(ang), 0.5 + 0.1 * np.sin(3 * ang)], axis=1)
+    xyz = np.vstack([[0.0, 0.0, 0.0], [0.0, 0.0, 1.0], ring])
+    tets = np.array([[0, 1, 2 + a, 2 + (a + 1) % k] for a in range(k)], np.int32)
+    mat = (np.arange(k) % 2).astype(np.int32)
+    src = [mesh.Source(mesh.SRC_BOX, (0.0, 0.0, 1.0), (-2.0, 2.0, -2.0, 2.0, -1.0, 2.0))]
+    return mesh.CubeMesh(n=0, xyz=xyz, tets=tets, material=mat, dirichlet=np.zeros((0, 2), np.int32),
+                         nu=np.array([1.0, 0.25]), sigma=np.array([1.0, 3.0]), sources=src, name="fan")
+
+
+@pytest.mark.parametrize("flags", [0, _abi.FLAG_MASS])
+def test_long_rows_match_oracle(flags):
+    m = fan_mesh()
+    l2g = maps(m, O.GAUGE_NONE)
+    s = System(m, l2g, flags=flags)
+    rp, col, kv, mv, rhs = s.export()
+    assert np.diff(rp).max() > 64
+    orp, ocol, okv, omv, orhs = oracle_system(m, l2g, flags=flags)
+    np.testing.assert_array_equal(col, ocol)
+    assert close(kv, okv) and close(rhs, orhs)
+    if flags:
+        assert close(mv, omv)
+
+
+def test_two_local_edges_on_one_column_match_oracle():
+    """A DOF map that sends two edges of one tet to the same column (merged
+    DOFs): both terms land on that entry, in the element loop's order."""
+    m = mesh.plain_scale(4)
+    l2g = maps(m, O.GAUGE_NONE).reshape(-1, 6).copy()
+    for t in (0, 7, 23):  # merge local edges 0 and 5 of a few tets, everywhere they occur
+        a, b = l2g[t, 0], l2g[t, 5]
+        l2g[l2g == b] = a
+    l2g = l2g.ravel()
+    used = np.unique(l2g[l2g >= 0])
+    remap = -np.ones(int(l2g.max()) + 1, np.int64)
+    remap[used] = np.arange(used.size)
+    l2g = np.where(l2g >= 0, remap[np.maximum(l2g, 0)], -1).astype(np.int32)
+    s = System(m, l2g, flags=_abi.FLAG_MASS, sigma=np.array([2.0, 5.8]))
+    rp, col, kv, mv, rhs = s.export()
+    orp, ocol, okv, omv, orhs = oracle_system(m, l2g, flags=_abi.FLAG_MASS, sigma=np.array([2.0, 5.8]))
+    np.testing.assert_array_equal(col, ocol)
+    assert close(kv, okv) and close(mv, omv) and close(rhs, orhs)
+
+
 def test_deterministic_and_reassembly():
     m = mesh.plain_scale(8)
     s = System(m, maps(m))
