@@ -59,6 +59,8 @@ SIGNATURES = {
     "emg_mesh_material_tags": ([H, VP], C.c_int),
     "emg_edge_ids": ([H, VP, VP, C.POINTER(C.c_int64)], C.c_int),
     "emg_dof_build": ([H, C.c_int32, C.POINTER(H)], C.c_int),
+    "emg_dof_build_device": ([C.c_int32, C.c_int64, C.c_int64, VP, C.c_int64, VP, C.c_int32, C.c_int32, VP,
+                              C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64), VP], C.c_int),
     "emg_dof_build_av": ([H, VP, C.c_int64, VP, C.c_int32, VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                           C.POINTER(C.c_int64)], C.c_int),
     "emg_dofmap_info": ([H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),

@@ -359,6 +359,16 @@ int emg_dof_build_av(emg_mesh mesh, const int32_t* dof_type, int64_t n_scalar_di
   });
 }
 
+int emg_dof_build_device(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems,
+                         int64_t n_dir, const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge_mode,
+                         int32_t* l2g, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs, void* stream) {
+  return guarded([&]() -> int {
+    emg::keep_pool_memory();
+    return emg::dof_build_gpu(elem_type, n_nodes, n_elems, elems, n_dir, dir_pairs, n_hole_markers, gauge_mode, l2g,
+                              n_edges, n_free, n_dofs, as_stream(stream));
+  });
+}
+
 int emg_dofmap_info(emg_dofmap map, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs) {
   if (!map) { set_error("null dofmap"); return EMG_INVALID_INPUT; }
   if (n_edges) *n_edges = map->d.n_edges;

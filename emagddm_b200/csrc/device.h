@@ -67,6 +67,12 @@ struct System {
   ~System();
 };
 
+// DOF numbering of a one-type mesh on the device (numbering_gpu.cu), bit-exact
+// to build_dofmap for EMG_GAUGE_NONE / EMG_GAUGE_REF.
+int dof_build_gpu(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems, int64_t n_dir,
+                  const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge, int32_t* l2g_out,
+                  int64_t* n_edges_out, int64_t* n_free_out, int64_t* n_dofs_out, cudaStream_t st);
+
 // Symbolic phase: incidence lists and the merged CSR pattern, all on the device.
 int system_build(System& s, cudaStream_t st);
 // Numeric phase: K (and M), F.

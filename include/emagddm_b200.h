@@ -181,6 +181,18 @@ int emg_dofmap_export(emg_dofmap map, int32_t* l2g, int32_t* edge_dof);
  * full[e] = reduced[edge_dof[e]] or 0. */
 int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full);
 void emg_dofmap_destroy(emg_dofmap map);
+/* emg_dof_build on the device: the same edge IDs, free numbering and `ref`
+ * tree-cotree gauge, bit for bit, computed by GPU kernels from DEVICE arrays
+ * (elems: nodes_per_elem * n_elems node indices; dir_pairs: 2 * n_dir
+ * Dirichlet node pairs) into the device array l2g (edges_per_elem * n_elems
+ * Local2Global::indices, -1 = constrained or tree edge), ready for
+ * emg_system_create_typed with on_device = 1.  gauge_mode: EMG_GAUGE_NONE or
+ * EMG_GAUGE_REF (EMG_GAUGE_BOUNDARY_FIRST is host-only: emg_dof_build).
+ * Returns the edge, free and equation counts; blocks the calling host thread
+ * (one read-back per tree level). */
+int emg_dof_build_device(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int32_t* elems,
+                         int64_t n_dir, const int32_t* dir_pairs, int32_t n_hole_markers, int32_t gauge_mode,
+                         int32_t* l2g, int64_t* n_edges, int64_t* n_free, int64_t* n_dofs, void* stream);
 
 /* ---- Per-element DOF types: EMDOFManager::build with Element::dof_type
  * (include/fe_em/em_mesh_data.hpp:45-49).  SCALAR_ONLY elements carry nodal
