@@ -242,6 +242,8 @@ def run_ours(args, rank, world, local_rank):
     sigma = np.ascontiguousarray(m.sigma)
     cfg = _abi.KrylovConfig(TOL, MAX_ITER, _abi.PRECOND_JACOBI)
     info = {}
+    device_numbering = numbering_on_device(L, m, d_tets, l2g, stream, sp, dev)
+    device_numbering["host_ms"] = setup_dof_ms
 
     if args.kernels_only:
         h = C.c_void_p()
@@ -416,7 +418,7 @@ def run_ours(args, rank, world, local_rank):
                  "synthetic (seedless structured cube mesh; iron block + annulus coil)"),
         "config": {**workload_config(args.n, n_dofs, nnz, args.workload), "parallelism": f"replicas{world}",
                    "pcg_iterations": iters, "final_residual": info["res"],
-                   "setup_dof_ms": setup_dof_ms,
+                   "setup_dof_ms": setup_dof_ms, "device_numbering": device_numbering,
                    "cg_kernel_ms": {"spmv_dot": kt[0], "update": kt[1], "direction": kt[2]},
                    "cg_iteration_ms_kernels": it_ms,
                    "solve_ms": info["solve_ms"], "phase_ms": phases, "step_ms": step_ms, "assembly": assembly,
@@ -469,6 +471,32 @@ def run_ours(args, rank, world, local_rank):
 
 def rel_err(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def numbering_on_device(L, m, d_tets, l2g, stream, sp, dev):
+    """The same DOF map computed by emg_dof_build_device from the device
+    element array (edge IDs, free numbering, `ref` gauge): host wall time of
+    the call (it synchronizes), median of 3 after one warm-up, and whether it
+    equals the host numbering bit for bit."""
+    import torch
+
+    from emagddm_b200 import _abi
+    d_dir = torch.from_numpy(np.ascontiguousarray(m.dirichlet, np.int32).reshape(-1)).to(dev)
+    out = torch.empty(l2g.size, dtype=torch.int32, device=dev)
+    ne, nf, nd = C.c_int64(), C.c_int64(), C.c_int64()
+    ms = []
+    for _ in range(4):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        _abi.check(L.emg_dof_build_device(m.elem_type, m.n_nodes, m.n_tets, d_tets.data_ptr(), len(m.dirichlet),
+                                          d_dir.data_ptr(), 0, _abi.GAUGE_REF, out.data_ptr(), C.byref(ne),
+                                          C.byref(nf), C.byref(nd), sp), "emg_dof_build_device")
+        ms.append((time.perf_counter() - t0) * 1e3)
+    equal = bool(np.array_equal(out.cpu().numpy(), l2g.reshape(-1)))
+    return {"ms": statistics.median(ms[1:]), "ms_runs": [round(x, 2) for x in ms], "equal_to_host": equal,
+            "n_dofs": nd.value,
+            "what": "emg_dof_build_device (GPU edge IDs, free numbering, ref tree-cotree gauge) from the device "
+                    "element array; host_ms: the host numbering the timed steps use"}
 
 
 def oracle_check_plain(csys, x_tol, x_tight, tight_iters):
