@@ -239,9 +239,9 @@ int emg_mesh_create_typed(int32_t elem_type, int64_t n_nodes, const double* xyz,
       set_error("bad Dirichlet pair list");
       return EMG_INVALID_INPUT;
     }
-    for (int64_t i = 0; i < npe * n_elems; ++i)
-      if (elems[i] < 0 || elems[i] >= n_nodes) {
-        set_error("element node index out of range");  // em_assembly.cpp:603-608
+    for (int64_t t = 0; t < n_elems; ++t)
+      if (!emg::valid_row(elem_type, elems + npe * t, n_nodes)) {
+        set_error("element " + std::to_string(t) + ": node index out of range or unknown element type");  // em_assembly.cpp:603-608
         return EMG_INVALID_INPUT;
       }
     auto* h = new emg_mesh_t();
@@ -346,6 +346,7 @@ int emg_dof_build_av(emg_mesh mesh, const int32_t* dof_type, int64_t n_scalar_di
                      int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs) {
   return guarded([&]() -> int {
     if (!mesh) { set_error("null handle"); return EMG_INVALID_INPUT; }
+    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_dof_build_av: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     std::vector<int32_t> rows;
     int64_t ns = 0, nf = 0, nd = 0;
     int rc = emg::build_dofmap_av(mesh->m, dof_type, n_scalar_dirichlet, scalar_dirichlet, gauge_mode, rows,
@@ -400,6 +401,7 @@ int emg_dof_build_partitioned(emg_mesh mesh, const int32_t* tet_part, int32_t n_
   return guarded([&]() -> int {
     if (!mesh || !out) { set_error("null handle"); return EMG_INVALID_INPUT; }
     *out = nullptr;
+    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_dof_build_partitioned: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     auto* h = new emg_dofmap_t();
     int rc = emg::build_dofmap_partitioned(mesh->m, tet_part, n_parts, h->d);
     if (rc) { delete h; return rc; }
@@ -866,6 +868,7 @@ int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* o
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
     *out = nullptr;
+    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_fetidp_create: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     emg::keep_pool_memory();
     auto* h = new emg_fetidp_t();
     int rc = h->fd.create(mesh->m, map->d, as_stream(stream));
@@ -997,6 +1000,7 @@ int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* o
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
     *out = nullptr;
+    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_direct_create: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     if (map->d.n_elems != mesh->m.n_elems || map->d.elem_type != mesh->m.elem_type ||
         map->d.l2g.size() != static_cast<size_t>(mesh->m.epe() * mesh->m.n_elems)) {
       set_error("DOF map does not belong to this mesh");

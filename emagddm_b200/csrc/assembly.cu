@@ -780,12 +780,22 @@ constexpr int kElemTile = 64;  // elements per block pass of k_elem_terms
 // terms run as separate launches; the packed sums accumulate in shared
 // memory, entry-major so that a warp's lanes touch consecutive words, and are
 // written coalesced.
-template <class S, bool kK, bool kMass, bool kSrc>
+//
+// kMixed: a mixed mesh (rows of 9 ints, the type in slot 8): the launch
+// integrates the rows of type S only, writes them in the 12-edge layout
+// (packed_index(12, i, j), 78 entries; F 12) that one gather reads for every
+// type, and scales the hexahedron's terms to its unit-circulation basis (1/4
+// of the reference's edge functions: K, M by 1/16, F by 1/4).
+template <class S, bool kK, bool kMass, bool kSrc, bool kMixed>
 __global__ void __launch_bounds__(kElemTile) k_elem_terms(AsmArgs A, int64_t n_el, double* __restrict__ ke,
                                                           double* __restrict__ me, double* __restrict__ fe) {
   constexpr int E = S::kEdges, N = S::kNodes, P = E * (E + 1) / 2;
+  constexpr int kRow = kMixed ? 9 : N;                 // ints per element row
+  constexpr int kEOut = kMixed ? 12 : E, kPOut = kEOut * (kEOut + 1) / 2;
+  constexpr double kScale = (kMixed && S::kType == 1) ? 0.25 : 1.0;
   constexpr int W = (kK || kMass) ? P : E;  // entries staged per element
   __shared__ double acc[W * kElemTile];
+  __shared__ bool mine[kElemTile];
   const bool signs = (A.flags & EMG_FLAG_NO_EDGE_SIGNS) == 0;
   const bool literal = (A.flags & EMG_FLAG_PIOLA_LITERAL) != 0;
   const int tid = threadIdx.x;
@@ -798,14 +808,22 @@ __global__ void __launch_bounds__(kElemTile) k_elem_terms(AsmArgs A, int64_t n_e
     double ft[kSrc ? E : 1];
 #pragma unroll
     for (int k = 0; k < (kSrc ? E : 1); ++k) ft[k] = 0.0;
-    const int32_t mid = t < n_el ? (A.material ? A.material[t] : 0) : -1;
+    bool is_mine = t < n_el;
+    if (kMixed && is_mine) {
+      const int32_t rt = A.elems[static_cast<int64_t>(kRow) * t + 8];
+      is_mine = rt == S::kType;
+      // the TET4 launch (the first) flags rows of no known type
+      if (S::kType == 0 && (rt < 0 || rt > 3)) atomicOr(A.err, kErrNode);
+    }
+    mine[tid] = is_mine;
+    const int32_t mid = is_mine ? (A.material ? A.material[t] : 0) : -1;
     bool use = mid >= 0 && mid < A.n_mat;  // em_assembly.cpp:270-276 skips the element
     int32_t node[N];
     double X[N][3];
     if (use) {
 #pragma unroll
       for (int a = 0; a < N; ++a) {
-        node[a] = A.elems[static_cast<int64_t>(N) * t + a];
+        node[a] = A.elems[static_cast<int64_t>(kRow) * t + a];
         if (node[a] < 0 || node[a] >= A.n_nodes) use = false;
       }
       if (!use) atomicOr(A.err, kErrNode);
@@ -917,31 +935,65 @@ __global__ void __launch_bounds__(kElemTile) k_elem_terms(AsmArgs A, int64_t n_e
 #pragma unroll
       for (int i = 0; i < E; ++i)
 #pragma unroll
-        for (int j = i; j < E; ++j, ++e) acc[e * kElemTile + tid] *= sg[i] * sg[j];
+        for (int j = i; j < E; ++j, ++e) acc[e * kElemTile + tid] *= (kScale * kScale) * (sg[i] * sg[j]);
       __syncthreads();
       double* out = kK ? ke : me;
-      for (int x = tid; x < cnt * P; x += kElemTile) out[t0 * P + x] = acc[(x % P) * kElemTile + x / P];
+      if (!kMixed) {
+        for (int x = tid; x < cnt * P; x += kElemTile) out[t0 * P + x] = acc[(x % P) * kElemTile + x / P];
+      } else {
+        for (int x = tid; x < cnt * P; x += kElemTile) {
+          const int el = x / P;
+          if (!mine[el]) continue;
+          int e2 = x - el * P, i = 0;
+          while (e2 >= E - i) { e2 -= E - i; ++i; }  // entry e2 of row i of the packed triangle
+          out[(t0 + el) * kPOut + packed_index(kEOut, i, i + e2)] = acc[(x - el * P) * kElemTile + el];
+        }
+      }
       __syncthreads();
     }
     if (kSrc && !kK) {
 #pragma unroll
-      for (int k = 0; k < (kSrc ? E : 1); ++k) acc[k * kElemTile + tid] = sg[k] * ft[k];
+      for (int k = 0; k < (kSrc ? E : 1); ++k) acc[k * kElemTile + tid] = kScale * sg[k] * ft[k];
       __syncthreads();
-      for (int x = tid; x < cnt * E; x += kElemTile) fe[t0 * E + x] = acc[(x % E) * kElemTile + x / E];
+      for (int x = tid; x < cnt * E; x += kElemTile) {
+        const int el = x / E;
+        if (kMixed && !mine[el]) continue;
+        fe[(t0 + el) * kEOut + (x - el * E)] = acc[(x % E) * kElemTile + el];
+      }
       __syncthreads();
     }
   }
 }
 
-template <class S, bool kMass, bool kSrc>
-void launch_elem_assembly(const AsmArgs& a, int64_t n_el, double* ke, double* me, double* fe, cudaStream_t st) {
+template <class S, bool kMass, bool kSrc, bool kMixed>
+void launch_elem_terms(const AsmArgs& a, int64_t n_el, double* ke, double* me, double* fe, cudaStream_t st) {
   const int64_t tiles = (n_el + kElemTile - 1) / kElemTile;
   const unsigned g = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(tiles, 148 * 32)));
-  k_elem_terms<S, true, false, false><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
-  if (kMass || kSrc) k_elem_terms<S, false, kMass, kSrc><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
+  k_elem_terms<S, true, false, false, kMixed><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
+  if (kMass || kSrc) k_elem_terms<S, false, kMass, kSrc, kMixed><<<g, kElemTile, 0, st>>>(a, n_el, ke, me, fe);
+}
+
+template <int kEpe, bool kMass, bool kSrc>
+void launch_rows(const AsmArgs& a, const double* ke, const double* me, const double* fe, cudaStream_t st) {
   const int64_t rb = (a.n * 16 + 255) / 256;
   const unsigned gr = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(rb, 148 * 64)));
-  k_rows_from_terms<S::kEdges, kMass, kSrc><<<gr, 256, 0, st>>>(a, ke, me, fe);
+  k_rows_from_terms<kEpe, kMass, kSrc><<<gr, 256, 0, st>>>(a, ke, me, fe);
+}
+
+template <class S, bool kMass, bool kSrc>
+void launch_elem_assembly(const AsmArgs& a, int64_t n_el, double* ke, double* me, double* fe, cudaStream_t st) {
+  launch_elem_terms<S, kMass, kSrc, false>(a, n_el, ke, me, fe, st);
+  launch_rows<S::kEdges, kMass, kSrc>(a, ke, me, fe, st);
+}
+
+// A mixed mesh: one terms launch per element type, one 12-edge gather.
+template <bool kMass, bool kSrc>
+void launch_mixed_assembly(const AsmArgs& a, int64_t n_el, double* ke, double* me, double* fe, cudaStream_t st) {
+  launch_elem_terms<shape::Tet, kMass, kSrc, true>(a, n_el, ke, me, fe, st);
+  launch_elem_terms<shape::Hex, kMass, kSrc, true>(a, n_el, ke, me, fe, st);
+  launch_elem_terms<shape::Prism, kMass, kSrc, true>(a, n_el, ke, me, fe, st);
+  launch_elem_terms<shape::Pyramid, kMass, kSrc, true>(a, n_el, ke, me, fe, st);
+  launch_rows<12, kMass, kSrc>(a, ke, me, fe, st);
 }
 
 template <class S>
@@ -1095,6 +1147,10 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
       return EMG_INVALID_INPUT;
     }
   const bool mass = (flags & EMG_FLAG_MASS) != 0;
+  if (s.elem_type == EMG_ELEM_MIXED && (flags & EMG_FLAG_QUAD3_LITERAL)) {
+    set_error("EMG_FLAG_QUAD3_LITERAL is a TET4_EDGE-mesh flag (a mixed mesh integrates its tets with the 4-point rule)");
+    return EMG_INVALID_INPUT;
+  }
   if (mass && !s.M.val) EMG_CK(cudaMallocAsync(&s.M.val, sizeof(double) * (s.K.nnz > 0 ? s.K.nnz : 1), st));
   s.has_mass = s.has_mass || mass;
   double* mat = nullptr;
@@ -1131,7 +1187,11 @@ int system_assemble(System& s, const double* nu, const double* sigma, int32_t n_
     double* fe = srcs ? terms + (mass ? 2 * P : P) * T : nullptr;
     if (s.elem_type == EMG_ELEM_HEX8_EDGE) launch_elem_assembly<shape::Hex>(a, T, mass, srcs, ke, me, fe, st);
     else if (s.elem_type == EMG_ELEM_PRISM6_EDGE) launch_elem_assembly<shape::Prism>(a, T, mass, srcs, ke, me, fe, st);
-    else launch_elem_assembly<shape::Pyramid>(a, T, mass, srcs, ke, me, fe, st);
+    else if (s.elem_type == EMG_ELEM_PYRAMID5_EDGE) launch_elem_assembly<shape::Pyramid>(a, T, mass, srcs, ke, me, fe, st);
+    else if (mass && srcs) launch_mixed_assembly<true, true>(a, T, ke, me, fe, st);
+    else if (mass) launch_mixed_assembly<true, false>(a, T, ke, me, fe, st);
+    else if (srcs) launch_mixed_assembly<false, true>(a, T, ke, me, fe, st);
+    else launch_mixed_assembly<false, false>(a, T, ke, me, fe, st);
   } else {
     if (reinterpret_cast<uintptr_t>(s.l2g) % 8 != 0) {
       cudaFreeAsync(mat, st);

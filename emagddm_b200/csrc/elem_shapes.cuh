@@ -1,5 +1,6 @@
 // elem_shapes.cuh -- reference-element data of the quadrature-integrated edge
-// elements (HEX8_EDGE, PRISM6_EDGE, PYRAMID5_EDGE): Lagrange map, edge basis and its
+// elements (HEX8_EDGE, PRISM6_EDGE, PYRAMID5_EDGE, and TET4_EDGE inside mixed
+// meshes): Lagrange map, edge basis and its
 // reference curl, quadrature.  Each shape is a struct of constexpr sizes and
 // __host__ __device__ functions, so the same definitions serve the assembly
 // kernels and their host-side tests.
@@ -17,6 +18,50 @@
 namespace emg {
 namespace shape {
 
+// ------------------------------------------------------------------ TET4 ----
+// The reference's Whitney tetrahedron in a mixed mesh (a mesh of tets alone
+// takes k_tet_terms): N_0 = xi, N_1 = eta, N_2 = zeta, N_3 = 1 - xi - eta -
+// zeta (lagrange_element.cpp:658-683); local edge k (ElementGeometry's
+// {0,1},{1,2},{0,2},{0,3},{1,3},{2,3}) carries the function of the Nedelec
+// pair (p, q) = {0,1},{1,2},{2,0},{0,3},{1,3},{2,3} (nedelec_element.cpp:54-60,
+// :411-505): N_q grad N_p - N_p grad N_q, which circulates from q to p, so
+// edge_a = q, edge_b = p; its curl is 2 grad N_q x grad N_p (the constant
+// curls of curlTet4Edge).  Hammer 4-point rule, weights 1/24
+// (gauss_quadrature.cpp:184-227 with its fourth point).
+struct Tet {
+  static constexpr int kType = 0, kNodes = 4, kEdges = 6, kPoints = 4;
+  __host__ __device__ static constexpr int ned_p(int k) { return k < 3 ? k : k - 3; }
+  __host__ __device__ static constexpr int ned_q(int k) { return k < 3 ? (k + 1) % 3 : 3; }
+  __host__ __device__ static constexpr int edge_a(int k) { return ned_q(k); }
+  __host__ __device__ static constexpr int edge_b(int k) { return ned_p(k); }
+  __host__ __device__ static double dcoord(int a, int c) { return a == 3 ? -1.0 : (a == c ? 1.0 : 0.0); }
+  __host__ __device__ static void point(int q, double* x, double* w) {
+    const double qa = 0.13819660112501051517954131656343619;  // (5 - sqrt 5) / 20
+    const double qb = 0.58541019662496845446137605030969143;  // (5 + 3 sqrt 5) / 20
+    x[0] = q == 2 ? qb : qa;
+    x[1] = q == 1 ? qb : qa;
+    x[2] = q == 0 ? qb : qa;
+    *w = 1.0 / 24.0;
+  }
+  __host__ __device__ static double n(int a, const double* x) { return a == 3 ? 1.0 - x[0] - x[1] - x[2] : x[a]; }
+  __host__ __device__ static void dn(int a, const double* x, double* d) {
+    (void)x;
+    for (int c = 0; c < 3; ++c) d[c] = dcoord(a, c);
+  }
+  __host__ __device__ static void basis(int k, const double* x, double* w) {
+    const int p = ned_p(k), q = ned_q(k);
+    const double np = n(p, x), nq = n(q, x);
+    for (int c = 0; c < 3; ++c) w[c] = nq * dcoord(p, c) - np * dcoord(q, c);
+  }
+  __host__ __device__ static void curl(int k, const double* x, double* c) {
+    (void)x;
+    const int p = ned_p(k), q = ned_q(k);
+    c[0] = 2.0 * (dcoord(q, 1) * dcoord(p, 2) - dcoord(q, 2) * dcoord(p, 1));
+    c[1] = 2.0 * (dcoord(q, 2) * dcoord(p, 0) - dcoord(q, 0) * dcoord(p, 2));
+    c[2] = 2.0 * (dcoord(q, 0) * dcoord(p, 1) - dcoord(q, 1) * dcoord(p, 0));
+  }
+};
+
 // ------------------------------------------------------------------ HEX8 ----
 // Reference hexahedron [-1,1]^3, nodes 0-3 on zeta = -1 (counter-clockwise
 // from (-1,-1)), 4-7 above them (nedelec_element.cpp:506-517; HEX8 map
@@ -32,7 +77,7 @@ namespace shape {
 // 2x2x2 Gauss-Legendre, weights 1, xi outermost (getHex8Points,
 // gauss_quadrature.cpp:247-276).
 struct Hex {
-  static constexpr int kNodes = 8, kEdges = 12, kPoints = 8;
+  static constexpr int kType = 1, kNodes = 8, kEdges = 12, kPoints = 8;
   __host__ __device__ static constexpr int coord(int a, int axis) {  // reference coordinate of node a
     return axis == 0 ? (((a & 3) == 1 || (a & 3) == 2) ? 1 : -1) : axis == 1 ? ((a & 2) ? 1 : -1) : ((a & 4) ? 1 : -1);
   }
@@ -94,7 +139,7 @@ static_assert(Hex::cp(0) == -1 && Hex::cq(0) == -1 && Hex::cp(1) == -1 && Hex::c
 // reference's 3-point triangle rule x 2-point Gauss in zeta
 // (GaussQuadrature::getPrism6Points, gauss_quadrature.cpp:304-345).
 struct Prism {
-  static constexpr int kNodes = 6, kEdges = 9, kPoints = 6;
+  static constexpr int kType = 2, kNodes = 6, kEdges = 9, kPoints = 6;
   __host__ __device__ static constexpr int edge_a(int k) { return k < 3 ? (k == 2 ? 0 : k) : k < 6 ? (k == 5 ? 3 : k) : k - 6; }
   __host__ __device__ static constexpr int edge_b(int k) {
     return k < 3 ? (k == 0 ? 1 : 2) : k < 6 ? (k == 3 ? 4 : 5) : k - 3;
@@ -181,7 +226,7 @@ struct Prism {
 // rule, gauss_quadrature.cpp:380-433, is stated on zeta in [-1, 1] with
 // weights summing to 4/3).
 struct Pyramid {
-  static constexpr int kNodes = 5, kEdges = 8, kPoints = 12;
+  static constexpr int kType = 3, kNodes = 5, kEdges = 8, kPoints = 12;
   __host__ __device__ static constexpr int edge_a(int k) { return k < 4 ? k : k - 4; }
   __host__ __device__ static constexpr int edge_b(int k) { return k < 4 ? (k + 1) & 3 : 4; }
   __host__ __device__ static double cx(int a) { return (a == 1 || a == 2) ? 1.0 : -1.0; }

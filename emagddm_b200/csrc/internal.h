@@ -21,21 +21,45 @@ constexpr int kHexEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
 constexpr int kPrismEdge[9][2] = {{0, 1}, {1, 2}, {0, 2}, {3, 4}, {4, 5}, {3, 5}, {0, 3}, {1, 4}, {2, 5}};
 constexpr int kPyramidEdge[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 4}, {2, 4}, {3, 4}};
 
-inline bool valid_elem_type(int32_t t) {
+inline bool valid_single_type(int32_t t) {
   return t == EMG_ELEM_TET4_EDGE || t == EMG_ELEM_HEX8_EDGE || t == EMG_ELEM_PRISM6_EDGE ||
          t == EMG_ELEM_PYRAMID5_EDGE;
 }
+inline bool valid_elem_type(int32_t t) { return valid_single_type(t) || t == EMG_ELEM_MIXED; }
+// Row width and edge slots of an element array (EMG_ELEM_MIXED: 9 and 12).
 inline int nodes_per_elem(int32_t t) {
-  return t == EMG_ELEM_HEX8_EDGE ? 8 : t == EMG_ELEM_PRISM6_EDGE ? 6 : t == EMG_ELEM_PYRAMID5_EDGE ? 5 : 4;
+  return t == EMG_ELEM_HEX8_EDGE       ? 8
+         : t == EMG_ELEM_PRISM6_EDGE   ? 6
+         : t == EMG_ELEM_PYRAMID5_EDGE ? 5
+         : t == EMG_ELEM_MIXED         ? 9
+                                       : 4;
 }
 inline int edges_per_elem(int32_t t) {
-  return t == EMG_ELEM_HEX8_EDGE ? 12 : t == EMG_ELEM_PRISM6_EDGE ? 9 : t == EMG_ELEM_PYRAMID5_EDGE ? 8 : 6;
+  return t == EMG_ELEM_HEX8_EDGE || t == EMG_ELEM_MIXED ? 12
+         : t == EMG_ELEM_PRISM6_EDGE                    ? 9
+         : t == EMG_ELEM_PYRAMID5_EDGE                  ? 8
+                                                        : 6;
 }
 inline const int (*local_edges(int32_t t))[2] {
   return t == EMG_ELEM_HEX8_EDGE       ? kHexEdge
          : t == EMG_ELEM_PRISM6_EDGE   ? kPrismEdge
          : t == EMG_ELEM_PYRAMID5_EDGE ? kPyramidEdge
                                        : kTetEdge;
+}
+// Type of one element row (a mixed mesh's rows carry it in slot 8).
+inline int32_t row_type(int32_t elem_type, const int32_t* row) { return elem_type == EMG_ELEM_MIXED ? row[8] : elem_type; }
+// Validates one row: its type and its node indices (-1 in the unused slots
+// of a mixed row).
+inline bool valid_row(int32_t elem_type, const int32_t* row, int64_t n_nodes) {
+  const int32_t et = row_type(elem_type, row);
+  if (!valid_single_type(et)) return false;
+  const int nn = nodes_per_elem(et);
+  for (int a = 0; a < nn; ++a)
+    if (row[a] < 0 || row[a] >= n_nodes) return false;
+  if (elem_type == EMG_ELEM_MIXED)
+    for (int a = nn; a < 8; ++a)
+      if (row[a] != -1) return false;
+  return true;
 }
 
 struct Mesh {

@@ -35,29 +35,40 @@ struct Buckets {
 int build_edge_ids(Mesh& m) {
   if (m.edges_built) return EMG_SUCCESS;
   const int npe = m.npe(), epe = m.epe();
-  const int (*le)[2] = local_edges(m.elem_type);
   const int64_t T = m.n_elems, V = m.n_nodes, M = epe * T;
+  // local edges of element t (a mixed mesh's rows name their own type)
+  auto edges_of = [&](int64_t t, const int (**le)[2]) {
+    const int32_t et = row_type(m.elem_type, &m.elems[npe * t]);
+    *le = local_edges(et);
+    return edges_per_elem(et);
+  };
   Buckets bk;
   bk.ptr.assign(V + 1, 0);
-  for (int64_t t = 0; t < T; ++t)
-    for (int k = 0; k < epe; ++k) {
+  for (int64_t t = 0; t < T; ++t) {
+    const int (*le)[2];
+    const int ne = edges_of(t, &le);
+    for (int k = 0; k < ne; ++k) {
       int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       bk.ptr[std::min(u, w) + 1]++;
     }
+  }
   for (int64_t v = 0; v < V; ++v) bk.ptr[v + 1] += bk.ptr[v];
-  bk.a.resize(M);  // hi node
-  bk.b.resize(M);  // position
+  bk.a.resize(bk.ptr[V]);  // hi node
+  bk.b.resize(bk.ptr[V]);  // position
   std::vector<int64_t> cur(bk.ptr.begin(), bk.ptr.end() - 1);
-  for (int64_t t = 0; t < T; ++t)
-    for (int k = 0; k < epe; ++k) {
+  for (int64_t t = 0; t < T; ++t) {
+    const int (*le)[2];
+    const int ne = edges_of(t, &le);
+    for (int k = 0; k < ne; ++k) {
       int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       int64_t s = cur[std::min(u, w)]++;
       bk.a[s] = std::max(u, w);
       bk.b[s] = static_cast<int32_t>(epe * t + k);
     }
+  }
   // leader position of every entry: the bucket's distinct hi nodes so far
   // (a handful per node) are searched instead of all its earlier entries
-  std::vector<int32_t> leader(M);
+  std::vector<int32_t> leader(M, -1);  // -1: slot past its element's edges
   std::vector<uint8_t> is_leader(M, 0);
   std::vector<int32_t> seen_hi, seen_pos;
   for (int64_t v = 0; v < V; ++v) {
@@ -82,11 +93,13 @@ int build_edge_ids(Mesh& m) {
   m.elem_edge.resize(M);
   m.edge_nodes.resize(2 * next);
   for (int64_t p = 0; p < M; ++p) {
-    int32_t id = id_at[leader[p]];
+    int32_t id = leader[p] < 0 ? -1 : id_at[leader[p]];
     m.elem_edge[p] = id;
     if (is_leader[p]) {
       int64_t t = p / epe;
       int k = static_cast<int>(p % epe);
+      const int (*le)[2];
+      edges_of(t, &le);
       int32_t u = m.elems[npe * t + le[k][0]], w = m.elems[npe * t + le[k][1]];
       m.edge_nodes[2 * id] = std::min(u, w);
       m.edge_nodes[2 * id + 1] = std::max(u, w);
@@ -111,7 +124,11 @@ struct EdgeGraph {
 EdgeGraph make_graph(const Mesh& m) {
   EdgeGraph g;
   g.compact.assign(m.n_nodes, -1);
-  for (int32_t v : m.elems) g.compact[v] = 0;
+  const int npe = m.npe();
+  for (int64_t t = 0; t < m.n_elems; ++t) {  // nodes referenced by the elements
+    const int nn = nodes_per_elem(row_type(m.elem_type, &m.elems[npe * t]));
+    for (int a = 0; a < nn; ++a) g.compact[m.elems[npe * t + a]] = 0;
+  }
   int32_t c = 0;
   for (int64_t v = 0; v < m.n_nodes; ++v)
     if (g.compact[v] == 0) g.compact[v] = c++;
@@ -325,7 +342,7 @@ int build_dofmap(Mesh& m, int32_t gauge_mode, DofMap& out) {
     return EMG_INVALID_INPUT;
   }
   out.l2g.resize(m.elem_edge.size());
-  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = m.elem_edge[p] < 0 ? -1 : out.edge_dof[m.elem_edge[p]];
   return EMG_SUCCESS;
 }
 

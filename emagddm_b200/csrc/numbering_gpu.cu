@@ -66,26 +66,44 @@ struct Arena {
   }
 };
 
-struct EdgeTable {
-  int a[12], b[12];
+// Local edge tables of the four element types (row t of a mixed mesh names
+// its type in slot 8).
+struct EdgeTables {
+  int a[4][12], b[4][12], ne[4];
 };
 
 // ------------------------------------------------------------ edge IDs ----
-__global__ void k_edge_keys(int64_t m, int npe, int epe, EdgeTable le, const int32_t* __restrict__ elems,
-                            int64_t n_nodes, uint64_t* __restrict__ key, int32_t* __restrict__ slot,
-                            int32_t* __restrict__ err) {
+// Key of every element-edge slot; slots past an element's own edges get the
+// largest key (they sort last and are left out) and count into *valid the
+// others.
+__global__ void k_edge_keys(int64_t m, int32_t elem_type, int npe, int epe, EdgeTables le,
+                            const int32_t* __restrict__ elems, int64_t n_nodes, uint64_t* __restrict__ key,
+                            int32_t* __restrict__ slot, int32_t* __restrict__ err, int32_t* __restrict__ valid) {
+  int32_t mine = 0;
   for (int64_t p = GTID; p < m; p += GSTRIDE) {
     const int64_t t = p / epe;
     const int k = static_cast<int>(p - t * epe);
-    const int32_t u = elems[npe * t + le.a[k]], w = elems[npe * t + le.b[k]];
+    const int32_t et = elem_type == EMG_ELEM_MIXED ? elems[npe * t + 8] : elem_type;
+    slot[p] = static_cast<int32_t>(p);
+    if (et < 0 || et > 3) {
+      atomicOr(err, 1);
+      key[p] = ~0ull;
+      continue;
+    }
+    if (k >= le.ne[et]) {
+      key[p] = ~0ull;
+      continue;
+    }
+    const int32_t u = elems[npe * t + le.a[et][k]], w = elems[npe * t + le.b[et][k]];
     if (u < 0 || w < 0 || u >= n_nodes || w >= n_nodes) {
       atomicOr(err, 1);
       key[p] = 0;
     } else {
       key[p] = (static_cast<uint64_t>(min(u, w)) << 32) | static_cast<uint32_t>(max(u, w));
     }
-    slot[p] = static_cast<int32_t>(p);
+    ++mine;
   }
+  if (mine) atomicAdd(valid, mine);
 }
 
 // head[i] = i where a run of equal keys starts, else 0 (a max-scan then gives
@@ -282,7 +300,7 @@ __global__ void k_free_dof(int64_t n, const int32_t* __restrict__ constrained, c
 
 __global__ void k_l2g(int64_t m, const int32_t* __restrict__ elem_edge, const int32_t* __restrict__ edge_dof,
                       int32_t* __restrict__ l2g) {
-  for (int64_t p = GTID; p < m; p += GSTRIDE) l2g[p] = edge_dof[elem_edge[p]];
+  for (int64_t p = GTID; p < m; p += GSTRIDE) l2g[p] = elem_edge[p] < 0 ? -1 : edge_dof[elem_edge[p]];
 }
 
 struct MaxOp {
@@ -312,11 +330,14 @@ int dof_build_gpu(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int
     set_error("emg_dof_build_device: more than 2^31 element edges or nodes");
     return EMG_INVALID_INPUT;
   }
-  EdgeTable le{};
-  const int (*tab)[2] = local_edges(elem_type);
-  for (int k = 0; k < epe; ++k) { le.a[k] = tab[k][0]; le.b[k] = tab[k][1]; }
+  EdgeTables le{};
+  for (int32_t et = 0; et < 4; ++et) {
+    const int (*tab)[2] = local_edges(et);
+    le.ne[et] = edges_per_elem(et);
+    for (int k = 0; k < le.ne[et]; ++k) { le.a[et][k] = tab[k][0]; le.b[et][k] = tab[k][1]; }
+  }
   Arena A(st);
-  int32_t* err = A.get<int32_t>(1);
+  int32_t* err = A.get<int32_t>(2);  // error flag, valid slot count
   uint64_t* key = A.get<uint64_t>(m);
   uint64_t* key_s = A.get<uint64_t>(m);
   int32_t* slot = A.get<int32_t>(m);
@@ -344,31 +365,40 @@ int dof_build_gpu(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const int
   tb = std::max(tb, tb2);
   void* tmp = A.get<char>(static_cast<int64_t>(tb));
   if (A.failed) { set_error("emg_dof_build_device: out of device memory"); return EMG_ERR_NOMEM; }
-  EMG_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
-  k_edge_keys<<<grid_of(m), kT, 0, st>>>(m, npe, epe, le, elems, n_nodes, key, slot, err);
-  EMG_CK(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key_s, slot, slot_s, mi, 0, 32 + bits, st));
-  k_runs<<<grid_of(m), kT, 0, st>>>(m, key_s, slot_s, head, leader);
-  EMG_CK(cub::DeviceScan::InclusiveScan(tmp, tb, head, run, MaxOp(), mi, st));
+  EMG_CK(cudaMemsetAsync(err, 0, 2 * sizeof(int32_t), st));
+  k_edge_keys<<<grid_of(m), kT, 0, st>>>(m, elem_type, npe, epe, le, elems, n_nodes, key, slot, err, err + 1);
+  // slots past an element's edges carry the largest key: all 64 bits sorted
+  EMG_CK(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key_s, slot, slot_s, mi, 0,
+                                         elem_type == EMG_ELEM_MIXED ? 64 : 32 + bits, st));
+  int32_t h[4] = {0, 0, 0, 0};  // error flag, valid slots, last id_at, last leader flag
+  EMG_CK(cudaMemcpyAsync(h, err, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  EMG_CK(cudaStreamSynchronize(st));
+  if (h[0]) {
+    set_error("emg_dof_build_device: element node index outside [0, n_nodes) or unknown element type");
+    return EMG_INVALID_INPUT;
+  }
+  const int64_t mv = h[1];  // sorted entries [0, mv) are element edges
+  EMG_CK(cudaMemsetAsync(leader, 0, sizeof(int32_t) * std::max<int64_t>(m, 1), st));
+  k_runs<<<grid_of(mv), kT, 0, st>>>(mv, key_s, slot_s, head, leader);
+  EMG_CK(cub::DeviceScan::InclusiveScan(tmp, tb, head, run, MaxOp(), static_cast<int>(mv), st));
   EMG_CK(cub::DeviceScan::ExclusiveSum(tmp, tb, leader, id_at, mi, st));
-  int32_t h[3] = {0, 0, 0};  // error flag, last id_at, last leader flag
-  EMG_CK(cudaMemcpyAsync(&h[0], err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   if (m > 0) {
-    EMG_CK(cudaMemcpyAsync(&h[1], id_at + m - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    EMG_CK(cudaMemcpyAsync(&h[2], leader + m - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaMemcpyAsync(&h[2], id_at + m - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    EMG_CK(cudaMemcpyAsync(&h[3], leader + m - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   }
   EMG_CK(cudaStreamSynchronize(st));
-  if (h[0]) { set_error("emg_dof_build_device: element node index outside [0, n_nodes)"); return EMG_INVALID_INPUT; }
-  const int64_t E = m > 0 ? static_cast<int64_t>(h[1]) + h[2] : 0;
+  const int64_t E = m > 0 ? static_cast<int64_t>(h[2]) + h[3] : 0;
   int32_t* edge_nodes = A.get<int32_t>(2 * E);
   int32_t* constrained = A.get<int32_t>(E);
   int32_t* ones = A.get<int32_t>(E);
   int32_t* free_rank = A.get<int32_t>(E + 1);
   int32_t* edge_dof = A.get<int32_t>(E);
   if (A.failed) { set_error("emg_dof_build_device: out of device memory"); return EMG_ERR_NOMEM; }
-  k_edge_ids<<<grid_of(m), kT, 0, st>>>(m, key_s, slot_s, run, id_at, elem_edge, edge_nodes);
+  EMG_CK(cudaMemsetAsync(elem_edge, 0xff, sizeof(int32_t) * std::max<int64_t>(m, 1), st));
+  k_edge_ids<<<grid_of(mv), kT, 0, st>>>(mv, key_s, slot_s, run, id_at, elem_edge, edge_nodes);
   EMG_CK(cudaMemsetAsync(constrained, 0, sizeof(int32_t) * std::max<int64_t>(E, 1), st));
   if (n_dir > 0)
-    k_mark_constrained<<<grid_of(n_dir), kT, 0, st>>>(n_dir, dir_pairs, n_nodes, m, key_s, slot_s, elem_edge,
+    k_mark_constrained<<<grid_of(n_dir), kT, 0, st>>>(n_dir, dir_pairs, n_nodes, mv, key_s, slot_s, elem_edge,
                                                       constrained);
   k_not<<<grid_of(E), kT, 0, st>>>(E, constrained, ones);
   const int ei = static_cast<int>(E);

@@ -45,8 +45,14 @@ ELEM_TET4_EDGE = 0
 ELEM_HEX8_EDGE = 1
 ELEM_PRISM6_EDGE = 2
 ELEM_PYRAMID5_EDGE = 3
-TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE}
-EDGES_OF_TYPE = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8}
+# mixed mesh: rows of 9 ints (8 node slots, -1 past the element's nodes, then
+# its type), 12 edge slots per element in l2g (-1 past the element's edges)
+ELEM_MIXED = 4
+TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE,
+                 9: ELEM_MIXED}
+EDGES_OF_TYPE = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8,
+                 ELEM_MIXED: 12}
+NODES_OF_TYPE = {ELEM_TET4_EDGE: 4, ELEM_HEX8_EDGE: 8, ELEM_PRISM6_EDGE: 6, ELEM_PYRAMID5_EDGE: 5}
 LOCAL_EDGES = {ELEM_TET4_EDGE: GEO_EDGES, ELEM_HEX8_EDGE: HEX_EDGES, ELEM_PRISM6_EDGE: PRISM_EDGES,
                ELEM_PYRAMID5_EDGE: PYRAMID_EDGES}
 
@@ -223,6 +229,81 @@ def hex_scale(n: int = 64, mu_iron: float = 1000.0) -> CubeMesh:
     m = plain_scale(1, mu_iron)
     return CubeMesh(n=n, xyz=xyz, tets=hexes, material=iron.astype(np.int32), dirichlet=dirichlet,
                     nu=m.nu, sigma=m.sigma, sources=m.sources, name=f"hex{n}_iron_coil")
+
+
+def mixed_rows(types, elems) -> np.ndarray:
+    """Padded mixed-mesh rows from per-element types and node lists."""
+    rows = -np.ones((len(types), 9), np.int32)
+    for r, (t, e) in enumerate(zip(types, elems)):
+        rows[r, : len(e)] = e
+        rows[r, 8] = t
+    return rows
+
+
+def element_edges(rows: np.ndarray) -> np.ndarray:
+    """(E, 2) node pairs of every element edge of a one-type or mixed
+    element array, elements in order, local edges in order."""
+    et = TYPE_OF_NODES[rows.shape[1]]
+    if et != ELEM_MIXED:
+        return rows[:, LOCAL_EDGES[et]].reshape(-1, 2)
+    out = [rows[rows[:, 8] == t][:, LOCAL_EDGES[t]].reshape(-1, 2) for t in range(4)]
+    return np.vstack([o for o in out if len(o)])
+
+
+def mixed_cells(n: int, kind_of_cell, small: bool = True, mu_iron: float = 1000.0) -> CubeMesh:
+    """Mixed mesh of the n^3 grid: every cell becomes the elements kind_of_cell
+    (i, j, k) names -- "hex" (one HEX8), "prism" (two PRISM6, as prism_topology),
+    "tet" (six Kuhn TET4) or "pyramid" (six PYRAMID5 around an added centre
+    node, as pyramid_topology) -- cells in k -> j -> i order.  Neighbouring
+    cells must share faces of one shape (quadrilaterals between hex, pyramid
+    and prism side faces; triangles between prisms' z-faces and tets)."""
+    xyz, hexes, _ = _hex_topology(n)
+    n1 = n + 1
+    faces = [[0, 1, 2, 3], [4, 7, 6, 5], [0, 4, 5, 1], [3, 2, 6, 7], [0, 3, 7, 4], [1, 5, 6, 2]]
+    types, elems, centres = [], [], []
+    for c, h in enumerate(hexes):
+        i, j, k = c % n, (c // n) % n, c // (n * n)
+        kind = kind_of_cell(i, j, k)
+        if kind == "hex":
+            types.append(ELEM_HEX8_EDGE); elems.append(h)
+        elif kind == "prism":
+            for sel in ([0, 1, 2, 4, 5, 6], [0, 2, 3, 4, 6, 7]):
+                types.append(ELEM_PRISM6_EDGE); elems.append(h[sel])
+        elif kind == "tet":
+            for tet in KUHN:
+                types.append(ELEM_TET4_EDGE); elems.append(h[tet])
+        else:
+            cid = n1 ** 3 + len(centres)
+            centres.append(xyz[h].mean(axis=0))
+            for f in faces:
+                types.append(ELEM_PYRAMID5_EDGE); elems.append(np.r_[h[f], cid])
+    rows = mixed_rows(types, elems)
+    allxyz = np.vstack([xyz] + ([np.array(centres)] if centres else []))
+    edges = element_edges(rows)
+    d = _boundary_pairs(np.asarray(edges, np.int64), np.array([[0, 1]]), n)
+    m = plain_small(1) if small else plain_scale(1, mu_iron)
+    c = np.array([allxyz[e[:NODES_OF_TYPE[t]]].mean(axis=0) for t, e in zip(types, elems)])
+    mat = np.zeros(len(types), np.int32) if small else (
+        (c[:, 0] > 0.25) & (c[:, 0] < 0.75) & (c[:, 1] > 0.25) & (c[:, 1] < 0.75)
+        & (c[:, 2] > 0.4) & (c[:, 2] < 0.6)).astype(np.int32)
+    return CubeMesh(n=n, xyz=allxyz, tets=rows, material=mat, dirichlet=d, nu=m.nu, sigma=m.sigma,
+                    sources=m.sources, name=f"mixed{n}")
+
+
+def mixed_hex_prism(n: int, small: bool = True) -> CubeMesh:
+    """Hexahedra for x < 1/2, prisms beyond (shared x-faces are quadrilaterals)."""
+    return mixed_cells(n, lambda i, j, k: "hex" if 2 * i < n else "prism", small)
+
+
+def mixed_prism_tet(n: int, small: bool = True) -> CubeMesh:
+    """Prisms for z < 1/2, Kuhn tetrahedra above (shared z-faces are triangles)."""
+    return mixed_cells(n, lambda i, j, k: "prism" if 2 * k < n else "tet", small)
+
+
+def mixed_hex_pyramid_prism(n: int, small: bool = True) -> CubeMesh:
+    """Hexahedra (x < 1/2, z < 1/2), pyramid cells (x < 1/2, z >= 1/2), prisms
+    (x >= 1/2): every shared face a quadrilateral."""
+    return mixed_cells(n, lambda i, j, k: "prism" if 2 * i >= n else ("hex" if 2 * k < n else "pyramid"), small)
 
 
 def _on_cells(kind: str, n: int, mu_iron: float, small: bool) -> CubeMesh:

@@ -60,7 +60,16 @@ enum {
   EMG_ELEM_TET4_EDGE = 0,    /* 4 nodes, 6 edges                                     */
   EMG_ELEM_HEX8_EDGE = 1,    /* 8 nodes (bottom face 0-3, top face 4-7 above them), 12 edges */
   EMG_ELEM_PRISM6_EDGE = 2,  /* 6 nodes (bottom triangle 0-2, top 3-5 above them), 9 edges */
-  EMG_ELEM_PYRAMID5_EDGE = 3 /* 5 nodes (base quadrilateral 0-3, apex 4), 8 edges    */
+  EMG_ELEM_PYRAMID5_EDGE = 3, /* 5 nodes (base quadrilateral 0-3, apex 4), 8 edges    */
+  /* A mesh of several of the types above (per element, as fe_em::Element::
+   * elem_type): every element is a row of 9 ints -- its nodes in the order of
+   * its own type, -1 in the unused node slots, and its type (EMG_ELEM_TET4_EDGE
+   * .. EMG_ELEM_PYRAMID5_EDGE) in slot 8 -- and has 12 entries in l2g (-1 past
+   * its own edges).  Numbering, assembly and the Krylov solvers take it; in
+   * such a mesh the hexahedron's edge functions are scaled to unit
+   * circulation (1/4 of the reference's) to agree with the other elements on
+   * shared edges. */
+  EMG_ELEM_MIXED = 4
 };
 
 /* ---- assembly flags ------------------------------------------------------ */
@@ -183,7 +192,8 @@ int emg_dofmap_expand(emg_dofmap map, const double* reduced, double* full);
 void emg_dofmap_destroy(emg_dofmap map);
 /* emg_dof_build on the device: the same edge IDs, free numbering and `ref`
  * tree-cotree gauge, bit for bit, computed by GPU kernels from DEVICE arrays
- * (elems: nodes_per_elem * n_elems node indices; dir_pairs: 2 * n_dir
+ * (elems: nodes_per_elem * n_elems node indices, or the 9-int rows of an
+ * EMG_ELEM_MIXED mesh; dir_pairs: 2 * n_dir
  * Dirichlet node pairs) into the device array l2g (edges_per_elem * n_elems
  * Local2Global::indices, -1 = constrained or tree edge), ready for
  * emg_system_create_typed with on_device = 1.  gauge_mode: EMG_GAUGE_NONE or

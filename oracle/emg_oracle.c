@@ -107,7 +107,17 @@ static int elem_shape(int32_t elem_type, int* npe, int* epe, const int (**tab)[2
   if (elem_type == ORC_ELEM_HEX8_EDGE) { *npe = 8; *epe = 12; *tab = HEX_EDGE; return 0; }
   if (elem_type == ORC_ELEM_PRISM6_EDGE) { *npe = 6; *epe = 9; *tab = PRISM_EDGE; return 0; }
   if (elem_type == ORC_ELEM_PYRAMID5_EDGE) { *npe = 5; *epe = 8; *tab = PYR_EDGE; return 0; }
+  if (elem_type == ORC_ELEM_MIXED) { *npe = 9; *epe = 12; *tab = NULL; return 0; }
   return ORC_INVALID_INPUT;
+}
+
+/* Nodes, edges, edge table and type of one element row (rows of a mixed mesh
+ * carry their type in slot 8). */
+static int row_shape(int32_t elem_type, const int32_t* row, int* nn, int* ne, const int (**tab)[2],
+                     int32_t* et) {
+  *et = elem_type == ORC_ELEM_MIXED ? row[8] : elem_type;
+  if (*et == ORC_ELEM_MIXED) return ORC_INVALID_INPUT;
+  return elem_shape(*et, nn, ne, tab);
 }
 
 int orc_edge_ids(int64_t n_tets, const int32_t* tets, int32_t* elem_edge,
@@ -121,33 +131,50 @@ int orc_edge_ids_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, i
   const int (*tab)[2];
   *n_edges = 0;
   if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
-  int64_t m = epe * n_tets;
+  const int64_t slots = epe * n_tets;
   if (n_tets <= 0) return 0;
   int32_t maxg = 0;
-  for (int64_t i = 0; i < npe * n_tets; i++) {
-    if (tets[i] < 0) return ORC_INVALID_INPUT;
-    if (tets[i] > maxg) maxg = tets[i];
-  }
-  uint64_t span = (uint64_t)maxg + 1;
-  uint64_t* key = (uint64_t*)malloc((size_t)m * sizeof(uint64_t));
-  int64_t* pos = (int64_t*)malloc((size_t)m * sizeof(int64_t));
-  int64_t* id_at = (int64_t*)malloc((size_t)m * sizeof(int64_t));
-  if (!key || !pos || !id_at) { free(key); free(pos); free(id_at); return -1; }
-  for (int64_t t = 0; t < n_tets; t++)
-    for (int k = 0; k < epe; k++) {
-      uint64_t a = (uint64_t)tets[npe * t + tab[k][0]];
-      uint64_t b = (uint64_t)tets[npe * t + tab[k][1]];
-      uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
-      key[epe * t + k] = lo * span + hi;
-      pos[epe * t + k] = epe * t + k;
+  int64_t m = 0; /* element edges (slots past an element's edges excluded) */
+  for (int64_t t = 0; t < n_tets; t++) {
+    int nn, ne;
+    const int (*rt)[2];
+    int32_t et;
+    if (row_shape(elem_type, tets + npe * t, &nn, &ne, &rt, &et)) return ORC_INVALID_INPUT;
+    for (int a = 0; a < nn; a++) {
+      if (tets[npe * t + a] < 0) return ORC_INVALID_INPUT;
+      if (tets[npe * t + a] > maxg) maxg = tets[npe * t + a];
     }
+    m += ne;
+  }
+  for (int64_t p = 0; p < slots; p++) elem_edge[p] = -1;
+  uint64_t span = (uint64_t)maxg + 1;
+  uint64_t* key = (uint64_t*)malloc((size_t)(m > 0 ? m : 1) * sizeof(uint64_t));
+  int64_t* pos = (int64_t*)malloc((size_t)(m > 0 ? m : 1) * sizeof(int64_t));
+  int64_t* id_at = (int64_t*)malloc((size_t)slots * sizeof(int64_t));
+  if (!key || !pos || !id_at) { free(key); free(pos); free(id_at); return -1; }
+  {
+    int64_t i = 0;
+    for (int64_t t = 0; t < n_tets; t++) {
+      int nn = 0, ne = 0;
+      const int (*rt)[2] = NULL;
+      int32_t et;
+      if (row_shape(elem_type, tets + npe * t, &nn, &ne, &rt, &et)) ne = 0;
+      for (int k = 0; k < ne; k++) {
+        uint64_t a = (uint64_t)tets[npe * t + rt[k][0]];
+        uint64_t b = (uint64_t)tets[npe * t + rt[k][1]];
+        uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+        key[i] = lo * span + hi;
+        pos[i++] = epe * t + k;
+      }
+    }
+  }
   if (radix_sort_u64(m, key, pos, span * span - 1)) { free(key); free(pos); free(id_at); return -1; }
   /* leader flags by position */
-  for (int64_t i = 0; i < m; i++) id_at[i] = 0;
+  for (int64_t i = 0; i < slots; i++) id_at[i] = 0;
   for (int64_t i = 0; i < m; i++)
     if (i == 0 || key[i] != key[i - 1]) id_at[pos[i]] = 1;
   int64_t run = 0;
-  for (int64_t i = 0; i < m; i++) {
+  for (int64_t i = 0; i < slots; i++) {
     int64_t f = id_at[i];
     id_at[i] = f ? run : -1;
     run += f;
@@ -205,7 +232,8 @@ int orc_dof_build_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, 
   if (n_tets <= 0 || E <= 0) return ORC_INVALID_INPUT;
   int32_t maxg = 0;
   for (int64_t i = 0; i < 2 * E; i++) if (edge_nodes[i] > maxg) maxg = edge_nodes[i];
-  for (int64_t i = 0; i < npe * n_tets; i++) if (tets[i] > maxg) maxg = tets[i];
+  for (int64_t i = 0; i < npe * n_tets; i++)
+    if (tets[i] > maxg && (elem_type != ORC_ELEM_MIXED || i % 9 != 8)) maxg = tets[i];
   uint64_t span = (uint64_t)maxg + 1;
 
   /* Edge lookup by sorted node pair (GlobalEdgeIDGenerator::getGlobalEdgeID,
@@ -249,7 +277,14 @@ int orc_dof_build_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, 
      * index = rank of the global node ID among referenced nodes. */
     int32_t* cidx = (int32_t*)malloc((size_t)span * sizeof(int32_t));
     for (uint64_t g = 0; g < span; g++) cidx[g] = -1;
-    for (int64_t i = 0; i < npe * n_tets; i++) cidx[tets[i]] = 1;
+    for (int64_t t = 0; t < n_tets; t++) {  /* nodes referenced by the elements */
+      int nn = 0, ne = 0;
+      const int (*rt)[2] = NULL;
+      int32_t et;
+      if (row_shape(elem_type, tets + npe * t, &nn, &ne, &rt, &et)) nn = 0;
+      for (int a = 0; a < nn; a++)
+        if (tets[npe * t + a] >= 0 && tets[npe * t + a] <= maxg) cidx[tets[npe * t + a]] = 1;
+    }
     int32_t V = 0;
     for (uint64_t g = 0; g < span; g++) if (cidx[g] == 1) cidx[g] = V++;
     /* sorted adjacency with the edge of each entry */
@@ -414,7 +449,7 @@ int orc_dof_build_typed(int32_t elem_type, int64_t n_tets, const int32_t* tets, 
     free(aptr); free(anb); free(aed); free(cidx);
   }
   /* buildVectorElementMapping (em_dof_manager.cpp:353-393) */
-  for (int64_t i = 0; i < epe * n_tets; i++) l2g[i] = edge_dof[elem_edge[i]];
+  for (int64_t i = 0; i < epe * n_tets; i++) l2g[i] = elem_edge[i] < 0 ? -1 : edge_dof[elem_edge[i]];
   free(skey); free(sid); free(constrained); free(free_of);
   return 0;
 }
@@ -1009,8 +1044,12 @@ int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, in
   for (int64_t t = 0; t < n_tets; t++) {
     int32_t mid = material ? material[t] : 0;
     if (mid < 0 || mid >= n_mat) continue; /* em_assembly.cpp:270-276 */
+    int nn, ne;
+    const int (*rt)[2];
+    int32_t et;
+    if (row_shape(elem_type, tets + npe * t, &nn, &ne, &rt, &et)) return ORC_INVALID_INPUT;
     double X[24];
-    for (int a = 0; a < npe; a++) {
+    for (int a = 0; a < nn; a++) {
       int32_t g = tets[npe * t + a];
       if (g < 0 || g >= n_nodes) return ORC_INVALID_INPUT;
       X[3 * a] = xyz[3 * g]; X[3 * a + 1] = xyz[3 * g + 1]; X[3 * a + 2] = xyz[3 * g + 2];
@@ -1018,28 +1057,34 @@ int orc_assemble_typed(int32_t elem_type, int64_t n_nodes, const double* xyz, in
     double Ke[144], Me[144], Fe[12];
     int32_t s[12];
     const double sg = sigma_mat ? sigma_mat[mid] : 0.0;
-    if (elem_type == ORC_ELEM_HEX8_EDGE) {
+    if (et == ORC_ELEM_HEX8_EDGE) {
       orc_element_hex(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
       orc_edge_signs_hex(tets + npe * t, s);
-    } else if (elem_type == ORC_ELEM_PRISM6_EDGE || elem_type == ORC_ELEM_PYRAMID5_EDGE) {
-      orc_element_shape(elem_type == ORC_ELEM_PRISM6_EDGE ? &ORC_PRISM : &ORC_PYRAMID, X, nu_mat[mid], sg, src,
-                        n_src, flags, Ke, Me, Fe);
-      for (int k = 0; k < epe; k++) s[k] = tets[npe * t + tab[k][0]] < tets[npe * t + tab[k][1]] ? 1 : -1;
+      if (elem_type == ORC_ELEM_MIXED) {
+        /* in a mixed mesh the hex basis is scaled to unit circulation (1/4)
+         * so that it agrees with the other elements on shared edges */
+        for (int i = 0; i < 144; i++) { Ke[i] *= 0.0625; Me[i] *= 0.0625; }
+        for (int i = 0; i < 12; i++) Fe[i] *= 0.25;
+      }
+    } else if (et == ORC_ELEM_PRISM6_EDGE || et == ORC_ELEM_PYRAMID5_EDGE) {
+      orc_element_shape(et == ORC_ELEM_PRISM6_EDGE ? &ORC_PRISM : &ORC_PYRAMID, X, nu_mat[mid], sg, src, n_src,
+                        flags, Ke, Me, Fe);
+      for (int k = 0; k < ne; k++) s[k] = tets[npe * t + rt[k][0]] < tets[npe * t + rt[k][1]] ? 1 : -1;
     } else {
       orc_element(X, nu_mat[mid], sg, src, n_src, flags, Ke, Me, Fe);
       orc_edge_signs(tets + npe * t, s);
     }
-    if (flags & ORC_FLAG_NO_EDGE_SIGNS) for (int k = 0; k < epe; k++) s[k] = 1;
+    if (flags & ORC_FLAG_NO_EDGE_SIGNS) for (int k = 0; k < ne; k++) s[k] = 1;
     const int32_t* L = l2g + epe * t;
-    for (int i = 0; i < epe; i++) {
+    for (int i = 0; i < ne; i++) {
       if (L[i] < 0) continue;
       if (rhs) rhs[L[i]] += s[i] * Fe[i];
-      for (int j = 0; j < epe; j++) {
+      for (int j = 0; j < ne; j++) {
         if (L[j] < 0) continue;
         int64_t p = slot_of(row_ptr, col, L[i], L[j]);
         if (p < 0) return ORC_INVALID_INPUT;
-        kval[p] += (double)(s[i] * s[j]) * Ke[epe * i + j];
-        if (mval && (flags & ORC_FLAG_MASS)) mval[p] += (double)(s[i] * s[j]) * Me[epe * i + j];
+        kval[p] += (double)(s[i] * s[j]) * Ke[ne * i + j];
+        if (mval && (flags & ORC_FLAG_MASS)) mval[p] += (double)(s[i] * s[j]) * Me[ne * i + j];
       }
     }
   }
@@ -1328,7 +1373,7 @@ int orc_dof_build_av(int32_t elem_type, int64_t n_nodes, int64_t n_elems, const 
                      int64_t* n_scalar_free, int64_t* n_free, int64_t* n_dofs) {
   int npe, epe;
   const int (*tab)[2];
-  if (elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
+  if (elem_type == ORC_ELEM_MIXED || elem_shape(elem_type, &npe, &epe, &tab)) return ORC_INVALID_INPUT;
   const int w = npe + epe;
   int64_t i, e, nv = 0, nsf = 0, ne = 0, vf = 0, vd = 0, k = 0;
   int32_t root = -1;

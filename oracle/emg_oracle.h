@@ -38,7 +38,10 @@ enum {
 };
 
 /* Element types (same values as the C ABI's EMG_ELEM_*). */
-enum { ORC_ELEM_TET4_EDGE = 0, ORC_ELEM_HEX8_EDGE = 1, ORC_ELEM_PRISM6_EDGE = 2, ORC_ELEM_PYRAMID5_EDGE = 3 };
+enum { ORC_ELEM_TET4_EDGE = 0, ORC_ELEM_HEX8_EDGE = 1, ORC_ELEM_PRISM6_EDGE = 2, ORC_ELEM_PYRAMID5_EDGE = 3,
+       /* mixed mesh: 9 ints per element (8 node slots, -1 past the element's
+        * nodes, then its type), 12 edge slots per element (-1 past its edges) */
+       ORC_ELEM_MIXED = 4 };
 
 /* Gauge modes. */
 enum { ORC_GAUGE_NONE = -1, ORC_GAUGE_REF = 0, ORC_GAUGE_BOUNDARY_FIRST = 1 };

@@ -81,14 +81,15 @@ def lib():
 
 
 ELEM_TET4_EDGE, ELEM_HEX8_EDGE, ELEM_PRISM6_EDGE, ELEM_PYRAMID5_EDGE = 0, 1, 2, 3
-_TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE}
-_EDGES = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8}
+ELEM_MIXED = 4  # rows of 8 node slots (-1 padded) + the element type; 12 edge slots
+_TYPE_OF_NODES = {4: ELEM_TET4_EDGE, 8: ELEM_HEX8_EDGE, 6: ELEM_PRISM6_EDGE, 5: ELEM_PYRAMID5_EDGE, 9: ELEM_MIXED}
+_EDGES = {ELEM_TET4_EDGE: 6, ELEM_HEX8_EDGE: 12, ELEM_PRISM6_EDGE: 9, ELEM_PYRAMID5_EDGE: 8, ELEM_MIXED: 12}
 _TYPE_OF_EDGES = {v: k for k, v in _EDGES.items()}
 
 
 def elem_type_of(elems) -> int:
     """Element type of a (T, nodes) array: 4 TET4_EDGE, 8 HEX8_EDGE, 6
-    PRISM6_EDGE, 5 PYRAMID5_EDGE."""
+    PRISM6_EDGE, 5 PYRAMID5_EDGE, 9 a mixed mesh."""
     return _TYPE_OF_NODES[np.asarray(elems).shape[-1]]
 
 

@@ -31,8 +31,11 @@
 namespace {
 
 // Element types of the C ABI (EMG_ELEM_*) as the reference's ElementType.
-static int bridge_npe(int32_t t) { return t == 1 ? 8 : t == 2 ? 6 : t == 3 ? 5 : 4; }
-static int bridge_epe(int32_t t) { return t == 1 ? 12 : t == 2 ? 9 : t == 3 ? 8 : 6; }
+// Type 4 is a mixed mesh: rows of 9 ints (8 node slots, -1 past the
+// element's nodes, then its type) and 12 edge slots per element.
+static int bridge_npe(int32_t t) { return t == 1 ? 8 : t == 2 ? 6 : t == 3 ? 5 : t == 4 ? 9 : 4; }
+static int bridge_epe(int32_t t) { return t == 1 ? 12 : t == 2 ? 9 : t == 3 ? 8 : t == 4 ? 12 : 6; }
+static int32_t row_type(int32_t elem_type, const int32_t* row) { return elem_type == 4 ? row[8] : elem_type; }
 static numeric::ElementType bridge_type(int32_t t) {
   return t == 1   ? numeric::ElementType::HEX8_EDGE
          : t == 2 ? numeric::ElementType::PRISM6_EDGE
@@ -54,8 +57,9 @@ fe_em::EMMeshData make_mesh(int64_t n_nodes, const double* xyz, int64_t n_tets, 
   for (int64_t t = 0; t < n_tets; ++t) {
     auto& e = m.elements[t];
     e.id = static_cast<int>(t);
-    e.node_ids.assign(tets + npe * t, tets + npe * (t + 1));
-    e.elem_type = bridge_type(elem_type);
+    const int32_t et = row_type(elem_type, tets + npe * t);
+    e.node_ids.assign(tets + npe * t, tets + npe * t + bridge_npe(et));
+    e.elem_type = bridge_type(et);
     e.dof_type = fe_em::DOFType::VECTOR_EDGE_ONLY;
     e.material_id = 0;
     e.region_id = 0;
@@ -131,8 +135,9 @@ int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, con
     gen.generate();
     const auto& l2e = gen.getElemLocalToGlobalEdge();
     for (int64_t t = 0; t < n_tets; ++t) {
-      if (static_cast<int>(l2e[t].size()) != epe) return -3;
-      for (int k = 0; k < epe; ++k) elem_edge_out[epe * t + k] = l2e[t][k];
+      const int ne = bridge_epe(row_type(elem_type, tets + bridge_npe(elem_type) * t));
+      if (static_cast<int>(l2e[t].size()) != ne) return -3;
+      for (int k = 0; k < epe; ++k) elem_edge_out[epe * t + k] = k < ne ? l2e[t][k] : -1;
     }
     *n_edges = gen.getNumGlobalEdges();
     fe_em::EMDOFManager dm(mesh, l2e, &gen);
@@ -142,8 +147,9 @@ int refb_dof_build_typed(int32_t elem_type, int64_t n_nodes, int64_t n_tets, con
     *n_dofs = dm.getNumFreeDOFs();
     const auto& l2g = dm.getElemLocalToGlobal();
     for (int64_t t = 0; t < n_tets; ++t) {
-      if (static_cast<int>(l2g[t].indices.size()) != epe) return -3;
-      for (int k = 0; k < epe; ++k) l2g_out[epe * t + k] = l2g[t].indices[k];
+      const int ne = bridge_epe(row_type(elem_type, tets + bridge_npe(elem_type) * t));
+      if (static_cast<int>(l2g[t].indices.size()) != ne) return -3;
+      for (int k = 0; k < epe; ++k) l2g_out[epe * t + k] = k < ne ? l2g[t].indices[k] : -1;
     }
     return 0;
   } catch (const std::exception&) {

@@ -58,7 +58,7 @@ def lib():
 
 
 def _elem_type(tets) -> int:
-    return {4: 0, 8: 1, 6: 2, 5: 3}[np.asarray(tets).shape[1]]
+    return {4: 0, 8: 1, 6: 2, 5: 3, 9: 4}[np.asarray(tets).shape[1]]
 
 
 def dof_build(n_nodes, tets, dirichlet, gauge=True, n_holes=0):
@@ -66,7 +66,7 @@ def dof_build(n_nodes, tets, dirichlet, gauge=True, n_holes=0):
     HEX8_EDGE elements."""
     tets = np.ascontiguousarray(tets, np.int32)
     et = _elem_type(tets)
-    epe = {0: 6, 1: 12, 2: 9, 3: 8}[et]
+    epe = {0: 6, 1: 12, 2: 9, 3: 8, 4: 12}[et]
     T = tets.shape[0]
     d = np.ascontiguousarray(dirichlet, np.int32).reshape(-1)
     ee = np.empty(epe * T, np.int32)

@@ -1,5 +1,6 @@
 """Device DOF numbering (emg_dof_build_device) against the host numbering and
-the oracle: Local2Global maps and counts bit-exact for every element type,
+the oracle: Local2Global maps and counts bit-exact for every element type and
+mixed meshes,
 the `ref` gauge and none, full / partial / empty Dirichlet lists, hole
 markers and meshes of several components; invalid input is rejected."""
 import ctypes as C
@@ -30,7 +31,9 @@ def device_map(elems, n_nodes, dirichlet, gauge, holes=0):
 
 MESHES = [("tet", lambda: mesh.plain_scale(6)), ("tet_perturbed", lambda: mesh.perturbed(mesh.plain_scale(5), 0.2, 1)),
           ("random", lambda: mesh.random_instance(7, seed=3)), ("hex", lambda: mesh.hex_scale(5)),
-          ("prism", lambda: mesh.prism_scale(5)), ("pyramid", lambda: mesh.pyramid_scale(4))]
+          ("prism", lambda: mesh.prism_scale(5)), ("pyramid", lambda: mesh.pyramid_scale(4)),
+          ("mixed_hex_prism", lambda: mesh.mixed_hex_prism(4)), ("mixed_prism_tet", lambda: mesh.mixed_prism_tet(4)),
+          ("mixed_hex_pyramid_prism", lambda: mesh.perturbed(mesh.mixed_hex_pyramid_prism(4), 0.2, 2))]
 
 
 @pytest.mark.parametrize("name,make", MESHES)
