@@ -401,7 +401,6 @@ int emg_dof_build_partitioned(emg_mesh mesh, const int32_t* tet_part, int32_t n_
   return guarded([&]() -> int {
     if (!mesh || !out) { set_error("null handle"); return EMG_INVALID_INPUT; }
     *out = nullptr;
-    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_dof_build_partitioned: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     auto* h = new emg_dofmap_t();
     int rc = emg::build_dofmap_partitioned(mesh->m, tet_part, n_parts, h->d);
     if (rc) { delete h; return rc; }
@@ -868,7 +867,6 @@ int emg_fetidp_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_fetidp* o
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
     *out = nullptr;
-    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_fetidp_create: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     emg::keep_pool_memory();
     auto* h = new emg_fetidp_t();
     int rc = h->fd.create(mesh->m, map->d, as_stream(stream));
@@ -1000,7 +998,6 @@ int emg_direct_create(emg_mesh mesh, emg_dofmap map, void* stream, emg_direct* o
   return guarded([&]() -> int {
     if (!mesh || !map || !out) { set_error("null argument"); return EMG_INVALID_INPUT; }
     *out = nullptr;
-    if (mesh->m.elem_type == EMG_ELEM_MIXED) { set_error("emg_direct_create: mixed-type meshes are numbered, assembled and solved by the Krylov solvers only"); return EMG_INVALID_INPUT; }
     if (map->d.n_elems != mesh->m.n_elems || map->d.elem_type != mesh->m.elem_type ||
         map->d.l2g.size() != static_cast<size_t>(mesh->m.epe() * mesh->m.n_elems)) {
       set_error("DOF map does not belong to this mesh");

@@ -41,7 +41,7 @@ namespace {
 #endif
 constexpr int kNB = EMG_FETI_NB;  // panel width of the partial Cholesky
 constexpr int kTile = 64;     // output tile of the rank-k updates
-constexpr int kKC = 32;       // k-chunk of the rank-k updates
+[[maybe_unused]] constexpr int kKC = 32;  // k-chunk of the FMA (non-tensor-core) rank-k updates
 constexpr int kTrsmRows = 128;
 constexpr double kMinInnerTol = 1e-12;  // floor of a pass's multiplier tolerance
 
@@ -589,132 +589,147 @@ __global__ void __launch_bounds__(tc::kThreads) k_tc_tile_test(double* C, int64_
 
 // --------------------------------------------------- triangular inverse
 
-// Blocked X = L^-1: one CTA per 64-column block J of one matrix; row blocks
-// I = J, J+1, ... in order: X_IJ = L_II^-1 (E_IJ - sum_{J<=K<I} L_IK X_KJ),
-// the sum as 64 x 64 tile products staged in shared memory, the small
-// triangular solve in shared memory.  The strict upper part of X is zero.
+// Blocked X = L^-1 for a batch of lower factors, stored in full: the lower
+// triangle holds X and the strict upper triangle its transpose (X^T), which
+// is what the column-dot mat-vecs of the multiplier loop read and what the
+// off-diagonal blocks read their right operand from.  Two launches:
+//   k_trtri_diag:  X_JJ = L_JJ^-1 for every 64 x 64 diagonal block
+//                  (forward substitution, one thread per column);
+//   k_trtri_off:   one CTA per column block J (J-major order, so the longest
+//                  chains start first), row blocks I = J+1, J+2, ... in order:
+//                  X_IJ = -X_II (sum_{J<=K<I} L_IK X_KJ), the sum a 64-wide
+//                  tile product on the FP64 tensor cores (mma m8n8k4, k-chunks
+//                  double-buffered by cp.async, X_KJ read from the transposes
+//                  this CTA stored in the upper blocks), the product with
+//                  X_II a second tile product from shared memory; X_IJ and
+//                  its transpose are stored through shared memory, coalesced.
 constexpr int kTB = 64;
-constexpr size_t kTrtriSmem = sizeof(double) * 2 * kTB * (kTB + 1);
+constexpr size_t kTrtriDiagSmem = sizeof(double) * 2 * kTB * (kTB + 1);
+constexpr size_t kTrtriOffSmem = sizeof(double) * 2 * kTB * kMmaPad;
+static_assert(kTB == kTile && sizeof(TileSmemMma) <= kTrtriOffSmem && (kGK * kTB) % kMmaThreads == 0,
+              "staging of the triangular inverse");
 
-__global__ void __launch_bounds__(256) k_trtri_blk(int32_t n_mat, const int32_t* __restrict__ dim,
-                                                   const int64_t* __restrict__ l_off,
-                                                   const int64_t* __restrict__ x_off,
-                                                   const double* __restrict__ Lbase, double* __restrict__ Xbase) {
+__global__ void __launch_bounds__(kTB) k_trtri_diag(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                    const int64_t* __restrict__ l_off,
+                                                    const int64_t* __restrict__ x_off,
+                                                    const double* __restrict__ Lbase, double* __restrict__ Xbase) {
   extern __shared__ double sm[];
-  const int32_t m = blockIdx.y;
+  double (*Ls)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);
+  double (*Is)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kTB * (kTB + 1));
+  const int32_t m = blockIdx.x;
   if (m >= n_mat) return;
   const int32_t n = dim[m];
-  const int32_t c0 = blockIdx.x * kTB;
+  const int32_t c0 = blockIdx.y * kTB;
   if (c0 >= n) return;
-  const int32_t w = min(kTB, n - c0);
+  const int32_t h = min(kTB, n - c0);
+  const double* L = Lbase + l_off[m] + c0 + static_cast<int64_t>(c0) * n;
+  double* X = Xbase + x_off[m] + c0 + static_cast<int64_t>(c0) * n;
+  const int c = threadIdx.x;
+  for (int q = 0; q < h; ++q) Ls[c][q] = (c < h && c >= q) ? L[c + static_cast<int64_t>(q) * n] : 0.0;
+  __syncthreads();
+  if (c < h)  // column c of the inverse: rows above the diagonal come out zero
+    for (int r = 0; r < h; ++r) {
+      double v = r == c ? 1.0 : 0.0;
+      for (int q = 0; q < r; ++q) v -= Ls[r][q] * Is[q][c];
+      Is[r][c] = v / Ls[r][r];
+    }
+  __syncthreads();
+  if (c < h)  // thread c writes row c of every column: lower X, upper X^T
+    for (int q = 0; q < h; ++q) X[c + static_cast<int64_t>(q) * n] = c >= q ? Is[c][q] : Is[q][c];
+}
+
+__global__ void __launch_bounds__(kMmaThreads) k_trtri_off(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                           const int64_t* __restrict__ l_off,
+                                                           const int64_t* __restrict__ x_off,
+                                                           const double* __restrict__ Lbase,
+                                                           double* __restrict__ Xbase) {
+  extern __shared__ double smd[];
+  TileSmemMma& sm = *reinterpret_cast<TileSmemMma*>(smd);
+  double (*Ts)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(smd);             // after the sum: T, then X_IJ
+  double (*Ds)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(smd + kTB * kMmaPad);  // X_II, k-major
+  const int32_t m = blockIdx.x;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m], nb = (n + kTB - 1) / kTB;
+  const int32_t J = blockIdx.y;
+  if (J + 1 >= nb) return;  // the last column block is its diagonal block alone
+  const int32_t c0 = J * kTB;
   const double* L = Lbase + l_off[m];
   double* X = Xbase + x_off[m];
-  const int tid = threadIdx.x;
-#if !EMG_FETI_DMMA
-  const int tx = tid & 15, ty = tid >> 4;
-  double (*As)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);               // [kKC][kTB+1]
-  double (*Bs)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kKC * (kTB + 1));
-#endif
-  double (*T)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);                // [kTB][kTB+1]
-  double (*Ls)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kTB * (kTB + 1));
-  for (int64_t e = tid; e < static_cast<int64_t>(c0) * w; e += blockDim.x) {
-    const int32_t c = static_cast<int32_t>(e / c0), r = static_cast<int32_t>(e - static_cast<int64_t>(c) * c0);
-    X[r + static_cast<int64_t>(c0 + c) * n] = 0.0;
-  }
-  const int32_t nb = (n + kTB - 1) / kTB;
-  for (int32_t I = blockIdx.x; I < nb; ++I) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, fr = lane >> 2, fk = lane & 3;
+  // right operand B(c, k) = X[c0 + k, c0 + c]: the stored transpose X[c0 + c, c0 + k]
+  const double* B = X + c0 + static_cast<int64_t>(c0) * n;
+  for (int32_t I = J + 1; I < nb; ++I) {
     const int32_t r0 = I * kTB, h = min(kTB, n - r0);
-#if EMG_FETI_DMMA
-    // E_IJ - sum_K L_IK X_KJ on the FP64 tensor cores: warp wp owns rows
-    // 8 wp .. 8 wp + 7 of the 64 x 64 block (fragments of mma m8n8k4)
-    {
-      static_assert(kTB == kTile && kKC % 4 == 0 && 2 * kKC * kMmaPad <= 2 * kTB * (kTB + 1),
-                    "staging of the tensor-core product");
-      const int lane = tid & 31, wp = tid >> 5, fr = lane >> 2, fk = lane & 3;
-      double (*As2)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(sm);
-      double (*Bs2)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(sm + kKC * kMmaPad);
-      double acc2[8][2];
+    const double* A = L + r0 + static_cast<int64_t>(c0) * n;
+    const int nk = (I - J) * (kTB / kGK);
+    auto load = [&](int chunk, int buf) {
+      const int k0 = chunk * kGK;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int i = 0; i < (kGK * kTB) / kMmaThreads; ++i) {
+        const int e = t + kMmaThreads * i;
+        const int c = e / kTB, r = e - c * kTB;
+        const int k = k0 + c;
+        const bool va = r < h;
+        const bool vb = k >= kTB || k >= r;  // X_JJ is lower triangular: its upper half reads as zero
+        cp_async8(&sm.a[buf][c][r], va ? A + r + static_cast<int64_t>(k) * n : A, va);
+        cp_async8(&sm.b[buf][c][r], vb ? B + r + static_cast<int64_t>(k) * n : B, vb);
+      }
+      cp_async_commit();
+    };
+    double acc[8][2];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) acc2[j][q] = (r0 == c0 && 8 * wp + fr == 8 * j + 2 * fk + q) ? 1.0 : 0.0;
-      for (int32_t k0 = c0; k0 < r0; k0 += kKC) {  // K blocks left of I are full
-        __syncthreads();
-        for (int e = tid; e < kKC * kTB; e += blockDim.x) {
-          const int k = e / kTB, r = e - k * kTB;
-          As2[k][r] = r < h ? L[(r0 + r) + static_cast<int64_t>(k0 + k) * n] : 0.0;
-        }
-        for (int e = tid; e < kKC * kTB; e += blockDim.x) {
-          const int c = e / kKC, k = e - c * kKC;
-          Bs2[k][c] = c < w ? X[(k0 + k) + static_cast<int64_t>(c0 + c) * n] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kKC; kk += 4) {
-          const double a = -As2[kk + fk][8 * wp + fr];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) dmma_8x8x4(acc2[j], a, Bs2[kk + fk][8 * j + fr]);
-        }
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+    load(0, 0);
+    for (int i = 0; i < nk; ++i) {
+      if (i + 1 < nk) {
+        load(i + 1, (i + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
       }
       __syncthreads();
+      const int buf = i & 1;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int kk = 0; kk < kGK; kk += 4) {
+        const double a = sm.a[buf][kk + fk][8 * w + fr];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) T[8 * wp + fr][8 * j + 2 * fk + q] = acc2[j][q];
+        for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[j], a, sm.b[buf][kk + fk][8 * j + fr]);
+      }
+      __syncthreads();
     }
-#else
-    double acc[4][4];
+    // T = -sum (rows of T are the k of the product with X_II); X_II lower, k-major
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = (r0 == c0 && 4 * tx + a == 4 * ty + b) ? 1.0 : 0.0;
-    for (int32_t k0 = c0; k0 < r0; k0 += kKC) {  // K blocks left of I are full
-      __syncthreads();
-      for (int e = tid; e < kKC * kTB; e += blockDim.x) {
-        const int k = e / kTB, r = e - k * kTB;
-        As[k][r] = r < h ? L[(r0 + r) + static_cast<int64_t>(k0 + k) * n] : 0.0;
-      }
-      for (int e = tid; e < kKC * kTB; e += blockDim.x) {
-        const int c = e / kKC, k = e - c * kKC;
-        Bs[k][c] = c < w ? X[(k0 + k) + static_cast<int64_t>(c0 + c) * n] : 0.0;
-      }
-      __syncthreads();
+      for (int q = 0; q < 2; ++q) Ts[8 * w + fr][8 * j + 2 * fk + q] = -acc[j][q];
+    for (int e = t; e < kTB * kTB; e += kMmaThreads) {
+      const int k = e / kTB, r = e - k * kTB;
+      Ds[k][r] = (r < h && k <= r) ? X[(r0 + r) + static_cast<int64_t>(r0 + k) * n] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
 #pragma unroll 4
-      for (int k = 0; k < kKC; ++k) {
-        double a[4], b[4];
+    for (int kk = 0; kk < kTB; kk += 4) {
+      const double a = Ds[kk + fk][8 * w + fr];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) { a[q] = As[k][4 * tx + q]; b[q] = Bs[k][4 * ty + q]; }
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = fma(-a[x], b[y], acc[x][y]);
-      }
+      for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[j], a, Ts[kk + fk][8 * j + fr]);
     }
     __syncthreads();
 #pragma unroll
-    for (int x = 0; x < 4; ++x)
+    for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int y = 0; y < 4; ++y) T[4 * tx + x][4 * ty + y] = acc[x][y];
-#endif
-    for (int e = tid; e < kTB * kTB; e += blockDim.x) {
-      const int q = e / kTB, r = e - q * kTB;
-      Ls[r][q] = (r < h && q < h && r >= q) ? L[(r0 + r) + static_cast<int64_t>(r0 + q) * n] : 0.0;
-    }
+      for (int q = 0; q < 2; ++q) Ts[8 * w + fr][8 * j + 2 * fk + q] = acc[j][q];
     __syncthreads();
-    for (int q = 0; q < h; ++q) {
-      if (tid < w) T[q][tid] /= Ls[q][q];
-      __syncthreads();
-      const int rows = h - q - 1;
-      for (int e = tid; e < rows * w; e += blockDim.x) {
-        const int r = q + 1 + e / w, c = e % w;
-        T[r][c] -= Ls[r][q] * T[q][c];
-      }
-      __syncthreads();
+    for (int e = t; e < kTB * kTB; e += kMmaThreads) {  // X_IJ, coalesced along its rows
+      const int c = e / kTB, r = e - c * kTB;
+      if (r < h) X[(r0 + r) + static_cast<int64_t>(c0 + c) * n] = Ts[r][c];
     }
-    for (int e = tid; e < h * w; e += blockDim.x) {
-      const int c = e / h, r = e - c * h;
-      X[(r0 + r) + static_cast<int64_t>(c0 + c) * n] = T[r][c];
+    for (int e = t; e < kTB * kTB; e += kMmaThreads) {  // its transpose in the upper block (J, I)
+      const int r = e / kTB, c = e - r * kTB;
+      if (r < h) X[(c0 + c) + static_cast<int64_t>(r0 + r) * n] = Ts[r][c];
     }
+    __threadfence_block();  // the next row block's sum reads these transposes
     __syncthreads();
   }
 }
@@ -942,6 +957,102 @@ __global__ void __launch_bounds__(kPivMax) k_front_bwd_piv(FrontsDev F, int32_t 
   }
 }
 
+// Levels whose fronts all have at most kSB pivots (the many small fronts
+// near the leaves): a warp per (front, column) does the front's whole forward
+// step -- the children's update vectors, the pivot block, the update rows --
+// or its whole backward step, eight fronts to a CTA instead of one wide CTA
+// per front.  The operations and their order are those of the block kernels
+// (the same substitution chains, the same fma order over the pivots, the
+// same warp sums), so the results are the same bit for bit.
+constexpr int kSmallWarps = 8;
+
+__global__ void __launch_bounds__(32 * kSmallWarps) k_front_fwd_small(FrontsDev F, int32_t f0, int32_t nf,
+                                                                      int32_t ncol, RhsDev R,
+                                                                      const int32_t* __restrict__ nI,
+                                                                      const int32_t* __restrict__ nD,
+                                                                      const double* __restrict__ fac) {
+  const int lane = threadIdx.x & 31;
+  const int64_t item = static_cast<int64_t>(blockIdx.x) * kSmallWarps + (threadIdx.x >> 5);
+  if (item >= static_cast<int64_t>(nf) * ncol) return;
+  const int32_t k = f0 + static_cast<int32_t>(item / ncol), col = static_cast<int32_t>(item % ncol);
+  if (F.is_root[k]) return;
+  const int32_t s = F.sub[k];
+  if (col >= R.ncol[s]) return;
+  const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
+  const int32_t ld = nI[s] + nD[s];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
+  for (int32_t i = lane; i < nu; i += 32) V[i] = 0.0;
+  __syncwarp();
+  for (int32_t ci = 0; ci < F.nchild[k]; ++ci) {
+    const int32_t c = F.child_v[F.child0[k] + ci];
+    const int32_t ncu = F.f[c] - F.npiv[c];
+    const double* Vc = R.v + R.voff[c] + static_cast<int64_t>(col) * ncu;
+    const int32_t* cp = F.cpos_v + F.cpos[c];
+    for (int32_t a = lane; a < ncu; a += 32) {
+      const int32_t r = cp[a];
+      if (r < np) x[p0 + r] += Vc[a];
+      else V[r - np] += Vc[a];
+    }
+    __syncwarp();
+  }
+  const double* L = fac + F.fac[k];
+  double v = lane < np ? x[p0 + lane] : 0.0;
+  for (int32_t j = 0; j < np; ++j) {
+    const double yj = __shfl_sync(0xffffffffu, v, j) / L[j + static_cast<int64_t>(j) * fs];
+    if (lane == j) v = yj;
+    if (lane > j && lane < np) v -= L[lane + static_cast<int64_t>(j) * fs] * yj;
+  }
+  if (lane < np) x[p0 + lane] = v;
+  for (int32_t b = np; b < fs; b += 32) {
+    const int32_t i = b + lane;
+    double acc = 0.0;
+    for (int32_t j = 0; j < np; ++j) {
+      const double yj = __shfl_sync(0xffffffffu, v, j);
+      if (i < fs) acc = fma(L[i + static_cast<int64_t>(j) * fs], yj, acc);
+    }
+    if (i < fs) V[i - np] -= acc;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kSmallWarps) k_front_bwd_small(FrontsDev F, int32_t f0, int32_t nf,
+                                                                      int32_t ncol, RhsDev R,
+                                                                      const int32_t* __restrict__ nI,
+                                                                      const int32_t* __restrict__ nD,
+                                                                      const double* __restrict__ fac) {
+  const int lane = threadIdx.x & 31;
+  const int64_t item = static_cast<int64_t>(blockIdx.x) * kSmallWarps + (threadIdx.x >> 5);
+  if (item >= static_cast<int64_t>(nf) * ncol) return;
+  const int32_t k = f0 + static_cast<int32_t>(item / ncol), col = static_cast<int32_t>(item % ncol);
+  if (F.is_root[k]) return;
+  const int32_t s = F.sub[k];
+  if (col >= R.ncol[s]) return;
+  const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
+  if (np == 0) return;
+  const int32_t ld = nI[s] + nD[s];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
+  const double* L = fac + F.fac[k];
+  const int32_t* rows = F.rows_v + F.rows[k];
+  // update rows: x_j -= sum_{i >= np} L[i, j] x[row i]
+  for (int32_t j = 0; j < np && fs > np; ++j) {
+    const double* Lj = L + static_cast<int64_t>(j) * fs;
+    double acc = 0.0;
+    for (int32_t i = np + lane; i < fs; i += 32) acc = fma(Lj[i], x[rows[i]], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) x[p0 + j] -= acc;
+  }
+  __syncwarp();
+  // pivot block: one panel, so no pivot rows below it to subtract
+  double v = lane < np ? x[p0 + lane] : 0.0;
+  for (int32_t j = np - 1; j >= 0; --j) {
+    double part = (lane > j && lane < np) ? L[lane + static_cast<int64_t>(j) * fs] * v : 0.0;
+    part = warp_sum(part);
+    const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / L[j + static_cast<int64_t>(j) * fs];
+    if (lane == j) v = xj;
+  }
+  if (lane < np) x[p0 + lane] = v;
+}
+
 // Root fronts, forward part: add the children's update vectors into x_D.
 __global__ void k_root_gather(FrontsDev F, const int32_t* __restrict__ root_k, RhsDev R,
                               const int32_t* __restrict__ nI, const int32_t* __restrict__ nD) {
@@ -961,7 +1072,7 @@ __global__ void k_root_gather(FrontsDev F, const int32_t* __restrict__ root_k, R
   }
 }
 
-// Root solve x_D = L^-T (L^-1 x_D) with the mirrored inverse M (M = L^-1 in
+// Root solve x_D = L^-T (L^-1 x_D) with the stored inverse M (M = L^-1 in
 // the lower triangle, its transpose in the upper): pass 0 tmp = L^-1 x_D
 // (column c, rows <= c), pass 1 x_D = L^-T tmp (column c, rows >= c).  One
 // warp per (root, column, row c).
@@ -994,25 +1105,10 @@ __global__ void __launch_bounds__(256) k_root_apply(const int32_t* __restrict__ 
   }
 }
 
-// Mirror the lower triangle of each n x n block into its upper triangle.
-__global__ void k_mirror_lower(int32_t n_mat, const int32_t* __restrict__ dim, const int64_t* __restrict__ off,
-                               double* __restrict__ M) {
-  const int32_t m = blockIdx.y;
-  if (m >= n_mat) return;
-  const int32_t n = dim[m];
-  double* A = M + off[m];
-  const int64_t tot = static_cast<int64_t>(n) * n;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t j = static_cast<int32_t>(e / n), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * n);
-    if (i < j) A[e] = A[j + static_cast<int64_t>(i) * n];
-  }
-}
-
 // Column-dot mat-vec of dense blocks: y_c = sum over rows r in the range of
 // column c of M[r, c] w_r; range 0: r <= c, 1: r >= c, 2: all rows.
 // y[c] = column c of block m (rows lo..hi) . w, one warp per column.  range
-// 0: rows 0..c (the mirrored upper part of L^-1: y = L^-1 w), 1: rows c..n-1
+// 0: rows 0..c (the stored transpose above the diagonal: y = L^-1 w), 1: rows c..n-1
 // (y = L^-T w), 2: all rows.  The column is read with 16-byte loads (after a
 // scalar head up to the first aligned element), four vectors in flight per
 // lane; w, which every column of the block reads, stays in L1/L2.
@@ -1267,6 +1363,10 @@ __global__ void k_face_gather(FacesDev Fc, const int32_t* __restrict__ lam_entry
   }
 }
 
+// Xt = X^T for every face block; kLower: the transpose of the lower
+// triangle alone (a stored inverse factor holds its own transpose above the
+// diagonal, which the product X^T X must not see).
+template <bool kLower>
 __global__ void k_face_transpose(FacesDev Fc, const double* __restrict__ X, double* __restrict__ Xt) {
   const int32_t f = blockIdx.y;
   const int32_t n = Fc.dim[f];
@@ -1274,7 +1374,7 @@ __global__ void k_face_transpose(FacesDev Fc, const double* __restrict__ X, doub
   for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int32_t j = static_cast<int32_t>(e / n), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * n);
-    Xt[Fc.off[f] + j + static_cast<int64_t>(i) * n] = X[Fc.off[f] + e];
+    Xt[Fc.off[f] + j + static_cast<int64_t>(i) * n] = (!kLower || i >= j) ? X[Fc.off[f] + e] : 0.0;
   }
 }
 
@@ -1879,18 +1979,25 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
   return EMG_SUCCESS;
 }
 
-// X = L^-1 for n_mat lower factors stored in fac_d (blocked kernel).
-// The shared-memory limit is a per-device attribute of the kernel: set it
-// on every call (cheap), so a solve on another device or thread launches
-// with it too.
+// X = L^-1 for n_mat lower factors stored in fac_d, in full (X below the
+// diagonal, X^T above it).  The shared-memory limits are per-device
+// attributes of the kernels: set them on every call (cheap), so a solve on
+// another device or thread launches with them too.
 int FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
                   double* X) {
   if (n_mat == 0 || max_n == 0) return EMG_SUCCESS;
-  if (!capturing)
-    EMG_CK(cudaFuncSetAttribute(k_trtri_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kTrtriSmem)));
-  k_trtri_blk<<<dim3(static_cast<unsigned>((max_n + kTB - 1) / kTB), static_cast<unsigned>(n_mat)), 256, kTrtriSmem,
-                st>>>(n_mat, dim, l_off, x_off, fac_d, X);
+  if (!capturing) {
+    EMG_CK(cudaFuncSetAttribute(k_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kTrtriDiagSmem)));
+    EMG_CK(cudaFuncSetAttribute(k_trtri_off, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kTrtriOffSmem)));
+  }
+  const unsigned nb = static_cast<unsigned>((max_n + kTB - 1) / kTB);
+  k_trtri_diag<<<dim3(static_cast<unsigned>(n_mat), nb), kTB, kTrtriDiagSmem, st>>>(n_mat, dim, l_off, x_off, fac_d,
+                                                                                   X);
+  if (nb > 1)
+    k_trtri_off<<<dim3(static_cast<unsigned>(n_mat), nb - 1), kMmaThreads, kTrtriOffSmem, st>>>(n_mat, dim, l_off,
+                                                                                                 x_off, fac_d, X);
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
 }
@@ -1916,6 +2023,12 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0) continue;  // (a front without pivots still gathers its children)
+    if (lvl_max_np[h] <= kSB) {
+      const int64_t items = static_cast<int64_t>(nf) * ncol;
+      k_front_fwd_small<<<static_cast<unsigned>((items + kSmallWarps - 1) / kSmallWarps), 32 * kSmallWarps, 0, st>>>(
+          fd, f0, nf, ncol, R, d_nI, d_nD, fac_d);
+      continue;
+    }
     k_front_fwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
     if (lvl_max_nu[h] > 0)
       k_front_fwd_upd<<<dim3(static_cast<unsigned>((lvl_max_nu[h] + upd_rows - 1) / upd_rows),
@@ -1935,6 +2048,12 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0 || lvl_max_np[h] == 0) continue;
+    if (lvl_max_np[h] <= kSB) {
+      const int64_t items = static_cast<int64_t>(nf) * ncol;
+      k_front_bwd_small<<<static_cast<unsigned>((items + kSmallWarps - 1) / kSmallWarps), 32 * kSmallWarps, 0, st>>>(
+          fd, f0, nf, ncol, R, d_nI, d_nD, fac_d);
+      continue;
+    }
     if (lvl_max_nu[h] > 0)
       k_front_bwd_upd<<<dim3(static_cast<unsigned>((lvl_max_np[h] + 7) / 8), static_cast<unsigned>(nf), ngroups), 256,
                         0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
@@ -2027,15 +2146,15 @@ int FetiDP::setup_deluxe() {
   if (rc) return rc;
   rc = trtri(NF, max_fdim, fc.dim, fc.fac, fc.off, fX_d);
   if (rc) return rc;
-  k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);
+  k_face_transpose<true><<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fX_d, fXt_d);  // (L^-1)^T
   const int32_t nt = (max_fdim + kTile - 1) / kTile;
   const dim3 g(static_cast<unsigned>(nt * nt), nf);
   k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fXt_d, fXt_d, fZ_d);   // (S_a + S_b)^-1 = X^T X
   k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fZ_d, fSb_d, fDa_d);   // D_a = (S_a + S_b)^-1 S_b
   k_face_gemm_nt<<<g, kTileThreads, 0, st>>>(fc, fZ_d, fSa_d, fDb_d);   // D_b = (S_a + S_b)^-1 S_a
   // transposes for the row pass, in the buffers of X and X^T (no longer needed)
-  k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
-  k_face_transpose<<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
+  k_face_transpose<false><<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDa_d, fX_d);
+  k_face_transpose<false><<<dim3(blocks_for(f2, 256, 256), nf), 256, 0, st>>>(fc, fDb_d, fXt_d);
   // FP32 copies for the mixed-precision preconditioner
   const int64_t fsz = P.face_off.back();
   k_to_f32<<<blocks_for(fsz, 256), 256, 0, st>>>(fsz, fDa_d, fDa32_d);
@@ -2177,10 +2296,8 @@ int FetiDP::factor_device() {
   if (!rc && !capturing) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
   if (n_roots > 0) {
-    rc = trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);
+    rc = trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);  // L^-1 with L^-T above the diagonal
     if (rc) return rc;
-    k_mirror_lower<<<dim3(blocks_for(static_cast<int64_t>(max_nD) * max_nD, 256, 256),
-                          static_cast<unsigned>(n_roots)), 256, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d);
   }
   // Phi = K_rr^-1 K_rP (columns 0..nP-1) and z = K_rr^-1 f_r (column nP)
   EMG_CK(cudaMemsetAsync(phi_d, 0, sizeof(double) * std::max<int64_t>(phi_size, 1), st));
@@ -2204,7 +2321,6 @@ int FetiDP::factor_device() {
     if (rc) return rc;
     rc = trtri(1, static_cast<int32_t>(nc), d_cdim, d_cfac, d_czero, Lcc_d);
     if (rc) return rc;
-    k_mirror_lower<<<dim3(blocks_for(nc * nc, 256, 256), 1), 256, 0, st>>>(1, d_cdim, d_czero, Lcc_d);
   }
   const int64_t ne = P.dual_off[S];
   if (ne > 0) {

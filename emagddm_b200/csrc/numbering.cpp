@@ -481,6 +481,7 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
     const int32_t p = tet_part[t];
     for (int k = 0; k < epe; ++k) {
       const int32_t e = m.elem_edge[epe * t + k];
+      if (e < 0) continue;  // slot past a mixed-mesh element's edges
       if (p1[e] < 0) p1[e] = p;
       else if (p1[e] != p) {
         if (p2[e] < 0) p2[e] = p;
@@ -550,11 +551,13 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
     edges.clear();
     for (int64_t q = tptr[p]; q < tptr[p + 1]; ++q) {
       const int64_t t = tlist[q];
-      for (int a = 0; a < npe; ++a) {
+      const int nn = nodes_per_elem(row_type(m.elem_type, &m.elems[npe * t]));
+      for (int a = 0; a < nn; ++a) {
         const int32_t v = m.elems[npe * t + a];
         if (node_loc[v] < 0) { node_loc[v] = static_cast<int32_t>(nodes.size()); nodes.push_back(v); }
       }
-      for (int k = 0; k < epe; ++k) edges.push_back(m.elem_edge[epe * t + k]);
+      for (int k = 0; k < epe; ++k)
+        if (m.elem_edge[epe * t + k] >= 0) edges.push_back(m.elem_edge[epe * t + k]);
     }
     std::sort(edges.begin(), edges.end());
     edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
@@ -587,7 +590,7 @@ int build_dofmap_partitioned(Mesh& m, const int32_t* tet_part, int32_t n_parts, 
   out.n_dofs = nr;
   out.n_primal_fix = fixes;
   out.l2g.resize(m.elem_edge.size());
-  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = out.edge_dof[m.elem_edge[p]];
+  for (size_t p = 0; p < m.elem_edge.size(); ++p) out.l2g[p] = m.elem_edge[p] < 0 ? -1 : out.edge_dof[m.elem_edge[p]];
   return EMG_SUCCESS;
 }
 

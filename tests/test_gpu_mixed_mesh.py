@@ -87,3 +87,25 @@ def test_tet_only_flag_is_rejected():
     l2g = O.dof_build(m.tets, m.dirichlet, gauge=O.GAUGE_REF)["l2g"]
     with pytest.raises(_abi.EmgError):
         System(m, l2g, flags=_abi.FLAG_QUAD3_LITERAL)
+
+
+@pytest.mark.parametrize("name,make", LAYOUTS)
+def test_fetidp_and_direct_match_monolithic_oracle(name, make):
+    from emagddm_b200 import fetidp
+    m = mesh.perturbed(make(8, small=False), 0.2, seed=5)
+    part = mesh.jittered_partition(m, 2)
+    fd = fetidp.FetiDP(m, part, 8)
+    assert fd.factor() == _abi.EMG_SUCCESS, _abi.lib().emg_last_error()
+    x, rc, out = fd.solve(tol=1e-10, max_iter=2000, precond=2)
+    assert rc == _abi.EMG_SUCCESS, (rc, _abi.lib().emg_last_error())
+    rp, col, kv, _, rhs = oracle_system(m, fd.map.l2g)
+    xo, st, it, res = O.pcg(rp, col, kv, rhs, tol=1e-13, max_iter=50000, precond=1)
+    assert np.linalg.norm(xo) > 1e-6
+    assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+    ds = fetidp.DirectSolver(m)
+    assert ds.factor() == _abi.EMG_SUCCESS, _abi.lib().emg_last_error()
+    xd, rc, out = ds.solve(tol=1e-12)
+    assert rc == _abi.EMG_SUCCESS
+    rp, col, kv, _, rhs = oracle_system(m, ds.l2g)
+    xo, st, it, res = O.pcg(rp, col, kv, rhs, tol=1e-13, max_iter=50000, precond=1)
+    assert np.linalg.norm(xd - xo) <= 1e-8 * np.linalg.norm(xo)

@@ -114,7 +114,7 @@ def test_malformed_rows_are_rejected():
     assert create(bad, m.n_nodes) == _abi.EMG_INVALID_INPUT
 
 
-def test_single_type_paths_reject_mixed_meshes():
+def test_av_map_rejects_mixed_meshes():
     m = mesh.mixed_prism_tet(2)
     rows = np.ascontiguousarray(m.tets, np.int32)
     h = C.c_void_p()
@@ -122,8 +122,24 @@ def test_single_type_paths_reject_mixed_meshes():
     assert L.emg_mesh_create_typed(mesh.ELEM_MIXED, m.n_nodes, None, rows.shape[0], _abi.ptr(rows), None, 0, None, 0,
                                    C.byref(h)) == 0
     try:
-        part = np.zeros(rows.shape[0], np.int32)
-        out = C.c_void_p()
-        assert L.emg_dof_build_partitioned(h, _abi.ptr(part), 1, C.byref(out)) == _abi.EMG_INVALID_INPUT
+        dof_type = np.full(rows.shape[0], 2, np.int32)
+        l2g = np.empty(rows.shape[0] * 21, np.int32)
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        assert L.emg_dof_build_av(h, _abi.ptr(dof_type), 0, None, 0, _abi.ptr(l2g), C.byref(a), C.byref(b),
+                                  C.byref(c)) == _abi.EMG_INVALID_INPUT
     finally:
         L.emg_mesh_destroy(h)
+
+
+def test_partitioned_gauge_on_mixed_mesh():
+    """The partitioned gauge (FETI-DP's numbering) on a mixed mesh: every
+    subdomain's DOFs stay connected and the map is a proper gauge (every free
+    edge numbered or in the tree)."""
+    from emagddm_b200 import fetidp
+    m = mesh.mixed_hex_pyramid_prism(4)
+    part = mesh.jittered_partition(m, 2)
+    pm = fetidp.partitioned_dofmap(m, part, 8)
+    assert pm.l2g.shape == (m.n_tets, 12)
+    for t, row in zip(m.tets[:, 8], pm.l2g):
+        assert (row[mesh.EDGES_OF_TYPE[t]:] == -1).all()
+    assert pm.n_dofs > 0
