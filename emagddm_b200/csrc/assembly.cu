@@ -413,15 +413,6 @@ __device__ __forceinline__ void source_at(const double* x, const emg_source* tab
   }
 }
 
-__device__ __forceinline__ int find_slot(const int32_t* __restrict__ col, int32_t lo, int32_t hi,
-                                         int32_t c) {
-  while (lo < hi) {
-    int32_t mid = (lo + hi) >> 1;
-    if (col[mid] < c) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
 struct AsmArgs {
   int64_t n, n_nodes;
   const int32_t* row_ptr;

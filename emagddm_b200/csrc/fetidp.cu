@@ -957,100 +957,170 @@ __global__ void __launch_bounds__(kPivMax) k_front_bwd_piv(FrontsDev F, int32_t 
   }
 }
 
-// Levels whose fronts all have at most kSB pivots (the many small fronts
-// near the leaves): a warp per (front, column) does the front's whole forward
-// step -- the children's update vectors, the pivot block, the update rows --
-// or its whole backward step, eight fronts to a CTA instead of one wide CTA
-// per front.  The operations and their order are those of the block kernels
-// (the same substitution chains, the same fma order over the pivots, the
-// same warp sums), so the results are the same bit for bit.
-constexpr int kSmallWarps = 8;
+// Levels of medium fronts (at most kMidMaxF rows: the leaves and the levels
+// above them): one CTA per (front, group of kC right-hand-side columns) does
+// the front's whole step with the group's front columns held in shared
+// memory -- forward: the children's update vectors, then per 32-pivot panel
+// the diagonal solves (a warp per column) and the update of every row below
+// the panel, pivot and update rows alike, for all kC columns at once;
+// backward: per panel, last first, the column dots of the panel with every
+// row below it, then the diagonal solves.  Each factor entry is read once per
+// column group, and the small CTAs keep many fronts in flight where the wide
+// pivot-block CTAs would idle on the panel chain.
+constexpr int kMidMaxF = 1024;
+constexpr int kMidCols = 8;  // columns per CTA of the multi-column variant
+template <int kC>
+constexpr int mid_threads() { return kC == 1 ? 128 : 256; }
+template <int kC>
+size_t mid_smem(int32_t max_f) { return sizeof(double) * (static_cast<size_t>(kC) * max_f + kC * kSB); }
 
-__global__ void __launch_bounds__(32 * kSmallWarps) k_front_fwd_small(FrontsDev F, int32_t f0, int32_t nf,
-                                                                      int32_t ncol, RhsDev R,
-                                                                      const int32_t* __restrict__ nI,
-                                                                      const int32_t* __restrict__ nD,
-                                                                      const double* __restrict__ fac) {
-  const int lane = threadIdx.x & 31;
-  const int64_t item = static_cast<int64_t>(blockIdx.x) * kSmallWarps + (threadIdx.x >> 5);
-  if (item >= static_cast<int64_t>(nf) * ncol) return;
-  const int32_t k = f0 + static_cast<int32_t>(item / ncol), col = static_cast<int32_t>(item % ncol);
+template <int kC>
+__global__ void __launch_bounds__(mid_threads<kC>()) k_front_fwd_mid(FrontsDev F, int32_t f0, RhsDev R,
+                                                                     const int32_t* __restrict__ nI,
+                                                                     const int32_t* __restrict__ nD,
+                                                                     const double* __restrict__ fac, int32_t ldx) {
+  constexpr int kT = mid_threads<kC>();
+  const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
-  if (col >= R.ncol[s]) return;
+  const int32_t c0 = blockIdx.x * kC;
+  const int32_t nc = min(kC, R.ncol[s] - c0);
+  if (nc <= 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int32_t np = F.npiv[k], fs = F.f[k], nu = fs - np, p0 = F.p0[k];
   const int32_t ld = nI[s] + nD[s];
-  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
-  double* V = R.v + R.voff[k] + static_cast<int64_t>(col) * nu;
-  for (int32_t i = lane; i < nu; i += 32) V[i] = 0.0;
-  __syncwarp();
+  double* x = R.x + R.off[s] + static_cast<int64_t>(c0) * ld;
+  double* V = R.v + R.voff[k] + static_cast<int64_t>(c0) * nu;
+  extern __shared__ double smid[];
+  double* xs = smid;                 // [kC][ldx]: the front's rows of each column
+  double* yb = smid + kC * ldx;      // [kC][kSB]: the panel's solved values
+  __shared__ double Db[kSB][kSB + 1];
+  for (int32_t e = tid; e < nc * fs; e += kT) {
+    const int32_t c = e / fs, i = e - c * fs;
+    xs[c * ldx + i] = i < np ? x[static_cast<int64_t>(c) * ld + p0 + i] : 0.0;
+  }
+  __syncthreads();
   for (int32_t ci = 0; ci < F.nchild[k]; ++ci) {
-    const int32_t c = F.child_v[F.child0[k] + ci];
-    const int32_t ncu = F.f[c] - F.npiv[c];
-    const double* Vc = R.v + R.voff[c] + static_cast<int64_t>(col) * ncu;
-    const int32_t* cp = F.cpos_v + F.cpos[c];
-    for (int32_t a = lane; a < ncu; a += 32) {
-      const int32_t r = cp[a];
-      if (r < np) x[p0 + r] += Vc[a];
-      else V[r - np] += Vc[a];
+    const int32_t ch = F.child_v[F.child0[k] + ci];
+    const int32_t ncu = F.f[ch] - F.npiv[ch];
+    const double* Vc = R.v + R.voff[ch] + static_cast<int64_t>(c0) * ncu;
+    const int32_t* cp = F.cpos_v + F.cpos[ch];
+    for (int32_t e = tid; e < nc * ncu; e += kT) {
+      const int32_t c = e / ncu, a = e - c * ncu;
+      xs[c * ldx + cp[a]] += Vc[static_cast<int64_t>(c) * ncu + a];
     }
-    __syncwarp();
+    __syncthreads();
   }
   const double* L = fac + F.fac[k];
-  double v = lane < np ? x[p0 + lane] : 0.0;
-  for (int32_t j = 0; j < np; ++j) {
-    const double yj = __shfl_sync(0xffffffffu, v, j) / L[j + static_cast<int64_t>(j) * fs];
-    if (lane == j) v = yj;
-    if (lane > j && lane < np) v -= L[lane + static_cast<int64_t>(j) * fs] * yj;
-  }
-  if (lane < np) x[p0 + lane] = v;
-  for (int32_t b = np; b < fs; b += 32) {
-    const int32_t i = b + lane;
-    double acc = 0.0;
-    for (int32_t j = 0; j < np; ++j) {
-      const double yj = __shfl_sync(0xffffffffu, v, j);
-      if (i < fs) acc = fma(L[i + static_cast<int64_t>(j) * fs], yj, acc);
+  for (int32_t jb = 0; jb < np; jb += kSB) {
+    const int32_t nb = min(kSB, np - jb);
+    for (int e = tid; e < nb * nb; e += kT) {
+      const int c = e / nb, r = e - c * nb;
+      Db[r][c] = L[(jb + r) + static_cast<int64_t>(jb + c) * fs];
     }
-    if (i < fs) V[i - np] -= acc;
+    __syncthreads();
+    for (int c = wid; c < nc; c += kT / 32) {
+      double v = lane < nb ? xs[c * ldx + jb + lane] : 0.0;
+      for (int32_t j = 0; j < nb; ++j) {
+        const double yj = __shfl_sync(0xffffffffu, v, j) / Db[j][j];
+        if (lane == j) v = yj;
+        if (lane > j && lane < nb) v -= Db[lane][j] * yj;
+      }
+      if (lane < nb) { xs[c * ldx + jb + lane] = v; yb[c * kSB + lane] = v; }
+    }
+    __syncthreads();
+    const double* Lp = L + static_cast<int64_t>(jb) * fs;
+    for (int32_t i = jb + nb + tid; i < fs; i += kT) {
+      double acc[kC];
+#pragma unroll
+      for (int c = 0; c < kC; ++c) acc[c] = 0.0;
+#pragma unroll 4
+      for (int32_t j = 0; j < nb; ++j) {
+        const double l = Lp[i + static_cast<int64_t>(j) * fs];
+#pragma unroll
+        for (int c = 0; c < kC; ++c) acc[c] = fma(l, yb[c * kSB + j], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < kC; ++c)
+        if (c < nc) xs[c * ldx + i] -= acc[c];
+    }
+    __syncthreads();
+  }
+  for (int32_t e = tid; e < nc * fs; e += kT) {
+    const int32_t c = e / fs, i = e - c * fs;
+    if (i < np) x[static_cast<int64_t>(c) * ld + p0 + i] = xs[c * ldx + i];
+    else V[static_cast<int64_t>(c) * nu + i - np] = xs[c * ldx + i];
   }
 }
 
-__global__ void __launch_bounds__(32 * kSmallWarps) k_front_bwd_small(FrontsDev F, int32_t f0, int32_t nf,
-                                                                      int32_t ncol, RhsDev R,
-                                                                      const int32_t* __restrict__ nI,
-                                                                      const int32_t* __restrict__ nD,
-                                                                      const double* __restrict__ fac) {
-  const int lane = threadIdx.x & 31;
-  const int64_t item = static_cast<int64_t>(blockIdx.x) * kSmallWarps + (threadIdx.x >> 5);
-  if (item >= static_cast<int64_t>(nf) * ncol) return;
-  const int32_t k = f0 + static_cast<int32_t>(item / ncol), col = static_cast<int32_t>(item % ncol);
+template <int kC>
+__global__ void __launch_bounds__(mid_threads<kC>()) k_front_bwd_mid(FrontsDev F, int32_t f0, RhsDev R,
+                                                                     const int32_t* __restrict__ nI,
+                                                                     const int32_t* __restrict__ nD,
+                                                                     const double* __restrict__ fac, int32_t ldx) {
+  constexpr int kT = mid_threads<kC>();
+  const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
-  if (col >= R.ncol[s]) return;
+  const int32_t c0 = blockIdx.x * kC;
+  const int32_t nc = min(kC, R.ncol[s] - c0);
+  if (nc <= 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int32_t np = F.npiv[k], fs = F.f[k], p0 = F.p0[k];
   if (np == 0) return;
   const int32_t ld = nI[s] + nD[s];
-  double* x = R.x + R.off[s] + static_cast<int64_t>(col) * ld;
-  const double* L = fac + F.fac[k];
+  double* x = R.x + R.off[s] + static_cast<int64_t>(c0) * ld;
   const int32_t* rows = F.rows_v + F.rows[k];
-  // update rows: x_j -= sum_{i >= np} L[i, j] x[row i]
-  for (int32_t j = 0; j < np && fs > np; ++j) {
-    const double* Lj = L + static_cast<int64_t>(j) * fs;
-    double acc = 0.0;
-    for (int32_t i = np + lane; i < fs; i += 32) acc = fma(Lj[i], x[rows[i]], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) x[p0 + j] -= acc;
+  extern __shared__ double smid[];
+  double* xs = smid;                 // [kC][ldx]
+  double* tb = smid + kC * ldx;      // [kC][kSB]: the panel's column dots
+  __shared__ double Db[kSB][kSB + 1];
+  for (int32_t e = tid; e < nc * fs; e += kT) {
+    const int32_t c = e / fs, i = e - c * fs;
+    xs[c * ldx + i] = x[static_cast<int64_t>(c) * ld + (i < np ? p0 + i : rows[i])];
   }
-  __syncwarp();
-  // pivot block: one panel, so no pivot rows below it to subtract
-  double v = lane < np ? x[p0 + lane] : 0.0;
-  for (int32_t j = np - 1; j >= 0; --j) {
-    double part = (lane > j && lane < np) ? L[lane + static_cast<int64_t>(j) * fs] * v : 0.0;
-    part = warp_sum(part);
-    const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / L[j + static_cast<int64_t>(j) * fs];
-    if (lane == j) v = xj;
+  const double* L = fac + F.fac[k];
+  for (int32_t jb = ((np - 1) / kSB) * kSB; jb >= 0; jb -= kSB) {
+    const int32_t nb = min(kSB, np - jb);
+    __syncthreads();
+    for (int e = tid; e < nb * nb; e += kT) {
+      const int c = e / nb, r = e - c * nb;
+      Db[r][c] = L[(jb + r) + static_cast<int64_t>(jb + c) * fs];
+    }
+    for (int32_t j = wid; j < nb; j += kT / 32) {
+      const double* Lj = L + static_cast<int64_t>(jb + j) * fs;
+      double acc[kC];
+#pragma unroll
+      for (int c = 0; c < kC; ++c) acc[c] = 0.0;
+      for (int32_t i = jb + nb + lane; i < fs; i += 32) {
+        const double l = Lj[i];
+#pragma unroll
+        for (int c = 0; c < kC; ++c)
+          if (c < nc) acc[c] = fma(l, xs[c * ldx + i], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        const double a = warp_sum(acc[c]);
+        if (lane == 0 && c < nc) tb[c * kSB + j] = a;
+      }
+    }
+    __syncthreads();
+    for (int c = wid; c < nc; c += kT / 32) {
+      double v = lane < nb ? xs[c * ldx + jb + lane] - tb[c * kSB + lane] : 0.0;
+      for (int32_t j = nb - 1; j >= 0; --j) {
+        double part = (lane > j && lane < nb) ? Db[lane][j] * v : 0.0;
+        part = warp_sum(part);
+        const double xj = (__shfl_sync(0xffffffffu, v, j) - part) / Db[j][j];
+        if (lane == j) v = xj;
+      }
+      if (lane < nb) xs[c * ldx + jb + lane] = v;
+    }
   }
-  if (lane < np) x[p0 + lane] = v;
+  __syncthreads();
+  for (int32_t e = tid; e < nc * np; e += kT) {
+    const int32_t c = e / np, i = e - c * np;
+    x[static_cast<int64_t>(c) * ld + p0 + i] = xs[c * ldx + i];
+  }
 }
 
 // Root fronts, forward part: add the children's update vectors into x_D.
@@ -2010,23 +2080,36 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   if (static_cast<int32_t>(lvl_max_np.size()) != nlev) {  // largest pivot / update counts per level
     lvl_max_np.assign(nlev, 0);
     lvl_max_nu.assign(nlev, 0);
+    lvl_max_f.assign(nlev, 0);
     for (int32_t h = 0; h < nlev; ++h)
       for (int32_t k = plan.level_ptr[h]; k < plan.level_ptr[h + 1]; ++k) {
         const FetiFront& x = plan.fronts[k];
         if (x.is_root) continue;
         lvl_max_np[h] = std::max(lvl_max_np[h], x.npiv);
         lvl_max_nu[h] = std::max(lvl_max_nu[h], x.f - x.npiv);
+        lvl_max_f[h] = std::max(lvl_max_f[h], x.f);
       }
   }
   const unsigned nc = static_cast<unsigned>(ncol);
   const unsigned ngroups = static_cast<unsigned>((ncol + kColB - 1) / kColB);
+  const unsigned ngroups_mid = static_cast<unsigned>((ncol + kMidCols - 1) / kMidCols);
+  if (mid_fronts && !capturing && ncol > 1)  // up to 8 x 1024 doubles of front columns a CTA
+    EMG_CK(cudaFuncSetAttribute(k_front_fwd_mid<kMidCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(mid_smem<kMidCols>(kMidMaxF))));
+  if (mid_fronts && !capturing && ncol > 1)
+    EMG_CK(cudaFuncSetAttribute(k_front_bwd_mid<kMidCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(mid_smem<kMidCols>(kMidMaxF))));
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0) continue;  // (a front without pivots still gathers its children)
-    if (lvl_max_np[h] <= kSB) {
-      const int64_t items = static_cast<int64_t>(nf) * ncol;
-      k_front_fwd_small<<<static_cast<unsigned>((items + kSmallWarps - 1) / kSmallWarps), 32 * kSmallWarps, 0, st>>>(
-          fd, f0, nf, ncol, R, d_nI, d_nD, fac_d);
+    if (mid_fronts && lvl_max_f[h] <= kMidMaxF) {
+      const int32_t ldx = std::max(lvl_max_f[h], 1);
+      if (ncol == 1)
+        k_front_fwd_mid<1><<<dim3(1, static_cast<unsigned>(nf)), mid_threads<1>(), mid_smem<1>(ldx), st>>>(
+            fd, f0, R, d_nI, d_nD, fac_d, ldx);
+      else
+        k_front_fwd_mid<kMidCols><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), mid_threads<kMidCols>(),
+                                    mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
       continue;
     }
     k_front_fwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
@@ -2048,10 +2131,14 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0 || lvl_max_np[h] == 0) continue;
-    if (lvl_max_np[h] <= kSB) {
-      const int64_t items = static_cast<int64_t>(nf) * ncol;
-      k_front_bwd_small<<<static_cast<unsigned>((items + kSmallWarps - 1) / kSmallWarps), 32 * kSmallWarps, 0, st>>>(
-          fd, f0, nf, ncol, R, d_nI, d_nD, fac_d);
+    if (mid_fronts && lvl_max_f[h] <= kMidMaxF) {
+      const int32_t ldx = std::max(lvl_max_f[h], 1);
+      if (ncol == 1)
+        k_front_bwd_mid<1><<<dim3(1, static_cast<unsigned>(nf)), mid_threads<1>(), mid_smem<1>(ldx), st>>>(
+            fd, f0, R, d_nI, d_nD, fac_d, ldx);
+      else
+        k_front_bwd_mid<kMidCols><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), mid_threads<kMidCols>(),
+                                    mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
       continue;
     }
     if (lvl_max_nu[h] > 0)
@@ -2336,9 +2423,10 @@ int FetiDP::factor_device() {
   return EMG_SUCCESS;
 }
 
-// CTA widths of the solve kernels, chosen by the autotuner on this plan's
-// shape (tune.h): the pivot-block and update-row kernels of the front
-// solves (a single-column solve into scratch vectors) and the dense column
+// Launch choices of the solve kernels, made by the autotuner on this plan's
+// shape (tune.h): the fused kernels on the medium-front levels or not, the
+// CTA widths of the pivot-block and update-row kernels of the front
+// solves (a single-column solve into scratch vectors) and of the dense column
 // dots of the multiplier iteration (an S_DD pass).  The values of the
 // vectors do not matter for the timing; the kernels read and write only the
 // solver's own scratch.
@@ -2347,6 +2435,10 @@ void FetiDP::tune_solve_kernels() {
                           std::to_string(plan.n_parts);
   RhsDev R1{xu_d, d_roff1, d_ncol1, d_voff1, v1_d};
   const int32_t saved_upd = upd_rows;
+  mid_fronts = tune::pick("feti.front_mid_levels", key, {1, 0}, [&](int v, cudaStream_t) {
+    mid_fronts = v != 0;
+    solve_fronts(R1, 1);
+  }, st) != 0;
   piv_threads = tune::pick("feti.front_pivot_threads", key, {512, 256, 1024}, [&](int v, cudaStream_t) {
     piv_threads = v;
     solve_fronts(R1, 1);

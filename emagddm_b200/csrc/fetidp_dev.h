@@ -77,6 +77,7 @@ struct FetiDP {
   bool tc_factor = false;  // factor contractions on the TF32 tensor cores (EMG_FLAG_FACTOR_TF32)
   // CTA widths of the solve kernels (autotuned after the first factorization)
   int32_t piv_threads = 512, upd_rows = 256, gemv_warps = 8;
+  bool mid_fronts = true;  // fused CTA-per-front solve kernels on the levels of medium fronts
   bool tuned = false;
   int32_t precond = 2;  // 0 none, 1 Dirichlet stiffness-scaled, 2 deluxe-scaled, 3 deluxe with FP32 blocks,
                         // 4 deluxe + learned correction (flexible CG)
@@ -104,7 +105,8 @@ struct FetiDP {
   int64_t coarse_fac = 0;
   // extra fronts after the plan's: [0] the coarse matrix, [1 + f] face f's S_a + S_b
   std::vector<int32_t> xnp;
-  std::vector<int32_t> lvl_max_np, lvl_max_nu;  // per level, non-root fronts: largest pivot / update counts
+  std::vector<int32_t> lvl_max_np, lvl_max_nu, lvl_max_f;  // per level, non-root fronts: largest pivot / update
+                                                         // counts and front size
   int32_t max_fdim = 0;
   // solve layouts
   int64_t *d_roff_s = nullptr, *d_roff1 = nullptr, *d_voff_s = nullptr, *d_voff1 = nullptr;
