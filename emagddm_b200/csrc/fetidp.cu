@@ -42,7 +42,6 @@ namespace {
 constexpr int kNB = EMG_FETI_NB;  // panel width of the partial Cholesky
 constexpr int kTile = 64;     // output tile of the rank-k updates
 [[maybe_unused]] constexpr int kKC = 32;  // k-chunk of the FMA (non-tensor-core) rank-k updates
-constexpr int kTrsmRows = 128;
 constexpr double kMinInnerTol = 1e-12;  // floor of a pass's multiplier tolerance
 
 enum : int32_t { kErrPivot = 1, kErrAsm = 2, kErrTc = 4 };
@@ -200,56 +199,27 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int
     const int c = e / nb, r = e - c * nb;
     if (r >= c) A[r + static_cast<int64_t>(c) * fs] = D[r][c];
   }
-}
-
-// Panel rows below the diagonal block: X L_kk^T = F[i, k0:k0+nb].
-constexpr size_t kTrsmSmem = sizeof(double) * (static_cast<size_t>(kNB) * (kNB + 1) +
-                                               static_cast<size_t>(kNB) * kTrsmRows);
-__global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(FrontsDev F, int32_t f0, int32_t k0,
-                                                          double* __restrict__ fac) {
-  extern __shared__ double trsm_sm[];
-  double (*D)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(trsm_sm);
-  double (*X)[kTrsmRows] = reinterpret_cast<double (*)[kTrsmRows]>(trsm_sm + kNB * (kNB + 1));
-  const int32_t k = f0 + blockIdx.y;
-  const int32_t np = F.npiv[k];
-  if (k0 >= np) return;
-  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
-  const int32_t r0 = k0 + nb + blockIdx.x * kTrsmRows;
-  if (r0 >= fs) return;
-  double* A = fac + F.fac[k];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int c = e / nb, r = e - c * nb;
-    D[r][c] = A[(k0 + r) + static_cast<int64_t>(k0 + c) * fs];
-  }
-  const int32_t i = r0 + threadIdx.x;
-  const bool live = i < fs;
-  if (nb == kNB) {
-    // full panel: the row in registers (the same operations in the same order)
-    __syncthreads();
-    double xr[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) xr[c] = live ? A[i + static_cast<int64_t>(k0 + c) * fs] : 0.0;
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) {
-      double v = xr[c];
-#pragma unroll
-      for (int q = 0; q < c; ++q) v -= xr[q] * D[c][q];
-      xr[c] = v / D[c][c];
+  // The inverse X = L_kk^-1 in place, last column first: X_jj = 1 / L_jj,
+  // X_rj = -(sum_{j<q<=r} X_rq L_qj) / L_jj.  Its strict lower part goes,
+  // transposed, into the strict upper part of the diagonal block, which no
+  // other step reads; the panel TRSM and the inverse factors multiply by it
+  // (its diagonal they recompute from L_kk's).
+  for (int j = nb - 1; j >= 0; --j) {
+    const int r = j + 1 + static_cast<int>(threadIdx.x);
+    double v = 0.0;
+    if (r < nb) {
+      for (int q = j + 1; q <= r; ++q) v += D[r][q] * D[q][j];
+      v = -v / D[j][j];
     }
-    if (live)
-#pragma unroll
-      for (int c = 0; c < kNB; ++c) A[i + static_cast<int64_t>(k0 + c) * fs] = xr[c];
-    return;
+    __syncthreads();
+    if (r < nb) D[r][j] = v;
+    if (threadIdx.x == 0) D[j][j] = 1.0 / D[j][j];
+    __syncthreads();
   }
-  for (int c = 0; c < nb; ++c) X[c][threadIdx.x] = live ? A[i + static_cast<int64_t>(k0 + c) * fs] : 0.0;
-  __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    double v = X[c][threadIdx.x];
-    for (int q = 0; q < c; ++q) v -= X[q][threadIdx.x] * D[c][q];
-    X[c][threadIdx.x] = v / D[c][c];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int r = e / nb, c = e - r * nb;
+    if (c < r) A[c + static_cast<int64_t>(r) * fs] = D[r][c];
   }
-  if (live)
-    for (int c = 0; c < nb; ++c) A[i + static_cast<int64_t>(k0 + c) * fs] = X[c][threadIdx.x];
 }
 
 // Asynchronous 8-byte global -> shared copy; `valid` false fills a zero
@@ -470,6 +440,63 @@ __device__ __forceinline__ void tile_update_wide(double* __restrict__ C, int64_t
 
 #endif
 
+// Panel rows below the diagonal block: X L_kk^T = F[i, k0:k0+nb], formed as
+// X = F L_kk^-T with the inverse that k_potrf_diag stored above the diagonal:
+// one 64-row tile a CTA, the tile and L_kk^-1 staged in shared memory, the
+// 64 x 64 x 64 product on the FP64 tensor cores (mma m8n8k4, warp w owns
+// rows 8w .. 8w+7), the result written back through shared memory.
+constexpr size_t kTrsmSmem = sizeof(double) * 2 * kTile * kMmaPad;
+__global__ void __launch_bounds__(kMmaThreads) k_trsm_panel(FrontsDev F, int32_t f0, int32_t k0,
+                                                            double* __restrict__ fac) {
+  static_assert(kNB == kTile, "the panel TRSM tile is the panel width");
+  extern __shared__ double trsm_sm[];
+  double (*As)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(trsm_sm);                  // [k][row]
+  double (*Bs)[kMmaPad] = reinterpret_cast<double (*)[kMmaPad]>(trsm_sm + kTile * kMmaPad);  // [k][col]: Linv(col, k)
+  const int32_t k = f0 + blockIdx.y;
+  const int32_t np = F.npiv[k];
+  if (k0 >= np) return;
+  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
+  const int32_t r0 = k0 + nb + blockIdx.x * kTile;
+  if (r0 >= fs) return;
+  const int32_t h = min(kTile, fs - r0);
+  double* A = fac + F.fac[k];
+  const int t = threadIdx.x;
+  for (int e = t; e < kTile * kTile; e += kMmaThreads) {
+    const int c = e / kTile, r = e - c * kTile;
+    As[c][r] = (r < h && c < nb) ? A[(r0 + r) + static_cast<int64_t>(k0 + c) * fs] : 0.0;
+  }
+  for (int e = t; e < kTile * kTile; e += kMmaThreads) {
+    const int c = e / kTile, q = e - c * kTile;  // Linv(c, q): stored at row q, column c of the block
+    double v = 0.0;
+    if (c < nb && q < nb) {
+      if (c > q) v = A[(k0 + q) + static_cast<int64_t>(k0 + c) * fs];
+      else if (c == q) v = 1.0 / A[(k0 + c) + static_cast<int64_t>(k0 + c) * fs];
+    }
+    Bs[q][c] = v;
+  }
+  __syncthreads();
+  const int lane = t & 31, w = t >> 5, fr = lane >> 2, fk = lane & 3;
+  double acc[8][2];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll 4
+  for (int kk = 0; kk < kTile; kk += 4) {
+    const double a = As[kk + fk][8 * w + fr];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[j], a, Bs[kk + fk][8 * j + fr]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) As[8 * j + 2 * fk + q][8 * w + fr] = acc[j][q];
+  __syncthreads();
+  for (int e = t; e < kTile * nb; e += kMmaThreads) {
+    const int c = e / kTile, r = e - c * kTile;
+    if (r < h) A[(r0 + r) + static_cast<int64_t>(k0 + c) * fs] = As[c][r];
+  }
+}
+
 // Right-looking update of the remaining pivot columns [k0+nb, npiv), rows >= column.
 __global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0, int32_t k0,
                                                         double* __restrict__ fac) {
@@ -593,8 +620,9 @@ __global__ void __launch_bounds__(tc::kThreads) k_tc_tile_test(double* C, int64_
 // triangle holds X and the strict upper triangle its transpose (X^T), which
 // is what the column-dot mat-vecs of the multiplier loop read and what the
 // off-diagonal blocks read their right operand from.  Two launches:
-//   k_trtri_diag:  X_JJ = L_JJ^-1 for every 64 x 64 diagonal block
-//                  (forward substitution, one thread per column);
+//   k_trtri_diag:  X_JJ = L_JJ^-1 for every 64 x 64 diagonal block, copied
+//                  from the inverse k_potrf_diag left above the diagonal of
+//                  each panel's diagonal block (diagonal 1 / L_jj);
 //   k_trtri_off:   one CTA per column block J (J-major order, so the longest
 //                  chains start first), row blocks I = J+1, J+2, ... in order:
 //                  X_IJ = -X_II (sum_{J<=K<I} L_IK X_KJ), the sum a 64-wide
@@ -604,18 +632,16 @@ __global__ void __launch_bounds__(tc::kThreads) k_tc_tile_test(double* C, int64_
 //                  X_II a second tile product from shared memory; X_IJ and
 //                  its transpose are stored through shared memory, coalesced.
 constexpr int kTB = 64;
-constexpr size_t kTrtriDiagSmem = sizeof(double) * 2 * kTB * (kTB + 1);
 constexpr size_t kTrtriOffSmem = sizeof(double) * 2 * kTB * kMmaPad;
 static_assert(kTB == kTile && sizeof(TileSmemMma) <= kTrtriOffSmem && (kGK * kTB) % kMmaThreads == 0,
               "staging of the triangular inverse");
 
-__global__ void __launch_bounds__(kTB) k_trtri_diag(int32_t n_mat, const int32_t* __restrict__ dim,
+__global__ void __launch_bounds__(256) k_trtri_diag(int32_t n_mat, const int32_t* __restrict__ dim,
                                                     const int64_t* __restrict__ l_off,
                                                     const int64_t* __restrict__ x_off,
                                                     const double* __restrict__ Lbase, double* __restrict__ Xbase) {
-  extern __shared__ double sm[];
-  double (*Ls)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm);
-  double (*Is)[kTB + 1] = reinterpret_cast<double (*)[kTB + 1]>(sm + kTB * (kTB + 1));
+  static_assert(kTB == kNB, "the diagonal blocks are the factorization's panels");
+  __shared__ double T[kTB][kTB + 1];  // T[r][c] = X_JJ(r, c), r >= c
   const int32_t m = blockIdx.x;
   if (m >= n_mat) return;
   const int32_t n = dim[m];
@@ -624,18 +650,16 @@ __global__ void __launch_bounds__(kTB) k_trtri_diag(int32_t n_mat, const int32_t
   const int32_t h = min(kTB, n - c0);
   const double* L = Lbase + l_off[m] + c0 + static_cast<int64_t>(c0) * n;
   double* X = Xbase + x_off[m] + c0 + static_cast<int64_t>(c0) * n;
-  const int c = threadIdx.x;
-  for (int q = 0; q < h; ++q) Ls[c][q] = (c < h && c >= q) ? L[c + static_cast<int64_t>(q) * n] : 0.0;
+  for (int e = threadIdx.x; e < h * h; e += blockDim.x) {
+    const int q = e / h, p = e - q * h;  // entry (p, q) of the block
+    if (p < q) T[q][p] = L[p + static_cast<int64_t>(q) * n];
+    else if (p == q) T[p][p] = 1.0 / L[p + static_cast<int64_t>(p) * n];
+  }
   __syncthreads();
-  if (c < h)  // column c of the inverse: rows above the diagonal come out zero
-    for (int r = 0; r < h; ++r) {
-      double v = r == c ? 1.0 : 0.0;
-      for (int q = 0; q < r; ++q) v -= Ls[r][q] * Is[q][c];
-      Is[r][c] = v / Ls[r][r];
-    }
-  __syncthreads();
-  if (c < h)  // thread c writes row c of every column: lower X, upper X^T
-    for (int q = 0; q < h; ++q) X[c + static_cast<int64_t>(q) * n] = c >= q ? Is[c][q] : Is[q][c];
+  for (int e = threadIdx.x; e < h * h; e += blockDim.x) {
+    const int q = e / h, p = e - q * h;
+    X[p + static_cast<int64_t>(q) * n] = p >= q ? T[p][q] : T[q][p];
+  }
 }
 
 __global__ void __launch_bounds__(kMmaThreads) k_trtri_off(int32_t n_mat, const int32_t* __restrict__ dim,
@@ -2024,8 +2048,8 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
     k_potrf_diag<<<active, 256, 0, st>>>(fd, f0, k0, fac_d, diag0_d, d_loc_off, F, err_d);
     const int32_t rows = mf - k0 - 1;
     if (rows > 0) {
-      const unsigned rb = static_cast<unsigned>((rows + kTrsmRows - 1) / kTrsmRows);
-      k_trsm_panel<<<dim3(rb, active), kTrsmRows, kTrsmSmem, st>>>(fd, f0, k0, fac_d);
+      const unsigned rb = static_cast<unsigned>((rows + kTile - 1) / kTile);
+      k_trsm_panel<<<dim3(rb, active), kMmaThreads, kTrsmSmem, st>>>(fd, f0, k0, fac_d);
     }
     const int32_t c0 = k0 + kNB;
     if (c0 < mnp && tc_here) {
@@ -2050,21 +2074,19 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
 }
 
 // X = L^-1 for n_mat lower factors stored in fac_d, in full (X below the
-// diagonal, X^T above it).  The shared-memory limits are per-device
-// attributes of the kernels: set them on every call (cheap), so a solve on
-// another device or thread launches with them too.
+// diagonal, X^T above it).  The factors come from factor_range, whose
+// k_potrf_diag left each 64 x 64 diagonal block's inverse above its
+// diagonal.  The shared-memory limit is a per-device attribute of the
+// kernel: set it on every call (cheap), so a solve on another device or
+// thread launches with it too.
 int FetiDP::trtri(int32_t n_mat, int32_t max_n, const int32_t* dim, const int64_t* l_off, const int64_t* x_off,
                   double* X) {
   if (n_mat == 0 || max_n == 0) return EMG_SUCCESS;
-  if (!capturing) {
-    EMG_CK(cudaFuncSetAttribute(k_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kTrtriDiagSmem)));
+  if (!capturing)
     EMG_CK(cudaFuncSetAttribute(k_trtri_off, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kTrtriOffSmem)));
-  }
   const unsigned nb = static_cast<unsigned>((max_n + kTB - 1) / kTB);
-  k_trtri_diag<<<dim3(static_cast<unsigned>(n_mat), nb), kTB, kTrtriDiagSmem, st>>>(n_mat, dim, l_off, x_off, fac_d,
-                                                                                   X);
+  k_trtri_diag<<<dim3(static_cast<unsigned>(n_mat), nb), 256, 0, st>>>(n_mat, dim, l_off, x_off, fac_d, X);
   if (nb > 1)
     k_trtri_off<<<dim3(static_cast<unsigned>(n_mat), nb - 1), kMmaThreads, kTrtriOffSmem, st>>>(n_mat, dim, l_off,
                                                                                                  x_off, fac_d, X);
