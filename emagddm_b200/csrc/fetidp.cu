@@ -54,17 +54,28 @@ enum : int32_t { kErrPivot = 1, kErrAsm = 2, kErrTc = 4 };
 
 // ---------------------------------------------------------------- assembly
 
-__global__ void k_front_zero(FrontsDev F, int32_t f0, double* __restrict__ fac, double* __restrict__ upd) {
+// Zero every level front before its assembly: the f x npiv factor block,
+// and of the nu x nu update block the 128 x 128 tiles on and below the
+// diagonal -- all that the update (U -= L21 L21^T on lower tiles of 64 or,
+// on the TF32 path, 128) and the parent's extend-add (entries i >= j) read.
+// The factor block is one contiguous span; the update block a warp per
+// column.
+constexpr int kZeroTile = 128;
+__global__ void __launch_bounds__(256) k_front_zero(FrontsDev F, int32_t f0, double* __restrict__ fac,
+                                                    double* __restrict__ upd) {
   const int32_t k = f0 + blockIdx.y;
   const int64_t n1 = static_cast<int64_t>(F.f[k]) * F.npiv[k];
-  const int64_t nu = F.f[k] - F.npiv[k];
-  const int64_t n2 = nu * nu;
+  const int32_t nu = F.f[k] - F.npiv[k];
   double* a = fac + F.fac[k];
-  double* b = n2 > 0 ? upd + F.upd[k] : nullptr;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n1 + n2;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (i < n1) a[i] = 0.0;
-    else b[i - n1] = 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n1; i += stride) a[i] = 0.0;
+  if (nu == 0) return;
+  double* b = upd + F.upd[k];
+  const int lane = threadIdx.x & 31;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < nu; j += nw) {
+    double* bj = b + static_cast<int64_t>(j) * nu;
+    for (int32_t i = (j / kZeroTile) * kZeroTile + lane; i < nu; i += 32) bj[i] = 0.0;
   }
 }
 
@@ -109,9 +120,10 @@ __global__ void k_front_scatter(FrontsDev F, int32_t f0, const int64_t* __restri
 // Extend-add of every level front's `slot`-th child update block (lower part)
 // into the front: columns left of npiv go to the factor block, the rest to the
 // front's own update block.  One child per front per launch, so no two
-// threads add into the same entry.
-__global__ void k_extend_add(FrontsDev F, int32_t f0, int32_t slot, double* __restrict__ fac,
-                             double* __restrict__ upd) {
+// threads add into the same entry; a warp per child column j, its lanes
+// over the rows i >= j (contiguous in the child, ascending in the parent).
+__global__ void __launch_bounds__(256) k_extend_add(FrontsDev F, int32_t f0, int32_t slot, double* __restrict__ fac,
+                                                    double* __restrict__ upd) {
   const int32_t k = f0 + blockIdx.y;
   if (slot >= F.nchild[k]) return;
   const int32_t c = F.child_v[F.child0[k] + slot];
@@ -121,15 +133,18 @@ __global__ void k_extend_add(FrontsDev F, int32_t f0, int32_t slot, double* __re
   const int32_t* cp = F.cpos_v + F.cpos[c];
   double* A = fac + F.fac[k];
   double* B = nup > 0 ? upd + F.upd[k] : nullptr;
-  const int64_t tot = static_cast<int64_t>(nc) * nc;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t j = static_cast<int32_t>(e / nc), i = static_cast<int32_t>(e - static_cast<int64_t>(j) * nc);
-    if (i < j) continue;
-    const int32_t ri = cp[i], rj = cp[j];
-    const double v = U[e];
-    if (rj < np) A[ri + static_cast<int64_t>(rj) * fp] += v;
-    else B[(ri - np) + static_cast<int64_t>(rj - np) * nup] += v;
+  const int lane = threadIdx.x & 31;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (int32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < nc; j += nw) {
+    const int32_t rj = cp[j];
+    const double* Uj = U + static_cast<int64_t>(j) * nc;
+    if (rj < np) {
+      double* Aj = A + static_cast<int64_t>(rj) * fp;
+      for (int32_t i = j + lane; i < nc; i += 32) Aj[cp[i]] += Uj[i];
+    } else {
+      double* Bj = B + static_cast<int64_t>(rj - np) * nup;
+      for (int32_t i = j + lane; i < nc; i += 32) Bj[cp[i] - np] += Uj[i];
+    }
   }
 }
 
@@ -2379,7 +2394,7 @@ int FetiDP::factor_device() {
     const unsigned nf = static_cast<unsigned>(f1 - f0);
     if (nf == 0) continue;
     int32_t max_np = 0, max_ch = 0, max_root = 0;
-    int64_t max_el = 0, max_cu = 0;
+    int64_t max_el = 0, max_cn = 0;
     for (int32_t k = f0; k < f1; ++k) {
       const FetiFront& x = P.fronts[k];
       const int64_t nu1 = x.f - x.npiv;
@@ -2389,14 +2404,14 @@ int FetiDP::factor_device() {
       max_el = std::max(max_el, static_cast<int64_t>(x.f) * x.npiv + nu1 * nu1);
       for (int32_t c = 0; c < x.nchild; ++c) {
         const FetiFront& y = P.fronts[P.child_list[x.child0 + c]];
-        max_cu = std::max(max_cu, static_cast<int64_t>(y.f - y.npiv) * (y.f - y.npiv));
+        max_cn = std::max(max_cn, static_cast<int64_t>(y.f - y.npiv));
       }
     }
-    k_front_zero<<<dim3(blocks_for(max_el, 256, 512), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
+    k_front_zero<<<dim3(blocks_for(max_el, 256 * 16, 512), nf), 256, 0, st>>>(fd, f0, fac_d, upd_d);
     k_front_scatter<<<dim3(static_cast<unsigned>((max_np + 7) / 8), nf), 256, 0, st>>>(
         fd, f0, d_loc_off, d_nI, d_nD, rp, cl, vl, fac_d, diag0_d, err_d);
     for (int32_t slot = 0; slot < max_ch; ++slot)
-      k_extend_add<<<dim3(blocks_for(max_cu, 256, 512), nf), 256, 0, st>>>(fd, f0, slot, fac_d, upd_d);
+      k_extend_add<<<dim3(blocks_for(max_cn, 8 * 4, 512), nf), 256, 0, st>>>(fd, f0, slot, fac_d, upd_d);
     if (max_root > 0)
       k_copy_roots<<<dim3(blocks_for(static_cast<int64_t>(max_root) * max_root, 256, 512), nf), 256, 0, st>>>(
           fd, f0, d_root_off, fac_d, S_d);
