@@ -40,6 +40,7 @@ namespace {
 #define EMG_FETI_NB 64
 #endif
 constexpr int kNB = EMG_FETI_NB;  // panel width of the partial Cholesky
+constexpr int kPivBlock = 4 * kNB;  // block of panels whose trailing columns are updated together
 constexpr int kTile = 64;     // output tile of the rank-k updates
 [[maybe_unused]] constexpr int kKC = 32;  // k-chunk of the FMA (non-tensor-core) rank-k updates
 constexpr double kMinInnerTol = 1e-12;  // floor of a pass's multiplier tolerance
@@ -172,6 +173,93 @@ __global__ void k_copy_roots(FrontsDev F, int32_t f0, const int64_t* __restrict_
 // problem leave round-off-sized pivots of either sign.
 constexpr double kPivRel = 1e-11;
 
+// A full 64-column diagonal block, 256 threads: thread (r, g) = (t & 63,
+// t >> 6) keeps row r's entries of the columns q = 4s + g (s = 0..15) in
+// registers.  Cholesky, column c in order: the pivot's owner takes the
+// square root (pivot test against d0, the matrix's own diagonal, when given),
+// the owners of column c divide by it and publish the column, every thread
+// subtracts l_rc l_qc from its entries -- two barriers a column, the same
+// operations in the same order as the shared-memory loop of partial panels.
+// Then the inverse X = L^-1 in the same registers, last column first:
+// X_jj = 1 / L_jj, X_rj = -(sum_{j<q<=r} X_rq L_qj) / L_jj, each thread
+// summing over its own columns q and the four partial sums added in fixed
+// order.  L goes to A's lower triangle, X's strict lower part transposed
+// into A's strict upper triangle (read by the panel TRSM and the inverse
+// factors).
+__device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t fs, const double* __restrict__ d0,
+                                              int32_t* __restrict__ err, double (*D)[kNB + 1]) {
+  static_assert(kNB == 64, "the register layout holds 64 columns in 4 groups of 16");
+  __shared__ double col[kNB];
+  __shared__ double part[4][kNB];
+  __shared__ double piv;
+  const int t = threadIdx.x, r = t & 63, g = t >> 6;
+  double d[16];
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const int q = 4 * s + g;
+    d[s] = q <= r ? A[r + static_cast<int64_t>(q) * fs] : 0.0;
+  }
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) {
+    if (g == (c & 3) && r == c) {
+      double v = d[c >> 2];
+      if (!(v > 0.0) || (d0 && !(v > kPivRel * fabs(d0[c])))) { atomicOr(err, kErrPivot); v = 1.0; }
+      v = sqrt(v);
+      d[c >> 2] = v;
+      piv = v;
+    }
+    __syncthreads();
+    if (g == (c & 3) && r > c) {
+      d[c >> 2] /= piv;
+      col[r] = d[c >> 2];
+    }
+    __syncthreads();
+    if (r > c) {
+      const double lr = col[r];
+#pragma unroll
+      for (int s = 0; s < 16; ++s) {
+        const int q = 4 * s + g;
+        if (q > c && q <= r) d[s] -= lr * col[q];
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const int q = 4 * s + g;
+    if (q <= r) {
+      A[r + static_cast<int64_t>(q) * fs] = d[s];
+      D[r][q] = d[s];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = kNB - 1; j >= 0; --j) {
+    double p = 0.0;
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+      const int q = 4 * s + g;
+      if (q > j && q <= r) p += d[s] * D[q][j];
+    }
+    part[g][r] = p;
+    __syncthreads();
+    if (g == (j & 3)) {
+      if (r > j) d[j >> 2] = -(part[0][r] + part[1][r] + part[2][r] + part[3][r]) / D[j][j];
+      else if (r == j) d[j >> 2] = 1.0 / D[j][j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const int q = 4 * s + g;
+    if (q < r) D[r][q] = d[s];
+  }
+  __syncthreads();
+  for (int e = t; e < kNB * kNB; e += blockDim.x) {
+    const int rr = e / kNB, c = e - rr * kNB;
+    if (c < rr) A[c + static_cast<int64_t>(rr) * fs] = D[rr][c];
+  }
+}
+
 // Diagonal block [k0, k0+nb) of every front in the range with npiv > k0.
 // diag0 (null for the coarse matrix and the face sums) holds the original
 // diagonal of the subdomain matrices in union numbering.
@@ -188,6 +276,10 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int
   const int64_t u0 = rel ? loc_off[F.sub[k]] + F.p0[k] + k0 : 0;
   const int32_t nb = min(kNB, np - k0), fs = F.f[k];
   double* A = fac + F.fac[k] + k0 + static_cast<int64_t>(k0) * fs;
+  if (nb == kNB) {
+    potrf_full_panel(A, fs, rel ? diag0 + u0 : nullptr, err, D);
+    return;
+  }
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     const int c = e / nb, r = e - c * nb;
     D[r][c] = r >= c ? A[r + static_cast<int64_t>(c) * fs] : 0.0;
@@ -512,9 +604,13 @@ __global__ void __launch_bounds__(kMmaThreads) k_trsm_panel(FrontsDev F, int32_t
   }
 }
 
-// Right-looking update of the remaining pivot columns [k0+nb, npiv), rows >= column.
-__global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0, int32_t k0,
-                                                        double* __restrict__ fac) {
+// Right-looking update of pivot columns [clo, min(chi, npiv)), rows >= column,
+// by the factored columns [ka, ka + kw) (clipped to npiv): after each
+// 64-column panel the rest of its 256-column block, after each block the
+// columns beyond it with K = 256 -- so the trailing columns are read and
+// written once per block instead of once per panel.
+__global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0, int32_t ka, int32_t kw,
+                                                        int32_t clo, int32_t chi, double* __restrict__ fac) {
 #if EMG_FETI_DMMA
   __shared__ TileSmemMma sm;
 #else
@@ -523,25 +619,25 @@ __global__ void __launch_bounds__(256) k_update_pivcols(FrontsDev F, int32_t f0,
 #endif
   const int32_t k = f0 + blockIdx.y;
   const int32_t np = F.npiv[k];
-  if (k0 >= np) return;
-  const int32_t nb = min(kNB, np - k0), fs = F.f[k];
-  const int32_t c0 = k0 + nb;
-  if (c0 >= np) return;
-  const int32_t nct = (np - c0 + kTile - 1) / kTile, nrt = (fs - c0 + kTile - 1) / kTile;
+  if (ka >= np) return;
+  const int32_t nb = min(kw, np - ka), fs = F.f[k];
+  const int32_t c0 = clo, c1 = min(chi, np);
+  if (c0 >= c1) return;
+  const int32_t nct = (c1 - c0 + kTile - 1) / kTile, nrt = (fs - c0 + kTile - 1) / kTile;
   const int32_t t = blockIdx.x;
   if (t >= nct * nrt) return;
   const int32_t tc = t % nct, tr = t / nct;
   const int32_t cs = c0 + tc * kTile, rs = c0 + tr * kTile;
   if (rs + kTile <= cs) return;  // strictly above the diagonal
-  const int mc = min(kTile, np - cs), mr = min(kTile, fs - rs);
+  const int mc = min(kTile, c1 - cs), mr = min(kTile, fs - rs);
   double* A = fac + F.fac[k];
 #if EMG_FETI_DMMA
   static_assert(kMmaThreads == 256, "k_update_pivcols runs 256 threads");
-  tile_update_mma(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
-                  A + cs + static_cast<int64_t>(k0) * fs, fs, nb, sm);
+  tile_update_mma(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(ka) * fs, fs,
+                  A + cs + static_cast<int64_t>(ka) * fs, fs, nb, sm);
 #else
-  tile_update_wide(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(k0) * fs, fs,
-                   A + cs + static_cast<int64_t>(k0) * fs, fs, nb, As, Bs);
+  tile_update_wide(A + rs + static_cast<int64_t>(cs) * fs, fs, mr, mc, A + rs + static_cast<int64_t>(ka) * fs, fs,
+                   A + cs + static_cast<int64_t>(ka) * fs, fs, nb, As, Bs);
 #endif
 }
 
@@ -1399,29 +1495,45 @@ __global__ void __launch_bounds__(256) k_lambda_scatter(int64_t nl, const int32_
   }
 }
 
-// t[P] = add[P] + sum over the primal entries (s, p) of coarse DOF P of Phi_D[:, p] . w_s
-__global__ void k_coarse_apply_t(int32_t nc, const int64_t* __restrict__ coarse_ptr,
-                                 const int32_t* __restrict__ coarse_list, const int32_t* __restrict__ pri_sub,
-                                 const int64_t* __restrict__ pri_off, const int32_t* __restrict__ nI,
-                                 const int32_t* __restrict__ nD, const int64_t* __restrict__ dual_off, RhsDev R,
-                                 const double* __restrict__ w, const double* __restrict__ add,
-                                 double* __restrict__ t) {
-  const int32_t P = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (P >= nc) return;
-  const int lane = threadIdx.x & 31;
-  double tot = 0.0;
-  for (int64_t q = coarse_ptr[P]; q < coarse_ptr[P + 1]; ++q) {
-    const int32_t e = coarse_list[q];
-    const int32_t s = pri_sub[e];
-    const int32_t p = static_cast<int32_t>(e - pri_off[s]);
-    const int32_t nr = nI[s] + nD[s];
-    const double* phi = R.x + R.off[s] + static_cast<int64_t>(p) * nr + nI[s];
-    const double* ws = w + dual_off[s];
-    double acc = 0.0;
-    for (int32_t i = lane; i < nD[s]; i += 32) acc = fma(phi[i], ws[i], acc);
-    tot += warp_sum(acc);
+// t_P = add_P + sum over the primal entries q = (s, p) of coarse DOF P of
+// Phi_D(s)[:, p] . w_s.  k_coarse_dots: one CTA per entry forms its dot
+// product (fixed reduction order); k_coarse_sum: one thread per coarse DOF
+// adds its entries in list order.  (A warp per coarse DOF running its
+// entries in sequence left the GPU nearly idle: 81 warps at 64^3.)
+__global__ void __launch_bounds__(256) k_coarse_dots(const int32_t* __restrict__ coarse_list,
+                                                     const int32_t* __restrict__ pri_sub,
+                                                     const int64_t* __restrict__ pri_off,
+                                                     const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
+                                                     const int64_t* __restrict__ dual_off, RhsDev R,
+                                                     const double* __restrict__ w, double* __restrict__ dots) {
+  __shared__ double part[8];
+  const int64_t q = blockIdx.x;
+  const int32_t e = coarse_list[q];
+  const int32_t s = pri_sub[e];
+  const int32_t p = static_cast<int32_t>(e - pri_off[s]);
+  const int32_t nr = nI[s] + nD[s];
+  const double* phi = R.x + R.off[s] + static_cast<int64_t>(p) * nr + nI[s];
+  const double* ws = w + dual_off[s];
+  double acc = 0.0;
+  for (int32_t i = threadIdx.x; i < nD[s]; i += 256) acc = fma(phi[i], ws[i], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tot += part[k];
+    dots[q] = tot;
   }
-  if (lane == 0) t[P] = (add ? add[P] : 0.0) + tot;
+}
+
+__global__ void k_coarse_sum(int32_t nc, const int64_t* __restrict__ coarse_ptr, const double* __restrict__ dots,
+                             const double* __restrict__ add, double* __restrict__ t) {
+  const int32_t P = blockIdx.x * blockDim.x + threadIdx.x;
+  if (P >= nc) return;
+  double tot = 0.0;
+  for (int64_t q = coarse_ptr[P]; q < coarse_ptr[P + 1]; ++q) tot += dots[q];
+  t[P] = (add ? add[P] : 0.0) + tot;
 }
 
 // y[e] = base + scale * sum_p Phi_D[i, p] u[coarse(s, p)] for every dual entry
@@ -1975,6 +2087,7 @@ int FetiDP::setup_device() {
       (rc = zalloc(&v1_d, P.vec_rows)) || (rc = zalloc(&cblk_d, P.cblk_off[S])) ||
       (rc = zalloc(&h_d, P.pri_off[S])) || (rc = zalloc(&gc_d, nc)) || (rc = zalloc(&uc_d, nc)) ||
       (rc = zalloc(&t_d, nc)) || (rc = zalloc(&t2_d, nc)) || (rc = zalloc(&rho_d, nd)) ||
+      (rc = zalloc(&cdots_d, std::max<int64_t>(P.coarse_ptr[P.n_coarse], 1))) ||
       (rc = zalloc(&diag0_d, P.n_union)) ||
       (rc = zalloc(&wt_d, nd)) || (rc = zalloc(&w_d, nd)) || (rc = zalloc(&y_d, nd)) || (rc = zalloc(&y2_d, nd)) ||
       (rc = zalloc(&xu_d, P.n_union)) || (rc = zalloc(&ru_d, P.n_union)) || (rc = zalloc(&xg_d, P.n_dofs)) ||
@@ -2072,8 +2185,19 @@ int FetiDP::factor_range(int32_t f0, int32_t f1) {
       k_update_pivcols_tc<<<dim3(static_cast<unsigned>(nct * nrt), active), tc::kThreads, tc::kSmemBytes, st>>>(
           fd, f0, k0, fac_d, err_d);
     } else if (c0 < mnp) {
-      const int32_t nct = (mnp - c0 + kTile - 1) / kTile, nrt = (mf - c0 + kTile - 1) / kTile;
-      k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), active), 256, 0, st>>>(fd, f0, k0, fac_d);
+      // the rest of this panel's block, then (after its last panel) the columns beyond the block
+      const int32_t b0 = (k0 / kPivBlock) * kPivBlock, b1 = b0 + kPivBlock;
+      const int32_t c1 = std::min(b1, mnp);
+      if (c0 < c1) {
+        const int32_t nct = (c1 - c0 + kTile - 1) / kTile, nrt = (mf - c0 + kTile - 1) / kTile;
+        k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), active), 256, 0, st>>>(fd, f0, k0, kNB, c0, b1,
+                                                                                          fac_d);
+      }
+      if (c0 == b1 && b1 < mnp) {
+        const int32_t nct = (mnp - b1 + kTile - 1) / kTile, nrt = (mf - b1 + kTile - 1) / kTile;
+        k_update_pivcols<<<dim3(static_cast<unsigned>(nct * nrt), active), 256, 0, st>>>(fd, f0, b0, kPivBlock, b1,
+                                                                                          INT32_MAX, fac_d);
+      }
     }
   }
   if (max_nu > 0 && tc_here) {
@@ -2187,6 +2311,15 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   return EMG_SUCCESS;
 }
 
+// t = add + Phi_D^T w gathered per coarse DOF (k_coarse_dots, k_coarse_sum).
+void FetiDP::coarse_apply_t(const RhsDev& R, const double* w, const double* add, double* t) {
+  const int64_t nq = plan.coarse_ptr[plan.n_coarse];
+  if (nq > 0)
+    k_coarse_dots<<<static_cast<unsigned>(nq), 256, 0, st>>>(d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD,
+                                                              d_dual_off, R, w, cdots_d);
+  k_coarse_sum<<<blocks_for(plan.n_coarse, 128), 128, 0, st>>>(plan.n_coarse, d_coarse_ptr, cdots_d, add, t);
+}
+
 // u = S_cc^-1 t = L^-T (L^-1 t)
 void FetiDP::coarse_solve(const double* t, double* u) {
   const int32_t nc = plan.n_coarse;
@@ -2206,8 +2339,7 @@ void FetiDP::apply_F(const double* p, double* q, double* part) {
   k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, w_d, y2_d, 0);
   k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, Linv_d, d_rvoff, y2_d, y_d, 1);
   if (P.n_coarse > 0) {
-    k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
-        P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, nullptr, t_d);
+    coarse_apply_t(R, w_d, nullptr, t_d);
     coarse_solve(t_d, uc_d);
     k_dual_add_phi<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_sub, d_dual_off, d_nI, d_nD, d_nP, d_pri_off,
                                                          d_pri_coarse, R, uc_d, y_d, 1.0, y_d);
@@ -2747,8 +2879,7 @@ int FetiDP::recover(const double* fu) {
   if (P.n_coarse > 0) {
     if (ne > 0) k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, nullptr, lam_d, w_d);
     else EMG_CK(cudaMemsetAsync(w_d, 0, sizeof(double), st));
-    k_coarse_apply_t<<<static_cast<unsigned>((P.n_coarse + 7) / 8), 256, 0, st>>>(
-        P.n_coarse, d_coarse_ptr, d_coarse_list, d_pri_sub, d_pri_off, d_nI, d_nD, d_dual_off, R, w_d, gc_d, t_d);
+    coarse_apply_t(R, w_d, gc_d, t_d);
     coarse_solve(t_d, uc_d);
   }
   k_recover_rhs<<<dim3(64, static_cast<unsigned>(S)), 256, 0, st>>>(

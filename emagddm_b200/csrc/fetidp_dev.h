@@ -116,6 +116,7 @@ struct FetiDP {
   double *fac_d = nullptr, *upd_d = nullptr, *S_d = nullptr, *Linv_d = nullptr, *Lcc_d = nullptr;
   double *phi_d = nullptr, *vs_d = nullptr, *v1_d = nullptr, *cblk_d = nullptr, *h_d = nullptr;
   double *gc_d = nullptr, *uc_d = nullptr, *t_d = nullptr, *t2_d = nullptr;
+  double* cdots_d = nullptr;  // per primal entry of each coarse DOF: its Phi_D column dot
   double *rho_d = nullptr, *wt_d = nullptr, *w_d = nullptr, *y_d = nullptr, *y2_d = nullptr;
   double *xu_d = nullptr, *ru_d = nullptr, *xg_d = nullptr, *rg_d = nullptr, *bg_d = nullptr;
   double *lam_d = nullptr, *r_d = nullptr, *z_d = nullptr, *p_d = nullptr, *q_d = nullptr, *rhs_d = nullptr;
@@ -168,6 +169,7 @@ struct FetiDP {
   int factor_device();
   int solve_fronts(const RhsDev& R, int32_t ncol);
   void coarse_solve(const double* t, double* u);
+  void coarse_apply_t(const RhsDev& R, const double* w, const double* add, double* t);
   void apply_F(const double* p, double* q, double* part);
   void apply_M(const double* r, double* z, double* part);
   int dot(const double* a, const double* b, int64_t n, int which);
