@@ -173,21 +173,22 @@ __global__ void k_copy_roots(FrontsDev F, int32_t f0, const int64_t* __restrict_
 // problem leave round-off-sized pivots of either sign.
 constexpr double kPivRel = 1e-11;
 
-// A full 64-column diagonal block, 256 threads: thread (r, g) = (t & 63,
-// t >> 6) keeps row r's entries of the columns q = 4s + g (s = 0..15) in
-// registers.  Cholesky, column c in order: the pivot's owner takes the
-// square root (pivot test against d0, the matrix's own diagonal, when given),
-// the owners of column c divide by it and publish the column, every thread
-// subtracts l_rc l_qc from its entries -- two barriers a column, the same
-// operations in the same order as the shared-memory loop of partial panels.
-// Then the inverse X = L^-1 in the same registers, last column first:
-// X_jj = 1 / L_jj, X_rj = -(sum_{j<q<=r} X_rq L_qj) / L_jj, each thread
-// summing over its own columns q and the four partial sums added in fixed
-// order.  L goes to A's lower triangle, X's strict lower part transposed
-// into A's strict upper triangle (read by the panel TRSM and the inverse
-// factors).
-__device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t fs, const double* __restrict__ d0,
-                                              int32_t* __restrict__ err, double (*D)[kNB + 1]) {
+// The diagonal block (nb <= 64 columns; a narrower last panel is padded with
+// identity rows and columns, which leave the real entries unchanged), 256
+// threads: thread (r, g) = (t & 63, t >> 6) keeps row r's entries of the
+// columns q = 4s + g (s = 0..15) in registers.  Cholesky, column c in order:
+// the pivot's owner takes the square root (pivot test against d0, the
+// matrix's own diagonal, when given), the owners of column c divide by it
+// and publish the column, every thread subtracts l_rc l_qc from its entries
+// -- two barriers a column.  Then the inverse X = L^-1 in the same
+// registers, last column first: X_jj = 1 / L_jj, X_rj = -(sum_{j<q<=r}
+// X_rq L_qj) / L_jj, each thread summing over its own columns q and the
+// four partial sums added in fixed order.  L goes to A's lower triangle, X's
+// strict lower part transposed into A's strict upper triangle (read by the
+// panel TRSM and the inverse factors).
+__device__ __forceinline__ void potrf_panel(double* __restrict__ A, int32_t fs, int32_t nb,
+                                            const double* __restrict__ d0, int32_t* __restrict__ err,
+                                            double (*D)[kNB + 1]) {
   static_assert(kNB == 64, "the register layout holds 64 columns in 4 groups of 16");
   __shared__ double col[kNB];
   __shared__ double part[4][kNB];
@@ -197,13 +198,13 @@ __device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t
 #pragma unroll
   for (int s = 0; s < 16; ++s) {
     const int q = 4 * s + g;
-    d[s] = q <= r ? A[r + static_cast<int64_t>(q) * fs] : 0.0;
+    d[s] = r < nb ? (q <= r ? A[r + static_cast<int64_t>(q) * fs] : 0.0) : (q == r ? 1.0 : 0.0);
   }
 #pragma unroll
   for (int c = 0; c < kNB; ++c) {
     if (g == (c & 3) && r == c) {
       double v = d[c >> 2];
-      if (!(v > 0.0) || (d0 && !(v > kPivRel * fabs(d0[c])))) { atomicOr(err, kErrPivot); v = 1.0; }
+      if (c < nb && (!(v > 0.0) || (d0 && !(v > kPivRel * fabs(d0[c]))))) { atomicOr(err, kErrPivot); v = 1.0; }
       v = sqrt(v);
       d[c >> 2] = v;
       piv = v;
@@ -227,7 +228,7 @@ __device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t
   for (int s = 0; s < 16; ++s) {
     const int q = 4 * s + g;
     if (q <= r) {
-      A[r + static_cast<int64_t>(q) * fs] = d[s];
+      if (r < nb) A[r + static_cast<int64_t>(q) * fs] = d[s];
       D[r][q] = d[s];
     }
   }
@@ -254,8 +255,8 @@ __device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t
     if (q < r) D[r][q] = d[s];
   }
   __syncthreads();
-  for (int e = t; e < kNB * kNB; e += blockDim.x) {
-    const int rr = e / kNB, c = e - rr * kNB;
+  for (int e = t; e < nb * nb; e += blockDim.x) {
+    const int rr = e / nb, c = e - rr * nb;
     if (c < rr) A[c + static_cast<int64_t>(rr) * fs] = D[rr][c];
   }
 }
@@ -263,12 +264,11 @@ __device__ __forceinline__ void potrf_full_panel(double* __restrict__ A, int32_t
 // Diagonal block [k0, k0+nb) of every front in the range with npiv > k0.
 // diag0 (null for the coarse matrix and the face sums) holds the original
 // diagonal of the subdomain matrices in union numbering.
-__global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
+__global__ void __launch_bounds__(256, 1) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
                                                     const double* __restrict__ diag0,
                                                     const int64_t* __restrict__ loc_off, int32_t n_plan,
                                                     int32_t* __restrict__ err) {
   __shared__ double D[kNB][kNB + 1];
-  __shared__ double piv;
   const int32_t k = f0 + blockIdx.x;
   const int32_t np = F.npiv[k];
   if (k0 >= np) return;
@@ -276,57 +276,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int
   const int64_t u0 = rel ? loc_off[F.sub[k]] + F.p0[k] + k0 : 0;
   const int32_t nb = min(kNB, np - k0), fs = F.f[k];
   double* A = fac + F.fac[k] + k0 + static_cast<int64_t>(k0) * fs;
-  if (nb == kNB) {
-    potrf_full_panel(A, fs, rel ? diag0 + u0 : nullptr, err, D);
-    return;
-  }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int c = e / nb, r = e - c * nb;
-    D[r][c] = r >= c ? A[r + static_cast<int64_t>(c) * fs] : 0.0;
-  }
-  __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    if (threadIdx.x == 0) {
-      double d = D[c][c];
-      if (!(d > 0.0) || (rel && !(d > kPivRel * fabs(diag0[u0 + c])))) { atomicOr(err, kErrPivot); d = 1.0; }
-      piv = sqrt(d);
-      D[c][c] = piv;
-    }
-    __syncthreads();
-    for (int r = c + 1 + threadIdx.x; r < nb; r += blockDim.x) D[r][c] /= piv;
-    __syncthreads();
-    const int m = nb - c - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int q = c + 1 + e / m, r = c + 1 + e % m;
-      if (r >= q) D[r][q] -= D[r][c] * D[q][c];
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int c = e / nb, r = e - c * nb;
-    if (r >= c) A[r + static_cast<int64_t>(c) * fs] = D[r][c];
-  }
-  // The inverse X = L_kk^-1 in place, last column first: X_jj = 1 / L_jj,
-  // X_rj = -(sum_{j<q<=r} X_rq L_qj) / L_jj.  Its strict lower part goes,
-  // transposed, into the strict upper part of the diagonal block, which no
-  // other step reads; the panel TRSM and the inverse factors multiply by it
-  // (its diagonal they recompute from L_kk's).
-  for (int j = nb - 1; j >= 0; --j) {
-    const int r = j + 1 + static_cast<int>(threadIdx.x);
-    double v = 0.0;
-    if (r < nb) {
-      for (int q = j + 1; q <= r; ++q) v += D[r][q] * D[q][j];
-      v = -v / D[j][j];
-    }
-    __syncthreads();
-    if (r < nb) D[r][j] = v;
-    if (threadIdx.x == 0) D[j][j] = 1.0 / D[j][j];
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int r = e / nb, c = e - r * nb;
-    if (c < r) A[c + static_cast<int64_t>(r) * fs] = D[r][c];
-  }
+  potrf_panel(A, fs, nb, rel ? diag0 + u0 : nullptr, err, D);
 }
 
 // Asynchronous 8-byte global -> shared copy; `valid` false fills a zero
