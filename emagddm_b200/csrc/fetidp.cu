@@ -264,7 +264,7 @@ __device__ __forceinline__ void potrf_panel(double* __restrict__ A, int32_t fs, 
 // Diagonal block [k0, k0+nb) of every front in the range with npiv > k0.
 // diag0 (null for the coarse matrix and the face sums) holds the original
 // diagonal of the subdomain matrices in union numbering.
-__global__ void __launch_bounds__(256, 1) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
+__global__ void __launch_bounds__(256) k_potrf_diag(FrontsDev F, int32_t f0, int32_t k0, double* __restrict__ fac,
                                                     const double* __restrict__ diag0,
                                                     const int64_t* __restrict__ loc_off, int32_t n_plan,
                                                     int32_t* __restrict__ err) {
@@ -1230,33 +1230,52 @@ __global__ void k_root_gather(FrontsDev F, const int32_t* __restrict__ root_k, R
 // Root solve x_D = L^-T (L^-1 x_D) with the stored inverse M (M = L^-1 in
 // the lower triangle, its transpose in the upper): pass 0 tmp = L^-1 x_D
 // (column c, rows <= c), pass 1 x_D = L^-T tmp (column c, rows >= c).  One
-// warp per (root, column, row c).
+// warp per (root, column c of M, group of kC right-hand sides): M is read
+// once per group, each right-hand side accumulated in the same order.
+template <int kC>
 __global__ void __launch_bounds__(256) k_root_apply(const int32_t* __restrict__ root_sub, RhsDev R,
                                                     const int32_t* __restrict__ nI, const int32_t* __restrict__ nD,
                                                     const int64_t* __restrict__ root_off, const double* __restrict__ M,
                                                     const int64_t* __restrict__ rvoff, double* __restrict__ tmp,
                                                     int32_t max_ncol, int pass) {
-  const int32_t r = blockIdx.y / max_ncol, col = blockIdx.y - r * max_ncol;
+  const int32_t ng = (max_ncol + kC - 1) / kC;
+  const int32_t r = blockIdx.y / ng, grp = blockIdx.y - r * ng;
   const int32_t s = root_sub[r];
-  if (col >= R.ncol[s]) return;
+  const int32_t c0 = grp * kC, nc = min(kC, R.ncol[s] - c0);
+  if (nc <= 0) return;
   const int32_t n = nD[s];
   const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (c >= n) return;
   const int lane = threadIdx.x & 31;
   const int32_t ld = nI[s] + n;
-  double* xd = R.x + R.off[s] + static_cast<int64_t>(col) * ld + nI[s];
-  double* t = tmp + rvoff[r] * max_ncol + static_cast<int64_t>(col) * n;
+  double* xd = R.x + R.off[s] + static_cast<int64_t>(c0) * ld + nI[s];
+  double* t = tmp + rvoff[r] * max_ncol + static_cast<int64_t>(c0) * n;
   const double* Mc = M + root_off[s] + static_cast<int64_t>(c) * n;
-  double acc = 0.0;
+  double acc[kC];
+#pragma unroll
+  for (int q = 0; q < kC; ++q) acc[q] = 0.0;
   if (pass == 0) {
-    for (int32_t i = lane; i <= c; i += 32) acc = fma(Mc[i], xd[i], acc);
+    for (int32_t i = lane; i <= c; i += 32) {
+      const double m = Mc[i];
+#pragma unroll
+      for (int q = 0; q < kC; ++q)
+        if (q < nc) acc[q] = fma(m, xd[static_cast<int64_t>(q) * ld + i], acc[q]);
+    }
   } else {
-    for (int32_t i = c + lane; i < n; i += 32) acc = fma(Mc[i], t[i], acc);
+    for (int32_t i = c + lane; i < n; i += 32) {
+      const double m = Mc[i];
+#pragma unroll
+      for (int q = 0; q < kC; ++q)
+        if (q < nc) acc[q] = fma(m, t[static_cast<int64_t>(q) * n + i], acc[q]);
+    }
   }
-  acc = warp_sum(acc);
-  if (lane == 0) {
-    if (pass == 0) t[c] = acc;
-    else xd[c] = acc;
+#pragma unroll
+  for (int q = 0; q < kC; ++q) {
+    const double v = warp_sum(acc[q]);
+    if (lane == 0 && q < nc) {
+      if (pass == 0) t[static_cast<int64_t>(q) * n + c] = v;
+      else xd[static_cast<int64_t>(q) * ld + c] = v;
+    }
   }
 }
 
@@ -2230,14 +2249,17 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
                         upd_rows, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
   }
   if (n_roots > 0) {
-    const unsigned rc = static_cast<unsigned>(n_roots * ncol);
     k_root_gather<<<dim3(static_cast<unsigned>(ncol), static_cast<unsigned>(n_roots)), 256, 0, st>>>(fd, d_root_k, R,
                                                                                                      d_nI, d_nD);
     const unsigned gx = static_cast<unsigned>((max_nD + 7) / 8);
-    k_root_apply<<<dim3(gx, rc), 256, 0, st>>>(d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d,
-                                               ncol, 0);
-    k_root_apply<<<dim3(gx, rc), 256, 0, st>>>(d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d,
-                                               ncol, 1);
+    for (int pass = 0; pass < 2; ++pass) {
+      if (ncol == 1)
+        k_root_apply<1><<<dim3(gx, static_cast<unsigned>(n_roots)), 256, 0, st>>>(
+            d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d, ncol, pass);
+      else
+        k_root_apply<kColB><<<dim3(gx, static_cast<unsigned>(n_roots) * ngroups), 256, 0, st>>>(
+            d_root_sub, R, d_nI, d_nD, d_root_off, Linv_d, d_rvoff, root_tmp_d, ncol, pass);
+    }
   }
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
