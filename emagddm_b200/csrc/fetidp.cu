@@ -174,88 +174,67 @@ __global__ void k_copy_roots(FrontsDev F, int32_t f0, const int64_t* __restrict_
 constexpr double kPivRel = 1e-11;
 
 // The diagonal block (nb <= 64 columns; a narrower last panel is padded with
-// identity rows and columns, which leave the real entries unchanged), 256
-// threads: thread (r, g) = (t & 63, t >> 6) keeps row r's entries of the
-// columns q = 4s + g (s = 0..15) in registers.  Cholesky, column c in order:
-// the pivot's owner takes the square root (pivot test against d0, the
-// matrix's own diagonal, when given), the owners of column c divide by it
-// and publish the column, every thread subtracts l_rc l_qc from its entries
-// -- two barriers a column.  Then the inverse X = L^-1 in the same
-// registers, last column first: X_jj = 1 / L_jj, X_rj = -(sum_{j<q<=r}
-// X_rq L_qj) / L_jj, each thread summing over its own columns q and the
-// four partial sums added in fixed order.  L goes to A's lower triangle, X's
+// identity rows and columns, which leave the real entries unchanged) in
+// shared memory, 256 threads, thread (r, g) = (t & 63, t >> 6) owning row r's
+// entries of the columns q = g + 4m.  Cholesky, column c in order (a
+// compact loop: the code stays in the instruction cache, which the fully
+// unrolled register version did not): the pivot's square root (pivot test
+// against d0, the matrix's own diagonal, when given), the column divided by
+// it, l_rc l_qc subtracted from the trailing entries -- three barriers a
+// column.  Then the inverse X = L^-1 in place, last column first: X_jj =
+// 1 / L_jj, X_rj = -(sum_{j<q<=r} X_rq L_qj) / L_jj, the four partial sums
+// of each row added in fixed order.  L goes to A's lower triangle, X's
 // strict lower part transposed into A's strict upper triangle (read by the
 // panel TRSM and the inverse factors).
 __device__ __forceinline__ void potrf_panel(double* __restrict__ A, int32_t fs, int32_t nb,
                                             const double* __restrict__ d0, int32_t* __restrict__ err,
                                             double (*D)[kNB + 1]) {
-  static_assert(kNB == 64, "the register layout holds 64 columns in 4 groups of 16");
-  __shared__ double col[kNB];
+  static_assert(kNB == 64, "the thread layout covers 64 rows in 4 column groups");
   __shared__ double part[4][kNB];
+  __shared__ double d0s[kNB];
   __shared__ double piv;
   const int t = threadIdx.x, r = t & 63, g = t >> 6;
-  double d[16];
-#pragma unroll
-  for (int s = 0; s < 16; ++s) {
-    const int q = 4 * s + g;
-    d[s] = r < nb ? (q <= r ? A[r + static_cast<int64_t>(q) * fs] : 0.0) : (q == r ? 1.0 : 0.0);
+  if (d0 && t < nb) d0s[t] = fabs(d0[t]);
+  for (int e = t; e < kNB * kNB; e += 256) {
+    const int c = e >> 6, rr = e & 63;
+    D[rr][c] = (rr < nb && c < nb) ? (rr >= c ? A[rr + static_cast<int64_t>(c) * fs] : 0.0) : (rr == c ? 1.0 : 0.0);
   }
-#pragma unroll
+  __syncthreads();
+#pragma unroll 1
   for (int c = 0; c < kNB; ++c) {
-    if (g == (c & 3) && r == c) {
-      double v = d[c >> 2];
-      if (c < nb && (!(v > 0.0) || (d0 && !(v > kPivRel * fabs(d0[c]))))) { atomicOr(err, kErrPivot); v = 1.0; }
+    if (t == 0) {
+      double v = D[c][c];
+      if (c < nb && (!(v > 0.0) || (d0 && !(v > kPivRel * d0s[c])))) { atomicOr(err, kErrPivot); v = 1.0; }
       v = sqrt(v);
-      d[c >> 2] = v;
+      D[c][c] = v;
       piv = v;
     }
     __syncthreads();
-    if (g == (c & 3) && r > c) {
-      d[c >> 2] /= piv;
-      col[r] = d[c >> 2];
-    }
+    if (g == 0 && r > c) D[r][c] /= piv;
     __syncthreads();
     if (r > c) {
-      const double lr = col[r];
-#pragma unroll
-      for (int s = 0; s < 16; ++s) {
-        const int q = 4 * s + g;
-        if (q > c && q <= r) d[s] -= lr * col[q];
-      }
+      const double lr = D[r][c];
+      for (int q = c + 1 + ((g - c - 1) & 3); q <= r; q += 4) D[r][q] -= lr * D[q][c];
     }
+    __syncthreads();
   }
-#pragma unroll
-  for (int s = 0; s < 16; ++s) {
-    const int q = 4 * s + g;
-    if (q <= r) {
-      if (r < nb) A[r + static_cast<int64_t>(q) * fs] = d[s];
-      D[r][q] = d[s];
-    }
+  for (int e = t; e < nb * nb; e += 256) {
+    const int c = e / nb, rr = e - c * nb;
+    if (rr >= c) A[rr + static_cast<int64_t>(c) * fs] = D[rr][c];
   }
-  __syncthreads();
-#pragma unroll
+#pragma unroll 1
   for (int j = kNB - 1; j >= 0; --j) {
+    const double ljj = D[j][j];
     double p = 0.0;
-#pragma unroll
-    for (int s = 0; s < 16; ++s) {
-      const int q = 4 * s + g;
-      if (q > j && q <= r) p += d[s] * D[q][j];
-    }
+    if (r > j)
+      for (int q = j + 1 + ((g - j - 1) & 3); q <= r; q += 4) p += D[r][q] * D[q][j];
     part[g][r] = p;
     __syncthreads();
-    if (g == (j & 3)) {
-      if (r > j) d[j >> 2] = -(part[0][r] + part[1][r] + part[2][r] + part[3][r]) / D[j][j];
-      else if (r == j) d[j >> 2] = 1.0 / D[j][j];
-    }
+    if (g == 0 && r > j) D[r][j] = -(part[0][r] + part[1][r] + part[2][r] + part[3][r]) / ljj;
+    if (t == 0) D[j][j] = 1.0 / ljj;
     __syncthreads();
   }
-#pragma unroll
-  for (int s = 0; s < 16; ++s) {
-    const int q = 4 * s + g;
-    if (q < r) D[r][q] = d[s];
-  }
-  __syncthreads();
-  for (int e = t; e < nb * nb; e += blockDim.x) {
+  for (int e = t; e < nb * nb; e += 256) {
     const int rr = e / nb, c = e - rr * nb;
     if (c < rr) A[c + static_cast<int64_t>(rr) * fs] = D[rr][c];
   }
