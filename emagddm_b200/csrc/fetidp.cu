@@ -1565,40 +1565,99 @@ __global__ void __launch_bounds__(kTileThreads) k_face_gemm_nt(FacesDev Fc, cons
 }
 
 // w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
-// as column dots over the stored transposes DT (one warp per i).
+// as column dots over the stored transposes DT (one warp per i, eight rows a
+// CTA).  The face's gathered vector is staged once per CTA in shared memory
+// (dynamic, the largest face's size, when that fits in 48 KB), so a row's
+// dot reads only its column.
+constexpr int32_t kFaceStaged = 6144;  // faces up to this size stage their vector (48 KB)
 template <class T>
+__device__ __forceinline__ double face_dot(const T* __restrict__ Dt, const double* __restrict__ v, int32_t n,
+                                           int lane) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // four loads in flight a lane
+  int32_t j = lane;
+  for (; j + 96 < n; j += 128) {
+    a0 = fma(static_cast<double>(Dt[j]), v[j], a0);
+    a1 = fma(static_cast<double>(Dt[j + 32]), v[j + 32], a1);
+    a2 = fma(static_cast<double>(Dt[j + 64]), v[j + 64], a2);
+    a3 = fma(static_cast<double>(Dt[j + 96]), v[j + 96], a3);
+  }
+  for (; j < n; j += 32) a0 = fma(static_cast<double>(Dt[j]), v[j], a0);
+  return warp_sum((a0 + a1) + (a2 + a3));
+}
+
+template <class T, bool kStaged>
 __global__ void __launch_bounds__(256) k_face_w(FacesDev Fc, const int32_t* __restrict__ lam_entry,
                                                 const T* __restrict__ DaT, const T* __restrict__ DbT,
                                                 const double* __restrict__ r, double* __restrict__ w) {
+  extern __shared__ double fv[];
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
-  const int32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i >= n) return;
-  const int lane = threadIdx.x & 31;
+  const int32_t i0 = blockIdx.x * (blockDim.x >> 5);
+  if (i0 >= n) return;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
+  const int32_t i = i0 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const T* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
-  double acc = 0.0;
-  for (int32_t j = lane; j < n; j += 32) acc = fma(static_cast<double>(Dt[j]), r[lam[j]], acc);
-  acc = warp_sum(acc);
+  double acc;
+  if (kStaged) {
+    for (int32_t j = threadIdx.x; j < n; j += blockDim.x) fv[j] = r[lam[j]];
+    __syncthreads();
+    if (i >= n) return;
+    acc = face_dot(Dt, fv, n, lane);
+  } else {
+    if (i >= n) return;
+    double a = 0.0;
+    for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(Dt[j]), r[lam[j]], a);
+    acc = warp_sum(a);
+  }
   if (lane == 0) w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
 }
 
-// c[e_i] = sum_j D[j, i] y[e_j] (column dot, one warp per i).
-template <class T>
+// c[e_i] = sum_j D[j, i] y[e_j] (column dot, one warp per i), the face's
+// gathered y staged as above.
+template <class T, bool kStaged>
 __global__ void __launch_bounds__(256) k_face_c(FacesDev Fc, const int32_t* __restrict__ lam_entry,
                                                 const T* __restrict__ Da, const T* __restrict__ Db,
                                                 const double* __restrict__ y, double* __restrict__ c) {
+  extern __shared__ double fv[];
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
-  const int32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i >= n) return;
-  const int lane = threadIdx.x & 31;
+  const int32_t i0 = blockIdx.x * (blockDim.x >> 5);
+  if (i0 >= n) return;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
+  const int32_t i = i0 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const T* D = (side ? Db : Da) + Fc.off[f] + static_cast<int64_t>(i) * n;
-  double acc = 0.0;
-  for (int32_t j = lane; j < n; j += 32) acc = fma(static_cast<double>(D[j]), y[lam_entry[2 * lam[j] + side]], acc);
-  acc = warp_sum(acc);
+  double acc;
+  if (kStaged) {
+    for (int32_t j = threadIdx.x; j < n; j += blockDim.x) fv[j] = y[lam_entry[2 * lam[j] + side]];
+    __syncthreads();
+    if (i >= n) return;
+    acc = face_dot(D, fv, n, lane);
+  } else {
+    if (i >= n) return;
+    double a = 0.0;
+    for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(D[j]), y[lam_entry[2 * lam[j] + side]], a);
+    acc = warp_sum(a);
+  }
   if (lane == 0) c[lam_entry[2 * lam[i] + side]] = acc;
+}
+
+template <class T>
+void launch_face_w(unsigned gx, unsigned nfs, int32_t max_fdim, cudaStream_t st, FacesDev fc, const int32_t* le,
+                   const T* a, const T* b, const double* r, double* w) {
+  if (max_fdim <= kFaceStaged)
+    k_face_w<T, true><<<dim3(gx, nfs), 256, sizeof(double) * max_fdim, st>>>(fc, le, a, b, r, w);
+  else
+    k_face_w<T, false><<<dim3(gx, nfs), 256, 0, st>>>(fc, le, a, b, r, w);
+}
+template <class T>
+void launch_face_c(unsigned gx, unsigned nfs, int32_t max_fdim, cudaStream_t st, FacesDev fc, const int32_t* le,
+                   const T* a, const T* b, const double* y, double* c) {
+  if (max_fdim <= kFaceStaged)
+    k_face_c<T, true><<<dim3(gx, nfs), 256, sizeof(double) * max_fdim, st>>>(fc, le, a, b, y, c);
+  else
+    k_face_c<T, false><<<dim3(gx, nfs), 256, 0, st>>>(fc, le, a, b, y, c);
 }
 
 // ------------------------------------------- arbitrary right-hand sides
@@ -2316,19 +2375,19 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
   if (precond >= 2 && P.n_faces > 0) {  // 4: the Dirichlet part of deluxe + learned
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
     if (precond == 3) {
-      k_face_w<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
-          fc, d_lam_entry, fDaT32_d, fDbT32_d, r, w_d);
+      launch_face_w<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDaT32_d,
+                           fDbT32_d, r, w_d);
       k_block_colgemv<float><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S32_d, d_rvoff, w_d, y_d, 2);
-      k_face_c<float><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(
-          fc, d_lam_entry, fDa32_d, fDb32_d, y_d, c_d);
+      launch_face_c<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa32_d,
+                           fDb32_d, y_d, c_d);
       k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
       return;
     }
-    k_face_w<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fX_d,
-                                                                                          fXt_d, r, w_d);
+    launch_face_w<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fX_d, fXt_d,
+                          r, w_d);
     k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
-    k_face_c<double><<<dim3(static_cast<unsigned>((max_fdim + 7) / 8), nfs), 256, 0, st>>>(fc, d_lam_entry, fDa_d, fDb_d,
-                                                                                  y_d, c_d);
+    launch_face_c<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa_d, fDb_d,
+                          y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
