@@ -65,6 +65,8 @@ def parse():
                     help="cube64 north-star comparison: training fields of the learned preconditioner")
     ap.add_argument("--ns-eval-fields", type=int, default=3,
                     help="cube64 north-star comparison: held-out fields of the learned preconditioner")
+    ap.add_argument("--ns-batch-instances", type=int, default=512,
+                    help="cube64 north-star comparison: instances of the batched many-instance run (0 skips it)")
     ap.add_argument("--feti-variants", default=",".join(["fp64", "fp32_precond", "tf32_factor"]),
                     help="cube64 north-star comparison: FETI-DP variants to time (comma-separated)")
     ap.add_argument("--mixed", action="store_true",
@@ -567,12 +569,15 @@ def cpu_baseline(args, m, l2g, n_dofs, iters, csys=None):
     return {"value": 1e3 / total_ms, "unit": "solves/s", **d}
 
 
-def run_batch(args, rank, world, local_rank):
+def batch_measure(n_inst, steps, warmup, local_rank, plain_stride, oracle_stride, clocks=None):
     """512 independent instances (n ~ U{8..32}, seed 7+i): one block-diagonal
-    system, lockstep Jacobi-PCG to 1e-8 in one device loop.  value = instance
-    solves per second (assembly + solve per step, inputs resident); also the
-    same instances solved one at a time through emg_system_solve (a sample,
-    projected) and the per-instance error of a sample against the oracle."""
+    system, lockstep Jacobi-PCG to 1e-8 in one device loop, `steps` timed
+    steps after `warmup` (assembly + solve per step, inputs resident), first
+    with the built-in launch configuration, then the autotuned one; the same
+    instances solved one at a time through emg_system_solve (every
+    `plain_stride`-th, projected) and the per-instance error of every
+    `oracle_stride`-th against the FP64 CPU oracle.  Returns (tuned ms per
+    step, config dict)."""
     import torch
 
     from emagddm_b200 import _abi, batch
@@ -581,7 +586,7 @@ def run_batch(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     t0 = time.perf_counter()
-    inst = batch.make_instances(args.instances)
+    inst = batch.make_instances(n_inst)
     b = batch.build_batch(inst)
     setup_ms = (time.perf_counter() - t0) * 1e3
     res_d = {k: torch.from_numpy(getattr(b, k)).to(dev) for k in ("xyz", "tets", "material", "l2g")}
@@ -599,26 +604,29 @@ def run_batch(args, rank, world, local_rank):
         del S
 
     def timed_steps():
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             step()
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / steps
 
     # the built-in launch configuration first (autotuner off), then the tuned one
     L.emg_tune_enable(0)
     ms_default = timed_steps()
     L.emg_tune_enable(1)
-    with Clocks(local_rank) as clk:
+    if clocks is not None:
+        with clocks:
+            ms = timed_steps()
+    else:
         ms = timed_steps()
     iters = [r["iterations"] for r in info["res"]]
     # plain path: the same instances one at a time (a sample, projected)
-    sample = list(range(0, len(inst), max(1, len(inst) // 16)))
+    sample = list(range(0, len(inst), plain_stride))
     t_plain = 0.0
     for k in sample:
         m = inst[k]
@@ -640,10 +648,10 @@ def run_batch(args, rank, world, local_rank):
         t_plain += time.perf_counter() - ta
     plain_per_inst_ms = t_plain / len(sample) * 1e3
     # per-instance error against the FP64 CPU oracle (its own assembly and a
-    # Jacobi-PCG solve to 1e-12) on every 16th instance: 32 of the 512
+    # Jacobi-PCG solve to 1e-12)
     xs_all = x.cpu().numpy()
     errs, t0 = [], time.perf_counter()
-    oracle_sample = list(range(0, len(inst), max(1, len(inst) // 32)))
+    oracle_sample = list(range(0, len(inst), oracle_stride))
     for k in oracle_sample:
         m = inst[k]
         r0, r1 = int(b.block_row_ptr[k]), int(b.block_row_ptr[k + 1])
@@ -651,26 +659,41 @@ def run_batch(args, rank, world, local_rank):
         xo, st, it, _ = O.pcg(orp, ocol, okv, orhs, tol=1e-12, max_iter=MAX_ITER, precond=1)
         errs.append(float(np.linalg.norm(xs_all[r0:r1] - xo) / max(np.linalg.norm(xo), 1e-300)))
     oracle_ms = (time.perf_counter() - t0) * 1e3
-    value = world * len(inst) / (ms * 1e-3)
+    value = len(inst) / (ms * 1e-3)
+    cfg = {"workload": f"batch{len(inst)}: n~U{{8..32}} cubes x 6 tets, random mu_r box, "
+                       f"J_z sub-box, ref tree gauge, Jacobi-PCG to 1e-8, one lockstep device loop",
+           "instances": len(inst), "rows": b.n_rows, "tets": int(b.tets.shape[0]),
+           "steps": steps, "warmup": warmup, "ms_per_step": ms, "solves_per_s": value,
+           "iterations_min_median_max": [min(iters), int(np.median(iters)), max(iters)],
+           "setup_ms": setup_ms,
+           "plain_one_at_a_time": {"ms_per_instance": plain_per_inst_ms,
+                                   "solves_per_s": 1e3 / plain_per_inst_ms,
+                                   "sample": len(sample)},
+           "batched_vs_plain": value / (1e3 / plain_per_inst_ms),
+           "oracle_rel_error_sample_max": max(errs), "oracle_rel_error_sample_median": float(np.median(errs)),
+           "oracle_sample": len(errs), "oracle_sample_instances": f"every {oracle_stride}th",
+           "oracle_ms": oracle_ms, "oracle_threads": O.num_threads(),
+           "autotune": {"ms_per_step_default": ms_default, "ms_per_step_tuned": ms,
+                        "tuned_vs_default": ms_default / ms}}
+    return ms, cfg
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batched many-instance workload as its own line (batch_measure);
+    value = instance solves per second over all ranks."""
+    from emagddm_b200 import _abi
+    clk = Clocks(local_rank)
+    ms, cfg = batch_measure(args.instances, args.steps, args.warmup, local_rank,
+                            plain_stride=max(1, args.instances // 16), oracle_stride=max(1, args.instances // 32),
+                            clocks=clk)
+    cfg["autotune"]["decisions"] = _abi.tune_report()
+    value = world * cfg["instances"] / (ms * 1e-3)
     return {
         "metric": METRIC + " [batched many-instance]", "value": value, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random instances, seed 7+i)",
-        "config": {"workload": f"batch{len(inst)}: n~U{{8..32}} cubes x 6 tets, random mu_r box, "
-                               f"J_z sub-box, ref tree gauge, Jacobi-PCG to 1e-8, one lockstep device loop",
-                   "instances": len(inst), "rows": b.n_rows, "tets": int(b.tets.shape[0]),
-                   "iterations_min_median_max": [min(iters), int(np.median(iters)), max(iters)],
-                   "setup_ms": setup_ms,
-                   "plain_one_at_a_time": {"ms_per_instance": plain_per_inst_ms,
-                                           "solves_per_s": 1e3 / plain_per_inst_ms,
-                                           "sample": len(sample)},
-                   "batched_vs_plain": value / world / (1e3 / plain_per_inst_ms),
-                   "oracle_rel_error_sample_max": max(errs), "oracle_rel_error_sample_median": float(np.median(errs)),
-                   "oracle_sample": len(errs), "oracle_sample_instances": "every 16th (0, 16, ..., 496)",
-                   "oracle_ms": oracle_ms, "oracle_threads": O.num_threads(),
-                   "autotune": {"decisions": _abi.tune_report(), "ms_per_step_default": ms_default,
-                                "ms_per_step_tuned": ms, "tuned_vs_default": ms_default / ms}},
+        "config": cfg,
         "clocks": clk.summary(),
     }
 
@@ -800,6 +823,11 @@ def north_star(args, local_rank):
     r = orhs - O.spmv(orp, ocol, okv, x_feti)
     del fd
     learned = north_star_learned(args, local_rank) if args.ns_train_fields > 0 else None
+    batched = None
+    if args.ns_batch_instances > 0:  # the batched many-instance addition, reduced to 2 timed steps
+        n_b = args.ns_batch_instances
+        _, batched = batch_measure(n_b, steps=2, warmup=1, local_rank=local_rank, plain_stride=max(1, n_b // 16),
+                                   oracle_stride=max(1, n_b // 16))
     plain_fetidp = var["fp64"]["ms"]
     plain_pcg = pcg[f"{TOL:g}"]["ms"]
     best = min(timed, key=lambda k: timed[k]["ms"])
@@ -809,6 +837,7 @@ def north_star(args, local_rank):
         "dofs": n_dofs, "n_lambda": info["n_lambda"], "n_coarse": info["n_coarse"],
         "setup_host_ms": setup_ms, "fetidp": var, "plain_pcg_same_gauge": pcg,
         "learned": learned,
+        "batched": batched,
         "combination": "mixed factor + learned + graph loop: not run, the mixed-precision factor does not converge "
                        "at 64^3 (fetidp.tf32_factor above)",
         "best": best, "best_ms": var[best]["ms"],
