@@ -1319,6 +1319,99 @@ __global__ void __launch_bounds__(512) k_block_colgemv(int32_t n_mat, const int3
   if (lane == 0) y[v_off[m] + c] = acc;
 }
 
+// y = S w for symmetric dense blocks S (the roots' S_DD, full column-major
+// storage), reading only the 64 x 64 tiles on and below the diagonal: half
+// the bytes of a full column-dot pass.  k_symv_rows: one CTA per block row
+// I, thread (r, cq) = (t & 63, t >> 6); for each tile S_IJ (J <= I) it adds
+// S_IJ w_J into row r over the columns of quarter cq (the row sums, four
+// partials added in fixed order at the end, are written to y) and, for
+// J < I, forms the column sums S_IJ^T w_I (a butterfly over the warp, two
+// halves in fixed order) into the tile's slot of pc.  k_symv_cols: y_J += the column sums of
+// the tiles below block J, in ascending I.  Deterministic.
+constexpr int kSy = 64;
+template <class T>
+__global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t* __restrict__ dim,
+                                                   const int64_t* __restrict__ m_off, const T* __restrict__ M,
+                                                   const int64_t* __restrict__ v_off, const int64_t* __restrict__ pc_off,
+                                                   const double* __restrict__ w, double* __restrict__ y,
+                                                   double* __restrict__ pc) {
+  __shared__ double rowp[4][kSy];
+  __shared__ double colp[2][kSy];
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m], nb = (n + kSy - 1) / kSy;
+  const int32_t I = blockIdx.x;
+  if (I >= nb) return;
+  const int t = threadIdx.x, r = t & 63, cq = t >> 6, lane = t & 31, half = (t >> 5) & 1;
+  const int32_t gr = I * kSy + r;
+  const bool live_r = gr < n;
+  const T* Mm = M + m_off[m];
+  const double* wm = w + v_off[m];
+  const double wr = live_r ? wm[gr] : 0.0;
+  double racc = 0.0;
+  for (int32_t J = 0; J <= I; ++J) {
+    double cacc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int32_t gc = J * kSy + 16 * cq + j;
+      const double v = (live_r && gc < n) ? static_cast<double>(Mm[gr + static_cast<int64_t>(gc) * n]) : 0.0;
+      racc = fma(v, gc < n ? wm[gc] : 0.0, racc);
+      cacc[j] = v * wr;
+    }
+    if (J < I) {
+      // the 16 column sums over the warp's 32 rows by a butterfly that halves
+      // the values at each exchange: 8 + 4 + 2 + 1 + 1 shuffles, after which
+      // lanes 2k and 2k + 1 hold column jc (fixed order, deterministic)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const bool up = lane & 16;
+        const double send = up ? cacc[i] : cacc[i + 8], keep = up ? cacc[i + 8] : cacc[i];
+        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const bool up = lane & 8;
+        const double send = up ? cacc[i] : cacc[i + 4], keep = up ? cacc[i + 4] : cacc[i];
+        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const bool up = lane & 4;
+        const double send = up ? cacc[i] : cacc[i + 2], keep = up ? cacc[i + 2] : cacc[i];
+        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+      }
+      {
+        const bool up = lane & 2;
+        const double send = up ? cacc[0] : cacc[1], keep = up ? cacc[1] : cacc[0];
+        cacc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+      }
+      cacc[0] += __shfl_xor_sync(0xffffffffu, cacc[0], 1);
+      const int jc = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+      if ((lane & 1) == 0) colp[half][16 * cq + jc] = cacc[0];
+      __syncthreads();
+      if (t < kSy) pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * kSy + t] = colp[0][t] + colp[1][t];
+      __syncthreads();
+    }
+  }
+  rowp[cq][r] = racc;
+  __syncthreads();
+  if (t < kSy && I * kSy + t < n)
+    y[v_off[m] + I * kSy + t] = (rowp[0][t] + rowp[1][t]) + (rowp[2][t] + rowp[3][t]);
+}
+
+__global__ void k_symv_cols(int32_t n_mat, const int32_t* __restrict__ dim, const int64_t* __restrict__ v_off,
+                            const int64_t* __restrict__ pc_off, const double* __restrict__ pc,
+                            double* __restrict__ y) {
+  const int32_t m = blockIdx.y;
+  if (m >= n_mat) return;
+  const int32_t n = dim[m], nb = (n + kSy - 1) / kSy;
+  const int32_t J = blockIdx.x, c = threadIdx.x;
+  if (J >= nb || J * kSy + c >= n) return;
+  double acc = 0.0;
+  for (int32_t I = J + 1; I < nb; ++I) acc += pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * kSy + c];
+  y[v_off[m] + J * kSy + c] += acc;
+}
+
 // ---------------------------------------------- right-hand sides, coarse
 
 // Setup right-hand sides of subdomain s: columns 0..nP-1 = K_rP, column nP = f_r.
@@ -2044,6 +2137,14 @@ int FetiDP::setup_device() {
       (rc = up(&d_rvoff, rvoff)) || (rc = up(&d_cdim, cdim)) || (rc = up(&d_cfac, cfac)) ||
       (rc = up(&d_czero, czero)))
     return rc;
+  {  // column-sum slots of the symmetric S_DD products: one per tile below the diagonal
+    std::vector<int64_t> pcoff(rdim.size() + 1, 0);
+    for (size_t q = 0; q < rdim.size(); ++q) {
+      const int64_t nb = (rdim[q] + kSy - 1) / kSy;
+      pcoff[q + 1] = pcoff[q] + nb * (nb - 1) / 2 * kSy;
+    }
+    if ((rc = up(&d_pcoff, pcoff)) || (rc = zalloc(&pc_d, std::max<int64_t>(pcoff.back(), 1)))) return rc;
+  }
   // setup solves: n_r x (nP + 1) per subdomain; recovery: one column in union layout
   std::vector<int64_t> roff_s(S), roff1(S);
   std::vector<int32_t> ncol_s(S), ncol1(S, 1);
@@ -2330,6 +2431,17 @@ void FetiDP::coarse_apply_t(const RhsDev& R, const double* w, const double* add,
   k_coarse_sum<<<blocks_for(plan.n_coarse, 128), 128, 0, st>>>(plan.n_coarse, d_coarse_ptr, cdots_d, add, t);
 }
 
+// y = S_DD w for every root, the lower tiles only (k_symv_rows, k_symv_cols).
+template <class T>
+void FetiDP::symv_roots(const T* M, const double* w, double* y) {
+  const unsigned nb = static_cast<unsigned>((max_nD + kSy - 1) / kSy);
+  k_symv_rows<T><<<dim3(nb, static_cast<unsigned>(n_roots)), 256, 0, st>>>(n_roots, d_rdim, d_roff, M, d_rvoff,
+                                                                           d_pcoff, w, y, pc_d);
+  k_symv_cols<<<dim3(nb, static_cast<unsigned>(n_roots)), kSy, 0, st>>>(n_roots, d_rdim, d_rvoff, d_pcoff, pc_d, y);
+}
+template void FetiDP::symv_roots<double>(const double*, const double*, double*);
+template void FetiDP::symv_roots<float>(const float*, const double*, double*);
+
 // u = S_cc^-1 t = L^-T (L^-1 t)
 void FetiDP::coarse_solve(const double* t, double* u) {
   const int32_t nc = plan.n_coarse;
@@ -2377,7 +2489,7 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     if (precond == 3) {
       launch_face_w<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDaT32_d,
                            fDbT32_d, r, w_d);
-      k_block_colgemv<float><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S32_d, d_rvoff, w_d, y_d, 2);
+      symv_roots(S32_d, w_d, y_d);
       launch_face_c<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa32_d,
                            fDb32_d, y_d, c_d);
       k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
@@ -2385,14 +2497,14 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
     }
     launch_face_w<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fX_d, fXt_d,
                           r, w_d);
-    k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+    symv_roots(S_d, w_d, y_d);
     launch_face_c<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa_d, fDb_d,
                           y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
   k_dual_gather<<<blocks_for(ne, 256), 256, 0, st>>>(ne, d_dual_lam, d_dual_sign, wt_d, r, w_d);
-  k_block_colgemv<double><<<gr, 32 * gemv_warps, 0, st>>>(n_roots, d_rdim, d_roff, S_d, d_rvoff, w_d, y_d, 2);
+  symv_roots(S_d, w_d, y_d);
   k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, wt_d, y_d, z, r, part);
 }
 

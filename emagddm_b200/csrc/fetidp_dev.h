@@ -100,6 +100,8 @@ struct FetiDP {
   int32_t* d_rdim = nullptr;
   int32_t *d_root_k = nullptr, *d_root_sub = nullptr;
   int64_t *d_rfac = nullptr, *d_roff = nullptr, *d_rvoff = nullptr;
+  int64_t* d_pcoff = nullptr;  // per root: offset of its column-sum slots in pc_d
+  double* pc_d = nullptr;       // column sums of the tiles below the diagonal (symmetric S_DD products)
   int32_t* d_cdim = nullptr;
   int64_t *d_cfac = nullptr, *d_czero = nullptr;
   int64_t coarse_fac = 0;
@@ -170,6 +172,8 @@ struct FetiDP {
   int solve_fronts(const RhsDev& R, int32_t ncol);
   void coarse_solve(const double* t, double* u);
   void coarse_apply_t(const RhsDev& R, const double* w, const double* add, double* t);
+  template <class T>
+  void symv_roots(const T* M, const double* w, double* y);
   void apply_F(const double* p, double* q, double* part);
   void apply_M(const double* r, double* z, double* part);
   int dot(const double* a, const double* b, int64_t n, int which);
