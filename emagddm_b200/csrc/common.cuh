@@ -16,6 +16,43 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Warp reduce-scatter of K values a lane (K a power of two, 1 <= K <= 32):
+// returns in every lane the warp sum of v[j] for j = reduce_scatter_index<K>
+// (lane).  Each halving exchange keeps half of the values (lanes with the
+// exchange's bit set keep the upper half), the rest are full exchanges: K - 1
+// + 5 - log2 K shuffles instead of the 5 K of K separate warp sums.  The
+// order of the additions is fixed, so the sums are deterministic; the lanes
+// whose low 5 - log2 K bits are zero hold distinct j.
+template <int K>
+__device__ __forceinline__ double warp_reduce_scatter(double (&v)[K], int lane) {
+  static_assert(K >= 1 && K <= 32 && (K & (K - 1)) == 0, "K must be a power of two up to 32");
+  int o = 16;
+#pragma unroll
+  for (int h = K / 2; h >= 1; h >>= 1, o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const double send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+#pragma unroll
+  for (; o >= 1; o >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+  return v[0];
+}
+template <int K>
+__device__ __forceinline__ int reduce_scatter_index(int lane) {
+  int j = 0, o = 16;
+#pragma unroll
+  for (int h = K / 2; h >= 1; h >>= 1, o >>= 1)
+    if (lane & o) j += h;
+  return j;
+}
+template <int K>
+__device__ __forceinline__ bool reduce_scatter_writer(int lane) {
+  return (lane & (32 / K - 1)) == 0;
+}
+
 // Deterministic block sum of one value per thread; result valid in every
 // thread.  `scratch` holds blockDim.x / 32 doubles.
 __device__ __forceinline__ double block_sum(double v, double* scratch) {

@@ -966,11 +966,9 @@ __global__ void __launch_bounds__(256) k_front_bwd_upd(FrontsDev F, int32_t f0, 
     for (int c = 0; c < kColB; ++c)
       if (c < nc) acc[c] = fma(l, x[static_cast<int64_t>(c) * ld + r], acc[c]);
   }
-#pragma unroll
-  for (int c = 0; c < kColB; ++c) {
-    const double a = warp_sum(acc[c]);
-    if (lane == 0 && c < nc) x[static_cast<int64_t>(c) * ld + p0 + j] -= a;
-  }
+  const double a = warp_reduce_scatter<kColB>(acc, lane);
+  const int c = reduce_scatter_index<kColB>(lane);
+  if (reduce_scatter_writer<kColB>(lane) && c < nc) x[static_cast<int64_t>(c) * ld + p0 + j] -= a;
 }
 
 // Backward, pivot block: per 32-pivot panel (last first) the warps form the
@@ -1162,11 +1160,9 @@ __global__ void __launch_bounds__(mid_threads<kC>()) k_front_bwd_mid(FrontsDev F
         for (int c = 0; c < kC; ++c)
           if (c < nc) acc[c] = fma(l, xs[c * ldx + i], acc[c]);
       }
-#pragma unroll
-      for (int c = 0; c < kC; ++c) {
-        const double a = warp_sum(acc[c]);
-        if (lane == 0 && c < nc) tb[c * kSB + j] = a;
-      }
+      const double a = warp_reduce_scatter<kC>(acc, lane);
+      const int c = reduce_scatter_index<kC>(lane);
+      if (reduce_scatter_writer<kC>(lane) && c < nc) tb[c * kSB + j] = a;
     }
     __syncthreads();
     for (int c = wid; c < nc; c += kT / 32) {
@@ -1248,13 +1244,11 @@ __global__ void __launch_bounds__(256) k_root_apply(const int32_t* __restrict__ 
         if (q < nc) acc[q] = fma(m, t[static_cast<int64_t>(q) * n + i], acc[q]);
     }
   }
-#pragma unroll
-  for (int q = 0; q < kC; ++q) {
-    const double v = warp_sum(acc[q]);
-    if (lane == 0 && q < nc) {
-      if (pass == 0) t[static_cast<int64_t>(q) * n + c] = v;
-      else xd[static_cast<int64_t>(q) * ld + c] = v;
-    }
+  const double v = warp_reduce_scatter<kC>(acc, lane);
+  const int q = reduce_scatter_index<kC>(lane);
+  if (reduce_scatter_writer<kC>(lane) && q < nc) {
+    if (pass == 0) t[static_cast<int64_t>(q) * n + c] = v;
+    else xd[static_cast<int64_t>(q) * ld + c] = v;
   }
 }
 
@@ -1359,35 +1353,10 @@ __global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t*
       cacc[j] = v * wr;
     }
     if (J < I) {
-      // the 16 column sums over the warp's 32 rows by a butterfly that halves
-      // the values at each exchange: 8 + 4 + 2 + 1 + 1 shuffles, after which
-      // lanes 2k and 2k + 1 hold column jc (fixed order, deterministic)
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const bool up = lane & 16;
-        const double send = up ? cacc[i] : cacc[i + 8], keep = up ? cacc[i + 8] : cacc[i];
-        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const bool up = lane & 8;
-        const double send = up ? cacc[i] : cacc[i + 4], keep = up ? cacc[i + 4] : cacc[i];
-        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const bool up = lane & 4;
-        const double send = up ? cacc[i] : cacc[i + 2], keep = up ? cacc[i + 2] : cacc[i];
-        cacc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-      }
-      {
-        const bool up = lane & 2;
-        const double send = up ? cacc[0] : cacc[1], keep = up ? cacc[1] : cacc[0];
-        cacc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-      }
-      cacc[0] += __shfl_xor_sync(0xffffffffu, cacc[0], 1);
-      const int jc = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-      if ((lane & 1) == 0) colp[half][16 * cq + jc] = cacc[0];
+      // the 16 column sums over the warp's 32 rows: 16 shuffles
+      const double cs = warp_reduce_scatter<16>(cacc, lane);
+      const int jc = reduce_scatter_index<16>(lane);
+      if (reduce_scatter_writer<16>(lane)) colp[half][16 * cq + jc] = cs;
       __syncthreads();
       if (t < kSy) pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * kSy + t] = colp[0][t] + colp[1][t];
       __syncthreads();
