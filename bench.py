@@ -61,20 +61,20 @@ def parse():
     ap.add_argument("--eval-fields", type=int, default=50, help="learned64: held-out fields (seeds 2000+)")
     ap.add_argument("--feti-precond", type=int, default=2,
                     help="fetidp64: 2 deluxe (FP64 blocks), 3 deluxe with FP32 blocks (mixed precision)")
-    ap.add_argument("--ns-train-fields", type=int, default=12,
-                    help="cube64 north-star comparison: training fields of the learned preconditioner")
-    ap.add_argument("--ns-eval-fields", type=int, default=3,
-                    help="cube64 north-star comparison: held-out fields of the learned preconditioner")
-    ap.add_argument("--ns-batch-instances", type=int, default=512,
-                    help="cube64 north-star comparison: instances of the batched many-instance run (0 skips it)")
+    ap.add_argument("--cmp-train-fields", type=int, default=12,
+                    help="cube64 metric comparison: training fields of the learned preconditioner")
+    ap.add_argument("--cmp-eval-fields", type=int, default=3,
+                    help="cube64 metric comparison: held-out fields of the learned preconditioner")
+    ap.add_argument("--cmp-batch-instances", type=int, default=512,
+                    help="cube64 metric comparison: instances of the batched many-instance run (0 skips it)")
     ap.add_argument("--feti-variants", default=",".join(["fp64", "fp32_precond", "tf32_factor"]),
-                    help="cube64 north-star comparison: FETI-DP variants to time (comma-separated)")
+                    help="cube64 metric comparison: FETI-DP variants to time (comma-separated)")
     ap.add_argument("--mixed", action="store_true",
                     help="fetidp64: mixed-precision factor (TF32 tensor-core contractions, FP64 refinement)")
     ap.add_argument("--instances", type=int, default=512, help="batch512: number of instances")
     ap.add_argument("--no-oracle", action="store_true",
                     help="cube64: skip the full-size FP64 oracle check after the timed region")
-    ap.add_argument("--no-north-star", action="store_true",
+    ap.add_argument("--no-comparison", action="store_true",
                     help="cube64: skip the 64-subdomain FETI-DP comparison of the default line")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="ITERS",
                     help="profiling mode: assemble once, then launch ITERS plain CG iterations "
@@ -466,8 +466,8 @@ def run_ours(args, rank, world, local_rank):
         line["config"]["oracle"] = oracle_check_plain(csys, x_tol, x_tight, tight_iters)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, m, l2g, n_dofs, iters, csys)
-    if rank == 0 and not args.no_north_star and args.workload == "cube64" and args.n == 64:
-        line["config"]["north_star"] = north_star(args, local_rank)
+    if rank == 0 and not args.no_comparison and args.workload == "cube64" and args.n == 64:
+        line["config"]["comparison"] = metric_comparison(args, local_rank)
     return line
 
 
@@ -789,7 +789,7 @@ def pcg_same_gauge(m, l2g, n_dofs, tols, dev):
     return out, sols
 
 
-def north_star(args, local_rank):
+def metric_comparison(args, local_rank):
     """The metric's own comparison on the 64-subdomain configuration: the
     64^3 plain-at-scale problem split into 4^3 jittered boxes (seed
     20261203), partition tree gauge, time to a true FP64 relative residual of
@@ -822,10 +822,10 @@ def north_star(args, local_rank):
     orp, ocol, okv, _, orhs = O.assemble(m, fd.map.l2g, n_dofs)
     r = orhs - O.spmv(orp, ocol, okv, x_feti)
     del fd
-    learned = north_star_learned(args, local_rank) if args.ns_train_fields > 0 else None
+    learned = comparison_learned(args, local_rank) if args.cmp_train_fields > 0 else None
     batched = None
-    if args.ns_batch_instances > 0:  # the batched many-instance addition, reduced to 2 timed steps
-        n_b = args.ns_batch_instances
+    if args.cmp_batch_instances > 0:  # the batched many-instance addition, reduced to 2 timed steps
+        n_b = args.cmp_batch_instances
         _, batched = batch_measure(n_b, steps=2, warmup=1, local_rank=local_rank, plain_stride=max(1, n_b // 16),
                                    oracle_stride=max(1, n_b // 16))
     plain_fetidp = var["fp64"]["ms"]
@@ -853,11 +853,11 @@ def north_star(args, local_rank):
     }
 
 
-def north_star_learned(args, local_rank):
+def comparison_learned(args, local_rank):
     """The learned interface preconditioner on its own configuration (64^3,
     64 jittered boxes, random log-normal mu_r fields, curl-T sources), with a
     reduced training set so that it fits the default run: training pairs from
-    `ns_train_fields` fields (seeds 1000+), 20 epochs, then `ns_eval_fields`
+    `cmp_train_fields` fields (seeds 1000+), 20 epochs, then `cmp_eval_fields`
     held-out fields (seeds 2000+) solved with deluxe alone and deluxe +
     learned (flexible CG) to a true residual of 1e-8."""
     import torch
@@ -866,7 +866,7 @@ def north_star_learned(args, local_rank):
     t0 = time.perf_counter()
     tr = learned.Trainer(n=64, parts=4, seed=1)
     R, T = [], []
-    for k in range(args.ns_train_fields):
+    for k in range(args.cmp_train_fields):
         r, t = tr.pairs(np.random.default_rng(1000 + k), per_solve=8, stride=3)
         R += r
         T += t
@@ -874,14 +874,14 @@ def north_star_learned(args, local_rank):
     torch.cuda.synchronize()
     prep_ms = (time.perf_counter() - t0) * 1e3
     rows = []
-    for k in range(args.ns_eval_fields):
+    for k in range(args.cmp_eval_fields):
         o = tr.evaluate(np.random.default_rng(2000 + k), tol=TOL)
         rows.append((o[2]["iterations"], o[4]["iterations"], o[2]["ms"], o[4]["ms"], o[2]["residual"],
                      o[4]["residual"], o[2]["status"], o[4]["status"]))
     a = np.array(rows, dtype=float)
     return {"what": "deluxe vs deluxe + learned MLP correction (flexible CG), random mu_r fields; reduced training "
                     "set (the learned64 workload trains on 200 fields)",
-            "train_fields": args.ns_train_fields, "pairs": len(R), "eval_fields": args.ns_eval_fields,
+            "train_fields": args.cmp_train_fields, "pairs": len(R), "eval_fields": args.cmp_eval_fields,
             "prep_ms": prep_ms, "loss_first_last": [losses[0], losses[-1]],
             "iterations_mean": {"deluxe": a[:, 0].mean(), "deluxe_plus_learned": a[:, 1].mean()},
             "solve_ms_mean": {"deluxe": a[:, 2].mean(), "deluxe_plus_learned": a[:, 3].mean()},
