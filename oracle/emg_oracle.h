@@ -2,8 +2,8 @@
  * emg_oracle.h -- CPU oracle for the TET4 / HEX8 Nedelec curl-curl solve path.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
- * algorithm (Poofee/emagddm) used as the checker for the CUDA product path and
- * as the CPU baseline in bench.py.  Nothing in the product library links,
+ * algorithm (Poofee/emagddm): the tests compare the CUDA product path with it,
+ * and bench.py times it as the CPU baseline.  Nothing in the product library links,
  * loads or calls it.
  *
  * Parity anchors:

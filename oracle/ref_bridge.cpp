@@ -1,6 +1,6 @@
 // ref_bridge.cpp -- TEST INFRASTRUCTURE: a thin extern "C" wrapper that links
 // the reference's own C++ sources (compiled in place by Makefile.ref, outputs
-// only into oracle/_ref/) so tests can compare this build's integer outputs
+// only into oracle/_ref/) so tests can compare this library's integer outputs
 // and solver behaviour with the reference itself, and so bench.py can time the
 // reference's CPU solver.  It calls only the reference's public API:
 //   GlobalEdgeIDGenerator::generate      (src/fe_em/global_edge_id_generator.cpp:30)

@@ -1,5 +1,5 @@
-"""Shared helpers of the GPU parity tests (product path through the C ABI,
-oracle as the checker)."""
+"""Shared helpers of the GPU parity tests (the product path through the C ABI,
+compared with the oracle)."""
 import ctypes as C
 
 import numpy as np
