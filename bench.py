@@ -739,10 +739,13 @@ def fetidp_variants(fd, names, steps, warmup, stream, dev):
             res[name] = {"what": what, "failed": failed}
             continue
         its = max(int(st["iterations"]), 1)
-        # dense blocks read per multiplier iteration: L^-1 (lower, then upper
-        # mirror: the whole n_D^2 block once) and S_DD (whole block; FP32
-        # copies with the FP32 preconditioner)
-        nb = fd.info()["dual_block_doubles"] * (8 + (4 if precond == 3 else 8))
+        # dense blocks read per multiplier iteration: L^-1 (lower part, then
+        # the stored transpose: the whole n_D^2 block once), the S_DD tiles on
+        # and below the diagonal and the four deluxe blocks of every face
+        # (FP32 copies of both with the FP32 preconditioner)
+        fi = fd.info()
+        pw = 4 if precond == 3 else 8
+        nb = fi["dual_block_doubles"] * 8 + fi["sym_tile_doubles"] * pw + 4 * fi["face_block_doubles"] * pw
         peak, _ = measured_peak()
         per_it = st["lambda_ms"] / its
         res[name] = {"what": what, "ms": statistics.mean(per), "ms_steps": [round(v, 3) for v in per],

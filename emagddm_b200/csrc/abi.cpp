@@ -161,7 +161,7 @@ int csr_from_device(int64_t n, int64_t nnz, const int32_t* rp, const int32_t* co
 }
 
 void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
-  int64_t v[20] = {0};
+  int64_t v[22] = {0};
   v[0] = p.n_parts;
   v[1] = p.n_dofs;
   v[2] = p.n_union;
@@ -198,7 +198,19 @@ void feti_info(const emg::FetiPlan& p, int64_t* info, int32_t n) {
   v[17] = static_cast<int64_t>(panel);
   v[18] = static_cast<int64_t>(syrk);
   v[19] = static_cast<int64_t>(other);
-  for (int32_t i = 0; i < n && i < 20; ++i) info[i] = v[i];
+  // entries of the S_DD blocks the symmetric products read (the 64 x 64
+  // tiles on and below the diagonal) and of the deluxe face blocks (one of
+  // each face's four n_F x n_F blocks)
+  for (int32_t s = 0; s < p.n_parts; ++s) {
+    const int64_t n = p.nD[s], nb = (n + 63) / 64;
+    for (int64_t I = 0; I < nb; ++I)
+      for (int64_t J = 0; J <= I; ++J) v[20] += std::min<int64_t>(64, n - 64 * I) * std::min<int64_t>(64, n - 64 * J);
+  }
+  for (int32_t f = 0; f < p.n_faces; ++f) {
+    const int64_t m = p.face_ptr[f + 1] - p.face_ptr[f];
+    v[21] += m * m;
+  }
+  for (int32_t i = 0; i < n && i < 22; ++i) info[i] = v[i];
 }
 
 // A DOF map viewed as one subdomain (the direct solver's plan).

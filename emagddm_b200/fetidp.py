@@ -83,7 +83,8 @@ def partitioned_dofmap(m, tet_part, n_parts: int, keep_handles: bool = False):
 
 INFO_KEYS = ("n_parts", "n_dofs", "n_union", "n_lambda", "n_coarse", "n_fronts", "n_levels", "max_front",
              "max_pivots", "factor_doubles", "update_pool_doubles", "dual_block_doubles", "sum_nI", "sum_nD",
-             "sum_nP", "max_nD", "max_children", "flops_panel", "flops_update", "flops_dense")
+             "sum_nP", "max_nD", "max_children", "flops_panel", "flops_update", "flops_dense",
+             "sym_tile_doubles", "face_block_doubles")
 STATS_KEYS = ("factor_ms", "solve_ms", "iterations", "lambda_residual", "residual", "passes", "lambda_ms",
               "fronts_ms")
 

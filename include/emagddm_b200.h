@@ -317,11 +317,14 @@ int emg_fetidp_lambda_rhs(emg_fetidp fd, const double* b_d, double* rhs_d);
  * and lam_entry (2 per multiplier: its + and - entries).  NULL skips. */
 int emg_fetidp_duals(emg_fetidp fd, int64_t* dual_off, int32_t* dual_lam, int32_t* dual_sign, int32_t* lam_entry);
 
-/* info[0..19]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
+/* info[0..21]: n_parts, n_dofs, n_union, n_lambda, n_coarse, n_fronts,
  * n_levels, max_front, max_pivots, factor doubles, update-pool doubles,
- * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children, and the
- * flops of the numeric phase: front panels, front update blocks, inverse
- * factors + deluxe weights. */
+ * dual-block doubles, sum nI, sum nD, sum nP, max nD, max children, the
+ * flops of the numeric phase (front panels, front update blocks, inverse
+ * factors + deluxe weights), the S_DD entries the preconditioner reads a
+ * multiplier iteration (64 x 64 tiles on and below the diagonal) and the
+ * entries of one of each face's four deluxe blocks.  A shorter n_info
+ * returns the first n_info values. */
 int emg_fetidp_info(emg_fetidp fd, int64_t* info, int32_t n_info);
 /* stats[0..7]: factor ms, solve ms, iterations, multiplier residual, true
  * residual, FETI-DP passes, and the solve's device ms split into the
