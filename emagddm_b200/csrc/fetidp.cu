@@ -1319,9 +1319,10 @@ __global__ void __launch_bounds__(512) k_block_colgemv(int32_t n_mat, const int3
 // I, thread (r, cq) = (t & 63, t >> 6); for each tile S_IJ (J <= I) it adds
 // S_IJ w_J into row r over the columns of quarter cq (the row sums, four
 // partials added in fixed order at the end, are written to y) and, for
-// J < I, forms the column sums S_IJ^T w_I (a butterfly over the warp, two
-// halves in fixed order) into the tile's slot of pc.  k_symv_cols: y_J += the column sums of
-// the tiles below block J, in ascending I.  Deterministic.
+// J < I, forms the column sums S_IJ^T w_I (a butterfly over the warp) into
+// its warp's half of the tile's slot of pc.  k_symv_cols: y_J += the column
+// sums of the tiles below block J (ascending I, the two halves of each slot
+// in order).  Deterministic.
 constexpr int kSy = 64;
 template <class T>
 __global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t* __restrict__ dim,
@@ -1330,7 +1331,6 @@ __global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t*
                                                    const double* __restrict__ w, double* __restrict__ y,
                                                    double* __restrict__ pc) {
   __shared__ double rowp[4][kSy];
-  __shared__ double colp[2][kSy];
   const int32_t m = blockIdx.y;
   if (m >= n_mat) return;
   const int32_t n = dim[m], nb = (n + kSy - 1) / kSy;
@@ -1353,13 +1353,12 @@ __global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t*
       cacc[j] = v * wr;
     }
     if (J < I) {
-      // the 16 column sums over the warp's 32 rows: 16 shuffles
+      // the 16 column sums over the warp's 32 rows (16 shuffles), written to
+      // this warp's half of the tile's slot: no barrier inside the tile loop
       const double cs = warp_reduce_scatter<16>(cacc, lane);
       const int jc = reduce_scatter_index<16>(lane);
-      if (reduce_scatter_writer<16>(lane)) colp[half][16 * cq + jc] = cs;
-      __syncthreads();
-      if (t < kSy) pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * kSy + t] = colp[0][t] + colp[1][t];
-      __syncthreads();
+      if (reduce_scatter_writer<16>(lane))
+        pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * (2 * kSy) + half * kSy + 16 * cq + jc] = cs;
     }
   }
   rowp[cq][r] = racc;
@@ -1377,7 +1376,10 @@ __global__ void k_symv_cols(int32_t n_mat, const int32_t* __restrict__ dim, cons
   const int32_t J = blockIdx.x, c = threadIdx.x;
   if (J >= nb || J * kSy + c >= n) return;
   double acc = 0.0;
-  for (int32_t I = J + 1; I < nb; ++I) acc += pc[pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * kSy + c];
+  for (int32_t I = J + 1; I < nb; ++I) {
+    const double* slot = pc + pc_off[m] + (static_cast<int64_t>(I) * (I - 1) / 2 + J) * (2 * kSy);
+    acc += slot[c] + slot[kSy + c];
+  }
   y[v_off[m] + J * kSy + c] += acc;
 }
 
@@ -2110,7 +2112,7 @@ int FetiDP::setup_device() {
     std::vector<int64_t> pcoff(rdim.size() + 1, 0);
     for (size_t q = 0; q < rdim.size(); ++q) {
       const int64_t nb = (rdim[q] + kSy - 1) / kSy;
-      pcoff[q + 1] = pcoff[q] + nb * (nb - 1) / 2 * kSy;
+      pcoff[q + 1] = pcoff[q] + nb * (nb - 1) / 2 * (2 * kSy);
     }
     if ((rc = up(&d_pcoff, pcoff)) || (rc = zalloc(&pc_d, std::max<int64_t>(pcoff.back(), 1)))) return rc;
   }
