@@ -1327,7 +1327,8 @@ constexpr int kSy = 64;
 template <class T>
 __global__ void __launch_bounds__(256) k_symv_rows(int32_t n_mat, const int32_t* __restrict__ dim,
                                                    const int64_t* __restrict__ m_off, const T* __restrict__ M,
-                                                   const int64_t* __restrict__ v_off, const int64_t* __restrict__ pc_off,
+                                                   const int64_t* __restrict__ v_off,
+                                                   const int64_t* __restrict__ pc_off,
                                                    const double* __restrict__ w, double* __restrict__ y,
                                                    double* __restrict__ pc) {
   __shared__ double rowp[4][kSy];
@@ -1629,11 +1630,12 @@ __global__ void __launch_bounds__(kTileThreads) k_face_gemm_nt(FacesDev Fc, cons
 }
 
 // w[e_i] = sum_j D[i, j] sign r[lam_j] for every face side (side = blockIdx.y & 1),
-// as column dots over the stored transposes DT (one warp per i, eight rows a
+// as column dots over the stored transposes DT (a warp per row i, 32 rows a
 // CTA).  The face's gathered vector is staged once per CTA in shared memory
 // (dynamic, the largest face's size, when that fits in 48 KB), so a row's
 // dot reads only its column.
 constexpr int32_t kFaceStaged = 6144;  // faces up to this size stage their vector (48 KB)
+constexpr int32_t kFaceRows = 32;      // rows of a face block per CTA (four a warp), sharing one staging
 template <class T>
 __device__ __forceinline__ double face_dot(const T* __restrict__ Dt, const double* __restrict__ v, int32_t n,
                                            int lane) {
@@ -1656,25 +1658,26 @@ __global__ void __launch_bounds__(256) k_face_w(FacesDev Fc, const int32_t* __re
   extern __shared__ double fv[];
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
-  const int32_t i0 = blockIdx.x * (blockDim.x >> 5);
+  const int32_t i0 = blockIdx.x * kFaceRows;
   if (i0 >= n) return;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
-  const int32_t i = i0 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  const T* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
-  double acc;
   if (kStaged) {
     for (int32_t j = threadIdx.x; j < n; j += blockDim.x) fv[j] = r[lam[j]];
     __syncthreads();
-    if (i >= n) return;
-    acc = face_dot(Dt, fv, n, lane);
-  } else {
-    if (i >= n) return;
-    double a = 0.0;
-    for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(Dt[j]), r[lam[j]], a);
-    acc = warp_sum(a);
   }
-  if (lane == 0) w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
+  for (int32_t i = i0 + (threadIdx.x >> 5); i < min(n, i0 + kFaceRows); i += blockDim.x >> 5) {
+    const T* Dt = (side ? DbT : DaT) + Fc.off[f] + static_cast<int64_t>(i) * n;
+    double acc;
+    if (kStaged) {
+      acc = face_dot(Dt, fv, n, lane);
+    } else {
+      double a = 0.0;
+      for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(Dt[j]), r[lam[j]], a);
+      acc = warp_sum(a);
+    }
+    if (lane == 0) w[lam_entry[2 * lam[i] + side]] = side ? -acc : acc;
+  }
 }
 
 // c[e_i] = sum_j D[j, i] y[e_j] (column dot, one warp per i), the face's
@@ -1686,25 +1689,26 @@ __global__ void __launch_bounds__(256) k_face_c(FacesDev Fc, const int32_t* __re
   extern __shared__ double fv[];
   const int32_t f = blockIdx.y >> 1, side = blockIdx.y & 1;
   const int32_t n = Fc.dim[f];
-  const int32_t i0 = blockIdx.x * (blockDim.x >> 5);
+  const int32_t i0 = blockIdx.x * kFaceRows;
   if (i0 >= n) return;
   const int32_t* lam = Fc.lam + Fc.ptr[f];
-  const int32_t i = i0 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  const T* D = (side ? Db : Da) + Fc.off[f] + static_cast<int64_t>(i) * n;
-  double acc;
   if (kStaged) {
     for (int32_t j = threadIdx.x; j < n; j += blockDim.x) fv[j] = y[lam_entry[2 * lam[j] + side]];
     __syncthreads();
-    if (i >= n) return;
-    acc = face_dot(D, fv, n, lane);
-  } else {
-    if (i >= n) return;
-    double a = 0.0;
-    for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(D[j]), y[lam_entry[2 * lam[j] + side]], a);
-    acc = warp_sum(a);
   }
-  if (lane == 0) c[lam_entry[2 * lam[i] + side]] = acc;
+  for (int32_t i = i0 + (threadIdx.x >> 5); i < min(n, i0 + kFaceRows); i += blockDim.x >> 5) {
+    const T* D = (side ? Db : Da) + Fc.off[f] + static_cast<int64_t>(i) * n;
+    double acc;
+    if (kStaged) {
+      acc = face_dot(D, fv, n, lane);
+    } else {
+      double a = 0.0;
+      for (int32_t j = lane; j < n; j += 32) a = fma(static_cast<double>(D[j]), y[lam_entry[2 * lam[j] + side]], a);
+      acc = warp_sum(a);
+    }
+    if (lane == 0) c[lam_entry[2 * lam[i] + side]] = acc;
+  }
 }
 
 template <class T>
@@ -2457,20 +2461,17 @@ void FetiDP::apply_M(const double* r, double* z, double* part) {
   const dim3 gr(static_cast<unsigned>((max_nD + gemv_warps - 1) / gemv_warps), static_cast<unsigned>(n_roots));
   if (precond >= 2 && P.n_faces > 0) {  // 4: the Dirichlet part of deluxe + learned
     const unsigned nfs = static_cast<unsigned>(2 * P.n_faces);
+    const unsigned gf = static_cast<unsigned>((max_fdim + kFaceRows - 1) / kFaceRows);
     if (precond == 3) {
-      launch_face_w<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDaT32_d,
-                           fDbT32_d, r, w_d);
+      launch_face_w<float>(gf, nfs, max_fdim, st, fc, d_lam_entry, fDaT32_d, fDbT32_d, r, w_d);
       symv_roots(S32_d, w_d, y_d);
-      launch_face_c<float>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa32_d,
-                           fDb32_d, y_d, c_d);
+      launch_face_c<float>(gf, nfs, max_fdim, st, fc, d_lam_entry, fDa32_d, fDb32_d, y_d, c_d);
       k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
       return;
     }
-    launch_face_w<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fX_d, fXt_d,
-                          r, w_d);
+    launch_face_w<double>(gf, nfs, max_fdim, st, fc, d_lam_entry, fX_d, fXt_d, r, w_d);
     symv_roots(S_d, w_d, y_d);
-    launch_face_c<double>(static_cast<unsigned>((max_fdim + 7) / 8), nfs, max_fdim, st, fc, d_lam_entry, fDa_d, fDb_d,
-                          y_d, c_d);
+    launch_face_c<double>(gf, nfs, max_fdim, st, fc, d_lam_entry, fDa_d, fDb_d, y_d, c_d);
     k_lambda_scatter<<<kParts, 256, 0, st>>>(P.n_lambda, d_lam_entry, nullptr, c_d, z, r, part);
     return;
   }
