@@ -2546,16 +2546,18 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
   int rc = system_assemble(un, nu, sigma, n_mat, src, n_src, flags & ~EMG_FLAG_MASS, st);
   if (rc) return rc;
   // The numeric factorization after the union assembly is the same launch
-  // sequence for every factorization of this plan: the first one runs
-  // eagerly (and the autotuner fixes the solve kernels' widths after it),
-  // the second is captured as one CUDA graph, later ones replay it.  While
-  // capturing, the breakdown checks are deferred to one read at the end.
+  // sequence for every factorization of this plan and kind (FP64 or TF32
+  // contractions): the first of a kind runs eagerly (it also sets the
+  // kernels' shared-memory limits, which a capture cannot; the autotuner
+  // fixes the solve kernels' widths after the first one), the second is
+  // captured as one CUDA graph, later ones replay it.  While capturing, the
+  // breakdown checks are deferred to one read at the end.
   static const bool graph_off = [] {
     const char* e = std::getenv("EMG_FETI_GRAPH");
     return e && e[0] == '0';
   }();
   cudaGraphExec_t& fg = fac_exec[tc_factor ? 1 : 0];
-  if (!graph_off && !fac_graph_failed && tuned && !fg) {
+  if (!graph_off && !fac_graph_failed && tuned && fac_eager[tc_factor ? 1 : 0] && !fg) {
     if (!cap_st && cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
       fac_graph_failed = true;
@@ -2587,6 +2589,7 @@ int FetiDP::factor(const double* nu, const double* sigma, int32_t n_mat, const e
     rc = check_err("FETI-DP factorization (subdomain, coarse or face matrices)");
   } else {
     rc = factor_device();
+    if (!rc) fac_eager[tc_factor ? 1 : 0] = true;
   }
   if (rc) return rc;
   EMG_CK(cudaGetLastError());

@@ -139,6 +139,7 @@ struct FetiDP {
   bool graph_failed = false;
   // the numeric factorization as one graph per factor mode (FP64, mixed)
   cudaGraphExec_t fac_exec[2] = {nullptr, nullptr};
+  bool fac_eager[2] = {false, false};  // a factorization of this kind (FP64 / TF32) has run eagerly
   bool fac_graph_failed = false;
   bool capturing = false;  // a capture is recording: defer checks, no attribute calls
   static constexpr int kParts = 592;

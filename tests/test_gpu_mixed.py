@@ -96,3 +96,24 @@ def test_mixed_factor_direct_matches_oracle(n):
     assert out.residual_norm <= 1e-12
     xo = _monolithic(m, ds.l2g)
     assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+
+
+def test_factor_kinds_alternate_with_graph_replay():
+    """FP64 and TF32 factorizations alternating on one solver: each kind runs
+    eagerly once before it is captured as a graph (its kernels' shared-memory
+    limits are set by the eager run), so no capture fails and every
+    factorization gives the solution of its kind bit for bit."""
+    m = mesh.plain_scale(8)
+    part = mesh.jittered_partition(m, 2)
+    fd = fetidp.FetiDP(m, part, 8)
+    xs = {0: [], FLAG_TF32: []}
+    for flags in (0, 0, FLAG_TF32, FLAG_TF32, 0, FLAG_TF32):
+        assert fd.factor(flags=flags) == _abi.EMG_SUCCESS, lib().emg_last_error()
+        assert b"capture" not in lib().emg_last_error()
+        x, rc, _ = fd.solve(tol=1e-11, max_iter=5000)
+        assert rc == _abi.EMG_SUCCESS, (rc, lib().emg_last_error())
+        xs[flags].append(x)
+    for kind in xs.values():
+        for x in kind[1:]:
+            np.testing.assert_array_equal(x, kind[0])
+    assert np.linalg.norm(xs[FLAG_TF32][0] - xs[0][0]) <= 1e-8 * np.linalg.norm(xs[0][0])
