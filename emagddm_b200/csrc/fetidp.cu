@@ -1271,8 +1271,11 @@ __global__ void __launch_bounds__(512) k_block_colgemv(int32_t n_mat, const int3
   const int32_t m = blockIdx.y;
   if (m >= n_mat) return;
   const int32_t n = dim[m];
-  const int32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (c >= n) return;
+  // range 0 reads rows 0..c: the longest columns come last, so they are
+  // handed out first (no tail of long columns)
+  const int32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= n) return;
+  const int32_t c = range == 0 ? n - 1 - q : q;
   const int lane = threadIdx.x & 31;
   const int64_t col0 = m_off[m] + static_cast<int64_t>(c) * n;  // element index of the column start
   const T* Mc = M + col0;
