@@ -1030,18 +1030,15 @@ __global__ void __launch_bounds__(kPivMax) k_front_bwd_piv(FrontsDev F, int32_t 
 // column group, and the small CTAs keep many fronts in flight where the wide
 // pivot-block CTAs would idle on the panel chain.
 constexpr int kMidMaxF = 1024;
-constexpr int kMidCols = 8;  // columns per CTA of the multi-column variant
-template <int kC>
-constexpr int mid_threads() { return kC == 1 ? 128 : 256; }
+constexpr int kMidCols = 8;     // columns per CTA of the multi-column variant
 template <int kC>
 size_t mid_smem(int32_t max_f) { return sizeof(double) * (static_cast<size_t>(kC) * max_f + kC * kSB); }
 
-template <int kC>
-__global__ void __launch_bounds__(mid_threads<kC>()) k_front_fwd_mid(FrontsDev F, int32_t f0, RhsDev R,
+template <int kC, int kT>
+__global__ void __launch_bounds__(kT) k_front_fwd_mid(FrontsDev F, int32_t f0, RhsDev R,
                                                                      const int32_t* __restrict__ nI,
                                                                      const int32_t* __restrict__ nD,
                                                                      const double* __restrict__ fac, int32_t ldx) {
-  constexpr int kT = mid_threads<kC>();
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
@@ -1115,12 +1112,11 @@ __global__ void __launch_bounds__(mid_threads<kC>()) k_front_fwd_mid(FrontsDev F
   }
 }
 
-template <int kC>
-__global__ void __launch_bounds__(mid_threads<kC>()) k_front_bwd_mid(FrontsDev F, int32_t f0, RhsDev R,
+template <int kC, int kT>
+__global__ void __launch_bounds__(kT) k_front_bwd_mid(FrontsDev F, int32_t f0, RhsDev R,
                                                                      const int32_t* __restrict__ nI,
                                                                      const int32_t* __restrict__ nD,
                                                                      const double* __restrict__ fac, int32_t ldx) {
-  constexpr int kT = mid_threads<kC>();
   const int32_t k = f0 + blockIdx.y;
   if (F.is_root[k]) return;
   const int32_t s = F.sub[k];
@@ -2340,23 +2336,28 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   const unsigned nc = static_cast<unsigned>(ncol);
   const unsigned ngroups = static_cast<unsigned>((ncol + kColB - 1) / kColB);
   const unsigned ngroups_mid = static_cast<unsigned>((ncol + kMidCols - 1) / kMidCols);
-  if (mid_fronts && !capturing && ncol > 1)  // up to 8 x 1024 doubles of front columns a CTA
-    EMG_CK(cudaFuncSetAttribute(k_front_fwd_mid<kMidCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // the autotuner's choices are timed on single-column passes and apply to
+  // them; multi-column solves (the coarse basis inside the factorization)
+  // always take the fused kernels on the medium levels, so a factorization's
+  // results do not depend on when the tuner ran
+  const bool use_mid = ncol > 1 || mid_fronts;
+  if (!capturing && ncol > 1)  // up to 8 x 1024 doubles of front columns a CTA
+    EMG_CK(cudaFuncSetAttribute(k_front_fwd_mid<kMidCols, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(mid_smem<kMidCols>(kMidMaxF))));
-  if (mid_fronts && !capturing && ncol > 1)
-    EMG_CK(cudaFuncSetAttribute(k_front_bwd_mid<kMidCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (!capturing && ncol > 1)
+    EMG_CK(cudaFuncSetAttribute(k_front_bwd_mid<kMidCols, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(mid_smem<kMidCols>(kMidMaxF))));
   for (int32_t h = 0; h < nlev; ++h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0) continue;  // (a front without pivots still gathers its children)
-    if (mid_fronts && lvl_max_f[h] <= kMidMaxF) {
+    if (use_mid && lvl_max_f[h] <= kMidMaxF) {
       const int32_t ldx = std::max(lvl_max_f[h], 1);
       if (ncol == 1)
-        k_front_fwd_mid<1><<<dim3(1, static_cast<unsigned>(nf)), mid_threads<1>(), mid_smem<1>(ldx), st>>>(
+        k_front_fwd_mid<1, 128><<<dim3(1, static_cast<unsigned>(nf)), 128, mid_smem<1>(ldx), st>>>(
             fd, f0, R, d_nI, d_nD, fac_d, ldx);
       else
-        k_front_fwd_mid<kMidCols><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), mid_threads<kMidCols>(),
-                                    mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
+        k_front_fwd_mid<kMidCols, 256><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), 256,
+                                         mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
       continue;
     }
     k_front_fwd_piv<<<dim3(nc, static_cast<unsigned>(nf)), piv_threads, 0, st>>>(fd, f0, R, d_nI, d_nD, fac_d);
@@ -2381,14 +2382,14 @@ int FetiDP::solve_fronts(const RhsDev& R, int32_t ncol) {
   for (int32_t h = nlev - 1; h >= 0; --h) {
     const int32_t f0 = plan.level_ptr[h], nf = plan.level_ptr[h + 1] - f0;
     if (nf == 0 || lvl_max_np[h] == 0) continue;
-    if (mid_fronts && lvl_max_f[h] <= kMidMaxF) {
+    if (use_mid && lvl_max_f[h] <= kMidMaxF) {
       const int32_t ldx = std::max(lvl_max_f[h], 1);
       if (ncol == 1)
-        k_front_bwd_mid<1><<<dim3(1, static_cast<unsigned>(nf)), mid_threads<1>(), mid_smem<1>(ldx), st>>>(
+        k_front_bwd_mid<1, 128><<<dim3(1, static_cast<unsigned>(nf)), 128, mid_smem<1>(ldx), st>>>(
             fd, f0, R, d_nI, d_nD, fac_d, ldx);
       else
-        k_front_bwd_mid<kMidCols><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), mid_threads<kMidCols>(),
-                                    mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
+        k_front_bwd_mid<kMidCols, 256><<<dim3(ngroups_mid, static_cast<unsigned>(nf)), 256,
+                                         mid_smem<kMidCols>(ldx), st>>>(fd, f0, R, d_nI, d_nD, fac_d, ldx);
       continue;
     }
     if (lvl_max_nu[h] > 0)
