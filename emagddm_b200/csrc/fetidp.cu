@@ -1947,6 +1947,9 @@ void FetiDP::release() {
   for (cudaGraphExec_t& g : fac_exec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   if (cap_st) { cudaStreamDestroy(cap_st); cap_st = nullptr; }
+  if (side_st) { cudaStreamDestroy(side_st); side_st = nullptr; }
+  if (ev_fork) { cudaEventDestroy(ev_fork); ev_fork = nullptr; }
+  if (ev_join) { cudaEventDestroy(ev_join); ev_join = nullptr; }
   for (void* p : dev) cudaFree(p);
   dev.clear();
 }
@@ -2652,6 +2655,28 @@ int FetiDP::factor_device() {
   }
   if (!rc && !capturing) rc = check_err("FETI-DP factorization");
   if (rc) return rc;
+  // In the captured factorization the deluxe face set-up, which reads only
+  // the assembled S_DD blocks and writes its own buffers, runs on a second
+  // stream beside the root inverse factors, the coarse basis and the coarse
+  // factor (the GPU is far from full during their chains); the breakdown
+  // flag is only OR-ed there, and the join comes before the capture ends.
+  const bool side = capturing && P.dual_off[S] > 0 && P.n_faces > 0;
+  if (side) {
+    if (!side_st && cudaStreamCreateWithFlags(&side_st, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("FETI-DP: cannot create the face set-up stream");
+      return EMG_ERR_CUDA;
+    }
+    if (!ev_fork) EMG_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (!ev_join) EMG_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    EMG_CK(cudaEventRecord(ev_fork, st));
+    EMG_CK(cudaStreamWaitEvent(side_st, ev_fork, 0));
+    const cudaStream_t main_st = st;
+    st = side_st;
+    rc = setup_deluxe();
+    st = main_st;
+    if (rc) return rc;
+    EMG_CK(cudaEventRecord(ev_join, side_st));
+  }
   if (n_roots > 0) {
     rc = trtri(n_roots, max_nD, d_rdim, d_rfac, d_roff, Linv_d);  // L^-1 with L^-T above the diagonal
     if (rc) return rc;
@@ -2686,9 +2711,12 @@ int FetiDP::factor_device() {
     k_dual_weights<<<blocks_for(ne, 256), 256, 0, st>>>(d_loc_off, d_nI, d_dual_off, d_dual_lam, d_dual_sign,
                                                          d_lam_entry, d_dual_sub, rp, cl, vl, ne, rho_d, wt_d, 1);
     k_to_f32<<<blocks_for(P.root_off[S], 256), 256, 0, st>>>(P.root_off[S], S_d, S32_d);
-    rc = setup_deluxe();
-    if (rc) return rc;
+    if (!side) {
+      rc = setup_deluxe();
+      if (rc) return rc;
+    }
   }
+  if (side) EMG_CK(cudaStreamWaitEvent(st, ev_join, 0));
   EMG_CK(cudaGetLastError());
   return EMG_SUCCESS;
 }

@@ -136,6 +136,11 @@ struct FetiDP {
   // device-side multiplier loop: one while-loop graph per preconditioner 0..3
   cudaGraphExec_t lam_exec[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaStream_t cap_st = nullptr;
+  // second stream of the captured factorization: the deluxe face set-up
+  // (which needs only the assembled S_DD blocks) beside the root inverse
+  // factors and the coarse basis
+  cudaStream_t side_st = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool graph_failed = false;
   // the numeric factorization as one graph per factor mode (FP64, mixed)
   cudaGraphExec_t fac_exec[2] = {nullptr, nullptr};
